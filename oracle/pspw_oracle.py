@@ -1,0 +1,434 @@
+"""TEST INFRASTRUCTURE -- CPU restatement of the reference hot path (the oracle).
+
+Only ``tests/``, ``__graft_entry__.smoke()`` and ``bench.py``'s CPU-baseline leg
+may import this module, and only as the checker; the product never calls it.
+
+Each function restates one reference routine of f-fathurrahman/ffr-pspw-dft-c in
+numpy/scipy FP64, citing the file:line it follows.  Arrays keep the reference's
+Fortran (column-major) layouts; complex arrays are complex128.
+
+A *cell* here is a dict with the basis and potential arrays the reference keeps
+in its globals (common_pspw.h:43-148) for one k-point (ik=1):
+
+    nr      (NR1, NR2, NR3)
+    n123    uint32[NGWX]     1-based linear FFT-grid index (GkVectorsGen.cpp:379)
+    xkg     float64[NGWX]    |k+G|^2 in (2pi/ALAT)^2 units
+    eigr    complex[NGWX, NAX, NSP]  (Fortran order)
+    pkg_a   float64[NLMAX, NGWX, NSP]
+    wnl     float64[NSP, NLMAX]
+    na      int[NSP]
+    lm_end  int[NSP]         L_MAX^2 - 2 L_LOC + 1  (ApplyHam_block.cpp:69)
+    tpiba2, alat, omega
+"""
+from __future__ import annotations
+
+import numpy as np
+import scipy.linalg.lapack as lapack
+
+# ---------------------------------------------------------------- FFT
+
+def _grid_view(flat, nr):
+    n1, n2, n3 = nr
+    return flat.reshape(n3, n2, n1)  # Fortran (i1,i2,i3) == C (i3,i2,i1)
+
+
+def fft_inverse(flat, nr):
+    """fft_fftw3.cpp:13-46, inverse=true: FFTW_BACKWARD (exponent +i), unscaled."""
+    g = _grid_view(flat, nr)
+    return (np.fft.ifftn(g) * g.size).reshape(-1)
+
+
+def fft_forward(flat, nr):
+    """fft_fftw3.cpp:13-46, inverse=false: FFTW_FORWARD (exponent -i), then 1/N."""
+    g = _grid_view(flat, nr)
+    return (np.fft.fftn(g) / g.size).reshape(-1)
+
+
+# ---------------------------------------------------------------- H*psi
+
+def projectors(cell, ngw):
+    """The KB projectors beta_p(G) = EIGR(G,a) * PKG_A(lm,G) and weights W_p,
+    enumerated species-major, then atom, then lm (ApplyHam_block.cpp:68-117).
+
+    Returns (beta[ngw, nproj] complex, w[nproj])."""
+    cols, ws = [], []
+    for s in range(len(cell["na"])):
+        for a in range(cell["na"][s]):
+            for lm in range(cell["lm_end"][s]):
+                cols.append(cell["eigr"][:ngw, a, s] * cell["pkg_a"][lm, :ngw, s])
+                ws.append(cell["wnl"][s, lm])
+    if not cols:
+        return np.zeros((ngw, 0), complex), np.zeros(0)
+    return np.stack(cols, axis=1), np.asarray(ws, dtype=float)
+
+
+def apply_ham_block(cell, vin, veff, nstates=None):
+    """ApplyHam_block.cpp:5-172.  vin: complex[ngw, nstates] (ld = ngw)."""
+    vin = np.asarray(vin, dtype=complex)
+    if vin.ndim == 1:
+        vin = vin[:, None]
+    ngw = vin.shape[0]
+    if nstates is None:
+        nstates = vin.shape[1]
+    nr = cell["nr"]
+    nnr = nr[0] * nr[1] * nr[2]
+    if veff.size != nnr:
+        raise ValueError("nnr != NNR")  # ApplyHam_block.cpp:18-21 aborts
+    if np.any(np.asarray(cell["lm_end"]) > 4):
+        raise ValueError("lm_end > 4 is not implemented")  # :70-73
+    idx = cell["n123"][:ngw].astype(np.int64) - 1
+    kin = 0.5 * cell["xkg"][:ngw] * cell["tpiba2"]
+    beta, w = projectors(cell, ngw)
+    vout = np.empty((ngw, nstates), dtype=complex)
+    for ist in range(nstates):
+        c = np.zeros(nnr, dtype=complex)
+        c[idx] = vin[:, ist]                      # :33-36
+        c = fft_inverse(c, nr)                    # :41
+        c = veff * c                              # :46-48
+        c = fft_forward(c, nr)                    # :53
+        vout[:, ist] = kin * vin[:, ist] + c[idx]  # :58-61
+    # nonlocal part (:68-165): zdotu with conj(EIGR)*PKG_A, back-projection
+    # with EIGR*PKG_A -- i.e. beta * W * beta^H * vin.
+    if beta.shape[1]:
+        p = w[:, None] * (beta.conj().T @ vin[:, :nstates])
+        vout += beta @ p
+    return vout
+
+
+def apply_ham(cell, v, veff):
+    """ApplyHam.cpp:5-142 (one vector)."""
+    return apply_ham_block(cell, np.asarray(v)[:, None], veff)[:, 0]
+
+
+# ---------------------------------------------------------------- filter
+
+def chebyfilt(cell, X, degree, lb, ub, veff):
+    """chebyfilt.cpp:6-74.  Returns the filtered block (X is not modified)."""
+    e = (ub - lb) / 2.0
+    c = (ub + lb) / 2.0
+    sigma = e / (lb - ub)
+    sigma1 = sigma
+    X = np.array(X, dtype=complex, copy=True)
+    Y = apply_ham_block(cell, X, veff)            # :26
+    Y = (Y - c * X) * (sigma1 / e)                # :36-39
+    for _ in range(2, degree + 1):                # :41-67
+        sigma2 = 1.0 / (2.0 / sigma1 - sigma)
+        Y1 = apply_ham_block(cell, Y, veff)
+        Y1 = Y1 * (2.0 * sigma2 / e)
+        Y1 = Y1 + (-c * 2.0 * sigma2 / e) * Y
+        Y1 = Y1 + (-sigma * sigma2) * X
+        X = Y
+        Y = Y1
+        sigma = sigma2
+    return Y
+
+
+def chebyfilt_step_coeffs(degree, lb, ub):
+    """The scalar coefficients of chebyfilt.cpp:26-67 per degree step d:
+    (a, b, c) with Y_d = a*H*Y_{d-1} + b*Y_{d-1} + c*Y_{d-2}, Y_0 = X."""
+    e = (ub - lb) / 2.0
+    cc = (ub + lb) / 2.0
+    sigma = e / (lb - ub)
+    sigma1 = sigma
+    out = [(sigma1 / e, -cc * sigma1 / e, 0.0)]
+    for _ in range(2, degree + 1):
+        sigma2 = 1.0 / (2.0 / sigma1 - sigma)
+        out.append((2.0 * sigma2 / e, -cc * 2.0 * sigma2 / e, -sigma * sigma2))
+        sigma = sigma2
+    return out
+
+
+# ---------------------------------------------------------------- Lanczos
+
+def lanczos(cell, v0, k, veff):
+    """lanczos.cpp:8-101.  Returns (T[k,k] real Fortran-layout matrix, f)."""
+    v0 = np.array(v0, dtype=complex, copy=True)
+    ngw = v0.size
+    T = np.zeros((k, k))
+    V = np.zeros((ngw, k), dtype=complex)
+    h = np.zeros(k, dtype=complex)
+    s = np.zeros(k, dtype=complex)
+    v0 = v0 / np.sqrt(np.vdot(v0, v0).real)
+    V[:, 0] = v0
+    Hv = apply_ham(cell, V[:, 0], veff)
+    h[0] = np.vdot(V[:, 0], Hv)
+    T[0, 0] = h[0].real
+    f = Hv - h[0] * V[:, 0]
+    s[0] = np.vdot(V[:, 0], f)
+    h[0] = h[0] + s[0]
+    f = f - s[0] * V[:, 0]
+    for j in range(1, k):
+        nf = np.vdot(f, f).real
+        T[j, j - 1] = np.sqrt(nf)
+        V[:, j] = f * (1.0 / np.sqrt(nf))
+        Hv = apply_ham(cell, V[:, j], veff)
+        f = Hv.copy()
+        for i in range(j + 1):
+            h[i] = np.vdot(V[:, i], Hv)
+            f = f - h[i] * V[:, i]
+        for i in range(j + 1):
+            s[i] = np.vdot(V[:, i], f)
+        h[: j + 1] += s[: j + 1]
+        for i in range(j + 1):
+            f = f - s[i] * V[:, i]
+        T[: j + 1, j] = h[: j + 1].real
+    return T, f
+
+
+def induced_norm_mat(T):
+    """ChebySCFLoop.cpp:7-34: || T * (1/sqrt(N)) 1 ||^2."""
+    n = T.shape[0]
+    v = T @ np.full(n, 1.0 / np.sqrt(n))
+    return float(v @ v)
+
+
+# ---------------------------------------------------------------- random start
+
+_LCG_TABLES: list[np.ndarray] = []
+
+
+def _lcg_next(a):
+    return ((a * 214013 + 2531011) >> 16) & 32767
+
+
+def _lcg_tables():
+    if not _LCG_TABLES:
+        f = _lcg_next(np.arange(32768, dtype=np.int64))
+        _LCG_TABLES.append(f)
+        for _ in range(40):
+            f = f[f]
+            _LCG_TABLES.append(f)
+    return _LCG_TABLES
+
+
+def random_col(nelem, seed):
+    """util_random_cpu.cpp:5-23: LCG a <- ((a*214013+2531011)>>16)&32767;
+    each value is ((a mod 100)+1)/a with the *updated* state a, re then im."""
+    L = 2 * nelem
+    first = _lcg_next(int(seed))  # the seed itself may exceed the table range
+    tabs = _lcg_tables()
+    t = np.arange(L, dtype=np.int64)  # state after t+1 steps = F^t(first)
+    st = np.full(L, first, dtype=np.int64)
+    k = 0
+    while (1 << k) <= L:
+        m = ((t >> k) & 1).astype(bool)
+        st[m] = tabs[k][st[m]]
+        k += 1
+    with np.errstate(divide="ignore", invalid="ignore"):
+        vals = ((st % 100) + 1).astype(float) / st.astype(float)
+    return vals[0::2] + 1j * vals[1::2]
+
+
+# ---------------------------------------------------------------- dense LA
+
+def ortho_qr(X):
+    """ortho_qr.cpp:3-34: zgeqrf + zungqr (Householder QR, explicit Q)."""
+    X = np.asfortranarray(np.array(X, dtype=complex, copy=True))
+    m, n = X.shape
+    qr, tau, _, info = lapack.zgeqrf(X, lwork=max(1, n))
+    if info != 0:
+        raise RuntimeError(f"zgeqrf info={info}")
+    q, _, info = lapack.zungqr(qr, tau, lwork=max(1, n))
+    if info != 0:
+        raise RuntimeError(f"zungqr info={info}")
+    return q[:, :n]
+
+
+def eig_zheevd(A):
+    """eig_zheevd.cpp:5-34: zheevd('V','U').  Returns (eigenvalues, vectors)."""
+    w, v, info = lapack.zheevd(np.asfortranarray(A), compute_v=1, lower=0)
+    if info != 0:
+        raise RuntimeError(f"zheevd info={info}")
+    return w, v
+
+
+SMALL_ZHEGV = 12.220446049250313e-16  # eig_zhegv.cpp:7
+
+
+def eig_zhegv_eval(A, B):
+    """eig_zhegv.cpp:86-161 (and eig_zhegv 5-83, which discards eval):
+    eigendecompose B, scale its vectors by 1/sqrt(eval) where eval > SMALL
+    (others left unscaled), A' = S^H (A S), eig(A'), back-transform.
+    Returns (eval of A', evec, number of independent vectors)."""
+    w, S = eig_zheevd(B)
+    S = S.copy()
+    nn = 0
+    for i in range(S.shape[1]):
+        if w[i] > SMALL_ZHEGV:
+            nn += 1
+            S[:, i] *= 1.0 / np.sqrt(w[i])
+    evec = A @ S
+    Ap = S.conj().T @ evec
+    lam, U = eig_zheevd(Ap)
+    return lam, S @ U, nn
+
+
+def symmetrize(v, ncol=None):
+    """lobpcg_cpu.cpp:15-27 over the leading ncol x ncol block: for i <= j,
+    v(i,j) = (v(i,j) + conj(v(j,i)))/2 and v(j,i) = conj(v(i,j)).  Every pair
+    is visited once, so the result equals (V + V^H)/2 entry by entry."""
+    v = np.array(v, copy=True)
+    n = v.shape[1] if ncol is None else ncol
+    b = v[:n, :n]
+    v[:n, :n] = 0.5 * (b + b.conj().T)
+    return v
+
+
+def gen_prec(xkg, alat, tpiba2, tau):
+    """GenPrec.cpp:5-24."""
+    xkg = np.asarray(xkg, dtype=float)
+    if tau <= 0.0:
+        x = xkg * (2.0 * np.pi / alat) ** 2
+        y = 27.0 + x * (18.0 + x * (12.0 + 8.0 * x))
+        return y / (y + 16.0 * x * x * x * x)
+    return tau / (0.5 * (xkg + 1.0) * tpiba2)
+
+
+# ---------------------------------------------------------------- solvers
+
+def _max_iter(nstates, user_max=None):
+    if user_max is not None:
+        return user_max
+    return max(30, nstates // 2)
+
+
+def davidson(cell, nbasis, nstates, veff, prec, nempty, max_iter=None):
+    """davidson_cpu.cpp:9-266.  Returns (evals, X, res_tol)."""
+    X = np.stack([random_col(nbasis, 100 + i) for i in range(nstates)], axis=1)  # :47-51
+    X = ortho_qr(X)                                                            # :53
+    HX = apply_ham_block(cell, X, veff)                                        # :56
+    evals = np.einsum("gi,gi->i", X.conj(), HX).real                           # :59-62
+    R = evals[None, :] * X - HX                                                # :65-72
+    res_tol = np.sqrt(np.einsum("gi,gi->i", R.conj(), R).real)
+    max_dir = _max_iter(nstates, max_iter)
+    machine_zero = 2.220446049250313e-16
+    TOL = 1.0e-6
+    n2 = 2 * nstates
+    for istep in range(1, max_dir + 1):
+        res_norm = np.where(res_tol > machine_zero, 1.0 / np.where(res_tol > 0, res_tol, 1), 1.0)
+        R = R * res_norm[None, :]                                              # :96-98
+        R = prec[:nbasis, None] * R                                            # :101-105
+        HR = apply_ham_block(cell, R, veff)                                    # :118
+        h = np.zeros((n2, n2), dtype=complex)
+        if istep == 1:
+            h[:nstates, :nstates] = X.conj().T @ HX                            # :123
+        else:
+            h[:nstates, :nstates] = np.diag(evals)                             # :127-132
+        h[:nstates, nstates:] = X.conj().T @ HR                                # :138
+        h[nstates:, :nstates] = HR.conj().T @ X                                # :141
+        h[nstates:, nstates:] = R.conj().T @ HR                                # :146
+        o = np.zeros((n2, n2), dtype=complex)
+        o[:nstates, :nstates] = np.eye(nstates)                                # :160-165
+        o[:nstates, nstates:] = X.conj().T @ R                                 # :169
+        o[nstates:, :nstates] = R.conj().T @ X                                 # :172
+        o[nstates:, nstates:] = R.conj().T @ R                                 # :177
+        lam, evec, _ = eig_zhegv_eval(h, o)                                    # :181
+        evals = lam[:nstates].copy()                                           # :184
+        c1 = evec[:nstates, :nstates]
+        c2 = evec[nstates:, :nstates]
+        X = X @ c1 + R @ c2                                                    # :189-204
+        HX = HX @ c1 + HR @ c2                                                 # :196-207
+        R = evals[None, :] * X - HX                                            # :210-217
+        res_tol = np.sqrt(np.einsum("gi,gi->i", R.conj(), R).real)
+        nconv = int(np.sum(res_tol < TOL))
+        if nconv >= nstates - nempty:
+            break
+        if np.mean(res_tol) < TOL / 10.0:
+            break
+    return evals, X, res_tol
+
+
+def lobpcg(cell, nbasis, nstates, veff, prec, nempty, max_iter=None):
+    """lobpcg_cpu.cpp:31-395.  Returns (lambda, X, resnrm)."""
+    TOL = 1.0e-6
+    TFUDGE = 1.0e10
+    maxiter = _max_iter(nstates, max_iter)
+    nb = nstates
+    X = np.stack([random_col(nbasis, 100 + i) for i in range(nb)], axis=1)    # :82-86
+    X = ortho_qr(X)                                                            # :90
+    HX = apply_ham_block(cell, X, veff)                                        # :95
+    P = HP = None
+
+    def chol_orth(W, HW):
+        C = symmetrize(W.conj().T @ W)
+        L = np.linalg.cholesky(C)  # C = L L^H, U = L^H
+        Ui = np.linalg.inv(L.conj().T)
+        return W @ Ui, HW @ Ui
+
+    it = 1
+    while True:
+        t1 = X.conj().T @ HX                                                   # :103 / :224
+        W = HX - X @ t1                                                        # :107-111
+        lam, _ = eig_zheevd(t1)                                                # :113
+        resnrm = np.sqrt(np.einsum("gi,gi->i", W.conj(), W).real)
+        nconv = int(np.sum(resnrm < TOL))
+        rnorm = float(np.mean(resnrm))
+        if nconv >= nstates - nempty or rnorm < TOL:
+            break
+        W = prec[:nbasis, None] * W                                            # :142-146
+        HW = apply_ham_block(cell, W, veff)                                    # :149
+        W, HW = chol_orth(W, HW)                                               # :153-180
+        if it == 1:
+            Q = np.concatenate([X, W], axis=1)
+            HQ = np.concatenate([HX, HW], axis=1)
+        else:
+            Q = np.concatenate([X, W, P], axis=1)
+            HQ = np.concatenate([HX, HW, HP], axis=1)
+        T = symmetrize(Q.conj().T @ HQ)                                        # :183-185
+        G = symmetrize(Q.conj().T @ Q)                                         # :189-191
+        _, U, _ = eig_zhegv_eval(T, G)                                         # :196
+        Un = U[:, :nb]
+        Xn = Q @ Un
+        HXn = HQ @ Un
+        if it == 1:
+            P, HP = W.copy(), HW.copy()                                        # :211-213
+        else:
+            P = W @ Un[nb:2 * nb] + P @ Un[2 * nb:3 * nb]                      # :328-335
+            HP = HW @ Un[nb:2 * nb] + HP @ Un[2 * nb:3 * nb]                  # :338-345
+            P, HP = chol_orth(P, HP)                                           # :348-370
+        X, HX = Xn, HXn
+        it += 1
+        if it > maxiter:
+            # the loop (:218) runs iter=2..maxiter and leaves after the
+            # rotation of the last iteration without a new check
+            break
+    return lam, X, resnrm
+
+
+# ---------------------------------------------------------------- density
+
+def eval_rho_psi(cell, eigvec_flat, ld, ngw, nx, focc, wkpt, omega, ngwx):
+    """EvalRhoPsi.cpp:83-157.  eigvec_flat is the caller's buffer (column
+    major with leading dimension ld); C0(:,ist) copies NGWX entries from
+    column ist, so with ld < NGWX it reads into the next column exactly as
+    the reference does.  The scatter runs over ig < NGW_ik, dropping the last
+    plane wave (:117).  Returns (rhoe_increment, ekin_increment, C0)."""
+    nr = cell["nr"]
+    nnr = nr[0] * nr[1] * nr[2]
+    rho = np.zeros(nnr)
+    c0 = np.zeros((ngwx, nx), dtype=complex)
+    idx = cell["n123"][: ngw - 1].astype(np.int64) - 1
+    xkin = 0.0
+    for ist in range(nx):
+        wdotf = wkpt * focc[ist]
+        c0[:, ist] = eigvec_flat[ist * ld: ist * ld + ngwx]
+        ct = c0[: ngw - 1, ist]
+        scg = np.abs(ct) ** 2
+        ss = float(np.sum(scg))
+        if abs(ss - 1.0) > 6.0e-3:
+            raise RuntimeError(f"Wrong charge density in G-space: {ss} (state {ist + 1})")
+        xkin += float(np.sum(cell["xkg"][: ngw - 1] * scg)) * wdotf * 0.5
+        c = np.zeros(nnr, dtype=complex)
+        c[idx] = ct
+        c = fft_inverse(c, nr)
+        rho += np.abs(c) ** 2 * (wdotf / omega)
+    return rho, xkin * cell["tpiba2"], c0
+
+
+def eval_enl(cell, c0, ngw, nx, focc, wkpt):
+    """EvalENL.cpp:5-49: FNL = C0^T (PKG_A conj(EIGR)) (unconjugated C0),
+    ENL = sum w f |FNL|^2 WNL.  Returns (ENL, FNL[nx, nproj])."""
+    beta, w = projectors(cell, ngw)
+    fnl = c0[:ngw, :nx].T @ beta.conj()
+    enl = float(np.sum(wkpt * (focc[:nx, None] * np.abs(fnl) ** 2) * w[None, :]))
+    return enl, fnl
