@@ -1,0 +1,442 @@
+// Cell set-up (the engine side of SetupArrays_ApplyHam_cuda /
+// CopyRho_ApplyHam_cuda, common_pspw.h:255-257), error state, workspaces and
+// the optional device timing hooks.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <string>
+#include <vector>
+
+#include "common.cuh"
+#include "engine.h"
+
+namespace pspw {
+
+static thread_local std::string g_last_error;
+
+int fail(int code, const std::string &msg) {
+  g_last_error = msg;
+  return code;
+}
+
+int cuda_fail(cudaError_t e, const char *what) {
+  g_last_error = std::string(what) + ": " + cudaGetErrorString(e);
+  return e == cudaErrorMemoryAllocation ? PSPW_ERR_OOM : PSPW_ERR_CUDA;
+}
+
+int ws_reserve(pspw_cell *c, int slot, size_t bytes, void **out) {
+  Workspace &w = c->ws[slot];
+  if (w.bytes < bytes) {
+    if (w.ptr) {
+      PSPW_CUDA(cudaStreamSynchronize(c->stream));
+      PSPW_CUDA(cudaFree(w.ptr));
+      w.ptr = nullptr;
+      w.bytes = 0;
+    }
+    size_t want = bytes + bytes / 8;  // headroom for slightly larger later calls
+    PSPW_CUDA(cudaMalloc(&w.ptr, want));
+    w.bytes = want;
+  }
+  *out = w.ptr;
+  return PSPW_OK;
+}
+
+void timing_begin(pspw_cell *c, int family, cudaEvent_t *ev) {
+  *ev = nullptr;
+  if (!(c->timing.mask & (1 << family))) return;
+  cudaEvent_t e;
+  if (cudaEventCreate(&e) != cudaSuccess) return;
+  cudaEventRecord(e, c->stream);
+  *ev = e;
+}
+
+void timing_end(pspw_cell *c, int family, cudaEvent_t ev) {
+  if (!ev) return;
+  cudaEvent_t e;
+  if (cudaEventCreate(&e) != cudaSuccess) return;
+  cudaEventRecord(e, c->stream);
+  c->timing.pending.push_back({family, {ev, e}});
+}
+
+static int drain_timing(pspw_cell *c) {
+  if (c->timing.pending.empty()) return PSPW_OK;
+  PSPW_CUDA(cudaStreamSynchronize(c->stream));
+  for (auto &p : c->timing.pending) {
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, p.second.first, p.second.second);
+    c->timing.ms[p.first] += ms;
+    c->timing.launches[p.first] += 1;
+    cudaEventDestroy(p.second.first);
+    cudaEventDestroy(p.second.second);
+  }
+  c->timing.pending.clear();
+  return PSPW_OK;
+}
+
+namespace {
+
+int factor_radices(int n, int *rad, int *nf) {
+  int k = 0;
+  auto push = [&](int r) {
+    if (k >= kMaxStages) return false;
+    rad[k++] = r;
+    return true;
+  };
+  while (n % 4 == 0) {
+    if (!push(4)) return PSPW_ERR_NOT_IMPL;
+    n /= 4;
+  }
+  while (n % 2 == 0) {
+    if (!push(2)) return PSPW_ERR_NOT_IMPL;
+    n /= 2;
+  }
+  for (int p = 3; n > 1; p += 2) {
+    while (n % p == 0) {
+      if (p > 64) return PSPW_ERR_NOT_IMPL;
+      if (!push(p)) return PSPW_ERR_NOT_IMPL;
+      n /= p;
+    }
+  }
+  *nf = k;
+  return PSPW_OK;
+}
+
+template <typename T>
+int upload(T **d, const std::vector<T> &h) {
+  PSPW_CUDA(cudaMalloc((void **)d, std::max<size_t>(1, h.size()) * sizeof(T)));
+  if (!h.empty()) PSPW_CUDA(cudaMemcpy(*d, h.data(), h.size() * sizeof(T), cudaMemcpyHostToDevice));
+  return PSPW_OK;
+}
+
+int make_dim(FftDim &d, int n) {
+  d.n = n;
+  int rc = factor_radices(n, d.rad, &d.nf);
+  if (rc) return fail(rc, "FFT length " + std::to_string(n) + " has a prime factor > 64");
+  std::vector<double2> w64(n);
+  std::vector<float2> w32(n);
+  for (int t = 0; t < n; t++) {
+    // exp(+2 pi i t/n), angle reduced to the first half turn for accuracy
+    const double ang = 2.0 * M_PI * (double)t / (double)n;
+    double c = std::cos(ang), s = std::sin(ang);
+    if (4 * t == n) {
+      c = 0.0;
+      s = 1.0;
+    } else if (2 * t == n) {
+      c = -1.0;
+      s = 0.0;
+    } else if (4 * t == 3 * n) {
+      c = 0.0;
+      s = -1.0;
+    }
+    w64[t] = make_double2(c, s);
+    w32[t] = make_float2((float)c, (float)s);
+  }
+  if ((rc = upload(&d.d_w64, w64))) return rc;
+  return upload(&d.d_w32, w32);
+}
+
+}  // namespace
+
+}  // namespace pspw
+
+using namespace pspw;
+
+extern "C" {
+
+const char *pspw_error_string(int code) {
+  switch (code) {
+    case PSPW_OK: return "ok";
+    case PSPW_ERR_ARG: return "invalid argument";
+    case PSPW_ERR_SHAPE: return "inconsistent sizes";
+    case PSPW_ERR_CUDA: return "CUDA error";
+    case PSPW_ERR_OOM: return "device out of memory";
+    case PSPW_ERR_NONFINITE: return "non-finite input";
+    case PSPW_ERR_TIMEOUT: return "device wait timed out";
+    case PSPW_ERR_LAPACK: return "dense factorisation failed";
+    case PSPW_ERR_CHARGE: return "wrong charge density in G-space";
+    case PSPW_ERR_NOT_IMPL: return "not implemented";
+    default: return "unknown error";
+  }
+}
+
+const char *pspw_last_error(void) { return g_last_error.c_str(); }
+
+int pspw_version(void) { return 100; }
+
+int pspw_cell_destroy(pspw_cell *c) {
+  if (!c) return PSPW_OK;
+  cudaSetDevice(c->device);
+  if (c->stream) cudaStreamSynchronize(c->stream);
+  Basis &B = c->basis;
+  void *ptrs[] = {B.d_col_start, B.d_sg_ig, B.d_sg_z, B.d_sg_col, B.d_col_of_xy, B.d_xa_list,
+                  B.d_xa_of_x, B.d_kin64, B.d_kin32, c->proj.d_eigr64, c->proj.d_eigr32,
+                  c->proj.d_pkga64, c->proj.d_pkga32, c->proj.d_patom, c->proj.d_psp,
+                  c->proj.d_plm, c->proj.d_pw64, c->proj.d_pw32, c->d_veff64, c->d_veff32};
+  for (void *p : ptrs)
+    if (p) cudaFree(p);
+  for (int i = 0; i < 3; i++) {
+    if (B.dim[i].d_w64) cudaFree(B.dim[i].d_w64);
+    if (B.dim[i].d_w32) cudaFree(B.dim[i].d_w32);
+  }
+  for (auto &w : c->ws)
+    if (w.ptr) cudaFree(w.ptr);
+  for (auto &p : c->timing.pending) {
+    cudaEventDestroy(p.second.first);
+    cudaEventDestroy(p.second.second);
+  }
+  if (c->stream) cudaStreamDestroy(c->stream);
+  delete c;
+  return PSPW_OK;
+}
+
+int pspw_cell_create(pspw_cell **out, int device, int nr1, int nr2, int nr3, int ngw, int ngwx,
+                     const unsigned int *n123, const double *xkg, double tpiba2, int nsp,
+                     const int *na, int nax, const int *lm_end, int nlmax, const double *eigr,
+                     const double *pkg_a, const double *wnl) {
+  if (!out || !n123 || !xkg || !na || !lm_end) return fail(PSPW_ERR_ARG, "cell_create: null argument");
+  *out = nullptr;
+  if (nr1 < 1 || nr2 < 1 || nr3 < 1 || ngw < 1 || ngwx < ngw || nsp < 0 || nax < 0 || nlmax < 0)
+    return fail(PSPW_ERR_ARG, "cell_create: bad sizes");
+  const long long nnr_ll = (long long)nr1 * nr2 * nr3;
+  if (nnr_ll > (1LL << 31) - 1) return fail(PSPW_ERR_SHAPE, "cell_create: grid too large");
+  int nat = 0, nproj = 0;
+  for (int s = 0; s < nsp; s++) {
+    if (na[s] < 0 || na[s] > nax) return fail(PSPW_ERR_ARG, "cell_create: na > nax");
+    if (lm_end[s] > 4)
+      return fail(PSPW_ERR_NOT_IMPL, "lm_end > 4 is not implemented (ApplyHam_block.cpp:70-73)");
+    if (lm_end[s] > nlmax) return fail(PSPW_ERR_SHAPE, "cell_create: lm_end > nlmax");
+    nat += na[s];
+    nproj += na[s] * std::max(0, lm_end[s]);
+  }
+  if (nproj > 0 && (!eigr || !pkg_a || !wnl)) return fail(PSPW_ERR_ARG, "cell_create: null projector arrays");
+  PSPW_CUDA(cudaSetDevice(device));
+  pspw_cell *c = new pspw_cell();
+  c->device = device;
+  c->ngwx = ngwx;
+  int rc = PSPW_OK;
+  auto bail = [&](int code) {
+    pspw_cell_destroy(c);
+    return code;
+  };
+  if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess)
+    return bail(fail(PSPW_ERR_CUDA, "cell_create: stream"));
+  Basis &B = c->basis;
+  B.n1 = nr1;
+  B.n2 = nr2;
+  B.n3 = nr3;
+  B.nnr = (int)nnr_ll;
+  B.ngw = ngw;
+  // ---- sticks
+  std::vector<int> gi1(ngw), gi2(ngw), gi3(ngw);
+  std::vector<int> col_of_xy((size_t)nr1 * nr2, -1);
+  for (int ig = 0; ig < ngw; ig++) {
+    const long long idx = (long long)n123[ig] - 1;
+    if (idx < 0 || idx >= nnr_ll) return bail(fail(PSPW_ERR_SHAPE, "cell_create: N123 outside the grid"));
+    gi1[ig] = (int)(idx % nr1);
+    gi2[ig] = (int)((idx / nr1) % nr2);
+    gi3[ig] = (int)(idx / ((long long)nr1 * nr2));
+    col_of_xy[(size_t)gi1[ig] + (size_t)nr1 * gi2[ig]] = 0;
+  }
+  int ncol = 0;
+  std::vector<int> col_x, col_y;
+  for (int y = 0; y < nr2; y++)
+    for (int x = 0; x < nr1; x++)
+      if (col_of_xy[(size_t)x + (size_t)nr1 * y] == 0) {
+        col_of_xy[(size_t)x + (size_t)nr1 * y] = ncol++;
+        col_x.push_back(x);
+        col_y.push_back(y);
+      }
+  std::vector<int> cnt(ncol + 1, 0);
+  for (int ig = 0; ig < ngw; ig++) cnt[col_of_xy[(size_t)gi1[ig] + (size_t)nr1 * gi2[ig]] + 1]++;
+  for (int k = 0; k < ncol; k++) cnt[k + 1] += cnt[k];
+  std::vector<int> col_start = cnt;
+  std::vector<std::pair<int, int>> entries(ngw);  // (stick, z) per G, sorted later
+  std::vector<int> order(ngw);
+  for (int ig = 0; ig < ngw; ig++) order[ig] = ig;
+  std::stable_sort(order.begin(), order.end(), [&](int a, int b) {
+    const int ca = col_of_xy[(size_t)gi1[a] + (size_t)nr1 * gi2[a]];
+    const int cb = col_of_xy[(size_t)gi1[b] + (size_t)nr1 * gi2[b]];
+    return ca != cb ? ca < cb : gi3[a] < gi3[b];
+  });
+  std::vector<int> sg_ig(ngw), sg_z(ngw), sg_col(ngw);
+  for (int k = 0; k < ngw; k++) {
+    const int ig = order[k];
+    sg_ig[k] = ig;
+    sg_z[k] = gi3[ig];
+    sg_col[k] = col_of_xy[(size_t)gi1[ig] + (size_t)nr1 * gi2[ig]];
+  }
+  std::vector<int> xa_of_x(nr1, -1), xa_list;
+  for (int k = 0; k < ncol; k++) xa_of_x[col_x[k]] = 0;
+  for (int x = 0; x < nr1; x++)
+    if (xa_of_x[x] == 0) {
+      xa_of_x[x] = (int)xa_list.size();
+      xa_list.push_back(x);
+    }
+  B.ncol = ncol;
+  B.nxa = (int)xa_list.size();
+  std::vector<double> kin64(ngw);
+  std::vector<float> kin32(ngw);
+  for (int ig = 0; ig < ngw; ig++) {
+    kin64[ig] = 0.5 * xkg[ig] * tpiba2;  // ApplyHam_block.cpp:59, same rounding order
+    kin32[ig] = (float)kin64[ig];
+  }
+  if ((rc = upload(&B.d_col_start, col_start)) || (rc = upload(&B.d_sg_ig, sg_ig)) ||
+      (rc = upload(&B.d_sg_z, sg_z)) || (rc = upload(&B.d_sg_col, sg_col)) ||
+      (rc = upload(&B.d_col_of_xy, col_of_xy)) || (rc = upload(&B.d_xa_list, xa_list)) ||
+      (rc = upload(&B.d_xa_of_x, xa_of_x)) || (rc = upload(&B.d_kin64, kin64)) ||
+      (rc = upload(&B.d_kin32, kin32)))
+    return bail(rc);
+  const int nr[3] = {nr1, nr2, nr3};
+  for (int i = 0; i < 3; i++)
+    if ((rc = make_dim(B.dim[i], nr[i]))) return bail(rc);
+  // ---- projectors, species-major then atom then lm (ApplyHam_block.cpp:68-117)
+  Projectors &P = c->proj;
+  P.nat = nat;
+  P.nsp = nsp;
+  P.nproj = nproj;
+  if (nproj > 0) {
+    std::vector<double2> e64((size_t)nat * ngw);
+    std::vector<float2> e32((size_t)nat * ngw);
+    std::vector<double> k64((size_t)nsp * ngw * 4, 0.0);
+    std::vector<float> k32((size_t)nsp * ngw * 4, 0.f);
+    std::vector<int> patom, psp, plm;
+    std::vector<double> pw64;
+    std::vector<float> pw32;
+    int ga = 0;
+    for (int s = 0; s < nsp; s++) {
+      for (int a = 0; a < na[s]; a++, ga++) {
+        const double *src = eigr + 2 * (((size_t)s * nax + a) * ngwx);
+        for (int ig = 0; ig < ngw; ig++) {
+          e64[(size_t)ga * ngw + ig] = make_double2(src[2 * ig], src[2 * ig + 1]);
+          e32[(size_t)ga * ngw + ig] = make_float2((float)src[2 * ig], (float)src[2 * ig + 1]);
+        }
+        for (int lm = 0; lm < lm_end[s]; lm++) {
+          patom.push_back(ga);
+          psp.push_back(s);
+          plm.push_back(lm);
+          const double wv = wnl[(size_t)lm * nsp + s];  // WNL(is,lm), NSP leading
+          pw64.push_back(wv);
+          pw32.push_back((float)wv);
+        }
+      }
+      for (int ig = 0; ig < ngw; ig++)
+        for (int lm = 0; lm < std::min(4, nlmax); lm++) {
+          const double v = pkg_a[((size_t)s * ngwx + ig) * nlmax + lm];  // PKG_A(lm,ig,is)
+          k64[((size_t)s * ngw + ig) * 4 + lm] = v;
+          k32[((size_t)s * ngw + ig) * 4 + lm] = (float)v;
+        }
+    }
+    if ((rc = upload(&P.d_eigr64, e64)) || (rc = upload(&P.d_eigr32, e32)) ||
+        (rc = upload(&P.d_pkga64, k64)) || (rc = upload(&P.d_pkga32, k32)) ||
+        (rc = upload(&P.d_patom, patom)) || (rc = upload(&P.d_psp, psp)) ||
+        (rc = upload(&P.d_plm, plm)) || (rc = upload(&P.d_pw64, pw64)) ||
+        (rc = upload(&P.d_pw32, pw32)))
+      return bail(rc);
+  }
+  if (cudaMalloc(&c->d_veff64, (size_t)B.nnr * sizeof(double)) != cudaSuccess ||
+      cudaMalloc(&c->d_veff32, (size_t)B.nnr * sizeof(float)) != cudaSuccess)
+    return bail(fail(PSPW_ERR_OOM, "cell_create: V_eff"));
+  *out = c;
+  return PSPW_OK;
+}
+
+}  // extern "C"
+
+namespace pspw {
+namespace {
+
+__global__ void k_veff_scale(const double *__restrict__ v, int n, double s, double *o64,
+                             float *o32) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const double x = v[i] * s;
+    o64[i] = x;
+    o32[i] = (float)x;
+  }
+}
+
+}  // namespace
+}  // namespace pspw
+
+extern "C" {
+
+int pspw_cell_set_veff_device(pspw_cell *c, const double *d_veff, int nnr) {
+  if (!c || !d_veff) return fail(PSPW_ERR_ARG, "set_veff: null argument");
+  if (nnr != c->basis.nnr) return fail(PSPW_ERR_SHAPE, "nnr != NNR (ApplyHam_block.cpp:18-21)");
+  PSPW_CUDA(cudaSetDevice(c->device));
+  k_veff_scale<<<2 * 148, 256, 0, c->stream>>>(d_veff, nnr, 1.0 / (double)nnr, c->d_veff64,
+                                                c->d_veff32);
+  PSPW_CUDA(cudaGetLastError());
+  c->veff_set = true;
+  return PSPW_OK;
+}
+
+int pspw_cell_set_veff(pspw_cell *c, const double *veff, int nnr) {
+  if (!c || !veff) return fail(PSPW_ERR_ARG, "set_veff: null argument");
+  if (nnr != c->basis.nnr) return fail(PSPW_ERR_SHAPE, "nnr != NNR (ApplyHam_block.cpp:18-21)");
+  PSPW_CUDA(cudaSetDevice(c->device));
+  double *tmp = nullptr;
+  int rc = ws_reserve(c, 11, (size_t)nnr * sizeof(double), (void **)&tmp);
+  if (rc) return rc;
+  PSPW_CUDA(cudaMemcpyAsync(tmp, veff, (size_t)nnr * sizeof(double), cudaMemcpyHostToDevice,
+                            c->stream));
+  rc = pspw_cell_set_veff_device(c, tmp, nnr);
+  if (rc) return rc;
+  PSPW_CUDA(cudaStreamSynchronize(c->stream));
+  return PSPW_OK;
+}
+
+int pspw_cell_get_stream(pspw_cell *c, void **stream) {
+  if (!c || !stream) return fail(PSPW_ERR_ARG, "get_stream: null argument");
+  *stream = (void *)c->stream;
+  return PSPW_OK;
+}
+
+int pspw_cell_sizes(pspw_cell *c, int *o) {
+  if (!c || !o) return fail(PSPW_ERR_ARG, "sizes: null argument");
+  o[0] = c->basis.n1;
+  o[1] = c->basis.n2;
+  o[2] = c->basis.n3;
+  o[3] = c->basis.ngw;
+  o[4] = c->basis.ncol;
+  o[5] = c->basis.nxa;
+  o[6] = c->proj.nat;
+  o[7] = c->proj.nproj;
+  return PSPW_OK;
+}
+
+int pspw_cell_set_band_batch(pspw_cell *c, int nbatch) {
+  if (!c || nbatch < 0) return fail(PSPW_ERR_ARG, "set_band_batch: bad argument");
+  c->band_batch = nbatch;
+  return PSPW_OK;
+}
+
+int pspw_timing_enable(pspw_cell *c, int mask) {
+  if (!c) return fail(PSPW_ERR_ARG, "timing: null cell");
+  c->timing.mask = mask;
+  return PSPW_OK;
+}
+
+int pspw_timing_read(pspw_cell *c, int family, double *total_ms, long long *launches) {
+  if (!c || family < 0 || family > 3) return fail(PSPW_ERR_ARG, "timing: bad argument");
+  int rc = drain_timing(c);
+  if (rc) return rc;
+  if (total_ms) *total_ms = c->timing.ms[family];
+  if (launches) *launches = c->timing.launches[family];
+  return PSPW_OK;
+}
+
+int pspw_timing_reset(pspw_cell *c) {
+  if (!c) return fail(PSPW_ERR_ARG, "timing: null cell");
+  int rc = drain_timing(c);
+  for (int i = 0; i < 4; i++) {
+    c->timing.ms[i] = 0;
+    c->timing.launches[i] = 0;
+  }
+  return rc;
+}
+
+}  // extern "C"

@@ -1,0 +1,117 @@
+// Internal state of one cell (one geometry and k-point) and the kernel
+// launchers shared by the C ABI.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <string>
+#include <vector>
+
+#include "pspw_gpu.h"
+
+namespace pspw {
+
+constexpr int kMaxStages = 16;
+
+// One 1D FFT length: radix schedule and the table of its n-th roots of unity
+// exp(+2 pi i t / n) (both precisions).
+struct FftDim {
+  int n = 0;
+  int nf = 0;
+  int rad[kMaxStages] = {};
+  double2 *d_w64 = nullptr;
+  float2 *d_w32 = nullptr;
+};
+
+// Device copy of the basis in the layouts the kernels read.
+//
+// The wavefunction sphere is organised in "sticks": the distinct (i1,i2)
+// grid columns that hold at least one G of the sphere, numbered in (i2,i1)
+// order.  A G entry of stick c sits at z = i3.  The x values that carry a
+// stick form the active-x set (nxa of the n1 planes' x positions).
+struct Basis {
+  int n1 = 0, n2 = 0, n3 = 0, nnr = 0;
+  int ngw = 0;
+  int ncol = 0;  // sticks
+  int nxa = 0;   // active x positions
+  int *d_col_start = nullptr;  // [ncol+1] CSR over G entries sorted by stick
+  int *d_sg_ig = nullptr;      // [ngw] G index (0-based, caller order)
+  int *d_sg_z = nullptr;       // [ngw] i3 of that G
+  int *d_sg_col = nullptr;     // [ngw] stick of that G
+  int *d_col_of_xy = nullptr;  // [n1*n2] stick at (i1,i2) or -1
+  int *d_xa_list = nullptr;    // [nxa] i1 of active x
+  int *d_xa_of_x = nullptr;    // [n1] active index or -1
+  double *d_kin64 = nullptr;   // [ngw] 0.5*XKG*TPIBA2
+  float *d_kin32 = nullptr;
+  FftDim dim[3];
+};
+
+// KB projectors beta_p(G) = EIGR(G, atom_p) * PKG_A(lm_p, G, species_p).
+struct Projectors {
+  int nat = 0, nsp = 0, nproj = 0;
+  double2 *d_eigr64 = nullptr;  // [nat][ngw], atoms species-major
+  float2 *d_eigr32 = nullptr;
+  double *d_pkga64 = nullptr;  // [nsp][ngw][4]
+  float *d_pkga32 = nullptr;
+  int *d_patom = nullptr;    // [nproj] atom (species-major global index)
+  int *d_psp = nullptr;      // [nproj] species
+  int *d_plm = nullptr;      // [nproj] lm (0..3)
+  double *d_pw64 = nullptr;  // [nproj] WNL(species, lm)
+  float *d_pw32 = nullptr;
+};
+
+struct Timing {
+  int mask = 0;
+  double ms[4] = {0, 0, 0, 0};
+  long long launches[4] = {0, 0, 0, 0};
+  std::vector<cudaEvent_t> ev_pool;
+  std::vector<std::pair<int, std::pair<cudaEvent_t, cudaEvent_t>>> pending;
+};
+
+struct Workspace {
+  void *ptr = nullptr;
+  size_t bytes = 0;
+};
+
+}  // namespace pspw
+
+struct pspw_cell {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  int ngwx = 0;
+  int band_batch = 0;
+  pspw::Basis basis;
+  pspw::Projectors proj;
+  double *d_veff64 = nullptr;  // V_eff / NNR on the grid (forward-FFT scale folded in)
+  float *d_veff32 = nullptr;
+  bool veff_set = false;
+  // persistent scratch: 0 = FFT sticks, 1 = FFT planes, 2 = projector
+  // partial sums, 3 = projections, 4.. = block buffers of the filter/solvers
+  pspw::Workspace ws[12];
+  pspw::Timing timing;
+};
+
+namespace pspw {
+
+// error state
+int fail(int code, const std::string &msg);
+int cuda_fail(cudaError_t e, const char *what);
+#define PSPW_CUDA(call)                                   \
+  do {                                                    \
+    cudaError_t _e = (call);                              \
+    if (_e != cudaSuccess) return ::pspw::cuda_fail(_e, #call); \
+  } while (0)
+
+int ws_reserve(pspw_cell *c, int slot, size_t bytes, void **out);
+
+// timing hooks (no-ops unless the family is enabled)
+void timing_begin(pspw_cell *c, int family, cudaEvent_t *ev);
+void timing_end(pspw_cell *c, int family, cudaEvent_t ev);
+
+// H*psi on device blocks of precision R.  out = a*(H in) + b*in + g*xm2
+// (xm2 may be null when g == 0).  ld_in/ld_out >= ngw.
+template <typename R>
+int hpsi_apply(pspw_cell *c, const void *in, int ld_in, void *out, int ld_out, int ngw,
+               int nb, double a, double b, double g, const void *xm2, int ld_xm2);
+
+}  // namespace pspw

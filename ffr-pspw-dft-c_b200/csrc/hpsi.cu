@@ -1,0 +1,558 @@
+// Block H*psi on the device (the work of ApplyHam_block.cpp:5-172).
+//
+// Local part: the scatter -> inverse 3D FFT -> V_eff -> forward 3D FFT ->
+// gather chain of ApplyHam_block.cpp:33-61, done as five passes that only
+// touch the part of the grid the wavefunction sphere can reach:
+//   1 sticks_inv   gather psi(G) of each stick (an (i1,i2) column holding
+//                  sphere G's) into shared memory, inverse FFT along z,
+//                  write the stick buffer S[band][z][stick]
+//   2 planes_inv   for each z and a tile of active x: read the y line from S
+//                  (zero where no stick), inverse FFT along y, write the
+//                  plane buffer P[band][z][y][active x]
+//   3 xlines       for each (y,z): expand the active x into the full x line,
+//                  inverse FFT along x, multiply by V_eff/NNR, forward FFT
+//                  along x, keep the active x -- V_eff is applied between the
+//                  last inverse and the first forward pass
+//   4 planes_fwd   forward FFT along y, keep the stick positions, write S
+//   5 sticks_fwd   forward FFT along z, pick the sphere G's, add the kinetic
+//                  term 0.5*XKG*TPIBA2*psi
+// The 1/NNR of the forward transform (fft_fftw3.cpp:27) is folded into V.
+//
+// Nonlocal part (ApplyHam_block.cpp:68-165): with beta_p(G) =
+// EIGR(G,a_p)*PKG_A(lm_p,G), the reference adds beta W beta^H psi (zdotu
+// against conj(EIGR)*PKG_A, back-projection with EIGR*PKG_A).  Here that is
+// two complex GEMMs whose A operand is generated from EIGR and PKG_A while it
+// is loaded, never stored: projection (split over G, partial sums reduced in
+// a fixed order, so results are deterministic) and back-projection, whose
+// epilogue also applies out = a*(H psi) + b*psi + g*x, the update of the
+// Chebyshev three-term recurrence (chebyfilt.cpp:36-59).
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstdio>
+
+#include "common.cuh"
+#include "engine.h"
+#include "fft.cuh"
+
+namespace pspw {
+
+namespace {
+
+constexpr int kNT = 256;        // threads per FFT-pass block
+constexpr int kTileElems = 2048;  // complex elements per FFT-pass tile
+
+struct Geo {
+  int n1, n2, n3, ncol, nxa, ngw;
+  const int *col_start, *sg_ig, *sg_z, *sg_col, *col_of_xy, *xa_list, *xa_of_x;
+};
+
+__host__ __device__ __forceinline__ int pad(int n) { return n + 1; }
+
+FftArg fft_arg(const FftDim &d) {
+  FftArg a;
+  a.n = d.n;
+  a.nf = d.nf;
+  for (int i = 0; i < kMaxStages; i++) a.rad[i] = d.rad[i];
+  return a;
+}
+
+template <typename T>
+const T *tw(const FftDim &d);
+template <>
+const double2 *tw<double2>(const FftDim &d) {
+  return d.d_w64;
+}
+template <>
+const float2 *tw<float2>(const FftDim &d) {
+  return d.d_w32;
+}
+
+// ---------------------------------------------------------------- pass 1
+template <typename T>
+__global__ void __launch_bounds__(kNT) k_sticks_inv(Geo g, FftArg fz, const T *__restrict__ wz,
+                                                    const T *__restrict__ psi, int ld, int ngw_call,
+                                                    T *__restrict__ S, int T1) {
+  extern __shared__ unsigned char smem_raw[];
+  T *a = reinterpret_cast<T *>(smem_raw);
+  const int ls = pad(g.n3);
+  T *b = a + T1 * ls;
+  const int c0 = blockIdx.x * T1;
+  const int band = blockIdx.y;
+  const int nc = min(T1, g.ncol - c0);
+  for (int e = threadIdx.x; e < T1 * ls; e += blockDim.x) a[e] = czero<T>();
+  __syncthreads();
+  const T *pb = psi + (size_t)band * ld;
+  const int k0 = g.col_start[c0], k1 = g.col_start[c0 + nc];
+  for (int k = k0 + threadIdx.x; k < k1; k += blockDim.x) {
+    const int ig = g.sg_ig[k];
+    if (ig < ngw_call) a[(g.sg_col[k] - c0) * ls + g.sg_z[k]] = pb[ig];
+  }
+  __syncthreads();
+  T *r = fft_lines(a, b, T1, ls, fz, wz, +1);
+  T *Sb = S + (size_t)band * g.n3 * g.ncol;
+  for (int e = threadIdx.x; e < T1 * g.n3; e += blockDim.x) {
+    const int z = e / T1, t = e - z * T1;
+    if (t < nc) Sb[(size_t)z * g.ncol + c0 + t] = r[t * ls + z];
+  }
+}
+
+// ---------------------------------------------------------------- pass 2
+template <typename T>
+__global__ void __launch_bounds__(kNT) k_planes_inv(Geo g, FftArg fy, const T *__restrict__ wy,
+                                                    const T *__restrict__ S, T *__restrict__ P,
+                                                    int T2) {
+  extern __shared__ unsigned char smem_raw[];
+  T *a = reinterpret_cast<T *>(smem_raw);
+  const int ls = pad(g.n2);
+  T *b = a + T2 * ls;
+  const int x0 = blockIdx.x * T2;
+  const int z = blockIdx.y;
+  const int band = blockIdx.z;
+  const int nx = min(T2, g.nxa - x0);
+  const T *Sz = S + ((size_t)band * g.n3 + z) * g.ncol;
+  for (int e = threadIdx.x; e < T2 * g.n2; e += blockDim.x) {
+    const int y = e / T2, t = e - y * T2;
+    T v = czero<T>();
+    if (t < nx) {
+      const int c = g.col_of_xy[g.xa_list[x0 + t] + g.n1 * y];
+      if (c >= 0) v = Sz[c];
+    }
+    a[t * ls + y] = v;
+  }
+  __syncthreads();
+  T *r = fft_lines(a, b, T2, ls, fy, wy, +1);
+  T *Pz = P + ((size_t)band * g.n3 + z) * g.n2 * g.nxa;
+  for (int e = threadIdx.x; e < T2 * g.n2; e += blockDim.x) {
+    const int y = e / T2, t = e - y * T2;
+    if (t < nx) Pz[(size_t)y * g.nxa + x0 + t] = r[t * ls + y];
+  }
+}
+
+// ---------------------------------------------------------------- pass 3
+template <typename T, typename R>
+__global__ void __launch_bounds__(kNT) k_xlines(Geo g, FftArg fx, const T *__restrict__ wx,
+                                                const R *__restrict__ vs, T *__restrict__ P,
+                                                int L3) {
+  extern __shared__ unsigned char smem_raw[];
+  T *a = reinterpret_cast<T *>(smem_raw);
+  const int ls = pad(g.n1);
+  T *b = a + L3 * ls;
+  const int l0 = blockIdx.x * L3;
+  const int band = blockIdx.y;
+  const int nlines = g.n2 * g.n3;
+  const int nl = min(L3, nlines - l0);
+  T *Pb = P + (size_t)band * nlines * g.nxa;
+  for (int e = threadIdx.x; e < L3 * g.n1; e += blockDim.x) {
+    const int l = e / g.n1, x = e - l * g.n1;
+    T v = czero<T>();
+    if (l < nl) {
+      const int xa = g.xa_of_x[x];
+      if (xa >= 0) v = Pb[(size_t)(l0 + l) * g.nxa + xa];
+    }
+    a[l * ls + x] = v;
+  }
+  __syncthreads();
+  T *r = fft_lines(a, b, L3, ls, fx, wx, +1);
+  T *o = (r == a) ? b : a;
+  for (int e = threadIdx.x; e < L3 * g.n1; e += blockDim.x) {
+    const int l = e / g.n1, x = e - l * g.n1;
+    const R v = (l < nl) ? vs[(size_t)(l0 + l) * g.n1 + x] : (R)0;
+    const T u = r[l * ls + x];
+    r[l * ls + x] = mk<T>(v * u.x, v * u.y);
+  }
+  __syncthreads();
+  r = fft_lines(r, o, L3, ls, fx, wx, -1);
+  for (int e = threadIdx.x; e < L3 * g.nxa; e += blockDim.x) {
+    const int l = e / g.nxa, xa = e - l * g.nxa;
+    if (l < nl) Pb[(size_t)(l0 + l) * g.nxa + xa] = r[l * ls + g.xa_list[xa]];
+  }
+}
+
+// ---------------------------------------------------------------- pass 4
+template <typename T>
+__global__ void __launch_bounds__(kNT) k_planes_fwd(Geo g, FftArg fy, const T *__restrict__ wy,
+                                                    const T *__restrict__ P, T *__restrict__ S,
+                                                    int T2) {
+  extern __shared__ unsigned char smem_raw[];
+  T *a = reinterpret_cast<T *>(smem_raw);
+  const int ls = pad(g.n2);
+  T *b = a + T2 * ls;
+  const int x0 = blockIdx.x * T2;
+  const int z = blockIdx.y;
+  const int band = blockIdx.z;
+  const int nx = min(T2, g.nxa - x0);
+  const T *Pz = P + ((size_t)band * g.n3 + z) * g.n2 * g.nxa;
+  for (int e = threadIdx.x; e < T2 * g.n2; e += blockDim.x) {
+    const int y = e / T2, t = e - y * T2;
+    a[t * ls + y] = (t < nx) ? Pz[(size_t)y * g.nxa + x0 + t] : czero<T>();
+  }
+  __syncthreads();
+  T *r = fft_lines(a, b, T2, ls, fy, wy, -1);
+  T *Sz = S + ((size_t)band * g.n3 + z) * g.ncol;
+  for (int e = threadIdx.x; e < T2 * g.n2; e += blockDim.x) {
+    const int y = e / T2, t = e - y * T2;
+    if (t < nx) {
+      const int c = g.col_of_xy[g.xa_list[x0 + t] + g.n1 * y];
+      if (c >= 0) Sz[c] = r[t * ls + y];
+    }
+  }
+}
+
+// ---------------------------------------------------------------- pass 5
+template <typename T, typename R>
+__global__ void __launch_bounds__(kNT) k_sticks_fwd(Geo g, FftArg fz, const T *__restrict__ wz,
+                                                    const T *__restrict__ S,
+                                                    const R *__restrict__ kin,
+                                                    const T *__restrict__ psi, int ld,
+                                                    T *__restrict__ out, int ldo, int ngw_call,
+                                                    int T1) {
+  extern __shared__ unsigned char smem_raw[];
+  T *a = reinterpret_cast<T *>(smem_raw);
+  const int ls = pad(g.n3);
+  T *b = a + T1 * ls;
+  const int c0 = blockIdx.x * T1;
+  const int band = blockIdx.y;
+  const int nc = min(T1, g.ncol - c0);
+  const T *Sb = S + (size_t)band * g.n3 * g.ncol;
+  for (int e = threadIdx.x; e < T1 * g.n3; e += blockDim.x) {
+    const int z = e / T1, t = e - z * T1;
+    a[t * ls + z] = (t < nc) ? Sb[(size_t)z * g.ncol + c0 + t] : czero<T>();
+  }
+  __syncthreads();
+  T *r = fft_lines(a, b, T1, ls, fz, wz, -1);
+  const T *pb = psi + (size_t)band * ld;
+  T *ob = out + (size_t)band * ldo;
+  const int k0 = g.col_start[c0], k1 = g.col_start[c0 + nc];
+  for (int k = k0 + threadIdx.x; k < k1; k += blockDim.x) {
+    const int ig = g.sg_ig[k];
+    if (ig < ngw_call) {
+      const R kk = kin[ig];
+      const T p = pb[ig];
+      const T f = r[(g.sg_col[k] - c0) * ls + g.sg_z[k]];
+      ob[ig] = mk<T>(kk * p.x + f.x, kk * p.y + f.y);
+    }
+  }
+}
+
+// ---------------------------------------------------------------- nonlocal
+constexpr int kBM = 64, kBN = 64;
+
+struct ProjArg {
+  const void *eigr;  // cx<R>[nat][ngw]
+  const void *pkga;  // R[nsp][ngw][4]
+  const int *patom, *psp, *plm;
+  const void *pw;  // R[nproj]
+  int ngw_cell, nproj;
+};
+
+template <typename R>
+__device__ __forceinline__ cx<R> beta_at(const ProjArg &pa, int ig, int p) {
+  const cx<R> e = reinterpret_cast<const cx<R> *>(pa.eigr)[(size_t)pa.patom[p] * pa.ngw_cell + ig];
+  const R f = reinterpret_cast<const R *>(pa.pkga)[((size_t)pa.psp[p] * pa.ngw_cell + ig) * 4 + pa.plm[p]];
+  return mk<cx<R>>(e.x * f, e.y * f);
+}
+
+// part[(split*nb + b)*nproj + p] = sum_{ig in split} conj(beta_p(ig)) psi_b(ig)
+template <typename R, int BK>
+__global__ void __launch_bounds__(256) k_proj(ProjArg pa, const cx<R> *__restrict__ psi, int ld,
+                                              int ngw, int nb, int kchunk, cx<R> *__restrict__ part) {
+  using T = cx<R>;
+  __shared__ T As[BK][kBM + 1];
+  __shared__ T Bs[BK][kBN + 1];
+  const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
+  const int p0 = blockIdx.x * kBM, b0 = blockIdx.y * kBN;
+  const int kb = blockIdx.z * kchunk;
+  const int ke = min(ngw, kb + kchunk);
+  T acc[4][4];
+#pragma unroll
+  for (int i = 0; i < 4; i++)
+#pragma unroll
+    for (int j = 0; j < 4; j++) acc[i][j] = czero<T>();
+  for (int k0 = kb; k0 < ke; k0 += BK) {
+    for (int e = threadIdx.x; e < BK * kBM; e += 256) {
+      const int kk = e % BK, m = e / BK;
+      const int ig = k0 + kk, p = p0 + m;
+      As[kk][m] = (ig < ke && p < pa.nproj) ? beta_at<R>(pa, ig, p) : czero<T>();
+    }
+    for (int e = threadIdx.x; e < BK * kBN; e += 256) {
+      const int kk = e % BK, n = e / BK;
+      const int ig = k0 + kk, bb = b0 + n;
+      Bs[kk][n] = (ig < ke && bb < nb) ? psi[(size_t)bb * ld + ig] : czero<T>();
+    }
+    __syncthreads();
+#pragma unroll 4
+    for (int kk = 0; kk < BK; kk++) {
+      T av[4], bv[4];
+#pragma unroll
+      for (int i = 0; i < 4; i++) av[i] = As[kk][tx + 16 * i];
+#pragma unroll
+      for (int j = 0; j < 4; j++) bv[j] = Bs[kk][ty + 16 * j];
+#pragma unroll
+      for (int i = 0; i < 4; i++)
+#pragma unroll
+        for (int j = 0; j < 4; j++) cfmac(acc[i][j], av[i], bv[j]);
+    }
+    __syncthreads();
+  }
+#pragma unroll
+  for (int i = 0; i < 4; i++)
+#pragma unroll
+    for (int j = 0; j < 4; j++) {
+      const int p = p0 + tx + 16 * i, bb = b0 + ty + 16 * j;
+      if (p < pa.nproj && bb < nb) part[((size_t)blockIdx.z * nb + bb) * pa.nproj + p] = acc[i][j];
+    }
+}
+
+// wp[b*nproj + p] = W_p * sum_s part[(s*nb + b)*nproj + p]   (fixed order in s)
+template <typename R>
+__global__ void k_proj_reduce(const cx<R> *__restrict__ part, const R *__restrict__ w, int nsplit,
+                              int nb, int nproj, cx<R> *__restrict__ wp) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= nb * nproj) return;
+  const int p = i % nproj;
+  cx<R> s = part[i];
+  for (int k = 1; k < nsplit; k++) s = s + part[(size_t)k * nb * nproj + i];
+  wp[i] = mk<cx<R>>(w[p] * s.x, w[p] * s.y);
+}
+
+// out = a*(out + sum_p beta_p(ig) wp[b][p]) + bc*in + g*xm2
+template <typename R, int BK>
+__global__ void __launch_bounds__(256) k_backproj(ProjArg pa, const cx<R> *__restrict__ wp, int ngw,
+                                                  int nb, cx<R> *out, int ldo,
+                                                  const cx<R> *__restrict__ in, int ldi,
+                                                  const cx<R> *__restrict__ xm2, int ldx, R a,
+                                                  R bc, R gc) {
+  using T = cx<R>;
+  __shared__ T As[BK][kBM + 1];
+  __shared__ T Bs[BK][kBN + 1];
+  const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
+  const int g0 = blockIdx.x * kBM, b0 = blockIdx.y * kBN;
+  T acc[4][4];
+#pragma unroll
+  for (int i = 0; i < 4; i++)
+#pragma unroll
+    for (int j = 0; j < 4; j++) acc[i][j] = czero<T>();
+  for (int k0 = 0; k0 < pa.nproj; k0 += BK) {
+    for (int e = threadIdx.x; e < BK * kBM; e += 256) {
+      const int m = e % kBM, kk = e / kBM;
+      const int ig = g0 + m, p = k0 + kk;
+      As[kk][m] = (ig < ngw && p < pa.nproj) ? beta_at<R>(pa, ig, p) : czero<T>();
+    }
+    for (int e = threadIdx.x; e < BK * kBN; e += 256) {
+      const int kk = e % BK, n = e / BK;
+      const int p = k0 + kk, bb = b0 + n;
+      Bs[kk][n] = (p < pa.nproj && bb < nb) ? wp[(size_t)bb * pa.nproj + p] : czero<T>();
+    }
+    __syncthreads();
+#pragma unroll 4
+    for (int kk = 0; kk < BK; kk++) {
+      T av[4], bv[4];
+#pragma unroll
+      for (int i = 0; i < 4; i++) av[i] = As[kk][tx + 16 * i];
+#pragma unroll
+      for (int j = 0; j < 4; j++) bv[j] = Bs[kk][ty + 16 * j];
+#pragma unroll
+      for (int i = 0; i < 4; i++)
+#pragma unroll
+        for (int j = 0; j < 4; j++) cfma(acc[i][j], av[i], bv[j]);
+    }
+    __syncthreads();
+  }
+#pragma unroll
+  for (int j = 0; j < 4; j++) {
+    const int bb = b0 + ty + 16 * j;
+    if (bb >= nb) continue;
+#pragma unroll
+    for (int i = 0; i < 4; i++) {
+      const int ig = g0 + tx + 16 * i;
+      if (ig >= ngw) continue;
+      T h = out[(size_t)bb * ldo + ig] + acc[i][j];
+      T v = mk<T>(a * h.x, a * h.y);
+      if (bc != (R)0) {
+        const T u = in[(size_t)bb * ldi + ig];
+        v.x += bc * u.x;
+        v.y += bc * u.y;
+      }
+      if (gc != (R)0) {
+        const T u = xm2[(size_t)bb * ldx + ig];
+        v.x += gc * u.x;
+        v.y += gc * u.y;
+      }
+      out[(size_t)bb * ldo + ig] = v;
+    }
+  }
+}
+
+// out = a*out + bc*in + g*xm2 (no projectors)
+template <typename R>
+__global__ void k_axpby3(int ngw, int nb, cx<R> *out, int ldo, const cx<R> *__restrict__ in,
+                         int ldi, const cx<R> *__restrict__ xm2, int ldx, R a, R bc, R gc) {
+  const size_t n = (size_t)ngw * nb;
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
+       i += (size_t)gridDim.x * blockDim.x) {
+    const int bb = (int)(i / ngw), ig = (int)(i - (size_t)bb * ngw);
+    cx<R> h = out[(size_t)bb * ldo + ig];
+    cx<R> v = mk<cx<R>>(a * h.x, a * h.y);
+    if (bc != (R)0) {
+      const cx<R> u = in[(size_t)bb * ldi + ig];
+      v.x += bc * u.x;
+      v.y += bc * u.y;
+    }
+    if (gc != (R)0) {
+      const cx<R> u = xm2[(size_t)bb * ldx + ig];
+      v.x += gc * u.x;
+      v.y += gc * u.y;
+    }
+    out[(size_t)bb * ldo + ig] = v;
+  }
+}
+
+template <typename R>
+struct Prec;
+template <>
+struct Prec<double> {
+  static const double *veff(const pspw_cell *c) { return c->d_veff64; }
+  static const double *kin(const pspw_cell *c) { return c->basis.d_kin64; }
+  static const void *eigr(const pspw_cell *c) { return c->proj.d_eigr64; }
+  static const void *pkga(const pspw_cell *c) { return c->proj.d_pkga64; }
+  static const double *pw(const pspw_cell *c) { return c->proj.d_pw64; }
+};
+template <>
+struct Prec<float> {
+  static const float *veff(const pspw_cell *c) { return c->d_veff32; }
+  static const float *kin(const pspw_cell *c) { return c->basis.d_kin32; }
+  static const void *eigr(const pspw_cell *c) { return c->proj.d_eigr32; }
+  static const void *pkga(const pspw_cell *c) { return c->proj.d_pkga32; }
+  static const float *pw(const pspw_cell *c) { return c->proj.d_pw32; }
+};
+
+int tile_lines(int n) { return std::max(1, std::min(64, kTileElems / n)); }
+
+template <typename T>
+size_t pass_smem(int lines, int n) {
+  return (size_t)2 * lines * pad(n) * sizeof(T);
+}
+
+template <typename T, typename K>
+int set_smem(K kernel, size_t bytes) {
+  if (bytes > 48 * 1024)
+    PSPW_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
+  return PSPW_OK;
+}
+
+}  // namespace
+
+template <typename R>
+int hpsi_apply(pspw_cell *c, const void *in_v, int ld_in, void *out_v, int ld_out, int ngw, int nb,
+               double a, double b, double g, const void *xm2_v, int ld_xm2) {
+  using T = cx<R>;
+  const Basis &B = c->basis;
+  if (nb <= 0) return PSPW_OK;
+  if (!in_v || !out_v) return fail(PSPW_ERR_ARG, "hpsi: null block");
+  if (in_v == out_v) return fail(PSPW_ERR_ARG, "hpsi: input and output blocks must differ");
+  if (ngw <= 0 || ngw > B.ngw) return fail(PSPW_ERR_SHAPE, "hpsi: ngw exceeds the cell's sphere");
+  if (ld_in < ngw || ld_out < ngw) return fail(PSPW_ERR_SHAPE, "hpsi: leading dimension < ngw");
+  if (g != 0.0 && (!xm2_v || ld_xm2 < ngw)) return fail(PSPW_ERR_ARG, "hpsi: missing x(d-2)");
+  if (!c->veff_set) return fail(PSPW_ERR_ARG, "hpsi: V_eff not set (pspw_cell_set_veff)");
+  const T *in = static_cast<const T *>(in_v);
+  T *out = static_cast<T *>(out_v);
+  const T *xm2 = static_cast<const T *>(xm2_v);
+  cudaStream_t st = c->stream;
+
+  // ---- projection
+  const int nproj = c->proj.nproj;
+  ProjArg pa;
+  pa.eigr = Prec<R>::eigr(c);
+  pa.pkga = Prec<R>::pkga(c);
+  pa.patom = c->proj.d_patom;
+  pa.psp = c->proj.d_psp;
+  pa.plm = c->proj.d_plm;
+  pa.pw = Prec<R>::pw(c);
+  pa.ngw_cell = B.ngw;
+  pa.nproj = nproj;
+  constexpr int BK = sizeof(R) == 8 ? 16 : 32;
+  T *wp = nullptr;
+  cudaEvent_t ev = nullptr;
+  if (nproj > 0) {
+    const int mt = (nproj + kBM - 1) / kBM, nt = (nb + kBN - 1) / kBN;
+    // split G so the grid covers the GPU about twice
+    int nsplit = std::max(1, std::min((ngw + 255) / 256, (2 * 148 + mt * nt - 1) / (mt * nt)));
+    int kchunk = (ngw + nsplit - 1) / nsplit;
+    kchunk = (kchunk + BK - 1) / BK * BK;
+    nsplit = (ngw + kchunk - 1) / kchunk;
+    T *part = nullptr;
+    int rc = ws_reserve(c, 2, sizeof(T) * (size_t)nsplit * nb * nproj, (void **)&part);
+    if (rc) return rc;
+    rc = ws_reserve(c, 3, sizeof(T) * (size_t)nb * nproj, (void **)&wp);
+    if (rc) return rc;
+    timing_begin(c, 2, &ev);
+    k_proj<R, BK><<<dim3(mt, nt, nsplit), 256, 0, st>>>(pa, in, ld_in, ngw, nb, kchunk, part);
+    k_proj_reduce<R><<<(nb * nproj + 255) / 256, 256, 0, st>>>(part, Prec<R>::pw(c), nsplit, nb,
+                                                              nproj, wp);
+    timing_end(c, 2, ev);
+    PSPW_CUDA(cudaGetLastError());
+  }
+
+  // ---- local part, in batches of bands
+  Geo geo{B.n1, B.n2, B.n3, B.ncol, B.nxa, B.ngw, B.d_col_start, B.d_sg_ig, B.d_sg_z,
+          B.d_sg_col, B.d_col_of_xy, B.d_xa_list, B.d_xa_of_x};
+  const size_t s_band = (size_t)B.n3 * B.ncol, p_band = (size_t)B.n3 * B.n2 * B.nxa;
+  int nbatch = c->band_batch;
+  if (nbatch <= 0) {
+    // keep a batch's stick and plane buffers within ~48 MB so they stay in L2
+    nbatch = (int)std::max<size_t>(1, (48u << 20) / ((s_band + p_band) * sizeof(T)));
+  }
+  nbatch = std::min(nbatch, nb);
+  T *S = nullptr, *P = nullptr;
+  int rc = ws_reserve(c, 0, sizeof(T) * s_band * nbatch, (void **)&S);
+  if (rc) return rc;
+  rc = ws_reserve(c, 1, sizeof(T) * p_band * nbatch, (void **)&P);
+  if (rc) return rc;
+  const int T1 = tile_lines(B.n3), T2 = tile_lines(B.n2), L3 = tile_lines(B.n1);
+  const size_t sm1 = pass_smem<T>(T1, B.n3), sm2 = pass_smem<T>(T2, B.n2),
+               sm3 = pass_smem<T>(L3, B.n1);
+  if ((rc = set_smem<T>(k_sticks_inv<T>, sm1)) || (rc = set_smem<T>(k_sticks_fwd<T, R>, sm1)) ||
+      (rc = set_smem<T>(k_planes_inv<T>, sm2)) || (rc = set_smem<T>(k_planes_fwd<T>, sm2)) ||
+      (rc = set_smem<T>(k_xlines<T, R>, sm3)))
+    return rc;
+  const FftArg fx = fft_arg(B.dim[0]), fy = fft_arg(B.dim[1]), fz = fft_arg(B.dim[2]);
+  const T *wx = tw<T>(B.dim[0]), *wy = tw<T>(B.dim[1]), *wz = tw<T>(B.dim[2]);
+  timing_begin(c, 1, &ev);
+  for (int b0 = 0; b0 < nb; b0 += nbatch) {
+    const int nbb = std::min(nbatch, nb - b0);
+    const T *inb = in + (size_t)b0 * ld_in;
+    T *outb = out + (size_t)b0 * ld_out;
+    k_sticks_inv<T><<<dim3((B.ncol + T1 - 1) / T1, nbb), kNT, sm1, st>>>(geo, fz, wz, inb, ld_in,
+                                                                          ngw, S, T1);
+    k_planes_inv<T><<<dim3((B.nxa + T2 - 1) / T2, B.n3, nbb), kNT, sm2, st>>>(geo, fy, wy, S, P, T2);
+    k_xlines<T, R><<<dim3((B.n2 * B.n3 + L3 - 1) / L3, nbb), kNT, sm3, st>>>(
+        geo, fx, wx, Prec<R>::veff(c), P, L3);
+    k_planes_fwd<T><<<dim3((B.nxa + T2 - 1) / T2, B.n3, nbb), kNT, sm2, st>>>(geo, fy, wy, P, S, T2);
+    k_sticks_fwd<T, R><<<dim3((B.ncol + T1 - 1) / T1, nbb), kNT, sm1, st>>>(
+        geo, fz, wz, S, Prec<R>::kin(c), inb, ld_in, outb, ld_out, ngw, T1);
+  }
+  timing_end(c, 1, ev);
+  PSPW_CUDA(cudaGetLastError());
+
+  // ---- back-projection + recurrence epilogue
+  if (nproj > 0) {
+    timing_begin(c, 2, &ev);
+    dim3 grid((ngw + kBM - 1) / kBM, (nb + kBN - 1) / kBN);
+    k_backproj<R, BK><<<grid, 256, 0, st>>>(pa, wp, ngw, nb, out, ld_out, in, ld_in, xm2, ld_xm2,
+                                            (R)a, (R)b, (R)g);
+    timing_end(c, 2, ev);
+  } else if (a != 1.0 || b != 0.0 || g != 0.0) {
+    k_axpby3<R><<<4 * 148, 256, 0, st>>>(ngw, nb, out, ld_out, in, ld_in, xm2, ld_xm2, (R)a, (R)b,
+                                        (R)g);
+  }
+  PSPW_CUDA(cudaGetLastError());
+  return PSPW_OK;
+}
+
+template int hpsi_apply<double>(pspw_cell *, const void *, int, void *, int, int, int, double,
+                                double, double, const void *, int);
+template int hpsi_apply<float>(pspw_cell *, const void *, int, void *, int, int, int, double,
+                               double, double, const void *, int);
+
+}  // namespace pspw

@@ -1,0 +1,163 @@
+"""Host-side handles over the C ABI: basis generation and the device cell.
+
+``Cell`` mirrors the reference's device API (SetupArrays_ApplyHam_cuda /
+CopyRho_ApplyHam_cuda / ApplyHam_block_cuda, common_pspw.h:252-259) with an
+explicit handle; arrays use the reference's Fortran layouts.
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from ._lib import PREC_F32, PREC_F64, BasisInfo, check, lib, ptr
+
+
+def _f(a, dtype):
+    return np.asfortranarray(np.asarray(a, dtype=dtype))
+
+
+def _flat(a, dtype):
+    return np.ascontiguousarray(np.asarray(a, dtype=dtype).reshape(-1, order="F"))
+
+
+def basis_gamma(lattice, ecut_ry, nr=None, na=(), tau=()):
+    """The reference's Gamma-point basis (Setup/GVectorsGen/GkVectorsGen/
+    PhaseFactor) for lattice rows A1, A2, A3 in bohr and ECUT in Rydberg.
+    tau: list per species of (na, 3) positions in bohr."""
+    L = lib()
+    lat = np.ascontiguousarray(np.asarray(lattice, dtype=float).reshape(9))
+    nrf = np.asarray(nr if nr is not None else (0, 0, 0), dtype=np.int32)
+    info = BasisInfo()
+    check(L.pspw_basis_info_gamma(lat.ctypes.data, float(ecut_ry), nrf.ctypes.data, C.byref(info)))
+    ngwx, ngx = info.ngwx, info.ngx
+    nsp = max(1, len(na))
+    na_arr = np.asarray(list(na) if len(na) else [0], dtype=np.int32)
+    nax = int(max(1, na_arr.max()))
+    taua = np.zeros((nsp, nax, 3))
+    for s in range(len(na)):
+        taua[s, : na[s]] = np.asarray(tau[s], dtype=float).reshape(na[s], 3)
+    out = dict(n123=np.zeros(ngwx, np.uint32), xkg=np.zeros(ngwx), igk=np.zeros(ngwx, np.int32),
+               N1=np.zeros(ngx, np.int32), N2=np.zeros(ngx, np.int32), N3=np.zeros(ngx, np.int32),
+               IN1=np.zeros(ngx, np.int32), IN2=np.zeros(ngx, np.int32),
+               IN3=np.zeros(ngx, np.int32), G=np.zeros(ngx), GG=np.zeros((ngx + 1) * 3),
+               eigr=np.zeros(2 * ngwx * nax * nsp))
+    check(L.pspw_basis_build_gamma(
+        lat.ctypes.data, float(ecut_ry), nrf.ctypes.data, nsp, na_arr.ctypes.data,
+        np.ascontiguousarray(taua.reshape(-1)).ctypes.data, C.byref(info),
+        *(out[k].ctypes.data for k in ("n123", "xkg", "igk", "N1", "N2", "N3", "IN1", "IN2", "IN3",
+                                       "G", "GG", "eigr"))))
+    out["eigr"] = out["eigr"].view(np.complex128).reshape((ngwx, nax, nsp), order="F")
+    out.update(nr=tuple(info.nr), ngw=info.ngw, ngwx=ngwx, ngx=ngx, ng=info.ng, alat=info.alat,
+               omega=info.omega, tpiba=info.tpiba, tpiba2=info.tpiba2, gcut=info.gcut,
+               gcutw=info.gcutw, nax=nax, nsp=nsp, na=list(na))
+    return out
+
+
+class Cell:
+    """One geometry/k-point on one GPU (pspw_cell)."""
+
+    def __init__(self, nr, ngw, ngwx, n123, xkg, tpiba2, na, lm_end, eigr, pkg_a, wnl, device=0):
+        L = lib()
+        self._h = C.c_void_p()
+        nsp = len(na)
+        nax = int(max(na)) if nsp else 0
+        nlmax = int(np.asarray(pkg_a).shape[0]) if nsp else 4
+        self._keep = dict(
+            n123=np.ascontiguousarray(np.asarray(n123, dtype=np.uint32)),
+            xkg=np.ascontiguousarray(np.asarray(xkg, dtype=float)),
+            na=np.asarray(na, dtype=np.int32), lm_end=np.asarray(lm_end, dtype=np.int32),
+            eigr=_flat(eigr, np.complex128).view(np.float64), pkg_a=_flat(pkg_a, float),
+            wnl=_flat(wnl, float))
+        k = self._keep
+        check(L.pspw_cell_create(C.byref(self._h), int(device), int(nr[0]), int(nr[1]), int(nr[2]),
+                                 int(ngw), int(ngwx), k["n123"].ctypes.data, k["xkg"].ctypes.data,
+                                 float(tpiba2), nsp, k["na"].ctypes.data, nax,
+                                 k["lm_end"].ctypes.data, nlmax, k["eigr"].ctypes.data,
+                                 k["pkg_a"].ctypes.data, k["wnl"].ctypes.data))
+        self.nr = tuple(int(x) for x in nr)
+        self.nnr = self.nr[0] * self.nr[1] * self.nr[2]
+        self.ngw = int(ngw)
+        self.device = device
+
+    @classmethod
+    def from_arrays(cls, cell, device=0):
+        """From a dict with keys nr, ngw, ngwx, n123, xkg, tpiba2, na, lm_end,
+        eigr, pkg_a, wnl (the reference's arrays)."""
+        return cls(cell["nr"], cell["ngw"], cell["ngwx"], cell["n123"], cell["xkg"],
+                   cell["tpiba2"], cell["na"], cell["lm_end"], cell["eigr"], cell["pkg_a"],
+                   cell["wnl"], device=device)
+
+    @property
+    def handle(self):
+        return self._h
+
+    def close(self):
+        if self._h:
+            lib().pspw_cell_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def sizes(self):
+        o = np.zeros(8, dtype=np.int32)
+        check(lib().pspw_cell_sizes(self._h, o.ctypes.data))
+        return dict(zip(("n1", "n2", "n3", "ngw", "nsticks", "nxa", "nat", "nproj"), o.tolist()))
+
+    def stream(self):
+        s = C.c_void_p()
+        check(lib().pspw_cell_get_stream(self._h, C.byref(s)))
+        return s.value
+
+    def set_veff(self, veff):
+        v = np.ascontiguousarray(np.asarray(veff, dtype=float).reshape(-1))
+        check(lib().pspw_cell_set_veff(self._h, v.ctypes.data, v.size))
+
+    def set_band_batch(self, n):
+        check(lib().pspw_cell_set_band_batch(self._h, int(n)))
+
+    # ---- host FP64 (the reference signatures' data)
+    def apply_ham_block(self, vin):
+        vin = _f(vin, np.complex128)
+        if vin.ndim == 1:
+            vin = vin[:, None]
+        ngw, nb = vin.shape
+        out = np.zeros((ngw, nb), dtype=np.complex128, order="F")
+        check(lib().pspw_apply_ham_block(self._h, vin.ctypes.data, out.ctypes.data, ngw, nb))
+        return out
+
+    def chebyfilt(self, X, degree, lb, ub, prec=PREC_F64):
+        X = np.array(_f(X, np.complex128), order="F", copy=True)
+        ngw, nb = X.shape
+        check(lib().pspw_chebyfilt(self._h, X.ctypes.data, ngw, nb, int(degree), float(lb),
+                                   float(ub), int(prec)))
+        return X
+
+    # ---- device buffers (torch tensors), enqueued on the cell stream
+    def apply_ham_block_dev(self, d_in, d_out, ld, ngw, nb, prec):
+        check(lib().pspw_apply_ham_block_dev(self._h, int(prec), ptr(d_in), ptr(d_out), int(ld),
+                                             int(ngw), int(nb)))
+
+    def chebyfilt_dev(self, d_x, ld, ngw, nb, degree, lb, ub, prec):
+        check(lib().pspw_chebyfilt_dev(self._h, int(prec), ptr(d_x), int(ld), int(ngw), int(nb),
+                                       int(degree), float(lb), float(ub)))
+
+    # ---- timing
+    def timing_enable(self, mask):
+        check(lib().pspw_timing_enable(self._h, int(mask)))
+
+    def timing_read(self, family):
+        ms = C.c_double()
+        n = C.c_longlong()
+        check(lib().pspw_timing_read(self._h, int(family), C.byref(ms), C.byref(n)))
+        return ms.value, n.value
+
+    def timing_reset(self):
+        check(lib().pspw_timing_reset(self._h))
+
+
+__all__ = ["Cell", "basis_gamma", "PREC_F32", "PREC_F64"]

@@ -74,7 +74,6 @@ def kb_form_factors(basis, lattice, nsp=1, rc=1.0, weights=(1.5, 0.8, 0.8, 0.8),
     xkg = np.asarray(basis["xkg"])
     t = np.sqrt(xkg[:ngw])
     q = t * tpiba
-    rad = np.exp(-0.5 * (q * rc) ** 2)
     gc = gk_cartesian(basis, lattice)[:ngw]
     pkg_a = np.zeros((nlmax, ngwx, nsp), order="F")
     wnl = np.zeros((nsp, nlmax), order="F")
@@ -86,7 +85,6 @@ def kb_form_factors(basis, lattice, nsp=1, rc=1.0, weights=(1.5, 0.8, 0.8, 0.8),
         for a in range(3):
             pkg_a[1 + a, :ngw, s] = np.where(nz, rad_s * gc[:, a] / np.where(nz, t, 1.0), 0.0)
         wnl[s, : len(weights)] = weights
-    del rad
     return pkg_a, wnl
 
 

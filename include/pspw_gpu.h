@@ -1,0 +1,145 @@
+/*
+ * pspw_gpu.h -- C ABI of the B200 Hamiltonian-application and eigensolver
+ * engine for the plane-wave Kohn-Sham method of f-fathurrahman/ffr-pspw-dft-c.
+ *
+ * Plain pointers and sizes only.  Complex arrays are interleaved (re, im)
+ * doubles (layout-identical to C99 `double complex`) or floats, column-major
+ * with an explicit leading dimension, exactly as the reference stores them.
+ * Every entry point returns a status code (PSPW_OK = 0); pspw_last_error()
+ * gives the message of the last failure on the calling thread.
+ *
+ * Handle model: one pspw_cell per geometry and k-point holds device copies of
+ * the basis and projector arrays and of V_eff(r), plus a CUDA stream and
+ * persistent workspaces.  Calls on one cell are serialised by the caller;
+ * different cells are independent.
+ *
+ * Reference interfaces replaced (file:line in the reference repository):
+ *   pspw_cell_create         SetupArrays_ApplyHam_cuda   common_pspw.h:255
+ *   pspw_cell_set_veff       CopyRho_ApplyHam_cuda       common_pspw.h:257
+ *   pspw_cell_destroy        FreeArrays_ApplyHam_cuda    common_pspw.h:258
+ *   pspw_apply_ham_block     ApplyHam_block              common_pspw.h:177, ApplyHam_block.cpp:5
+ *   pspw_apply_ham_block_dev ApplyHam_block_cuda         common_pspw.h:254
+ *   pspw_chebyfilt           chebyfilt                   common_pspw.h:187, chebyfilt.cpp:6
+ */
+#ifndef PSPW_GPU_H
+#define PSPW_GPU_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#if defined(__GNUC__)
+#pragma GCC visibility push(default)
+#endif
+
+/* status codes */
+#define PSPW_OK 0
+#define PSPW_ERR_ARG 1       /* invalid argument (null pointer, negative size)   */
+#define PSPW_ERR_SHAPE 2     /* inconsistent sizes (nnr != NNR, ngw > cell ngw)  */
+#define PSPW_ERR_CUDA 3      /* CUDA runtime / library failure                    */
+#define PSPW_ERR_OOM 4       /* device allocation failed                          */
+#define PSPW_ERR_NONFINITE 5 /* NaN/Inf detected in an input that is checked      */
+#define PSPW_ERR_TIMEOUT 6   /* a bounded device-side wait ran out                */
+#define PSPW_ERR_LAPACK 7    /* dense factorisation/eigensolver info != 0         */
+#define PSPW_ERR_CHARGE 8    /* EvalRhoPsi: |sum |c|^2 - 1| > 6e-3                */
+#define PSPW_ERR_NOT_IMPL 9  /* e.g. more than 4 KB projectors per atom           */
+
+/* arithmetic of device-resident wavefunction blocks */
+#define PSPW_PREC_F64 0 /* complex128 (interleaved double) */
+#define PSPW_PREC_F32 1 /* complex64  (interleaved float)  */
+
+typedef struct pspw_cell pspw_cell;
+
+typedef struct {
+  int nr[3];   /* FFT grid NR1, NR2, NR3                 */
+  int ngw;     /* wavefunction sphere size NGW(1)        */
+  int ngwx;    /* padded leading dimension NGWX          */
+  int ngx;     /* NGX                                    */
+  int ng;      /* density sphere size NG                 */
+  double alat, omega, tpiba, tpiba2, gcut, gcutw;
+} pspw_basis_info;
+
+const char *pspw_error_string(int code);
+const char *pspw_last_error(void);
+int pspw_version(void);
+
+/* ------------------------------------------------------------------ basis
+ * Gamma-point basis generation with the reference's set-up rules
+ * (Setup.cpp:20-66, GVectorsGen0.cpp, GVectorsGen.cpp, GkVectorsGen.cpp,
+ * PhaseFactor.cpp).  lattice9 = A1, A2, A3 (bohr), ecut_ry = ECUT in Rydberg,
+ * nr_forced = {NR1,NR2,NR3} or NULL/{0,..} for the reference grid rule.
+ * _info fills sizes (ngw and ng stay -1 until _build); _build fills the
+ * arrays: n123/xkg/igk [ngwx]; n1..in3, g [ngx]; gg [(ngx+1)*3];
+ * eigr [2*ngwx*nax*nsp] (may be NULL), tau = TAU(3,NAX,NSP) in bohr. */
+int pspw_basis_info_gamma(const double *lattice9, double ecut_ry, const int *nr_forced,
+                          pspw_basis_info *info);
+int pspw_basis_build_gamma(const double *lattice9, double ecut_ry, const int *nr_forced, int nsp,
+                           const int *na, const double *tau, pspw_basis_info *info,
+                           unsigned int *n123, double *xkg, int *igk, int *n1, int *n2, int *n3,
+                           int *in1, int *in2, int *in3, double *g, double *gg, double *eigr);
+
+/* ------------------------------------------------------------------ cell
+ * Device copy of one k-point's Hamiltonian data (replaces
+ * SetupArrays_ApplyHam_cuda, common_pspw.h:255).  Arguments are the
+ * reference globals for column ik:
+ *   n123[ngwx]   N123(:,ik), 1-based FFT-grid index        (GkVectorsGen.cpp:379)
+ *   xkg[ngwx]    XKG(:,ik), |k+G|^2 in (2 pi/ALAT)^2
+ *   eigr         EIGR(:,:,:,ik), 2*ngwx*nax*nsp doubles
+ *   pkg_a        PKG_A(:,:,:,ik), nlmax*ngwx*nsp doubles
+ *   wnl          WNL(nsp, nlmax)
+ *   lm_end[nsp]  L_MAX^2 - 2 L_LOC + 1 per species (<= 4, ApplyHam_block.cpp:69-73)
+ * ngw is the number of plane waves of this k-point (NGW(ik)). */
+int pspw_cell_create(pspw_cell **cell, int device, int nr1, int nr2, int nr3, int ngw, int ngwx,
+                     const unsigned int *n123, const double *xkg, double tpiba2, int nsp,
+                     const int *na, int nax, const int *lm_end, int nlmax, const double *eigr,
+                     const double *pkg_a, const double *wnl);
+int pspw_cell_destroy(pspw_cell *cell);
+/* V_eff(r) on the FFT grid, NR1 fastest (the `rho` argument of ApplyHam*;
+ * replaces CopyRho_ApplyHam_cuda, common_pspw.h:257).  nnr must equal
+ * NR1*NR2*NR3 (ApplyHam_block.cpp:18-21). */
+int pspw_cell_set_veff(pspw_cell *cell, const double *veff, int nnr);
+int pspw_cell_set_veff_device(pspw_cell *cell, const double *d_veff, int nnr);
+/* the cell's CUDA stream (cudaStream_t) and basic sizes */
+int pspw_cell_get_stream(pspw_cell *cell, void **stream);
+int pspw_cell_sizes(pspw_cell *cell, int *out8);
+/* cap the number of bands transformed per batch of the FFT passes
+ * (0 = automatic); results do not depend on it */
+int pspw_cell_set_band_batch(pspw_cell *cell, int nbatch);
+
+/* ------------------------------------------------------------------ H*psi
+ * vout = H vin for nstates bands (ApplyHam_block.cpp:5-172): kinetic
+ * 0.5*XKG*TPIBA2, local V_eff through an FFT sandwich, KB nonlocal
+ * sum_a,lm beta W beta^H.  Host FP64 buffers, ld = ngw. */
+int pspw_apply_ham_block(pspw_cell *cell, const double *vin, double *vout, int ngw, int nstates);
+/* Device buffers of precision `prec`, leading dimension ld >= ngw
+ * (replaces ApplyHam_block_cuda, common_pspw.h:254).  Enqueued on the cell
+ * stream; returns without synchronising. */
+int pspw_apply_ham_block_dev(pspw_cell *cell, int prec, const void *d_vin, void *d_vout, int ld,
+                             int ngw, int nstates);
+
+/* ------------------------------------------------------------------ filter
+ * Degree-`degree` scaled Chebyshev filter of chebyfilt.cpp:6-74 applied to
+ * the ngw x nstates block X in place.  Host FP64 X; `prec` selects the
+ * arithmetic on the device (F64 = the reference's, F32 = mixed precision). */
+int pspw_chebyfilt(pspw_cell *cell, double *X, int ngw, int nstates, int degree, double lb,
+                   double ub, int prec);
+int pspw_chebyfilt_dev(pspw_cell *cell, int prec, void *d_X, int ld, int ngw, int nstates,
+                       int degree, double lb, double ub);
+
+/* ------------------------------------------------------------------ timing
+ * Optional per-kernel-family device timing on the cell stream (CUDA events
+ * around each launch of the selected family, summed until reset).  Families:
+ * 0 = all H*psi work, 1 = FFT passes, 2 = projector GEMMs. */
+int pspw_timing_enable(pspw_cell *cell, int family_mask);
+int pspw_timing_read(pspw_cell *cell, int family, double *total_ms, long long *launches);
+int pspw_timing_reset(pspw_cell *cell);
+
+#if defined(__GNUC__)
+#pragma GCC visibility pop
+#endif
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif

@@ -1,0 +1,59 @@
+"""The C ABI library loads (no GPU needed) and exports every function that
+include/pspw_gpu.h declares; the drop-in library exports the reference's
+C++ signatures under their g++ mangled names."""
+import ctypes
+import os
+import re
+import subprocess
+
+import pytest
+
+from pspw import _lib
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+HEADER = os.path.join(ROOT, "include", "pspw_gpu.h")
+
+
+def declared_functions():
+    src = open(HEADER).read()
+    src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
+    return sorted(set(re.findall(r"\b(pspw_[a-z0-9_]+)\s*\(", src)))
+
+
+def test_header_declares_functions():
+    names = declared_functions()
+    assert "pspw_apply_ham_block" in names and "pspw_cell_create" in names
+
+
+def test_library_exports_every_declared_symbol():
+    lib = ctypes.CDLL(_lib.LIB_PATH)
+    missing = [n for n in declared_functions() if not hasattr(lib, n)]
+    assert not missing, missing
+
+
+def test_python_binding_covers_the_header():
+    missing = [n for n in declared_functions() if n not in _lib.SIGNATURES]
+    assert not missing, missing
+
+
+def test_error_strings_without_gpu():
+    L = _lib.lib()
+    assert L.pspw_error_string(2) == b"inconsistent sizes"
+    assert L.pspw_version() >= 100
+
+
+# g++ mangled names of the reference functions the drop-in replaces
+# (signatures from common_pspw.h:176-222)
+DROPIN_SYMBOLS = [
+    "_Z14ApplyHam_blockPCdS0_iiPdii",
+    "_Z8ApplyHamPCdS0_iiPdi",
+    "_Z9chebyfiltiPCdiddPdi",
+]
+
+
+@pytest.mark.skipif(not os.path.exists(_lib.DROPIN_PATH), reason="drop-in library not built")
+def test_dropin_exports_reference_mangled_names():
+    out = subprocess.run(["nm", "-D", "--defined-only", _lib.DROPIN_PATH], capture_output=True,
+                         text=True).stdout
+    for s in DROPIN_SYMBOLS:
+        assert re.search(r"\bT " + re.escape(s) + r"$", out, re.M), s

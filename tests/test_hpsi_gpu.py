@@ -1,0 +1,220 @@
+"""GPU parity of block H*psi and the Chebyshev filter against the oracle.
+
+Bar: FP64 path within 1e-12 relative max-norm of the reference's
+ApplyHam_block (golden fixture made by the reference) and of the oracle; the
+FP32 path within 2e-5 relative max-norm (single-precision FFT and projector
+sums with FP32 accumulation over NGW <= 24k terms).
+"""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+torch = pytest.importorskip("torch")
+if not torch.cuda.is_available():  # pragma: no cover
+    pytest.skip("needs a CUDA device", allow_module_level=True)
+
+import pspw_oracle as O  # noqa: E402
+from helpers import engine_cell_args, golden, oracle_cell, relmax  # noqa: E402
+from pspw import PREC_F32, PREC_F64, Cell, PspwError, basis_gamma, synth  # noqa: E402
+from pspw import workloads  # noqa: E402
+
+TOL64 = 1e-12
+TOL32 = 2e-5
+
+G = golden("si8_8ry")
+
+
+def engine_cell(d, veff):
+    c = Cell.from_arrays(engine_cell_args(d))
+    c.set_veff(veff)
+    return c
+
+
+@pytest.fixture(scope="module")
+def gcell():
+    return engine_cell(G, G["veff"])
+
+
+@pytest.fixture(scope="module")
+def cfg0():
+    w = workloads.workload("si8")
+    cell = workloads.make_cell(w)
+    return w, cell
+
+
+def test_fp64_matches_reference_golden(gcell):
+    out = gcell.apply_ham_block(G["psi"])
+    assert relmax(out, G["hpsi"]) < TOL64
+
+
+def test_single_band_matches_reference_apply_ham(gcell):
+    out = gcell.apply_ham_block(G["psi"][:, :1])
+    assert relmax(out[:, 0], G["h1"]) < TOL64
+
+
+def test_fp64_config0_matches_oracle(cfg0):
+    w, cell = cfg0
+    out = cell.apply_ham_block(w["psi"])
+    ref = O.apply_ham_block(oracle_cell(w), w["psi"], w["veff"])
+    assert relmax(out, ref) < TOL64
+
+
+def test_fp32_device_config0(cfg0):
+    w, cell = cfg0
+    psi = w["psi"]
+    ngw, nb = psi.shape
+    d_in = torch.from_numpy(np.ascontiguousarray(psi.T)).to(torch.complex64).cuda()
+    d_out = torch.zeros_like(d_in)
+    torch.cuda.synchronize()
+    cell.apply_ham_block_dev(d_in, d_out, ngw, ngw, nb, PREC_F32)
+    torch.cuda.synchronize()
+    out = d_out.cpu().numpy().T
+    ref = O.apply_ham_block(oracle_cell(w), psi.astype(np.complex64).astype(complex), w["veff"])
+    assert relmax(out, ref) < TOL32
+
+
+def test_fp64_device_leading_dimension(cfg0):
+    w, cell = cfg0
+    psi = w["psi"][:, :5]
+    ngw = psi.shape[0]
+    ld = ngw + 7
+    host = np.zeros((5, ld), dtype=complex)
+    host[:, :ngw] = psi.T
+    d_in = torch.from_numpy(host).cuda()
+    d_out = torch.zeros_like(d_in)
+    torch.cuda.synchronize()
+    cell.apply_ham_block_dev(d_in, d_out, ld, ngw, 5, PREC_F64)
+    torch.cuda.synchronize()
+    out = d_out.cpu().numpy()[:, :ngw].T
+    ref = O.apply_ham_block(oracle_cell(w), psi, w["veff"])
+    assert relmax(out, ref) < TOL64
+
+
+def test_band_batches_give_identical_bits(cfg0):
+    w, cell = cfg0
+    outs = []
+    for nbatch in (0, 1, 3, 16):
+        cell.set_band_batch(nbatch)
+        outs.append(cell.apply_ham_block(w["psi"]))
+    cell.set_band_batch(0)
+    for o in outs[1:]:
+        assert np.array_equal(o, outs[0])
+
+
+def test_repeat_is_deterministic(cfg0):
+    w, cell = cfg0
+    a = cell.apply_ham_block(w["psi"])
+    b = cell.apply_ham_block(w["psi"])
+    assert np.array_equal(a, b)
+
+
+def test_fewer_plane_waves_than_the_cell(cfg0):
+    # NGW_ik below the cell's sphere: only the first ngw G's exist
+    w, cell = cfg0
+    ngw = 2000
+    psi = np.asfortranarray(w["psi"][:ngw, :4])
+    out = cell.apply_ham_block(psi)
+    oc = oracle_cell(w)
+    ref = O.apply_ham_block(oc, psi, w["veff"])
+    assert relmax(out, ref) < TOL64
+
+
+@pytest.mark.parametrize("nr", [(22, 21, 26), (25, 27, 30), (20, 24, 18)])
+def test_non_power_of_two_grids(nr):
+    # radices 7, 11, 13 take the generic butterfly; 25/27/30 mix 3 and 5
+    lat, pos = synth.si_diamond(1)
+    b = basis_gamma(lat, 8.0, nr, [8], [pos])
+    pkg_a, wnl = synth.kb_form_factors(b, lat)
+    b.update(pkg_a=pkg_a, wnl=wnl, lm_end=[4])
+    veff = synth.local_potential(b["nr"], lat, pos)
+    psi = synth.wavefunctions(b, lat, 3, 5)
+    cell = Cell.from_arrays(b)
+    cell.set_veff(veff)
+    out = cell.apply_ham_block(psi)
+    ref = O.apply_ham_block(oracle_cell(b), psi, veff)
+    assert relmax(out, ref) < TOL64
+
+
+@pytest.mark.parametrize("lm_end", [[1], [0], [3]])
+def test_projector_counts(lm_end):
+    d = dict(G)
+    args = engine_cell_args(d)
+    args["lm_end"] = lm_end
+    cell = Cell.from_arrays(args)
+    cell.set_veff(G["veff"])
+    out = cell.apply_ham_block(G["psi"][:, :3])
+    oc = oracle_cell(d)
+    oc["lm_end"] = lm_end
+    ref = O.apply_ham_block(oc, G["psi"][:, :3], G["veff"])
+    assert relmax(out, ref) < TOL64
+
+
+def test_two_species():
+    # species-major projector order with different lm_end per species
+    lat, pos = synth.si_diamond(1)
+    na = [5, 3]
+    tau = [pos[:5], pos[5:]]
+    b = basis_gamma(lat, 8.0, None, na, tau)
+    pkg_a, wnl = synth.kb_form_factors(b, lat, nsp=2, rc=[1.0, 0.8])
+    wnl[1] = [0.7, -0.3, -0.3, -0.3]
+    b.update(pkg_a=pkg_a, wnl=wnl, lm_end=[4, 1])
+    veff = synth.local_potential(b["nr"], lat, pos)
+    psi = synth.wavefunctions(b, lat, 4, 9)
+    cell = Cell.from_arrays(b)
+    cell.set_veff(veff)
+    out = cell.apply_ham_block(psi)
+    oc = oracle_cell(b)
+    oc.update(na=na, lm_end=[4, 1])
+    ref = O.apply_ham_block(oc, psi, veff)
+    assert relmax(out, ref) < TOL64
+
+
+def test_chebyfilt_fp64_matches_reference_golden(gcell):
+    out = gcell.chebyfilt(G["psi"], int(G["cheb_degree"]), float(G["cheb_lb"]),
+                          float(G["cheb_ub"]), PREC_F64)
+    assert relmax(out, G["cheb"]) < TOL64
+
+
+@pytest.mark.parametrize("degree", [1, 2, 3, 10])
+def test_chebyfilt_fp64_degrees(cfg0, degree):
+    w, cell = cfg0
+    X = w["psi"][:, :6]
+    out = cell.chebyfilt(X, degree, 1.5, 5.0, PREC_F64)
+    ref = O.chebyfilt(oracle_cell(w), X, degree, 1.5, 5.0, w["veff"])
+    assert relmax(out, ref) < TOL64
+
+
+def test_chebyfilt_fp32(cfg0):
+    w, cell = cfg0
+    X = w["psi"]
+    out = cell.chebyfilt(X, 10, 1.5, 5.0, PREC_F32)
+    ref = O.chebyfilt(oracle_cell(w), X, 10, 1.5, 5.0, w["veff"])
+    assert relmax(out, ref) < 1e-4
+
+
+def test_errors_are_reported(gcell):
+    with pytest.raises(PspwError) as e:
+        gcell.set_veff(np.zeros(17))
+    assert e.value.code == 2  # nnr != NNR (ApplyHam_block.cpp:18-21)
+    args = engine_cell_args(G)
+    args["lm_end"] = [5]
+    args["pkg_a"] = np.zeros((5,) + G["pkg_a"].shape[1:])
+    with pytest.raises(PspwError) as e:
+        Cell.from_arrays(args)
+    assert e.value.code == 9  # lm_end > 4 (ApplyHam_block.cpp:70-73)
+    d = torch.zeros(4, int(G["ngw"]), dtype=torch.complex128, device="cuda")
+    with pytest.raises(PspwError) as e:
+        gcell.apply_ham_block_dev(d, d, int(G["ngw"]), int(G["ngw"]), 4, PREC_F64)
+    assert e.value.code == 1
+
+
+def test_si64_subset_parity_and_hermiticity():
+    # the 64-atom, 64^3 cell: FP64 parity on 8 bands, and <x|H y> = <H x|y>
+    w = workloads.workload("si64")
+    cell = workloads.make_cell(w)
+    psi = np.asfortranarray(w["psi"][:, :8])
+    out = cell.apply_ham_block(psi)
+    ref = O.apply_ham_block(oracle_cell(w), psi, w["veff"])
+    assert relmax(out, ref) < TOL64
+    m = psi.conj().T @ out
+    assert np.abs(m - m.conj().T).max() < 1e-12 * np.abs(m).max()

@@ -1,0 +1,151 @@
+"""The oracle (oracle/pspw_oracle.py) pinned against the reference.
+
+Two anchors:
+  * golden fixtures made by running the reference itself (tests/golden/,
+    generated by make_golden.py from oracle/_ref/libref.so) -- always run;
+  * the reference built from its own sources, called on the same inputs --
+    run when oracle/_ref/libref.so is present.
+"""
+import numpy as np
+import pytest
+
+import pspw_oracle as O
+from helpers import golden, oracle_cell, ref_lib_or_none, relmax
+
+G = golden("si8_8ry")
+CELL = oracle_cell(G)
+
+
+def test_apply_ham_block_matches_reference_output():
+    out = O.apply_ham_block(CELL, G["psi"], G["veff"])
+    assert relmax(out, G["hpsi"]) < 1e-13
+
+
+def test_apply_ham_single_vector():
+    out = O.apply_ham(CELL, G["psi"][:, 0], G["veff"])
+    assert relmax(out, G["h1"]) < 1e-13
+
+
+def test_chebyfilt_matches_reference_output():
+    out = O.chebyfilt(CELL, G["psi"], int(G["cheb_degree"]), float(G["cheb_lb"]),
+                      float(G["cheb_ub"]), G["veff"])
+    assert relmax(out, G["cheb"]) < 1e-12
+
+
+def test_chebyfilt_coefficients_reproduce_filter():
+    # the (a, b, c) step form used by the fused device recurrence
+    X = G["psi"]
+    coeffs = O.chebyfilt_step_coeffs(int(G["cheb_degree"]), float(G["cheb_lb"]),
+                                     float(G["cheb_ub"]))
+    ym2, ym1 = None, X
+    for d, (a, b, c) in enumerate(coeffs):
+        y = a * O.apply_ham_block(CELL, ym1, G["veff"]) + b * ym1
+        if d > 0:
+            y = y + c * ym2
+        ym2, ym1 = ym1, y
+    assert relmax(ym1, G["cheb"]) < 1e-12
+
+
+def test_lanczos_matches_reference_output():
+    T, f = O.lanczos(CELL, G["psi"][:, 1], 8, G["veff"])
+    assert np.abs(T - G["lanczos_T"]).max() < 1e-11
+    assert relmax(f, G["lanczos_f"]) < 1e-8
+
+
+def test_random_col_bit_exact():
+    assert np.array_equal(O.random_col(64, 100), G["random_col"])
+
+
+def test_gen_prec_bit_exact():
+    ngw = int(G["ngw"])
+    p = O.gen_prec(G["xkg"][:ngw], float(G["alat"]), float(G["tpiba2"]), -10.0)
+    assert np.array_equal(p, G["prec"])
+
+
+def test_ortho_qr_matches_householder():
+    q = O.ortho_qr(G["ortho_in"])
+    assert np.abs(q - G["ortho_q"]).max() < 1e-14
+
+
+def test_eval_rho_psi_matches_reference_output():
+    ngw, ngwx = int(G["ngw"]), int(G["ngwx"])
+    psi = G["psi"]
+    flat = np.concatenate([psi.reshape(-1, order="F"), np.zeros(ngwx, complex)])
+    rho, ekin, c0 = O.eval_rho_psi(CELL, flat, ngw, ngw, 4, G["focc"], 1.0, float(G["omega"]),
+                                   ngwx)
+    assert relmax(rho, G["rho"]) < 1e-13
+    assert abs(ekin - float(G["ekin"])) < 1e-12 * abs(float(G["ekin"]))
+    assert np.array_equal(c0, G["c0"])
+
+
+def test_eval_rho_psi_charge_check_aborts():
+    # EvalRhoPsi.cpp:129-133: a band whose |c|^2 sum is off by > 6e-3 is an error
+    ngw, ngwx = int(G["ngw"]), int(G["ngwx"])
+    bad = 1.01 * G["psi"]
+    flat = np.concatenate([bad.reshape(-1, order="F"), np.zeros(ngwx, complex)])
+    with pytest.raises(RuntimeError, match="Wrong charge"):
+        O.eval_rho_psi(CELL, flat, ngw, ngw, 4, G["focc"], 1.0, float(G["omega"]), ngwx)
+
+
+def test_symmetrize_equals_loop_form():
+    rng = np.random.default_rng(0)
+    v = rng.standard_normal((7, 7)) + 1j * rng.standard_normal((7, 7))
+    ref = v.copy()
+    for j in range(7):
+        for i in range(j + 1):
+            t = 0.5 * (ref[i, j] + np.conj(ref[j, i]))
+            ref[i, j] = t
+            ref[j, i] = np.conj(t)
+    assert np.array_equal(O.symmetrize(v), ref)
+
+
+# ------------------------------------------------------------ live reference
+REF = ref_lib_or_none()
+need_ref = pytest.mark.skipif(REF is None, reason="oracle/_ref/libref.so not built")
+
+
+@pytest.fixture(scope="module")
+def ref_cell():
+    from pspw import synth
+    lat, pos = synth.si_diamond(1)
+    b = REF.setup(lat, 8.0, None, [8], [pos], [4.0], [3], [3], 4)
+    pkg_a, wnl = synth.kb_form_factors(b, lat)
+    REF.set_nl(pkg_a, wnl)
+    cell = dict(nr=b["nr"], n123=b["n123"], xkg=b["xkg"], eigr=b["eigr"], pkg_a=pkg_a, wnl=wnl,
+                na=[8], lm_end=[4], tpiba2=b["tpiba2"])
+    veff = synth.local_potential(b["nr"], lat, pos)
+    return b, cell, veff, lat
+
+
+@need_ref
+def test_live_davidson_eigenvalues(ref_cell):
+    b, cell, veff, _ = ref_cell
+    ngw = b["ngw"]
+    prec = O.gen_prec(b["xkg"][:ngw], b["alat"], b["tpiba2"], -10.0)
+    ev_r, _ = REF.davidson(ngw, 12, veff, prec, 4, max_iter=6)
+    ev_o, _, _ = O.davidson(cell, ngw, 12, veff, prec, 4, max_iter=6)
+    assert np.abs(ev_r - ev_o).max() < 1e-9
+
+
+@need_ref
+def test_live_lobpcg_eigenvalues(ref_cell):
+    b, cell, veff, _ = ref_cell
+    ngw = b["ngw"]
+    prec = O.gen_prec(b["xkg"][:ngw], b["alat"], b["tpiba2"], -10.0)
+    ev_r, _ = REF.lobpcg(ngw, 12, veff, prec, 4, max_iter=6)
+    ev_o, _, _ = O.lobpcg(cell, ngw, 12, veff, prec, 4, max_iter=6)
+    assert np.abs(ev_r - ev_o).max() < 1e-9
+
+
+@need_ref
+def test_live_eig_zhegv_eval(ref_cell):
+    rng = np.random.default_rng(3)
+    n = 10
+    a = rng.standard_normal((n, n)) + 1j * rng.standard_normal((n, n))
+    a = a + a.conj().T
+    m = rng.standard_normal((n, n)) + 1j * rng.standard_normal((n, n))
+    bm = m @ m.conj().T + n * np.eye(n)
+    w_r, v_r = REF.eig_zhegv_eval(a, bm)
+    w_o, v_o, _ = O.eig_zhegv_eval(a, bm)
+    assert np.abs(w_r - w_o).max() < 1e-12
+    assert np.abs(np.abs(v_r) - np.abs(v_o)).max() < 1e-10
