@@ -1,0 +1,402 @@
+#!/usr/bin/env python
+"""Benchmark of the block H*psi path (Chebyshev-filter form) on B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl engine|reference]
+                    [--prec f32|f64] [--workload si64]
+
+One step = one call of the degree-10 Chebyshev filter (chebyfilt.cpp:6-74)
+on the Si64 cell (64 atoms, a = 20.52 bohr, ecutwfc 15 Ha, 64^3 grid,
+NGW 23847, 144 bands, synthetic local + s/p KB pseudopotential): ten block
+H*psi applications with the three-term recurrence fused into the projector
+GEMM epilogue.  The metric is H*psi GB/s: the algorithmic bytes of one block
+H*psi (every 3D FFT = one grid read + one write, psi in/out once, V and the
+projector inputs once per block; FP32 complex 8 B / real 4 B) times the ten
+applications, divided by the device time of the step.  The same byte count
+is used for every arm, so ratios are ratios of work per second.
+
+Engine arm: inputs resident in HBM; each step restores X from a device copy
+(the filter overwrites X) and runs the filter; L2 is flushed between steps
+(256 MB write, outside the event-timed interval).  Multi-GPU: one process
+per GPU, each filters its own replica of the block (weak scaling, no
+collective: bands are independent).  e2e: the same filter through the C ABI
+with pinned host FP64 buffers, host->device and device->host copies inside.
+
+Reference arm (--impl reference): the reference's own chebyfilt built from
+its sources (oracle/_ref/libref.so; FFT by the oracle's FFTW-API shim,
+BLAS by scipy's OpenBLAS) on the host cores, one process per core, each
+filtering a slice of bands of the same cell (a bounded sample).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "ffr-pspw-dft-c_b200"))
+
+import numpy as np  # noqa: E402
+
+DEGREE = 10
+LB, UB = 0.5, 16.0  # filter window (Ha) for the Si64 cell's spectrum
+METRIC = "Hpsi GB/s (algorithmic, FP32 byte model; Chebyshev filter degree 10)"
+WORKLOAD = ("Chebyshev filter (degree 10, chebyfilt.cpp) on Si64: 64 atoms, a=20.52 bohr, "
+            "ecutwfc 15 Ha, grid 64^3, NGW 23847, 144 bands, s+p KB projectors")
+
+
+def hpsi_bytes_model(ngw, nnr, nb, nat, fp64=False):
+    sc, sr = (16, 8) if fp64 else (8, 4)
+    return nb * (2 * ngw + 4 * nnr) * sc + nnr * sr + ngw * (4 + sr) + ngw * (nat * sc + 4 * sr)
+
+
+# ------------------------------------------------------------------ clocks
+class ClockSampler:
+    """nvidia-smi samples (200 ms) of SM clock and throttle reasons."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index=0):
+        self.index = index
+        self.rows = []
+        self.proc = None
+        self.thread = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except Exception:
+            self.proc = None
+            return
+        self.thread = threading.Thread(target=self._read, daemon=True)
+        self.thread.start()
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.rows.append([x.strip() for x in line.split(",")])
+
+    def stop(self):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+        if self.thread:
+            self.thread.join(timeout=2)
+
+    def summary(self):
+        sm = [float(r[1]) for r in self.rows if len(r) > 8 and r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in self.rows if len(r) > 8 and r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = set()
+        for r in self.rows:
+            if len(r) > 8:
+                for k, v in zip(names, r[5:9]):
+                    if v.strip().lower() == "active":
+                        reasons.add(k)
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": max(mx) if mx else None, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+# ------------------------------------------------------------------ reference arm
+def _ref_worker(args):
+    """One host process: the reference's chebyfilt on `nbands` bands of the Si64
+    cell, `steps` timed calls after `warmup`.  Returns per-step seconds."""
+    nbands, steps, warmup, seed = args
+    os.environ.setdefault("OPENBLAS_NUM_THREADS", "1")
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    from ref_lib import RefLib
+    from pspw import synth
+    lat, pos = synth.si_diamond(2)
+    R = RefLib()
+    b = R.setup(lat, 30.0, (64, 64, 64), [64], [pos], [4.0], [3], [3], 4)
+    pkg_a, wnl = synth.kb_form_factors(b, lat)
+    R.set_nl(pkg_a, wnl)
+    veff = synth.local_potential(b["nr"], lat, pos)
+    psi = synth.wavefunctions(b, lat, nbands, seed)
+    R.set_nx(nbands - 2, 0)  # chebyfilt's width is NX+2 (chebyfilt.cpp:20)
+    devnull = os.open(os.devnull, os.O_WRONLY)
+    os.dup2(devnull, 1)  # the reference prints; keep the JSON line clean
+    times = []
+    for i in range(warmup + steps):
+        t0 = time.perf_counter()
+        R.chebyfilt(psi, DEGREE, LB, UB, veff)
+        dt = time.perf_counter() - t0
+        if i >= warmup:
+            times.append(dt)
+    return b["ngw"], times
+
+
+def reference_sample(steps, warmup, bands_per_proc=4, procs=None):
+    """Time the reference filter on all host cores.  Returns a dict with the
+    metric value (same byte model as the engine arm) and the sample."""
+    import multiprocessing as mp
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    from ref_lib import ref_available
+    if not ref_available():
+        return None, "oracle/_ref/libref.so not built (make -C oracle)"
+    procs = procs or len(os.sched_getaffinity(0)) or 1
+    ctx = mp.get_context("spawn")
+    with ctx.Pool(procs) as pool:
+        res = pool.map(_ref_worker, [(bands_per_proc, steps, warmup, 100 + i) for i in range(procs)])
+    ngw = res[0][0]
+    per_step = [max(r[1][k] for r in res) for k in range(steps)]
+    t = sum(per_step) / len(per_step)
+    nb_total = bands_per_proc * procs
+    bytes_step = DEGREE * hpsi_bytes_model(ngw, 64 ** 3, nb_total, 64)
+    return {"value": bytes_step / t / 1e9, "unit": "GB/s", "cores": procs, "kind": "reference",
+            "seconds_per_step": t, "bands": nb_total,
+            "sample": (f"reference chebyfilt (degree {DEGREE}) built from its sources, FFT by the "
+                       f"oracle's FFTW-API shim (FFTW3 not installed), scipy OpenBLAS; {procs} "
+                       f"processes x {bands_per_proc} bands of the Si64 cell = {nb_total} of 144 "
+                       f"bands; {steps} timed calls")}, None
+
+
+# ------------------------------------------------------------------ engine arm
+def run_engine(args, rank, world, local_rank):
+    import torch
+    from pspw import PREC_F32, PREC_F64, workloads
+    torch.cuda.set_device(local_rank)
+    dev = torch.device("cuda", local_rank)
+    w = workloads.workload(args.workload)
+    cell = workloads.make_cell(w, device=local_rank)
+    sizes = cell.sizes()
+    psi = w["psi"]
+    ngw, nb = psi.shape
+    nnr = int(np.prod(w["nr"]))
+    nat = sizes["nat"]
+    fp64 = args.prec == "f64"
+    prec = PREC_F64 if fp64 else PREC_F32
+    cdt = torch.complex128 if fp64 else torch.complex64
+    x0 = torch.from_numpy(np.ascontiguousarray(psi.T)).to(cdt).to(dev)  # (nb, ngw) = ngw x nb col-major
+    x = torch.empty_like(x0)
+    stream = torch.cuda.ExternalStream(cell.stream(), device=dev)
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
+
+    def step():
+        x.copy_(x0)
+        cell.chebyfilt_dev(x, ngw, ngw, nb, DEGREE, LB, UB, prec)
+
+    with torch.cuda.stream(stream):
+        for _ in range(args.warmup):
+            step()
+    torch.cuda.synchronize()
+    clocks = ClockSampler(local_rank)
+    clocks.start()
+    time.sleep(0.5)
+    fam_mask = sum(1 << f for f in range(3, 10))
+    cell.timing_reset()
+    cell.timing_enable(fam_mask)
+    l0 = cell.kernel_launches()
+    evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+           for _ in range(args.steps)]
+    if world > 1:
+        torch.distributed.barrier()
+    torch.cuda.synchronize()
+    t_wall = time.perf_counter()
+    with torch.cuda.stream(stream):
+        for k in range(args.steps):
+            flush.fill_(float(k))  # evict L2 between steps (not timed)
+            evs[k][0].record(stream)
+            step()
+            evs[k][1].record(stream)
+    torch.cuda.synchronize()
+    if world > 1:
+        torch.distributed.barrier()
+    t_wall = time.perf_counter() - t_wall
+    launches = (cell.kernel_launches() - l0) // args.steps
+    cell.timing_enable(0)
+    fam = {f: cell.timing_read(f) for f in range(3, 10)}
+    clocks.stop()
+    step_ms = [a.elapsed_time(b) for a, b in evs]
+    ms = sum(step_ms) / len(step_ms)
+    ms_t = torch.tensor([ms], device=dev)
+    if world > 1:
+        torch.distributed.all_reduce(ms_t, op=torch.distributed.ReduceOp.MAX)
+    ms_max = float(ms_t.item())
+    bytes_step = DEGREE * hpsi_bytes_model(ngw, nnr, nb, nat, fp64=False)
+    value = world * bytes_step / (ms_max * 1e-3) / 1e9
+
+    # ---- per-kernel roofline (dominant kernel family on the cell stream)
+    sc, sr = (16, 8) if fp64 else (8, 4)
+    n1, n2, n3 = w["nr"]
+    ncol, nxa = sizes["nsticks"], sizes["nxa"]
+    nproj = sizes["nproj"]
+    calls = args.steps * DEGREE
+    names = {3: "k_sticks_inv", 4: "k_planes_inv", 5: "k_xlines", 6: "k_planes_fwd",
+             7: "k_sticks_fwd", 8: "k_proj(+reduce)", 9: "k_backproj"}
+    per_band = {  # algorithmic bytes per band (inputs and outputs once)
+        3: ngw * sc + n3 * ncol * sc,
+        4: n3 * ncol * sc + n3 * n2 * nxa * sc,
+        5: 2 * n3 * n2 * nxa * sc,
+        6: n3 * n2 * nxa * sc + n3 * ncol * sc,
+        7: n3 * ncol * sc + 2 * ngw * sc,
+    }
+    fam_ms = {f: fam[f][0] for f in fam}
+    top = max(fam_ms, key=lambda f: fam_ms[f])
+    peaks = {}
+    try:
+        peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+    except Exception:
+        pass
+    hbm_peak = peaks.get("hbm_gbs", 6650.0)
+    hbm_src = "measured" if "hbm_gbs" in peaks else "fallback"
+    n_launch = fam[top][1]
+    if top in per_band:
+        bytes_total = per_band[top] * nb * calls + (nnr * sr * n_launch if top == 5 else 0)
+        achieved = bytes_total / n_launch / (fam_ms[top] / n_launch * 1e-3) / 1e9
+        roof = {"kernel": names[top], "bound": "hbm", "achieved": round(achieved, 1),
+                "peak": hbm_peak, "unit": "GB/s", "frac": round(achieved / hbm_peak, 4),
+                "peak_source": hbm_src,
+                "bytes_per_launch": int(bytes_total / n_launch),
+                "launches": n_launch, "avg_launch_us": round(fam_ms[top] / n_launch * 1e3, 2)}
+    else:
+        flops = 8.0 * ngw * nproj * nb * calls
+        achieved = flops / (fam_ms[top] * 1e-3) / 1e12
+        simt_peak = 148 * 128 * 2 * 1.965e9 / 1e12 * (0.5 if fp64 else 1.0)
+        roof = {"kernel": names[top], "bound": "fp32 SIMT" if not fp64 else "fp64",
+                "achieved": round(achieved, 2), "peak": round(simt_peak, 1), "unit": "TFLOP/s",
+                "frac": round(achieved / simt_peak, 4), "peak_source": "nominal SIMT",
+                "launches": n_launch, "avg_launch_us": round(fam_ms[top] / n_launch * 1e3, 2)}
+    roof["traffic"] = _ncu_traffic(roof["kernel"], args.prec)
+    kernels_ms = {names[f]: round(fam_ms[f] / args.steps, 4) for f in fam_ms}
+    hpsi_ms = ms_max / DEGREE
+    hpsi_roof = {"bytes_per_hpsi": hpsi_bytes_model(ngw, nnr, nb, nat, fp64=fp64),
+                 "ms_per_hpsi": round(hpsi_ms, 4),
+                 "achieved_gbs": round(hpsi_bytes_model(ngw, nnr, nb, nat, fp64=fp64)
+                                       / (hpsi_ms * 1e-3) / 1e9, 1),
+                 "frac_of_measured_hbm": None}
+    hpsi_roof["frac_of_measured_hbm"] = round(hpsi_roof["achieved_gbs"] / hbm_peak, 4)
+
+    # ---- e2e through the C ABI with pinned host buffers (FP64 host data)
+    e2e = None
+    if not args.no_e2e:
+        host = torch.empty((nb, ngw), dtype=torch.complex128, pin_memory=True)
+        host.copy_(torch.from_numpy(np.ascontiguousarray(psi.T)))
+        hx = host.numpy()  # pinned, Fortran-ordered ngw x nb when viewed transposed
+        from pspw._lib import check, lib
+        L = lib()
+        for _ in range(2):
+            hx[:] = psi.T
+            check(L.pspw_chebyfilt(cell.handle, hx.ctypes.data, ngw, nb, DEGREE, LB, UB, prec))
+        e_steps = max(3, args.steps // 2)
+        tt = []
+        for _ in range(e_steps):
+            hx[:] = psi.T  # the filter overwrites X; restore (host memcpy, not timed)
+            t0 = time.perf_counter()
+            check(L.pspw_chebyfilt(cell.handle, hx.ctypes.data, ngw, nb, DEGREE, LB, UB, prec))
+            tt.append(time.perf_counter() - t0)
+        et = sum(tt) / len(tt)
+        et_t = torch.tensor([et], device=dev)
+        if world > 1:
+            torch.distributed.all_reduce(et_t, op=torch.distributed.ReduceOp.MAX)
+        e2e = {"value": round(world * bytes_step / float(et_t.item()) / 1e9, 2), "unit": "GB/s",
+               "h2d_bytes_per_step": ngw * nb * 16, "d2h_bytes_per_step": ngw * nb * 16,
+               "seconds_per_step": round(float(et_t.item()), 6),
+               "path": "pspw_chebyfilt (C ABI, host FP64 X, FP32 on device)" if not fp64
+               else "pspw_chebyfilt (C ABI, host FP64 X, FP64 on device)"}
+
+    return dict(value=value, ms=ms_max, wall=t_wall, launches=launches, roof=roof,
+                hpsi_roof=hpsi_roof, kernels_ms=kernels_ms, clocks=clocks.summary(), e2e=e2e,
+                ngw=ngw, nb=nb, sizes=sizes)
+
+
+def _ncu_traffic(kernel, prec):
+    """DRAM bytes per launch of `kernel` from the committed ncu summary, or None."""
+    path = os.path.join(ROOT, "profiles", "ncu_traffic.txt")
+    if not os.path.exists(path):
+        return None
+    for line in open(path):
+        parts = line.split()
+        if len(parts) >= 3 and parts[0] == kernel and parts[1] == prec:
+            try:
+                return int(float(parts[2]))
+            except ValueError:
+                return None
+    return None
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="engine", choices=["engine", "reference"])
+    ap.add_argument("--prec", default="f32", choices=["f32", "f64"])
+    ap.add_argument("--workload", default="si64")
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+
+    config = {"workload": WORKLOAD, "cell": "Si64 diamond-cubic, synthetic pseudopotential",
+              "grid": [64, 64, 64], "ngw": 23847, "bands": 144, "filter_degree": DEGREE,
+              "filter_window_ha": [LB, UB], "global_batch": 144 * world,
+              "parallelism": f"replica x{world} (bands independent, no collective)",
+              "l2": "flushed between steps (256 MB write, outside the timed interval)"}
+
+    if args.impl == "reference":
+        if rank != 0:
+            return
+        ref, why = reference_sample(args.steps, args.warmup)
+        if ref is None:
+            print(json.dumps({"impl": "reference", "unavailable": why}))
+            return
+        print(json.dumps({
+            "impl": "reference", "metric": METRIC, "value": round(ref["value"], 4), "unit": "GB/s",
+            "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": round(ref["seconds_per_step"] * 1e3, 3), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "c128", "data": "synthetic",
+            "config": config,
+            "cpu_baseline": {k: ref[k] for k in ("value", "unit", "cores", "kind", "sample")},
+            "e2e": {"value": round(ref["value"], 4), "unit": "GB/s", "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}))
+        return
+
+    import torch
+    if world > 1:
+        import datetime
+        torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                             device_id=torch.device("cuda", local_rank))
+    r = run_engine(args, rank, world, local_rank)
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        ref, why = reference_sample(steps=1, warmup=0)
+        cpu = ({k: (round(v, 4) if isinstance(v, float) else v) for k, v in ref.items()
+                if k in ("value", "unit", "cores", "kind", "sample")} if ref else
+               {"value": None, "unavailable": why})
+    if rank == 0:
+        out = {
+            "metric": METRIC, "value": round(r["value"], 2), "unit": "GB/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(r["ms"], 4),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "c128" if args.prec == "f64" else "c64", "data": "synthetic",
+            "config": config, "roofline": r["roof"], "hpsi": r["hpsi_roof"],
+            "kernels_ms_per_step": r["kernels_ms"], "cpu_baseline": cpu, "e2e": r["e2e"],
+            "gpu_launches": r["launches"], "clocks": r["clocks"],
+            "wall_s_timed": round(r["wall"], 4),
+        }
+        print(json.dumps(out))
+    if world > 1:
+        torch.distributed.barrier()
+        torch.distributed.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

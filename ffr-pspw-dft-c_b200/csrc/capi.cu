@@ -77,7 +77,7 @@ int chebyfilt_dev(pspw_cell *c, void *Xv, int ld, int ngw, int nb, int degree, d
     rc = hpsi_apply<R>(c, buf[im1], lds[im1], buf[io], lds[io], ngw, nb, 2.0 * sigma2 / e,
                        -cc * 2.0 * sigma2 / e, -sigma * sigma2, buf[im2], lds[im2]);
     if (rc) return rc;
-    // the slot that held Y_{d-2} receives Y_d next time round
+    // Y_{d-1} becomes Y_{d-2}; the slot Y_{d-2} had is reused for Y_{d+1}
     im2 = im1;
     im1 = io;
     sigma = sigma2;
@@ -159,8 +159,10 @@ int pspw_chebyfilt(pspw_cell *c, double *X, int ngw, int nstates, int degree, do
     float2 *fx = nullptr;
     if ((rc = ws_reserve(c, 8, n * sizeof(float2), (void **)&fx))) return rc;
     k_z_to_c<<<4 * 148, 256, 0, c->stream>>>(dx, ngw, fx, ngw, ngw, nstates);
+    c->kernel_launches++;
     if ((rc = pspw_chebyfilt_dev(c, PSPW_PREC_F32, fx, ngw, ngw, nstates, degree, lb, ub))) return rc;
     k_c_to_z<<<4 * 148, 256, 0, c->stream>>>(fx, ngw, dx, ngw, ngw, nstates);
+    c->kernel_launches++;
   } else {
     if ((rc = pspw_chebyfilt_dev(c, PSPW_PREC_F64, dx, ngw, ngw, nstates, degree, lb, ub))) return rc;
   }

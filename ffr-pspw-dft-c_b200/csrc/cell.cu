@@ -369,6 +369,7 @@ int pspw_cell_set_veff_device(pspw_cell *c, const double *d_veff, int nnr) {
   PSPW_CUDA(cudaSetDevice(c->device));
   k_veff_scale<<<2 * 148, 256, 0, c->stream>>>(d_veff, nnr, 1.0 / (double)nnr, c->d_veff64,
                                                 c->d_veff32);
+  c->kernel_launches++;
   PSPW_CUDA(cudaGetLastError());
   c->veff_set = true;
   return PSPW_OK;
@@ -392,6 +393,13 @@ int pspw_cell_set_veff(pspw_cell *c, const double *veff, int nnr) {
 int pspw_cell_get_stream(pspw_cell *c, void **stream) {
   if (!c || !stream) return fail(PSPW_ERR_ARG, "get_stream: null argument");
   *stream = (void *)c->stream;
+  return PSPW_OK;
+}
+
+int pspw_cell_synchronize(pspw_cell *c) {
+  if (!c) return fail(PSPW_ERR_ARG, "synchronize: null cell");
+  PSPW_CUDA(cudaSetDevice(c->device));
+  PSPW_CUDA(cudaStreamSynchronize(c->stream));
   return PSPW_OK;
 }
 
@@ -421,7 +429,7 @@ int pspw_timing_enable(pspw_cell *c, int mask) {
 }
 
 int pspw_timing_read(pspw_cell *c, int family, double *total_ms, long long *launches) {
-  if (!c || family < 0 || family > 3) return fail(PSPW_ERR_ARG, "timing: bad argument");
+  if (!c || family < 0 || family >= kNumFamilies) return fail(PSPW_ERR_ARG, "timing: bad argument");
   int rc = drain_timing(c);
   if (rc) return rc;
   if (total_ms) *total_ms = c->timing.ms[family];
@@ -432,11 +440,17 @@ int pspw_timing_read(pspw_cell *c, int family, double *total_ms, long long *laun
 int pspw_timing_reset(pspw_cell *c) {
   if (!c) return fail(PSPW_ERR_ARG, "timing: null cell");
   int rc = drain_timing(c);
-  for (int i = 0; i < 4; i++) {
+  for (int i = 0; i < kNumFamilies; i++) {
     c->timing.ms[i] = 0;
     c->timing.launches[i] = 0;
   }
   return rc;
+}
+
+int pspw_kernel_launches(pspw_cell *c, long long *count) {
+  if (!c || !count) return fail(PSPW_ERR_ARG, "kernel_launches: null argument");
+  *count = c->kernel_launches;
+  return PSPW_OK;
 }
 
 }  // extern "C"

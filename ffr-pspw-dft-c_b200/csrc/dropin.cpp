@@ -1,0 +1,212 @@
+// Drop-in replacement of the reference's hot-path translation units.
+//
+// Exports the reference's C++ functions with their exact signatures (and so
+// the same g++ mangled names, common_pspw.h:176-222 and 252-259), reading
+// the reference program's globals (common_pspw.h:43-148) as that code does,
+// and forwards to the C ABI in include/pspw_gpu.h.  A program links this
+// library in place of ApplyHam_block.o, ApplyHam.o and chebyfilt.o.
+//
+// Device state: one pspw_cell per k-point, built from N123/XKG/EIGR/PKG_A/
+// WNL on first use (or by SetupArrays_ApplyHam_cuda) and reused while those
+// arrays keep their addresses and sizes.  A program that rewrites them in
+// place (new atomic positions) calls SetupArrays_ApplyHam_cuda again.  V_eff
+// (the `rho` argument) is uploaded on every call, as the reference passes it
+// on every call.
+//
+// Arithmetic: FP64 throughout by default, matching the reference to
+// rounding.  PSPW_DROPIN_FILTER_PREC=f32 runs chebyfilt in FP32 on the device
+// (the mixed-precision filter; the host block stays FP64).
+//
+// Errors keep the reference's behaviour: the invariant checks of
+// ApplyHam_block.cpp:18-21 (nnr != NNR) and :70-73 (lm_end > 4) print the
+// same message and abort; an engine failure prints the engine's message and
+// aborts (the reference has no error return on these paths).
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <vector>
+
+#include "pspw_gpu.h"
+
+typedef double _Complex zcomplex;
+
+// ---- the reference program's globals (defined by its global_variables.cpp)
+extern int NSP;
+extern int *NA;
+extern int NAX;
+extern int NLMAX;
+extern int *L_MAX;
+extern int *L_LOC;
+extern int NX;
+extern int NR1, NR2, NR3, NNR;
+extern int NKPT;
+extern double TPIBA2;
+extern int NGWX;
+extern int *NGW;
+extern double *XKG;
+extern unsigned int *N123;
+extern zcomplex *EIGR;
+extern double *PKG_A;
+extern double *WNL;
+
+#define DROPIN_API __attribute__((visibility("default")))
+
+namespace {
+
+struct KCell {
+  pspw_cell *cell = nullptr;
+  const void *key[5] = {};
+  int ngw = -1, ngwx = -1, nnr = -1;
+};
+
+std::vector<KCell> g_cells;  // index ik-1
+int g_device = 0;
+bool g_device_set = false;
+
+[[noreturn]] void die(const char *where, int rc) {
+  std::printf("ERROR in %s: pspw engine error %d (%s): %s\n", where, rc, pspw_error_string(rc),
+              pspw_last_error());
+  std::fflush(stdout);
+  std::abort();
+}
+
+void check_nnr(int nnr) {
+  if (nnr != NNR) {  // ApplyHam_block.cpp:18-21
+    std::printf("nnr != NNR : %d %d\n", nnr, NNR);
+    std::abort();
+  }
+}
+
+std::vector<int> lm_ends() {
+  std::vector<int> lm(NSP);
+  for (int is = 0; is < NSP; is++) {
+    lm[is] = L_MAX[is] * L_MAX[is] - 2 * L_LOC[is] + 1;  // ApplyHam_block.cpp:69
+    if (lm[is] > 4) {                                    // :70-73
+      std::printf("ERROR: lm_end > 4 is not implemented\n");
+      std::abort();
+    }
+  }
+  return lm;
+}
+
+int device() {
+  if (!g_device_set) {
+    const char *d = std::getenv("PSPW_DEVICE");
+    g_device = d ? std::atoi(d) : 0;
+    g_device_set = true;
+  }
+  return g_device;
+}
+
+void drop_cell(KCell &k) {
+  if (k.cell) pspw_cell_destroy(k.cell);
+  k = KCell();
+}
+
+pspw_cell *build_cell(int ik, const unsigned int *n123, const double *xkg, const zcomplex *eigr,
+                      const double *pkg_a) {
+  if ((int)g_cells.size() < ik) g_cells.resize(ik);
+  KCell &k = g_cells[ik - 1];
+  const void *key[5] = {n123, xkg, eigr, pkg_a, WNL};
+  const int ngw = NGW[ik - 1];
+  bool same = k.cell && k.ngw == ngw && k.ngwx == NGWX && k.nnr == NNR;
+  for (int i = 0; same && i < 5; i++) same = (k.key[i] == key[i]);
+  if (same) return k.cell;
+  drop_cell(k);
+  std::vector<int> lm = lm_ends();
+  const size_t col = (size_t)ik - 1;
+  pspw_cell *c = nullptr;
+  int rc = pspw_cell_create(
+      &c, device(), NR1, NR2, NR3, ngw, NGWX, n123 + col * NGWX, xkg + col * NGWX, TPIBA2, NSP, NA,
+      NAX, lm.data(), NLMAX,
+      reinterpret_cast<const double *>(eigr + col * (size_t)NGWX * NAX * NSP),
+      pkg_a + col * (size_t)NLMAX * NGWX * NSP, WNL);
+  if (rc) die("pspw_cell_create", rc);
+  k.cell = c;
+  for (int i = 0; i < 5; i++) k.key[i] = key[i];
+  k.ngw = ngw;
+  k.ngwx = NGWX;
+  k.nnr = NNR;
+  return c;
+}
+
+pspw_cell *cell_for(int ik) { return build_cell(ik, N123, XKG, EIGR, PKG_A); }
+
+int filter_prec() {
+  const char *p = std::getenv("PSPW_DROPIN_FILTER_PREC");
+  return (p && (!std::strcmp(p, "f32") || !std::strcmp(p, "F32"))) ? PSPW_PREC_F32 : PSPW_PREC_F64;
+}
+
+}  // namespace
+
+// ------------------------------------------------------------ host signatures
+
+// ApplyHam_block.cpp:5 / common_pspw.h:177
+DROPIN_API void ApplyHam_block(zcomplex *vin, zcomplex *vout, int NGW_ik, int ik, double *rho,
+                               int nnr, int nstates) {
+  check_nnr(nnr);
+  pspw_cell *c = cell_for(ik);
+  int rc = pspw_cell_set_veff(c, rho, nnr);
+  if (rc) die("ApplyHam_block", rc);
+  rc = pspw_apply_ham_block(c, reinterpret_cast<const double *>(vin),
+                            reinterpret_cast<double *>(vout), NGW_ik, nstates);
+  if (rc) die("ApplyHam_block", rc);
+}
+
+// ApplyHam.cpp:5 / common_pspw.h:176
+DROPIN_API void ApplyHam(zcomplex *vin, zcomplex *vout, int NGW_ik, int ik, double *rho, int nnr) {
+  ApplyHam_block(vin, vout, NGW_ik, ik, rho, nnr, 1);
+}
+
+// chebyfilt.cpp:6 / common_pspw.h:187.  The block width is the global NX+2
+// (chebyfilt.cpp:20,26,44), as in the reference.
+DROPIN_API void chebyfilt(int ik, zcomplex *X, int degree, double lb, double ub, double *rhoe,
+                          int nnr) {
+  check_nnr(nnr);
+  pspw_cell *c = cell_for(ik);
+  int rc = pspw_cell_set_veff(c, rhoe, nnr);
+  if (rc) die("chebyfilt", rc);
+  rc = pspw_chebyfilt(c, reinterpret_cast<double *>(X), NGW[ik - 1], NX + 2, degree, lb, ub,
+                      filter_prec());
+  if (rc) die("chebyfilt", rc);
+}
+
+// ------------------------------------------------------------ device API
+// (the CUDA layer the reference declares, common_pspw.h:252-259)
+
+DROPIN_API void SetupCUDA() { (void)device(); }
+
+DROPIN_API void ShutdownCUDA() {
+  for (auto &k : g_cells) drop_cell(k);
+  g_cells.clear();
+}
+
+DROPIN_API int SetupArrays_ApplyHam_cuda(unsigned int *n123, double *xkg, zcomplex *eigr,
+                                         double *pkg_a) {
+  for (auto &k : g_cells) drop_cell(k);
+  for (int ik = 1; ik <= NKPT; ik++) build_cell(ik, n123, xkg, eigr, pkg_a);
+  return 0;
+}
+
+DROPIN_API int SetupRho_ApplyHam_cuda() { return 0; }
+
+DROPIN_API int CopyRho_ApplyHam_cuda(double *rho) {
+  for (int ik = 1; ik <= NKPT; ik++) {
+    int rc = pspw_cell_set_veff(cell_for(ik), rho, NNR);
+    if (rc) return rc;
+  }
+  return 0;
+}
+
+// d_vin, d_vout: device FP64 blocks, ld = NGW_ik
+DROPIN_API int ApplyHam_block_cuda(zcomplex *d_vin, zcomplex *d_vout, int NGW_ik, int ik,
+                                   int nstates) {
+  pspw_cell *c = cell_for(ik);
+  int rc = pspw_apply_ham_block_dev(c, PSPW_PREC_F64, d_vin, d_vout, NGW_ik, NGW_ik, nstates);
+  if (rc) return rc;
+  return pspw_cell_synchronize(c);
+}
+
+DROPIN_API void FreeArrays_ApplyHam_cuda() { ShutdownCUDA(); }
+
+DROPIN_API void FreeRho_ApplyHam_cuda() {}

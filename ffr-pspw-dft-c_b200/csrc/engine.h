@@ -60,10 +60,25 @@ struct Projectors {
   float *d_pw32 = nullptr;
 };
 
+// Timing families (bit i of the mask enables family i).
+enum Family {
+  kFamAll = 0,       // a whole H*psi / filter call
+  kFamLocal = 1,     // the five FFT passes of a band batch
+  kFamNonlocal = 2,  // projector GEMMs
+  kFamSticksInv = 3,
+  kFamPlanesInv = 4,
+  kFamXlines = 5,
+  kFamPlanesFwd = 6,
+  kFamSticksFwd = 7,
+  kFamProj = 8,
+  kFamBackproj = 9,
+  kNumFamilies = 10
+};
+
 struct Timing {
   int mask = 0;
-  double ms[4] = {0, 0, 0, 0};
-  long long launches[4] = {0, 0, 0, 0};
+  double ms[kNumFamilies] = {};
+  long long launches[kNumFamilies] = {};
   std::vector<cudaEvent_t> ev_pool;
   std::vector<std::pair<int, std::pair<cudaEvent_t, cudaEvent_t>>> pending;
 };
@@ -89,6 +104,7 @@ struct pspw_cell {
   // partial sums, 3 = projections, 4.. = block buffers of the filter/solvers
   pspw::Workspace ws[12];
   pspw::Timing timing;
+  long long kernel_launches = 0;  // kernels this cell has enqueued
 };
 
 namespace pspw {

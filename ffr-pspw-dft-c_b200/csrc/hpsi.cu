@@ -474,6 +474,14 @@ int hpsi_apply(pspw_cell *c, const void *in_v, int ld_in, void *out_v, int ld_ou
   constexpr int BK = sizeof(R) == 8 ? 16 : 32;
   T *wp = nullptr;
   cudaEvent_t ev = nullptr;
+  // enqueue one kernel, with optional event timing of its family
+  auto run = [&](int fam, auto &&launch) {
+    cudaEvent_t e;
+    timing_begin(c, fam, &e);
+    launch();
+    timing_end(c, fam, e);
+    c->kernel_launches++;
+  };
   if (nproj > 0) {
     const int mt = (nproj + kBM - 1) / kBM, nt = (nb + kBN - 1) / kBN;
     // split G so the grid covers the GPU about twice
@@ -486,11 +494,15 @@ int hpsi_apply(pspw_cell *c, const void *in_v, int ld_in, void *out_v, int ld_ou
     if (rc) return rc;
     rc = ws_reserve(c, 3, sizeof(T) * (size_t)nb * nproj, (void **)&wp);
     if (rc) return rc;
-    timing_begin(c, 2, &ev);
-    k_proj<R, BK><<<dim3(mt, nt, nsplit), 256, 0, st>>>(pa, in, ld_in, ngw, nb, kchunk, part);
-    k_proj_reduce<R><<<(nb * nproj + 255) / 256, 256, 0, st>>>(part, Prec<R>::pw(c), nsplit, nb,
-                                                              nproj, wp);
-    timing_end(c, 2, ev);
+    timing_begin(c, kFamNonlocal, &ev);
+    run(kFamProj, [&] {
+      k_proj<R, BK><<<dim3(mt, nt, nsplit), 256, 0, st>>>(pa, in, ld_in, ngw, nb, kchunk, part);
+    });
+    run(kFamProj, [&] {
+      k_proj_reduce<R><<<(nb * nproj + 255) / 256, 256, 0, st>>>(part, Prec<R>::pw(c), nsplit, nb,
+                                                                nproj, wp);
+    });
+    timing_end(c, kFamNonlocal, ev);
     PSPW_CUDA(cudaGetLastError());
   }
 
@@ -518,33 +530,49 @@ int hpsi_apply(pspw_cell *c, const void *in_v, int ld_in, void *out_v, int ld_ou
     return rc;
   const FftArg fx = fft_arg(B.dim[0]), fy = fft_arg(B.dim[1]), fz = fft_arg(B.dim[2]);
   const T *wx = tw<T>(B.dim[0]), *wy = tw<T>(B.dim[1]), *wz = tw<T>(B.dim[2]);
-  timing_begin(c, 1, &ev);
+  timing_begin(c, kFamLocal, &ev);
   for (int b0 = 0; b0 < nb; b0 += nbatch) {
     const int nbb = std::min(nbatch, nb - b0);
     const T *inb = in + (size_t)b0 * ld_in;
     T *outb = out + (size_t)b0 * ld_out;
-    k_sticks_inv<T><<<dim3((B.ncol + T1 - 1) / T1, nbb), kNT, sm1, st>>>(geo, fz, wz, inb, ld_in,
-                                                                          ngw, S, T1);
-    k_planes_inv<T><<<dim3((B.nxa + T2 - 1) / T2, B.n3, nbb), kNT, sm2, st>>>(geo, fy, wy, S, P, T2);
-    k_xlines<T, R><<<dim3((B.n2 * B.n3 + L3 - 1) / L3, nbb), kNT, sm3, st>>>(
-        geo, fx, wx, Prec<R>::veff(c), P, L3);
-    k_planes_fwd<T><<<dim3((B.nxa + T2 - 1) / T2, B.n3, nbb), kNT, sm2, st>>>(geo, fy, wy, P, S, T2);
-    k_sticks_fwd<T, R><<<dim3((B.ncol + T1 - 1) / T1, nbb), kNT, sm1, st>>>(
-        geo, fz, wz, S, Prec<R>::kin(c), inb, ld_in, outb, ld_out, ngw, T1);
+    run(kFamSticksInv, [&] {
+      k_sticks_inv<T><<<dim3((B.ncol + T1 - 1) / T1, nbb), kNT, sm1, st>>>(geo, fz, wz, inb, ld_in,
+                                                                            ngw, S, T1);
+    });
+    run(kFamPlanesInv, [&] {
+      k_planes_inv<T><<<dim3((B.nxa + T2 - 1) / T2, B.n3, nbb), kNT, sm2, st>>>(geo, fy, wy, S, P,
+                                                                                T2);
+    });
+    run(kFamXlines, [&] {
+      k_xlines<T, R><<<dim3((B.n2 * B.n3 + L3 - 1) / L3, nbb), kNT, sm3, st>>>(
+          geo, fx, wx, Prec<R>::veff(c), P, L3);
+    });
+    run(kFamPlanesFwd, [&] {
+      k_planes_fwd<T><<<dim3((B.nxa + T2 - 1) / T2, B.n3, nbb), kNT, sm2, st>>>(geo, fy, wy, P, S,
+                                                                                T2);
+    });
+    run(kFamSticksFwd, [&] {
+      k_sticks_fwd<T, R><<<dim3((B.ncol + T1 - 1) / T1, nbb), kNT, sm1, st>>>(
+          geo, fz, wz, S, Prec<R>::kin(c), inb, ld_in, outb, ld_out, ngw, T1);
+    });
   }
-  timing_end(c, 1, ev);
+  timing_end(c, kFamLocal, ev);
   PSPW_CUDA(cudaGetLastError());
 
   // ---- back-projection + recurrence epilogue
   if (nproj > 0) {
-    timing_begin(c, 2, &ev);
+    timing_begin(c, kFamNonlocal, &ev);
     dim3 grid((ngw + kBM - 1) / kBM, (nb + kBN - 1) / kBN);
-    k_backproj<R, BK><<<grid, 256, 0, st>>>(pa, wp, ngw, nb, out, ld_out, in, ld_in, xm2, ld_xm2,
-                                            (R)a, (R)b, (R)g);
-    timing_end(c, 2, ev);
+    run(kFamBackproj, [&] {
+      k_backproj<R, BK><<<grid, 256, 0, st>>>(pa, wp, ngw, nb, out, ld_out, in, ld_in, xm2, ld_xm2,
+                                              (R)a, (R)b, (R)g);
+    });
+    timing_end(c, kFamNonlocal, ev);
   } else if (a != 1.0 || b != 0.0 || g != 0.0) {
-    k_axpby3<R><<<4 * 148, 256, 0, st>>>(ngw, nb, out, ld_out, in, ld_in, xm2, ld_xm2, (R)a, (R)b,
-                                        (R)g);
+    run(kFamBackproj, [&] {
+      k_axpby3<R><<<4 * 148, 256, 0, st>>>(ngw, nb, out, ld_out, in, ld_in, xm2, ld_xm2, (R)a,
+                                          (R)b, (R)g);
+    });
   }
   PSPW_CUDA(cudaGetLastError());
   return PSPW_OK;

@@ -54,6 +54,7 @@ SIGNATURES = {
     "pspw_cell_set_veff": [_vp, _vp, _i],
     "pspw_cell_set_veff_device": [_vp, _vp, _i],
     "pspw_cell_get_stream": [_vp, _vp],
+    "pspw_cell_synchronize": [_vp],
     "pspw_cell_sizes": [_vp, _vp],
     "pspw_cell_set_band_batch": [_vp, _i],
     "pspw_apply_ham_block": [_vp, _vp, _vp, _i, _i],
@@ -63,6 +64,7 @@ SIGNATURES = {
     "pspw_timing_enable": [_vp, _i],
     "pspw_timing_read": [_vp, _i, _vp, _vp],
     "pspw_timing_reset": [_vp],
+    "pspw_kernel_launches": [_vp, _vp],
 }
 _RESTYPE = {"pspw_error_string": C.c_char_p, "pspw_last_error": C.c_char_p}
 

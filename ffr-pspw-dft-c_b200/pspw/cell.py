@@ -159,5 +159,10 @@ class Cell:
     def timing_reset(self):
         check(lib().pspw_timing_reset(self._h))
 
+    def kernel_launches(self):
+        n = C.c_longlong()
+        check(lib().pspw_kernel_launches(self._h, C.byref(n)))
+        return n.value
+
 
 __all__ = ["Cell", "basis_gamma", "PREC_F32", "PREC_F64"]

@@ -99,8 +99,10 @@ int pspw_cell_destroy(pspw_cell *cell);
  * NR1*NR2*NR3 (ApplyHam_block.cpp:18-21). */
 int pspw_cell_set_veff(pspw_cell *cell, const double *veff, int nnr);
 int pspw_cell_set_veff_device(pspw_cell *cell, const double *d_veff, int nnr);
-/* the cell's CUDA stream (cudaStream_t) and basic sizes */
+/* the cell's CUDA stream (cudaStream_t), a wait for its queued work, and
+ * basic sizes {n1,n2,n3,ngw,sticks,active x,atoms,projectors} */
 int pspw_cell_get_stream(pspw_cell *cell, void **stream);
+int pspw_cell_synchronize(pspw_cell *cell);
 int pspw_cell_sizes(pspw_cell *cell, int *out8);
 /* cap the number of bands transformed per batch of the FFT passes
  * (0 = automatic); results do not depend on it */
@@ -127,12 +129,16 @@ int pspw_chebyfilt_dev(pspw_cell *cell, int prec, void *d_X, int ld, int ngw, in
                        int degree, double lb, double ub);
 
 /* ------------------------------------------------------------------ timing
- * Optional per-kernel-family device timing on the cell stream (CUDA events
- * around each launch of the selected family, summed until reset).  Families:
- * 0 = all H*psi work, 1 = FFT passes, 2 = projector GEMMs. */
+ * Optional device timing on the cell stream: CUDA events around each launch
+ * of the enabled families, summed until reset.  Families (bit i of the mask):
+ * 0 whole H*psi / filter call, 1 FFT pass chain, 2 projector GEMMs,
+ * 3 sticks_inv, 4 planes_inv, 5 xlines, 6 planes_fwd, 7 sticks_fwd,
+ * 8 projection GEMM (+ reduction), 9 back-projection GEMM. */
 int pspw_timing_enable(pspw_cell *cell, int family_mask);
 int pspw_timing_read(pspw_cell *cell, int family, double *total_ms, long long *launches);
 int pspw_timing_reset(pspw_cell *cell);
+/* number of kernels the cell has enqueued since creation */
+int pspw_kernel_launches(pspw_cell *cell, long long *count);
 
 #if defined(__GNUC__)
 #pragma GCC visibility pop

@@ -45,9 +45,13 @@ def test_error_strings_without_gpu():
 # g++ mangled names of the reference functions the drop-in replaces
 # (signatures from common_pspw.h:176-222)
 DROPIN_SYMBOLS = [
-    "_Z14ApplyHam_blockPCdS0_iiPdii",
-    "_Z8ApplyHamPCdS0_iiPdi",
-    "_Z9chebyfiltiPCdiddPdi",
+    "_Z14ApplyHam_blockPCdS0_iiPdii",       # ApplyHam_block        common_pspw.h:177
+    "_Z8ApplyHamPCdS0_iiPdi",               # ApplyHam              common_pspw.h:176
+    "_Z9chebyfiltiPCdiddPdi",               # chebyfilt             common_pspw.h:187
+    "_Z19ApplyHam_block_cudaPCdS0_iii",     # ApplyHam_block_cuda   common_pspw.h:254
+    "_Z25SetupArrays_ApplyHam_cudaPjPdPCdS0_",  # SetupArrays_...   common_pspw.h:255
+    "_Z21CopyRho_ApplyHam_cudaPd",          # CopyRho_ApplyHam_cuda common_pspw.h:257
+    "_Z9SetupCUDAv", "_Z12ShutdownCUDAv",   # common_pspw.h:252-253
 ]
 
 
