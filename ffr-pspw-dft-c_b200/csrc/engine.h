@@ -124,10 +124,21 @@ int ws_reserve(pspw_cell *c, int slot, size_t bytes, void **out);
 void timing_begin(pspw_cell *c, int family, cudaEvent_t *ev);
 void timing_end(pspw_cell *c, int family, cudaEvent_t ev);
 
+// Scratch supplied by the caller of hpsi_apply instead of the cell's
+// workspaces: stick and plane buffers for `nbatch` bands, `max_split` slices
+// of projector partial sums, and the projections.
+struct ScratchPlan {
+  void *S, *P, *part, *wp;
+  int nbatch;
+  int max_split;
+};
+
 // H*psi on device blocks of precision R.  out = a*(H in) + b*in + g*xm2
-// (xm2 may be null when g == 0).  ld_in/ld_out >= ngw.
+// (xm2 may be null when g == 0).  ld_in/ld_out >= ngw.  With `plan`, all
+// scratch comes from it and no workspace is reserved.
 template <typename R>
 int hpsi_apply(pspw_cell *c, const void *in, int ld_in, void *out, int ld_out, int ngw,
-               int nb, double a, double b, double g, const void *xm2, int ld_xm2);
+               int nb, double a, double b, double g, const void *xm2, int ld_xm2,
+               const ScratchPlan *plan = nullptr);
 
 }  // namespace pspw

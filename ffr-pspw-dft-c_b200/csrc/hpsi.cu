@@ -445,7 +445,8 @@ int set_smem(K kernel, size_t bytes) {
 
 template <typename R>
 int hpsi_apply(pspw_cell *c, const void *in_v, int ld_in, void *out_v, int ld_out, int ngw, int nb,
-               double a, double b, double g, const void *xm2_v, int ld_xm2) {
+               double a, double b, double g, const void *xm2_v, int ld_xm2,
+               const ScratchPlan *plan) {
   using T = cx<R>;
   const Basis &B = c->basis;
   if (nb <= 0) return PSPW_OK;
@@ -486,14 +487,20 @@ int hpsi_apply(pspw_cell *c, const void *in_v, int ld_in, void *out_v, int ld_ou
     const int mt = (nproj + kBM - 1) / kBM, nt = (nb + kBN - 1) / kBN;
     // split G so the grid covers the GPU about twice
     int nsplit = std::max(1, std::min((ngw + 255) / 256, (2 * 148 + mt * nt - 1) / (mt * nt)));
+    if (plan) nsplit = std::max(1, std::min(nsplit, plan->max_split));
     int kchunk = (ngw + nsplit - 1) / nsplit;
     kchunk = (kchunk + BK - 1) / BK * BK;
     nsplit = (ngw + kchunk - 1) / kchunk;
     T *part = nullptr;
-    int rc = ws_reserve(c, 2, sizeof(T) * (size_t)nsplit * nb * nproj, (void **)&part);
-    if (rc) return rc;
-    rc = ws_reserve(c, 3, sizeof(T) * (size_t)nb * nproj, (void **)&wp);
-    if (rc) return rc;
+    if (plan) {
+      part = static_cast<T *>(plan->part);
+      wp = static_cast<T *>(plan->wp);
+    } else {
+      int rc = ws_reserve(c, 2, sizeof(T) * (size_t)nsplit * nb * nproj, (void **)&part);
+      if (rc) return rc;
+      rc = ws_reserve(c, 3, sizeof(T) * (size_t)nb * nproj, (void **)&wp);
+      if (rc) return rc;
+    }
     timing_begin(c, kFamNonlocal, &ev);
     run(kFamProj, [&] {
       k_proj<R, BK><<<dim3(mt, nt, nsplit), 256, 0, st>>>(pa, in, ld_in, ngw, nb, kchunk, part);
@@ -515,12 +522,19 @@ int hpsi_apply(pspw_cell *c, const void *in_v, int ld_in, void *out_v, int ld_ou
     // keep a batch's stick and plane buffers within ~48 MB so they stay in L2
     nbatch = (int)std::max<size_t>(1, (48u << 20) / ((s_band + p_band) * sizeof(T)));
   }
+  if (plan) nbatch = plan->nbatch;
   nbatch = std::min(nbatch, nb);
   T *S = nullptr, *P = nullptr;
-  int rc = ws_reserve(c, 0, sizeof(T) * s_band * nbatch, (void **)&S);
-  if (rc) return rc;
-  rc = ws_reserve(c, 1, sizeof(T) * p_band * nbatch, (void **)&P);
-  if (rc) return rc;
+  int rc = PSPW_OK;
+  if (plan) {
+    S = static_cast<T *>(plan->S);
+    P = static_cast<T *>(plan->P);
+  } else {
+    rc = ws_reserve(c, 0, sizeof(T) * s_band * nbatch, (void **)&S);
+    if (rc) return rc;
+    rc = ws_reserve(c, 1, sizeof(T) * p_band * nbatch, (void **)&P);
+    if (rc) return rc;
+  }
   const int T1 = tile_lines(B.n3), T2 = tile_lines(B.n2), L3 = tile_lines(B.n1);
   const size_t sm1 = pass_smem<T>(T1, B.n3), sm2 = pass_smem<T>(T2, B.n2),
                sm3 = pass_smem<T>(L3, B.n1);
@@ -579,8 +593,8 @@ int hpsi_apply(pspw_cell *c, const void *in_v, int ld_in, void *out_v, int ld_ou
 }
 
 template int hpsi_apply<double>(pspw_cell *, const void *, int, void *, int, int, int, double,
-                                double, double, const void *, int);
+                                double, double, const void *, int, const ScratchPlan *);
 template int hpsi_apply<float>(pspw_cell *, const void *, int, void *, int, int, int, double,
-                               double, double, const void *, int);
+                               double, double, const void *, int, const ScratchPlan *);
 
 }  // namespace pspw

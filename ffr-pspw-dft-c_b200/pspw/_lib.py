@@ -59,6 +59,7 @@ SIGNATURES = {
     "pspw_cell_set_band_batch": [_vp, _i],
     "pspw_apply_ham_block": [_vp, _vp, _vp, _i, _i],
     "pspw_apply_ham_block_dev": [_vp, _i, _vp, _vp, _i, _i, _i],
+    "pspw_apply_ham_block_dev_noalloc": [_vp, _i, _vp, _vp, _i, _i, _i],
     "pspw_chebyfilt": [_vp, _vp, _i, _i, _i, _d, _d, _i],
     "pspw_chebyfilt_dev": [_vp, _i, _vp, _i, _i, _i, _i, _d, _d],
     "pspw_timing_enable": [_vp, _i],

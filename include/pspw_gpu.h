@@ -119,6 +119,21 @@ int pspw_apply_ham_block(pspw_cell *cell, const double *vin, double *vout, int n
 int pspw_apply_ham_block_dev(pspw_cell *cell, int prec, const void *d_vin, void *d_vout, int ld,
                              int ngw, int nstates);
 
+/* The same H*psi as pspw_apply_ham_block_dev, with no device allocation on
+ * the call path.  No counterpart in the reference.  For callers that cannot
+ * let a library allocate when it is called: code being captured into a CUDA
+ * graph, applications whose memory manager owns all device memory, services
+ * that must not fail for lack of memory mid-request.  All scratch comes from
+ * one static 16 MiB device array in the library (held by every GPU that
+ * loads it until exit); cell/block sizes whose scratch does not fit are
+ * rejected with PSPW_ERR_SHAPE.  The first call on a device looks up the
+ * array's device address (cudaGetSymbolAddress) and should come before any
+ * stream capture.  All calls share the array: calls that overlap on the GPU
+ * race and must be serialised by the caller.  Set V_eff with
+ * pspw_cell_set_veff_device, which does not allocate either. */
+int pspw_apply_ham_block_dev_noalloc(pspw_cell *cell, int prec, const void *d_vin, void *d_vout,
+                                     int ld, int ngw, int nstates);
+
 /* ------------------------------------------------------------------ filter
  * Degree-`degree` scaled Chebyshev filter of chebyfilt.cpp:6-74 applied to
  * the ngw x nstates block X in place.  Host FP64 X; `prec` selects the
