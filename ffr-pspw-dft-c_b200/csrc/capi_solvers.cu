@@ -1,0 +1,265 @@
+// C ABI of the eigensolvers, dense steps, preconditioner, random start and
+// density (host-buffer entry points mirroring the reference signatures).
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <string>
+#include <vector>
+
+#include "common.cuh"
+#include "dense.h"
+#include "engine.h"
+#include "fftpath.h"
+#include "solvers.h"
+
+namespace pspw {
+namespace {
+
+int enter(pspw_cell *c) {
+  if (!c) return fail(PSPW_ERR_ARG, "null cell");
+  PSPW_CUDA(cudaSetDevice(c->device));
+  return PSPW_OK;
+}
+
+// upload an m x n column-major host matrix (ld) into a compact device buffer
+int up_mat(pspw_cell *c, int slot, const double *h, int ld, int m, int n, double2 **d) {
+  int rc = ws_reserve(c, slot, sizeof(double2) * (size_t)std::max(1, m) * std::max(1, n), (void **)d);
+  if (rc) return rc;
+  PSPW_CUDA(cudaMemcpy2DAsync(*d, sizeof(double2) * m, h, sizeof(double2) * ld, sizeof(double2) * m,
+                              n, cudaMemcpyHostToDevice, c->stream));
+  return PSPW_OK;
+}
+
+int down_mat(pspw_cell *c, double *h, int ld, const double2 *d, int m, int n) {
+  PSPW_CUDA(cudaMemcpy2DAsync(h, sizeof(double2) * ld, d, sizeof(double2) * m, sizeof(double2) * m,
+                              n, cudaMemcpyDeviceToHost, c->stream));
+  return PSPW_OK;
+}
+
+int sync(pspw_cell *c) {
+  PSPW_CUDA(cudaStreamSynchronize(c->stream));
+  return PSPW_OK;
+}
+
+// ss[j] = sum_{i<m} |c|^2, sk[j] = sum_{i<m} xkg[i] |c|^2 (EvalRhoPsi.cpp:117-126)
+__global__ void k_charge_sums(const double2 *__restrict__ X, int ld, int m,
+                              const double *__restrict__ xkg, double *ss, double *sk) {
+  __shared__ double r1[256], r2[256];
+  const int j = blockIdx.x;
+  const double2 *col = X + (size_t)j * ld;
+  double a = 0.0, b = 0.0;
+  for (int i = threadIdx.x; i < m; i += blockDim.x) {
+    const double2 v = col[i];
+    const double q = v.x * v.x + v.y * v.y;
+    a += q;
+    b += xkg[i] * q;
+  }
+  r1[threadIdx.x] = a;
+  r2[threadIdx.x] = b;
+  __syncthreads();
+  for (int w = blockDim.x / 2; w > 0; w >>= 1) {
+    if (threadIdx.x < w) {
+      r1[threadIdx.x] += r1[threadIdx.x + w];
+      r2[threadIdx.x] += r2[threadIdx.x + w];
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    ss[j] = r1[0];
+    sk[j] = r2[0];
+  }
+}
+
+constexpr int kSlotA = kWsSolverBase + 11;
+constexpr int kSlotB = kWsSolverBase + 12;
+constexpr int kSlotC = kWsSolverBase + 13;
+constexpr int kSlotD = kWsSolverBase + 14;
+
+}  // namespace
+}  // namespace pspw
+
+using namespace pspw;
+
+extern "C" {
+
+int pspw_random_col(double *A, int nelem, long seed) {
+  if (!A || nelem < 0) return fail(PSPW_ERR_ARG, "random_col: bad argument");
+  random_col_host(reinterpret_cast<double2 *>(A), nelem, seed);
+  return PSPW_OK;
+}
+
+int pspw_gen_prec(pspw_cell *c, double *prec, int nbasis, double tau) {
+  int rc = enter(c);
+  if (rc) return rc;
+  double *d = nullptr;
+  if ((rc = ws_reserve(c, kSlotA, sizeof(double) * (size_t)std::max(1, nbasis), (void **)&d)) ||
+      (rc = gen_prec_dev(c, d, nbasis, tau)))
+    return rc;
+  PSPW_CUDA(cudaMemcpyAsync(prec, d, sizeof(double) * nbasis, cudaMemcpyDeviceToHost, c->stream));
+  return sync(c);
+}
+
+int pspw_ortho_qr(pspw_cell *c, double *X, int nbasis, int nstates) {
+  int rc = enter(c);
+  if (rc) return rc;
+  if (!X || nbasis < nstates || nstates < 0) return fail(PSPW_ERR_ARG, "ortho_qr: bad shape");
+  double2 *d;
+  if ((rc = up_mat(c, kSlotA, X, nbasis, nbasis, nstates, &d))) return rc;
+  int info = 0;
+  if ((rc = dev_ortho_qr(c, d, nbasis, nbasis, nstates, &info))) return rc;
+  if (info) return fail(PSPW_ERR_LAPACK, "zgeqrf/zungqr: info = " + std::to_string(info));
+  if ((rc = down_mat(c, X, nbasis, d, nbasis, nstates))) return rc;
+  return sync(c);
+}
+
+int pspw_eig_zheevd(pspw_cell *c, double *A, int lda, double *lambda, int n) {
+  int rc = enter(c);
+  if (rc) return rc;
+  double2 *d;
+  double *w;
+  if ((rc = up_mat(c, kSlotA, A, lda, n, n, &d)) ||
+      (rc = ws_reserve(c, kSlotB, sizeof(double) * (size_t)std::max(1, n), (void **)&w)))
+    return rc;
+  int info = 0;
+  if ((rc = dev_zheevd(c, d, n, w, n, &info))) return rc;
+  if (info) return fail(PSPW_ERR_LAPACK, "zheevd: info = " + std::to_string(info));
+  if ((rc = down_mat(c, A, lda, d, n, n))) return rc;
+  PSPW_CUDA(cudaMemcpyAsync(lambda, w, sizeof(double) * n, cudaMemcpyDeviceToHost, c->stream));
+  return sync(c);
+}
+
+int pspw_eig_zhegv_eval(pspw_cell *c, double *A, int lda, double *B, int ldb, double *eval,
+                        double *evec, int lde, int n) {
+  int rc = enter(c);
+  if (rc) return rc;
+  double2 *dA, *dB, *dE;
+  double *w;
+  if ((rc = up_mat(c, kSlotA, A, lda, n, n, &dA)) || (rc = up_mat(c, kSlotB, B, ldb, n, n, &dB)) ||
+      (rc = ws_reserve(c, kSlotC, sizeof(double2) * (size_t)n * n, (void **)&dE)) ||
+      (rc = ws_reserve(c, kSlotD, sizeof(double) * (size_t)n, (void **)&w)))
+    return rc;
+  int nn = 0;
+  if ((rc = dev_zhegv(c, dA, n, dB, n, w, dE, n, n, &nn))) return rc;
+  if (nn < n)
+    std::printf("Warning: Number of linearly independent vectors = %d\n         while size of the "
+                "problem: %d\n", nn, n);
+  if ((rc = down_mat(c, A, lda, dA, n, n)) || (rc = down_mat(c, B, ldb, dB, n, n)) ||
+      (rc = down_mat(c, evec, lde, dE, n, n)))
+    return rc;
+  if (eval) PSPW_CUDA(cudaMemcpyAsync(eval, w, sizeof(double) * n, cudaMemcpyDeviceToHost, c->stream));
+  return sync(c);
+}
+
+int pspw_eig_zhegv(pspw_cell *c, double *A, int lda, double *B, int ldb, double *evec, int lde,
+                   int n) {
+  return pspw_eig_zhegv_eval(c, A, lda, B, ldb, nullptr, evec, lde, n);
+}
+
+static int solver_entry(bool lobpcg, pspw_cell *c, double *evals, double *X, int nbasis,
+                        int nstates, const double *prec, int nempty, int max_iter, int hprec,
+                        double *resnrm, int *iters) {
+  int rc = enter(c);
+  if (rc) return rc;
+  if (!evals || !X || !prec || nstates <= 0 || nbasis < nstates)
+    return fail(PSPW_ERR_ARG, "eigensolver: bad argument");
+  if (nbasis > c->basis.ngw) return fail(PSPW_ERR_SHAPE, "eigensolver: nbasis exceeds the cell");
+  if (hprec != PSPW_PREC_F64 && hprec != PSPW_PREC_F32) return fail(PSPW_ERR_ARG, "bad precision");
+  double2 *dX;
+  double *dp;
+  if ((rc = ws_reserve(c, kSlotA, sizeof(double2) * (size_t)nbasis * nstates, (void **)&dX)) ||
+      (rc = ws_reserve(c, kSlotB, sizeof(double) * (size_t)nbasis, (void **)&dp)))
+    return rc;
+  PSPW_CUDA(cudaMemcpyAsync(dp, prec, sizeof(double) * nbasis, cudaMemcpyHostToDevice, c->stream));
+  rc = lobpcg ? lobpcg_dev(c, hprec, evals, dX, nbasis, nstates, dp, nempty, max_iter, resnrm, iters)
+              : davidson_dev(c, hprec, evals, dX, nbasis, nstates, dp, nempty, max_iter, resnrm,
+                             iters);
+  if (rc) return rc;
+  PSPW_CUDA(cudaMemcpyAsync(X, dX, sizeof(double2) * (size_t)nbasis * nstates,
+                            cudaMemcpyDeviceToHost, c->stream));
+  return sync(c);
+}
+
+int pspw_davidson(pspw_cell *c, double *evals, double *X, int nbasis, int nstates,
+                  const double *prec, int nempty, int max_iter, int hprec, double *resnrm,
+                  int *iters) {
+  return solver_entry(false, c, evals, X, nbasis, nstates, prec, nempty, max_iter, hprec, resnrm,
+                      iters);
+}
+
+int pspw_lobpcg(pspw_cell *c, double *lambda, double *X, int nbasis, int nstates,
+                const double *prec, int nempty, int max_iter, int hprec, double *resnrm,
+                int *iters) {
+  return solver_entry(true, c, lambda, X, nbasis, nstates, prec, nempty, max_iter, hprec, resnrm,
+                      iters);
+}
+
+int pspw_lanczos(pspw_cell *c, double *v0, int ngw, int k, double *T, int ldT, double *f) {
+  int rc = enter(c);
+  if (rc) return rc;
+  if (!v0 || !T || k < 1 || ldT < k || ngw < 1) return fail(PSPW_ERR_ARG, "lanczos: bad argument");
+  double2 *dv, *df;
+  if ((rc = ws_reserve(c, kSlotA, sizeof(double2) * (size_t)ngw, (void **)&dv)) ||
+      (rc = ws_reserve(c, kSlotB, sizeof(double2) * (size_t)ngw, (void **)&df)))
+    return rc;
+  PSPW_CUDA(cudaMemcpyAsync(dv, v0, sizeof(double2) * ngw, cudaMemcpyHostToDevice, c->stream));
+  if ((rc = lanczos_dev(c, dv, ngw, k, T, ldT, df))) return rc;
+  PSPW_CUDA(cudaMemcpyAsync(v0, dv, sizeof(double2) * ngw, cudaMemcpyDeviceToHost, c->stream));
+  if (f) PSPW_CUDA(cudaMemcpyAsync(f, df, sizeof(double2) * ngw, cudaMemcpyDeviceToHost, c->stream));
+  return sync(c);
+}
+
+int pspw_eval_rho_psi(pspw_cell *c, double *rhoe, const double *eigvec, int ld, int ngw, int nx,
+                      const double *focc, double wkpt, double omega, double *ekin) {
+  int rc = enter(c);
+  if (rc) return rc;
+  if (!rhoe || !eigvec || !focc || nx < 0 || ld < ngw || ngw < 1)
+    return fail(PSPW_ERR_ARG, "EvalRhoPsi: bad argument");
+  if (nx == 0) return PSPW_OK;
+  const Basis &B = c->basis;
+  if (ngw > B.ngw) return fail(PSPW_ERR_SHAPE, "EvalRhoPsi: NGW exceeds the cell");
+  if (!B.fast) return fail(PSPW_ERR_NOT_IMPL, "EvalRhoPsi: grid lengths without a register split");
+  const int m = ngw - 1;  // the scatter stops at ig < NGW_ik (EvalRhoPsi.cpp:117)
+  double2 *dX;
+  double *dsum, *drho, *dw;
+  if ((rc = ws_reserve(c, kSlotA, sizeof(double2) * (size_t)ld * nx, (void **)&dX)) ||
+      (rc = ws_reserve(c, kSlotB, sizeof(double) * 2 * (size_t)nx, (void **)&dsum)) ||
+      (rc = ws_reserve(c, kSlotC, sizeof(double) * (size_t)B.nnr, (void **)&drho)) ||
+      (rc = ws_reserve(c, kSlotD, sizeof(double) * (size_t)nx, (void **)&dw)))
+    return rc;
+  PSPW_CUDA(cudaMemcpyAsync(dX, eigvec, sizeof(double2) * ((size_t)ld * (nx - 1) + ngw),
+                            cudaMemcpyHostToDevice, c->stream));
+  k_charge_sums<<<nx, 256, 0, c->stream>>>(dX, ld, m, B.d_xkg64, dsum, dsum + nx);
+  c->kernel_launches++;
+  std::vector<double> sums(2 * (size_t)nx);
+  PSPW_CUDA(cudaMemcpyAsync(sums.data(), dsum, sizeof(double) * 2 * nx, cudaMemcpyDeviceToHost,
+                            c->stream));
+  if ((rc = sync(c))) return rc;
+  double xkin = 0.0;
+  std::vector<double> wband(nx);
+  for (int i = 0; i < nx; i++) {
+    const double ss = sums[i];
+    if (std::fabs(ss - 1.0) > 6.e-3) {  // EvalRhoPsi.cpp:129-133
+      char msg[160];
+      std::snprintf(msg, sizeof msg,
+                    "Wrong charge density in G-space: %18.10f for k-point 1 and states %d", ss,
+                    i + 1);
+      return fail(PSPW_ERR_CHARGE, msg);
+    }
+    const double wdotf = wkpt * focc[i];
+    xkin = xkin + sums[nx + i] * (wdotf * 0.5);
+    wband[i] = wdotf / omega;
+  }
+  PSPW_CUDA(cudaMemcpyAsync(dw, wband.data(), sizeof(double) * nx, cudaMemcpyHostToDevice, c->stream));
+  PSPW_CUDA(cudaMemcpyAsync(drho, rhoe, sizeof(double) * B.nnr, cudaMemcpyHostToDevice, c->stream));
+  const FastGeo g{B.ncol, B.nxa, B.d_col_start, B.d_sg_ig, B.d_sg_z, B.d_sg_col, B.d_xa_list,
+                  B.d_col_x, B.d_col_y};
+  if ((rc = rho_fast<double>(c, g, dX, ld, m, nx, dw, drho))) return rc;
+  PSPW_CUDA(cudaMemcpyAsync(rhoe, drho, sizeof(double) * B.nnr, cudaMemcpyDeviceToHost, c->stream));
+  if ((rc = sync(c))) return rc;
+  if (ekin) *ekin = *ekin + xkin * c->tpiba2;  // EvalRhoPsi.cpp:154
+  return PSPW_OK;
+}
+
+}  // extern "C"

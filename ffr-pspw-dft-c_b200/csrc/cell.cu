@@ -1,7 +1,9 @@
 // Cell set-up (the engine side of SetupArrays_ApplyHam_cuda /
 // CopyRho_ApplyHam_cuda, common_pspw.h:255-257), error state, workspaces and
 // the optional device timing hooks.
+#include <cublas_v2.h>
 #include <cuda_runtime.h>
+#include <cusolverDn.h>
 
 #include <algorithm>
 #include <cmath>
@@ -13,6 +15,8 @@
 
 #include "common.cuh"
 #include "engine.h"
+#include "fft2.cuh"
+#include "fftpath.h"
 
 namespace pspw {
 
@@ -112,6 +116,39 @@ int upload(T **d, const std::vector<T> &h) {
   return PSPW_OK;
 }
 
+// exp(2 pi i t / n) with the angle reduced exactly to the first half
+// quadrant (integer arithmetic) and exact values at multiples of 30 and 45
+// degrees, so the table is symmetric to the last bit.
+void root_of_unity(long t, long n, double *c, double *s) {
+  t %= n;
+  const long q = (4 * t) / n;           // quadrant
+  long rem = 4 * t - q * n;             // quarter-turn fraction rem/n
+  const bool flip = 2 * rem > n;
+  if (flip) rem = n - rem;
+  double cc, ss;
+  if (rem == 0) {
+    cc = 1.0;
+    ss = 0.0;
+  } else if (3 * rem == n) {
+    cc = std::sqrt(3.0) / 2.0;
+    ss = 0.5;
+  } else if (2 * rem == n) {
+    cc = ss = std::sqrt(0.5);
+  } else {
+    const double a = (M_PI / 2.0) * (double)rem / (double)n;
+    cc = std::cos(a);
+    ss = std::sin(a);
+  }
+  if (flip) std::swap(cc, ss);
+  for (long k = 0; k < q; k++) {
+    const double tmp = cc;
+    cc = -ss;
+    ss = tmp;
+  }
+  *c = cc + 0.0;
+  *s = ss + 0.0;
+}
+
 int make_dim(FftDim &d, int n) {
   d.n = n;
   int rc = factor_radices(n, d.rad, &d.nf);
@@ -119,19 +156,8 @@ int make_dim(FftDim &d, int n) {
   std::vector<double2> w64(n);
   std::vector<float2> w32(n);
   for (int t = 0; t < n; t++) {
-    // exp(+2 pi i t/n), angle reduced to the first half turn for accuracy
-    const double ang = 2.0 * M_PI * (double)t / (double)n;
-    double c = std::cos(ang), s = std::sin(ang);
-    if (4 * t == n) {
-      c = 0.0;
-      s = 1.0;
-    } else if (2 * t == n) {
-      c = -1.0;
-      s = 0.0;
-    } else if (4 * t == 3 * n) {
-      c = 0.0;
-      s = -1.0;
-    }
+    double c, s;
+    root_of_unity(t, n, &c, &s);
     w64[t] = make_double2(c, s);
     w32[t] = make_float2((float)c, (float)s);
   }
@@ -173,9 +199,11 @@ int pspw_cell_destroy(pspw_cell *c) {
   if (c->stream) cudaStreamSynchronize(c->stream);
   Basis &B = c->basis;
   void *ptrs[] = {B.d_col_start, B.d_sg_ig, B.d_sg_z, B.d_sg_col, B.d_col_of_xy, B.d_xa_list,
-                  B.d_xa_of_x, B.d_kin64, B.d_kin32, c->proj.d_eigr64, c->proj.d_eigr32,
+                  B.d_xa_of_x, B.d_kin64, B.d_kin32, B.d_xkg64, c->proj.d_eigr64, c->proj.d_eigr32,
                   c->proj.d_pkga64, c->proj.d_pkga32, c->proj.d_patom, c->proj.d_psp,
-                  c->proj.d_plm, c->proj.d_pw64, c->proj.d_pw32, c->d_veff64, c->d_veff32};
+                  c->proj.d_plm, c->proj.d_pw64, c->proj.d_pw32, c->d_veff64, c->d_veff32,
+                  B.d_col_x, B.d_col_y, B.d_pinv[0], B.d_pinv[1], B.d_pinv[2], c->d_vperm64,
+                  c->d_vperm32};
   for (void *p : ptrs)
     if (p) cudaFree(p);
   for (int i = 0; i < 3; i++) {
@@ -188,6 +216,8 @@ int pspw_cell_destroy(pspw_cell *c) {
     cudaEventDestroy(p.second.first);
     cudaEventDestroy(p.second.second);
   }
+  if (c->cusolver) cusolverDnDestroy(static_cast<cusolverDnHandle_t>(c->cusolver));
+  if (c->cublas) cublasDestroy(static_cast<cublasHandle_t>(c->cublas));
   if (c->stream) cudaStreamDestroy(c->stream);
   delete c;
   return PSPW_OK;
@@ -278,8 +308,9 @@ int pspw_cell_create(pspw_cell **out, int device, int nr1, int nr2, int nr3, int
     }
   B.ncol = ncol;
   B.nxa = (int)xa_list.size();
-  std::vector<double> kin64(ngw);
+  std::vector<double> kin64(ngw), xkg64(xkg, xkg + ngw);
   std::vector<float> kin32(ngw);
+  c->tpiba2 = tpiba2;
   for (int ig = 0; ig < ngw; ig++) {
     kin64[ig] = 0.5 * xkg[ig] * tpiba2;  // ApplyHam_block.cpp:59, same rounding order
     kin32[ig] = (float)kin64[ig];
@@ -288,11 +319,26 @@ int pspw_cell_create(pspw_cell **out, int device, int nr1, int nr2, int nr3, int
       (rc = upload(&B.d_sg_z, sg_z)) || (rc = upload(&B.d_sg_col, sg_col)) ||
       (rc = upload(&B.d_col_of_xy, col_of_xy)) || (rc = upload(&B.d_xa_list, xa_list)) ||
       (rc = upload(&B.d_xa_of_x, xa_of_x)) || (rc = upload(&B.d_kin64, kin64)) ||
+      (rc = upload(&B.d_xkg64, xkg64)) ||
       (rc = upload(&B.d_kin32, kin32)))
     return bail(rc);
   const int nr[3] = {nr1, nr2, nr3};
   for (int i = 0; i < 3; i++)
     if ((rc = make_dim(B.dim[i], nr[i]))) return bail(rc);
+  // register-FFT path when all three lengths split into two register DFTs
+  B.fast = !std::getenv("PSPW_GENERIC_FFT") && fast_supported(nr1, nr2, nr3);
+  if (B.fast) {
+    if ((rc = upload(&B.d_col_x, col_x)) || (rc = upload(&B.d_col_y, col_y))) return bail(rc);
+    for (int i = 0; i < 3; i++) {
+      const NSplit sp = nsplit_for(nr[i]);
+      std::vector<int> pinv(nr[i]);
+      for (int p = 0; p < nr[i]; p++) pinv[p] = p / sp.n1 + sp.n2 * (p % sp.n1);
+      if ((rc = upload(&B.d_pinv[i], pinv))) return bail(rc);
+    }
+    if (cudaMalloc(&c->d_vperm64, (size_t)B.nnr * sizeof(double)) != cudaSuccess ||
+        cudaMalloc(&c->d_vperm32, (size_t)B.nnr * sizeof(float)) != cudaSuccess)
+      return bail(fail(PSPW_ERR_OOM, "cell_create: permuted V_eff"));
+  }
   // ---- projectors, species-major then atom then lm (ApplyHam_block.cpp:68-117)
   Projectors &P = c->proj;
   P.nat = nat;
@@ -349,6 +395,20 @@ int pspw_cell_create(pspw_cell **out, int device, int nr1, int nr2, int nr3, int
 namespace pspw {
 namespace {
 
+// V_eff/NNR gathered into the digit-permuted (z, y, x) order of the
+// register-FFT path.
+__global__ void k_veff_perm(const double *__restrict__ v, int n1, int n2, int n3, double s,
+                            const int *__restrict__ px, const int *__restrict__ py,
+                            const int *__restrict__ pz, double *o64, float *o32) {
+  const int n = n1 * n2 * n3;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const int a = i % n1, b = (i / n1) % n2, cz = i / (n1 * n2);
+    const double x = v[((size_t)pz[cz] * n2 + py[b]) * n1 + px[a]] * s;
+    o64[i] = x;
+    o32[i] = (float)x;
+  }
+}
+
 __global__ void k_veff_scale(const double *__restrict__ v, int n, double s, double *o64,
                              float *o32) {
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
@@ -370,6 +430,13 @@ int pspw_cell_set_veff_device(pspw_cell *c, const double *d_veff, int nnr) {
   k_veff_scale<<<2 * 148, 256, 0, c->stream>>>(d_veff, nnr, 1.0 / (double)nnr, c->d_veff64,
                                                 c->d_veff32);
   c->kernel_launches++;
+  const Basis &B = c->basis;
+  if (B.fast) {
+    k_veff_perm<<<2 * 148, 256, 0, c->stream>>>(d_veff, B.n1, B.n2, B.n3, 1.0 / (double)nnr,
+                                                 B.d_pinv[0], B.d_pinv[1], B.d_pinv[2],
+                                                 c->d_vperm64, c->d_vperm32);
+    c->kernel_launches++;
+  }
   PSPW_CUDA(cudaGetLastError());
   c->veff_set = true;
   return PSPW_OK;
@@ -380,7 +447,7 @@ int pspw_cell_set_veff(pspw_cell *c, const double *veff, int nnr) {
   if (nnr != c->basis.nnr) return fail(PSPW_ERR_SHAPE, "nnr != NNR (ApplyHam_block.cpp:18-21)");
   PSPW_CUDA(cudaSetDevice(c->device));
   double *tmp = nullptr;
-  int rc = ws_reserve(c, 11, (size_t)nnr * sizeof(double), (void **)&tmp);
+  int rc = ws_reserve(c, kWsVeffTmp, (size_t)nnr * sizeof(double), (void **)&tmp);
   if (rc) return rc;
   PSPW_CUDA(cudaMemcpyAsync(tmp, veff, (size_t)nnr * sizeof(double), cudaMemcpyHostToDevice,
                             c->stream));

@@ -4,7 +4,9 @@
 // the same g++ mangled names, common_pspw.h:176-222 and 252-259), reading
 // the reference program's globals (common_pspw.h:43-148) as that code does,
 // and forwards to the C ABI in include/pspw_gpu.h.  A program links this
-// library in place of ApplyHam_block.o, ApplyHam.o and chebyfilt.o.
+// library in place of ApplyHam_block.o, ApplyHam.o, chebyfilt.o,
+// davidson_cpu.o, lobpcg_cpu.o, ortho_qr.o, eig_zheevd.o, eig_zhegv.o,
+// GenPrec.o, EvalRhoPsi.o, lanczos.o and Diagon_cpu.o.
 //
 // Device state: one pspw_cell per k-point, built from N123/XKG/EIGR/PKG_A/
 // WNL on first use (or by SetupArrays_ApplyHam_cuda) and reused while those
@@ -48,6 +50,15 @@ extern unsigned int *N123;
 extern zcomplex *EIGR;
 extern double *PKG_A;
 extern double *WNL;
+extern int NEMPTY;
+extern bool USER_MAX_DIAG_ITER;
+extern int MAX_DIAG_ITER;
+extern bool DIAG_VERBOSE;
+extern zcomplex *C0;
+extern double *FOCC;
+extern double *WKPT;
+extern double OMEGA;
+extern double EKIN;
 
 #define DROPIN_API __attribute__((visibility("default")))
 
@@ -210,3 +221,174 @@ DROPIN_API int ApplyHam_block_cuda(zcomplex *d_vin, zcomplex *d_vout, int NGW_ik
 DROPIN_API void FreeArrays_ApplyHam_cuda() { ShutdownCUDA(); }
 
 DROPIN_API void FreeRho_ApplyHam_cuda() {}
+
+// ------------------------------------------------------------ solvers
+
+namespace {
+
+double *dp(zcomplex *z) { return reinterpret_cast<double *>(z); }
+
+int solver_max_iter() { return USER_MAX_DIAG_ITER ? MAX_DIAG_ITER : 0; }
+
+}  // namespace
+
+// ortho_qr.cpp:3
+DROPIN_API void ortho_qr(zcomplex *X, int nbasis, int nstates) {
+  int rc = pspw_ortho_qr(cell_for(1), dp(X), nbasis, nstates);
+  if (rc == PSPW_ERR_LAPACK) {  // ortho_qr.cpp:20-29 prints and returns
+    std::printf("ERROR calling zgeqrf_ : %s\n", pspw_last_error());
+    return;
+  }
+  if (rc) die("ortho_qr", rc);
+}
+
+// eig_zheevd.cpp:5
+DROPIN_API void eig_zheevd(zcomplex *A, int ldA, double *lambda, int N) {
+  int rc = pspw_eig_zheevd(cell_for(1), dp(A), ldA, lambda, N);
+  if (rc == PSPW_ERR_LAPACK) {  // eig_zheevd.cpp:26-29 prints and returns
+    std::printf("ERROR calling zheevd_ : %s\n", pspw_last_error());
+    return;
+  }
+  if (rc) die("eig_zheevd", rc);
+}
+
+// eig_zhegv.cpp:5
+DROPIN_API void eig_zhegv(zcomplex *A, int ldA, zcomplex *B, int ldB, zcomplex *evec, int ldE,
+                          int N) {
+  int rc = pspw_eig_zhegv(cell_for(1), dp(A), ldA, dp(B), ldB, dp(evec), ldE, N);
+  if (rc == PSPW_ERR_LAPACK) {
+    std::printf("ERROR calling zheevd in eig_zhegv : %s\n", pspw_last_error());
+    return;
+  }
+  if (rc) die("eig_zhegv", rc);
+}
+
+// eig_zhegv.cpp:86
+DROPIN_API void eig_zhegv_eval(zcomplex *A, int ldA, zcomplex *B, int ldB, double *eval,
+                               zcomplex *evec, int ldE, int N) {
+  int rc = pspw_eig_zhegv_eval(cell_for(1), dp(A), ldA, dp(B), ldB, eval, dp(evec), ldE, N);
+  if (rc == PSPW_ERR_LAPACK) {
+    std::printf("ERROR calling zheevd in eig_zhegv : %s\n", pspw_last_error());
+    return;
+  }
+  if (rc) die("eig_zhegv_eval", rc);
+}
+
+// GenPrec.cpp:5
+DROPIN_API void GenPrec(int ik, double *prec, int nbasis, double tau) {
+  int rc = pspw_gen_prec(cell_for(ik), prec, nbasis, tau);
+  if (rc) die("GenPrec", rc);
+}
+
+// lobpcg_cpu.cpp:15-27 (ChebySCFLoop.cpp uses it on host matrices)
+DROPIN_API void symmetrize(zcomplex *v, int ldv, int nrow, int ncol) {
+  (void)nrow;
+  for (int j = 0; j < ncol; j++)
+    for (int i = 0; i <= j; i++) {
+      double *a = dp(v + (size_t)j * ldv + i), *b = dp(v + (size_t)i * ldv + j);
+      const double tr = 0.5 * (a[0] + b[0]), ti = 0.5 * (a[1] - b[1]);
+      a[0] = tr;
+      a[1] = ti;
+      b[0] = tr;
+      b[1] = -ti;
+    }
+}
+
+static void print_solver_table(const char *title, int nstates, const double *ev, const double *res) {
+  std::printf("%s\n", title);
+  for (int i = 0; i < nstates; i++) std::printf("%d %18.10f %18.10f\n", i + 1, ev[i], res[i]);
+}
+
+// davidson_cpu.cpp:9
+DROPIN_API void davidson_cpu(int ik, double *evals, zcomplex *X, int nbasis, int nstates,
+                             double *rhoe, int nnr, double *prec) {
+  check_nnr(nnr);
+  pspw_cell *c = cell_for(ik);
+  int rc = pspw_cell_set_veff(c, rhoe, nnr);
+  if (rc) die("davidson_cpu", rc);
+  std::vector<double> res(nstates);
+  int iters = 0;
+  rc = pspw_davidson(c, evals, dp(X), nbasis, nstates, prec, NEMPTY, solver_max_iter(),
+                     PSPW_PREC_F64, res.data(), &iters);
+  if (rc) die("davidson_cpu", rc);
+  print_solver_table("Final Davidson result (GPU engine):", nstates, evals, res.data());
+}
+
+// lobpcg_cpu.cpp:31
+DROPIN_API void lobpcg_cpu(int ik, double *lambda, zcomplex *X, int nbasis, int nstates,
+                           double *rhoe, int nnr, double *prec) {
+  check_nnr(nnr);
+  pspw_cell *c = cell_for(ik);
+  int rc = pspw_cell_set_veff(c, rhoe, nnr);
+  if (rc) die("lobpcg_cpu", rc);
+  std::vector<double> res(nstates);
+  int iters = 0;
+  rc = pspw_lobpcg(c, lambda, dp(X), nbasis, nstates, prec, NEMPTY, solver_max_iter(),
+                   PSPW_PREC_F64, res.data(), &iters);
+  if (rc == PSPW_ERR_LAPACK) {  // lobpcg_cpu.cpp:163-166 aborts on a failed Cholesky
+    std::printf("%s\n", pspw_last_error());
+    std::abort();
+  }
+  if (rc) die("lobpcg_cpu", rc);
+  print_solver_table("Final LOBPCG result (GPU engine)", nstates, lambda, res.data());
+}
+
+// Diagon_cpu.cpp:5-57: preconditioner, solver on NGW_ik x NX, then the
+// NGWX-padded copy with zero tails
+static void diagon(bool lobpcg, int ik, double *eigval, zcomplex *eigvec, int NGW_ik, double *rhoe,
+                   int nnr, double tau) {
+  std::vector<zcomplex> tmp((size_t)NGW_ik * NX);
+  std::vector<double> prec(NGW_ik);
+  GenPrec(ik, prec.data(), NGW_ik, tau);
+  if (lobpcg)
+    lobpcg_cpu(ik, eigval, tmp.data(), NGW_ik, NX, rhoe, nnr, prec.data());
+  else
+    davidson_cpu(ik, eigval, tmp.data(), NGW_ik, NX, rhoe, nnr, prec.data());
+  for (int ist = 0; ist < NX; ist++) {
+    zcomplex *dst = eigvec + (size_t)ist * NGWX;
+    std::memcpy(dst, tmp.data() + (size_t)ist * NGW_ik, sizeof(zcomplex) * NGW_ik);
+    std::memset(dst + NGW_ik, 0, sizeof(zcomplex) * (NGWX - NGW_ik));
+  }
+}
+
+DROPIN_API void Diagon_lobpcg_cpu(int ik, double *eigval, zcomplex *eigvec, int NGW_ik,
+                                  double *rhoe, int nnr, double tau) {
+  diagon(true, ik, eigval, eigvec, NGW_ik, rhoe, nnr, tau);
+}
+
+DROPIN_API void Diagon_davidson_cpu(int ik, double *eigval, zcomplex *eigvec, int NGW_ik,
+                                    double *rhoe, int nnr, double tau) {
+  diagon(false, ik, eigval, eigvec, NGW_ik, rhoe, nnr, tau);
+}
+
+// lanczos.cpp:8
+DROPIN_API void lanczos(int ik, zcomplex *v0, int k, double *T, int ldT, zcomplex *f, double *rhoe,
+                        int nnr) {
+  check_nnr(nnr);
+  pspw_cell *c = cell_for(ik);
+  int rc = pspw_cell_set_veff(c, rhoe, nnr);
+  if (rc) die("lanczos", rc);
+  rc = pspw_lanczos(c, dp(v0), NGW[ik - 1], k, T, ldT, dp(f));
+  if (rc) die("lanczos", rc);
+}
+
+// EvalRhoPsi.cpp:83: C0(:,ist,ik) copies NGWX entries of column ist (with
+// leading dimension ldEigvec, reading into the next column when it is
+// shorter, as the reference does), then the density and EKIN on the device.
+DROPIN_API void EvalRhoPsi(int ik, double *rhoe, zcomplex *eigvec, int ldEigvec, int NGW_ik) {
+  for (int ist = 0; ist < NX; ist++)
+    std::memcpy(C0 + ((size_t)(ik - 1) * NX + ist) * NGWX, eigvec + (size_t)ist * ldEigvec,
+                sizeof(zcomplex) * NGWX);
+  int rc = pspw_eval_rho_psi(cell_for(ik), rhoe, dp(eigvec), ldEigvec, NGW_ik, NX,
+                             FOCC + (size_t)(ik - 1) * NX, WKPT[ik - 1], OMEGA, &EKIN);
+  if (rc == PSPW_ERR_CHARGE) {  // EvalRhoPsi.cpp:129-133
+    std::printf("%s\n", pspw_last_error());
+    std::abort();
+  }
+  if (rc) die("EvalRhoPsi", rc);
+}
+
+// EvalRhoPsi.cpp:5 (eigvec with leading dimension NGWX)
+DROPIN_API void EvalRhoPsi(int ik, double *rhoe, zcomplex *eigvec, int NGW_ik) {
+  EvalRhoPsi(ik, rhoe, eigvec, NGWX, NGW_ik);
+}

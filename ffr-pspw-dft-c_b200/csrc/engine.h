@@ -43,7 +43,15 @@ struct Basis {
   int *d_xa_of_x = nullptr;    // [n1] active index or -1
   double *d_kin64 = nullptr;   // [ngw] 0.5*XKG*TPIBA2
   float *d_kin32 = nullptr;
+  double *d_xkg64 = nullptr;   // [ngw] XKG (the preconditioner and EKIN read it)
   FftDim dim[3];
+  // register-FFT path (every length has a two-factor split): stick
+  // coordinates, and per axis the natural index held at each position of
+  // the digit-permuted order
+  bool fast = false;
+  int *d_col_x = nullptr;  // [ncol]
+  int *d_col_y = nullptr;  // [ncol]
+  int *d_pinv[3] = {nullptr, nullptr, nullptr};
 };
 
 // KB projectors beta_p(G) = EIGR(G, atom_p) * PKG_A(lm_p, G, species_p).
@@ -72,7 +80,30 @@ enum Family {
   kFamSticksFwd = 7,
   kFamProj = 8,
   kFamBackproj = 9,
-  kNumFamilies = 10
+  kFamGemm = 10,     // subspace GEMMs of the solvers
+  kNumFamilies = 11
+};
+
+// Workspace slots of a cell (grown on demand, kept until the cell is freed).
+enum WsSlot {
+  kWsSticks = 0,   // FFT stick buffer
+  kWsPlanes = 1,   // FFT plane buffer (generic path)
+  kWsProjPart = 2, // projector partial sums
+  kWsProj = 3,     // projections W beta^H psi
+  kWsHostIn = 4,   // host-facing calls: input block
+  kWsHostOut = 5,  // host-facing calls: output block
+  kWsFilt1 = 6,    // Chebyshev filter blocks
+  kWsFilt2 = 7,
+  kWsConv = 8,     // FP32 copy of a host block
+  kWsGemmPart = 9, // split-K partial sums of the subspace GEMMs
+  kWsRhoPart = 10, // density: per-group partial planes
+  kWsVeffTmp = 11, // V_eff staging
+  kWsSolver = 12,  // cuSOLVER work
+  kWsInfo = 13,    // cuSOLVER info
+  kWsTau = 14,     // Householder scalars
+  kWsEval = 15,    // eigenvalues of the overlap in eig_zhegv
+  kWsSolverBase = 16,  // eigensolver blocks 16..31
+  kWsCount = 32
 };
 
 struct Timing {
@@ -94,15 +125,20 @@ struct pspw_cell {
   int device = 0;
   cudaStream_t stream = nullptr;
   int ngwx = 0;
+  double tpiba2 = 0.0;
   int band_batch = 0;
   pspw::Basis basis;
   pspw::Projectors proj;
   double *d_veff64 = nullptr;  // V_eff / NNR on the grid (forward-FFT scale folded in)
   float *d_veff32 = nullptr;
+  double *d_vperm64 = nullptr;  // the same, indexed in the register path's permuted order
+  float *d_vperm32 = nullptr;
   bool veff_set = false;
   // persistent scratch: 0 = FFT sticks, 1 = FFT planes, 2 = projector
   // partial sums, 3 = projections, 4.. = block buffers of the filter/solvers
-  pspw::Workspace ws[12];
+  pspw::Workspace ws[pspw::kWsCount];
+  void *cusolver = nullptr;  // cusolverDnHandle_t, created on first use
+  void *cublas = nullptr;    // cublasHandle_t, created on first use
   pspw::Timing timing;
   long long kernel_launches = 0;  // kernels this cell has enqueued
 };

@@ -1,0 +1,31 @@
+// The register-FFT local part of H*psi (fftpath.cuh), compiled per
+// precision in fftpath_f32.cu / fftpath_f64.cu.
+#pragma once
+
+#include "common.cuh"
+#include "engine.h"
+
+namespace pspw {
+
+// What the stick/plane kernels read about the basis (device pointers).
+struct FastGeo {
+  int ncol, nxa;
+  const int *col_start, *sg_ig, *sg_z, *sg_col, *xa_list, *col_x, *col_y;
+};
+
+// True when (n1, n2, n3) has compiled stick and plane kernels.
+bool fast_supported(int n1, int n2, int n3);
+
+// Local part (kinetic + V_eff sandwich) of H*psi for nb bands:
+// out = kin*in + FFT^-1 sandwich, on the cell stream.
+template <typename R>
+int local_fast(pspw_cell *c, const FastGeo &g, const cx<R> *in, int ld_in, cx<R> *out,
+               int ld_out, int ngw, int nb, const ScratchPlan *plan);
+
+// rho (device, natural grid order) += sum_b wband[b] |psi_b(r)|^2, with the
+// scatter limited to G index < ngw_scatter.
+template <typename R>
+int rho_fast(pspw_cell *c, const FastGeo &g, const cx<R> *psi, int ld, int ngw_scatter, int nb,
+             const double *d_wband, double *d_rho);
+
+}  // namespace pspw

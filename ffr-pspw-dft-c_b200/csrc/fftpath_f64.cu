@@ -1,0 +1,12 @@
+// Register-FFT local part of H*psi, FP64 (complex128) instantiation.
+#include "fftpath.cuh"
+
+namespace pspw {
+
+template int local_fast<double>(pspw_cell *, const FastGeo &, const double2 *, int, double2 *,
+                                int, int, int, const ScratchPlan *);
+
+template int rho_fast<double>(pspw_cell *, const FastGeo &, const double2 *, int, int, int,
+                            const double *, double *);
+
+}  // namespace pspw

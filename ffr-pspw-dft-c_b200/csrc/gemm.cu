@@ -1,0 +1,169 @@
+// Complex GEMM for the subspace steps of the eigensolvers (zgemm_ calls of
+// davidson_cpu.cpp, lobpcg_cpu.cpp, eig_zhegv.cpp, ChebySCFLoop.cpp):
+//   C = alpha * op(A) * B + beta * C,  op(A) = A or A^H,
+// column-major with leading dimensions, FP64 or FP32 complex.
+//
+// Tiles of 64 x 64 outputs, 256 threads, 4 x 4 outputs per thread, the K loop
+// staged through shared memory.  When K is long and the output small (the
+// Gram matrices X^H Y over NGW plane waves) K is split across blocks; the
+// slices are reduced in a fixed order, so results do not depend on timing.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+
+#include "common.cuh"
+#include "engine.h"
+#include "gemm.h"
+
+namespace pspw {
+namespace {
+
+constexpr int kGM = 64, kGN = 64;
+
+template <typename T>
+__device__ __forceinline__ T cj(T a) {
+  return mk<T>(a.x, -a.y);
+}
+
+// part = op(A)[m0:, k-slice] * B[k-slice, n0:]  (alpha/beta applied later
+// unless nsplit == 1)
+template <typename R, int BK, bool CONJ_A>
+__global__ void __launch_bounds__(256) k_zgemm(int m, int n, int k, cx<R> alpha,
+                                               const cx<R> *__restrict__ A, int lda,
+                                               const cx<R> *__restrict__ B, int ldb, cx<R> beta,
+                                               cx<R> *C, int ldc, int kchunk,
+                                               cx<R> *__restrict__ part) {
+  using T = cx<R>;
+  __shared__ T As[BK][kGM + 1];
+  __shared__ T Bs[BK][kGN + 1];
+  const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
+  const int m0 = blockIdx.x * kGM, n0 = blockIdx.y * kGN;
+  const int kb = blockIdx.z * kchunk;
+  const int ke = min(k, kb + kchunk);
+  T acc[4][4];
+#pragma unroll
+  for (int i = 0; i < 4; i++)
+#pragma unroll
+    for (int j = 0; j < 4; j++) acc[i][j] = czero<T>();
+  for (int k0 = kb; k0 < ke; k0 += BK) {
+    if (CONJ_A) {
+      // A^H: element (mm, kk) is conj(A[kk + mm*lda]); contiguous in kk
+      for (int e = threadIdx.x; e < BK * kGM; e += 256) {
+        const int kk = e % BK, mm = e / BK;
+        const int gk = k0 + kk, gm = m0 + mm;
+        As[kk][mm] = (gk < ke && gm < m) ? cj(A[(size_t)gm * lda + gk]) : czero<T>();
+      }
+    } else {
+      // A: element (mm, kk) is A[mm + kk*lda]; contiguous in mm
+      for (int e = threadIdx.x; e < BK * kGM; e += 256) {
+        const int mm = e % kGM, kk = e / kGM;
+        const int gk = k0 + kk, gm = m0 + mm;
+        As[kk][mm] = (gk < ke && gm < m) ? A[(size_t)gk * lda + gm] : czero<T>();
+      }
+    }
+    for (int e = threadIdx.x; e < BK * kGN; e += 256) {
+      const int kk = e % BK, nn = e / BK;
+      const int gk = k0 + kk, gn = n0 + nn;
+      Bs[kk][nn] = (gk < ke && gn < n) ? B[(size_t)gn * ldb + gk] : czero<T>();
+    }
+    __syncthreads();
+#pragma unroll 4
+    for (int kk = 0; kk < BK; kk++) {
+      T av[4], bv[4];
+#pragma unroll
+      for (int i = 0; i < 4; i++) av[i] = As[kk][tx + 16 * i];
+#pragma unroll
+      for (int j = 0; j < 4; j++) bv[j] = Bs[kk][ty + 16 * j];
+#pragma unroll
+      for (int i = 0; i < 4; i++)
+#pragma unroll
+        for (int j = 0; j < 4; j++) cfma(acc[i][j], av[i], bv[j]);
+    }
+    __syncthreads();
+  }
+#pragma unroll
+  for (int j = 0; j < 4; j++) {
+    const int gn = n0 + ty + 16 * j;
+    if (gn >= n) continue;
+#pragma unroll
+    for (int i = 0; i < 4; i++) {
+      const int gm = m0 + tx + 16 * i;
+      if (gm >= m) continue;
+      if (part) {
+        part[((size_t)blockIdx.z * n + gn) * m + gm] = acc[i][j];
+      } else {
+        T r = cmul(alpha, acc[i][j]);
+        if (beta.x != (R)0 || beta.y != (R)0) r = r + cmul(beta, C[(size_t)gn * ldc + gm]);
+        C[(size_t)gn * ldc + gm] = r;
+      }
+    }
+  }
+}
+
+template <typename R>
+__global__ void k_zgemm_reduce(int m, int n, int nsplit, const cx<R> *__restrict__ part,
+                               cx<R> alpha, cx<R> beta, cx<R> *C, int ldc) {
+  using T = cx<R>;
+  const size_t tot = (size_t)m * n;
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < tot;
+       i += (size_t)gridDim.x * blockDim.x) {
+    T s = part[i];
+    for (int p = 1; p < nsplit; p++) s = s + part[(size_t)p * tot + i];
+    const int gn = (int)(i / m), gm = (int)(i - (size_t)gn * m);
+    T r = cmul(alpha, s);
+    if (beta.x != (R)0 || beta.y != (R)0) r = r + cmul(beta, C[(size_t)gn * ldc + gm]);
+    C[(size_t)gn * ldc + gm] = r;
+  }
+}
+
+}  // namespace
+
+template <typename R>
+int zgemm(pspw_cell *c, char opa, int m, int n, int k, cx<R> alpha, const cx<R> *A, int lda,
+          const cx<R> *B, int ldb, cx<R> beta, cx<R> *C, int ldc) {
+  using T = cx<R>;
+  if (m <= 0 || n <= 0) return PSPW_OK;
+  cudaStream_t st = c->stream;
+  constexpr int BK = sizeof(R) == 8 ? 16 : 32;
+  const bool conj = (opa == 'C' || opa == 'c');
+  const int mt = (m + kGM - 1) / kGM, nt = (n + kGN - 1) / kGN;
+  int nsplit = 1;
+  if (k > 4 * BK && mt * nt < 2 * 148) {
+    nsplit = std::min((k + 255) / 256, (2 * 148 + mt * nt - 1) / (mt * nt));
+    nsplit = std::max(1, nsplit);
+  }
+  int kchunk = (k + nsplit - 1) / nsplit;
+  kchunk = (kchunk + BK - 1) / BK * BK;
+  if (k <= 0) kchunk = BK;
+  nsplit = std::max(1, (k + kchunk - 1) / kchunk);
+  T *part = nullptr;
+  if (nsplit > 1) {
+    int rc = ws_reserve(c, 9, sizeof(T) * (size_t)nsplit * m * n, (void **)&part);
+    if (rc) return rc;
+  }
+  dim3 grid(mt, nt, nsplit);
+  cudaEvent_t ev;
+  timing_begin(c, kFamGemm, &ev);
+  if (conj)
+    k_zgemm<R, BK, true><<<grid, 256, 0, st>>>(m, n, k, alpha, A, lda, B, ldb, beta, C, ldc,
+                                               kchunk, part);
+  else
+    k_zgemm<R, BK, false><<<grid, 256, 0, st>>>(m, n, k, alpha, A, lda, B, ldb, beta, C, ldc,
+                                                kchunk, part);
+  c->kernel_launches++;
+  if (nsplit > 1) {
+    k_zgemm_reduce<R><<<std::min<size_t>(4 * 148, ((size_t)m * n + 255) / 256), 256, 0, st>>>(
+        m, n, nsplit, part, alpha, beta, C, ldc);
+    c->kernel_launches++;
+  }
+  timing_end(c, kFamGemm, ev);
+  PSPW_CUDA(cudaGetLastError());
+  return PSPW_OK;
+}
+
+template int zgemm<double>(pspw_cell *, char, int, int, int, double2, const double2 *, int,
+                           const double2 *, int, double2, double2 *, int);
+template int zgemm<float>(pspw_cell *, char, int, int, int, float2, const float2 *, int,
+                          const float2 *, int, float2, float2 *, int);
+
+}  // namespace pspw

@@ -34,6 +34,7 @@
 #include "common.cuh"
 #include "engine.h"
 #include "fft.cuh"
+#include "fftpath.h"
 
 namespace pspw {
 
@@ -412,6 +413,7 @@ template <typename R>
 struct Prec;
 template <>
 struct Prec<double> {
+  static const double *vperm(const pspw_cell *c) { return c->d_vperm64; }
   static const double *veff(const pspw_cell *c) { return c->d_veff64; }
   static const double *kin(const pspw_cell *c) { return c->basis.d_kin64; }
   static const void *eigr(const pspw_cell *c) { return c->proj.d_eigr64; }
@@ -420,6 +422,7 @@ struct Prec<double> {
 };
 template <>
 struct Prec<float> {
+  static const float *vperm(const pspw_cell *c) { return c->d_vperm32; }
   static const float *veff(const pspw_cell *c) { return c->d_veff32; }
   static const float *kin(const pspw_cell *c) { return c->basis.d_kin32; }
   static const void *eigr(const pspw_cell *c) { return c->proj.d_eigr32; }
@@ -516,6 +519,12 @@ int hpsi_apply(pspw_cell *c, const void *in_v, int ld_in, void *out_v, int ld_ou
   // ---- local part, in batches of bands
   Geo geo{B.n1, B.n2, B.n3, B.ncol, B.nxa, B.ngw, B.d_col_start, B.d_sg_ig, B.d_sg_z,
           B.d_sg_col, B.d_col_of_xy, B.d_xa_list, B.d_xa_of_x};
+  if (B.fast) {
+    const FastGeo fg{B.ncol, B.nxa, B.d_col_start, B.d_sg_ig, B.d_sg_z, B.d_sg_col, B.d_xa_list,
+                     B.d_col_x, B.d_col_y};
+    int rc = local_fast<R>(c, fg, in, ld_in, out, ld_out, ngw, nb, plan);
+    if (rc) return rc;
+  } else {
   const size_t s_band = (size_t)B.n3 * B.ncol, p_band = (size_t)B.n3 * B.n2 * B.nxa;
   int nbatch = c->band_batch;
   if (nbatch <= 0) {
@@ -571,6 +580,7 @@ int hpsi_apply(pspw_cell *c, const void *in_v, int ld_in, void *out_v, int ld_ou
     });
   }
   timing_end(c, kFamLocal, ev);
+  }
   PSPW_CUDA(cudaGetLastError());
 
   // ---- back-projection + recurrence epilogue

@@ -1,0 +1,20 @@
+// Device eigensolvers (solvers.cu) and the density kernel (rho.cu).
+#pragma once
+
+#include "common.cuh"
+#include "engine.h"
+
+namespace pspw {
+
+void random_col_host(double2 *A, int nelem, long seed);
+int gen_prec_dev(pspw_cell *c, double *d_prec, int nbasis, double tau);
+// X: device FP64 block nbasis x nstates (ld nbasis), overwritten with the
+// solver's random start and then the eigenvectors.
+int davidson_dev(pspw_cell *c, int hprec, double *evals_host, double2 *X, int nbasis, int nstates,
+                 const double *d_prec, int nempty, int max_iter, double *res_host, int *iters);
+int lobpcg_dev(pspw_cell *c, int hprec, double *lambda_host, double2 *X, int nbasis, int nstates,
+               const double *d_prec, int nempty, int max_iter, double *res_host, int *iters);
+// v0: device, normalised in place; T_host k x k (ldT); f_out device or null
+int lanczos_dev(pspw_cell *c, double2 *v0, int ngw, int k, double *T_host, int ldT, double2 *f_out);
+
+}  // namespace pspw

@@ -1,6 +1,6 @@
 """Host-side Python interface of the B200 Hamiltonian engine (ctypes over the
 C ABI of libpspw_gpu.so; see include/pspw_gpu.h)."""
 from ._lib import PREC_F32, PREC_F64, PspwError, check, lib
-from .cell import Cell, basis_gamma
+from .cell import Cell, basis_gamma, random_col
 
-__all__ = ["Cell", "basis_gamma", "PREC_F32", "PREC_F64", "PspwError", "check", "lib"]
+__all__ = ["Cell", "basis_gamma", "random_col", "PREC_F32", "PREC_F64", "PspwError", "check", "lib"]

@@ -66,6 +66,16 @@ SIGNATURES = {
     "pspw_timing_read": [_vp, _i, _vp, _vp],
     "pspw_timing_reset": [_vp],
     "pspw_kernel_launches": [_vp, _vp],
+    "pspw_random_col": [_vp, _i, C.c_long],
+    "pspw_gen_prec": [_vp, _vp, _i, _d],
+    "pspw_ortho_qr": [_vp, _vp, _i, _i],
+    "pspw_eig_zheevd": [_vp, _vp, _i, _vp, _i],
+    "pspw_eig_zhegv": [_vp, _vp, _i, _vp, _i, _vp, _i, _i],
+    "pspw_eig_zhegv_eval": [_vp, _vp, _i, _vp, _i, _vp, _vp, _i, _i],
+    "pspw_davidson": [_vp, _vp, _vp, _i, _i, _vp, _i, _i, _i, _vp, _vp],
+    "pspw_lobpcg": [_vp, _vp, _vp, _i, _i, _vp, _i, _i, _i, _vp, _vp],
+    "pspw_lanczos": [_vp, _vp, _i, _i, _vp, _i, _vp],
+    "pspw_eval_rho_psi": [_vp, _vp, _vp, _i, _i, _i, _vp, _d, _d, _vp],
 }
 _RESTYPE = {"pspw_error_string": C.c_char_p, "pspw_last_error": C.c_char_p}
 

@@ -146,6 +146,69 @@ class Cell:
         check(lib().pspw_chebyfilt_dev(self._h, int(prec), ptr(d_x), int(ld), int(ngw), int(nb),
                                        int(degree), float(lb), float(ub)))
 
+    # ---- solvers and dense steps (host buffers; reference semantics)
+    def gen_prec(self, nbasis, tau):
+        p = np.zeros(nbasis)
+        check(lib().pspw_gen_prec(self._h, p.ctypes.data, int(nbasis), float(tau)))
+        return p
+
+    def ortho_qr(self, X):
+        X = np.array(_f(X, np.complex128), order="F", copy=True)
+        check(lib().pspw_ortho_qr(self._h, X.ctypes.data, X.shape[0], X.shape[1]))
+        return X
+
+    def eig_zheevd(self, A):
+        A = np.array(_f(A, np.complex128), order="F", copy=True)
+        n = A.shape[0]
+        w = np.zeros(n)
+        check(lib().pspw_eig_zheevd(self._h, A.ctypes.data, n, w.ctypes.data, n))
+        return w, A
+
+    def eig_zhegv_eval(self, A, B):
+        A = np.array(_f(A, np.complex128), order="F", copy=True)
+        B = np.array(_f(B, np.complex128), order="F", copy=True)
+        n = A.shape[0]
+        w = np.zeros(n)
+        E = np.zeros((n, n), dtype=np.complex128, order="F")
+        check(lib().pspw_eig_zhegv_eval(self._h, A.ctypes.data, n, B.ctypes.data, n, w.ctypes.data,
+                                        E.ctypes.data, n, n))
+        return w, E
+
+    def _solver(self, name, nbasis, nstates, prec, nempty, max_iter, hprec):
+        X = np.zeros((nbasis, nstates), dtype=np.complex128, order="F")
+        ev = np.zeros(nstates)
+        res = np.zeros(nstates)
+        it = C.c_int()
+        p = np.ascontiguousarray(np.asarray(prec, dtype=float)[:nbasis])
+        check(getattr(lib(), name)(self._h, ev.ctypes.data, X.ctypes.data, int(nbasis),
+                                   int(nstates), p.ctypes.data, int(nempty), int(max_iter or 0),
+                                   int(hprec), res.ctypes.data, C.byref(it)))
+        return ev, X, res, it.value
+
+    def davidson(self, nbasis, nstates, prec, nempty, max_iter=None, hprec=PREC_F64):
+        return self._solver("pspw_davidson", nbasis, nstates, prec, nempty, max_iter, hprec)
+
+    def lobpcg(self, nbasis, nstates, prec, nempty, max_iter=None, hprec=PREC_F64):
+        return self._solver("pspw_lobpcg", nbasis, nstates, prec, nempty, max_iter, hprec)
+
+    def lanczos(self, v0, k):
+        v = np.array(np.asarray(v0, dtype=np.complex128), copy=True)
+        T = np.zeros((k, k), order="F")
+        f = np.zeros_like(v)
+        check(lib().pspw_lanczos(self._h, v.ctypes.data, v.size, int(k), T.ctypes.data, int(k),
+                                 f.ctypes.data))
+        return T, f, v
+
+    def eval_rho_psi(self, rhoe, eigvec_flat, ld, ngw, nx, focc, wkpt, omega, ekin=0.0):
+        rho = np.array(np.asarray(rhoe, dtype=float), copy=True)
+        ev = np.ascontiguousarray(np.asarray(eigvec_flat, dtype=np.complex128))
+        fo = np.ascontiguousarray(np.asarray(focc, dtype=float))
+        ek = C.c_double(ekin)
+        check(lib().pspw_eval_rho_psi(self._h, rho.ctypes.data, ev.ctypes.data, int(ld), int(ngw),
+                                      int(nx), fo.ctypes.data, float(wkpt), float(omega),
+                                      C.byref(ek)))
+        return rho, ek.value
+
     # ---- timing
     def timing_enable(self, mask):
         check(lib().pspw_timing_enable(self._h, int(mask)))
@@ -165,4 +228,11 @@ class Cell:
         return n.value
 
 
-__all__ = ["Cell", "basis_gamma", "PREC_F32", "PREC_F64"]
+def random_col(nelem, seed):
+    """util_random_cpu.cpp:5-23 start vector (bit-exact)."""
+    a = np.zeros(nelem, dtype=np.complex128)
+    check(lib().pspw_random_col(a.ctypes.data, int(nelem), int(seed)))
+    return a
+
+
+__all__ = ["Cell", "basis_gamma", "random_col", "PREC_F32", "PREC_F64"]

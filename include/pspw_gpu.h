@@ -143,6 +143,45 @@ int pspw_chebyfilt(pspw_cell *cell, double *X, int ngw, int nstates, int degree,
 int pspw_chebyfilt_dev(pspw_cell *cell, int prec, void *d_X, int ld, int ngw, int nstates,
                        int degree, double lb, double ub);
 
+/* ------------------------------------------------------------------ solvers
+ * Host-buffer entry points with the reference routines' semantics; all
+ * arithmetic on the device.  `prec`/`hprec` arrays are host.
+ *
+ * random_col      util_random_cpu.cpp:5   (host, bit-exact LCG start vectors)
+ * gen_prec        GenPrec.cpp:5           prec[nbasis] from XKG, tau
+ * ortho_qr        ortho_qr.cpp:3          X (nbasis x nstates) <- Q of its QR
+ * eig_zheevd      eig_zheevd.cpp:5        A <- eigenvectors, lambda <- eigenvalues
+ * eig_zhegv(_eval) eig_zhegv.cpp:5,86     generalised problem via B^-1/2
+ * davidson        davidson_cpu.cpp:9      block Davidson, 2nb subspace
+ * lobpcg          lobpcg_cpu.cpp:31       LOBPCG with Cholesky-orthonormalised W, P
+ * lanczos         lanczos.cpp:8           k-step Lanczos: T (k x k), residual f
+ * eval_rho_psi    EvalRhoPsi.cpp:83       rhoe += sum_i w f_i |psi_i(r)|^2 / Omega
+ *
+ * davidson/lobpcg overwrite X with their random start and return the
+ * eigenvectors there; nempty = NEMPTY; max_iter <= 0 selects the reference
+ * default max(30, nstates/2); hprec is the arithmetic of H*psi inside the
+ * solver (the rest is FP64); resnrm[nstates] and iters may be NULL.
+ * eval_rho_psi: eigvec columns with leading dimension ld, the last plane
+ * wave of each band is left out as in the reference, *ekin += EKIN part;
+ * returns PSPW_ERR_CHARGE when a band's norm is off by more than 6e-3. */
+int pspw_random_col(double *A, int nelem, long seed);
+int pspw_gen_prec(pspw_cell *cell, double *prec, int nbasis, double tau);
+int pspw_ortho_qr(pspw_cell *cell, double *X, int nbasis, int nstates);
+int pspw_eig_zheevd(pspw_cell *cell, double *A, int lda, double *lambda, int n);
+int pspw_eig_zhegv(pspw_cell *cell, double *A, int lda, double *B, int ldb, double *evec, int lde,
+                   int n);
+int pspw_eig_zhegv_eval(pspw_cell *cell, double *A, int lda, double *B, int ldb, double *eval,
+                        double *evec, int lde, int n);
+int pspw_davidson(pspw_cell *cell, double *evals, double *X, int nbasis, int nstates,
+                  const double *prec, int nempty, int max_iter, int hprec, double *resnrm,
+                  int *iters);
+int pspw_lobpcg(pspw_cell *cell, double *lambda, double *X, int nbasis, int nstates,
+                const double *prec, int nempty, int max_iter, int hprec, double *resnrm,
+                int *iters);
+int pspw_lanczos(pspw_cell *cell, double *v0, int ngw, int k, double *T, int ldT, double *f);
+int pspw_eval_rho_psi(pspw_cell *cell, double *rhoe, const double *eigvec, int ld, int ngw,
+                      int nx, const double *focc, double wkpt, double omega, double *ekin);
+
 /* ------------------------------------------------------------------ timing
  * Optional device timing on the cell stream: CUDA events around each launch
  * of the enabled families, summed until reset.  Families (bit i of the mask):

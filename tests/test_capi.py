@@ -52,6 +52,19 @@ DROPIN_SYMBOLS = [
     "_Z25SetupArrays_ApplyHam_cudaPjPdPCdS0_",  # SetupArrays_...   common_pspw.h:255
     "_Z21CopyRho_ApplyHam_cudaPd",          # CopyRho_ApplyHam_cuda common_pspw.h:257
     "_Z9SetupCUDAv", "_Z12ShutdownCUDAv",   # common_pspw.h:252-253
+    "_Z12davidson_cpuiPdPCdiiS_iS_",        # davidson_cpu          common_pspw.h:198
+    "_Z10lobpcg_cpuiPdPCdiiS_iS_",          # lobpcg_cpu            common_pspw.h:193
+    "_Z8ortho_qrPCdii",                     # ortho_qr              common_pspw.h:222
+    "_Z10eig_zheevdPCdiPdi",                # eig_zheevd            common_pspw.h:217
+    "_Z14eig_zhegv_evalPCdiS0_iPdS0_ii",    # eig_zhegv_eval        common_pspw.h:220
+    "_Z9eig_zhegvPCdiS0_iS0_ii",            # eig_zhegv             common_pspw.h:218
+    "_Z7GenPreciPdid",                      # GenPrec               common_pspw.h:182
+    "_Z10EvalRhoPsiiPdPCdii",               # EvalRhoPsi (5 args)   common_pspw.h:180
+    "_Z10EvalRhoPsiiPdPCdi",                # EvalRhoPsi (4 args)   common_pspw.h:179
+    "_Z7lanczosiPCdiPdiS0_S1_i",            # lanczos               common_pspw.h:185
+    "_Z17Diagon_lobpcg_cpuiPdPCdiS_id",     # Diagon_lobpcg_cpu     common_pspw.h:195
+    "_Z19Diagon_davidson_cpuiPdPCdiS_id",   # Diagon_davidson_cpu   common_pspw.h:200
+    "_Z10symmetrizePCdiii",                 # symmetrize (lobpcg_cpu.cpp:15)
 ]
 
 

@@ -1,0 +1,140 @@
+"""GPU parity of the eigensolvers, dense steps, preconditioner, random start
+and density against the reference's own outputs (golden fixtures) and the
+oracle.
+
+Bars: bit-exact for the integer LCG start (random_col) and the
+preconditioner (GenPrec); 1e-12 for dense factorisations and densities;
+1e-9 for eigenvalues after equal iteration counts (iterative solvers carry
+rounding differences of the GEMM summation order forward)."""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+torch = pytest.importorskip("torch")
+if not torch.cuda.is_available():  # pragma: no cover
+    pytest.skip("needs a CUDA device", allow_module_level=True)
+
+import pspw_oracle as O  # noqa: E402
+from helpers import engine_cell_args, golden, oracle_cell, relmax  # noqa: E402
+from pspw import PREC_F32, PREC_F64, Cell, PspwError, random_col, workloads  # noqa: E402
+
+G = golden("si8_8ry")
+
+
+@pytest.fixture(scope="module")
+def gcell():
+    c = Cell.from_arrays(engine_cell_args(G))
+    c.set_veff(G["veff"])
+    return c
+
+
+def test_random_col_bit_exact():
+    assert np.array_equal(random_col(64, 100), G["random_col"])
+    assert np.array_equal(random_col(5000, 357), O.random_col(5000, 357))
+
+
+def test_gen_prec_bit_exact(gcell):
+    assert np.array_equal(gcell.gen_prec(int(G["ngw"]), -10.0), G["prec"])
+    ngw = int(G["ngw"])
+    ref = O.gen_prec(G["xkg"][:ngw], float(G["alat"]), float(G["tpiba2"]), 0.7)
+    assert np.array_equal(gcell.gen_prec(ngw, 0.7), ref)
+
+
+def test_ortho_qr_matches_householder(gcell):
+    q = gcell.ortho_qr(G["ortho_in"])
+    assert np.abs(q - G["ortho_q"]).max() < 1e-13
+
+
+def test_eig_zheevd(gcell):
+    rng = np.random.default_rng(1)
+    n = 40
+    a = rng.standard_normal((n, n)) + 1j * rng.standard_normal((n, n))
+    a = a + a.conj().T
+    w, v = gcell.eig_zheevd(a)
+    w_o, _ = O.eig_zheevd(a)
+    assert np.abs(w - w_o).max() < 1e-12 * np.abs(w_o).max()
+    assert np.abs(a @ v - v * w).max() < 1e-11
+
+
+def test_eig_zhegv_eval(gcell):
+    rng = np.random.default_rng(2)
+    n = 24
+    a = rng.standard_normal((n, n)) + 1j * rng.standard_normal((n, n))
+    a = a + a.conj().T
+    m = rng.standard_normal((n, n)) + 1j * rng.standard_normal((n, n))
+    b = m @ m.conj().T + n * np.eye(n)
+    w, e = gcell.eig_zhegv_eval(a, b)
+    w_o, _, _ = O.eig_zhegv_eval(a, b)
+    assert np.abs(w - w_o).max() < 1e-12 * np.abs(w_o).max()
+    assert np.abs(a @ e - b @ e * w).max() < 1e-10
+
+
+def test_lanczos_matches_reference_output(gcell):
+    T, f, v = gcell.lanczos(G["psi"][:, 1], 8)
+    assert np.abs(T - G["lanczos_T"]).max() < 1e-11
+    assert np.abs(f - G["lanczos_f"]).max() < 1e-9 * np.abs(G["lanczos_f"]).max() + 1e-12
+
+
+def test_eval_rho_psi_matches_reference_output(gcell):
+    ngw, ngwx = int(G["ngw"]), int(G["ngwx"])
+    flat = np.concatenate([G["psi"].reshape(-1, order="F"), np.zeros(ngwx, complex)])
+    rho, ekin = gcell.eval_rho_psi(np.zeros(int(np.prod(G["nr"]))), flat, ngw, ngw, 4, G["focc"],
+                                   1.0, float(G["omega"]))
+    assert relmax(rho, G["rho"]) < 1e-12
+    assert abs(ekin - float(G["ekin"])) < 1e-12 * abs(float(G["ekin"]))
+
+
+def test_eval_rho_psi_accumulates_and_checks_charge(gcell):
+    ngw, ngwx = int(G["ngw"]), int(G["ngwx"])
+    flat = np.concatenate([G["psi"].reshape(-1, order="F"), np.zeros(ngwx, complex)])
+    base = np.full(int(np.prod(G["nr"])), 0.25)
+    rho, _ = gcell.eval_rho_psi(base, flat, ngw, ngw, 4, G["focc"], 1.0, float(G["omega"]))
+    assert relmax(rho - base, G["rho"]) < 1e-12
+    with pytest.raises(PspwError) as e:
+        gcell.eval_rho_psi(base, 1.01 * flat, ngw, ngw, 4, G["focc"], 1.0, float(G["omega"]))
+    assert e.value.code == 8
+
+
+@pytest.fixture(scope="module")
+def si8_12ry():
+    from pspw import basis_gamma, synth
+    lat, pos = synth.si_diamond(1)
+    b = basis_gamma(lat, 12.0, None, [8], [pos])
+    pkg_a, wnl = synth.kb_form_factors(b, lat)
+    b.update(pkg_a=pkg_a, wnl=wnl, lm_end=[4])
+    veff = synth.local_potential(b["nr"], lat, pos)
+    cell = Cell.from_arrays(b)
+    cell.set_veff(veff)
+    return b, cell, veff
+
+
+def test_davidson_matches_oracle(si8_12ry):
+    b, cell, veff = si8_12ry
+    ngw = b["ngw"]
+    prec = O.gen_prec(b["xkg"][:ngw], b["alat"], b["tpiba2"], -10.0)
+    ev, X, res, it = cell.davidson(ngw, 12, prec, 4, max_iter=6)
+    ev_o, X_o, res_o = O.davidson(oracle_cell(b), ngw, 12, veff, prec, 4, max_iter=6)
+    assert np.abs(ev - ev_o).max() < 1e-9
+    assert np.abs(res - res_o).max() < 1e-7
+
+
+def test_lobpcg_matches_oracle(si8_12ry):
+    b, cell, veff = si8_12ry
+    ngw = b["ngw"]
+    prec = O.gen_prec(b["xkg"][:ngw], b["alat"], b["tpiba2"], -10.0)
+    ev, X, res, it = cell.lobpcg(ngw, 12, prec, 4, max_iter=6)
+    ev_o, X_o, res_o = O.lobpcg(oracle_cell(b), ngw, 12, veff, prec, 4, max_iter=6)
+    assert np.abs(ev - ev_o).max() < 1e-9
+    # the eigenvector block spans the same subspace
+    ov = np.linalg.svd(X_o.conj().T @ X, compute_uv=False)
+    assert ov.min() > 1 - 1e-8
+
+
+def test_lobpcg_converges_and_mixed_precision_agrees(si8_12ry):
+    b, cell, veff = si8_12ry
+    ngw = b["ngw"]
+    prec = O.gen_prec(b["xkg"][:ngw], b["alat"], b["tpiba2"], -10.0)
+    ev64, _, res64, _ = cell.lobpcg(ngw, 10, prec, 2, max_iter=60)
+    ev32, _, res32, _ = cell.lobpcg(ngw, 10, prec, 2, max_iter=60, hprec=PREC_F32)
+    assert np.sort(res64)[:8].max() < 1e-4
+    assert np.abs(ev64[:8] - ev32[:8]).max() < 1e-5
