@@ -123,7 +123,7 @@ int pspw_apply_ham_block(pspw_cell *c, const double *vin, double *vout, int ngw,
   if (rc) return rc;
   PSPW_CUDA(cudaMemcpyAsync(vout, dout, bytes, cudaMemcpyDeviceToHost, c->stream));
   PSPW_CUDA(cudaStreamSynchronize(c->stream));
-  return PSPW_OK;
+  return device_status(c);
 }
 
 int pspw_chebyfilt_dev(pspw_cell *c, int prec, void *d_X, int ld, int ngw, int nstates, int degree,
@@ -168,7 +168,7 @@ int pspw_chebyfilt(pspw_cell *c, double *X, int ngw, int nstates, int degree, do
   }
   PSPW_CUDA(cudaMemcpyAsync(X, dx, n * sizeof(double2), cudaMemcpyDeviceToHost, c->stream));
   PSPW_CUDA(cudaStreamSynchronize(c->stream));
-  return PSPW_OK;
+  return device_status(c);
 }
 
 }  // extern "C"

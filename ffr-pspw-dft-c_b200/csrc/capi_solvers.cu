@@ -40,7 +40,7 @@ int down_mat(pspw_cell *c, double *h, int ld, const double2 *d, int m, int n) {
 
 int sync(pspw_cell *c) {
   PSPW_CUDA(cudaStreamSynchronize(c->stream));
-  return PSPW_OK;
+  return device_status(c);
 }
 
 // ss[j] = sum_{i<m} |c|^2, sk[j] = sum_{i<m} xkg[i] |c|^2 (EvalRhoPsi.cpp:117-126)

@@ -15,6 +15,7 @@
 
 #include "common.cuh"
 #include "engine.h"
+#include "nl_tc.h"
 #include "fft2.cuh"
 #include "fftpath.h"
 
@@ -46,6 +47,15 @@ int ws_reserve(pspw_cell *c, int slot, size_t bytes, void **out) {
     w.bytes = want;
   }
   *out = w.ptr;
+  return PSPW_OK;
+}
+
+int device_status(pspw_cell *c) {
+  volatile int *e = c->h_err;
+  if (e && *e) {
+    *e = 0;
+    return fail(PSPW_ERR_TIMEOUT, "a tensor-core kernel gave up waiting on its pipeline barrier");
+  }
   return PSPW_OK;
 }
 
@@ -212,6 +222,7 @@ int pspw_cell_destroy(pspw_cell *c) {
   }
   for (auto &w : c->ws)
     if (w.ptr) cudaFree(w.ptr);
+  if (c->h_err) cudaFreeHost(c->h_err);
   for (auto &p : c->timing.pending) {
     cudaEventDestroy(p.second.first);
     cudaEventDestroy(p.second.second);
@@ -386,6 +397,10 @@ int pspw_cell_create(pspw_cell **out, int device, int nr1, int nr2, int nr3, int
   if (cudaMalloc(&c->d_veff64, (size_t)B.nnr * sizeof(double)) != cudaSuccess ||
       cudaMalloc(&c->d_veff32, (size_t)B.nnr * sizeof(float)) != cudaSuccess)
     return bail(fail(PSPW_ERR_OOM, "cell_create: V_eff"));
+  if (cudaHostAlloc((void **)&c->h_err, sizeof(int), cudaHostAllocMapped) != cudaSuccess ||
+      cudaHostGetDevicePointer((void **)&c->d_err, c->h_err, 0) != cudaSuccess)
+    return bail(fail(PSPW_ERR_OOM, "cell_create: error word"));
+  *c->h_err = 0;
   *out = c;
   return PSPW_OK;
 }
@@ -467,7 +482,7 @@ int pspw_cell_synchronize(pspw_cell *c) {
   if (!c) return fail(PSPW_ERR_ARG, "synchronize: null cell");
   PSPW_CUDA(cudaSetDevice(c->device));
   PSPW_CUDA(cudaStreamSynchronize(c->stream));
-  return PSPW_OK;
+  return pspw::device_status(c);
 }
 
 int pspw_cell_sizes(pspw_cell *c, int *o) {
@@ -486,6 +501,20 @@ int pspw_cell_sizes(pspw_cell *c, int *o) {
 int pspw_cell_set_band_batch(pspw_cell *c, int nbatch) {
   if (!c || nbatch < 0) return fail(PSPW_ERR_ARG, "set_band_batch: bad argument");
   c->band_batch = nbatch;
+  return PSPW_OK;
+}
+
+int pspw_cell_set_nl_path(pspw_cell *c, int path) {
+  if (!c || path < PSPW_NL_AUTO || path > PSPW_NL_TENSOR_CORE)
+    return fail(PSPW_ERR_ARG, "set_nl_path: bad argument");
+  const int keep = c->nl_path;
+  c->nl_path = PSPW_NL_AUTO;
+  if (path == PSPW_NL_TENSOR_CORE && !pspw::nl_tc_usable(c)) {
+    c->nl_path = keep;
+    return fail(PSPW_ERR_NOT_IMPL, "set_nl_path: tensor-core projector kernels need one species "
+                                   "and 1..256 atoms");
+  }
+  c->nl_path = path;
   return PSPW_OK;
 }
 

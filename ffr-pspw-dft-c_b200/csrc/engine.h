@@ -127,6 +127,7 @@ struct pspw_cell {
   int ngwx = 0;
   double tpiba2 = 0.0;
   int band_batch = 0;
+  int nl_path = 0;  // PSPW_NL_AUTO / _SIMT / _TENSOR_CORE
   pspw::Basis basis;
   pspw::Projectors proj;
   double *d_veff64 = nullptr;  // V_eff / NNR on the grid (forward-FFT scale folded in)
@@ -141,6 +142,11 @@ struct pspw_cell {
   void *cublas = nullptr;    // cublasHandle_t, created on first use
   pspw::Timing timing;
   long long kernel_launches = 0;  // kernels this cell has enqueued
+  // Error word the kernels raise when a bounded wait gives up (pinned,
+  // mapped host memory: d_err is its device alias).  Read after every
+  // stream synchronisation by device_status().
+  int *h_err = nullptr;
+  int *d_err = nullptr;
 };
 
 namespace pspw {
@@ -155,6 +161,10 @@ int cuda_fail(cudaError_t e, const char *what);
   } while (0)
 
 int ws_reserve(pspw_cell *c, int slot, size_t bytes, void **out);
+
+// After a stream synchronisation: PSPW_ERR_TIMEOUT (and the flag cleared)
+// when a kernel gave up on a bounded wait since the last check.
+int device_status(pspw_cell *c);
 
 // timing hooks (no-ops unless the family is enabled)
 void timing_begin(pspw_cell *c, int family, cudaEvent_t *ev);

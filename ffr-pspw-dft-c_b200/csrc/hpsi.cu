@@ -35,6 +35,7 @@
 #include "engine.h"
 #include "fft.cuh"
 #include "fftpath.h"
+#include "nl_tc.h"
 
 namespace pspw {
 
@@ -486,6 +487,9 @@ int hpsi_apply(pspw_cell *c, const void *in_v, int ld_in, void *out_v, int ld_ou
     timing_end(c, fam, e);
     c->kernel_launches++;
   };
+  // FP32 with one species: projector GEMMs on the tensor cores
+  bool use_tc = false;
+  if constexpr (sizeof(R) == 4) use_tc = nproj > 0 && nl_tc_usable(c);
   if (nproj > 0) {
     const int mt = (nproj + kBM - 1) / kBM, nt = (nb + kBN - 1) / kBN;
     // split G so the grid covers the GPU about twice
@@ -499,19 +503,31 @@ int hpsi_apply(pspw_cell *c, const void *in_v, int ld_in, void *out_v, int ld_ou
       part = static_cast<T *>(plan->part);
       wp = static_cast<T *>(plan->wp);
     } else {
-      int rc = ws_reserve(c, 2, sizeof(T) * (size_t)nsplit * nb * nproj, (void **)&part);
+      int rc = PSPW_OK;
+      if (!use_tc) rc = ws_reserve(c, 2, sizeof(T) * (size_t)nsplit * nb * nproj, (void **)&part);
       if (rc) return rc;
       rc = ws_reserve(c, 3, sizeof(T) * (size_t)nb * nproj, (void **)&wp);
       if (rc) return rc;
     }
     timing_begin(c, kFamNonlocal, &ev);
-    run(kFamProj, [&] {
-      k_proj<R, BK><<<dim3(mt, nt, nsplit), 256, 0, st>>>(pa, in, ld_in, ngw, nb, kchunk, part);
-    });
-    run(kFamProj, [&] {
-      k_proj_reduce<R><<<(nb * nproj + 255) / 256, 256, 0, st>>>(part, Prec<R>::pw(c), nsplit, nb,
-                                                                nproj, wp);
-    });
+    if (use_tc) {
+      cudaEvent_t e;
+      timing_begin(c, kFamProj, &e);
+      const int rc = nl_tc_project(c, reinterpret_cast<const float2 *>(in), ld_in, ngw, nb,
+                                   reinterpret_cast<float2 *>(wp),
+                                   plan ? static_cast<float *>(plan->part) : nullptr,
+                                   plan ? plan->max_split : 0);
+      timing_end(c, kFamProj, e);
+      if (rc) return rc;
+    } else {
+      run(kFamProj, [&] {
+        k_proj<R, BK><<<dim3(mt, nt, nsplit), 256, 0, st>>>(pa, in, ld_in, ngw, nb, kchunk, part);
+      });
+      run(kFamProj, [&] {
+        k_proj_reduce<R><<<(nb * nproj + 255) / 256, 256, 0, st>>>(part, Prec<R>::pw(c), nsplit,
+                                                                  nb, nproj, wp);
+      });
+    }
     timing_end(c, kFamNonlocal, ev);
     PSPW_CUDA(cudaGetLastError());
   }
@@ -586,11 +602,22 @@ int hpsi_apply(pspw_cell *c, const void *in_v, int ld_in, void *out_v, int ld_ou
   // ---- back-projection + recurrence epilogue
   if (nproj > 0) {
     timing_begin(c, kFamNonlocal, &ev);
-    dim3 grid((ngw + kBM - 1) / kBM, (nb + kBN - 1) / kBN);
-    run(kFamBackproj, [&] {
-      k_backproj<R, BK><<<grid, 256, 0, st>>>(pa, wp, ngw, nb, out, ld_out, in, ld_in, xm2, ld_xm2,
-                                              (R)a, (R)b, (R)g);
-    });
+    if (use_tc) {
+      cudaEvent_t e;
+      timing_begin(c, kFamBackproj, &e);
+      const int rc = nl_tc_backproject(
+          c, reinterpret_cast<const float2 *>(wp), ngw, nb, reinterpret_cast<float2 *>(out), ld_out,
+          reinterpret_cast<const float2 *>(in), ld_in, reinterpret_cast<const float2 *>(xm2),
+          ld_xm2, (float)a, (float)b, (float)g);
+      timing_end(c, kFamBackproj, e);
+      if (rc) return rc;
+    } else {
+      dim3 grid((ngw + kBM - 1) / kBM, (nb + kBN - 1) / kBN);
+      run(kFamBackproj, [&] {
+        k_backproj<R, BK><<<grid, 256, 0, st>>>(pa, wp, ngw, nb, out, ld_out, in, ld_in, xm2,
+                                                ld_xm2, (R)a, (R)b, (R)g);
+      });
+    }
     timing_end(c, kFamNonlocal, ev);
   } else if (a != 1.0 || b != 0.0 || g != 0.0) {
     run(kFamBackproj, [&] {

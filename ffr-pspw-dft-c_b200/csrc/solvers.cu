@@ -115,7 +115,7 @@ int apply_h(pspw_cell *c, int hprec, const double2 *X, double2 *HX, int m, int n
 int d2h(pspw_cell *c, void *dst, const void *src, size_t bytes) {
   PSPW_CUDA(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, c->stream));
   PSPW_CUDA(cudaStreamSynchronize(c->stream));
-  return PSPW_OK;
+  return device_status(c);
 }
 int h2d(pspw_cell *c, void *dst, const void *src, size_t bytes) {
   PSPW_CUDA(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, c->stream));

@@ -17,6 +17,9 @@ DROPIN_PATH = os.path.join(LIB_DIR, "libpspw_dropin.so")
 
 PREC_F64 = 0
 PREC_F32 = 1
+NL_AUTO = 0
+NL_SIMT = 1
+NL_TENSOR_CORE = 2
 
 OK = 0
 ERRORS = {1: "ARG", 2: "SHAPE", 3: "CUDA", 4: "OOM", 5: "NONFINITE", 6: "TIMEOUT", 7: "LAPACK",
@@ -57,6 +60,7 @@ SIGNATURES = {
     "pspw_cell_synchronize": [_vp],
     "pspw_cell_sizes": [_vp, _vp],
     "pspw_cell_set_band_batch": [_vp, _i],
+    "pspw_cell_set_nl_path": [_vp, _i],
     "pspw_apply_ham_block": [_vp, _vp, _vp, _i, _i],
     "pspw_apply_ham_block_dev": [_vp, _i, _vp, _vp, _i, _i, _i],
     "pspw_apply_ham_block_dev_noalloc": [_vp, _i, _vp, _vp, _i, _i, _i],

@@ -120,6 +120,10 @@ class Cell:
     def set_band_batch(self, n):
         check(lib().pspw_cell_set_band_batch(self._h, int(n)))
 
+    def set_nl_path(self, path):
+        """NL_AUTO / NL_SIMT / NL_TENSOR_CORE kernels for the FP32 projector GEMMs."""
+        check(lib().pspw_cell_set_nl_path(self._h, int(path)))
+
     # ---- host FP64 (the reference signatures' data)
     def apply_ham_block(self, vin):
         vin = _f(vin, np.complex128)

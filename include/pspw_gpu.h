@@ -108,6 +108,16 @@ int pspw_cell_sizes(pspw_cell *cell, int *out8);
  * (0 = automatic); results do not depend on it */
 int pspw_cell_set_band_batch(pspw_cell *cell, int nbatch);
 
+/* Kernels of the FP32 projector GEMMs (no reference counterpart: the
+ * reference has one CPU path).  AUTO takes the tensor-core (tcgen05, 3xTF32)
+ * kernels when the cell has one species and at most 256 atoms, else the
+ * SIMT kernels; TENSOR_CORE on a cell outside that range is
+ * PSPW_ERR_NOT_IMPL.  The FP64 path always uses the SIMT kernels. */
+#define PSPW_NL_AUTO 0
+#define PSPW_NL_SIMT 1
+#define PSPW_NL_TENSOR_CORE 2
+int pspw_cell_set_nl_path(pspw_cell *cell, int path);
+
 /* ------------------------------------------------------------------ H*psi
  * vout = H vin for nstates bands (ApplyHam_block.cpp:5-172): kinetic
  * 0.5*XKG*TPIBA2, local V_eff through an FFT sandwich, KB nonlocal

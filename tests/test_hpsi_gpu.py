@@ -15,7 +15,8 @@ if not torch.cuda.is_available():  # pragma: no cover
 
 import pspw_oracle as O  # noqa: E402
 from helpers import engine_cell_args, golden, oracle_cell, relmax  # noqa: E402
-from pspw import PREC_F32, PREC_F64, Cell, PspwError, basis_gamma, synth  # noqa: E402
+from pspw import (NL_SIMT, NL_TENSOR_CORE, PREC_F32, PREC_F64, Cell, PspwError,  # noqa: E402
+                  basis_gamma, synth)
 from pspw import workloads  # noqa: E402
 
 TOL64 = 1e-12
@@ -218,3 +219,83 @@ def test_si64_subset_parity_and_hermiticity():
     assert relmax(out, ref) < TOL64
     m = psi.conj().T @ out
     assert np.abs(m - m.conj().T).max() < 1e-12 * np.abs(m).max()
+
+
+def _hpsi32(cell, psi, ld=None):
+    ngw, nb = psi.shape
+    ld = ld or ngw
+    host = np.zeros((nb, ld), dtype=np.complex64)
+    host[:, :ngw] = psi.T
+    d_in = torch.from_numpy(host).cuda()
+    d_out = torch.zeros_like(d_in)
+    torch.cuda.synchronize()
+    cell.apply_ham_block_dev(d_in, d_out, ld, ngw, nb, PREC_F32)
+    torch.cuda.synchronize()
+    return d_out.cpu().numpy()[:, :ngw].T.astype(complex)
+
+
+@pytest.mark.parametrize("lm_end,nb", [([4], 1), ([4], 16), ([3], 7), ([2], 33), ([1], 5)])
+def test_fp32_tensor_core_projectors(lm_end, nb):
+    """tcgen05 3xTF32 projector GEMMs against the oracle and the SIMT kernels,
+    over projector counts L = 1..4 and band counts that leave ragged M and N
+    tiles (N tile = bands x 2L rounded to a multiple of 16)."""
+    d = dict(G)
+    args = engine_cell_args(d)
+    args["lm_end"] = lm_end
+    cell = Cell.from_arrays(args)
+    cell.set_veff(G["veff"])
+    rng = np.random.default_rng(nb)
+    psi = G["psi"][:, rng.integers(0, G["psi"].shape[1], nb)]
+    psi = np.asfortranarray(psi.astype(np.complex64).astype(complex))
+    oc = oracle_cell(d)
+    oc["lm_end"] = lm_end
+    ref = O.apply_ham_block(oc, psi, G["veff"])
+    cell.set_nl_path(NL_TENSOR_CORE)
+    out_tc = _hpsi32(cell, psi, ld=psi.shape[0] + 3)
+    cell.set_nl_path(NL_SIMT)
+    out_simt = _hpsi32(cell, psi)
+    assert relmax(out_tc, ref) < TOL32
+    assert relmax(out_simt, ref) < TOL32
+    assert relmax(out_tc, out_simt) < TOL32
+
+
+def test_fp32_tensor_core_atoms_not_a_multiple_of_16():
+    # 5 atoms: the atom (N) dimension of the projection is padded to 16
+    lat, pos = synth.si_diamond(1)
+    b = basis_gamma(lat, 8.0, None, [5], [pos[:5]])
+    pkg_a, wnl = synth.kb_form_factors(b, lat)
+    b.update(pkg_a=pkg_a, wnl=wnl, lm_end=[4])
+    veff = synth.local_potential(b["nr"], lat, pos)
+    psi = synth.wavefunctions(b, lat, 9, 3).astype(np.complex64).astype(complex)
+    cell = Cell.from_arrays(b)
+    cell.set_veff(veff)
+    cell.set_nl_path(NL_TENSOR_CORE)
+    oc = oracle_cell(b)
+    oc.update(na=[5])
+    ref = O.apply_ham_block(oc, psi, veff)
+    assert relmax(_hpsi32(cell, psi), ref) < TOL32
+
+
+def test_fp32_tensor_core_si64_all_bands():
+    # 64 atoms, 144 bands: 9 M tiles x split-K in the projection, 5 band
+    # tiles in the back-projection; against the engine's own FP64 path
+    w = workloads.workload("si64")
+    cell = workloads.make_cell(w)
+    psi = np.asfortranarray(w["psi"].astype(np.complex64).astype(complex))
+    ref = cell.apply_ham_block(psi)
+    cell.set_nl_path(NL_TENSOR_CORE)
+    out = _hpsi32(cell, psi)
+    assert relmax(out, ref) < TOL32
+    out2 = _hpsi32(cell, psi)
+    assert np.array_equal(out, out2)  # fixed-order split-K reduction
+
+
+def test_tensor_core_path_refused_for_two_species():
+    lat, pos = synth.si_diamond(1)
+    b = basis_gamma(lat, 8.0, None, [5, 3], [pos[:5], pos[5:]])
+    pkg_a, wnl = synth.kb_form_factors(b, lat, nsp=2, rc=[1.0, 0.8])
+    b.update(pkg_a=pkg_a, wnl=wnl, lm_end=[4, 1])
+    cell = Cell.from_arrays(b)
+    with pytest.raises(PspwError) as e:
+        cell.set_nl_path(NL_TENSOR_CORE)
+    assert e.value.code == 9

@@ -130,11 +130,19 @@ def test_lobpcg_matches_oracle(si8_12ry):
     assert ov.min() > 1 - 1e-8
 
 
-def test_lobpcg_converges_and_mixed_precision_agrees(si8_12ry):
+def test_lobpcg_long_run_and_mixed_precision(si8_12ry):
+    """60 iterations: the residual trajectory follows the oracle's (the
+    reference converges slowly on this cell, whose 10 states cut a
+    near-degenerate cluster), and FP32 H*psi inside the solver moves the
+    eigenvalues of the resolved states by less than 1e-5 Ha."""
     b, cell, veff = si8_12ry
     ngw = b["ngw"]
     prec = O.gen_prec(b["xkg"][:ngw], b["alat"], b["tpiba2"], -10.0)
     ev64, _, res64, _ = cell.lobpcg(ngw, 10, prec, 2, max_iter=60)
+    ev_o, _, res_o = O.lobpcg(oracle_cell(b), ngw, 10, veff, prec, 2, max_iter=60)
+    assert np.abs(ev64 - ev_o).max() < 1e-8
+    assert np.abs(res64 - res_o).max() < 1e-6
     ev32, _, res32, _ = cell.lobpcg(ngw, 10, prec, 2, max_iter=60, hprec=PREC_F32)
-    assert np.sort(res64)[:8].max() < 1e-4
-    assert np.abs(ev64[:8] - ev32[:8]).max() < 1e-5
+    ok = res64 < 1e-3
+    assert ok.sum() >= 5
+    assert np.abs(ev64[ok] - ev32[ok]).max() < 1e-5
