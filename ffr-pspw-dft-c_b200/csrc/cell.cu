@@ -213,7 +213,7 @@ int pspw_cell_destroy(pspw_cell *c) {
                   c->proj.d_pkga64, c->proj.d_pkga32, c->proj.d_patom, c->proj.d_psp,
                   c->proj.d_plm, c->proj.d_pw64, c->proj.d_pw32, c->d_veff64, c->d_veff32,
                   B.d_col_x, B.d_col_y, B.d_pinv[0], B.d_pinv[1], B.d_pinv[2], c->d_vperm64,
-                  c->d_vperm32};
+                  c->d_vperm32, c->proj.d_etp, c->proj.d_etb};
   for (void *p : ptrs)
     if (p) cudaFree(p);
   for (int i = 0; i < 3; i++) {
@@ -401,6 +401,7 @@ int pspw_cell_create(pspw_cell **out, int device, int nr1, int nr2, int nr3, int
       cudaHostGetDevicePointer((void **)&c->d_err, c->h_err, 0) != cudaSuccess)
     return bail(fail(PSPW_ERR_OOM, "cell_create: error word"));
   *c->h_err = 0;
+  if ((rc = pspw::nl_tc_prepare(c))) return bail(rc);
   *out = c;
   return PSPW_OK;
 }

@@ -66,6 +66,11 @@ struct Projectors {
   int *d_plm = nullptr;      // [nproj] lm (0..3)
   double *d_pw64 = nullptr;  // [nproj] WNL(species, lm)
   float *d_pw32 = nullptr;
+  // EIGR split into TF32 hi/lo operand tiles of the tensor-core projector
+  // GEMMs (one species only; built at cell creation, nl_tc.cu)
+  float *d_etp = nullptr;  // projection: per 8 G, [npad atoms x 16] hi then lo
+  float *d_etb = nullptr;  // back-projection: per (128 G, 8 atoms), [128 x 16] hi then lo
+  int tc_npad = 0;         // atoms padded to a multiple of 16
 };
 
 // Timing families (bit i of the mask enables family i).
@@ -103,7 +108,8 @@ enum WsSlot {
   kWsTau = 14,     // Householder scalars
   kWsEval = 15,    // eigenvalues of the overlap in eig_zhegv
   kWsSolverBase = 16,  // eigensolver blocks 16..31
-  kWsCount = 32
+  kWsWTile = 32,       // projections as tensor-core operand tiles
+  kWsCount = 33
 };
 
 struct Timing {
@@ -172,9 +178,11 @@ void timing_end(pspw_cell *c, int family, cudaEvent_t ev);
 
 // Scratch supplied by the caller of hpsi_apply instead of the cell's
 // workspaces: stick and plane buffers for `nbatch` bands, `max_split` slices
-// of projector partial sums, and the projections.
+// of projector partial sums, the projections, and (FP32 on the tensor-core
+// path) their operand tiles.
 struct ScratchPlan {
   void *S, *P, *part, *wp;
+  void *wt;  // projection operand tiles of the tensor-core back-projection
   int nbatch;
   int max_split;
 };

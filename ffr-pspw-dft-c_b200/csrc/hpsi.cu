@@ -490,6 +490,8 @@ int hpsi_apply(pspw_cell *c, const void *in_v, int ld_in, void *out_v, int ld_ou
   // FP32 with one species: projector GEMMs on the tensor cores
   bool use_tc = false;
   if constexpr (sizeof(R) == 4) use_tc = nproj > 0 && nl_tc_usable(c);
+  float *tc_part = nullptr, *tc_wt = nullptr;
+  int tc_split = 0;
   if (nproj > 0) {
     const int mt = (nproj + kBM - 1) / kBM, nt = (nb + kBN - 1) / kBN;
     // split G so the grid covers the GPU about twice
@@ -503,20 +505,27 @@ int hpsi_apply(pspw_cell *c, const void *in_v, int ld_in, void *out_v, int ld_ou
       part = static_cast<T *>(plan->part);
       wp = static_cast<T *>(plan->wp);
     } else {
-      int rc = PSPW_OK;
-      if (!use_tc) rc = ws_reserve(c, 2, sizeof(T) * (size_t)nsplit * nb * nproj, (void **)&part);
-      if (rc) return rc;
-      rc = ws_reserve(c, 3, sizeof(T) * (size_t)nb * nproj, (void **)&wp);
-      if (rc) return rc;
+      if (!use_tc) {
+        int rc = ws_reserve(c, 2, sizeof(T) * (size_t)nsplit * nb * nproj, (void **)&part);
+        if (rc) return rc;
+        rc = ws_reserve(c, 3, sizeof(T) * (size_t)nb * nproj, (void **)&wp);
+        if (rc) return rc;
+      }
     }
     timing_begin(c, kFamNonlocal, &ev);
     if (use_tc) {
+      if (plan) {
+        tc_part = static_cast<float *>(plan->part);
+        tc_wt = static_cast<float *>(plan->wt);
+        tc_split = plan->max_split;
+      } else {
+        const int rc = nl_tc_reserve(c, ngw, nb, &tc_part, &tc_split, &tc_wt);
+        if (rc) return rc;
+      }
       cudaEvent_t e;
       timing_begin(c, kFamProj, &e);
       const int rc = nl_tc_project(c, reinterpret_cast<const float2 *>(in), ld_in, ngw, nb,
-                                   reinterpret_cast<float2 *>(wp),
-                                   plan ? static_cast<float *>(plan->part) : nullptr,
-                                   plan ? plan->max_split : 0);
+                                   tc_part, tc_split, tc_wt);
       timing_end(c, kFamProj, e);
       if (rc) return rc;
     } else {
@@ -606,7 +615,7 @@ int hpsi_apply(pspw_cell *c, const void *in_v, int ld_in, void *out_v, int ld_ou
       cudaEvent_t e;
       timing_begin(c, kFamBackproj, &e);
       const int rc = nl_tc_backproject(
-          c, reinterpret_cast<const float2 *>(wp), ngw, nb, reinterpret_cast<float2 *>(out), ld_out,
+          c, tc_wt, ngw, nb, reinterpret_cast<float2 *>(out), ld_out,
           reinterpret_cast<const float2 *>(in), ld_in, reinterpret_cast<const float2 *>(xm2),
           ld_xm2, (float)a, (float)b, (float)g);
       timing_end(c, kFamBackproj, e);

@@ -12,20 +12,33 @@
 //   A'[(b,lm,re)][(G,*)] = PKG (Re psi,  Im psi)
 //   A'[(b,lm,im)][(G,*)] = PKG (Im psi, -Re psi)
 //   M = (band, lm, re/im) in tiles of 128, N = atoms, K = 2*NGW split over
-//   blocks; slices reduced in a fixed order with the weights WNL.
+//   blocks; the slices are reduced in a fixed order with the weights WNL.
 // back-projection NL[G][b] = sum_lm PKG[G][lm] sum_a E[a][G] W[(a,lm)][b]
 //   D[G][(b,lm,p)] = sum_{(a,c)} A'[G][(a,c)] B'[(b,lm,p)][(a,c)]
 //   A'[G][(a,0)] = Re E, A'[G][(a,1)] = Im E
 //   B'[(b,lm,re)][(a,*)] = (Re W, -Im W), B'[(b,lm,im)][(a,*)] = (Im W, Re W)
-//   M = G in tiles of 128, N = (band, lm, re/im) in tiles of up to 256,
+//   M = G in tiles of 128, N = (band, lm, re/im) in tiles of at most 128,
 //   K = 2*atoms; the epilogue contracts lm with PKG and applies the
 //   Chebyshev update out = a (H psi) + b psi + g x.
 //
-// Operands go global -> registers -> (TF32 hi/lo split) -> shared memory in
-// the K-major no-swizzle layout of tc.cuh, two stages deep: the global loads
-// of step k+1 are in flight while the MMAs of step k run.  One thread issues
-// the MMAs and commits them to the stage's mbarrier; every wait is bounded and
-// raises the cell's error word instead of hanging.
+// Operands that do not depend on psi (both EIGR operands) are split into
+// TF32 hi/lo tiles once per cell, in the K-major no-swizzle layout of tc.cuh,
+// and reach shared memory as single bulk copies.  The reduction of the
+// projection writes W' in the same tile form, so the back-projection is a
+// GEMM fed by bulk copies alone.  The psi operand of the projection is built
+// on the fly.
+//
+// Both GEMM kernels are warp-specialised (192 threads):
+//   warps 0-3  one thread per row of the 128-row M tile: build A' tiles
+//              (projection) and run the epilogue (TMEM -> registers);
+//   warp 4     producer: cp.async of psi / PKG_A into a raw ring
+//              (projection) and the bulk copies of the fixed tiles;
+//   warp 5     one thread issues the MMAs of a K step once its operand slot
+//              is full and commits them to the slot's "empty" barrier.
+// Slots are handed over with mbarriers only; there is no block-wide barrier
+// in the main loop.  Every wait is bounded and gives up as soon as any
+// thread of the block has given up; the block then raises the cell's error
+// word.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -39,22 +52,25 @@
 namespace pspw {
 namespace {
 
-constexpr int kBK = 16;                                 // fp32 of K per stage (8 complex)
+constexpr int kBK = 16;                                 // fp32 of K per step
 constexpr int kTileBytes128 = 128 * kBK * 4;            // 128 rows x BK fp32
 constexpr uint32_t kLBO = 128, kSBO = (kBK / 4) * 128;  // core-matrix strides
+constexpr int kNTP = 4;                                 // operand slots, projection
+constexpr int kNTB = 3;                                 // operand slots, back-projection
+constexpr int kNR = 6;                                  // raw slots, projection
+constexpr int kThreads = 192;
+constexpr int kMaxBackN = 128;  // N tile of the back-projection
 
-__device__ __forceinline__ void st_split(unsigned char *hi, unsigned char *lo, uint32_t off,
-                                         float x) {
-  uint32_t h, l;
-  tc::split_tf32(x, h, l);
-  *reinterpret_cast<uint32_t *>(hi + off) = h;
-  *reinterpret_cast<uint32_t *>(lo + off) = l;
+__host__ __device__ constexpr int round16(int x) { return (x + 15) & ~15; }
+
+__host__ __device__ constexpr uint32_t tmem_cols(int n) {
+  return n <= 32 ? 32u : (n <= 64 ? 64u : (n <= 128 ? 128u : 256u));
 }
 
-// The 3xTF32 MMAs of one stage (K = 16 as two K = 8 steps), from one thread.
-__device__ __forceinline__ void issue_stage(uint32_t tmem, uint32_t a_hi, uint32_t a_lo,
-                                            uint32_t b_hi, uint32_t b_lo, uint32_t idesc,
-                                            bool first) {
+// The 3xTF32 MMAs of one K step (K = 16 as two K = 8 instructions).
+__device__ __forceinline__ void issue_step(uint32_t tmem, uint32_t a_hi, uint32_t a_lo,
+                                           uint32_t b_hi, uint32_t b_lo, uint32_t idesc,
+                                           bool first) {
 #pragma unroll
   for (int s = 0; s < kBK / 8; s++) {
     const uint32_t o = s * 256;
@@ -66,24 +82,35 @@ __device__ __forceinline__ void issue_stage(uint32_t tmem, uint32_t a_hi, uint32
   }
 }
 
-__host__ __device__ constexpr uint32_t tmem_cols(int n) {
-  return n <= 32 ? 32u : (n <= 64 ? 64u : (n <= 128 ? 128u : 256u));
-}
-
-// Shared state of one block: stage barriers and the TMEM base address.
-struct Pipe {
-  uint64_t bar[2];
+// Barriers and state shared by the roles of one block.
+struct Sync {
+  uint64_t full[kNTP];   // A' tile written by the row threads (projection)
+  uint64_t bfull[kNTP];  // bulk-copied operands landed
+  uint64_t empty[kNTP];  // MMAs reading the slot finished
+  uint64_t rfull[kNR];   // raw slot landed (projection)
+  uint64_t rempty[kNR];  // raw slot consumed (projection)
+  uint64_t done;         // every MMA of the block finished
   uint32_t tmem;
+  int abort;
 };
 
-__device__ __forceinline__ void pipe_open(Pipe &p, uint32_t ncols) {
+__device__ __forceinline__ void open_block(Sync &sy, uint32_t ncols, int nt, int nfull, int nraw) {
   if (threadIdx.x < 32) {
-    tc::tmem_alloc(&p.tmem, ncols);
+    tc::tmem_alloc(&sy.tmem, ncols);
     tc::tmem_relinquish();
   }
   if (threadIdx.x == 0) {
-    tc::mbar_init(&p.bar[0], 1);
-    tc::mbar_init(&p.bar[1], 1);
+    for (int i = 0; i < nt; i++) {
+      tc::mbar_init(&sy.full[i], nfull);
+      tc::mbar_init(&sy.bfull[i], 1);
+      tc::mbar_init(&sy.empty[i], 1);
+    }
+    for (int i = 0; i < nraw; i++) {
+      tc::mbar_init(&sy.rfull[i], 32);
+      tc::mbar_init(&sy.rempty[i], 128);
+    }
+    tc::mbar_init(&sy.done, 1);
+    sy.abort = 0;
     tc::fence_mbar_init();
   }
   tc::fence_before_sync();
@@ -91,363 +118,527 @@ __device__ __forceinline__ void pipe_open(Pipe &p, uint32_t ncols) {
   tc::fence_after_sync();
 }
 
-// Wait (bounded, block-uniform result) until the MMAs reading stage `st`
-// have finished.
-__device__ __forceinline__ bool stage_free(Pipe &p, int st, uint32_t *nphase) {
-  const bool done = tc::mbar_wait(&p.bar[st], nphase[st] & 1);
-  nphase[st]++;
-  return __syncthreads_and(done) != 0;
-}
-
-// Staged tile written: make it visible to the tensor core and issue.
-__device__ __forceinline__ void stage_issue(Pipe &p, int st, unsigned char *a_hi,
-                                            unsigned char *b_hi, int bbytes, uint32_t idesc,
-                                            bool first) {
-  tc::fence_proxy_async();
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    tc::fence_after_sync();
-    issue_stage(p.tmem, tc::smem_addr(a_hi), tc::smem_addr(a_hi + kTileBytes128),
-                tc::smem_addr(b_hi), tc::smem_addr(b_hi + bbytes), idesc, first);
-    tc::mma_commit(&p.bar[st]);
-  }
-}
-
-// After the main loop: wait for the last commit (it covers every earlier
-// MMA of the thread that issued them).  Block-uniform result.
-__device__ __forceinline__ bool pipe_drain(Pipe &p, int nissued, uint32_t *nphase) {
-  bool done = true;
-  if (nissued > 0) {
-    const int st = (nissued - 1) & 1;
-    done = tc::mbar_wait(&p.bar[st], nphase[st] & 1);
-  }
-  const bool ok = __syncthreads_and(done) != 0;
-  tc::fence_after_sync();
-  return ok;
-}
-
-__device__ __forceinline__ void pipe_close(Pipe &p, uint32_t ncols) {
+__device__ __forceinline__ void close_block(Sync &sy, uint32_t ncols, int *err) {
   tc::fence_before_sync();
   __syncthreads();
-  if (threadIdx.x < 32) tc::tmem_dealloc(p.tmem, ncols);
+  if (threadIdx.x == 0 && sy.abort) atomicOr(err, 1);
+  if (threadIdx.x < 32) tc::tmem_dealloc(sy.tmem, ncols);
+}
+
+// Producer tail: wait (bounded) until the bulk copies of the last `nt`
+// issued steps have landed, so none is in flight when the block exits.
+__device__ __forceinline__ void drain_bulk(Sync &sy, int issued, int nt) {
+  for (int k = max(0, issued - nt); k < issued; k++) tc::mbar_wait(&sy.bfull[k % nt], (k / nt) & 1);
 }
 
 // ------------------------------------------------------------------ projection
-// grid (M tiles of 128 rows, K splits of ksplit_g G each); block 128.
-// part[split][m][a] with m = b*2L + 2*lm + p.
-__global__ void __launch_bounds__(128) k_proj_tc(const float2 *__restrict__ psi, int ld, int ngw,
-                                                 int nb, const float2 *__restrict__ eigr,
-                                                 int ngw_cell, const float *__restrict__ pkga,
-                                                 int L, int nat, int npad, int ksplit_g,
-                                                 float *__restrict__ part, int *err) {
+// grid (M tiles of 128 rows, K splits of ksplit_g G each); 192 threads.
+// etp: per 8 G, [npad x 16] hi then lo.  part[split][m][a], m = b*2L + 2lm + p.
+template <int L>
+__global__ void __launch_bounds__(kThreads) k_proj_tc(const float2 *__restrict__ psi, int ld,
+                                                      int ngw, int nb,
+                                                      const float *__restrict__ etp,
+                                                      const float *__restrict__ pkga, int nat,
+                                                      int npad, int ksplit_g,
+                                                      float *__restrict__ part, int *err) {
+  constexpr int per = 2 * L;
+  constexpr int nbr_max = 127 / per + 2;  // bands a 128-row tile touches
+  constexpr int raw_psi = round16(nbr_max * 9 * 8);
+  constexpr int raw_bytes = raw_psi + 128;
   extern __shared__ __align__(1024) unsigned char sm[];
-  __shared__ Pipe pipe;
-  const int tid = threadIdx.x, warp = tid >> 5;
-  const int Mtot = nb * 2 * L;
+  __shared__ Sync sy;
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int Mtot = nb * per;
   const int m0 = blockIdx.x * 128;
+  const int bfirst = m0 / per;
+  const int nbr = min(Mtot - 1, m0 + 127) / per - bfirst + 1;
   const int gb = blockIdx.y * ksplit_g, ge = min(ngw, gb + ksplit_g);
-  const int bbytes = npad * kBK * 4;
-  const int stage_bytes = 2 * kTileBytes128 + 2 * bbytes;
-  const uint32_t ncols = tmem_cols(npad);
-  pipe_open(pipe, ncols);
-  const uint32_t idesc = tc::idesc_tf32(128, npad);
-  // this thread's row of A'
-  const int m = m0 + tid;
-  const bool mvalid = m < Mtot;
-  const int b = mvalid ? m / (2 * L) : 0;
-  const int lm = mvalid ? (m % (2 * L)) >> 1 : 0;
-  const int p = m & 1;
-  const float2 *pcol = psi + (size_t)b * ld;
-  uint32_t nphase[2] = {0, 0};
-  bool ok = true;
   const int nsteps = ge > gb ? (ge - gb + 7) / 8 : 0;
-  int issued = 0;
-  for (int step = 0; step < nsteps; step++) {
-    const int st = step & 1;
-    const int g0 = gb + step * 8;
-    // global loads of this step
-    float2 v[8];
-    float f[8];
+  const uint32_t ebytes = (uint32_t)npad * 128;  // hi + lo EIGR tile of one step
+  const int slot_bytes = 2 * kTileBytes128 + (int)ebytes;
+  unsigned char *raw0 = sm + kNTP * slot_bytes;
+  const uint32_t ncols = tmem_cols(npad);
+  open_block(sy, ncols, kNTP, 128, kNR);
+
+  if (warp < 4) {
+    // ---- A' rows: thread tid owns row m of every A' tile
+    const int m = m0 + tid;
+    const bool mv = m < Mtot;
+    const int bl = mv ? m / per - bfirst : 0;
+    const int lm = (m % per) >> 1, p = m & 1;
+    for (int k = 0; k < nsteps; k++) {
+      const int rs = k % kNR, ts = k % kNTP;
+      if (!tc::mbar_wait_abort(&sy.rfull[rs], (k / kNR) & 1, &sy.abort)) break;
+      if (k >= kNTP && !tc::mbar_wait_abort(&sy.empty[ts], ((k / kNTP) - 1) & 1, &sy.abort))
+        break;
+      if (mv) {
+        const unsigned char *r = raw0 + rs * raw_bytes;
+        const float2 *rp = reinterpret_cast<const float2 *>(r) + bl * 9;
+        const float *rk = reinterpret_cast<const float *>(r + raw_psi);
+        unsigned char *a_hi = sm + ts * slot_bytes;
 #pragma unroll
-    for (int j = 0; j < 8; j++) {
-      const int g = g0 + j;
-      const bool in = mvalid && g < ge;
-      v[j] = in ? pcol[g] : make_float2(0.f, 0.f);
-      f[j] = in ? pkga[(size_t)g * 4 + lm] : 0.f;
-    }
-    float2 e[2][8];
-#pragma unroll
-    for (int rr = 0; rr < 2; rr++) {
-      const int r = tid + 128 * rr;
-#pragma unroll
-      for (int j = 0; j < 8; j++) {
-        const int g = g0 + j;
-        e[rr][j] = (r < nat && g < ge) ? eigr[(size_t)r * ngw_cell + g] : make_float2(0.f, 0.f);
+        for (int c = 0; c < 4; c++) {
+          const float2 v0 = rp[2 * c], v1 = rp[2 * c + 1];
+          const float f0 = rk[8 * c + lm], f1 = rk[8 * c + 4 + lm];
+          const float4 x = p ? make_float4(f0 * v0.y, -f0 * v0.x, f1 * v1.y, -f1 * v1.x)
+                             : make_float4(f0 * v0.x, f0 * v0.y, f1 * v1.x, f1 * v1.y);
+          tc::st_split4(a_hi, a_hi + kTileBytes128, tc::core_off<kBK>(tid, 4 * c), x);
+        }
       }
+      tc::fence_proxy_async();
+      tc::mbar_arrive(&sy.full[ts]);
+      tc::mbar_arrive(&sy.rempty[rs]);
     }
-    if (step >= 2 && !(ok = stage_free(pipe, st, nphase))) break;
-    unsigned char *a_hi = sm + st * stage_bytes, *a_lo = a_hi + kTileBytes128;
-    unsigned char *b_hi = a_lo + kTileBytes128, *b_lo = b_hi + bbytes;
+    // ---- epilogue: D row m -> part (tcgen05.ld is warp-collective, so the
+    // decision is taken per warp and rows past Mtot load without storing)
+    const bool ok = __all_sync(0xffffffffu, tc::mbar_wait_abort(&sy.done, 0, &sy.abort));
+    tc::fence_after_sync();
+    if (ok) {
+      float *dst = part + ((size_t)blockIdx.y * Mtot + m) * nat;
+      float acc[16];
+      for (int c0 = 0; c0 < npad; c0 += 16) {
+        if (nsteps > 0) {
+          tc::tmem_ld16(sy.tmem + ((uint32_t)(32 * warp) << 16) + (uint32_t)c0, acc);
+        } else {
 #pragma unroll
-    for (int j = 0; j < 8; j++) {
-      const float x0 = p ? f[j] * v[j].y : f[j] * v[j].x;
-      const float x1 = p ? -f[j] * v[j].x : f[j] * v[j].y;
-      st_split(a_hi, a_lo, tc::core_off<kBK>(tid, 2 * j), x0);
-      st_split(a_hi, a_lo, tc::core_off<kBK>(tid, 2 * j + 1), x1);
-    }
+          for (int i = 0; i < 16; i++) acc[i] = 0.f;
+        }
+        if (mv) {
 #pragma unroll
-    for (int rr = 0; rr < 2; rr++) {
-      const int r = tid + 128 * rr;
-      if (r < npad) {
-#pragma unroll
-        for (int j = 0; j < 8; j++) {
-          st_split(b_hi, b_lo, tc::core_off<kBK>(r, 2 * j), e[rr][j].x);
-          st_split(b_hi, b_lo, tc::core_off<kBK>(r, 2 * j + 1), e[rr][j].y);
+          for (int i = 0; i < 16; i++)
+            if (c0 + i < nat) dst[c0 + i] = acc[i];
         }
       }
     }
-    stage_issue(pipe, st, a_hi, b_hi, bbytes, idesc, step == 0);
-    issued++;
-  }
-  const bool drained = pipe_drain(pipe, issued, nphase);
-  if (!(ok && drained)) {
-    if (tid == 0) atomicOr(err, 1);
-  } else {
-    const int mg = m0 + 32 * warp + (tid & 31);
-    float acc[16];
-    for (int c0 = 0; c0 < npad; c0 += 16) {
-      if (issued > 0) {
-        tc::tmem_ld16(pipe.tmem + ((uint32_t)(32 * warp) << 16) + (uint32_t)c0, acc);
-      } else {
-#pragma unroll
-        for (int i = 0; i < 16; i++) acc[i] = 0.f;
+  } else if (warp == 4) {
+    // ---- producer: raw psi / PKG_A by all lanes, EIGR tiles by lane 0
+    int issued = 0;
+    for (int k = 0; k < nsteps; k++) {
+      const int rs = k % kNR, ts = k % kNTP;
+      if (k >= kNR && !tc::mbar_wait_abort(&sy.rempty[rs], ((k / kNR) - 1) & 1, &sy.abort))
+        break;
+      unsigned char *r = raw0 + rs * raw_bytes;
+      float2 *rp = reinterpret_cast<float2 *>(r);
+      float *rk = reinterpret_cast<float *>(r + raw_psi);
+      const int g0 = gb + 8 * k;
+      for (int e = lane; e < nbr * 8; e += 32) {
+        const int b = e >> 3, g = g0 + (e & 7);
+        const bool v = g < ge;
+        tc::cp_async8(rp + b * 9 + (e & 7), psi + (size_t)(bfirst + b) * ld + (v ? g : 0), v);
       }
-      if (mg < Mtot) {
-        float *dst = part + ((size_t)blockIdx.y * Mtot + mg) * nat;
-#pragma unroll
-        for (int i = 0; i < 16; i++)
-          if (c0 + i < nat) dst[c0 + i] = acc[i];
+      if (lane < 8) {
+        const int g = g0 + lane;
+        const bool v = g < ge;
+        tc::cp_async16(rk + 4 * lane, pkga + (size_t)(v ? g : 0) * 4, v);
+      }
+      tc::cp_async_mbar_arrive_noinc(&sy.rfull[rs]);
+      if (lane == 0) {
+        if (k >= kNTP && !tc::mbar_wait_abort(&sy.empty[ts], ((k / kNTP) - 1) & 1, &sy.abort))
+          break;
+        tc::mbar_arrive_expect_tx(&sy.bfull[ts], ebytes);
+        tc::bulk_g2s(sm + ts * slot_bytes + 2 * kTileBytes128,
+                     etp + (size_t)(gb / 8 + k) * (ebytes / 4), ebytes, &sy.bfull[ts]);
+        issued = k + 1;
       }
     }
+    tc::cp_async_wait<0>();
+    if (lane == 0) drain_bulk(sy, issued, kNTP);
+  } else if (lane == 0) {
+    // ---- MMA issuer
+    const uint32_t idesc = tc::idesc_tf32(128, npad);
+    for (int k = 0; k < nsteps; k++) {
+      const int ts = k % kNTP;
+      const uint32_t par = (k / kNTP) & 1;
+      if (!tc::mbar_wait_abort(&sy.bfull[ts], par, &sy.abort) ||
+          !tc::mbar_wait_abort(&sy.full[ts], par, &sy.abort))
+        break;
+      tc::fence_after_sync();
+      const uint32_t a = tc::smem_addr(sm + ts * slot_bytes);
+      issue_step(sy.tmem, a, a + kTileBytes128, a + 2 * kTileBytes128,
+                 a + 2 * kTileBytes128 + npad * 64, idesc, k == 0);
+      tc::mma_commit(&sy.empty[ts]);
+    }
+    tc::mma_commit(&sy.done);  // arrives once every MMA issued above has finished
   }
-  pipe_close(pipe, ncols);
+  close_block(sy, ncols, err);
 }
 
-// wp[b*nproj + a*L + lm] = W * sum_s (part[s][(b,lm,re)][a] + i part[s][(b,lm,im)][a]),
-// the slices summed in a fixed order.
-__global__ void k_proj_tc_reduce(const float *__restrict__ part, int nsplit, int nb, int L,
-                                 int nat, const float *__restrict__ w, float2 *__restrict__ wp) {
-  const int nproj = nat * L;
-  const int Mtot = nb * 2 * L;
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= nb * nproj) return;
-  const int b = i / nproj, pj = i - b * nproj;
-  const int a = pj / L, lm = pj - a * L;
-  const int mre = b * 2 * L + 2 * lm;
-  float re = 0.f, im = 0.f;
-  for (int s = 0; s < nsplit; s++) {
-    re += part[((size_t)s * Mtot + mre) * nat + a];
-    im += part[((size_t)s * Mtot + mre + 1) * nat + a];
+// Reduction of the projection slices, written as the B' operand tiles of the
+// back-projection: tile (band tile bt, atom step s) holds ncolN = nbt*2L rows
+// x 16 fp32 (8 atoms x re/im), hi then lo.  Every element of every tile is
+// written (zeros outside nb x nat).  One thread per (bt, s, band, lm, pair of
+// atoms); the slices are summed in a fixed order.
+template <int L>
+__global__ void k_proj_tc_wtiles(const float *__restrict__ part, int nsplit, int nb, int nat,
+                                 const float *__restrict__ w, int nbt, int nsa, int total,
+                                 float *__restrict__ wt) {
+  constexpr int per = 2 * L;
+  const int idx = blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= total) return;
+  int t = idx;
+  const int c = t & 3;
+  t >>= 2;
+  const int lm = t % L;
+  t /= L;
+  const int bl = t % nbt;
+  t /= nbt;
+  const int s = t % nsa;
+  const int bt = t / nsa;
+  const int b = bt * nbt + bl;
+  const int Mtot = nb * per;
+  float2 W[2];
+#pragma unroll
+  for (int q = 0; q < 2; q++) {
+    const int a = 8 * s + 2 * c + q;
+    float re = 0.f, im = 0.f;
+    if (b < nb && a < nat) {
+      const int mre = b * per + 2 * lm;
+      for (int sl = 0; sl < nsplit; sl++) {
+        re += part[((size_t)sl * Mtot + mre) * nat + a];
+        im += part[((size_t)sl * Mtot + mre + 1) * nat + a];
+      }
+      const float wl = w[a * L + lm];
+      re *= wl;
+      im *= wl;
+    }
+    W[q] = make_float2(re, im);
   }
-  const float wl = w[pj];
-  wp[i] = make_float2(wl * re, wl * im);
+  const int ncolN = nbt * per;
+  unsigned char *hi = reinterpret_cast<unsigned char *>(wt + ((size_t)bt * nsa + s) * ncolN * 32);
+  unsigned char *lo = hi + ncolN * 64;
+  const int r = bl * per + 2 * lm;
+  tc::st_split4(hi, lo, tc::core_off<kBK>(r, 4 * c),
+                make_float4(W[0].x, -W[0].y, W[1].x, -W[1].y));
+  tc::st_split4(hi, lo, tc::core_off<kBK>(r + 1, 4 * c),
+                make_float4(W[0].y, W[0].x, W[1].y, W[1].x));
 }
 
 // ------------------------------------------------------------------ back-projection
-// grid (G tiles of 128, N tiles of nbt bands); block 128.
-__global__ void __launch_bounds__(128) k_backproj_tc(
-    const float2 *__restrict__ wp, int nproj, int ngw, int nb, int nbt,
-    const float2 *__restrict__ eigr, int ngw_cell, const float *__restrict__ pkga, int L, int nat,
-    float2 *out, int ldo, const float2 *__restrict__ in, int ldi, const float2 *__restrict__ xm2,
-    int ldx, float ca, float cb, float cg, int *err) {
+// grid (G tiles of 128, band tiles of nbt); 192 threads.
+// etb: per (G tile, 8 atoms), [128 x 16] hi then lo.  wt: see k_proj_tc_wtiles.
+template <int L>
+__global__ void __launch_bounds__(kThreads) k_backproj_tc(
+    const float *__restrict__ etb, const float *__restrict__ wt, int nsa, int ngw, int nb, int nbt,
+    const float *__restrict__ pkga, float2 *out, int ldo, const float2 *__restrict__ in, int ldi,
+    const float2 *__restrict__ xm2, int ldx, float ca, float cb, float cg, int *err) {
+  constexpr int per = 2 * L;
   extern __shared__ __align__(1024) unsigned char sm[];
-  __shared__ Pipe pipe;
-  const int tid = threadIdx.x, warp = tid >> 5;
-  const int g0 = blockIdx.x * 128;
-  const int b0 = blockIdx.y * nbt;
+  __shared__ Sync sy;
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int gt = blockIdx.x, bt = blockIdx.y;
+  const int g0 = gt * 128, b0 = bt * nbt;
   const int nbb = min(nbt, nb - b0);
-  const int per = 2 * L;             // columns per band
-  const int ncolN = nbt * per;       // N of the MMA: a multiple of 16, <= 256
-  const int bbytes = ncolN * kBK * 4;
-  const int stage_bytes = 2 * kTileBytes128 + 2 * bbytes;
+  const int ncolN = nbt * per;  // a multiple of 16, <= 128
+  const uint32_t abytes = 2 * kTileBytes128, bbytes = (uint32_t)ncolN * 128;
+  const int slot_bytes = (int)(abytes + bbytes);
   const uint32_t ncols = tmem_cols(ncolN);
-  pipe_open(pipe, ncols);
-  const uint32_t idesc = tc::idesc_tf32(128, ncolN);
-  const int ga = g0 + tid;  // this thread's G row of A'
-  uint32_t nphase[2] = {0, 0};
-  bool ok = true;
-  const int nsteps = (nat + 7) / 8;  // 8 atoms = 16 fp32 of K per stage
-  int issued = 0;
-  for (int step = 0; step < nsteps; step++) {
-    const int st = step & 1;
-    const int a0 = step * 8;
-    float2 e[8];
-#pragma unroll
-    for (int j = 0; j < 8; j++) {
-      const int a = a0 + j;
-      e[j] = (a < nat && ga < ngw) ? eigr[(size_t)a * ngw_cell + ga] : make_float2(0.f, 0.f);
-    }
-    float2 w[2][8];
-#pragma unroll
-    for (int rr = 0; rr < 2; rr++) {
-      const int r = tid + 128 * rr;
-      const int bl = r / per, lm = (r % per) >> 1;
-      const bool rv = r < ncolN && bl < nbb;
-#pragma unroll
-      for (int j = 0; j < 8; j++) {
-        const int a = a0 + j;
-        w[rr][j] = (rv && a < nat) ? wp[(size_t)(b0 + bl) * nproj + a * L + lm]
-                                   : make_float2(0.f, 0.f);
+  open_block(sy, ncols, kNTB, 1, 0);
+
+  if (warp == 4) {
+    if (lane == 0) {
+      int issued = 0;
+      for (int k = 0; k < nsa; k++) {
+        const int ts = k % kNTB;
+        if (k >= kNTB && !tc::mbar_wait_abort(&sy.empty[ts], ((k / kNTB) - 1) & 1, &sy.abort))
+          break;
+        unsigned char *slot = sm + ts * slot_bytes;
+        tc::mbar_arrive_expect_tx(&sy.bfull[ts], abytes + bbytes);
+        tc::bulk_g2s(slot, etb + ((size_t)gt * nsa + k) * (abytes / 4), abytes, &sy.bfull[ts]);
+        tc::bulk_g2s(slot + abytes, wt + ((size_t)bt * nsa + k) * (bbytes / 4), bbytes,
+                     &sy.bfull[ts]);
+        issued = k + 1;
       }
+      drain_bulk(sy, issued, kNTB);
     }
-    if (step >= 2 && !(ok = stage_free(pipe, st, nphase))) break;
-    unsigned char *a_hi = sm + st * stage_bytes, *a_lo = a_hi + kTileBytes128;
-    unsigned char *b_hi = a_lo + kTileBytes128, *b_lo = b_hi + bbytes;
-#pragma unroll
-    for (int j = 0; j < 8; j++) {
-      st_split(a_hi, a_lo, tc::core_off<kBK>(tid, 2 * j), e[j].x);
-      st_split(a_hi, a_lo, tc::core_off<kBK>(tid, 2 * j + 1), e[j].y);
-    }
-#pragma unroll
-    for (int rr = 0; rr < 2; rr++) {
-      const int r = tid + 128 * rr;
-      if (r < ncolN) {
-        const int pr = r & 1;
-#pragma unroll
-        for (int j = 0; j < 8; j++) {
-          const float x0 = pr ? w[rr][j].y : w[rr][j].x;
-          const float x1 = pr ? w[rr][j].x : -w[rr][j].y;
-          st_split(b_hi, b_lo, tc::core_off<kBK>(r, 2 * j), x0);
-          st_split(b_hi, b_lo, tc::core_off<kBK>(r, 2 * j + 1), x1);
-        }
+  } else if (warp == 5) {
+    if (lane == 0) {
+      const uint32_t idesc = tc::idesc_tf32(128, ncolN);
+      for (int k = 0; k < nsa; k++) {
+        const int ts = k % kNTB;
+        if (!tc::mbar_wait_abort(&sy.bfull[ts], (k / kNTB) & 1, &sy.abort)) break;
+        tc::fence_after_sync();
+        const uint32_t a = tc::smem_addr(sm + ts * slot_bytes);
+        issue_step(sy.tmem, a, a + kTileBytes128, a + abytes, a + abytes + ncolN * 64, idesc,
+                   k == 0);
+        tc::mma_commit(&sy.empty[ts]);
       }
+      tc::mma_commit(&sy.done);
     }
-    stage_issue(pipe, st, a_hi, b_hi, bbytes, idesc, step == 0);
-    issued++;
-  }
-  const bool drained = pipe_drain(pipe, issued, nphase);
-  if (!(ok && drained)) {
-    if (tid == 0) atomicOr(err, 1);
   } else {
-    // epilogue: this thread owns G row g of the warp's 32-lane slice
-    const int g = g0 + 32 * warp + (tid & 31);
-    float pk[4] = {0.f, 0.f, 0.f, 0.f};
-    if (g < ngw)
-      for (int l = 0; l < L; l++) pk[l] = pkga[(size_t)g * 4 + l];
-    float acc[16];
-    float accr = 0.f, acci = 0.f;
-    int col = 0;
-    for (int c0 = 0; c0 < ncolN; c0 += 16) {
-      if (issued > 0) {
-        tc::tmem_ld16(pipe.tmem + ((uint32_t)(32 * warp) << 16) + (uint32_t)c0, acc);
-      } else {
-#pragma unroll
-        for (int i = 0; i < 16; i++) acc[i] = 0.f;
+    // ---- epilogue: this thread owns G row g of the warp's 32-lane slice
+    const bool ok = __all_sync(0xffffffffu, tc::mbar_wait_abort(&sy.done, 0, &sy.abort));
+    tc::fence_after_sync();
+    if (ok) {
+      const int g = g0 + tid;
+      float pk[4] = {0.f, 0.f, 0.f, 0.f};
+      if (g < ngw) {
+        const float4 p4 = *reinterpret_cast<const float4 *>(pkga + (size_t)g * 4);
+        pk[0] = p4.x;
+        pk[1] = p4.y;
+        pk[2] = p4.z;
+        pk[3] = p4.w;
       }
+      float acc[16];
+      float accr = 0.f, acci = 0.f;
+      for (int c0 = 0; c0 < ncolN; c0 += 16) {
+        tc::tmem_ld16(sy.tmem + ((uint32_t)(32 * warp) << 16) + (uint32_t)c0, acc);
 #pragma unroll
-      for (int i = 0; i < 16; i++, col++) {
-        const int cc = col % per;
-        const float pv = pk[cc >> 1];
-        if (cc & 1)
-          acci += pv * acc[i];
-        else
-          accr += pv * acc[i];
-        if (cc == per - 1) {
-          const int bl = col / per;
-          if (bl < nbb && g < ngw) {
-            const size_t bb = (size_t)(b0 + bl);
-            const float2 h = out[bb * ldo + g];
-            float rr = ca * (h.x + accr), ii = ca * (h.y + acci);
-            if (cb != 0.f) {
-              const float2 u = in[bb * ldi + g];
-              rr += cb * u.x;
-              ii += cb * u.y;
+        for (int i = 0; i < 16; i++) {
+          const int col = c0 + i;
+          const int cc = col % per;
+          if (cc & 1)
+            acci += pk[cc >> 1] * acc[i];
+          else
+            accr += pk[cc >> 1] * acc[i];
+          if (cc == per - 1) {
+            const int bl = col / per;
+            if (bl < nbb && g < ngw) {
+              const size_t bb = (size_t)(b0 + bl);
+              const float2 h = out[bb * ldo + g];
+              float rr = ca * (h.x + accr), ii = ca * (h.y + acci);
+              if (cb != 0.f) {
+                const float2 u = in[bb * ldi + g];
+                rr += cb * u.x;
+                ii += cb * u.y;
+              }
+              if (cg != 0.f) {
+                const float2 u = xm2[bb * ldx + g];
+                rr += cg * u.x;
+                ii += cg * u.y;
+              }
+              out[bb * ldo + g] = make_float2(rr, ii);
             }
-            if (cg != 0.f) {
-              const float2 u = xm2[bb * ldx + g];
-              rr += cg * u.x;
-              ii += cg * u.y;
-            }
-            out[bb * ldo + g] = make_float2(rr, ii);
+            accr = acci = 0.f;
           }
-          accr = acci = 0.f;
         }
       }
     }
   }
-  pipe_close(pipe, ncols);
+  close_block(sy, ncols, err);
 }
 
-// Dynamic shared memory of a block whose B' tile has nrows_b rows: the two
-// stages, raised where needed so that no more blocks fit on an SM than its
-// 512 TMEM columns can serve at once (an allocation would otherwise wait for
-// a resident block to finish).
-int tile_smem(int nrows_b) {
-  const int stages = 2 * (2 * kTileBytes128 + 2 * nrows_b * kBK * 4);
-  const int per_sm = 512 / (int)tmem_cols(nrows_b);
+// ------------------------------------------------------------------ EIGR tiles
+__global__ void k_build_etp(const float2 *__restrict__ eigr, int ngw, int nat, int npad, int nst,
+                            float *__restrict__ etp) {
+  const long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (idx >= (long long)nst * npad * 4) return;
+  const int c = (int)(idx & 3);
+  const int r = (int)((idx >> 2) % npad);
+  const int s = (int)(idx / (4 * npad));
+  float v[4];
+#pragma unroll
+  for (int q = 0; q < 4; q++) {
+    const int k = 4 * c + q, g = 8 * s + (k >> 1);
+    float x = 0.f;
+    if (r < nat && g < ngw) {
+      const float2 e = eigr[(size_t)r * ngw + g];
+      x = (k & 1) ? e.y : e.x;
+    }
+    v[q] = x;
+  }
+  unsigned char *hi = reinterpret_cast<unsigned char *>(etp + (size_t)s * npad * 32);
+  tc::st_split4(hi, hi + npad * 64, tc::core_off<kBK>(r, 4 * c), make_float4(v[0], v[1], v[2], v[3]));
+}
+
+__global__ void k_build_etb(const float2 *__restrict__ eigr, int ngw, int nat, int nsa, int ngt,
+                            float *__restrict__ etb) {
+  const long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (idx >= (long long)ngt * nsa * 512) return;
+  const int c = (int)(idx & 3);
+  const int gg = (int)((idx >> 2) & 127);
+  const int s = (int)((idx >> 9) % nsa);
+  const int t = (int)(idx / (512LL * nsa));
+  float v[4];
+#pragma unroll
+  for (int q = 0; q < 4; q++) {
+    const int k = 4 * c + q, a = 8 * s + (k >> 1), g = 128 * t + gg;
+    float x = 0.f;
+    if (a < nat && g < ngw) {
+      const float2 e = eigr[(size_t)a * ngw + g];
+      x = (k & 1) ? e.y : e.x;
+    }
+    v[q] = x;
+  }
+  unsigned char *hi = reinterpret_cast<unsigned char *>(etb + ((size_t)t * nsa + s) * 4096);
+  tc::st_split4(hi, hi + 8192, tc::core_off<kBK>(gg, 4 * c), make_float4(v[0], v[1], v[2], v[3]));
+}
+
+// ------------------------------------------------------------------ host side
+struct Shape {
+  int L, per, nat, npad, nsa, nbt, ncolN, nbtiles;
+};
+
+bool fits(const Projectors &P) {
+  return P.nsp == 1 && P.nat >= 1 && P.nat <= 256 && P.nproj > 0 && P.nproj % P.nat == 0 &&
+         P.nproj / P.nat <= 4;
+}
+
+Shape shape_of(const pspw_cell *c, int nb) {
+  const Projectors &P = c->proj;
+  Shape s;
+  s.nat = P.nat;
+  s.L = P.nproj / P.nat;
+  s.per = 2 * s.L;
+  s.npad = (P.nat + 15) / 16 * 16;
+  s.nsa = (P.nat + 7) / 8;
+  // bands per back-projection N tile: nbt*2L a multiple of 16, at most 128
+  int nmax = kMaxBackN / s.per;
+  while ((nmax * s.per) % 16) nmax--;
+  int nbt = std::min(nmax, nb);
+  while ((nbt * s.per) % 16) nbt++;
+  s.nbt = nbt;
+  s.ncolN = nbt * s.per;
+  s.nbtiles = (nb + nbt - 1) / nbt;
+  return s;
+}
+
+// Dynamic shared memory, raised where needed so that no more blocks fit on
+// an SM than its 512 TMEM columns can serve at once (an allocation would
+// otherwise wait for a resident block to finish).
+int block_smem(int need, int ncols) {
+  const int per_sm = 512 / ncols;
   const int floor_bytes = 233472 / (per_sm + 1) + 1024;
-  return std::max(stages, floor_bytes);
+  return std::max(need, floor_bytes);
+}
+
+int proj_smem(const Shape &s) {
+  const int nbr_max = 127 / s.per + 2;
+  const int raw = round16(nbr_max * 9 * 8) + 128;
+  return block_smem(kNTP * (2 * kTileBytes128 + s.npad * 128) + kNR * raw, tmem_cols(s.npad));
+}
+
+int back_smem(const Shape &s) {
+  return block_smem(kNTB * (2 * kTileBytes128 + s.ncolN * 128), tmem_cols(s.ncolN));
+}
+
+// splits of the projection's K range: enough blocks to fill the GPU once
+int proj_splits(pspw_cell *c, const Shape &s, int ngw, int nb, int *kg_out) {
+  const int mt = (nb * s.per + 127) / 128;
+  static int sms = 0;
+  if (!sms) {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    if (sms <= 0) sms = 148;
+  }
+  const int smem = proj_smem(s);
+  const int per_sm = std::max(1, std::min(233472 / (smem + 1024), 512 / (int)tmem_cols(s.npad)));
+  int nsplit = std::max(1, std::min((ngw + 63) / 64, per_sm * sms / mt));
+  int kg = (ngw + nsplit - 1) / nsplit;
+  kg = (kg + 7) / 8 * 8;
+  *kg_out = kg;
+  return (ngw + kg - 1) / kg;
+}
+
+template <int L>
+int launch_project(pspw_cell *c, const Shape &s, const float2 *psi, int ld, int ngw, int nb,
+                   float *part, int nsplit, int kg, float *wt) {
+  const Projectors &P = c->proj;
+  const int mt = (nb * s.per + 127) / 128;
+  const int smem = proj_smem(s);
+  PSPW_CUDA(cudaFuncSetAttribute(k_proj_tc<L>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+  k_proj_tc<L><<<dim3(mt, nsplit), kThreads, smem, c->stream>>>(
+      psi, ld, ngw, nb, P.d_etp, P.d_pkga32, s.nat, s.npad, kg, part, c->d_err);
+  const int total = s.nbtiles * s.nsa * s.nbt * L * 4;
+  k_proj_tc_wtiles<L><<<(total + 255) / 256, 256, 0, c->stream>>>(part, nsplit, nb, s.nat,
+                                                                   P.d_pw32, s.nbt, s.nsa, total,
+                                                                   wt);
+  c->kernel_launches += 2;
+  PSPW_CUDA(cudaGetLastError());
+  return PSPW_OK;
+}
+
+template <int L>
+int launch_back(pspw_cell *c, const Shape &s, const float *wt, int ngw, int nb, float2 *out,
+                int ldo, const float2 *in, int ldi, const float2 *xm2, int ldx, float a, float b,
+                float g) {
+  const int smem = back_smem(s);
+  PSPW_CUDA(
+      cudaFuncSetAttribute(k_backproj_tc<L>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+  dim3 grid((ngw + 127) / 128, s.nbtiles);
+  k_backproj_tc<L><<<grid, kThreads, smem, c->stream>>>(c->proj.d_etb, wt, s.nsa, ngw, nb, s.nbt,
+                                                        c->proj.d_pkga32, out, ldo, in, ldi, xm2,
+                                                        ldx, a, b, g, c->d_err);
+  c->kernel_launches++;
+  PSPW_CUDA(cudaGetLastError());
+  return PSPW_OK;
 }
 
 }  // namespace
 
 bool nl_tc_usable(const pspw_cell *c) {
   static const bool off = std::getenv("PSPW_NL_SIMT") != nullptr;
-  const Projectors &P = c->proj;
   if (c->nl_path == PSPW_NL_SIMT || (off && c->nl_path != PSPW_NL_TENSOR_CORE)) return false;
-  return P.nsp == 1 && P.nat >= 1 && P.nat <= 256 && P.nproj > 0 &&
-         P.nproj % P.nat == 0 && P.nproj / P.nat <= 4 && c->d_err != nullptr;
+  return fits(c->proj) && c->proj.d_etp && c->proj.d_etb && c->d_err;
 }
 
-int nl_tc_project(pspw_cell *c, const float2 *in, int ld, int ngw, int nb, float2 *wp,
-                  float *part, int max_split) {
-  const Projectors &P = c->proj;
-  const int nat = P.nat, L = P.nproj / P.nat;
-  const int npad = (nat + 15) / 16 * 16;
-  const int Mtot = nb * 2 * L;
-  const int mt = (Mtot + 127) / 128;
-  // split G so the grid covers the GPU about twice, at least 64 G per split
-  int nsplit = std::max(1, std::min((ngw + 63) / 64, (2 * 148 + mt - 1) / mt));
-  if (part) nsplit = std::max(1, std::min(nsplit, max_split));
-  int kg = (ngw + nsplit - 1) / nsplit;
-  kg = (kg + 7) / 8 * 8;
-  nsplit = (ngw + kg - 1) / kg;
-  if (!part) {
-    int rc = ws_reserve(c, kWsProjPart, sizeof(float) * (size_t)nsplit * Mtot * nat, (void **)&part);
-    if (rc) return rc;
-  }
-  const int smem = tile_smem(npad);
-  PSPW_CUDA(cudaFuncSetAttribute(k_proj_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
-  k_proj_tc<<<dim3(mt, nsplit), 128, smem, c->stream>>>(in, ld, ngw, nb, P.d_eigr32, c->basis.ngw,
-                                                        P.d_pkga32, L, nat, npad, kg, part,
-                                                        c->d_err);
-  k_proj_tc_reduce<<<(nb * P.nproj + 255) / 256, 256, 0, c->stream>>>(part, nsplit, nb, L, nat,
-                                                                      P.d_pw32, wp);
+int nl_tc_prepare(pspw_cell *c) {
+  Projectors &P = c->proj;
+  if (!fits(P) || P.d_etp) return PSPW_OK;
+  const int ngw = c->basis.ngw;
+  const int npad = (P.nat + 15) / 16 * 16, nsa = (P.nat + 7) / 8;
+  const int nst = (ngw + 7) / 8, ngt = (ngw + 127) / 128;
+  const size_t bp = (size_t)nst * npad * 128, bb = (size_t)ngt * nsa * 16384;
+  if (cudaMalloc(&P.d_etp, bp) != cudaSuccess || cudaMalloc(&P.d_etb, bb) != cudaSuccess)
+    return fail(PSPW_ERR_OOM, "cell_create: EIGR operand tiles");
+  P.tc_npad = npad;
+  const long long n1 = (long long)nst * npad * 4, n2 = (long long)ngt * nsa * 512;
+  k_build_etp<<<(unsigned)((n1 + 255) / 256), 256, 0, c->stream>>>(P.d_eigr32, ngw, P.nat, npad,
+                                                                   nst, P.d_etp);
+  k_build_etb<<<(unsigned)((n2 + 255) / 256), 256, 0, c->stream>>>(P.d_eigr32, ngw, P.nat, nsa,
+                                                                   ngt, P.d_etb);
   c->kernel_launches += 2;
   PSPW_CUDA(cudaGetLastError());
   return PSPW_OK;
 }
 
-int nl_tc_backproject(pspw_cell *c, const float2 *wp, int ngw, int nb, float2 *out, int ldo,
+size_t nl_tc_wtile_bytes(const pspw_cell *c, int nb) {
+  if (!fits(c->proj)) return 0;
+  const Shape s = shape_of(c, nb);
+  return (size_t)s.nbtiles * s.nsa * s.ncolN * 128;
+}
+
+int nl_tc_reserve(pspw_cell *c, int ngw, int nb, float **part, int *max_split, float **wt) {
+  const Shape s = shape_of(c, nb);
+  int kg = 0;
+  const int nsplit = proj_splits(c, s, ngw, nb, &kg);
+  int rc = ws_reserve(c, kWsProjPart, sizeof(float) * (size_t)nsplit * nb * s.per * s.nat,
+                      (void **)part);
+  if (rc) return rc;
+  rc = ws_reserve(c, kWsWTile, nl_tc_wtile_bytes(c, nb), (void **)wt);
+  if (rc) return rc;
+  *max_split = nsplit;
+  return PSPW_OK;
+}
+
+int nl_tc_project(pspw_cell *c, const float2 *psi, int ld, int ngw, int nb, float *part,
+                  int max_split, float *wt) {
+  const Shape s = shape_of(c, nb);
+  int kg = 0;
+  int nsplit = proj_splits(c, s, ngw, nb, &kg);
+  if (nsplit > max_split) {
+    nsplit = std::max(1, max_split);
+    kg = ((ngw + nsplit - 1) / nsplit + 7) / 8 * 8;
+    nsplit = (ngw + kg - 1) / kg;
+  }
+  switch (s.L) {
+    case 1: return launch_project<1>(c, s, psi, ld, ngw, nb, part, nsplit, kg, wt);
+    case 2: return launch_project<2>(c, s, psi, ld, ngw, nb, part, nsplit, kg, wt);
+    case 3: return launch_project<3>(c, s, psi, ld, ngw, nb, part, nsplit, kg, wt);
+    default: return launch_project<4>(c, s, psi, ld, ngw, nb, part, nsplit, kg, wt);
+  }
+}
+
+int nl_tc_backproject(pspw_cell *c, const float *wt, int ngw, int nb, float2 *out, int ldo,
                       const float2 *in, int ldi, const float2 *xm2, int ldx, float a, float b,
                       float g) {
-  const Projectors &P = c->proj;
-  const int L = P.nproj / P.nat, per = 2 * L;
-  // bands per N tile: nbt*2L a multiple of 16 and at most 256
-  int nmax = 256 / per;
-  while (nmax > 0 && (nmax * per) % 16) nmax--;
-  int nbt = std::min(nmax, nb);
-  while (nbt > 0 && (nbt * per) % 16) nbt++;
-  if (nbt < 1 || nbt * per > 256) return fail(PSPW_ERR_NOT_IMPL, "tensor-core back-projection: tile");
-  const int smem = tile_smem(nbt * per);
-  PSPW_CUDA(cudaFuncSetAttribute(k_backproj_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
-  dim3 grid((ngw + 127) / 128, (nb + nbt - 1) / nbt);
-  k_backproj_tc<<<grid, 128, smem, c->stream>>>(wp, P.nproj, ngw, nb, nbt, P.d_eigr32, c->basis.ngw,
-                                                P.d_pkga32, L, P.nat, out, ldo, in, ldi, xm2, ldx,
-                                                a, b, g, c->d_err);
-  c->kernel_launches++;
-  PSPW_CUDA(cudaGetLastError());
-  return PSPW_OK;
+  const Shape s = shape_of(c, nb);
+  switch (s.L) {
+    case 1: return launch_back<1>(c, s, wt, ngw, nb, out, ldo, in, ldi, xm2, ldx, a, b, g);
+    case 2: return launch_back<2>(c, s, wt, ngw, nb, out, ldo, in, ldi, xm2, ldx, a, b, g);
+    case 3: return launch_back<3>(c, s, wt, ngw, nb, out, ldo, in, ldi, xm2, ldx, a, b, g);
+    default: return launch_back<4>(c, s, wt, ngw, nb, out, ldo, in, ldi, xm2, ldx, a, b, g);
+  }
 }
 
 }  // namespace pspw

@@ -6,17 +6,27 @@
 namespace pspw {
 
 // True when the cell's projectors fit the tensor-core kernels (one species,
-// at most 256 atoms).
+// 1..256 atoms, at most 4 projectors per atom) and the kernels are selected.
 bool nl_tc_usable(const pspw_cell *c);
 
-// wp[b*nproj + a*L + lm] = WNL(lm) sum_G conj(EIGR(G,a)) PKG_A(lm,G) psi_b(G)
-// for the first ngw G of nb bands.  `part` holds max_split * 2*nb*nproj
-// floats (null: the cell's workspace).
-int nl_tc_project(pspw_cell *c, const float2 *psi, int ld, int ngw, int nb, float2 *wp,
-                  float *part, int max_split);
+// Builds the EIGR operand tiles of a cell whose projectors fit the kernels
+// (no-op otherwise).  Called once at cell creation.
+int nl_tc_prepare(pspw_cell *c);
 
-// out = a*(out + sum_{a,lm} EIGR PKG_A wp) + b*in + g*xm2 on the first ngw G.
-int nl_tc_backproject(pspw_cell *c, const float2 *wp, int ngw, int nb, float2 *out, int ldo,
+// Bytes of the projection operand tiles for nb bands.
+size_t nl_tc_wtile_bytes(const pspw_cell *c, int nb);
+
+// Scratch of nl_tc_project from the cell's workspaces: partial sums (at most
+// *max_split slices) and the projection operand tiles.
+int nl_tc_reserve(pspw_cell *c, int ngw, int nb, float **part, int *max_split, float **wt);
+
+// Projections of nb bands (first ngw G) into the operand tiles `wt`:
+// W(a,lm,b) = WNL(lm) sum_G conj(EIGR(G,a)) PKG_A(lm,G) psi_b(G).
+int nl_tc_project(pspw_cell *c, const float2 *psi, int ld, int ngw, int nb, float *part,
+                  int max_split, float *wt);
+
+// out = a*(out + sum_{a,lm} EIGR PKG_A W) + b*in + g*xm2 on the first ngw G.
+int nl_tc_backproject(pspw_cell *c, const float *wt, int ngw, int nb, float2 *out, int ldo,
                       const float2 *in, int ldi, const float2 *xm2, int ldx, float a, float b,
                       float g);
 

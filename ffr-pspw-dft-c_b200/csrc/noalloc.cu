@@ -31,6 +31,7 @@
 
 #include "common.cuh"
 #include "engine.h"
+#include "nl_tc.h"
 
 #define PSPW_NOALLOC_SCRATCH_BYTES (16u << 20)
 
@@ -79,7 +80,10 @@ extern "C" int pspw_apply_ham_block_dev_noalloc(pspw_cell *c, int prec, const vo
   const size_t cap = PSPW_NOALLOC_SCRATCH_BYTES;
   const size_t per_band = ((size_t)B.n3 * B.ncol + (size_t)B.n3 * B.n2 * B.nxa) * sc;
   const size_t slice = (size_t)nstates * c->proj.nproj * sc;  // one projection block
-  const size_t wp_bytes = up256(slice);
+  // FP32 on the tensor-core path: the projections as operand tiles
+  const size_t wt_bytes =
+      prec == PSPW_PREC_F32 && nl_tc_usable(c) ? up256(nl_tc_wtile_bytes(c, nstates)) : 0;
+  const size_t wp_bytes = up256(slice) + wt_bytes;
   // partial-sum slices: up to a quarter of the array, at least one
   int nsplit = slice ? (int)std::max<size_t>(1, std::min<size_t>(64, cap / 4 / slice)) : 1;
   auto fit_bands = [&](int ns) -> long long {
@@ -103,6 +107,7 @@ extern "C" int pspw_apply_ham_block_dev_noalloc(pspw_cell *c, int prec, const vo
   unsigned char *p = static_cast<unsigned char *>(base);
   ScratchPlan plan;
   plan.wp = p;
+  plan.wt = p + up256(slice);
   p += wp_bytes;
   plan.part = p;
   p += up256((size_t)nsplit * slice);

@@ -96,6 +96,62 @@ __device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity) {
   return false;
 }
 
+// As mbar_wait, for blocks whose warps wait on different barriers: gives up
+// as soon as another thread has raised *abort, and raises it on a timeout.
+__device__ __forceinline__ bool mbar_wait_abort(uint64_t *bar, uint32_t parity, int *abort) {
+  const uint32_t a = smem_addr(bar);
+  volatile int *ab = abort;
+  uint64_t t0 = 0;
+  for (uint32_t i = 0; i < kSpinLimit; i++) {
+    uint32_t done;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(done)
+        : "r"(a), "r"(parity)
+        : "memory");
+    if (done) return true;
+    if ((i & 63u) == 0 && *ab) return false;
+    if ((i & 1023u) == 0) {
+      const uint64_t t = globaltimer_ns();
+      if (i == 0) {
+        t0 = t;
+      } else if (t - t0 > kWaitNs) {
+        *ab = 1;
+        return false;
+      }
+    }
+  }
+  *ab = 1;
+  return false;
+}
+__device__ __forceinline__ void mbar_arrive(uint64_t *bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_addr(bar)) : "memory");
+}
+// arrive and add `bytes` to the transaction count the phase waits for
+__device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t *bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(bar)),
+               "r"(bytes)
+               : "memory");
+}
+// bulk copy global -> this block's shared memory, completing `bytes` of the
+// barrier's transaction count (both addresses 16-byte aligned, bytes % 16 == 0)
+__device__ __forceinline__ void bulk_g2s(void *dst, const void *src, uint32_t bytes,
+                                         uint64_t *bar) {
+  asm volatile(
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+          smem_addr(dst)),
+      "l"(src), "r"(bytes), "r"(smem_addr(bar))
+      : "memory");
+}
+// arrive on the barrier once this thread's earlier cp.async copies land
+// (the arrival counts against the barrier's expected count)
+__device__ __forceinline__ void cp_async_mbar_arrive_noinc(uint64_t *bar) {
+  asm volatile("cp.async.mbarrier.arrive.noinc.shared::cta.b64 [%0];" ::"r"(smem_addr(bar))
+               : "memory");
+}
+
 // ---- tensor memory
 __device__ __forceinline__ void tmem_alloc(uint32_t *dst_smem, uint32_t ncols) {
   asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
@@ -149,6 +205,38 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, float *v) {
   asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
 #pragma unroll
   for (int i = 0; i < 16; i++) v[i] = __uint_as_float(r[i]);
+}
+
+// x = hi + lo for four values, stored as one 16-byte core-matrix row each
+__device__ __forceinline__ void st_split4(unsigned char *hi, unsigned char *lo, uint32_t off,
+                                          float4 x) {
+  uint4 h, l;
+  split_tf32(x.x, h.x, l.x);
+  split_tf32(x.y, h.y, l.y);
+  split_tf32(x.z, h.z, l.z);
+  split_tf32(x.w, h.w, l.w);
+  *reinterpret_cast<uint4 *>(hi + off) = h;
+  *reinterpret_cast<uint4 *>(lo + off) = l;
+}
+
+// ---- asynchronous global -> shared copies (cp.async); `valid` false fills
+// the destination with zeros without reading the source
+__device__ __forceinline__ void cp_async8(void *dst, const void *src, bool valid) {
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;" ::"r"(smem_addr(dst)), "l"(src),
+               "r"(valid ? 8 : 0)
+               : "memory");
+}
+__device__ __forceinline__ void cp_async16(void *dst, const void *src, bool valid) {
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(smem_addr(dst)), "l"(src),
+               "r"(valid ? 16 : 0)
+               : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() {
+  asm volatile("cp.async.commit_group;" ::: "memory");
+}
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+  asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
 }
 
 // byte offset of element (row, k) in a K-major no-swizzle tile of BK fp32 per row

@@ -290,6 +290,17 @@ def test_fp32_tensor_core_si64_all_bands():
     assert np.array_equal(out, out2)  # fixed-order split-K reduction
 
 
+def test_fp32_tensor_core_fewer_plane_waves_than_the_cell(cfg0):
+    # the projection K range stops at ngw inside an 8-G operand tile
+    w, cell = cfg0
+    ngw = 2003
+    psi = np.asfortranarray(w["psi"][:ngw, :12].astype(np.complex64).astype(complex))
+    cell.set_nl_path(NL_TENSOR_CORE)
+    out = _hpsi32(cell, psi)
+    ref = O.apply_ham_block(oracle_cell(w), psi, w["veff"])
+    assert relmax(out, ref) < TOL32
+
+
 def test_tensor_core_path_refused_for_two_species():
     lat, pos = synth.si_diamond(1)
     b = basis_gamma(lat, 8.0, None, [5, 3], [pos[:5], pos[5:]])
