@@ -23,18 +23,23 @@
 //
 // Operands that do not depend on psi (both EIGR operands) are split into
 // TF32 hi/lo tiles once per cell, in the K-major no-swizzle layout of tc.cuh,
-// and reach shared memory as single bulk copies.  The reduction of the
-// projection writes W' in the same tile form, so the back-projection is a
-// GEMM fed by bulk copies alone.  The psi operand of the projection is built
-// on the fly.
+// and reach shared memory as single bulk copies.  The psi operand of the
+// projection is built on the fly by the row threads and stored straight into
+// tensor memory (the MMA reads A from TMEM), so it never passes through
+// shared memory.  The reduction of the projection writes W' as operand
+// tiles, so the back-projection is a GEMM fed by bulk copies alone.
 //
-// Both GEMM kernels are warp-specialised (192 threads):
-//   warps 0-3  one thread per row of the 128-row M tile: build A' tiles
-//              (projection) and run the epilogue (TMEM -> registers);
-//   warp 4     producer: cp.async of psi / PKG_A into a raw ring
-//              (projection) and the bulk copies of the fixed tiles;
-//   warp 5     one thread issues the MMAs of a K step once its operand slot
-//              is full and commits them to the slot's "empty" barrier.
+// Both GEMM kernels are warp-specialised (320 threads, 352 for the projection):
+//   warps 0-7  row threads: warp w serves TMEM lanes 32 (w % 4) .. + 31
+//              (rows of the 128-row M tile) and half w / 4 of the columns;
+//              they build the A' operand (projection) and run the epilogue;
+//   warp 8     producer: cp.async of psi / PKG_A into a raw ring
+//              (projection) or the bulk copies of the fixed tiles
+//              (back-projection);
+//   warp 9     one thread issues the MMAs of a K step once its operand slot
+//              is full and commits them to the slot's "empty" barrier;
+//   warp 10    (projection) one thread bulk-copies the EIGR tiles, so the
+//              raw producer never waits on the MMAs.
 // Slots are handed over with mbarriers only; there is no block-wide barrier
 // in the main loop.  Every wait is bounded and gives up as soon as any
 // thread of the block has given up; the block then raises the cell's error
@@ -56,15 +61,19 @@ constexpr int kBK = 16;                                 // fp32 of K per step
 constexpr int kTileBytes128 = 128 * kBK * 4;            // 128 rows x BK fp32
 constexpr uint32_t kLBO = 128, kSBO = (kBK / 4) * 128;  // core-matrix strides
 constexpr int kNTP = 4;                                 // operand slots, projection
-constexpr int kNTB = 3;                                 // operand slots, back-projection
+constexpr int kNTB = 2;                                 // operand slots, back-projection
 constexpr int kNR = 6;                                  // raw slots, projection
-constexpr int kThreads = 192;
+constexpr int kRowWarps = 8;                            // row / epilogue warps
+constexpr int kRowThreads = 32 * kRowWarps;
+constexpr int kThreads = kRowThreads + 64;              // + producer + MMA warps
+constexpr int kThreadsP = kThreads + 32;                // projection: + tile producer
 constexpr int kMaxBackN = 128;  // N tile of the back-projection
 
 __host__ __device__ constexpr int round16(int x) { return (x + 15) & ~15; }
 
+// TMEM columns to allocate for n: a power of two from 32 to 512
 __host__ __device__ constexpr uint32_t tmem_cols(int n) {
-  return n <= 32 ? 32u : (n <= 64 ? 64u : (n <= 128 ? 128u : 256u));
+  return n <= 32 ? 32u : (n <= 64 ? 64u : (n <= 128 ? 128u : (n <= 256 ? 256u : 512u)));
 }
 
 // The 3xTF32 MMAs of one K step (K = 16 as two K = 8 instructions).
@@ -84,8 +93,8 @@ __device__ __forceinline__ void issue_step(uint32_t tmem, uint32_t a_hi, uint32_
 
 // Barriers and state shared by the roles of one block.
 struct Sync {
-  uint64_t full[kNTP];   // A' tile written by the row threads (projection)
-  uint64_t bfull[kNTP];  // bulk-copied operands landed
+  uint64_t full[kNTP];   // projection: A' written by the row warps and EIGR landed
+  uint64_t bfull[kNTP];  // back-projection: bulk-copied operands landed
   uint64_t empty[kNTP];  // MMAs reading the slot finished
   uint64_t rfull[kNR];   // raw slot landed (projection)
   uint64_t rempty[kNR];  // raw slot consumed (projection)
@@ -107,7 +116,7 @@ __device__ __forceinline__ void open_block(Sync &sy, uint32_t ncols, int nt, int
     }
     for (int i = 0; i < nraw; i++) {
       tc::mbar_init(&sy.rfull[i], 32);
-      tc::mbar_init(&sy.rempty[i], 128);
+      tc::mbar_init(&sy.rempty[i], kRowWarps);
     }
     tc::mbar_init(&sy.done, 1);
     sy.abort = 0;
@@ -132,10 +141,20 @@ __device__ __forceinline__ void drain_bulk(Sync &sy, int issued, int nt) {
 }
 
 // ------------------------------------------------------------------ projection
-// grid (M tiles of 128 rows, K splits of ksplit_g G each); 192 threads.
+// grid (M tiles of 128 rows, K splits of ksplit_g G each, ksplit_g % 16 == 0);
+// kThreadsP threads.  One K step = 16 G = 32 fp32 of K = two EIGR tiles.
 // etp: per 8 G, [npad x 16] hi then lo.  part[split][m][a], m = b*2L + 2lm + p.
+//
+// The A' operand lives in tensor memory: D occupies columns [0, dcols) and
+// A' slot ts the 64 columns acol + 64 ts: hi of the step's 32 fp32 of K, then
+// lo.  Row thread (warp w, lane l) owns TMEM lane 32 (w % 4) + l = row
+// m - m0 and K half w / 4 (8 of the step's 16 G).  Slot ts is "ready" when
+// the 8 row warps have arrived and the EIGR bulk copy has landed.
+__host__ __device__ constexpr int proj_slots(int npad) { return tmem_cols(npad) <= 64 ? 3 : 2; }
+constexpr int kStepG = 16;  // G per projection step
+
 template <int L>
-__global__ void __launch_bounds__(kThreads) k_proj_tc(const float2 *__restrict__ psi, int ld,
+__global__ void __launch_bounds__(kThreadsP) k_proj_tc(const float2 *__restrict__ psi, int ld,
                                                       int ngw, int nb,
                                                       const float *__restrict__ etp,
                                                       const float *__restrict__ pkga, int nat,
@@ -143,8 +162,9 @@ __global__ void __launch_bounds__(kThreads) k_proj_tc(const float2 *__restrict__
                                                       float *__restrict__ part, int *err) {
   constexpr int per = 2 * L;
   constexpr int nbr_max = 127 / per + 2;  // bands a 128-row tile touches
-  constexpr int raw_psi = round16(nbr_max * 9 * 8);
-  constexpr int raw_bytes = raw_psi + 128;
+  constexpr int prow = kStepG + 1;        // raw psi row (float2), padded
+  constexpr int raw_psi = round16(nbr_max * prow * 8);
+  constexpr int raw_bytes = raw_psi + kStepG * 16;
   extern __shared__ __align__(1024) unsigned char sm[];
   __shared__ Sync sy;
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
@@ -153,109 +173,130 @@ __global__ void __launch_bounds__(kThreads) k_proj_tc(const float2 *__restrict__
   const int bfirst = m0 / per;
   const int nbr = min(Mtot - 1, m0 + 127) / per - bfirst + 1;
   const int gb = blockIdx.y * ksplit_g, ge = min(ngw, gb + ksplit_g);
-  const int nsteps = ge > gb ? (ge - gb + 7) / 8 : 0;
-  const uint32_t ebytes = (uint32_t)npad * 128;  // hi + lo EIGR tile of one step
-  const int slot_bytes = 2 * kTileBytes128 + (int)ebytes;
-  unsigned char *raw0 = sm + kNTP * slot_bytes;
-  const uint32_t ncols = tmem_cols(npad);
-  open_block(sy, ncols, kNTP, 128, kNR);
+  const int nsteps = ge > gb ? (ge - gb + kStepG - 1) / kStepG : 0;
+  const int nts = proj_slots(npad);
+  const uint32_t ebytes = (uint32_t)npad * 128;  // hi + lo EIGR tile of 8 G
+  unsigned char *raw0 = sm + nts * 2 * ebytes;
+  const uint32_t acol = tmem_cols(npad);
+  const uint32_t ncols = tmem_cols(acol + 64 * nts);
+  open_block(sy, ncols, nts, kRowWarps + 1, kNR);
 
-  if (warp < 4) {
-    // ---- A' rows: thread tid owns row m of every A' tile
-    const int m = m0 + tid;
+  if (warp < kRowWarps) {
+    // ---- A' rows
+    const int row = 32 * (warp & 3) + lane, half = warp >> 2;
+    const uint32_t lane_base = sy.tmem + ((uint32_t)(32 * (warp & 3)) << 16);
+    const int m = m0 + row;
     const bool mv = m < Mtot;
     const int bl = mv ? m / per - bfirst : 0;
     const int lm = (m % per) >> 1, p = m & 1;
     for (int k = 0; k < nsteps; k++) {
-      const int rs = k % kNR, ts = k % kNTP;
+      const int rs = k % kNR, ts = k % nts;
       if (!tc::mbar_wait_abort(&sy.rfull[rs], (k / kNR) & 1, &sy.abort)) break;
-      if (k >= kNTP && !tc::mbar_wait_abort(&sy.empty[ts], ((k / kNTP) - 1) & 1, &sy.abort))
-        break;
-      if (mv) {
-        const unsigned char *r = raw0 + rs * raw_bytes;
-        const float2 *rp = reinterpret_cast<const float2 *>(r) + bl * 9;
-        const float *rk = reinterpret_cast<const float *>(r + raw_psi);
-        unsigned char *a_hi = sm + ts * slot_bytes;
+      if (k >= nts && !tc::mbar_wait_abort(&sy.empty[ts], ((k / nts) - 1) & 1, &sy.abort)) break;
+      tc::fence_after_sync();
+      const unsigned char *r = raw0 + rs * raw_bytes;
+      const float2 *rp = reinterpret_cast<const float2 *>(r) + bl * prow + 8 * half;
+      const float *rk = reinterpret_cast<const float *>(r + raw_psi) + 32 * half + lm;
+      uint32_t hi[16], lo[16];
 #pragma unroll
-        for (int c = 0; c < 4; c++) {
-          const float2 v0 = rp[2 * c], v1 = rp[2 * c + 1];
-          const float f0 = rk[8 * c + lm], f1 = rk[8 * c + 4 + lm];
-          const float4 x = p ? make_float4(f0 * v0.y, -f0 * v0.x, f1 * v1.y, -f1 * v1.x)
-                             : make_float4(f0 * v0.x, f0 * v0.y, f1 * v1.x, f1 * v1.y);
-          tc::st_split4(a_hi, a_hi + kTileBytes128, tc::core_off<kBK>(tid, 4 * c), x);
-        }
+      for (int j = 0; j < 8; j++) {
+        const float2 v = rp[j];
+        const float f = rk[4 * j];
+        const float x0 = p ? f * v.y : f * v.x;
+        const float x1 = p ? -f * v.x : f * v.y;
+        tc::split_tf32(mv ? x0 : 0.f, hi[2 * j], lo[2 * j]);
+        tc::split_tf32(mv ? x1 : 0.f, hi[2 * j + 1], lo[2 * j + 1]);
       }
-      tc::fence_proxy_async();
-      tc::mbar_arrive(&sy.full[ts]);
-      tc::mbar_arrive(&sy.rempty[rs]);
+      const uint32_t ca = lane_base + acol + 64 * ts + 16 * half;
+      tc::tmem_st16(ca, hi);
+      tc::tmem_st16(ca + 32, lo);
+      tc::tmem_wait_st();
+      tc::fence_before_sync();
+      __syncwarp();  // one arrival per warp: the barriers count warps
+      if (lane == 0) {
+        tc::mbar_arrive(&sy.full[ts]);
+        tc::mbar_arrive(&sy.rempty[rs]);
+      }
     }
-    // ---- epilogue: D row m -> part (tcgen05.ld is warp-collective, so the
-    // decision is taken per warp and rows past Mtot load without storing)
+    // ---- epilogue: D row m, this warp's half of the atom columns -> part
+    // (tcgen05.ld is warp-collective: decided per warp, rows past Mtot load
+    // without storing)
     const bool ok = __all_sync(0xffffffffu, tc::mbar_wait_abort(&sy.done, 0, &sy.abort));
     tc::fence_after_sync();
     if (ok) {
       float *dst = part + ((size_t)blockIdx.y * Mtot + m) * nat;
-      float acc[16];
-      for (int c0 = 0; c0 < npad; c0 += 16) {
+      const int hw = npad / 2;
+      for (int c0 = half * hw; c0 < (half + 1) * hw; c0 += 8) {
+        uint32_t acc[8] = {0, 0, 0, 0, 0, 0, 0, 0};
         if (nsteps > 0) {
-          tc::tmem_ld16(sy.tmem + ((uint32_t)(32 * warp) << 16) + (uint32_t)c0, acc);
-        } else {
-#pragma unroll
-          for (int i = 0; i < 16; i++) acc[i] = 0.f;
+          tc::tmem_ld<8>(lane_base + (uint32_t)c0, acc);
+          tc::tmem_wait_ld();
         }
         if (mv) {
 #pragma unroll
-          for (int i = 0; i < 16; i++)
-            if (c0 + i < nat) dst[c0 + i] = acc[i];
+          for (int i = 0; i < 8; i++)
+            if (c0 + i < nat) dst[c0 + i] = __uint_as_float(acc[i]);
         }
       }
     }
-  } else if (warp == 4) {
-    // ---- producer: raw psi / PKG_A by all lanes, EIGR tiles by lane 0
-    int issued = 0;
+  } else if (warp == kRowWarps) {
+    // ---- raw producer: psi / PKG_A by all lanes
     for (int k = 0; k < nsteps; k++) {
-      const int rs = k % kNR, ts = k % kNTP;
+      const int rs = k % kNR;
       if (k >= kNR && !tc::mbar_wait_abort(&sy.rempty[rs], ((k / kNR) - 1) & 1, &sy.abort))
         break;
       unsigned char *r = raw0 + rs * raw_bytes;
       float2 *rp = reinterpret_cast<float2 *>(r);
       float *rk = reinterpret_cast<float *>(r + raw_psi);
-      const int g0 = gb + 8 * k;
-      for (int e = lane; e < nbr * 8; e += 32) {
-        const int b = e >> 3, g = g0 + (e & 7);
+      const int g0 = gb + kStepG * k;
+      for (int e = lane; e < nbr * kStepG; e += 32) {
+        const int b = e / kStepG, j = e % kStepG, g = g0 + j;
         const bool v = g < ge;
-        tc::cp_async8(rp + b * 9 + (e & 7), psi + (size_t)(bfirst + b) * ld + (v ? g : 0), v);
+        tc::cp_async8(rp + b * prow + j, psi + (size_t)(bfirst + b) * ld + (v ? g : 0), v);
       }
-      if (lane < 8) {
+      if (lane < kStepG) {
         const int g = g0 + lane;
         const bool v = g < ge;
         tc::cp_async16(rk + 4 * lane, pkga + (size_t)(v ? g : 0) * 4, v);
       }
       tc::cp_async_mbar_arrive_noinc(&sy.rfull[rs]);
-      if (lane == 0) {
-        if (k >= kNTP && !tc::mbar_wait_abort(&sy.empty[ts], ((k / kNTP) - 1) & 1, &sy.abort))
-          break;
-        tc::mbar_arrive_expect_tx(&sy.bfull[ts], ebytes);
-        tc::bulk_g2s(sm + ts * slot_bytes + 2 * kTileBytes128,
-                     etp + (size_t)(gb / 8 + k) * (ebytes / 4), ebytes, &sy.bfull[ts]);
-        issued = k + 1;
-      }
     }
     tc::cp_async_wait<0>();
-    if (lane == 0) drain_bulk(sy, issued, kNTP);
+  } else if (warp == kRowWarps + 2) {
+    // ---- tile producer: two EIGR tiles (one bulk copy) per step
+    if (lane == 0) {
+      int issued = 0;
+      for (int k = 0; k < nsteps; k++) {
+        const int ts = k % nts;
+        if (k >= nts && !tc::mbar_wait_abort(&sy.empty[ts], ((k / nts) - 1) & 1, &sy.abort))
+          break;
+        tc::mbar_arrive_expect_tx(&sy.full[ts], 2 * ebytes);
+        tc::bulk_g2s(sm + ts * 2 * ebytes, etp + (size_t)(gb / 8 + 2 * k) * (ebytes / 4),
+                     2 * ebytes, &sy.full[ts]);
+        issued = k + 1;
+      }
+      // let the copies still in flight land before the block can exit
+      for (int k = max(0, issued - nts); k < issued; k++)
+        tc::mbar_wait(&sy.full[k % nts], (k / nts) & 1);
+    }
   } else if (lane == 0) {
     // ---- MMA issuer
     const uint32_t idesc = tc::idesc_tf32(128, npad);
     for (int k = 0; k < nsteps; k++) {
-      const int ts = k % kNTP;
-      const uint32_t par = (k / kNTP) & 1;
-      if (!tc::mbar_wait_abort(&sy.bfull[ts], par, &sy.abort) ||
-          !tc::mbar_wait_abort(&sy.full[ts], par, &sy.abort))
-        break;
+      const int ts = k % nts;
+      if (!tc::mbar_wait_abort(&sy.full[ts], (k / nts) & 1, &sy.abort)) break;
       tc::fence_after_sync();
-      const uint32_t a = tc::smem_addr(sm + ts * slot_bytes);
-      issue_step(sy.tmem, a, a + kTileBytes128, a + 2 * kTileBytes128,
-                 a + 2 * kTileBytes128 + npad * 64, idesc, k == 0);
+      const uint32_t b = tc::smem_addr(sm + ts * 2 * ebytes);
+      const uint32_t a = sy.tmem + acol + 64 * ts;
+#pragma unroll
+      for (int s = 0; s < 4; s++) {
+        const uint32_t bt = b + (s >> 1) * ebytes + (s & 1) * 256;
+        const uint64_t bh = tc::sdesc(bt, kLBO, kSBO);
+        const uint64_t bl = tc::sdesc(bt + npad * 64, kLBO, kSBO);
+        tc::mma_tf32_ts(sy.tmem, a + 8 * s, bh, idesc, (k == 0 && s == 0) ? 0u : 1u);
+        tc::mma_tf32_ts(sy.tmem, a + 8 * s, bl, idesc, 1u);
+        tc::mma_tf32_ts(sy.tmem, a + 32 + 8 * s, bh, idesc, 1u);
+      }
       tc::mma_commit(&sy.empty[ts]);
     }
     tc::mma_commit(&sy.done);  // arrives once every MMA issued above has finished
@@ -266,16 +307,18 @@ __global__ void __launch_bounds__(kThreads) k_proj_tc(const float2 *__restrict__
 // Reduction of the projection slices, written as the B' operand tiles of the
 // back-projection: tile (band tile bt, atom step s) holds ncolN = nbt*2L rows
 // x 16 fp32 (8 atoms x re/im), hi then lo.  Every element of every tile is
-// written (zeros outside nb x nat).  One thread per (bt, s, band, lm, pair of
-// atoms); the slices are summed in a fixed order.
+// written (zeros outside nb x nat).  One warp per (bt, s, band, lm, pair of
+// atoms): lane l sums slices l, l+32, ... and a fixed shuffle tree adds the
+// lanes, so the result does not depend on scheduling.
 template <int L>
 __global__ void k_proj_tc_wtiles(const float *__restrict__ part, int nsplit, int nb, int nat,
                                  const float *__restrict__ w, int nbt, int nsa, int total,
                                  float *__restrict__ wt) {
   constexpr int per = 2 * L;
-  const int idx = blockIdx.x * blockDim.x + threadIdx.x;
-  if (idx >= total) return;
-  int t = idx;
+  const int item = (int)((blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5);
+  const int lane = threadIdx.x & 31;
+  if (item >= total) return;
+  int t = item;
   const int c = t & 3;
   t >>= 2;
   const int lm = t % L;
@@ -286,36 +329,62 @@ __global__ void k_proj_tc_wtiles(const float *__restrict__ part, int nsplit, int
   const int bt = t / nsa;
   const int b = bt * nbt + bl;
   const int Mtot = nb * per;
-  float2 W[2];
-#pragma unroll
-  for (int q = 0; q < 2; q++) {
-    const int a = 8 * s + 2 * c + q;
-    float re = 0.f, im = 0.f;
-    if (b < nb && a < nat) {
-      const int mre = b * per + 2 * lm;
-      for (int sl = 0; sl < nsplit; sl++) {
-        re += part[((size_t)sl * Mtot + mre) * nat + a];
-        im += part[((size_t)sl * Mtot + mre + 1) * nat + a];
+  const int a0 = 8 * s + 2 * c;
+  // x = (Re, Im) of atom a0, (Re, Im) of atom a0 + 1
+  float x[4] = {0.f, 0.f, 0.f, 0.f};
+  if (b < nb) {
+    const int mre = b * per + 2 * lm;
+    for (int sl = lane; sl < nsplit; sl += 32) {
+      const float *p0 = part + ((size_t)sl * Mtot + mre) * nat;
+      const float *p1 = p0 + nat;
+      if (a0 < nat) {
+        x[0] += p0[a0];
+        x[1] += p1[a0];
       }
-      const float wl = w[a * L + lm];
-      re *= wl;
-      im *= wl;
+      if (a0 + 1 < nat) {
+        x[2] += p0[a0 + 1];
+        x[3] += p1[a0 + 1];
+      }
     }
-    W[q] = make_float2(re, im);
   }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1)
+#pragma unroll
+    for (int q = 0; q < 4; q++) x[q] += __shfl_xor_sync(0xffffffffu, x[q], o);
+  if (lane != 0) return;
+  const float w0 = a0 < nat ? w[a0 * L + lm] : 0.f;
+  const float w1 = a0 + 1 < nat ? w[(a0 + 1) * L + lm] : 0.f;
+  const float2 W0 = make_float2(w0 * x[0], w0 * x[1]), W1 = make_float2(w1 * x[2], w1 * x[3]);
   const int ncolN = nbt * per;
   unsigned char *hi = reinterpret_cast<unsigned char *>(wt + ((size_t)bt * nsa + s) * ncolN * 32);
   unsigned char *lo = hi + ncolN * 64;
   const int r = bl * per + 2 * lm;
-  tc::st_split4(hi, lo, tc::core_off<kBK>(r, 4 * c),
-                make_float4(W[0].x, -W[0].y, W[1].x, -W[1].y));
-  tc::st_split4(hi, lo, tc::core_off<kBK>(r + 1, 4 * c),
-                make_float4(W[0].y, W[0].x, W[1].y, W[1].x));
+  tc::st_split4(hi, lo, tc::core_off<kBK>(r, 4 * c), make_float4(W0.x, -W0.y, W1.x, -W1.y));
+  tc::st_split4(hi, lo, tc::core_off<kBK>(r + 1, 4 * c), make_float4(W0.y, W0.x, W1.y, W1.x));
 }
 
 // ------------------------------------------------------------------ back-projection
-// grid (G tiles of 128, band tiles of nbt); 192 threads.
+// The 2L TMEM columns of one band (warp-collective).
+template <int per>
+__device__ __forceinline__ void ld_band(uint32_t taddr, uint32_t *v) {
+  if constexpr (per == 8) {
+    tc::tmem_ld<8>(taddr, v);
+  } else if constexpr (per == 4) {
+    tc::tmem_ld<4>(taddr, v);
+  } else if constexpr (per == 2) {
+    tc::tmem_ld<2>(taddr, v);
+  } else {
+    tc::tmem_ld<2>(taddr, v);
+    tc::tmem_ld<2>(taddr + 2, v + 2);
+    tc::tmem_ld<2>(taddr + 4, v + 4);
+  }
+  tc::tmem_wait_ld();
+}
+
+// grid (G tiles of 128, band tiles of nbt); kThreads threads.
 // etb: per (G tile, 8 atoms), [128 x 16] hi then lo.  wt: see k_proj_tc_wtiles.
+// Epilogue thread (warp w, lane l): G row 32 (w % 4) + l, bands of half w / 4
+// of the band tile.
 template <int L>
 __global__ void __launch_bounds__(kThreads) k_backproj_tc(
     const float *__restrict__ etb, const float *__restrict__ wt, int nsa, int ngw, int nb, int nbt,
@@ -328,13 +397,13 @@ __global__ void __launch_bounds__(kThreads) k_backproj_tc(
   const int gt = blockIdx.x, bt = blockIdx.y;
   const int g0 = gt * 128, b0 = bt * nbt;
   const int nbb = min(nbt, nb - b0);
-  const int ncolN = nbt * per;  // a multiple of 16, <= 128
+  const int ncolN = nbt * per;  // a multiple of 16, <= 128; nbt is even
   const uint32_t abytes = 2 * kTileBytes128, bbytes = (uint32_t)ncolN * 128;
   const int slot_bytes = (int)(abytes + bbytes);
   const uint32_t ncols = tmem_cols(ncolN);
   open_block(sy, ncols, kNTB, 1, 0);
 
-  if (warp == 4) {
+  if (warp == kRowWarps) {
     if (lane == 0) {
       int issued = 0;
       for (int k = 0; k < nsa; k++) {
@@ -350,7 +419,7 @@ __global__ void __launch_bounds__(kThreads) k_backproj_tc(
       }
       drain_bulk(sy, issued, kNTB);
     }
-  } else if (warp == 5) {
+  } else if (warp == kRowWarps + 1) {
     if (lane == 0) {
       const uint32_t idesc = tc::idesc_tf32(128, ncolN);
       for (int k = 0; k < nsa; k++) {
@@ -365,51 +434,59 @@ __global__ void __launch_bounds__(kThreads) k_backproj_tc(
       tc::mma_commit(&sy.done);
     }
   } else {
-    // ---- epilogue: this thread owns G row g of the warp's 32-lane slice
+    // ---- epilogue
+    const int row = 32 * (warp & 3) + lane, half = warp >> 2;
+    const uint32_t lane_base = sy.tmem + ((uint32_t)(32 * (warp & 3)) << 16);
+    const int g = g0 + row;
+    const bool gv = g < ngw;
+    const int nbh = nbt / 2;
+    const int bstart = half * nbh;
+    float pk[4] = {0.f, 0.f, 0.f, 0.f};
+    if (gv) {
+      const float4 p4 = *reinterpret_cast<const float4 *>(pkga + (size_t)g * 4);
+      pk[0] = p4.x;
+      pk[1] = p4.y;
+      pk[2] = p4.z;
+      pk[3] = p4.w;
+    }
+    // the first band's operands are fetched while the MMAs run
+    auto fetch = [&](int j, float2 &h, float2 &u, float2 &x) {
+      const int bl = bstart + j;
+      if (gv && bl < nbb) {
+        const size_t bb = (size_t)(b0 + bl);
+        h = out[bb * ldo + g];
+        if (cb != 0.f) u = in[bb * ldi + g];
+        if (cg != 0.f) x = xm2[bb * ldx + g];
+      }
+    };
+    float2 h = make_float2(0.f, 0.f), u = h, x = h;
+    fetch(0, h, u, x);
     const bool ok = __all_sync(0xffffffffu, tc::mbar_wait_abort(&sy.done, 0, &sy.abort));
     tc::fence_after_sync();
     if (ok) {
-      const int g = g0 + tid;
-      float pk[4] = {0.f, 0.f, 0.f, 0.f};
-      if (g < ngw) {
-        const float4 p4 = *reinterpret_cast<const float4 *>(pkga + (size_t)g * 4);
-        pk[0] = p4.x;
-        pk[1] = p4.y;
-        pk[2] = p4.z;
-        pk[3] = p4.w;
-      }
-      float acc[16];
-      float accr = 0.f, acci = 0.f;
-      for (int c0 = 0; c0 < ncolN; c0 += 16) {
-        tc::tmem_ld16(sy.tmem + ((uint32_t)(32 * warp) << 16) + (uint32_t)c0, acc);
+      for (int j = 0; j < nbh; j++) {
+        const float2 hc = h, uc = u, xc = x;
+        if (j + 1 < nbh) fetch(j + 1, h, u, x);
+        uint32_t v[per];
+        ld_band<per>(lane_base + (uint32_t)((bstart + j) * per), v);
+        float accr = 0.f, acci = 0.f;
 #pragma unroll
-        for (int i = 0; i < 16; i++) {
-          const int col = c0 + i;
-          const int cc = col % per;
-          if (cc & 1)
-            acci += pk[cc >> 1] * acc[i];
-          else
-            accr += pk[cc >> 1] * acc[i];
-          if (cc == per - 1) {
-            const int bl = col / per;
-            if (bl < nbb && g < ngw) {
-              const size_t bb = (size_t)(b0 + bl);
-              const float2 h = out[bb * ldo + g];
-              float rr = ca * (h.x + accr), ii = ca * (h.y + acci);
-              if (cb != 0.f) {
-                const float2 u = in[bb * ldi + g];
-                rr += cb * u.x;
-                ii += cb * u.y;
-              }
-              if (cg != 0.f) {
-                const float2 u = xm2[bb * ldx + g];
-                rr += cg * u.x;
-                ii += cg * u.y;
-              }
-              out[bb * ldo + g] = make_float2(rr, ii);
-            }
-            accr = acci = 0.f;
+        for (int l = 0; l < L; l++) {
+          accr += pk[l] * __uint_as_float(v[2 * l]);
+          acci += pk[l] * __uint_as_float(v[2 * l + 1]);
+        }
+        const int bl = bstart + j;
+        if (gv && bl < nbb) {
+          float rr = ca * (hc.x + accr), ii = ca * (hc.y + acci);
+          if (cb != 0.f) {
+            rr += cb * uc.x;
+            ii += cb * uc.y;
           }
+          if (cg != 0.f) {
+            rr += cg * xc.x;
+            ii += cg * xc.y;
+          }
+          out[(size_t)(b0 + bl) * ldo + g] = make_float2(rr, ii);
         }
       }
     }
@@ -501,10 +578,14 @@ int block_smem(int need, int ncols) {
   return std::max(need, floor_bytes);
 }
 
+int proj_tmem_cols(const Shape &s) {
+  return tmem_cols(tmem_cols(s.npad) + 64 * proj_slots(s.npad));
+}
+
 int proj_smem(const Shape &s) {
   const int nbr_max = 127 / s.per + 2;
-  const int raw = round16(nbr_max * 9 * 8) + 128;
-  return block_smem(kNTP * (2 * kTileBytes128 + s.npad * 128) + kNR * raw, tmem_cols(s.npad));
+  const int raw = round16(nbr_max * (kStepG + 1) * 8) + kStepG * 16;
+  return block_smem(proj_slots(s.npad) * 2 * s.npad * 128 + kNR * raw, proj_tmem_cols(s));
 }
 
 int back_smem(const Shape &s) {
@@ -522,10 +603,10 @@ int proj_splits(pspw_cell *c, const Shape &s, int ngw, int nb, int *kg_out) {
     if (sms <= 0) sms = 148;
   }
   const int smem = proj_smem(s);
-  const int per_sm = std::max(1, std::min(233472 / (smem + 1024), 512 / (int)tmem_cols(s.npad)));
+  const int per_sm = std::max(1, std::min(233472 / (smem + 1024), 512 / proj_tmem_cols(s)));
   int nsplit = std::max(1, std::min((ngw + 63) / 64, per_sm * sms / mt));
   int kg = (ngw + nsplit - 1) / nsplit;
-  kg = (kg + 7) / 8 * 8;
+  kg = (kg + kStepG - 1) / kStepG * kStepG;
   *kg_out = kg;
   return (ngw + kg - 1) / kg;
 }
@@ -537,12 +618,11 @@ int launch_project(pspw_cell *c, const Shape &s, const float2 *psi, int ld, int 
   const int mt = (nb * s.per + 127) / 128;
   const int smem = proj_smem(s);
   PSPW_CUDA(cudaFuncSetAttribute(k_proj_tc<L>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
-  k_proj_tc<L><<<dim3(mt, nsplit), kThreads, smem, c->stream>>>(
+  k_proj_tc<L><<<dim3(mt, nsplit), kThreadsP, smem, c->stream>>>(
       psi, ld, ngw, nb, P.d_etp, P.d_pkga32, s.nat, s.npad, kg, part, c->d_err);
-  const int total = s.nbtiles * s.nsa * s.nbt * L * 4;
-  k_proj_tc_wtiles<L><<<(total + 255) / 256, 256, 0, c->stream>>>(part, nsplit, nb, s.nat,
-                                                                   P.d_pw32, s.nbt, s.nsa, total,
-                                                                   wt);
+  const int total = s.nbtiles * s.nsa * s.nbt * L * 4;  // one warp each
+  k_proj_tc_wtiles<L><<<(total + 7) / 8, 256, 0, c->stream>>>(part, nsplit, nb, s.nat, P.d_pw32,
+                                                              s.nbt, s.nsa, total, wt);
   c->kernel_launches += 2;
   PSPW_CUDA(cudaGetLastError());
   return PSPW_OK;
@@ -577,7 +657,9 @@ int nl_tc_prepare(pspw_cell *c) {
   if (!fits(P) || P.d_etp) return PSPW_OK;
   const int ngw = c->basis.ngw;
   const int npad = (P.nat + 15) / 16 * 16, nsa = (P.nat + 7) / 8;
-  const int nst = (ngw + 7) / 8, ngt = (ngw + 127) / 128;
+  // projection tiles: every 8 G of the sphere, rounded up to whole steps of
+  // kStepG G (the tail tiles hold zeros)
+  const int nst = (ngw + kStepG - 1) / kStepG * (kStepG / 8), ngt = (ngw + 127) / 128;
   const size_t bp = (size_t)nst * npad * 128, bb = (size_t)ngt * nsa * 16384;
   if (cudaMalloc(&P.d_etp, bp) != cudaSuccess || cudaMalloc(&P.d_etb, bb) != cudaSuccess)
     return fail(PSPW_ERR_OOM, "cell_create: EIGR operand tiles");
@@ -618,7 +700,7 @@ int nl_tc_project(pspw_cell *c, const float2 *psi, int ld, int ngw, int nb, floa
   int nsplit = proj_splits(c, s, ngw, nb, &kg);
   if (nsplit > max_split) {
     nsplit = std::max(1, max_split);
-    kg = ((ngw + nsplit - 1) / nsplit + 7) / 8 * 8;
+    kg = ((ngw + nsplit - 1) / nsplit + kStepG - 1) / kStepG * kStepG;
     nsplit = (ngw + kg - 1) / kg;
   }
   switch (s.L) {

@@ -16,8 +16,8 @@
 // (bits 15, 16 = 0), N >> 3 in bits [17,23), M >> 4 in bits [24,29).
 //
 // Every wait on a barrier is bounded: after about a second (or kSpinLimit
-// polls) it gives up and reports failure, so a kernel can flag the error and return instead of
-// hanging the GPU.
+// polls) it gives up and reports failure, so a kernel can flag the error and
+// return instead of hanging the GPU.
 #pragma once
 
 #include <cstdint>
@@ -45,16 +45,13 @@ __device__ __forceinline__ uint64_t sdesc(uint32_t saddr, uint32_t lbo, uint32_t
   return d;                // layout type 0: no swizzle
 }
 
-__device__ __forceinline__ uint32_t to_tf32(float x) {
-  uint32_t r;
-  asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(x));
-  return r;
-}
-
-// x = hi + lo with hi and lo both representable in TF32 (3xTF32 split)
+// x = hi + lo exactly, hi = x with the 13 low mantissa bits cleared (a TF32
+// value).  The tensor core reads only the TF32 part of lo, so the pair
+// carries x to about 2^-20 relative (3xTF32 split; the lo*lo product is
+// dropped, which is of the same order).
 __device__ __forceinline__ void split_tf32(float x, uint32_t &hi, uint32_t &lo) {
-  hi = to_tf32(x);
-  lo = to_tf32(x - __uint_as_float(hi));
+  hi = __float_as_uint(x) & 0xffffe000u;
+  lo = __float_as_uint(x - __uint_as_float(hi));
 }
 
 // ---- mbarrier
@@ -69,29 +66,30 @@ __device__ __forceinline__ uint64_t globaltimer_ns() {
   asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
   return t;
 }
-// True when the phase with the given parity has completed.  Bounded: gives up
+__device__ __forceinline__ bool mbar_try(uint32_t a, uint32_t parity) {
+  uint32_t done;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+      "selp.u32 %0, 1, 0, p;\n\t}"
+      : "=r"(done)
+      : "r"(a), "r"(parity)
+      : "memory");
+  return done != 0;
+}
+// True when the phase with the given parity has completed.  Bounded: after
+// kFastPolls plain polls it keeps polling against the clock and gives up
 // (false) after about kWaitNs of wall time or kSpinLimit polls.
 constexpr uint64_t kWaitNs = 1000000000ull;
+constexpr uint32_t kFastPolls = 64;
 __device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity) {
   const uint32_t a = smem_addr(bar);
-  uint64_t t0 = 0;
+  for (uint32_t i = 0; i < kFastPolls; i++)
+    if (mbar_try(a, parity)) return true;
+  const uint64_t t0 = globaltimer_ns();
   for (uint32_t i = 0; i < kSpinLimit; i++) {
-    uint32_t done;
-    asm volatile(
-        "{\n\t.reg .pred p;\n\t"
-        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
-        "selp.u32 %0, 1, 0, p;\n\t}"
-        : "=r"(done)
-        : "r"(a), "r"(parity)
-        : "memory");
-    if (done) return true;
-    if ((i & 1023u) == 0) {
-      const uint64_t t = globaltimer_ns();
-      if (i == 0)
-        t0 = t;
-      else if (t - t0 > kWaitNs)
-        return false;
-    }
+    if (mbar_try(a, parity)) return true;
+    if ((i & 1023u) == 1023u && globaltimer_ns() - t0 > kWaitNs) return false;
   }
   return false;
 }
@@ -100,27 +98,16 @@ __device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity) {
 // as soon as another thread has raised *abort, and raises it on a timeout.
 __device__ __forceinline__ bool mbar_wait_abort(uint64_t *bar, uint32_t parity, int *abort) {
   const uint32_t a = smem_addr(bar);
+  for (uint32_t i = 0; i < kFastPolls; i++)
+    if (mbar_try(a, parity)) return true;
   volatile int *ab = abort;
-  uint64_t t0 = 0;
+  const uint64_t t0 = globaltimer_ns();
   for (uint32_t i = 0; i < kSpinLimit; i++) {
-    uint32_t done;
-    asm volatile(
-        "{\n\t.reg .pred p;\n\t"
-        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
-        "selp.u32 %0, 1, 0, p;\n\t}"
-        : "=r"(done)
-        : "r"(a), "r"(parity)
-        : "memory");
-    if (done) return true;
-    if ((i & 63u) == 0 && *ab) return false;
-    if ((i & 1023u) == 0) {
-      const uint64_t t = globaltimer_ns();
-      if (i == 0) {
-        t0 = t;
-      } else if (t - t0 > kWaitNs) {
-        *ab = 1;
-        return false;
-      }
+    if (mbar_try(a, parity)) return true;
+    if ((i & 63u) == 63u && *ab) return false;
+    if ((i & 1023u) == 1023u && globaltimer_ns() - t0 > kWaitNs) {
+      *ab = 1;
+      return false;
     }
   }
   *ab = 1;
@@ -183,6 +170,58 @@ __device__ __forceinline__ void mma_tf32(uint32_t d_tmem, uint64_t a_desc, uint6
       "setp.ne.b32 p, %4, 0;\n\t"
       "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, p;\n\t}" ::"r"(d_tmem),
       "l"(a_desc), "l"(b_desc), "r"(idesc), "r"(accumulate));
+}
+// D (tmem) (+)= A (tmem) * B (smem)^T, issued by one thread; A is 128 lanes
+// (rows) x K consecutive 32-bit columns
+__device__ __forceinline__ void mma_tf32_ts(uint32_t d_tmem, uint32_t a_tmem, uint64_t b_desc,
+                                            uint32_t idesc, uint32_t accumulate) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "setp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::tf32 [%0], [%1], %2, %3, p;\n\t}" ::"r"(d_tmem),
+      "r"(a_tmem), "l"(b_desc), "r"(idesc), "r"(accumulate));
+}
+// 8 consecutive 32-bit columns of this thread's TMEM lane (warp-collective;
+// complete with tmem_wait_st)
+__device__ __forceinline__ void tmem_st8(uint32_t taddr, const uint32_t *v) {
+  asm volatile(
+      "tcgen05.st.sync.aligned.32x32b.x8.b32 [%0], {%1,%2,%3,%4,%5,%6,%7,%8};" ::"r"(taddr),
+      "r"(v[0]), "r"(v[1]), "r"(v[2]), "r"(v[3]), "r"(v[4]), "r"(v[5]), "r"(v[6]), "r"(v[7])
+      : "memory");
+}
+__device__ __forceinline__ void tmem_st16(uint32_t taddr, const uint32_t *v) {
+  asm volatile(
+      "tcgen05.st.sync.aligned.32x32b.x16.b32 [%0], {%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,"
+      "%14,%15,%16};" ::"r"(taddr),
+      "r"(v[0]), "r"(v[1]), "r"(v[2]), "r"(v[3]), "r"(v[4]), "r"(v[5]), "r"(v[6]), "r"(v[7]),
+      "r"(v[8]), "r"(v[9]), "r"(v[10]), "r"(v[11]), "r"(v[12]), "r"(v[13]), "r"(v[14]), "r"(v[15])
+      : "memory");
+}
+__device__ __forceinline__ void tmem_wait_st() {
+  asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory");
+}
+// N (2, 4 or 8) consecutive 32-bit columns of this thread's TMEM lane
+// (warp-collective; complete with tmem_wait_ld)
+template <int N>
+__device__ __forceinline__ void tmem_ld(uint32_t taddr, uint32_t *r) {
+  if constexpr (N == 2) {
+    asm volatile("tcgen05.ld.sync.aligned.32x32b.x2.b32 {%0,%1}, [%2];"
+                 : "=r"(r[0]), "=r"(r[1])
+                 : "r"(taddr));
+  } else if constexpr (N == 4) {
+    asm volatile("tcgen05.ld.sync.aligned.32x32b.x4.b32 {%0,%1,%2,%3}, [%4];"
+                 : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3])
+                 : "r"(taddr));
+  } else {
+    static_assert(N == 8, "tmem_ld: 2, 4 or 8 columns");
+    asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
+                 : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]),
+                   "=r"(r[6]), "=r"(r[7])
+                 : "r"(taddr));
+  }
+}
+__device__ __forceinline__ void tmem_wait_ld() {
+  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
 }
 // arrive on the barrier when all previously issued MMAs of this thread finish
 __device__ __forceinline__ void mma_commit(uint64_t *bar) {
