@@ -149,15 +149,24 @@ __device__ __forceinline__ void inv_fwd_stepB_v(T *base, Lines L, const T *w,
     const int l = it % L.nl, k = it / L.nl;
     T *line = base + L(l);
     const R *vr = vrows + (size_t)l * vld + N1 * k;
+    // the N1 potential values of the block, in 16-byte loads where the row
+    // segment allows (one sector per thread instead of N1 lookups)
+    alignas(16) R s[N1];
+    if constexpr ((N1 * sizeof(R)) % 16 == 0) {
+      constexpr int NV = N1 * sizeof(R) / 16;
+      const uint4 *vv = reinterpret_cast<const uint4 *>(vr);
+#pragma unroll
+      for (int q = 0; q < NV; q++) reinterpret_cast<uint4 *>(s)[q] = __ldg(vv + q);
+    } else {
+#pragma unroll
+      for (int i = 0; i < N1; i++) s[i] = vr[i];
+    }
     T v[N1];
 #pragma unroll
     for (int i = 0; i < N1; i++) v[i] = line[i + N1 * k];
     RDft<N1, +1>::run(v);
 #pragma unroll
-    for (int i = 0; i < N1; i++) {
-      const R s = vr[i];
-      v[i] = mk<T>(s * v[i].x, s * v[i].y);
-    }
+    for (int i = 0; i < N1; i++) v[i] = mk<T>(s[i] * v[i].x, s[i] * v[i].y);
     RDft<N1, -1>::run(v);
     if (k) {
 #pragma unroll
