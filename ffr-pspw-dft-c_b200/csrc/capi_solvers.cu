@@ -254,7 +254,7 @@ int pspw_eval_rho_psi(pspw_cell *c, double *rhoe, const double *eigvec, int ld, 
   PSPW_CUDA(cudaMemcpyAsync(dw, wband.data(), sizeof(double) * nx, cudaMemcpyHostToDevice, c->stream));
   PSPW_CUDA(cudaMemcpyAsync(drho, rhoe, sizeof(double) * B.nnr, cudaMemcpyHostToDevice, c->stream));
   const FastGeo g{B.ncol, B.nxa, B.d_col_start, B.d_sg_ig, B.d_sg_z, B.d_sg_col, B.d_xa_list,
-                  B.d_col_x, B.d_col_y};
+                  B.d_col_x, B.d_col_y, B.d_xa_of_x};
   if ((rc = rho_fast<double>(c, g, dX, ld, m, nx, dw, drho))) return rc;
   PSPW_CUDA(cudaMemcpyAsync(rhoe, drho, sizeof(double) * B.nnr, cudaMemcpyDeviceToHost, c->stream));
   if ((rc = sync(c))) return rc;

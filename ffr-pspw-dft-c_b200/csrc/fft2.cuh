@@ -177,6 +177,78 @@ __device__ __forceinline__ void inv_fwd_stepB_v(T *base, Lines L, const T *w,
   }
 }
 
+// The first (inverse) and last (forward) x steps of the plane kernel, which
+// move between two views of one shared buffer: the compact view holds only
+// the active x positions of each row (row stride la), the full view all NX
+// positions (row stride lb).  Every item first loads its inputs, the block
+// synchronises, then the items write; so the views may overlap.  Items are
+// (row l, j) with the row fastest; NY rows, NT threads.
+//
+// inverse: compact -> full, stepS<N2, N1> with twiddles; inactive x are zero.
+template <int NY, int N1, int N2, int NT, typename T>
+__device__ __forceinline__ void x_inv_expand(T *buf, int la, int lb, const int *xa_of_x,
+                                             const T *w) {
+  constexpr int NI = NY * N1, NR = (NI + NT - 1) / NT;
+  T v[NR][N2];
+#pragma unroll
+  for (int r = 0; r < NR; r++) {
+    const int it = threadIdx.x + r * NT;
+    if (it < NI) {
+      const int l = it % NY, j = it / NY;
+#pragma unroll
+      for (int i = 0; i < N2; i++) {
+        const int q = xa_of_x[j + N1 * i];
+        v[r][i] = q >= 0 ? buf[l * la + q] : czero<T>();
+      }
+    }
+  }
+  __syncthreads();
+#pragma unroll
+  for (int r = 0; r < NR; r++) {
+    const int it = threadIdx.x + r * NT;
+    if (it < NI) {
+      const int l = it % NY, j = it / NY;
+      RDft<N2, +1>::run(v[r]);
+      if (j) {
+#pragma unroll
+        for (int k = 1; k < N2; k++) v[r][k] = cmul(v[r][k], twv(w, j * k, +1));
+      }
+#pragma unroll
+      for (int i = 0; i < N2; i++) buf[l * lb + j + N1 * i] = v[r][i];
+    }
+  }
+}
+// forward: full -> compact, stepS<N2, N1> without twiddles; only the active
+// x positions are stored.
+template <int NY, int N1, int N2, int NT, typename T>
+__device__ __forceinline__ void x_fwd_compact(T *buf, int la, int lb, const int *xa_of_x) {
+  constexpr int NI = NY * N1, NR = (NI + NT - 1) / NT;
+  T v[NR][N2];
+#pragma unroll
+  for (int r = 0; r < NR; r++) {
+    const int it = threadIdx.x + r * NT;
+    if (it < NI) {
+      const int l = it % NY, j = it / NY;
+#pragma unroll
+      for (int i = 0; i < N2; i++) v[r][i] = buf[l * lb + j + N1 * i];
+    }
+  }
+  __syncthreads();
+#pragma unroll
+  for (int r = 0; r < NR; r++) {
+    const int it = threadIdx.x + r * NT;
+    if (it < NI) {
+      const int l = it % NY, j = it / NY;
+      RDft<N2, -1>::run(v[r]);
+#pragma unroll
+      for (int i = 0; i < N2; i++) {
+        const int q = xa_of_x[j + N1 * i];
+        if (q >= 0) buf[l * la + q] = v[r][i];
+      }
+    }
+  }
+}
+
 // Runtime dispatch over the supported lengths.  Returns false if n has no
 // register split (the caller then uses the generic path).
 #define PSPW_FOR_EACH_SPLIT(X) \

@@ -111,46 +111,54 @@ constexpr size_t plane_smem() {
   return sizeof(T) * ((size_t)NY * PlaneCfg<NX, NY>::LS + NX + NY) + sizeof(int) * NX;
 }
 
+// One z-plane of one band.  The y transforms and the stick scatter/gather
+// work on the compact view [y][xa] (active x only, odd row stride la), the x
+// transforms on full rows [y][x] (stride LS); the two x steps at the ends of
+// the x sandwich convert between the views (x_inv_expand / x_fwd_compact).
+// Only the compact view needs clearing.
 template <int NX, int NY, typename T, typename R>
 __global__ void __launch_bounds__(PlaneCfg<NX, NY>::NT) k_plane(FastGeo g, int n3,
                                                                 const T *__restrict__ wx_g,
                                                                 const T *__restrict__ wy_g,
                                                                 const R *__restrict__ vperm,
                                                                 T *__restrict__ S) {
-  constexpr int LS = PlaneCfg<NX, NY>::LS;
+  constexpr int LS = PlaneCfg<NX, NY>::LS, NT = PlaneCfg<NX, NY>::NT;
   constexpr int AX = nsplit_for(NX).n1, BX = nsplit_for(NX).n2;
   constexpr int AY = nsplit_for(NY).n1, BY = nsplit_for(NY).n2;
   extern __shared__ unsigned char smem_raw[];
   T *plane = reinterpret_cast<T *>(smem_raw);
   T *wx = plane + NY * LS;
   T *wy = wx + NX;
-  int *xoff = reinterpret_cast<int *>(wy + NY);
+  int *xa = reinterpret_cast<int *>(wy + NY);  // x -> active index or -1
+  const int la = g.nxa | 1;
   const int zp = blockIdx.x, band = blockIdx.y;
   T *Sz = S + ((size_t)band * n3 + zp) * g.ncol;
-  for (int e = threadIdx.x; e < NY * LS; e += blockDim.x) plane[e] = czero<T>();
-  for (int t = threadIdx.x; t < NX; t += blockDim.x) wx[t] = wx_g[t];
-  for (int t = threadIdx.x; t < NY; t += blockDim.x) wy[t] = wy_g[t];
-  for (int t = threadIdx.x; t < g.nxa; t += blockDim.x) xoff[t] = g.xa_list[t];
+  for (int e = threadIdx.x; e < NY * la; e += NT) plane[e] = czero<T>();
+  for (int t = threadIdx.x; t < NX; t += NT) {
+    wx[t] = wx_g[t];
+    xa[t] = g.xa_of_x[t];
+  }
+  for (int t = threadIdx.x; t < NY; t += NT) wy[t] = wy_g[t];
   __syncthreads();
-  for (int c = threadIdx.x; c < g.ncol; c += blockDim.x) plane[g.col_y[c] * LS + g.col_x[c]] = Sz[c];
+  for (int c = threadIdx.x; c < g.ncol; c += NT) plane[g.col_y[c] * la + xa[g.col_x[c]]] = Sz[c];
   __syncthreads();
-  const Lines cols{xoff, 0, g.nxa};
+  const Lines cols{nullptr, 1, g.nxa};
   const Lines rows{nullptr, LS, NY};
-  inv_stepS<AY, BY>(plane, cols, LS, wy);
+  inv_stepS<AY, BY>(plane, cols, la, wy);
   __syncthreads();
-  inv_stepB<AY, BY>(plane, cols, LS, wy);
+  inv_stepB<AY, BY>(plane, cols, la, wy);
   __syncthreads();
-  inv_stepS<AX, BX>(plane, rows, 1, wx);
+  x_inv_expand<NY, AX, BX, NT>(plane, la, LS, xa, wx);
   __syncthreads();
   inv_fwd_stepB_v<AX, BX>(plane, rows, wx, vperm + (size_t)zp * NY * NX, NX);
   __syncthreads();
-  fwd_stepS<AX, BX>(plane, rows, 1, wx);
+  x_fwd_compact<NY, AX, BX, NT>(plane, la, LS, xa);
   __syncthreads();
-  fwd_stepB<AY, BY>(plane, cols, LS, wy);
+  fwd_stepB<AY, BY>(plane, cols, la, wy);
   __syncthreads();
-  fwd_stepS<AY, BY>(plane, cols, LS, wy);
+  fwd_stepS<AY, BY>(plane, cols, la, wy);
   __syncthreads();
-  for (int c = threadIdx.x; c < g.ncol; c += blockDim.x) Sz[c] = plane[g.col_y[c] * LS + g.col_x[c]];
+  for (int c = threadIdx.x; c < g.ncol; c += NT) Sz[c] = plane[g.col_y[c] * la + xa[g.col_x[c]]];
 }
 
 // Density accumulation (EvalRhoPsi.cpp:139-150): inverse y and x FFTs of one

@@ -11,6 +11,7 @@ namespace pspw {
 struct FastGeo {
   int ncol, nxa;
   const int *col_start, *sg_ig, *sg_z, *sg_col, *xa_list, *col_x, *col_y;
+  const int *xa_of_x;  // [n1] active index of x, or -1
 };
 
 // True when (n1, n2, n3) has compiled stick and plane kernels.

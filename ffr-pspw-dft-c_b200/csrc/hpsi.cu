@@ -546,7 +546,7 @@ int hpsi_apply(pspw_cell *c, const void *in_v, int ld_in, void *out_v, int ld_ou
           B.d_sg_col, B.d_col_of_xy, B.d_xa_list, B.d_xa_of_x};
   if (B.fast) {
     const FastGeo fg{B.ncol, B.nxa, B.d_col_start, B.d_sg_ig, B.d_sg_z, B.d_sg_col, B.d_xa_list,
-                     B.d_col_x, B.d_col_y};
+                     B.d_col_x, B.d_col_y, B.d_xa_of_x};
     int rc = local_fast<R>(c, fg, in, ld_in, out, ld_out, ngw, nb, plan);
     if (rc) return rc;
   } else {
