@@ -50,6 +50,12 @@ WORKLOAD = ("Chebyshev filter (degree 10, chebyfilt.cpp) on Si64: 64 atoms, a=20
             "ecutwfc 15 Ha, grid 64^3, NGW 23847, 144 bands, s+p KB projectors")
 
 
+# tcgen05.mma kind::tf32 dense rate measured on this pool's B200s
+# (ffr-pspw-dft-c_b200/microbench/tcgen05_tf32_rate.cu): 4086 flop per cycle
+# per SM (M=128, N=256, K=8 in 128.3 cycles), x 148 SMs x 1.965 GHz
+TF32_DENSE_TFLOPS = 1188.3
+
+
 def hpsi_bytes_model(ngw, nnr, nb, nat, fp64=False):
     sc, sr = (16, 8) if fp64 else (8, 4)
     return nb * (2 * ngw + 4 * nnr) * sc + nnr * sr + ngw * (4 + sr) + ngw * (nat * sc + 4 * sr)
@@ -230,21 +236,27 @@ def run_engine(args, rank, world, local_rank):
     value = world * bytes_step / (ms_max * 1e-3) / 1e9
 
     # ---- per-kernel roofline (dominant kernel family on the cell stream)
+    # Algorithmic bytes of each kernel = its share of the block H*psi byte
+    # model B_Hpsi (psi in/out and the maps to the stick kernels, the 3D-FFT
+    # grid traffic 4*NNR*s_c per band and V_eff to the plane kernel, the
+    # projector inputs to the projector kernels).  The projector GEMMs are
+    # reported in flops (F_NL = 8*NGW*nproj*nb per GEMM, complex MAC = 8).
     sc, sr = (16, 8) if fp64 else (8, 4)
-    n1, n2, n3 = w["nr"]
-    ncol, nxa = sizes["nsticks"], sizes["nxa"]
-    nproj = sizes["nproj"]
     calls = args.steps * DEGREE
-    names = {3: "k_sticks_inv", 4: "k_planes_inv", 5: "k_xlines", 6: "k_planes_fwd",
-             7: "k_sticks_fwd", 8: "k_proj(+reduce)", 9: "k_backproj"}
-    per_band = {  # algorithmic bytes per band (inputs and outputs once)
-        3: ngw * sc + n3 * ncol * sc,
-        4: n3 * ncol * sc + n3 * n2 * nxa * sc,
-        5: 2 * n3 * n2 * nxa * sc,
-        6: n3 * n2 * nxa * sc + n3 * ncol * sc,
-        7: n3 * ncol * sc + 2 * ngw * sc,
+    names = {3: "k_sticks_inv", 5: "k_plane", 7: "k_sticks_fwd", 8: "k_proj_tc(+k_proj_tc_wtiles)",
+             9: "k_backproj_tc"}
+    if fp64:
+        names.update({8: "k_proj(+k_proj_reduce)", 9: "k_backproj"})
+    fam_ms = {f: fam[f][0] for f in fam if fam[f][1] > 0}
+    nproj = sizes["nproj"]
+    alg_bytes = {  # per H*psi call
+        3: nb * ngw * sc + ngw * 4,
+        5: nb * 4 * nnr * sc + nnr * sr,
+        7: nb * 2 * ngw * sc + ngw * (4 + sr),
+        8: nb * ngw * sc + ngw * (nat * sc + 4 * sr),
+        9: 3 * nb * ngw * sc + ngw * (nat * sc + 4 * sr),
     }
-    fam_ms = {f: fam[f][0] for f in fam}
+    alg_flops = {8: 8.0 * ngw * nproj * nb, 9: 8.0 * ngw * nproj * nb}
     top = max(fam_ms, key=lambda f: fam_ms[f])
     peaks = {}
     try:
@@ -254,24 +266,35 @@ def run_engine(args, rank, world, local_rank):
     hbm_peak = peaks.get("hbm_gbs", 6650.0)
     hbm_src = "measured" if "hbm_gbs" in peaks else "fallback"
     n_launch = fam[top][1]
-    if top in per_band:
-        bytes_total = per_band[top] * nb * calls + (nnr * sr * n_launch if top == 5 else 0)
-        achieved = bytes_total / n_launch / (fam_ms[top] / n_launch * 1e-3) / 1e9
+    avg_us = fam_ms[top] / n_launch * 1e3
+    if top in (3, 5, 7):
+        per_launch = alg_bytes[top] * calls / n_launch
+        achieved = per_launch / (avg_us * 1e-6) / 1e9
         roof = {"kernel": names[top], "bound": "hbm", "achieved": round(achieved, 1),
                 "peak": hbm_peak, "unit": "GB/s", "frac": round(achieved / hbm_peak, 4),
-                "peak_source": hbm_src,
-                "bytes_per_launch": int(bytes_total / n_launch),
-                "launches": n_launch, "avg_launch_us": round(fam_ms[top] / n_launch * 1e3, 2)}
+                "peak_source": hbm_src, "bytes_per_launch": int(per_launch),
+                "launches": n_launch, "avg_launch_us": round(avg_us, 2)}
     else:
-        flops = 8.0 * ngw * nproj * nb * calls
-        achieved = flops / (fam_ms[top] * 1e-3) / 1e12
-        simt_peak = 148 * 128 * 2 * 1.965e9 / 1e12 * (0.5 if fp64 else 1.0)
-        roof = {"kernel": names[top], "bound": "fp32 SIMT" if not fp64 else "fp64",
-                "achieved": round(achieved, 2), "peak": round(simt_peak, 1), "unit": "TFLOP/s",
-                "frac": round(achieved / simt_peak, 4), "peak_source": "nominal SIMT",
-                "launches": n_launch, "avg_launch_us": round(fam_ms[top] / n_launch * 1e3, 2)}
+        per_launch = alg_flops[top] * calls / n_launch
+        achieved = per_launch / (avg_us * 1e-6) / 1e12
+        roof = {"kernel": names[top], "bound": "tensor", "achieved": round(achieved, 2),
+                "peak": TF32_DENSE_TFLOPS, "unit": "TFLOP/s",
+                "frac": round(achieved / TF32_DENSE_TFLOPS, 4),
+                "peak_source": "measured tcgen05 kind::tf32 MMA rate (4086 flop/cycle/SM at "
+                               "1965 MHz); the kernels issue 3 TF32 products per FP32 product",
+                "flops_per_launch": int(per_launch), "launches": n_launch,
+                "avg_launch_us": round(avg_us, 2)}
+    # every family on the same footing, for the launch-share table
+    fam_report = {}
+    for f, t in fam_ms.items():
+        d = {"ms_per_step": round(t / args.steps, 4), "launches_per_step": fam[f][1] // args.steps}
+        if f in alg_bytes:
+            d["alg_gbs"] = round(alg_bytes[f] * calls / (t * 1e-3) / 1e9, 1)
+        if f in alg_flops:
+            d["alg_tflops"] = round(alg_flops[f] * calls / (t * 1e-3) / 1e12, 2)
+        fam_report[names.get(f, str(f))] = d
     roof["traffic"] = _ncu_traffic(roof["kernel"], args.prec)
-    kernels_ms = {names[f]: round(fam_ms[f] / args.steps, 4) for f in fam_ms}
+    kernels_ms = fam_report
     hpsi_ms = ms_max / DEGREE
     hpsi_roof = {"bytes_per_hpsi": hpsi_bytes_model(ngw, nnr, nb, nat, fp64=fp64),
                  "ms_per_hpsi": round(hpsi_ms, 4),

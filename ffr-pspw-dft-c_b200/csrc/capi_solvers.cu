@@ -262,4 +262,49 @@ int pspw_eval_rho_psi(pspw_cell *c, double *rhoe, const double *eigvec, int ld, 
   return PSPW_OK;
 }
 
+int pspw_eval_enl(pspw_cell *c, const double *c0, int ld, int ngw, int nx, const double *focc,
+                  double wkpt, double *enl, double *fnl) {
+  int rc = enter(c);
+  if (rc) return rc;
+  if (!c0 || !focc || !enl || nx < 0 || ld < ngw || ngw < 1)
+    return fail(PSPW_ERR_ARG, "EvalENL: bad argument");
+  if (ngw > c->basis.ngw) return fail(PSPW_ERR_SHAPE, "EvalENL: NGW exceeds the cell");
+  const int nproj = c->proj.nproj;
+  *enl = 0.0;
+  if (nx == 0 || nproj == 0) return PSPW_OK;
+  double2 *dX, *dP;
+  if ((rc = up_mat(c, kSlotA, c0, ld, ngw, nx, &dX)) ||
+      (rc = ws_reserve(c, kSlotB, sizeof(double2) * (size_t)nx * nproj, (void **)&dP)))
+    return rc;
+  if ((rc = project_fp64(c, dX, ngw, ngw, nx, dP))) return rc;
+  std::vector<double2> P((size_t)nx * nproj);
+  std::vector<double> w(nproj);
+  PSPW_CUDA(cudaMemcpyAsync(P.data(), dP, sizeof(double2) * P.size(), cudaMemcpyDeviceToHost,
+                            c->stream));
+  PSPW_CUDA(cudaMemcpyAsync(w.data(), c->proj.d_pw64, sizeof(double) * nproj,
+                            cudaMemcpyDeviceToHost, c->stream));
+  if ((rc = sync(c))) return rc;
+  // projectors are species-major, then atom, then lm: the reference's loop
+  // order (EvalENL.cpp:21-45) for one k-point
+  double e = 0.0;
+  for (int p = 0; p < nproj; p++) {
+    double enl_m = 0.0;
+    for (int ist = 0; ist < nx; ist++) {
+      const double2 sf = P[(size_t)ist * nproj + p];
+      const double a = std::hypot(sf.x, sf.y);
+      enl_m = enl_m + focc[ist] * (a * a);
+    }
+    e = e + wkpt * enl_m * w[p];
+  }
+  *enl = e;
+  if (fnl)
+    for (int p = 0; p < nproj; p++)
+      for (int ist = 0; ist < nx; ist++) {
+        const double2 sf = P[(size_t)ist * nproj + p];
+        fnl[2 * ((size_t)p * nx + ist)] = sf.x;
+        fnl[2 * ((size_t)p * nx + ist) + 1] = sf.y;
+      }
+  return PSPW_OK;
+}
+
 }  // extern "C"

@@ -6,7 +6,7 @@
 // and forwards to the C ABI in include/pspw_gpu.h.  A program links this
 // library in place of ApplyHam_block.o, ApplyHam.o, chebyfilt.o,
 // davidson_cpu.o, lobpcg_cpu.o, ortho_qr.o, eig_zheevd.o, eig_zhegv.o,
-// GenPrec.o, EvalRhoPsi.o, lanczos.o and Diagon_cpu.o.
+// GenPrec.o, EvalRhoPsi.o, EvalENL.o, lanczos.o and Diagon_cpu.o.
 //
 // Device state: one pspw_cell per k-point, built from N123/XKG/EIGR/PKG_A/
 // WNL on first use (or by SetupArrays_ApplyHam_cuda) and reused while those
@@ -23,6 +23,7 @@
 // ApplyHam_block.cpp:18-21 (nnr != NNR) and :70-73 (lm_end > 4) print the
 // same message and abort; an engine failure prints the engine's message and
 // aborts (the reference has no error return on these paths).
+#include <cmath>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
@@ -59,6 +60,8 @@ extern double *FOCC;
 extern double *WKPT;
 extern double OMEGA;
 extern double EKIN;
+extern double ENL;
+extern zcomplex *FNL;
 
 #define DROPIN_API __attribute__((visibility("default")))
 
@@ -386,6 +389,49 @@ DROPIN_API void EvalRhoPsi(int ik, double *rhoe, zcomplex *eigvec, int ldEigvec,
     std::abort();
   }
   if (rc) die("EvalRhoPsi", rc);
+}
+
+// EvalENL.cpp:5-49: FNL of every k-point on the device (unconjugated C0
+// against PKG_A conj(EIGR)), written into the global FNL, then ENL summed on
+// the host in the reference's loop order (species, atom, k-point, lm).
+DROPIN_API void EvalENL() {
+  std::vector<std::vector<double>> fnl(NKPT);
+  int nproj = 0;
+  for (int is = 0; is < NSP; is++) nproj += NA[is] * (L_MAX[is] * L_MAX[is] - 2 * L_LOC[is] + 1);
+  for (int ik = 1; ik <= NKPT; ik++) {
+    fnl[ik - 1].assign(2 * (size_t)NX * nproj, 0.0);
+    double e = 0.0;
+    const int rc = pspw_eval_enl(cell_for(ik), dp(C0 + (size_t)(ik - 1) * NGWX * NX), NGWX,
+                                 NGW[ik - 1], NX, FOCC + (size_t)(ik - 1) * NX, WKPT[ik - 1], &e,
+                                 fnl[ik - 1].data());
+    if (rc) die("EvalENL", rc);
+  }
+  ENL = 0.0;
+  int p0 = 0;  // first projector of (is, ia)
+  for (int is = 1; is <= NSP; is++) {
+    const int lm_end = L_MAX[is - 1] * L_MAX[is - 1] - 2 * L_LOC[is - 1] + 1;
+    for (int ia = 1; ia <= NA[is - 1]; ia++, p0 += lm_end) {
+      for (int ik = 1; ik <= NKPT; ik++) {
+        for (int lm = 1; lm <= lm_end; lm++) {
+          const double *f = fnl[ik - 1].data() + 2 * (size_t)(p0 + lm - 1) * NX;
+          double enl_m = 0.0;
+          for (int ist = 1; ist <= NX; ist++) {
+            const double re = f[2 * (ist - 1)], im = f[2 * (ist - 1) + 1];
+            // FNL(ist, ik, is, ia, lm), dimensions NX x NKPT x NSP x NAX
+            const size_t at =
+                ((((size_t)(lm - 1) * NAX + (ia - 1)) * NSP + (is - 1)) * NKPT + (ik - 1)) * NX +
+                (ist - 1);
+            double *g = reinterpret_cast<double *>(FNL + at);
+            g[0] = re;
+            g[1] = im;
+            const double a = std::hypot(re, im);
+            enl_m = enl_m + FOCC[(size_t)(ik - 1) * NX + ist - 1] * (a * a);
+          }
+          ENL = ENL + WKPT[ik - 1] * enl_m * WNL[(size_t)(lm - 1) * NSP + (is - 1)];
+        }
+      }
+    }
+  }
 }
 
 // EvalRhoPsi.cpp:5 (eigvec with leading dimension NGWX)

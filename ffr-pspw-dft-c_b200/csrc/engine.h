@@ -195,4 +195,8 @@ int hpsi_apply(pspw_cell *c, const void *in, int ld_in, void *out, int ld_out, i
                int nb, double a, double b, double g, const void *xm2, int ld_xm2,
                const ScratchPlan *plan = nullptr);
 
+// Unweighted FP64 projections P[b*nproj + p] = sum_G conj(beta_p) psi_b
+// (hpsi.cu), on the cell stream.
+int project_fp64(pspw_cell *c, const double2 *psi, int ld, int ngw, int nb, double2 *P);
+
 }  // namespace pspw

@@ -315,7 +315,8 @@ __global__ void k_proj_reduce(const cx<R> *__restrict__ part, const R *__restric
   const int p = i % nproj;
   cx<R> s = part[i];
   for (int k = 1; k < nsplit; k++) s = s + part[(size_t)k * nb * nproj + i];
-  wp[i] = mk<cx<R>>(w[p] * s.x, w[p] * s.y);
+  const R wl = w ? w[p] : R(1);  // null: the projections themselves
+  wp[i] = mk<cx<R>>(wl * s.x, wl * s.y);
 }
 
 // out = a*(out + sum_p beta_p(ig) wp[b][p]) + bc*in + g*xm2
@@ -634,6 +635,38 @@ int hpsi_apply(pspw_cell *c, const void *in_v, int ld_in, void *out_v, int ld_ou
                                           (R)b, (R)g);
     });
   }
+  PSPW_CUDA(cudaGetLastError());
+  return PSPW_OK;
+}
+
+// P[b*nproj + p] = sum_{G < ngw} conj(beta_p(G)) psi_b(G), FP64, without the
+// weights WNL (the projections FNL of EvalENL.cpp:27-33).
+int project_fp64(pspw_cell *c, const double2 *psi, int ld, int ngw, int nb, double2 *P) {
+  using R = double;
+  const int nproj = c->proj.nproj;
+  if (nproj <= 0 || nb <= 0) return PSPW_OK;
+  ProjArg pa;
+  pa.eigr = Prec<R>::eigr(c);
+  pa.pkga = Prec<R>::pkga(c);
+  pa.patom = c->proj.d_patom;
+  pa.psp = c->proj.d_psp;
+  pa.plm = c->proj.d_plm;
+  pa.pw = Prec<R>::pw(c);
+  pa.ngw_cell = c->basis.ngw;
+  pa.nproj = nproj;
+  constexpr int BK = 16;
+  const int mt = (nproj + kBM - 1) / kBM, nt = (nb + kBN - 1) / kBN;
+  int nsplit = std::max(1, std::min((ngw + 255) / 256, (2 * 148 + mt * nt - 1) / (mt * nt)));
+  int kchunk = (ngw + nsplit - 1) / nsplit;
+  kchunk = (kchunk + BK - 1) / BK * BK;
+  nsplit = (ngw + kchunk - 1) / kchunk;
+  cx<R> *part = nullptr;
+  int rc = ws_reserve(c, kWsProjPart, sizeof(cx<R>) * (size_t)nsplit * nb * nproj, (void **)&part);
+  if (rc) return rc;
+  k_proj<R, BK><<<dim3(mt, nt, nsplit), 256, 0, c->stream>>>(pa, psi, ld, ngw, nb, kchunk, part);
+  k_proj_reduce<R><<<(nb * nproj + 255) / 256, 256, 0, c->stream>>>(part, nullptr, nsplit, nb,
+                                                                    nproj, P);
+  c->kernel_launches += 2;
   PSPW_CUDA(cudaGetLastError());
   return PSPW_OK;
 }

@@ -80,6 +80,7 @@ SIGNATURES = {
     "pspw_lobpcg": [_vp, _vp, _vp, _i, _i, _vp, _i, _i, _i, _vp, _vp],
     "pspw_lanczos": [_vp, _vp, _i, _i, _vp, _i, _vp],
     "pspw_eval_rho_psi": [_vp, _vp, _vp, _i, _i, _i, _vp, _d, _d, _vp],
+    "pspw_eval_enl": [_vp, _vp, _i, _i, _i, _vp, _d, _vp, _vp],
 }
 _RESTYPE = {"pspw_error_string": C.c_char_p, "pspw_last_error": C.c_char_p}
 

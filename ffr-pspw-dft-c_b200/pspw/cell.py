@@ -213,6 +213,18 @@ class Cell:
                                       C.byref(ek)))
         return rho, ek.value
 
+    def eval_enl(self, c0, nx, focc, wkpt):
+        """EvalENL for one k-point: (ENL, FNL[nx, nproj]) from C0 (ngw x >= nx)."""
+        a = np.asfortranarray(np.asarray(c0, dtype=np.complex128))
+        ngw = a.shape[0]
+        fo = np.ascontiguousarray(np.asarray(focc, dtype=float))
+        nproj = self.sizes()["nproj"]
+        fnl = np.zeros((nx, max(1, nproj)), dtype=np.complex128, order="F")
+        e = C.c_double(0.0)
+        check(lib().pspw_eval_enl(self._h, a.ctypes.data, ngw, ngw, int(nx), fo.ctypes.data,
+                                  float(wkpt), C.byref(e), fnl.ctypes.data))
+        return e.value, fnl[:, :nproj]
+
     # ---- timing
     def timing_enable(self, mask):
         check(lib().pspw_timing_enable(self._h, int(mask)))

@@ -192,6 +192,16 @@ int pspw_lanczos(pspw_cell *cell, double *v0, int ngw, int k, double *T, int ldT
 int pspw_eval_rho_psi(pspw_cell *cell, double *rhoe, const double *eigvec, int ld, int ngw,
                       int nx, const double *focc, double wkpt, double omega, double *ekin);
 
+/* Nonlocal energy of one k-point (EvalENL.cpp:5-49): with C0 (host,
+ * ngw x nx complex, leading dimension ld, used unconjugated)
+ *   FNL(ist, p) = sum_{G < ngw} C0(G, ist) PKG_A(lm_p, G) conj(EIGR(G, atom_p))
+ *   *enl        = wkpt * sum_p WNL(p) sum_ist focc[ist] |FNL(ist, p)|^2
+ * accumulated over projectors in the reference's (species, atom, lm) order.
+ * fnl (may be null) receives FNL as nx x nproj complex, column-major.  FP64
+ * on the device. */
+int pspw_eval_enl(pspw_cell *cell, const double *c0, int ld, int ngw, int nx,
+                  const double *focc, double wkpt, double *enl, double *fnl);
+
 /* ------------------------------------------------------------------ timing
  * Optional device timing on the cell stream: CUDA events around each launch
  * of the enabled families, summed until reset.  Families (bit i of the mask):

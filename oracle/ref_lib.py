@@ -48,6 +48,7 @@ class RefLib:
         L.ref_set_ekin.argtypes = [C.c_double]
         L.ref_get_ekin.restype = C.c_double
         L.ref_get_enl.restype = C.c_double
+        L.ref_EvalENL.argtypes = []
         L.ref_ApplyHam_block.argtypes = [_zp, _zp, C.c_int, _dp, C.c_int]
         L.ref_ApplyHam.argtypes = [_zp, _zp, C.c_int, _dp]
         L.ref_chebyfilt.argtypes = [_zp, C.c_int, C.c_double, C.c_double, _dp]
@@ -193,6 +194,11 @@ class RefLib:
     def set_nx(self, nx, nempty):
         self.lib.ref_set_nx(nx, nempty)
         self.cell["nx"] = nx
+
+    def eval_enl(self):
+        """EvalENL() on the C0 / FOCC the last eval_rho_psi left; returns ENL."""
+        self.lib.ref_EvalENL()
+        return self.lib.ref_get_enl()
 
     def eval_rho_psi(self, eigvec_flat, ld, ngw, nx, focc):
         """Returns (rho increment, EKIN increment, C0)."""

@@ -65,6 +65,7 @@ DROPIN_SYMBOLS = [
     "_Z17Diagon_lobpcg_cpuiPdPCdiS_id",     # Diagon_lobpcg_cpu     common_pspw.h:195
     "_Z19Diagon_davidson_cpuiPdPCdiS_id",   # Diagon_davidson_cpu   common_pspw.h:200
     "_Z10symmetrizePCdiii",                 # symmetrize (lobpcg_cpu.cpp:15)
+    "_Z7EvalENLv",                          # EvalENL               common_pspw.h:181
 ]
 
 

@@ -86,6 +86,9 @@ def test_eval_rho_psi_and_solvers_through_dropin(pair):
     assert relmax(r_d, r_r) < 1e-12
     assert abs(ek_d - ek_r) < 1e-12 * abs(ek_r)
     assert np.array_equal(c0_d, c0_r)
+    # EvalENL on the C0 that EvalRhoPsi just copied, in both programs
+    enl_r, enl_d = ref.eval_enl(), drop.eval_enl()
+    assert abs(enl_d - enl_r) < 1e-12 * abs(enl_r)
     prec = ref.gen_prec(ngw, -10.0)
     assert np.array_equal(drop.gen_prec(ngw, -10.0), prec)
     ev_r, _ = ref.lobpcg(ngw, 12, veff, prec, 4, max_iter=6)

@@ -149,3 +149,18 @@ def test_live_eig_zhegv_eval(ref_cell):
     w_o, v_o, _ = O.eig_zhegv_eval(a, bm)
     assert np.abs(w_r - w_o).max() < 1e-12
     assert np.abs(np.abs(v_r) - np.abs(v_o)).max() < 1e-10
+
+
+@need_ref
+def test_live_eval_enl(ref_cell):
+    # EvalENL.cpp:5-49 on the C0 that EvalRhoPsi copies, with unequal occupations
+    b, cell, veff, lat = ref_cell
+    from pspw import synth
+    ngw, ngwx = b["ngw"], b["ngwx"]
+    psi = synth.wavefunctions(b, lat, 6, 31)
+    flat = np.concatenate([psi.reshape(-1, order="F"), np.zeros(ngwx, complex)])
+    focc = np.array([2.0, 2.0, 2.0, 1.5, 0.5, 0.0])
+    REF.eval_rho_psi(flat, ngw, ngw, 6, focc)
+    enl_r = REF.eval_enl()
+    enl_o, _ = O.eval_enl(cell, psi, ngw, 6, focc, 1.0)
+    assert abs(enl_o - enl_r) < 1e-12 * abs(enl_r)

@@ -95,6 +95,17 @@ def test_eval_rho_psi_accumulates_and_checks_charge(gcell):
     assert e.value.code == 8
 
 
+def test_eval_enl_matches_oracle(gcell):
+    # EvalENL.cpp:5-49: FNL from the unconjugated C0, ENL = sum w f |FNL|^2 WNL
+    ngw = int(G["ngw"])
+    c0 = G["psi"]
+    focc = np.array([2.0, 2.0, 1.0, 0.5])
+    enl, fnl = gcell.eval_enl(c0, 4, focc, 0.75)
+    enl_o, fnl_o = O.eval_enl(oracle_cell(G), c0, ngw, 4, focc, 0.75)
+    assert abs(enl - enl_o) < 1e-12 * abs(enl_o)
+    assert relmax(fnl, fnl_o) < 1e-12
+
+
 @pytest.fixture(scope="module")
 def si8_12ry():
     from pspw import basis_gamma, synth
