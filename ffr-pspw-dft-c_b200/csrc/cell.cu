@@ -213,7 +213,7 @@ int pspw_cell_destroy(pspw_cell *c) {
                   c->proj.d_pkga64, c->proj.d_pkga32, c->proj.d_patom, c->proj.d_psp,
                   c->proj.d_plm, c->proj.d_pw64, c->proj.d_pw32, c->d_veff64, c->d_veff32,
                   B.d_col_x, B.d_col_y, B.d_pinv[0], B.d_pinv[1], B.d_pinv[2], c->d_vperm64,
-                  c->d_vperm32, c->proj.d_etp, c->proj.d_etb};
+                  c->d_vperm32, c->proj.d_etp, c->proj.d_etb, B.d_wgrid};
   for (void *p : ptrs)
     if (p) cudaFree(p);
   for (int i = 0; i < 3; i++) {
@@ -320,6 +320,8 @@ int pspw_cell_create(pspw_cell **out, int device, int nr1, int nr2, int nr3, int
   B.ncol = ncol;
   B.nxa = (int)xa_list.size();
   std::vector<double> kin64(ngw), xkg64(xkg, xkg + ngw);
+  std::vector<int> wgrid(ngw);
+  for (int ig = 0; ig < ngw; ig++) wgrid[ig] = (int)(n123[ig] - 1);
   std::vector<float> kin32(ngw);
   c->tpiba2 = tpiba2;
   for (int ig = 0; ig < ngw; ig++) {
@@ -330,7 +332,7 @@ int pspw_cell_create(pspw_cell **out, int device, int nr1, int nr2, int nr3, int
       (rc = upload(&B.d_sg_z, sg_z)) || (rc = upload(&B.d_sg_col, sg_col)) ||
       (rc = upload(&B.d_col_of_xy, col_of_xy)) || (rc = upload(&B.d_xa_list, xa_list)) ||
       (rc = upload(&B.d_xa_of_x, xa_of_x)) || (rc = upload(&B.d_kin64, kin64)) ||
-      (rc = upload(&B.d_xkg64, xkg64)) ||
+      (rc = upload(&B.d_xkg64, xkg64)) || (rc = upload(&B.d_wgrid, wgrid)) ||
       (rc = upload(&B.d_kin32, kin32)))
     return bail(rc);
   const int nr[3] = {nr1, nr2, nr3};

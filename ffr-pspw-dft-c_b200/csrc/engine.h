@@ -44,6 +44,7 @@ struct Basis {
   double *d_kin64 = nullptr;   // [ngw] 0.5*XKG*TPIBA2
   float *d_kin32 = nullptr;
   double *d_xkg64 = nullptr;   // [ngw] XKG (the preconditioner and EKIN read it)
+  int *d_wgrid = nullptr;      // [ngw] 0-based grid index of G (N123 - 1)
   FftDim dim[3];
   // register-FFT path (every length has a two-factor split): stick
   // coordinates, and per axis the natural index held at each position of

@@ -20,6 +20,7 @@ PREC_F32 = 1
 NL_AUTO = 0
 NL_SIMT = 1
 NL_TENSOR_CORE = 2
+MIX_SIMPLE, MIX_KERKER, MIX_ANDERSON, MIX_PULAY = 0, 1, 2, 3
 
 OK = 0
 ERRORS = {1: "ARG", 2: "SHAPE", 3: "CUDA", 4: "OOM", 5: "NONFINITE", 6: "TIMEOUT", 7: "LAPACK",
@@ -81,6 +82,16 @@ SIGNATURES = {
     "pspw_lanczos": [_vp, _vp, _i, _i, _vp, _i, _vp],
     "pspw_eval_rho_psi": [_vp, _vp, _vp, _i, _i, _i, _vp, _d, _d, _vp],
     "pspw_eval_enl": [_vp, _vp, _i, _i, _i, _vp, _d, _vp, _vp],
+    "pspw_scf_create": [_vp, _i, _vp, _vp, _vp, _vp, _i, _vp, _vp, _vp, _d, _d, _d, _d, _vp],
+    "pspw_scf_destroy": [_vp],
+    "pspw_eval_energy": [_vp, _vp, _d, _d, _vp],
+    "pspw_eval_energy_dev": [_vp, _vp, _d, _d, _vp],
+    "pspw_xc_pz": [_vp, _vp, _vp, _vp],
+    "pspw_normalize_rho": [_vp, _vp, _vp],
+    "pspw_kerker_prec": [_vp, _vp, _d, _d],
+    "pspw_mix_init": [_vp, _i, _i, _d, _d, _vp],
+    "pspw_mix": [_vp, _i, _vp, _vp],
+    "pspw_mix_dev": [_vp, _i, _vp, _vp],
 }
 _RESTYPE = {"pspw_error_string": C.c_char_p, "pspw_last_error": C.c_char_p}
 

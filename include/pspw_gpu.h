@@ -202,6 +202,57 @@ int pspw_eval_rho_psi(pspw_cell *cell, double *rhoe, const double *eigvec, int l
 int pspw_eval_enl(pspw_cell *cell, const double *c0, int ld, int ngw, int nx,
                   const double *focc, double wkpt, double *enl, double *fnl);
 
+/* ------------------------------------------------------------------ SCF pieces
+ * The steps of the SCF iteration around the eigensolver, on the device in
+ * FP64, with the local-potential data and the density-mixing history kept
+ * in a pspw_scf handle bound to a cell (same grid, same stream).
+ *
+ * pspw_scf_create   the data EvalEnergy.cpp reads besides the density: the
+ *                   NG density G vectors as 1-based grid indices N1, N2, N3
+ *                   (G = 0 first) and |G|^2 in (2 pi/alat)^2 units (the
+ *                   global G), SFAC (complex), VPS and RHOPS (real), each
+ *                   NSP x NG with the species index fastest, OMEGA, NEL,
+ *                   ESR, ESELF.
+ * eval_energy       EvalEnergy.cpp:5-163: rhoe in = density, out = V_eff =
+ *                   Re(V_H + V_loc) + V_xc; e6 = {ETOT, EKIN, EHT, EPSEU,
+ *                   ENL, EXC} with EKIN and ENL supplied by the caller.
+ *                   Grid points outside the density sphere keep the
+ *                   transformed density before the inverse transform, as in
+ *                   the reference.
+ * xc_pz             xc_PZ.cpp:7-63 (Perdew-Zunger LDA): vxc and Exc (the
+ *                   plain sum of rho (ex + ec), not yet x OMEGA/NNR).
+ * normalize_rho     NormalizeRho.cpp:7-33 with the handle's OMEGA and NEL;
+ *                   *warn = 1 where the reference prints its warning;
+ *                   PSPW_ERR_CHARGE where it aborts (sum < 1e-15).
+ * kerker_prec       KerkerRhoMix.cpp:53-81: x <- FFT^-1 [beta gg/(gg+q0)
+ *                   FFT x] on the wavefunction sphere of the cell (other
+ *                   components unchanged, as in the reference).
+ * mix_init / mix    SimpleRhoMix.cpp, KerkerRhoMix.cpp:5-50,
+ *                   AndersonRhoMix.cpp:8-91, PulayRhoMix.cpp:5-91 (beta is a
+ *                   parameter; the reference's Pulay uses 0.25).  The history
+ *                   starts at zero as in ChebySCFLoop.cpp:123-148; rho_old
+ *                   (may be null) fills its first column.  iter counts from
+ *                   1; *d = the mixer's residual measure. */
+typedef struct pspw_scf pspw_scf;
+#define PSPW_MIX_SIMPLE 0
+#define PSPW_MIX_KERKER 1
+#define PSPW_MIX_ANDERSON 2
+#define PSPW_MIX_PULAY 3
+int pspw_scf_create(pspw_cell *cell, int ng, const int *n1, const int *n2, const int *n3,
+                    const double *g, int nsp, const double *sfac, const double *vps,
+                    const double *rhops, double omega, double nel, double esr, double eself,
+                    pspw_scf **out);
+int pspw_scf_destroy(pspw_scf *scf);
+int pspw_eval_energy(pspw_scf *scf, double *rhoe, double ekin, double enl, double *e6);
+int pspw_eval_energy_dev(pspw_scf *scf, double *d_rhoe, double ekin, double enl, double *e6);
+int pspw_xc_pz(pspw_scf *scf, const double *rho, double *vxc, double *exc);
+int pspw_normalize_rho(pspw_scf *scf, double *rho, int *warn);
+int pspw_kerker_prec(pspw_scf *scf, double *x, double beta, double q0);
+int pspw_mix_init(pspw_scf *scf, int kind, int mixdim, double beta, double q0,
+                  const double *rho_old);
+int pspw_mix(pspw_scf *scf, int iter, double *rhoe, double *d);
+int pspw_mix_dev(pspw_scf *scf, int iter, double *d_rhoe, double *d);
+
 /* ------------------------------------------------------------------ timing
  * Optional device timing on the cell stream: CUDA events around each launch
  * of the enabled families, summed until reset.  Families (bit i of the mask):

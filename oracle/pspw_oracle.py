@@ -432,3 +432,182 @@ def eval_enl(cell, c0, ngw, nx, focc, wkpt):
     fnl = c0[:ngw, :nx].T @ beta.conj()
     enl = float(np.sum(wkpt * (focc[:nx, None] * np.abs(fnl) ** 2) * w[None, :]))
     return enl, fnl
+
+
+# ---------------------------------------------------------------- SCF pieces
+# Restatements of the steps around the eigensolver; the engine's versions are
+# in ffr-pspw-dft-c_b200/csrc/scf.cu.
+
+def _pz_point(r):
+    """xc_PZ.cpp:24-59 at one point: (ux + uc, ex + ec); zeros for r <= 1e-13."""
+    A, B, C = -0.1423, 1.0529, 0.3334
+    a, b, c, d = 0.0311, -0.0480, 0.0020, -0.0116
+    if r <= 1.e-13:
+        return 0.0, 0.0
+    ax = -(3.0 / 4.0) * (3.0 / 2.0 / np.pi) ** (2.0 / 3.0)
+    rs = (3.0 / (4.0 * np.pi * r)) ** (1.0 / 3.0)
+    rrs = np.sqrt(rs)
+    ex = ax / rs
+    ux = 4.0 / 3.0 * ex
+    if rs >= 1.0:
+        bpr = 1.0 + B * rrs + C * rs
+        ec = A / bpr
+        uc = (1.0 + 7.0 / 6.0 * B * rrs + 4.0 / 3.0 * C * rs) * ec / bpr
+    else:
+        rsl = np.log(rs)
+        ec = a * rsl + b + c * rs * rsl + d * rs
+        uc = (2.0 * d - c) / 3.0 * rs + b - a / 3.0 + a * rsl + 2.0 * c / 3.0 * rs * rsl
+    return ux + uc, ex + ec
+
+
+def xc_pz(rho):
+    """xc_PZ.cpp:7-63: (vxc, Exc = sum rho (ex + ec)).  A point with rho < -0.1
+    keeps the previous point's values (the loop variables are not reset)."""
+    vxc = np.zeros(len(rho))
+    exc = 0.0
+    v = e = 0.0
+    for i, r in enumerate(rho):
+        if not r < -0.1:
+            v, e = _pz_point(float(r))
+        vxc[i] = v
+        exc = exc + r * e
+    return vxc, exc
+
+
+def normalize_rho(rho, omega, nel):
+    """NormalizeRho.cpp:7-33 (negatives clipped, scaled to NEL electrons)."""
+    r = np.array(rho, dtype=float, copy=True)
+    r[r < 0.0] = 0.0
+    s = r.sum()
+    if s < 1.0e-15:
+        raise RuntimeError("NormalizeRho: sum(rho) too small")
+    truesum = len(r) * nel / omega
+    return r * truesum / s
+
+
+def kerker_prec(x, cell, beta, q0):
+    """KerkerRhoMix.cpp:53-81: filter the wavefunction-sphere components of
+    FFT(x) by beta gg/(gg+q0); the others are unchanged."""
+    c = fft_forward(np.asarray(x, dtype=complex), cell["nr"])
+    ngw = int(cell["ngw"])
+    idx = np.asarray(cell["n123"])[:ngw].astype(np.int64) - 1
+    gg = np.asarray(cell["xkg"])[:ngw]
+    c[idx] = (beta * gg / (gg + q0)) * c[idx]
+    return fft_inverse(c, cell["nr"]).real
+
+
+def eval_energy(rho, local, cell, ekin, enl):
+    """EvalEnergy.cpp:5-163.  local: dict with gidx (0-based grid index of the
+    density G's, G = 0 first), g (|G|^2, tpiba^2 units), vp and rp (sums over
+    species of SFAC*VPS and SFAC*RHOPS), omega, esr, eself.  Returns (V_eff,
+    energies).  Grid points outside the density sphere keep FFT(rho)."""
+    nr = cell["nr"]
+    c = fft_forward(np.asarray(rho, dtype=complex), nr)
+    gidx, g, vp, rp = local["gidx"], local["g"], local["vp"], local["rp"]
+    eps = vp[0] * np.conj(c[0])
+    rhet = c[gidx[1:]]
+    rhog = rhet + rp[1:]
+    fpibg = 4.0 * np.pi / (cell["tpiba2"] * g[1:])
+    vcg = fpibg * rhog
+    eh = np.sum(0.5 * vcg * np.conj(rhog))
+    eps = eps + np.sum(np.conj(rhet) * vp[1:])
+    vtemp = np.concatenate([[vp[0]], vcg + vp[1:]])
+    c[gidx] = vtemp
+    v = fft_inverse(c, nr)
+    vxc, exc = xc_pz(rho)
+    veff = v.real + vxc
+    n = len(rho)
+    EXC = exc * local["omega"] / n
+    EHT = eh.real * local["omega"] + local["esr"] - local["eself"]
+    EPSEU = eps.real * local["omega"]
+    return veff, dict(ETOT=ekin + EHT + EPSEU + enl + EXC, EKIN=ekin, EHT=EHT, EPSEU=EPSEU,
+                      ENL=enl, EXC=EXC)
+
+
+class Mixer:
+    """SimpleRhoMix.cpp, KerkerRhoMix.cpp:5-50, AndersonRhoMix.cpp:8-91 and
+    PulayRhoMix.cpp:5-91 with their history (zero at the start, as the
+    ChebySCF loop allocates it).  kind: 0 simple, 1 Kerker, 2 Anderson,
+    3 Pulay."""
+
+    def __init__(self, kind, nnr, cell, mixdim=0, beta=0.25, q0=0.0, omega=1.0, nel=0.0,
+                 rho_old=None):
+        self.kind, self.cell, self.mixdim, self.beta, self.q0 = kind, cell, mixdim, beta, q0
+        self.omega, self.nel = omega, nel
+        ncol = mixdim if kind == 3 else (3 if kind == 2 else 1)
+        self.h = np.zeros((nnr, ncol))
+        self.f = np.zeros((nnr, ncol))
+        self.g = np.zeros((nnr, 2))
+        if rho_old is not None:
+            self.h[:, 0] = rho_old
+
+    def mix(self, it, rhoe):
+        rhoe = np.array(rhoe, dtype=float, copy=True)
+        b, h, f, g, n = self.beta, self.h, self.f, self.g, len(rhoe)
+        if self.kind == 0:
+            d = np.sum((rhoe - h[:, 0]) ** 2)
+            rhoe = b * rhoe + (1.0 - b) * h[:, 0]
+            h[:, 0] = rhoe
+            return rhoe, np.sqrt(d / n)
+        if self.kind == 1:
+            d = np.sum((rhoe - h[:, 0]) ** 2)
+            rhoe = h[:, 0] + kerker_prec(rhoe - h[:, 0], self.cell, b, self.q0)
+            h[:, 0] = rhoe
+            return rhoe, np.sqrt(d / n)
+        if self.kind == 2:
+            if it == 1:
+                h[:, 0] = rhoe
+                f[:, 0] = 0.0
+                return rhoe, 1.0
+            j0, j1, j2 = (it - 1) % 3, (it - 2) % 3, (it - 3) % 3
+            f[:, j0] = rhoe - h[:, j1]
+            d = float(f[:, j0] @ f[:, j0])
+            if it == 2:
+                rhoe = b * rhoe + (1.0 - b) * h[:, j1]
+                h[:, j0] = rhoe
+                return rhoe, d
+            g[:, 0] = f[:, j1] - f[:, j0]
+            d11 = g[:, 0] @ g[:, 0]
+            r1 = f[:, j0] @ g[:, 0]
+            if it == 3:
+                t1 = -r1 / d11
+                rhoe = (1 - t1) * h[:, j1] + t1 * h[:, j2] + b * (f[:, j0] + t1 * g[:, 0])
+            else:
+                g[:, 1] = f[:, j2] - f[:, j0]
+                d22 = g[:, 1] @ g[:, 1]
+                d12 = g[:, 0] @ g[:, 1]
+                r2 = f[:, j0] @ g[:, 1]
+                t1 = d11 * d22
+                t2 = t1 - d12 * d12
+                if abs(t2) > abs(t1) * 1.0e-8:
+                    t1, t2 = (-r1 * d22 + r2 * d12) / t2, (r1 * d12 - r2 * d11) / t2
+                else:
+                    t1 = t2 = 0.0
+                rhoe = ((1 - t1 - t2) * h[:, j1] + t1 * h[:, j2] + t2 * h[:, j0]
+                        + b * (f[:, j0] + t1 * g[:, 0] + t2 * g[:, 0]))
+            h[:, j0] = rhoe
+            return rhoe, d
+        # Pulay
+        md = self.mixdim
+        if it < md:
+            rhoe = b * rhoe + (1.0 - b) * h[:, it - 1]
+            f[:, it] = kerker_prec(rhoe - h[:, it - 1], self.cell, 1.0, self.q0)
+            h[:, it] = rhoe
+            return rhoe, np.sqrt(np.sum(f[:, it] ** 2) / n)
+        jc, jn = it % md, (it + 1) % md
+        m = min(it + 1, md) + 1
+        f[:, jc] = kerker_prec(rhoe - h[:, jc], self.cell, 1.0, self.q0)
+        d = np.sqrt(np.sum(f[:, jc] ** 2) / n)
+        a = np.zeros((m, m))
+        for i in range(m - 1):
+            for j in range(i, m - 1):
+                a[i, j] = f[:, i] @ f[:, j]
+                a[j, i] = a[i, j]
+            a[i, m - 1] = a[m - 1, i] = 1.0
+        rhs = np.zeros(m)
+        rhs[m - 1] = 1.0
+        alpha = np.linalg.solve(a, rhs)
+        rhoe = sum(alpha[j] * (h[:, j] + f[:, j]) for j in range(m - 1))
+        rhoe = normalize_rho(rhoe, self.omega, self.nel)
+        h[:, jn] = rhoe
+        return rhoe, d

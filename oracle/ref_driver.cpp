@@ -273,4 +273,82 @@ void ref_random_col(double complex *A, int nelem, long seed) { random_col(A, nel
 
 void ref_fft(double complex *data, int inverse) { fft_fftw3(data, NR1, NR2, NR3, inverse != 0); }
 
+/* ---- SCF pieces (EvalEnergy.cpp, xc_PZ.cpp, NormalizeRho.cpp, the mixers) ---- */
+
+/* The local-potential data EvalEnergy reads: SFAC(is,ig) complex, VPS(is,ig),
+ * RHOPS(is,ig) real (NSP x NG, species fastest), and the scalars. */
+void ref_set_local(const double complex *sfac, const double *vps, const double *rhops, double esr,
+                   double eself, double nel) {
+  const long n = (long)NSP * NG;
+  free(SFAC);
+  free(VPS);
+  free(RHOPS);
+  SFAC = (double complex *)malloc(n * sizeof(double complex));
+  VPS = (double *)malloc(n * sizeof(double));
+  RHOPS = (double *)malloc(n * sizeof(double));
+  for (long i = 0; i < n; i++) {
+    SFAC[i] = sfac[i];
+    VPS[i] = vps[i];
+    RHOPS[i] = rhops[i];
+  }
+  ESR = esr;
+  ESELF = eself;
+  NEL = nel;
+}
+
+/* EvalEnergy(rhoe): rhoe in = density, out = V_eff; e = {ETOT, EKIN, EHT,
+ * EPSEU, ENL, EXC} with EKIN and ENL taken from the arguments. */
+void ref_EvalEnergy(double *rhoe, double ekin, double enl, double *e) {
+  EKIN = ekin;
+  ENL = enl;
+  EvalEnergy(rhoe);
+  e[0] = ETOT;
+  e[1] = EKIN;
+  e[2] = EHT;
+  e[3] = EPSEU;
+  e[4] = ENL;
+  e[5] = EXC;
+}
+
+double ref_xc_PZ(double *rho, double *vxc, int nnr) {
+  double exc = 0.0;
+  xc_PZ(rho, vxc, exc, nnr);
+  return exc;
+}
+
+void ref_NormalizeRho(double *rho, int nnr, double omega, double nel) {
+  NormalizeRho(rho, nnr, omega, nel);
+}
+
+void ref_KerkerPrec(double *diff, int idx1, int nnr, double beta, double q0) {
+  KerkerPrec(diff, idx1, nnr, beta, q0);
+}
+
+void ref_set_mixing(double kerker_q0) { KERKER_Q0 = kerker_q0; }
+
+double ref_PulayRhoMix(int iter, double *rhoe, double *rho_old, double *f, int mixdim, int nnr) {
+  double d = 0.0;
+  PulayRhoMix(iter, rhoe, rho_old, f, mixdim, nnr, d);
+  return d;
+}
+
+double ref_AndersonRhoMix(int iter, double beta, double *rhoe, double *rho_old, double *f,
+                          double *g, int nnr) {
+  double d = 0.0;
+  AndersonRhoMix(iter, beta, rhoe, rho_old, f, g, nnr, d);
+  return d;
+}
+
+double ref_KerkerRhoMix(double beta, double q0, double *rhoe, double *rho_old, int nnr) {
+  double d = 0.0;
+  KerkerRhoMix(beta, q0, rhoe, rho_old, nnr, d);
+  return d;
+}
+
+double ref_SimpleRhoMix(double beta, double *rhoe, double *rho_old, int nnr) {
+  double d = 0.0;
+  SimpleRhoMix(beta, rhoe, rho_old, nnr, d);
+  return d;
+}
+
 }  // extern "C"

@@ -49,6 +49,21 @@ class RefLib:
         L.ref_get_ekin.restype = C.c_double
         L.ref_get_enl.restype = C.c_double
         L.ref_EvalENL.argtypes = []
+        L.ref_set_local.argtypes = [_zp, _dp, _dp, C.c_double, C.c_double, C.c_double]
+        L.ref_EvalEnergy.argtypes = [_dp, C.c_double, C.c_double, _dp]
+        L.ref_xc_PZ.argtypes = [_dp, _dp, C.c_int]
+        L.ref_xc_PZ.restype = C.c_double
+        L.ref_NormalizeRho.argtypes = [_dp, C.c_int, C.c_double, C.c_double]
+        L.ref_KerkerPrec.argtypes = [_dp, C.c_int, C.c_int, C.c_double, C.c_double]
+        L.ref_set_mixing.argtypes = [C.c_double]
+        L.ref_PulayRhoMix.argtypes = [C.c_int, _dp, _dp, _dp, C.c_int, C.c_int]
+        L.ref_PulayRhoMix.restype = C.c_double
+        L.ref_AndersonRhoMix.argtypes = [C.c_int, C.c_double, _dp, _dp, _dp, _dp, C.c_int]
+        L.ref_AndersonRhoMix.restype = C.c_double
+        L.ref_KerkerRhoMix.argtypes = [C.c_double, C.c_double, _dp, _dp, C.c_int]
+        L.ref_KerkerRhoMix.restype = C.c_double
+        L.ref_SimpleRhoMix.argtypes = [C.c_double, _dp, _dp, C.c_int]
+        L.ref_SimpleRhoMix.restype = C.c_double
         L.ref_ApplyHam_block.argtypes = [_zp, _zp, C.c_int, _dp, C.c_int]
         L.ref_ApplyHam.argtypes = [_zp, _zp, C.c_int, _dp]
         L.ref_chebyfilt.argtypes = [_zp, C.c_int, C.c_double, C.c_double, _dp]
@@ -194,6 +209,35 @@ class RefLib:
     def set_nx(self, nx, nempty):
         self.lib.ref_set_nx(nx, nempty)
         self.cell["nx"] = nx
+
+    # ---- SCF pieces (EvalEnergy.cpp, xc_PZ.cpp, NormalizeRho.cpp, the mixers)
+    def set_local(self, sfac, vps, rhops, esr, eself, nel):
+        """sfac, vps, rhops: (NG, NSP) arrays (species fastest in memory)."""
+        self.lib.ref_set_local(np.ascontiguousarray(sfac, dtype=complex),
+                               np.ascontiguousarray(vps, dtype=float),
+                               np.ascontiguousarray(rhops, dtype=float), esr, eself, nel)
+
+    def eval_energy(self, rho, ekin, enl):
+        r = np.array(rho, dtype=float, copy=True)
+        e = np.zeros(6)
+        self.lib.ref_EvalEnergy(r, ekin, enl, e)
+        return r, dict(zip(("ETOT", "EKIN", "EHT", "EPSEU", "ENL", "EXC"), e.tolist()))
+
+    def xc_pz(self, rho):
+        r = np.array(rho, dtype=float, copy=True)
+        v = np.zeros_like(r)
+        exc = self.lib.ref_xc_PZ(r, v, len(r))
+        return v, exc
+
+    def normalize_rho(self, rho, omega, nel):
+        r = np.array(rho, dtype=float, copy=True)
+        self.lib.ref_NormalizeRho(r, len(r), omega, nel)
+        return r
+
+    def kerker_prec(self, x, beta, q0):
+        r = np.array(x, dtype=float, copy=True)
+        self.lib.ref_KerkerPrec(r, 1, len(r), beta, q0)
+        return r
 
     def eval_enl(self):
         """EvalENL() on the C0 / FOCC the last eval_rho_psi left; returns ENL."""

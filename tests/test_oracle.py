@@ -164,3 +164,84 @@ def test_live_eval_enl(ref_cell):
     enl_r = REF.eval_enl()
     enl_o, _ = O.eval_enl(cell, psi, ngw, 6, focc, 1.0)
     assert abs(enl_o - enl_r) < 1e-12 * abs(enl_r)
+
+
+# ------------------------------------------------------------ SCF pieces
+@pytest.fixture(scope="module")
+def scf_case():
+    from scf_case import make_case
+    return make_case()
+
+
+@need_ref
+def test_live_xc_pz_with_stale_points(scf_case):
+    rho = scf_case["rho"].copy()
+    rho[0] = -0.3  # no earlier point: the reference's variables start unset
+    rho[11] = -0.2  # keeps point 10's values (xc_PZ.cpp:27-30)
+    rho[12] = 1e-14
+    v_r, e_r = scf_case["ref"].xc_pz(rho)
+    v_o, e_o = O.xc_pz(rho)
+    assert np.abs(v_o[1:] - v_r[1:]).max() < 1e-14
+    assert abs(e_o - e_r) < 1e-12 * abs(e_r)
+
+
+@need_ref
+def test_live_eval_energy(scf_case):
+    c = scf_case
+    v_r, e_r = c["ref"].eval_energy(c["rho"], 12.5, 0.75)
+    v_o, e_o = O.eval_energy(c["rho"], c["local"], dict(c["ocell"]), 12.5, 0.75)
+    assert np.abs(v_o - v_r).max() < 1e-12 * np.abs(v_r).max()
+    for k in e_r:
+        assert abs(e_o[k] - e_r[k]) < 1e-11 * max(1.0, abs(e_r[k])), k
+
+
+@need_ref
+def test_live_normalize_and_kerker(scf_case):
+    c = scf_case
+    r = c["rho"] * 1.01
+    r[3] = -0.5
+    n_r = c["ref"].normalize_rho(r, c["b"]["omega"], c["nel"])
+    assert np.abs(O.normalize_rho(r, c["b"]["omega"], c["nel"]) - n_r).max() < 1e-14 * n_r.max()
+    x = c["rho"] - c["rho"].mean()
+    k_r = c["ref"].kerker_prec(x, 0.8, 0.6)
+    assert np.abs(O.kerker_prec(x, c["ocell"], 0.8, 0.6) - k_r).max() < 1e-12 * np.abs(k_r).max()
+
+
+def _mix_sequence(c, n=6, seed=3):
+    rng = np.random.default_rng(seed)
+    return [c["rho"] * (1.0 + 0.05 * rng.standard_normal(c["nnr"])) for _ in range(n)]
+
+
+@need_ref
+@pytest.mark.parametrize("kind", [0, 1, 2, 3])
+def test_live_mixers(scf_case, kind):
+    import ctypes as C
+    c = scf_case
+    R, nnr = c["ref"], c["nnr"]
+    mixdim = 3
+    R.lib.ref_set_mixing(0.6)
+    seq = _mix_sequence(c)
+    om = O.Mixer(kind, nnr, c["ocell"], mixdim=mixdim, beta=0.3 if kind != 3 else 0.25, q0=0.6,
+                 omega=c["b"]["omega"], nel=c["nel"], rho_old=c["rho"] if kind < 2 else None)
+    cols = mixdim if kind == 3 else 3
+    h = np.zeros((nnr, cols), order="F")
+    f = np.zeros((nnr, cols), order="F")
+    g = np.zeros((nnr, 2), order="F")
+    if kind < 2:
+        h[:, 0] = c["rho"]
+    for it, rin in enumerate(seq, start=1):
+        r_ref = rin.copy()
+        if kind == 0:
+            d_r = R.lib.ref_SimpleRhoMix(0.3, r_ref, h[:, 0], nnr)
+        elif kind == 1:
+            d_r = R.lib.ref_KerkerRhoMix(0.3, 0.6, r_ref, h[:, 0], nnr)
+        elif kind == 2:
+            d_r = R.lib.ref_AndersonRhoMix(it, 0.3, r_ref, h.reshape(-1, order="F"),
+                                           f.reshape(-1, order="F"), g.reshape(-1, order="F"),
+                                           nnr)
+        else:
+            d_r = R.lib.ref_PulayRhoMix(it, r_ref, h.reshape(-1, order="F"),
+                                        f.reshape(-1, order="F"), mixdim, nnr)
+        r_o, d_o = om.mix(it, rin)
+        assert np.abs(r_o - r_ref).max() < 1e-9 * np.abs(r_ref).max(), (kind, it)
+        assert abs(d_o - d_r) < 1e-9 * max(1.0, abs(d_r)), (kind, it)

@@ -1,0 +1,109 @@
+"""The SCF pieces on the device (pspw_eval_energy, pspw_xc_pz,
+pspw_normalize_rho, pspw_kerker_prec, pspw_mix*) against the reference's own
+EvalEnergy, xc_PZ, NormalizeRho, KerkerPrec and mixers (oracle/_ref/libref.so)
+on the same synthetic 8-atom cell.  FP64 throughout; bars: 1e-12 relative
+for the energy terms and potentials, 1e-9 for densities after mixing (the
+Pulay coefficients come from a different small solver than dsysv)."""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+torch = pytest.importorskip("torch")
+if not torch.cuda.is_available():  # pragma: no cover
+    pytest.skip("needs a CUDA device", allow_module_level=True)
+
+from ref_lib import ref_available  # noqa: E402
+
+if not ref_available("libref.so"):
+    pytest.skip("oracle/_ref reference build not present", allow_module_level=True)
+
+import pspw_oracle as O  # noqa: E402
+from pspw import MIX_ANDERSON, MIX_KERKER, MIX_PULAY, MIX_SIMPLE, PspwError  # noqa: E402
+from scf_case import engine_scf, make_case  # noqa: E402
+
+
+@pytest.fixture(scope="module")
+def case():
+    c = make_case()
+    cell, scf = engine_scf(c)
+    c.update(cell=cell, scf=scf)
+    return c
+
+
+def test_eval_energy_matches_reference(case):
+    v_r, e_r = case["ref"].eval_energy(case["rho"], 12.5, 0.75)
+    v_e, e_e = case["scf"].eval_energy(case["rho"], 12.5, 0.75)
+    assert np.abs(v_e - v_r).max() < 1e-12 * np.abs(v_r).max()
+    for k in e_r:
+        assert abs(e_e[k] - e_r[k]) < 1e-12 * max(1.0, abs(e_r[k])), k
+
+
+def test_eval_energy_is_deterministic(case):
+    a = case["scf"].eval_energy(case["rho"], 1.0, 0.0)
+    b = case["scf"].eval_energy(case["rho"], 1.0, 0.0)
+    assert np.array_equal(a[0], b[0]) and a[1] == b[1]
+
+
+def test_xc_pz_with_stale_points(case):
+    rho = case["rho"].copy()
+    rho[0] = -0.3
+    rho[11] = -0.2
+    rho[12] = 1e-14
+    v_e, e_e = case["scf"].xc_pz(rho)
+    v_r, e_r = case["ref"].xc_pz(rho)
+    assert np.abs(v_e[1:] - v_r[1:]).max() < 1e-14 * np.abs(v_r).max()
+    assert v_e[0] == 0.0
+    assert abs(e_e - e_r) < 1e-12 * abs(e_r)
+
+
+def test_normalize_rho_and_its_errors(case):
+    r = case["rho"] * 1.01
+    r[3] = -0.5
+    n_e, warned = case["scf"].normalize_rho(r)
+    n_r = case["ref"].normalize_rho(r, case["b"]["omega"], case["nel"])
+    assert np.abs(n_e - n_r).max() < 1e-14 * n_r.max()
+    assert warned  # 1% off: the reference prints its warning
+    with pytest.raises(PspwError) as e:
+        case["scf"].normalize_rho(-np.abs(r))
+    assert e.value.code == 8
+
+
+def test_kerker_prec(case):
+    x = case["rho"] - case["rho"].mean()
+    k_e = case["scf"].kerker_prec(x, 0.8, 0.6)
+    k_r = case["ref"].kerker_prec(x, 0.8, 0.6)
+    assert np.abs(k_e - k_r).max() < 1e-12 * np.abs(k_r).max()
+
+
+@pytest.mark.parametrize("kind", [MIX_SIMPLE, MIX_KERKER, MIX_ANDERSON, MIX_PULAY])
+def test_mixers_follow_the_reference(case, kind):
+    c = case
+    R, nnr, mixdim = c["ref"], c["nnr"], 3
+    R.lib.ref_set_mixing(0.6)
+    rng = np.random.default_rng(3)
+    seq = [c["rho"] * (1.0 + 0.05 * rng.standard_normal(nnr)) for _ in range(7)]
+    beta = 0.3 if kind != MIX_PULAY else 0.25
+    c["scf"].mix_init(kind, mixdim=mixdim, beta=beta, q0=0.6,
+                      rho_old=c["rho"] if kind in (MIX_SIMPLE, MIX_KERKER) else None)
+    cols = mixdim if kind == MIX_PULAY else 3
+    h = np.zeros((nnr, cols), order="F")
+    f = np.zeros((nnr, cols), order="F")
+    g = np.zeros((nnr, 2), order="F")
+    if kind in (MIX_SIMPLE, MIX_KERKER):
+        h[:, 0] = c["rho"]
+    for it, rin in enumerate(seq, start=1):
+        r_ref = rin.copy()
+        if kind == MIX_SIMPLE:
+            d_r = R.lib.ref_SimpleRhoMix(beta, r_ref, h[:, 0], nnr)
+        elif kind == MIX_KERKER:
+            d_r = R.lib.ref_KerkerRhoMix(beta, 0.6, r_ref, h[:, 0], nnr)
+        elif kind == MIX_ANDERSON:
+            d_r = R.lib.ref_AndersonRhoMix(it, beta, r_ref, h.reshape(-1, order="F"),
+                                           f.reshape(-1, order="F"), g.reshape(-1, order="F"),
+                                           nnr)
+        else:
+            d_r = R.lib.ref_PulayRhoMix(it, r_ref, h.reshape(-1, order="F"),
+                                        f.reshape(-1, order="F"), mixdim, nnr)
+        r_e, d_e = c["scf"].mix(it, rin)
+        assert np.abs(r_e - r_ref).max() < 1e-9 * np.abs(r_ref).max(), (kind, it)
+        assert abs(d_e - d_r) < 1e-9 * max(1.0, abs(d_r)), (kind, it)
