@@ -76,8 +76,94 @@ constexpr int kSlotA = kWsSolverBase + 11;
 constexpr int kSlotB = kWsSolverBase + 12;
 constexpr int kSlotC = kWsSolverBase + 13;
 constexpr int kSlotD = kWsSolverBase + 14;
+constexpr int kSlotE = kWsEnl;
 
 }  // namespace
+
+// EvalRhoPsi.cpp:83-157 on a device block (ld >= ngw): the charge check and
+// EKIN from column sums, then d_rho += sum_i wkpt focc_i |psi_i(r)|^2 / omega
+// with the scatter stopping at ig < ngw - 1 (EvalRhoPsi.cpp:117).
+// *ekin += the kinetic energy (x TPIBA2).
+int eval_rho_psi_dev(pspw_cell *c, const double2 *dX, int ld, int ngw, int nx, const double *focc,
+                     double wkpt, double omega, double *d_rho, double *ekin) {
+  const Basis &B = c->basis;
+  if (!B.fast) return fail(PSPW_ERR_NOT_IMPL, "EvalRhoPsi: grid lengths without a register split");
+  const int m = ngw - 1;  // the scatter stops at ig < NGW_ik (EvalRhoPsi.cpp:117)
+  double *dsum, *dw;
+  int rc;
+  if ((rc = ws_reserve(c, kSlotB, sizeof(double) * 2 * (size_t)nx, (void **)&dsum)) ||
+      (rc = ws_reserve(c, kSlotD, sizeof(double) * (size_t)nx, (void **)&dw)))
+    return rc;
+  k_charge_sums<<<nx, 256, 0, c->stream>>>(dX, ld, m, B.d_xkg64, dsum, dsum + nx);
+  c->kernel_launches++;
+  std::vector<double> sums(2 * (size_t)nx);
+  PSPW_CUDA(cudaMemcpyAsync(sums.data(), dsum, sizeof(double) * 2 * nx, cudaMemcpyDeviceToHost,
+                            c->stream));
+  if ((rc = sync(c))) return rc;
+  double xkin = 0.0;
+  std::vector<double> wband(nx);
+  for (int i = 0; i < nx; i++) {
+    const double ss = sums[i];
+    if (std::fabs(ss - 1.0) > 6.e-3) {  // EvalRhoPsi.cpp:129-133
+      char msg[160];
+      std::snprintf(msg, sizeof msg,
+                    "Wrong charge density in G-space: %18.10f for k-point 1 and states %d", ss,
+                    i + 1);
+      return fail(PSPW_ERR_CHARGE, msg);
+    }
+    const double wdotf = wkpt * focc[i];
+    xkin = xkin + sums[nx + i] * (wdotf * 0.5);
+    wband[i] = wdotf / omega;
+  }
+  PSPW_CUDA(cudaMemcpyAsync(dw, wband.data(), sizeof(double) * nx, cudaMemcpyHostToDevice, c->stream));
+  const FastGeo g{B.ncol, B.nxa, B.d_col_start, B.d_sg_ig, B.d_sg_z, B.d_sg_col, B.d_xa_list,
+                  B.d_col_x, B.d_col_y, B.d_xa_of_x};
+  if ((rc = rho_fast<double>(c, g, dX, ld, m, nx, dw, d_rho))) return rc;
+  if ((rc = sync(c))) return rc;  // wband lives on the host stack
+  if (ekin) *ekin = *ekin + xkin * c->tpiba2;  // EvalRhoPsi.cpp:154
+  return PSPW_OK;
+}
+
+// EvalENL.cpp:5-49 for one k-point on a device block X (ngw x nx, ld).
+int eval_enl_dev(pspw_cell *c, const double2 *dX, int ld, int ngw, int nx, const double *focc,
+                 double wkpt, double *enl, double *fnl) {
+  const int nproj = c->proj.nproj;
+  *enl = 0.0;
+  if (nx == 0 || nproj == 0) return PSPW_OK;
+  double2 *dP;
+  int rc;
+  if ((rc = ws_reserve(c, kSlotE, sizeof(double2) * (size_t)nx * nproj, (void **)&dP))) return rc;
+  if ((rc = project_fp64(c, dX, ld, ngw, nx, dP))) return rc;
+  std::vector<double2> P((size_t)nx * nproj);
+  std::vector<double> w(nproj);
+  PSPW_CUDA(cudaMemcpyAsync(P.data(), dP, sizeof(double2) * P.size(), cudaMemcpyDeviceToHost,
+                            c->stream));
+  PSPW_CUDA(cudaMemcpyAsync(w.data(), c->proj.d_pw64, sizeof(double) * nproj,
+                            cudaMemcpyDeviceToHost, c->stream));
+  if ((rc = sync(c))) return rc;
+  // projectors are species-major, then atom, then lm: the reference's loop
+  // order (EvalENL.cpp:21-45) for one k-point
+  double e = 0.0;
+  for (int p = 0; p < nproj; p++) {
+    double enl_m = 0.0;
+    for (int ist = 0; ist < nx; ist++) {
+      const double2 sf = P[(size_t)ist * nproj + p];
+      const double a = std::hypot(sf.x, sf.y);
+      enl_m = enl_m + focc[ist] * (a * a);
+    }
+    e = e + wkpt * enl_m * w[p];
+  }
+  *enl = e;
+  if (fnl)
+    for (int p = 0; p < nproj; p++)
+      for (int ist = 0; ist < nx; ist++) {
+        const double2 sf = P[(size_t)ist * nproj + p];
+        fnl[2 * ((size_t)p * nx + ist)] = sf.x;
+        fnl[2 * ((size_t)p * nx + ist) + 1] = sf.y;
+      }
+  return PSPW_OK;
+}
+
 }  // namespace pspw
 
 using namespace pspw;
@@ -219,47 +305,17 @@ int pspw_eval_rho_psi(pspw_cell *c, double *rhoe, const double *eigvec, int ld, 
   if (nx == 0) return PSPW_OK;
   const Basis &B = c->basis;
   if (ngw > B.ngw) return fail(PSPW_ERR_SHAPE, "EvalRhoPsi: NGW exceeds the cell");
-  if (!B.fast) return fail(PSPW_ERR_NOT_IMPL, "EvalRhoPsi: grid lengths without a register split");
-  const int m = ngw - 1;  // the scatter stops at ig < NGW_ik (EvalRhoPsi.cpp:117)
   double2 *dX;
-  double *dsum, *drho, *dw;
+  double *drho;
   if ((rc = ws_reserve(c, kSlotA, sizeof(double2) * (size_t)ld * nx, (void **)&dX)) ||
-      (rc = ws_reserve(c, kSlotB, sizeof(double) * 2 * (size_t)nx, (void **)&dsum)) ||
-      (rc = ws_reserve(c, kSlotC, sizeof(double) * (size_t)B.nnr, (void **)&drho)) ||
-      (rc = ws_reserve(c, kSlotD, sizeof(double) * (size_t)nx, (void **)&dw)))
+      (rc = ws_reserve(c, kSlotC, sizeof(double) * (size_t)B.nnr, (void **)&drho)))
     return rc;
   PSPW_CUDA(cudaMemcpyAsync(dX, eigvec, sizeof(double2) * ((size_t)ld * (nx - 1) + ngw),
                             cudaMemcpyHostToDevice, c->stream));
-  k_charge_sums<<<nx, 256, 0, c->stream>>>(dX, ld, m, B.d_xkg64, dsum, dsum + nx);
-  c->kernel_launches++;
-  std::vector<double> sums(2 * (size_t)nx);
-  PSPW_CUDA(cudaMemcpyAsync(sums.data(), dsum, sizeof(double) * 2 * nx, cudaMemcpyDeviceToHost,
-                            c->stream));
-  if ((rc = sync(c))) return rc;
-  double xkin = 0.0;
-  std::vector<double> wband(nx);
-  for (int i = 0; i < nx; i++) {
-    const double ss = sums[i];
-    if (std::fabs(ss - 1.0) > 6.e-3) {  // EvalRhoPsi.cpp:129-133
-      char msg[160];
-      std::snprintf(msg, sizeof msg,
-                    "Wrong charge density in G-space: %18.10f for k-point 1 and states %d", ss,
-                    i + 1);
-      return fail(PSPW_ERR_CHARGE, msg);
-    }
-    const double wdotf = wkpt * focc[i];
-    xkin = xkin + sums[nx + i] * (wdotf * 0.5);
-    wband[i] = wdotf / omega;
-  }
-  PSPW_CUDA(cudaMemcpyAsync(dw, wband.data(), sizeof(double) * nx, cudaMemcpyHostToDevice, c->stream));
   PSPW_CUDA(cudaMemcpyAsync(drho, rhoe, sizeof(double) * B.nnr, cudaMemcpyHostToDevice, c->stream));
-  const FastGeo g{B.ncol, B.nxa, B.d_col_start, B.d_sg_ig, B.d_sg_z, B.d_sg_col, B.d_xa_list,
-                  B.d_col_x, B.d_col_y, B.d_xa_of_x};
-  if ((rc = rho_fast<double>(c, g, dX, ld, m, nx, dw, drho))) return rc;
+  if ((rc = eval_rho_psi_dev(c, dX, ld, ngw, nx, focc, wkpt, omega, drho, ekin))) return rc;
   PSPW_CUDA(cudaMemcpyAsync(rhoe, drho, sizeof(double) * B.nnr, cudaMemcpyDeviceToHost, c->stream));
-  if ((rc = sync(c))) return rc;
-  if (ekin) *ekin = *ekin + xkin * c->tpiba2;  // EvalRhoPsi.cpp:154
-  return PSPW_OK;
+  return sync(c);
 }
 
 int pspw_eval_enl(pspw_cell *c, const double *c0, int ld, int ngw, int nx, const double *focc,
@@ -269,42 +325,11 @@ int pspw_eval_enl(pspw_cell *c, const double *c0, int ld, int ngw, int nx, const
   if (!c0 || !focc || !enl || nx < 0 || ld < ngw || ngw < 1)
     return fail(PSPW_ERR_ARG, "EvalENL: bad argument");
   if (ngw > c->basis.ngw) return fail(PSPW_ERR_SHAPE, "EvalENL: NGW exceeds the cell");
-  const int nproj = c->proj.nproj;
   *enl = 0.0;
-  if (nx == 0 || nproj == 0) return PSPW_OK;
-  double2 *dX, *dP;
-  if ((rc = up_mat(c, kSlotA, c0, ld, ngw, nx, &dX)) ||
-      (rc = ws_reserve(c, kSlotB, sizeof(double2) * (size_t)nx * nproj, (void **)&dP)))
-    return rc;
-  if ((rc = project_fp64(c, dX, ngw, ngw, nx, dP))) return rc;
-  std::vector<double2> P((size_t)nx * nproj);
-  std::vector<double> w(nproj);
-  PSPW_CUDA(cudaMemcpyAsync(P.data(), dP, sizeof(double2) * P.size(), cudaMemcpyDeviceToHost,
-                            c->stream));
-  PSPW_CUDA(cudaMemcpyAsync(w.data(), c->proj.d_pw64, sizeof(double) * nproj,
-                            cudaMemcpyDeviceToHost, c->stream));
-  if ((rc = sync(c))) return rc;
-  // projectors are species-major, then atom, then lm: the reference's loop
-  // order (EvalENL.cpp:21-45) for one k-point
-  double e = 0.0;
-  for (int p = 0; p < nproj; p++) {
-    double enl_m = 0.0;
-    for (int ist = 0; ist < nx; ist++) {
-      const double2 sf = P[(size_t)ist * nproj + p];
-      const double a = std::hypot(sf.x, sf.y);
-      enl_m = enl_m + focc[ist] * (a * a);
-    }
-    e = e + wkpt * enl_m * w[p];
-  }
-  *enl = e;
-  if (fnl)
-    for (int p = 0; p < nproj; p++)
-      for (int ist = 0; ist < nx; ist++) {
-        const double2 sf = P[(size_t)ist * nproj + p];
-        fnl[2 * ((size_t)p * nx + ist)] = sf.x;
-        fnl[2 * ((size_t)p * nx + ist) + 1] = sf.y;
-      }
-  return PSPW_OK;
+  if (nx == 0 || c->proj.nproj == 0) return PSPW_OK;
+  double2 *dX;
+  if ((rc = up_mat(c, kSlotA, c0, ld, ngw, nx, &dX))) return rc;
+  return eval_enl_dev(c, dX, ngw, ngw, nx, focc, wkpt, enl, fnl);
 }
 
 }  // extern "C"

@@ -110,7 +110,10 @@ enum WsSlot {
   kWsEval = 15,    // eigenvalues of the overlap in eig_zhegv
   kWsSolverBase = 16,  // eigensolver blocks 16..31
   kWsWTile = 32,       // projections as tensor-core operand tiles
-  kWsCount = 33
+  kWsEnl = 33,         // EvalENL projections
+  kWsScfA = 34,        // SCF-piece host entry points: vectors on the device
+  kWsScfB = 35,
+  kWsCount = 36
 };
 
 struct Timing {

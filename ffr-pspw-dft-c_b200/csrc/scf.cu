@@ -738,8 +738,8 @@ int down(pspw_scf *s, double *h, const double *d) {
 int host_vec(pspw_scf *s, int slot, double **d) {
   return ws_reserve(s->cell, slot, sizeof(double) * s->cell->basis.nnr, (void **)d);
 }
-constexpr int kSlotScfA = kWsSolverBase + 9;
-constexpr int kSlotScfB = kWsSolverBase + 10;
+constexpr int kSlotScfA = kWsScfA;
+constexpr int kSlotScfB = kWsScfB;
 }  // namespace
 
 int pspw_eval_energy_dev(pspw_scf *s, double *d_rhoe, double ekin, double enl, double *e6) {

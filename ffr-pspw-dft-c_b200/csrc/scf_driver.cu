@@ -1,0 +1,250 @@
+// The Chebyshev-filtered SCF loop of ChebySCFLoop.cpp:36-378 with every
+// array on the device: V_eff, the densities and the mixing history stay in
+// HBM between iterations, and the host only steers (bounds, convergence).
+// Step for step:
+//   EvalEnergy(start density) -> V_eff; Lanczos (k = max(2 NX, 10) steps)
+//   and the eigenvalues of its T for the filter bounds lb, ub;
+//   first iteration by Davidson (IDIAG >= 0) or the caller's random block;
+//   then per iteration: Chebyshev filter of the NX+2 block, QR, Rayleigh-Ritz
+//   (H X, X^H H X, symmetrize, eigendecomposition, rotation), EvalRhoPsi,
+//   EvalENL, mixing, EvalEnergy, |dETOT| test, new bounds from the Ritz
+//   values and a 10-step Lanczos (ChebySCFLoop.cpp:351-366).
+// The filter may run in FP32 (the mixed-precision mode); everything else is
+// FP64.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <vector>
+
+#include "common.cuh"
+#include "dense.h"
+#include "engine.h"
+#include "gemm.h"
+#include "scf.h"
+#include "solvers.h"
+
+namespace pspw {
+namespace {
+
+__global__ void k_z2c(const double2 *__restrict__ a, float2 *b, size_t n) {
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
+       i += (size_t)gridDim.x * blockDim.x)
+    b[i] = make_float2((float)a[i].x, (float)a[i].y);
+}
+__global__ void k_c2z(const float2 *__restrict__ a, double2 *b, size_t n) {
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
+       i += (size_t)gridDim.x * blockDim.x)
+    b[i] = make_double2(a[i].x, a[i].y);
+}
+__global__ void k_real_to_z(const double *__restrict__ a, double2 *b, int k, int lda) {
+  // the upper triangle of the k x k real matrix a (lda) as a complex matrix
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= k * k) return;
+  const int r = i % k, col = i / k;
+  b[i] = make_double2(r <= col ? a[r + (size_t)lda * col] : 0.0, 0.0);
+}
+
+// ChebySCFLoop.cpp:7-34: |A v1|^2 with v1 = 1/sqrt(N) (ones), A the leading
+// N x N block of the lda-strided matrix
+double induced_norm_mat(const double *A, int lda, int N) {
+  const double d = 1.0 / std::sqrt((double)N);
+  std::vector<double> v(N, 0.0);
+  for (int j = 0; j < N; j++)
+    for (int i = 0; i < N; i++) v[i] += A[i + (size_t)lda * j] * d;
+  double res = 0.0;
+  for (int i = 0; i < N; i++) res += v[i] * v[i];
+  return res;
+}
+
+struct DevBuf {
+  std::vector<void *> p;
+  ~DevBuf() {
+    for (void *q : p) cudaFree(q);
+  }
+  template <typename T>
+  bool get(T **out, size_t n) {
+    void *q = nullptr;
+    if (cudaMalloc(&q, std::max<size_t>(1, n) * sizeof(T)) != cudaSuccess) return false;
+    p.push_back(q);
+    *out = static_cast<T *>(q);
+    return true;
+  }
+};
+
+}  // namespace
+}  // namespace pspw
+
+using namespace pspw;
+
+extern "C" int pspw_cheby_scf(pspw_scf *s, const pspw_scf_params *p, const double *focc,
+                              const double *rho_start, const double *v0, double *X_io,
+                              double *eig, double *rho_out, double *hist, int *iterations,
+                              int *converged, double *e6) {
+  if (!s || !p || !focc || !rho_start || !v0 || !X_io || !eig || !iterations || !converged || !e6)
+    return fail(PSPW_ERR_ARG, "cheby_scf: null argument");
+  pspw_cell *c = s->cell;
+  PSPW_CUDA(cudaSetDevice(c->device));
+  const Basis &B = c->basis;
+  const int nx = p->nx, nx2 = nx + 2, ngw = B.ngw, nnr = B.nnr;
+  const int k = std::max(2 * nx, 10);
+  if (nx < 1 || p->degree < 1 || p->max_scf_iter < 1 || nx2 > ngw || k > ngw)
+    return fail(PSPW_ERR_ARG, "cheby_scf: bad sizes");
+  if (p->imix == 4) return fail(PSPW_ERR_NOT_IMPL, "cheby_scf: Broyden mixing (IMIX = 4)");
+  if (p->filter_prec != PSPW_PREC_F64 && p->filter_prec != PSPW_PREC_F32)
+    return fail(PSPW_ERR_ARG, "cheby_scf: unknown filter precision");
+  const int kind = (p->imix == PSPW_MIX_KERKER || p->imix == PSPW_MIX_ANDERSON ||
+                    p->imix == PSPW_MIX_PULAY)
+                       ? p->imix
+                       : PSPW_MIX_SIMPLE;
+  const double beta = kind == PSPW_MIX_PULAY ? p->pulay_beta : p->mix_beta;
+  int rc;
+  // ---- device arrays
+  DevBuf mem;
+  double2 *X, *HX, *T, *dv0, *df, *dRT;
+  float2 *Xf = nullptr;
+  double *veff, *rho, *wT, *dprec;
+  if (!mem.get(&X, (size_t)ngw * nx2) || !mem.get(&HX, (size_t)ngw * nx2) ||
+      !mem.get(&T, (size_t)nx2 * nx2) || !mem.get(&dv0, ngw) || !mem.get(&df, ngw) ||
+      !mem.get(&dRT, (size_t)k * k) || !mem.get(&veff, nnr) || !mem.get(&rho, nnr) ||
+      !mem.get(&wT, std::max(k, nx2)) || !mem.get(&dprec, ngw) ||
+      (p->filter_prec == PSPW_PREC_F32 && !mem.get(&Xf, (size_t)ngw * nx2)))
+    return fail(PSPW_ERR_OOM, "cheby_scf: device memory");
+  cudaStream_t st = c->stream;
+  // rhoe2 = rho_old = the starting density (ChebySCFLoop.cpp:164-175)
+  PSPW_CUDA(cudaMemcpyAsync(veff, rho_start, sizeof(double) * nnr, cudaMemcpyHostToDevice, st));
+  PSPW_CUDA(cudaMemcpyAsync(dv0, v0, sizeof(double2) * ngw, cudaMemcpyHostToDevice, st));
+  // simple and Kerker mixing start from rho_old = the start density; the
+  // Anderson and Pulay histories start at zero (ChebySCFLoop.cpp:123-148),
+  // so the first Pulay step mixes the new density with zero
+  const bool mix_from_start = kind == PSPW_MIX_SIMPLE || kind == PSPW_MIX_KERKER;
+  if ((rc = pspw_mix_init(s, kind, p->mixdim, beta, p->kerker_q0,
+                          mix_from_start ? rho_start : nullptr)))
+    return rc;
+  double en[6];
+  // EvalEnergy(rhoe2) with the EKIN, ENL of before the loop (zero)
+  if ((rc = eval_energy_dev(s, veff, 0.0, 0.0, en))) return rc;
+  double etot_old = en[0];
+  if ((rc = pspw_cell_set_veff_device(c, veff, nnr))) return rc;
+  // ---- Lanczos bounds (ChebySCFLoop.cpp:180-198)
+  std::vector<double> rT((size_t)k * k, 0.0), evT(std::max(k, nx2));
+  if ((rc = lanczos_dev(c, dv0, ngw, k, rT.data(), k, df))) return rc;
+  {
+    double *dr;
+    if (!mem.get(&dr, (size_t)k * k)) return fail(PSPW_ERR_OOM, "cheby_scf: device memory");
+    PSPW_CUDA(cudaMemcpyAsync(dr, rT.data(), sizeof(double) * k * k, cudaMemcpyHostToDevice, st));
+    k_real_to_z<<<(k * k + 255) / 256, 256, 0, st>>>(dr, dRT, k, k);
+    c->kernel_launches++;
+    int info = 0;
+    if ((rc = dev_zheevd(c, dRT, k, wT, k, &info))) return rc;  // dsyev('N','U') values
+    PSPW_CUDA(cudaMemcpyAsync(evT.data(), wT, sizeof(double) * k, cudaMemcpyDeviceToHost, st));
+    PSPW_CUDA(cudaStreamSynchronize(st));
+    if (info) return fail(PSPW_ERR_LAPACK, "cheby_scf: eigenvalues of the Lanczos T");
+  }
+  double lb = evT[nx + 1], ub = evT[2 * nx - 1];
+  std::vector<double> evals(nx2), res(nx2);
+  int iter_start = 1, done_iters = 0;
+  *converged = 0;
+  auto record = [&](int it, double etot, double detot, double drms) {
+    if (hist && it >= 1 && it <= p->max_scf_iter) {
+      hist[3 * (it - 1)] = etot;
+      hist[3 * (it - 1) + 1] = detot;
+      hist[3 * (it - 1) + 2] = drms;
+    }
+  };
+  // density, EKIN, ENL of the first nx columns of X (ld ngw), then mixing
+  // and EvalEnergy (ChebySCFLoop.cpp:232-262 and 321-348)
+  auto density_step = [&](int it, double *etot, double *drms) -> int {
+    int r;
+    PSPW_CUDA(cudaMemsetAsync(rho, 0, sizeof(double) * nnr, st));
+    double ekin = 0.0, enl = 0.0;
+    if ((r = eval_rho_psi_dev(c, X, ngw, ngw, nx, focc, 1.0, s->omega, rho, &ekin))) return r;
+    if ((r = eval_enl_dev(c, X, ngw, ngw, nx, focc, 1.0, &enl, nullptr))) return r;
+    if ((r = mix_dev(s, it, rho, drms))) return r;
+    PSPW_CUDA(cudaMemcpyAsync(veff, rho, sizeof(double) * nnr, cudaMemcpyDeviceToDevice, st));
+    if ((r = eval_energy_dev(s, veff, ekin, enl, en))) return r;
+    *etot = en[0];
+    return pspw_cell_set_veff_device(c, veff, nnr);
+  };
+  if (p->idiag < 0) {
+    // the caller's random block, orthonormalised (ChebySCFLoop.cpp:201-209)
+    PSPW_CUDA(cudaMemcpyAsync(X, X_io, sizeof(double2) * (size_t)ngw * nx2, cudaMemcpyHostToDevice,
+                              st));
+    int info = 0;
+    if ((rc = dev_ortho_qr(c, X, ngw, ngw, nx2, &info))) return rc;
+  } else {
+    // first iteration by Davidson (ChebySCFLoop.cpp:210-262)
+    if ((rc = gen_prec_dev(c, dprec, ngw, -10.0))) return rc;
+    int its = 0;
+    if ((rc = davidson_dev(c, PSPW_PREC_F64, evals.data(), X, ngw, nx2, dprec, p->nempty,
+                           p->max_diag_iter, res.data(), &its)))
+      return rc;
+    double etot = 0.0, drms = 0.0;
+    if ((rc = density_step(1, &etot, &drms))) return rc;
+    const double detot = std::fabs(etot - etot_old);
+    record(1, etot, detot, drms);
+    etot_old = etot;
+    iter_start = 2;
+    done_iters = 1;
+  }
+  std::vector<double> rT10((size_t)k * k, 0.0);
+  double *dfn;
+  if (!mem.get(&dfn, 1)) return fail(PSPW_ERR_OOM, "cheby_scf: device memory");
+  for (int it = iter_start; it <= p->max_scf_iter; it++) {
+    // filter the NX+2 block (ChebySCFLoop.cpp:285)
+    if (p->filter_prec == PSPW_PREC_F32) {
+      const size_t n = (size_t)ngw * nx2;
+      k_z2c<<<4 * 148, 256, 0, st>>>(X, Xf, n);
+      if ((rc = pspw_chebyfilt_dev(c, PSPW_PREC_F32, Xf, ngw, ngw, nx2, p->degree, lb, ub)))
+        return rc;
+      k_c2z<<<4 * 148, 256, 0, st>>>(Xf, X, n);
+      c->kernel_launches += 2;
+    } else if ((rc = pspw_chebyfilt_dev(c, PSPW_PREC_F64, X, ngw, ngw, nx2, p->degree, lb, ub))) {
+      return rc;
+    }
+    int info = 0;
+    if ((rc = dev_ortho_qr(c, X, ngw, ngw, nx2, &info))) return rc;
+    // Rayleigh-Ritz (ChebySCFLoop.cpp:293-307)
+    if ((rc = hpsi_apply<double>(c, X, ngw, HX, ngw, ngw, nx2, 1.0, 0.0, 0.0, nullptr, ngw)))
+      return rc;
+    const double2 one = make_double2(1.0, 0.0), zero = make_double2(0.0, 0.0);
+    if ((rc = zgemm<double>(c, 'C', nx2, nx2, ngw, one, X, ngw, HX, ngw, zero, T, nx2))) return rc;
+    if ((rc = dev_symmetrize(c, T, nx2, nx2))) return rc;
+    if ((rc = dev_zheevd(c, T, nx2, wT, nx2, &info))) return rc;
+    if ((rc = zgemm<double>(c, 'N', ngw, nx2, nx2, one, X, ngw, T, nx2, zero, HX, ngw))) return rc;
+    std::swap(X, HX);
+    PSPW_CUDA(cudaMemcpyAsync(evals.data(), wT, sizeof(double) * nx2, cudaMemcpyDeviceToHost, st));
+    PSPW_CUDA(cudaStreamSynchronize(st));
+    if (info) return fail(PSPW_ERR_LAPACK, "cheby_scf: Rayleigh-Ritz eigensolver");
+    double etot = 0.0, drms = 0.0;
+    if ((rc = density_step(it, &etot, &drms))) return rc;
+    const double detot = std::fabs(etot - etot_old);
+    record(it, etot, detot, drms);
+    etot_old = etot;
+    done_iters = it;
+    if (detot <= p->conv) {
+      *converged = 1;
+      break;
+    }
+    // new bounds (ChebySCFLoop.cpp:356-366)
+    lb = evals[nx + 1];
+    const int kl = k > 10 ? 10 : k;
+    if ((rc = lanczos_dev(c, dv0, ngw, kl, rT10.data(), k, df))) return rc;
+    double fn = 0.0;
+    if ((rc = dev_coldot(c, df, ngw, df, ngw, ngw, 1, dfn))) return rc;
+    PSPW_CUDA(cudaMemcpyAsync(&fn, dfn, sizeof(double), cudaMemcpyDeviceToHost, st));
+    PSPW_CUDA(cudaStreamSynchronize(st));
+    ub = induced_norm_mat(rT10.data(), k, kl) + std::sqrt(fn);
+  }
+  // results
+  for (int i = 0; i < nx; i++) eig[i] = evals[i];
+  PSPW_CUDA(cudaMemcpyAsync(X_io, X, sizeof(double2) * (size_t)ngw * nx2, cudaMemcpyDeviceToHost,
+                            st));
+  if (rho_out)
+    PSPW_CUDA(cudaMemcpyAsync(rho_out, rho, sizeof(double) * nnr, cudaMemcpyDeviceToHost, st));
+  PSPW_CUDA(cudaStreamSynchronize(st));
+  for (int i = 0; i < 6; i++) e6[i] = en[i];
+  *iterations = done_iters;
+  return device_status(c);
+}

@@ -17,4 +17,10 @@ int lobpcg_dev(pspw_cell *c, int hprec, double *lambda_host, double2 *X, int nba
 // v0: device, normalised in place; T_host k x k (ldT); f_out device or null
 int lanczos_dev(pspw_cell *c, double2 *v0, int ngw, int k, double *T_host, int ldT, double2 *f_out);
 
+// EvalRhoPsi / EvalENL on device blocks (capi_solvers.cu); see pspw_gpu.h.
+int eval_rho_psi_dev(pspw_cell *c, const double2 *dX, int ld, int ngw, int nx, const double *focc,
+                     double wkpt, double omega, double *d_rho, double *ekin);
+int eval_enl_dev(pspw_cell *c, const double2 *dX, int ld, int ngw, int nx, const double *focc,
+                 double wkpt, double *enl, double *fnl);
+
 }  // namespace pspw

@@ -92,6 +92,7 @@ SIGNATURES = {
     "pspw_mix_init": [_vp, _i, _i, _d, _d, _vp],
     "pspw_mix": [_vp, _i, _vp, _vp],
     "pspw_mix_dev": [_vp, _i, _vp, _vp],
+    "pspw_cheby_scf": [_vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp],
 }
 _RESTYPE = {"pspw_error_string": C.c_char_p, "pspw_last_error": C.c_char_p}
 

@@ -1,5 +1,6 @@
 """The SCF pieces of the C ABI (pspw_scf_*, pspw_eval_energy, pspw_xc_pz,
-pspw_normalize_rho, pspw_kerker_prec, pspw_mix*) over a Cell."""
+pspw_normalize_rho, pspw_kerker_prec, pspw_mix*) and the device SCF loop
+(pspw_cheby_scf) over a Cell."""
 from __future__ import annotations
 
 import ctypes as C
@@ -7,6 +8,15 @@ import ctypes as C
 import numpy as np
 
 from ._lib import check, lib
+
+
+class ScfParams(C.Structure):
+    """pspw_scf_params: the INPUT controls of the SCF loop."""
+    _fields_ = [("nx", C.c_int), ("nempty", C.c_int), ("degree", C.c_int),
+                ("max_scf_iter", C.c_int), ("conv", C.c_double), ("imix", C.c_int),
+                ("mixdim", C.c_int), ("mix_beta", C.c_double), ("pulay_beta", C.c_double),
+                ("kerker_q0", C.c_double), ("idiag", C.c_int), ("max_diag_iter", C.c_int),
+                ("filter_prec", C.c_int)]
 
 
 def _c(a, dtype):
@@ -87,3 +97,36 @@ class Scf:
         d = C.c_double(0.0)
         check(lib().pspw_mix(self._h, int(it), r.ctypes.data, C.byref(d)))
         return r, d.value
+
+    def cheby_scf(self, focc, rho_start, v0, X=None, *, nx, nempty, degree=10,
+                  max_scf_iter=40, conv=1e-6, imix=0, mixdim=4, mix_beta=0.3,
+                  pulay_beta=0.25, kerker_q0=0.5, idiag=0, max_diag_iter=0, filter_prec=0):
+        """The SCF loop of ChebySCFLoop.cpp on the device (pspw_cheby_scf).
+        X: NGW x (NX+2) start block for idiag < 0 (ignored otherwise).
+        Returns a dict with eig (NX), X (final block), rho (final mixed
+        density), hist (iterations x {ETOT, |dETOT|, d}), energies,
+        iterations and converged."""
+        ngw = self.cell.sizes()["ngw"]
+        nx2 = nx + 2
+        p = ScfParams(nx, nempty, degree, max_scf_iter, conv, imix, mixdim, mix_beta, pulay_beta,
+                      kerker_q0, idiag, max_diag_iter, filter_prec)
+        fo = _c(focc, float)
+        rs = _c(rho_start, float)
+        v = _c(np.asarray(v0, complex)[:ngw], complex)
+        x = (np.zeros((ngw, nx2), complex) if X is None
+             else np.asarray(X, complex)[:ngw, :nx2].copy())
+        xf = np.asfortranarray(x)
+        eig = np.zeros(nx)
+        rho = np.zeros(self.nnr)
+        hist = np.zeros(3 * max_scf_iter)
+        its, cv = C.c_int(0), C.c_int(0)
+        e6 = np.zeros(6)
+        check(lib().pspw_cheby_scf(self._h, C.byref(p), fo.ctypes.data, rs.ctypes.data,
+                                   v.ctypes.data, xf.ctypes.data, eig.ctypes.data,
+                                   rho.ctypes.data, hist.ctypes.data, C.byref(its), C.byref(cv),
+                                   e6.ctypes.data))
+        n = its.value
+        return dict(eig=eig, X=xf, rho=rho, hist=hist.reshape(-1, 3)[:n], iterations=n,
+                    converged=bool(cv.value),
+                    energies=dict(zip(("ETOT", "EKIN", "EHT", "EPSEU", "ENL", "EXC"),
+                                      e6.tolist())))

@@ -253,6 +253,44 @@ int pspw_mix_init(pspw_scf *scf, int kind, int mixdim, double beta, double q0,
 int pspw_mix(pspw_scf *scf, int iter, double *rhoe, double *d);
 int pspw_mix_dev(pspw_scf *scf, int iter, double *d_rhoe, double *d);
 
+/* ------------------------------------------------------------------ SCF loop
+ * pspw_cheby_scf: the Chebyshev-filtered SCF iteration of ChebySCFLoop.cpp:
+ * 36-378 (one k-point) with V_eff, the densities, the mixing history and the
+ * wavefunction block on the device.
+ *   params     the reference's INPUT controls (below)
+ *   focc       NX occupations (FOCC)
+ *   rho_start  the normalised starting density (NNR; the reference builds it
+ *              with FormFactorAtomic + NormalizeRho, ChebySCFLoop.cpp:160-168)
+ *   v0         the Lanczos start vector (NGW complex; the reference draws it
+ *              with rand(), ChebySCFLoop.cpp:100-106)
+ *   X          NGW x (NX+2) complex: the start block when idiag < 0 (it is
+ *              orthonormalised), the final block on return
+ *   eig        NX eigenvalues (EIG); rho_out (may be null) the final mixed
+ *              density; hist (may be null) 3 x max_scf_iter (ETOT, |dETOT|,
+ *              the mixer's d) per iteration; e6 the final {ETOT, EKIN, EHT,
+ *              EPSEU, ENL, EXC}; *iterations the last iteration done;
+ *              *converged = 1 if |dETOT| <= conv was reached.
+ * The pspw_scf handle supplies the local potential data, OMEGA and NEL. */
+typedef struct {
+  int nx;             /* NX: occupied + empty states; the filter works on NX + 2 */
+  int nempty;         /* NEMPTY (Davidson's convergence count) */
+  int degree;         /* CHEBYPOL_DEGREE */
+  int max_scf_iter;   /* MAX_SCF_ITER */
+  double conv;        /* SCF_CONV_CRIT on |ETOT - ETOT_old| (Ha) */
+  int imix;           /* IMIX: 1 Kerker, 2 Anderson, 3 Pulay, 4 Broyden (not
+                         built: PSPW_ERR_NOT_IMPL), other: simple */
+  int mixdim;         /* MIXDIM (Pulay) */
+  double mix_beta;    /* RHO_MIX_FAC (simple, Kerker, Anderson) */
+  double pulay_beta;  /* the Pulay warm-up beta (0.25 in the reference) */
+  double kerker_q0;   /* KERKER_Q0 */
+  int idiag;          /* IDIAG: >= 0 first iteration by Davidson, < 0 start from X */
+  int max_diag_iter;  /* Davidson iteration cap; 0 = the reference's default */
+  int filter_prec;    /* PSPW_PREC_F64, or PSPW_PREC_F32 for the filter only */
+} pspw_scf_params;
+int pspw_cheby_scf(pspw_scf *scf, const pspw_scf_params *params, const double *focc,
+                   const double *rho_start, const double *v0, double *X, double *eig,
+                   double *rho_out, double *hist, int *iterations, int *converged, double *e6);
+
 /* ------------------------------------------------------------------ timing
  * Optional device timing on the cell stream: CUDA events around each launch
  * of the enabled families, summed until reset.  Families (bit i of the mask):

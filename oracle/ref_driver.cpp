@@ -345,6 +345,89 @@ double ref_KerkerRhoMix(double beta, double q0, double *rhoe, double *rho_old, i
   return d;
 }
 
+/* ---- the reference program's own set-up and SCF loop (main.cpp) ---- */
+
+/* ReadInputFile + Setup + PrepareSCF on the INPUT in the current directory */
+void ref_prog_setup(void) {
+  ReadInputFile();
+  Setup();
+  PrepareSCF();
+}
+
+/* the starting density of ChebySCFLoop.cpp:157-168 and EwaldEnergy() */
+void ref_prog_start_density(double *rho) {
+  double complex *c = (double complex *)malloc(NNR * sizeof(double complex));
+  for (int i = 0; i < NNR; i++) c[i] = Z_ZERO;
+  FormFactorAtomic(c);
+  fft_fftw3(c, NR1, NR2, NR3, true);
+  for (int i = 0; i < NNR; i++) rho[i] = creal(c[i]);
+  NormalizeRho(rho, NNR, OMEGA, NEL);
+  free(c);
+  EwaldEnergy();
+}
+
+/* SFAC (NSP x NG complex), VPS, RHOPS (NSP x NG of NSP x NGX), and
+ * scal = {ESR, ESELF, NEL, OMEGA} */
+void ref_get_local(double complex *sfac, double *vps, double *rhops, double *scal) {
+  for (long i = 0; i < (long)NSP * NG; i++) {
+    sfac[i] = SFAC[i];
+    vps[i] = VPS[i];
+    rhops[i] = RHOPS[i];
+  }
+  scal[0] = ESR;
+  scal[1] = ESELF;
+  scal[2] = NEL;
+  scal[3] = OMEGA;
+}
+
+/* PKG_A (NLMAX x NGWX x NSP, k-point 1) and WNL (NSP x NLMAX) */
+void ref_get_nl(double *pkg_a, double *wnl) {
+  for (long i = 0; i < (long)NLMAX * NGWX * NSP; i++) pkg_a[i] = PKG_A[i];
+  for (long i = 0; i < (long)NSP * NLMAX; i++) wnl[i] = WNL[i];
+}
+
+/* NA, L_MAX, L_LOC per species (NSP entries each) */
+void ref_get_species(int *na, int *lmax, int *lloc) {
+  for (int is = 0; is < NSP; is++) {
+    na[is] = NA[is];
+    lmax[is] = L_MAX[is];
+    lloc[is] = L_LOC[is];
+  }
+}
+
+/* iv = {NX, NEMPTY, CHEBYPOL_DEGREE, MAX_SCF_ITER, IMIX, MIXDIM, IDIAG,
+ *       USER_MAX_DIAG_ITER, MAX_DIAG_ITER},
+ * dv = {SCF_CONV_CRIT, RHO_MIX_FAC, KERKER_Q0}, focc = FOCC (NX) */
+void ref_get_ctrl(int *iv, double *dv, double *focc) {
+  iv[0] = NX;
+  iv[1] = NEMPTY;
+  iv[2] = CHEBYPOL_DEGREE;
+  iv[3] = MAX_SCF_ITER;
+  iv[4] = IMIX;
+  iv[5] = MIXDIM;
+  iv[6] = IDIAG;
+  iv[7] = USER_MAX_DIAG_ITER ? 1 : 0;
+  iv[8] = MAX_DIAG_ITER;
+  dv[0] = SCF_CONV_CRIT;
+  dv[1] = RHO_MIX_FAC;
+  dv[2] = KERKER_Q0;
+  for (int i = 0; i < NX; i++) focc[i] = FOCC[i];
+}
+
+/* ChebySCFLoop() with rand() seeded by srand(1); eig = EIG (NX), e6 =
+ * {ETOT, EKIN, EHT, EPSEU, ENL, EXC} at the end */
+void ref_prog_cheby_scf(double *eig, double *e6) {
+  srand(1);
+  ChebySCFLoop();
+  for (int i = 0; i < NX; i++) eig[i] = EIG[i];
+  e6[0] = ETOT;
+  e6[1] = EKIN;
+  e6[2] = EHT;
+  e6[3] = EPSEU;
+  e6[4] = ENL;
+  e6[5] = EXC;
+}
+
 double ref_SimpleRhoMix(double beta, double *rhoe, double *rho_old, int nnr) {
   double d = 0.0;
   SimpleRhoMix(beta, rhoe, rho_old, nnr, d);

@@ -80,6 +80,13 @@ class RefLib:
         L.ref_EvalRhoPsi.argtypes = [_dp, _zp, C.c_int, C.c_int]
         L.ref_random_col.argtypes = [_zp, C.c_int, C.c_long]
         L.ref_fft.argtypes = [_zp, C.c_int]
+        L.ref_prog_setup.argtypes = []
+        L.ref_prog_start_density.argtypes = [_dp]
+        L.ref_get_local.argtypes = [_zp, _dp, _dp, _dp]
+        L.ref_get_nl.argtypes = [_dp, _dp]
+        L.ref_get_species.argtypes = [_ip, _ip, _ip]
+        L.ref_get_ctrl.argtypes = [_ip, _dp, _dp]
+        L.ref_prog_cheby_scf.argtypes = [_dp, _dp]
         self.cell = None
 
     # ------------------------------------------------------------ set-up
@@ -96,6 +103,10 @@ class RefLib:
             float(ecut_ry), nr_arr, nsp, np.asarray(na, dtype=np.int32),
             np.ascontiguousarray(taua.reshape(-1)), np.asarray(zv, dtype=float),
             np.asarray(lmax, dtype=np.int32), np.asarray(lloc, dtype=np.int32), int(nempty))
+        return self._read_cell(list(na), lmax, lloc)
+
+    def _read_cell(self, na, lmax, lloc):
+        nsp = len(na)
         d = np.zeros(12, dtype=np.int32)
         self.lib.ref_get_dims(d)
         sc = np.zeros(8)
@@ -120,6 +131,60 @@ class RefLib:
                     na=list(na), lm_end=[int(l * l - 2 * ll + 1) for l, ll in zip(lmax, lloc)])
         self.cell = dims
         return dims
+
+    # ------------------------------------------------ the reference program
+    def program_setup(self, workdir):
+        """The reference program's own set-up (main.cpp: ReadInputFile,
+        Setup, PrepareSCF) on the INPUT in ``workdir``, its starting density
+        (ChebySCFLoop.cpp:157-168) and EwaldEnergy.  Returns the cell dict of
+        ``setup`` plus pkg_a, wnl, sfac/vps/rhops (ng x nsp), esr, eself,
+        rho_start and the control values of the INPUT."""
+        cwd = os.getcwd()
+        os.chdir(workdir)
+        try:
+            self.lib.ref_prog_setup()
+            d = np.zeros(12, dtype=np.int32)
+            self.lib.ref_get_dims(d)
+            nsp, nnr = int(d[11]), int(d[3])
+            na, lmax, lloc = (np.zeros(nsp, dtype=np.int32) for _ in range(3))
+            self.lib.ref_get_species(na, lmax, lloc)
+            b = self._read_cell([int(x) for x in na], [int(x) for x in lmax],
+                                [int(x) for x in lloc])
+            rho = np.zeros(nnr)
+            self.lib.ref_prog_start_density(rho)
+        finally:
+            os.chdir(cwd)
+        ng, nlmax, ngwx = b["ng"], b["nlmax"], b["ngwx"]
+        sfac = np.zeros(ng * nsp, dtype=complex)
+        vps, rhops, scal = np.zeros(ng * nsp), np.zeros(ng * nsp), np.zeros(4)
+        self.lib.ref_get_local(sfac, vps, rhops, scal)
+        pkg_a, wnl = np.zeros(nlmax * ngwx * nsp), np.zeros(nsp * nlmax)
+        self.lib.ref_get_nl(pkg_a, wnl)
+        iv, dv, focc = np.zeros(9, dtype=np.int32), np.zeros(3), np.zeros(b["nx"])
+        self.lib.ref_get_ctrl(iv, dv, focc)
+        b.update(sfac=sfac.reshape((ng, nsp), order="F"), vps=vps.reshape((ng, nsp), order="F"),
+                 rhops=rhops.reshape((ng, nsp), order="F"), esr=scal[0], eself=scal[1],
+                 pkg_a=pkg_a.reshape((nlmax, ngwx, nsp), order="F"),
+                 wnl=wnl.reshape((nsp, nlmax), order="F"), rho_start=rho, focc=focc,
+                 ctrl=dict(nx=int(iv[0]), nempty=int(iv[1]), degree=int(iv[2]),
+                           max_scf_iter=int(iv[3]), imix=int(iv[4]), mixdim=int(iv[5]),
+                           idiag=int(iv[6]), user_max_diag_iter=int(iv[7]),
+                           max_diag_iter=int(iv[8]), conv=dv[0], rho_mix_fac=dv[1],
+                           kerker_q0=dv[2]))
+        return b
+
+    def program_cheby_scf(self, workdir):
+        """ChebySCFLoop() after ``program_setup`` with rand() seeded by
+        srand(1); returns (EIG[:NX], {ETOT, EKIN, EHT, EPSEU, ENL, EXC})."""
+        nx = self.cell["nx"]
+        eig, e6 = np.zeros(nx), np.zeros(6)
+        cwd = os.getcwd()
+        os.chdir(workdir)
+        try:
+            self.lib.ref_prog_cheby_scf(eig, e6)
+        finally:
+            os.chdir(cwd)
+        return eig, e6
 
     def set_nl(self, pkg_a, wnl):
         self.lib.ref_set_nl(np.ascontiguousarray(np.asarray(pkg_a).reshape(-1, order="F")),

@@ -1,0 +1,126 @@
+"""The device SCF loop (pspw_cheby_scf) against the reference program's own
+ChebySCFLoop on the same INPUT: an 8-atom Si cell with a synthetic FHI98
+pseudopotential at ECUT 8 Ry.  The reference's set-up (cell, form factors,
+structure factors, start density) comes from the reference itself, run in a
+separate process by tests/ref_program_case.py; the Lanczos start vector is
+the same glibc rand() stream after srand(1) (ChebySCFLoop.cpp:100-106)."""
+import ctypes as C
+import os
+import subprocess
+import sys
+
+import numpy as np
+import pytest
+
+from helpers import scf_lines, write_input, write_synthetic_fhi
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+REF_LIB = os.path.join(HERE, "..", "oracle", "_ref", "libref.so")
+
+pytestmark = pytest.mark.gpu
+
+
+def _glibc_rand_stream(n):
+    """n values rand()/RAND_MAX after srand(1) from the C library the
+    reference links."""
+    libc = C.CDLL("libc.so.6")
+    libc.srand(1)
+    return np.array([libc.rand() for _ in range(n)], dtype=float) / 2147483647.0
+
+
+def _reference_run(tmp_path, name, **input_kw):
+    d = tmp_path / name
+    d.mkdir()
+    write_synthetic_fhi(str(d / "X.fhi"))
+    from pspw import synth
+    lat, pos = synth.si_diamond(1)
+    write_input(str(d / "INPUT"), "X.fhi", pos, 10.26, ecut_ry=8.0, **input_kw)
+    out = str(d / "case.npz")
+    r = subprocess.run([sys.executable, os.path.join(HERE, "ref_program_case.py"), str(d), out],
+                       capture_output=True, text=True, timeout=900)
+    assert r.returncode == 0, r.stdout[-2000:] + r.stderr[-2000:]
+    z = dict(np.load(out))
+    ctrl = dict(zip(z.pop("ctrl_names").tolist(), z.pop("ctrl_values").tolist()))
+    return z, ctrl, scf_lines(r.stdout)
+
+
+def _engine(z):
+    from pspw import Cell
+    from pspw.scf import Scf
+    ng = int(z["ng"])
+    cell = Cell.from_arrays(dict(nr=tuple(int(x) for x in z["nr"]), ngw=int(z["ngw"]),
+                                 ngwx=int(z["ngwx"]), n123=z["n123"], xkg=z["xkg"],
+                                 tpiba2=float(z["tpiba2"]), na=[int(x) for x in z["na"]],
+                                 lm_end=[int(x) for x in z["lm_end"]], eigr=z["eigr"],
+                                 pkg_a=z["pkg_a"], wnl=z["wnl"]))
+    s = Scf(cell, z["N1"][:ng], z["N2"][:ng], z["N3"][:ng], z["G"][:ng], z["sfac"], z["vps"],
+            z["rhops"], float(z["omega"]), float(z["nel"]), float(z["esr"]), float(z["eself"]))
+    return cell, s
+
+
+def _run_engine(z, ctrl, filter_prec=0):
+    cell, s = _engine(z)
+    ngw, ngwx, nx = int(z["ngw"]), int(z["ngwx"]), int(ctrl["nx"])
+    nx2 = nx + 2
+    r = _glibc_rand_stream(2 * ngwx + 2 * ngw * nx2)
+    v0 = r[0:2 * ngwx:2] + 1j * r[1:2 * ngwx:2]
+    xr = r[2 * ngwx:]
+    X = (xr[0::2] + 1j * xr[1::2]).reshape((ngw, nx2), order="F")
+    res = s.cheby_scf(z["focc"], z["rho_start"], v0[:ngw], X, nx=nx, nempty=int(ctrl["nempty"]),
+                      degree=int(ctrl["degree"]), max_scf_iter=int(ctrl["max_scf_iter"]),
+                      conv=ctrl["conv"], imix=int(ctrl["imix"]), mixdim=int(ctrl["mixdim"]),
+                      mix_beta=ctrl["rho_mix_fac"], pulay_beta=0.25,
+                      kerker_q0=ctrl["kerker_q0"], idiag=int(ctrl["idiag"]),
+                      max_diag_iter=int(ctrl["max_diag_iter"]) if ctrl["user_max_diag_iter"]
+                      else 0, filter_prec=filter_prec)
+    s.close()
+    cell.close()
+    return res
+
+
+def _check(ref_lines, z, res, nat=8, final_tol=1e-6):
+    """Same start, same fixed point.  The first iteration's Davidson (or the
+    first filter) stops on a residual test, so rounding moves early densities
+    by ~1e-6; both loops then stop on |dETOT| <= 1e-6 at the same fixed
+    point, possibly one or two iterations apart."""
+    hist = res["hist"]
+    assert res["converged"] and ref_lines[-1][2] <= 1e-6
+    assert abs(hist[0, 0] - ref_lines[0][1]) < 1e-4
+    n = min(4, len(ref_lines), len(hist))
+    assert np.abs(hist[:n, 0] - np.array([l[1] for l in ref_lines[:n]])).max() < 1e-3
+    assert abs(res["iterations"] - len(ref_lines)) <= 4
+    assert abs(res["energies"]["ETOT"] - z["e6"][0]) / nat < final_tol
+    assert abs(hist[-1, 0] - ref_lines[-1][1]) / nat < final_tol
+    nocc = int(round(float(z["nel"]) / 2))
+    assert np.abs(res["eig"][:nocc] - z["eig"][:nocc]).max() < 1e-4
+
+
+def test_cheby_scf_davidson_start_anderson(tmp_path):
+    """IDIAG = 0 (first iteration by Davidson), Anderson mixing."""
+    z, ctrl, lines = _reference_run(tmp_path, "anderson", imix=2, max_scf=40)
+    res = _run_engine(z, ctrl)
+    _check(lines, z, res)
+
+
+def test_cheby_scf_random_start_pulay(tmp_path):
+    """IDIAG < 0 (random start block from the same rand() stream), Pulay."""
+    z, ctrl, lines = _reference_run(tmp_path, "pulay", imix=3, idiag=-1, max_scf=60)
+    res = _run_engine(z, ctrl)
+    _check(lines, z, res)
+
+
+def test_cheby_scf_kerker(tmp_path):
+    z, ctrl, lines = _reference_run(tmp_path, "kerker", imix=1, max_scf=60)
+    res = _run_engine(z, ctrl)
+    _check(lines, z, res)
+
+
+def test_cheby_scf_f32_filter(tmp_path):
+    """The filter in FP32, everything else FP64: the same converged energy
+    (to 1e-5 Ha/atom) and occupied eigenvalues."""
+    z, ctrl, lines = _reference_run(tmp_path, "f32", imix=2, max_scf=40)
+    res = _run_engine(z, ctrl, filter_prec=1)
+    assert res["converged"]
+    assert abs(res["energies"]["ETOT"] - z["e6"][0]) / 8 < 1e-5
+    nocc = int(round(float(z["nel"]) / 2))
+    assert np.abs(res["eig"][:nocc] - z["eig"][:nocc]).max() < 1e-4
