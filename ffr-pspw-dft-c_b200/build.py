@@ -27,7 +27,7 @@ CUDA = os.environ.get("CUDA_HOME", "/usr/local/cuda")
 NVCC = os.path.join(CUDA, "bin", "nvcc")
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
-NVFLAGS = ARCH + ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC,-fvisibility=hidden",
+NVFLAGS = ARCH + ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC,-fvisibility=hidden,-ffp-contract=off",
                   "--expt-relaxed-constexpr", "-I", INC, "-I", CSRC]
 CXXFLAGS = ["-O2", "-std=c++17", "-fPIC", "-ffp-contract=off", "-fvisibility=hidden", "-I", INC,
             "-I", CSRC]
@@ -35,7 +35,7 @@ CXXFLAGS = ["-O2", "-std=c++17", "-fPIC", "-ffp-contract=off", "-fvisibility=hid
 # libpspw_gpu.so
 GPU_SOURCES = ["basis.cpp", "cell.cu", "hpsi.cu", "fftpath_f32.cu", "fftpath_f64.cu", "capi.cu",
                "noalloc.cu", "gemm.cu", "dense.cu", "solvers.cu", "capi_solvers.cu", "nl_tc.cu",
-               "scf.cu", "scf_driver.cu"]
+               "scf.cu", "scf_driver.cu", "input.cpp", "geom.cu"]
 GPU_LIBS = ["-lcusolver", "-lcublas", "-lcudart"]
 # libpspw_dropin.so (links libpspw_gpu.so)
 DROPIN_SOURCES = ["dropin.cpp"]

@@ -20,6 +20,7 @@
 #include <vector>
 
 #include "pspw_gpu.h"
+#include "basis.h"
 
 namespace {
 
@@ -201,6 +202,60 @@ void fill_info(const Lattice &L, double ecut, const int *nr_forced, pspw_basis_i
 
 }  // namespace
 
+namespace pspw {
+
+void phase_tables(const double *lattice9, const int nr[3], int nsp, const int *na,
+                  const double *tau, PhaseTables *pt) {
+  Lattice L = make_lattice(lattice9);
+  int nax = 0;
+  for (int s = 0; s < nsp; s++) nax = na[s] > nax ? na[s] : nax;
+  pt->nax = nax;
+  pt->nsp = nsp;
+  double xmat[9], xmati[9];
+  for (int i = 0; i < 3; i++) {
+    xmat[0 * 3 + i] = L.a1[i];
+    xmat[1 * 3 + i] = L.a2[i];
+    xmat[2 * 3 + i] = L.a3[i];
+  }
+  inv3(xmat, xmati);
+  for (int d = 0; d < 3; d++) {
+    pt->zero[d] = (nr[d] + 1) / 2 + 1;
+    // The reference sizes these tables NR+1 (AllocateArrays.cpp:29-34) but its
+    // loops (PhaseFactor.cpp:44-61) reach index NR+2 when NR is odd, one
+    // past the end; one spare slot keeps that write inside the table here.
+    pt->len[d] = nr[d] + 2;
+    // zero for atoms a >= na[s] (the reference's zero-filled arrays)
+    pt->ei[d].assign((size_t)2 * pt->len[d] * nax * nsp, 0.0);
+  }
+  for (int s = 0; s < nsp; s++) {
+    for (int a = 0; a < na[s]; a++) {
+      const double *tp = tau + ((size_t)s * nax + a) * 3;
+      const size_t sa = (size_t)s * nax + a;
+      for (int d = 0; d < 3; d++) {
+        double acc = xmati[0 * 3 + d] * tp[0];
+        acc = acc + xmati[1 * 3 + d] * tp[1];
+        acc = acc + xmati[2 * 3 + d] * tp[2];
+        const double ar = -2.0 * M_PI * acc;
+        std::vector<double> &e = pt->ei[d];
+        const size_t b = sa * pt->len[d] + pt->zero[d] - 1;
+        e[2 * b] = 1.0;
+        e[2 * b + 1] = 0.0;
+        for (int i = 1; i <= (nr[d] + 1) / 2; i++) {
+          const double c = std::cos(i * ar), sn = std::sin(i * ar);
+          e[2 * (b + i)] = c;
+          e[2 * (b + i) + 1] = sn;
+          e[2 * (b - i)] = c;
+          e[2 * (b - i) + 1] = -sn;
+        }
+      }
+    }
+  }
+}
+
+void matinv3(const double *hm, double *hi) { inv3(hm, hi); }
+
+}  // namespace pspw
+
 extern "C" int pspw_basis_info_gamma(const double *lattice9, double ecut_ry, const int *nr_forced,
                                      pspw_basis_info *info) {
   if (!lattice9 || !info || !(ecut_ry > 0.0)) return PSPW_ERR_ARG;
@@ -311,75 +366,24 @@ extern "C" int pspw_basis_build_gamma(const double *lattice9, double ecut_ry, co
   info->ngw = ngw;
   // phase factors EIGR(NGWX, NAX, NSP), interleaved complex
   if (eigr && tau) {
-    int nax = 0;
-    for (int s = 0; s < nsp; s++) nax = na[s] > nax ? na[s] : nax;
-    double xmat[9], xmati[9];
-    for (int i = 0; i < 3; i++) {
-      xmat[0 * 3 + i] = L.a1[i];
-      xmat[1 * 3 + i] = L.a2[i];
-      xmat[2 * 3 + i] = L.a3[i];
-    }
-    inv3(xmat, xmati);
-    const int z1 = (nr1 + 1) / 2 + 1, z2 = (nr2 + 1) / 2 + 1, z3 = (nr3 + 1) / 2 + 1;
-    // The reference sizes these tables NR+1 (AllocateArrays.cpp:29-34) but its
-    // loops (PhaseFactor.cpp:182-199) reach index NR+2 when NR is odd, one
-    // past the end; one spare slot keeps that write inside the table here.
-    const int l1 = nr1 + 2, l2 = nr2 + 2, l3 = nr3 + 2;
-    // EI tables, zero for atoms a >= na[s] (the reference's zero-filled arrays)
-    std::vector<double> ei1((size_t)2 * l1 * nax * nsp, 0.0), ei2((size_t)2 * l2 * nax * nsp, 0.0),
-        ei3((size_t)2 * l3 * nax * nsp, 0.0);
-    auto set = [](std::vector<double> &e, size_t at, double re, double im) {
-      e[2 * at] = re;
-      e[2 * at + 1] = im;
-    };
-    for (int s = 0; s < nsp; s++) {
-      for (int a = 0; a < na[s]; a++) {
-        const double *tp = tau + ((size_t)s * nax + a) * 3;
-        double taup[3];
-        for (int i = 0; i < 3; i++) {
-          double acc = xmati[0 * 3 + i] * tp[0];
-          acc = acc + xmati[1 * 3 + i] * tp[1];
-          acc = acc + xmati[2 * 3 + i] * tp[2];
-          taup[i] = acc;
-        }
-        const size_t b1 = ((size_t)s * nax + a) * l1, b2 = ((size_t)s * nax + a) * l2,
-                     b3 = ((size_t)s * nax + a) * l3;
-        set(ei1, b1 + z1 - 1, 1.0, 0.0);
-        set(ei2, b2 + z2 - 1, 1.0, 0.0);
-        set(ei3, b3 + z3 - 1, 1.0, 0.0);
-        const double ar1 = -2.0 * M_PI * taup[0], ar2 = -2.0 * M_PI * taup[1],
-                     ar3 = -2.0 * M_PI * taup[2];
-        for (int i = 1; i <= (nr1 + 1) / 2; i++) {
-          const double c = std::cos(i * ar1), sn = std::sin(i * ar1);
-          set(ei1, b1 + z1 + i - 1, c, sn);
-          set(ei1, b1 + z1 - i - 1, c, -sn);
-        }
-        for (int i = 1; i <= (nr2 + 1) / 2; i++) {
-          const double c = std::cos(i * ar2), sn = std::sin(i * ar2);
-          set(ei2, b2 + z2 + i - 1, c, sn);
-          set(ei2, b2 + z2 - i - 1, c, -sn);
-        }
-        for (int i = 1; i <= (nr3 + 1) / 2; i++) {
-          const double c = std::cos(i * ar3), sn = std::sin(i * ar3);
-          set(ei3, b3 + z3 + i - 1, c, sn);
-          set(ei3, b3 + z3 - i - 1, c, -sn);
-        }
-      }
-    }
+    pspw::PhaseTables pt;
+    const int nr[3] = {nr1, nr2, nr3};
+    pspw::phase_tables(lattice9, nr, nsp, na, tau, &pt);
+    const int nax = pt.nax;
     for (long i = 0; i < 2L * ngwx * nax * nsp; i++) eigr[i] = 0.0;
     for (int s = 0; s < nsp; s++) {
       for (int a = 0; a < nax; a++) {
-        const size_t b1 = ((size_t)s * nax + a) * l1, b2 = ((size_t)s * nax + a) * l2,
-                     b3 = ((size_t)s * nax + a) * l3;
+        const size_t sa = (size_t)s * nax + a;
         for (int ig = 0; ig < ngw; ig++) {
           const int igp = igk[ig];
-          const size_t p1 = b1 + z1 + in1[igp - 1] - 1, p2 = b2 + z2 + in2[igp - 1] - 1,
-                       p3 = b3 + z3 + in3[igp - 1] - 1;
-          const double ar = ei1[2 * p1], ai = ei1[2 * p1 + 1];
-          const double br = ei2[2 * p2], bi = ei2[2 * p2 + 1];
-          const double cr = ei3[2 * p3], ci = ei3[2 * p3 + 1];
+          const size_t p1 = sa * pt.len[0] + pt.zero[0] + in1[igp - 1] - 1,
+                       p2 = sa * pt.len[1] + pt.zero[1] + in2[igp - 1] - 1,
+                       p3 = sa * pt.len[2] + pt.zero[2] + in3[igp - 1] - 1;
+          const double ar = pt.ei[0][2 * p1], ai = pt.ei[0][2 * p1 + 1];
+          const double br = pt.ei[1][2 * p2], bi = pt.ei[1][2 * p2 + 1];
+          const double cr = pt.ei[2][2 * p3], ci = pt.ei[2][2 * p3 + 1];
           const double tr = ar * br - ai * bi, ti = ar * bi + ai * br;
-          const size_t o = (((size_t)s * nax + a) * ngwx + ig) * 2;
+          const size_t o = (sa * ngwx + ig) * 2;
           eigr[o] = tr * cr - ti * ci;
           eigr[o + 1] = tr * ci + ti * cr;
         }

@@ -87,7 +87,6 @@ constexpr int kSlotE = kWsEnl;
 int eval_rho_psi_dev(pspw_cell *c, const double2 *dX, int ld, int ngw, int nx, const double *focc,
                      double wkpt, double omega, double *d_rho, double *ekin) {
   const Basis &B = c->basis;
-  if (!B.fast) return fail(PSPW_ERR_NOT_IMPL, "EvalRhoPsi: grid lengths without a register split");
   const int m = ngw - 1;  // the scatter stops at ig < NGW_ik (EvalRhoPsi.cpp:117)
   double *dsum, *dw;
   int rc;
@@ -116,9 +115,13 @@ int eval_rho_psi_dev(pspw_cell *c, const double2 *dX, int ld, int ngw, int nx, c
     wband[i] = wdotf / omega;
   }
   PSPW_CUDA(cudaMemcpyAsync(dw, wband.data(), sizeof(double) * nx, cudaMemcpyHostToDevice, c->stream));
-  const FastGeo g{B.ncol, B.nxa, B.d_col_start, B.d_sg_ig, B.d_sg_z, B.d_sg_col, B.d_xa_list,
-                  B.d_col_x, B.d_col_y, B.d_xa_of_x};
-  if ((rc = rho_fast<double>(c, g, dX, ld, m, nx, dw, d_rho))) return rc;
+  if (B.fast) {
+    const FastGeo g{B.ncol, B.nxa, B.d_col_start, B.d_sg_ig, B.d_sg_z, B.d_sg_col, B.d_xa_list,
+                    B.d_col_x, B.d_col_y, B.d_xa_of_x};
+    if ((rc = rho_fast<double>(c, g, dX, ld, m, nx, dw, d_rho))) return rc;
+  } else if ((rc = rho_generic(c, dX, ld, m, nx, dw, d_rho))) {
+    return rc;
+  }
   if ((rc = sync(c))) return rc;  // wband lives on the host stack
   if (ekin) *ekin = *ekin + xkin * c->tpiba2;  // EvalRhoPsi.cpp:154
   return PSPW_OK;

@@ -238,6 +238,45 @@ int pspw_cell_create(pspw_cell **out, int device, int nr1, int nr2, int nr3, int
                      const unsigned int *n123, const double *xkg, double tpiba2, int nsp,
                      const int *na, int nax, const int *lm_end, int nlmax, const double *eigr,
                      const double *pkg_a, const double *wnl) {
+  return pspw::cell_create(out, device, nr1, nr2, nr3, ngw, ngwx, n123, xkg, tpiba2, nsp, na, nax,
+                           lm_end, nlmax, eigr, pkg_a, wnl, nullptr, nullptr);
+}
+
+}  // extern "C"
+
+namespace pspw {
+namespace {
+
+// Projector arrays of the cell from device copies of EIGR(NGWX, NAX, NSP) and
+// PKG_A(NLMAX, NGWX, NSP): the same packing as the host loop of cell_create.
+__global__ void k_pack_projectors(const double2 *__restrict__ eigr, const double *__restrict__ pkga,
+                                  const int *__restrict__ atom_col, int nat, int ngw, int ngwx,
+                                  int nsp, int nlmax, double2 *e64, float2 *e32, double *k64,
+                                  float *k32) {
+  const long long ne = (long long)nat * ngw, nk = (long long)nsp * ngw * 4;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < ne + nk;
+       i += (long long)gridDim.x * blockDim.x) {
+    if (i < ne) {
+      const int ga = (int)(i / ngw), ig = (int)(i % ngw);
+      const double2 v = eigr[(size_t)atom_col[ga] * ngwx + ig];
+      e64[i] = v;
+      e32[i] = make_float2((float)v.x, (float)v.y);
+    } else {
+      const long long j = i - ne;
+      const int lm = (int)(j % 4), ig = (int)((j / 4) % ngw), s = (int)(j / (4LL * ngw));
+      const double v = lm < nlmax ? pkga[((size_t)s * ngwx + ig) * nlmax + lm] : 0.0;
+      k64[j] = v;
+      k32[j] = (float)v;
+    }
+  }
+}
+
+}  // namespace
+
+int cell_create(pspw_cell **out, int device, int nr1, int nr2, int nr3, int ngw, int ngwx,
+                const unsigned int *n123, const double *xkg, double tpiba2, int nsp, const int *na,
+                int nax, const int *lm_end, int nlmax, const double *eigr, const double *pkg_a,
+                const double *wnl, const double2 *d_eigr, const double *d_pkg_a) {
   if (!out || !n123 || !xkg || !na || !lm_end) return fail(PSPW_ERR_ARG, "cell_create: null argument");
   *out = nullptr;
   if (nr1 < 1 || nr2 < 1 || nr3 < 1 || ngw < 1 || ngwx < ngw || nsp < 0 || nax < 0 || nlmax < 0)
@@ -253,7 +292,9 @@ int pspw_cell_create(pspw_cell **out, int device, int nr1, int nr2, int nr3, int
     nat += na[s];
     nproj += na[s] * std::max(0, lm_end[s]);
   }
-  if (nproj > 0 && (!eigr || !pkg_a || !wnl)) return fail(PSPW_ERR_ARG, "cell_create: null projector arrays");
+  const bool dev_src = d_eigr && d_pkg_a;
+  if (nproj > 0 && (!wnl || (!dev_src && (!eigr || !pkg_a))))
+    return fail(PSPW_ERR_ARG, "cell_create: null projector arrays");
   PSPW_CUDA(cudaSetDevice(device));
   pspw_cell *c = new pspw_cell();
   c->device = device;
@@ -358,18 +399,19 @@ int pspw_cell_create(pspw_cell **out, int device, int nr1, int nr2, int nr3, int
   P.nsp = nsp;
   P.nproj = nproj;
   if (nproj > 0) {
-    std::vector<double2> e64((size_t)nat * ngw);
-    std::vector<float2> e32((size_t)nat * ngw);
-    std::vector<double> k64((size_t)nsp * ngw * 4, 0.0);
-    std::vector<float> k32((size_t)nsp * ngw * 4, 0.f);
-    std::vector<int> patom, psp, plm;
+    std::vector<double2> e64(dev_src ? 0 : (size_t)nat * ngw);
+    std::vector<float2> e32(dev_src ? 0 : (size_t)nat * ngw);
+    std::vector<double> k64(dev_src ? 0 : (size_t)nsp * ngw * 4, 0.0);
+    std::vector<float> k32(dev_src ? 0 : (size_t)nsp * ngw * 4, 0.f);
+    std::vector<int> patom, psp, plm, atom_col;
     std::vector<double> pw64;
     std::vector<float> pw32;
     int ga = 0;
     for (int s = 0; s < nsp; s++) {
       for (int a = 0; a < na[s]; a++, ga++) {
-        const double *src = eigr + 2 * (((size_t)s * nax + a) * ngwx);
-        for (int ig = 0; ig < ngw; ig++) {
+        atom_col.push_back(s * nax + a);
+        for (int ig = 0; ig < ngw && !dev_src; ig++) {
+          const double *src = eigr + 2 * (((size_t)s * nax + a) * ngwx);
           e64[(size_t)ga * ngw + ig] = make_double2(src[2 * ig], src[2 * ig + 1]);
           e32[(size_t)ga * ngw + ig] = make_float2((float)src[2 * ig], (float)src[2 * ig + 1]);
         }
@@ -382,16 +424,37 @@ int pspw_cell_create(pspw_cell **out, int device, int nr1, int nr2, int nr3, int
           pw32.push_back((float)wv);
         }
       }
-      for (int ig = 0; ig < ngw; ig++)
+      for (int ig = 0; ig < ngw && !dev_src; ig++)
         for (int lm = 0; lm < std::min(4, nlmax); lm++) {
           const double v = pkg_a[((size_t)s * ngwx + ig) * nlmax + lm];  // PKG_A(lm,ig,is)
           k64[((size_t)s * ngw + ig) * 4 + lm] = v;
           k32[((size_t)s * ngw + ig) * 4 + lm] = (float)v;
         }
     }
-    if ((rc = upload(&P.d_eigr64, e64)) || (rc = upload(&P.d_eigr32, e32)) ||
-        (rc = upload(&P.d_pkga64, k64)) || (rc = upload(&P.d_pkga32, k32)) ||
-        (rc = upload(&P.d_patom, patom)) || (rc = upload(&P.d_psp, psp)) ||
+    if (dev_src) {
+      int *d_col = nullptr;
+      if ((rc = upload(&d_col, atom_col))) return bail(rc);
+      const size_t ne = (size_t)nat * ngw, nk = (size_t)nsp * ngw * 4;
+      const bool ok = cudaMalloc(&P.d_eigr64, ne * sizeof(double2)) == cudaSuccess &&
+                      cudaMalloc(&P.d_eigr32, ne * sizeof(float2)) == cudaSuccess &&
+                      cudaMalloc(&P.d_pkga64, nk * sizeof(double)) == cudaSuccess &&
+                      cudaMalloc(&P.d_pkga32, nk * sizeof(float)) == cudaSuccess;
+      if (ok) {
+        const int blocks = (int)std::min<size_t>((ne + nk + 255) / 256, 148 * 16);
+        k_pack_projectors<<<blocks, 256, 0, c->stream>>>(d_eigr, d_pkg_a, d_col, nat, ngw, ngwx,
+                                                         nsp, nlmax,
+                                                         P.d_eigr64, P.d_eigr32, P.d_pkga64,
+                                                         P.d_pkga32);
+        c->kernel_launches++;
+      }
+      const cudaError_t e = ok ? cudaStreamSynchronize(c->stream) : cudaErrorMemoryAllocation;
+      cudaFree(d_col);
+      if (e != cudaSuccess) return bail(fail(ok ? PSPW_ERR_CUDA : PSPW_ERR_OOM, "cell_create: packing projectors"));
+    } else if ((rc = upload(&P.d_eigr64, e64)) || (rc = upload(&P.d_eigr32, e32)) ||
+               (rc = upload(&P.d_pkga64, k64)) || (rc = upload(&P.d_pkga32, k32))) {
+      return bail(rc);
+    }
+    if ((rc = upload(&P.d_patom, patom)) || (rc = upload(&P.d_psp, psp)) ||
         (rc = upload(&P.d_plm, plm)) || (rc = upload(&P.d_pw64, pw64)) ||
         (rc = upload(&P.d_pw32, pw32)))
       return bail(rc);
@@ -408,7 +471,7 @@ int pspw_cell_create(pspw_cell **out, int device, int nr1, int nr2, int nr3, int
   return PSPW_OK;
 }
 
-}  // extern "C"
+}  // namespace pspw
 
 namespace pspw {
 namespace {

@@ -163,6 +163,13 @@ namespace pspw {
 
 // error state
 int fail(int code, const std::string &msg);
+// pspw_cell_create, with the projector arrays taken from device copies of
+// EIGR(NGWX, NAX, NSP) and PKG_A(NLMAX, NGWX, NSP) when d_eigr and d_pkg_a
+// are given (eigr and pkg_a are then unused).
+int cell_create(pspw_cell **out, int device, int nr1, int nr2, int nr3, int ngw, int ngwx,
+                const unsigned int *n123, const double *xkg, double tpiba2, int nsp, const int *na,
+                int nax, const int *lm_end, int nlmax, const double *eigr, const double *pkg_a,
+                const double *wnl, const double2 *d_eigr, const double *d_pkg_a);
 int cuda_fail(cudaError_t e, const char *what);
 #define PSPW_CUDA(call)                                   \
   do {                                                    \

@@ -29,4 +29,8 @@ template <typename R>
 int rho_fast(pspw_cell *c, const FastGeo &g, const cx<R> *psi, int ld, int ngw_scatter, int nb,
              const double *d_wband, double *d_rho);
 
+// The same on the generic FFT path (any grid length; hpsi.cu), FP64.
+int rho_generic(pspw_cell *c, const double2 *psi, int ld, int ngw_scatter, int nb,
+                const double *d_wband, double *d_rho);
+
 }  // namespace pspw

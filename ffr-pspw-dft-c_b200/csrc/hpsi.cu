@@ -171,6 +171,54 @@ __global__ void __launch_bounds__(kNT) k_xlines(Geo g, FftArg fx, const T *__res
   }
 }
 
+// ---------------------------------------------------------------- density
+// EvalRhoPsi on the generic path: after the stick and plane passes, each
+// block takes L3 x-lines of every band of the batch in band order, inverse-
+// transforms them and accumulates w_b |psi_b(r)|^2 in FP64; one block owns
+// each line, so rho is updated band after band in the reference's order
+// (EvalRhoPsi.cpp:136-149) with no atomics.
+template <typename T>
+__global__ void __launch_bounds__(kNT) k_xlines_rho(Geo g, FftArg fx, const T *__restrict__ wx,
+                                                    const T *__restrict__ P, int nbb,
+                                                    const double *__restrict__ wband,
+                                                    double *__restrict__ rho, int L3) {
+  extern __shared__ unsigned char smem_raw[];
+  T *a = reinterpret_cast<T *>(smem_raw);
+  const int ls = pad(g.n1);
+  T *b = a + L3 * ls;
+  double *acc = reinterpret_cast<double *>(b + L3 * ls);
+  const int l0 = blockIdx.x * L3;
+  const int nlines = g.n2 * g.n3;
+  const int nl = min(L3, nlines - l0);
+  for (int e = threadIdx.x; e < L3 * g.n1; e += blockDim.x) acc[e] = 0.0;
+  for (int band = 0; band < nbb; band++) {
+    const T *Pb = P + (size_t)band * nlines * g.nxa;
+    __syncthreads();
+    for (int e = threadIdx.x; e < L3 * g.n1; e += blockDim.x) {
+      const int l = e / g.n1, x = e - l * g.n1;
+      T v = czero<T>();
+      if (l < nl) {
+        const int xa = g.xa_of_x[x];
+        if (xa >= 0) v = Pb[(size_t)(l0 + l) * g.nxa + xa];
+      }
+      a[l * ls + x] = v;
+    }
+    __syncthreads();
+    const T *r = fft_lines(a, b, L3, ls, fx, wx, +1);
+    const double w = wband[band];
+    for (int e = threadIdx.x; e < L3 * g.n1; e += blockDim.x) {
+      const int l = e / g.n1, x = e - l * g.n1;
+      const T v = r[l * ls + x];
+      acc[e] += w * ((double)v.x * (double)v.x + (double)v.y * (double)v.y);
+    }
+  }
+  __syncthreads();
+  for (int e = threadIdx.x; e < L3 * g.n1; e += blockDim.x) {
+    const int l = e / g.n1, x = e - l * g.n1;
+    if (l < nl) rho[(size_t)(l0 + l) * g.n1 + x] += acc[e];
+  }
+}
+
 // ---------------------------------------------------------------- pass 4
 template <typename T>
 __global__ void __launch_bounds__(kNT) k_planes_fwd(Geo g, FftArg fy, const T *__restrict__ wy,
@@ -447,6 +495,46 @@ int set_smem(K kernel, size_t bytes) {
 }
 
 }  // namespace
+
+// rho += sum_b wband[b] |psi_b(r)|^2 for any grid the generic FFT handles;
+// psi scattered for ig < ngw_scatter (EvalRhoPsi.cpp:117).
+int rho_generic(pspw_cell *c, const double2 *psi, int ld, int ngw_scatter, int nb,
+                const double *d_wband, double *d_rho) {
+  using T = double2;
+  const Basis &B = c->basis;
+  cudaStream_t st = c->stream;
+  Geo geo{B.n1, B.n2, B.n3, B.ncol, B.nxa, B.ngw, B.d_col_start, B.d_sg_ig, B.d_sg_z,
+          B.d_sg_col, B.d_col_of_xy, B.d_xa_list, B.d_xa_of_x};
+  const size_t s_band = (size_t)B.n3 * B.ncol, p_band = (size_t)B.n3 * B.n2 * B.nxa;
+  int nbatch = c->band_batch;
+  if (nbatch <= 0) nbatch = (int)std::max<size_t>(1, (48u << 20) / ((s_band + p_band) * sizeof(T)));
+  nbatch = std::min(nbatch, nb);
+  T *S = nullptr, *P = nullptr;
+  int rc;
+  if ((rc = ws_reserve(c, kWsSticks, sizeof(T) * s_band * nbatch, (void **)&S)) ||
+      (rc = ws_reserve(c, kWsPlanes, sizeof(T) * p_band * nbatch, (void **)&P)))
+    return rc;
+  const int T1 = tile_lines(B.n3), T2 = tile_lines(B.n2), L3 = tile_lines(B.n1);
+  const size_t sm1 = pass_smem<T>(T1, B.n3), sm2 = pass_smem<T>(T2, B.n2),
+               sm3 = pass_smem<T>(L3, B.n1) + sizeof(double) * (size_t)L3 * B.n1;
+  if ((rc = set_smem<T>(k_sticks_inv<T>, sm1)) || (rc = set_smem<T>(k_planes_inv<T>, sm2)) ||
+      (rc = set_smem<T>(k_xlines_rho<T>, sm3)))
+    return rc;
+  const FftArg fx = fft_arg(B.dim[0]), fy = fft_arg(B.dim[1]), fz = fft_arg(B.dim[2]);
+  const T *wx = tw<T>(B.dim[0]), *wy = tw<T>(B.dim[1]), *wz = tw<T>(B.dim[2]);
+  for (int b0 = 0; b0 < nb; b0 += nbatch) {
+    const int nbb = std::min(nbatch, nb - b0);
+    k_sticks_inv<T><<<dim3((B.ncol + T1 - 1) / T1, nbb), kNT, sm1, st>>>(
+        geo, fz, wz, psi + (size_t)b0 * ld, ld, ngw_scatter, S, T1);
+    k_planes_inv<T><<<dim3((B.nxa + T2 - 1) / T2, B.n3, nbb), kNT, sm2, st>>>(geo, fy, wy, S, P,
+                                                                              T2);
+    k_xlines_rho<T><<<(B.n2 * B.n3 + L3 - 1) / L3, kNT, sm3, st>>>(geo, fx, wx, P, nbb,
+                                                                   d_wband + b0, d_rho, L3);
+    c->kernel_launches += 3;
+  }
+  PSPW_CUDA(cudaGetLastError());
+  return PSPW_OK;
+}
 
 template <typename R>
 int hpsi_apply(pspw_cell *c, const void *in_v, int ld_in, void *out_v, int ld_out, int ngw, int nb,

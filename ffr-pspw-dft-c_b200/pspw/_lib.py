@@ -93,6 +93,16 @@ SIGNATURES = {
     "pspw_mix": [_vp, _i, _vp, _vp],
     "pspw_mix_dev": [_vp, _i, _vp, _vp],
     "pspw_cheby_scf": [_vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp],
+    "pspw_system_load": [C.c_char_p, _i, _vp],
+    "pspw_system_destroy": [_vp],
+    "pspw_system_info": [_vp, _vp, _vp],
+    "pspw_system_params": [_vp, _vp],
+    "pspw_system_array": [_vp, _i, _vp, C.c_longlong],
+    "pspw_system_cell": [_vp, _vp],
+    "pspw_system_scf": [_vp, _vp],
+    "pspw_system_timing": [_vp, _vp],
+    "pspw_system_cheby_scf": [_vp, _i, C.c_char_p, _vp, _vp, _vp, _vp, _vp],
+    "pspw_print_3d_array": [_vp, _i, _i, _i, C.c_char_p],
 }
 _RESTYPE = {"pspw_error_string": C.c_char_p, "pspw_last_error": C.c_char_p}
 

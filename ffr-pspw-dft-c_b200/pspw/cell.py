@@ -88,14 +88,28 @@ class Cell:
                    cell["tpiba2"], cell["na"], cell["lm_end"], cell["eigr"], cell["pkg_a"],
                    cell["wnl"], device=device)
 
+    @classmethod
+    def borrow(cls, handle, nr, ngw, device=0, owner=None):
+        """A view of a cell owned elsewhere (e.g. by a System): closing it
+        does not destroy the handle; `owner` is kept alive."""
+        c = cls.__new__(cls)
+        c._h = handle
+        c._owned = False
+        c._owner = owner
+        c.nr = tuple(int(x) for x in nr)
+        c.nnr = c.nr[0] * c.nr[1] * c.nr[2]
+        c.ngw = int(ngw)
+        c.device = device
+        return c
+
     @property
     def handle(self):
         return self._h
 
     def close(self):
-        if self._h:
+        if self._h and getattr(self, "_owned", True):
             lib().pspw_cell_destroy(self._h)
-            self._h = C.c_void_p()
+        self._h = C.c_void_p()
 
     def __del__(self):
         try:

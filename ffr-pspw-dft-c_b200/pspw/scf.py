@@ -50,10 +50,22 @@ class Scf:
         self._h = h
         self.nnr = int(np.prod(cell.sizes()["n1"] * cell.sizes()["n2"] * cell.sizes()["n3"]))
 
+    @classmethod
+    def borrow(cls, handle, cell, owner=None):
+        """A view of an SCF handle owned elsewhere (e.g. by a System)."""
+        s = cls.__new__(cls)
+        s._h = handle
+        s._owned = False
+        s._owner = owner
+        s.cell = cell
+        sz = cell.sizes()
+        s.nnr = int(sz["n1"] * sz["n2"] * sz["n3"])
+        return s
+
     def close(self):
-        if self._h:
+        if self._h and getattr(self, "_owned", True):
             lib().pspw_scf_destroy(self._h)
-            self._h = C.c_void_p()
+        self._h = C.c_void_p()
 
     def __del__(self):
         try:

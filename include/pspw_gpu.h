@@ -291,6 +291,61 @@ int pspw_cheby_scf(pspw_scf *scf, const pspw_scf_params *params, const double *f
                    const double *rho_start, const double *v0, double *X, double *eig,
                    double *rho_out, double *hist, int *iterations, int *converged, double *e6);
 
+/* ------------------------------------------------------------------ system
+ * One system set up from the reference's own input files, the way its main
+ * program does before the SCF loop (main.cpp:20-30):
+ *   pspw_system_load      ReadInputFile (INPUT in `dir`), ReadPseudopotentials
+ *                         (FHI98 files named in INPUT, relative to `dir`),
+ *                         Setup, PrepareSCF (PhaseFactor, StructureFactor,
+ *                         FormFactor, NLFormFactor), the starting density of
+ *                         ChebySCFLoop.cpp:157-168 and EwaldEnergy.  The
+ *                         G-vector list and its heap-sort order are built on
+ *                         the host; EIGR, SFAC, VPS/RHOPS, PKG_A, the
+ *                         starting density and ESR on the device, which then
+ *                         holds a ready pspw_cell and pspw_scf.
+ *   pspw_system_cheby_scf ChebySCFLoop() on that system (rand() seeded 1 as in
+ *                         a fresh reference process, drawn from a private
+ *                         generator state); with outdir it writes
+ *                         STARTING_RHO.dat and FINAL_RHO.dat (Print3DArray).
+ * device < 0 stops after the host part (readers, basis, occupations, WNL,
+ * ESELF): no GPU is touched, the device arrays, cell and SCF are absent.
+ * One Gamma-point k-point only (ChebySCFLoop.cpp:74-77); L_MAX <= 3.
+ * info: dims16 = {NR1, NR2, NR3, NNR, NGW, NGWX, NG, NGX, NX, NLMAX, NAX, NSP,
+ * NEMPTY, ISCF, NKPT, IDIAG}; scal16 = {TPIBA, TPIBA2, OMEGA, ALAT, GCUT,
+ * GCUTW, NEL, ESR, ESELF, ECUT, WKPT, 0...}.
+ * array: a copy of one set-up array, nbytes must equal its size:
+ *   EIGR 16*NGWX*NAX*NSP, SFAC 16*NSP*NG (NSP leading), VPS and RHOPS
+ *   8*NSP*NG, PKG_A 8*NLMAX*NGWX*NSP, RHO_START 8*NNR, WNL 8*NSP*NLMAX,
+ *   FOCC 8*NX, N123 4*NGWX, XKG 8*NGWX, TAU 8*3*NAX*NSP, G 8*NG.
+ * timing: ms8 = {host input + basis, phase + structure factors, local form
+ * factors, nonlocal form factors, cell + SCF handles, starting density,
+ * Ewald sum, total}. */
+typedef struct pspw_system pspw_system;
+#define PSPW_SYS_EIGR 0
+#define PSPW_SYS_SFAC 1
+#define PSPW_SYS_VPS 2
+#define PSPW_SYS_RHOPS 3
+#define PSPW_SYS_PKG_A 4
+#define PSPW_SYS_RHO_START 5
+#define PSPW_SYS_WNL 6
+#define PSPW_SYS_FOCC 7
+#define PSPW_SYS_N123 8
+#define PSPW_SYS_XKG 9
+#define PSPW_SYS_TAU 10
+#define PSPW_SYS_G 11
+int pspw_system_load(const char *dir, int device, pspw_system **out);
+int pspw_system_destroy(pspw_system *sys);
+int pspw_system_info(pspw_system *sys, int *dims16, double *scal16);
+int pspw_system_params(pspw_system *sys, pspw_scf_params *params);
+int pspw_system_array(pspw_system *sys, int which, void *host, long long nbytes);
+int pspw_system_cell(pspw_system *sys, pspw_cell **cell);
+int pspw_system_scf(pspw_system *sys, pspw_scf **scf);
+int pspw_system_timing(pspw_system *sys, double *ms8);
+int pspw_system_cheby_scf(pspw_system *sys, int filter_prec, const char *outdir, double *eig,
+                          double *e6, int *iterations, int *converged, double *hist);
+/* Print3DArray.cpp:5-22: n1*n2*n3 values, one `%18.10f` per line */
+int pspw_print_3d_array(const double *a, int n1, int n2, int n3, const char *path);
+
 /* ------------------------------------------------------------------ timing
  * Optional device timing on the cell stream: CUDA events around each launch
  * of the enabled families, summed until reset.  Families (bit i of the mask):

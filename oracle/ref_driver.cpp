@@ -386,6 +386,11 @@ void ref_get_nl(double *pkg_a, double *wnl) {
   for (long i = 0; i < (long)NSP * NLMAX; i++) wnl[i] = WNL[i];
 }
 
+/* TAU(3, NAX, NSP) in bohr after ReadInputFile's conversions */
+void ref_get_tau(double *tau) {
+  for (int i = 0; i < 3 * NAX * NSP; i++) tau[i] = TAU[i];
+}
+
 /* NA, L_MAX, L_LOC per species (NSP entries each) */
 void ref_get_species(int *na, int *lmax, int *lloc) {
   for (int is = 0; is < NSP; is++) {

@@ -85,6 +85,7 @@ class RefLib:
         L.ref_get_local.argtypes = [_zp, _dp, _dp, _dp]
         L.ref_get_nl.argtypes = [_dp, _dp]
         L.ref_get_species.argtypes = [_ip, _ip, _ip]
+        L.ref_get_tau.argtypes = [_dp]
         L.ref_get_ctrl.argtypes = [_ip, _dp, _dp]
         L.ref_prog_cheby_scf.argtypes = [_dp, _dp]
         self.cell = None
@@ -137,7 +138,8 @@ class RefLib:
         """The reference program's own set-up (main.cpp: ReadInputFile,
         Setup, PrepareSCF) on the INPUT in ``workdir``, its starting density
         (ChebySCFLoop.cpp:157-168) and EwaldEnergy.  Returns the cell dict of
-        ``setup`` plus pkg_a, wnl, sfac/vps/rhops (ng x nsp), esr, eself,
+        ``setup`` plus pkg_a, wnl, sfac/vps/rhops (nsp x ng, the reference's
+        SFAC(NSP, NG) layout), esr, eself, tau,
         rho_start and the control values of the INPUT."""
         cwd = os.getcwd()
         os.chdir(workdir)
@@ -162,10 +164,13 @@ class RefLib:
         self.lib.ref_get_nl(pkg_a, wnl)
         iv, dv, focc = np.zeros(9, dtype=np.int32), np.zeros(3), np.zeros(b["nx"])
         self.lib.ref_get_ctrl(iv, dv, focc)
-        b.update(sfac=sfac.reshape((ng, nsp), order="F"), vps=vps.reshape((ng, nsp), order="F"),
-                 rhops=rhops.reshape((ng, nsp), order="F"), esr=scal[0], eself=scal[1],
+        tau = np.zeros(3 * b["nax"] * nsp)
+        self.lib.ref_get_tau(tau)
+        b.update(sfac=sfac.reshape((nsp, ng), order="F"), vps=vps.reshape((nsp, ng), order="F"),
+                 rhops=rhops.reshape((nsp, ng), order="F"), esr=scal[0], eself=scal[1],
                  pkg_a=pkg_a.reshape((nlmax, ngwx, nsp), order="F"),
                  wnl=wnl.reshape((nsp, nlmax), order="F"), rho_start=rho, focc=focc,
+                 tau=tau.reshape((3, b["nax"], nsp), order="F"),
                  ctrl=dict(nx=int(iv[0]), nempty=int(iv[1]), degree=int(iv[2]),
                            max_scf_iter=int(iv[3]), imix=int(iv[4]), mixdim=int(iv[5]),
                            idiag=int(iv[6]), user_max_diag_iter=int(iv[7]),

@@ -2,14 +2,14 @@
 in a process of its own (the reference keeps its state in globals) and saves
 what the device SCF loop needs to start from the same point.
 
-    python ref_program_case.py WORKDIR OUT.npz
+    python ref_program_case.py WORKDIR OUT.npz [setup]
 
 WORKDIR holds INPUT and the pseudopotential files.  The script runs
 ReadInputFile, Setup, PrepareSCF (main.cpp), the starting density of
 ChebySCFLoop.cpp:157-168 and EwaldEnergy, saves the cell, the local and
 nonlocal pseudopotential arrays, the start density and the INPUT controls,
-then runs ChebySCFLoop() with rand() seeded by srand(1) and saves its final
-EIG and energies.  The reference's `!` lines go to stdout.
+then (unless `setup` is given) runs ChebySCFLoop() with rand() seeded by
+srand(1) and saves its final EIG and energies.  The reference's `!` lines go to stdout.
 Needs oracle/_ref/libref.so."""
 import os
 import sys
@@ -22,12 +22,15 @@ import numpy as np  # noqa: E402
 from ref_lib import RefLib  # noqa: E402
 
 
-def main(workdir, out):
+def main(workdir, out, setup_only=False):
     R = RefLib("libref.so")
     b = R.program_setup(workdir)
     ctrl = b.pop("ctrl")
     sys.stdout.flush()
-    eig, e6 = R.program_cheby_scf(workdir)
+    if setup_only:
+        eig, e6 = np.zeros(0), np.zeros(6)
+    else:
+        eig, e6 = R.program_cheby_scf(workdir)
     arrays = {k: np.asarray(v) for k, v in b.items() if not isinstance(v, (list, tuple, dict))}
     arrays.update(nr=np.asarray(b["nr"]), na=np.asarray(b["na"]), lm_end=np.asarray(b["lm_end"]),
                   eig=eig, e6=e6,
@@ -37,4 +40,4 @@ def main(workdir, out):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1], sys.argv[2])
+    main(sys.argv[1], sys.argv[2], len(sys.argv) > 3 and sys.argv[3] == "setup")

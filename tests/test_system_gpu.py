@@ -1,0 +1,100 @@
+"""The device set-up of a system (pspw_system_load) against the reference's own
+set-up of the same input files, and the reference main program's ChebySCF run
+(pspw_system_cheby_scf) against the reference program itself
+(oracle/_ref/ffr_pspw_dft.x, a fresh process: rand() starts from seed 1).
+
+Tolerances: EIGR and SFAC are products of the same host phase tables with
+every product and sum rounded as the reference does (bit-exact expected,
+1e-15 allowed); VPS, RHOPS and PKG_A go through the device sin/cos/exp
+(1e-12 relative max-norm); the starting density also through the device FFT
+(1e-11); ESR through the device erf and a tree sum (1e-12)."""
+import os
+import subprocess
+
+import numpy as np
+import pytest
+
+from helpers import scf_lines
+from system_cases import reference_setup, write_molecule, write_si8
+
+pytestmark = pytest.mark.gpu
+HERE = os.path.dirname(os.path.abspath(__file__))
+REF_DIR = os.path.join(HERE, "..", "oracle", "_ref")
+
+
+def _rel(a, b):
+    a, b = np.asarray(a), np.asarray(b)
+    return float(np.abs(a - b).max() / max(np.abs(b).max(), 1e-300))
+
+
+def _case(tmp_path, name, **kw):
+    d = str(tmp_path / name)
+    return write_si8(d, **kw) if name.startswith("si8") else write_molecule(d, **kw)
+
+
+@pytest.mark.parametrize("name", ["si8", "molecule"])
+def test_device_setup_matches_reference(tmp_path, name):
+    from pspw.system import System
+    d = _case(tmp_path, name)
+    z, _, _ = reference_setup(d)
+    S = System(d, device=0)
+    dm = S.dims
+    ng, nsp = dm["ng"], dm["nsp"]
+    assert _rel(S.array("eigr"), z["eigr"]) <= 1e-15
+    assert _rel(S.array("sfac"), z["sfac"][:, :ng]) <= 1e-15
+    assert _rel(S.array("vps"), z["vps"][:, :ng]) < 1e-12
+    assert _rel(S.array("rhops"), z["rhops"][:, :ng]) < 1e-12
+    pk = S.array("pkg_a")
+    assert _rel(pk, z["pkg_a"]) < 1e-12
+    assert np.array_equal(S.array("wnl"), z["wnl"])
+    assert _rel(S.array("rho_start"), z["rho_start"]) < 1e-11
+    assert abs(S.scalars["esr"] - float(z["esr"])) <= 1e-12 * max(1.0, abs(float(z["esr"])))
+    assert S.scalars["eself"] == float(z["eself"])
+    t = S.timing()
+    assert all(v >= 0.0 for v in t.values()) and t["total"] > 0.0
+    S.close()
+
+
+def _run_reference_program(d):
+    exe = os.path.join(REF_DIR, "ffr_pspw_dft.x")
+    if not os.path.exists(exe):
+        pytest.skip("reference program build not present")
+    r = subprocess.run([exe], cwd=d, capture_output=True, text=True, timeout=900)
+    assert r.returncode == 0, r.stdout[-2000:]
+    return scf_lines(r.stdout)
+
+
+def _read_dat(path):
+    return np.loadtxt(path)
+
+
+@pytest.mark.parametrize("name,nat,kw", [
+    ("si8", 8, dict(max_scf=40)),
+    ("molecule", 4, dict(imix=3, max_scf=60)),
+])
+def test_system_cheby_scf_matches_reference_program(tmp_path, name, nat, kw):
+    """Same INPUT, the reference main program against the engine's system
+    run: the first iteration's energy, convergence and the converged energy
+    (|dETOT| <= 1e-6 on both sides; the trajectories may part at the 1e-6
+    level after the first Davidson step, as in the drop-in test, so the
+    stopping iteration is not compared), and the density dumps in
+    Print3DArray's format."""
+    from pspw.system import System
+    d = _case(tmp_path, name, **kw)
+    ref = _run_reference_program(d)
+    out = os.path.join(d, "engine")
+    os.makedirs(out)
+    S = System(d, device=0)
+    res = S.cheby_scf(outdir=out)
+    hist = res["hist"]
+    print("engine", hist[:, 0].tolist())
+    print("reference", [l[1] for l in ref])
+    assert res["converged"] and ref[-1][2] <= 1e-6
+    assert abs(hist[0, 0] - ref[0][1]) < 1e-4
+    assert abs(hist[-1, 0] - ref[-1][1]) / nat < 1e-6
+    r0, e0 = _read_dat(os.path.join(d, "STARTING_RHO.dat")), _read_dat(os.path.join(out, "STARTING_RHO.dat"))
+    assert r0.shape == e0.shape == (S.dims["nnr"],)
+    assert np.abs(r0 - e0).max() <= 1e-9 * max(1.0, np.abs(r0).max())
+    r1, e1 = _read_dat(os.path.join(d, "FINAL_RHO.dat")), _read_dat(os.path.join(out, "FINAL_RHO.dat"))
+    assert _rel(e1, r1) < 1e-3
+    S.close()
