@@ -173,7 +173,7 @@ def reference_sample(steps, warmup, bands_per_proc=4, procs=None):
 # ------------------------------------------------------------------ engine arm
 def run_engine(args, rank, world, local_rank):
     import torch
-    from pspw import PREC_F32, PREC_F64, workloads
+    from pspw import PREC_F32, PREC_F64, replica, workloads
     torch.cuda.set_device(local_rank)
     dev = torch.device("cuda", local_rank)
     w = workloads.workload(args.workload)
@@ -208,8 +208,7 @@ def run_engine(args, rank, world, local_rank):
     l0 = cell.kernel_launches()
     evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
            for _ in range(args.steps)]
-    if world > 1:
-        torch.distributed.barrier()
+    replica.barrier()
     torch.cuda.synchronize()
     t_wall = time.perf_counter()
     with torch.cuda.stream(stream):
@@ -219,8 +218,7 @@ def run_engine(args, rank, world, local_rank):
             step()
             evs[k][1].record(stream)
     torch.cuda.synchronize()
-    if world > 1:
-        torch.distributed.barrier()
+    replica.barrier()
     t_wall = time.perf_counter() - t_wall
     launches = (cell.kernel_launches() - l0) // args.steps
     cell.timing_enable(0)
@@ -228,12 +226,9 @@ def run_engine(args, rank, world, local_rank):
     clocks.stop()
     step_ms = [a.elapsed_time(b) for a, b in evs]
     ms = sum(step_ms) / len(step_ms)
-    ms_t = torch.tensor([ms], device=dev)
-    if world > 1:
-        torch.distributed.all_reduce(ms_t, op=torch.distributed.ReduceOp.MAX)
-    ms_max = float(ms_t.item())
+    ms_max = replica.max_over_ranks(ms, device=dev)
     bytes_step = DEGREE * hpsi_bytes_model(ngw, nnr, nb, nat, fp64=False)
-    value = world * bytes_step / (ms_max * 1e-3) / 1e9
+    value = replica.weak_throughput(bytes_step, world, ms_max * 1e-3) / 1e9
 
     # ---- per-kernel roofline (dominant kernel family on the cell stream)
     # Algorithmic bytes of each kernel = its share of the block H*psi byte
@@ -321,13 +316,11 @@ def run_engine(args, rank, world, local_rank):
             t0 = time.perf_counter()
             check(L.pspw_chebyfilt(cell.handle, hx.ctypes.data, ngw, nb, DEGREE, LB, UB, prec))
             tt.append(time.perf_counter() - t0)
-        et = sum(tt) / len(tt)
-        et_t = torch.tensor([et], device=dev)
-        if world > 1:
-            torch.distributed.all_reduce(et_t, op=torch.distributed.ReduceOp.MAX)
-        e2e = {"value": round(world * bytes_step / float(et_t.item()) / 1e9, 2), "unit": "GB/s",
+        et = replica.max_over_ranks(sum(tt) / len(tt), device=dev)
+        e2e = {"value": round(replica.weak_throughput(bytes_step, world, et) / 1e9, 2),
+               "unit": "GB/s",
                "h2d_bytes_per_step": ngw * nb * 16, "d2h_bytes_per_step": ngw * nb * 16,
-               "seconds_per_step": round(float(et_t.item()), 6),
+               "seconds_per_step": round(et, 6),
                "path": "pspw_chebyfilt (C ABI, host FP64 X, FP32 on device)" if not fp64
                else "pspw_chebyfilt (C ABI, host FP64 X, FP64 on device)"}
 
