@@ -3,7 +3,7 @@
 //     a full-grid FFT, xc_PZ, V_eff = Re(V_H + V_loc) + V_xc, energy terms;
 //   xc_PZ (xc_PZ.cpp:7-63), NormalizeRho (NormalizeRho.cpp:7-33),
 //   KerkerPrec (KerkerRhoMix.cpp:53-81) and the density mixers
-//   SimpleRhoMix, KerkerRhoMix, AndersonRhoMix and PulayRhoMix
+//   SimpleRhoMix, KerkerRhoMix, AndersonRhoMix, PulayRhoMix and BroydenRhoMix
 //   (SimpleRhoMix.cpp, KerkerRhoMix.cpp:5-50, AndersonRhoMix.cpp:8-91,
 //   PulayRhoMix.cpp:5-91).
 // Every sum over the grid or the G list is a two-stage reduction with a
@@ -332,10 +332,12 @@ __global__ void __launch_bounds__(kRedThreads) k_diff_sq(const double *__restric
 }
 
 // out = ca*a + cb*b (+ cc*c) elementwise; any of the outputs may alias inputs
+// out = ca a + cb b + cc c; b and c may be null (their terms are dropped)
 __global__ void k_lin3(double *out, double ca, const double *a, double cb, const double *b,
                        double cc, const double *c, int n) {
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-    double v = ca * a[i] + cb * b[i];
+    double v = ca * a[i];
+    if (b) v += cb * b[i];
     if (c) v += cc * c[i];
     out[i] = v;
   }
@@ -627,6 +629,46 @@ int mix_dev(pspw_scf *s, int iter, double *d_rhoe, double *d_out) {
       if ((rc = copy(col(H, jn), d_rhoe))) return rc;
       break;
     }
+    case PSPW_MIX_BROYDEN: {
+      // BroydenRhoMix.cpp:10-104 with alpha = beta (0.25) and w0 = 0.01 as
+      // the ChebySCF loop calls it (ChebySCFLoop.cpp:240,336).  H: rho_old
+      // (2 columns), F: f (2 columns), Gm: df (mixdim columns) then u.
+      const int mixdim = s->mixdim;
+      const double w0 = 0.01;
+      double *DF = Gm, *U = Gm + (size_t)mixdim * n;
+      const int m = std::min(iter + 1, mixdim);
+      const int jc = iter % m + 1, kp = (iter - 1) % 2 + 1, kc = iter % 2 + 1;
+      lin(col(F, kc), 1.0, d_rhoe, -1.0, col(H, kp), 0.0, nullptr);
+      double t3[3];
+      if ((rc = dots(col(F, kc), col(F, kc), nullptr, nullptr, nullptr, nullptr, t3))) return rc;
+      d = std::sqrt(t3[0] / (double)n);
+      lin(col(DF, jc), 1.0, col(F, kc), -1.0, col(F, kp), 0.0, nullptr);
+      if ((rc = dots(col(DF, jc), col(DF, jc), nullptr, nullptr, nullptr, nullptr, t3))) return rc;
+      double t1 = std::sqrt(t3[0]);
+      if (t1 > 1.e-8) t1 = 1.0 / t1;  // a norm below 1e-8 is used as it is (:45-46)
+      lin(col(DF, jc), t1, col(DF, jc), 0.0, col(DF, jc), 0.0, nullptr);
+      lin(s->d_tmp, 1.0, col(H, kp), -1.0, col(H, kc), 0.0, nullptr);
+      lin(col(U, jc), beta, col(DF, jc), t1, s->d_tmp, 0.0, nullptr);
+      std::vector<double> cvec(m), &A = s->mix_a;
+      for (int k = 1; k <= m; k++) {
+        if ((rc = dots(col(DF, k), col(F, kc), col(DF, jc), col(DF, k), nullptr, nullptr, t3)))
+          return rc;
+        cvec[k - 1] = t3[0];
+        A[(k - 1) + (size_t)mixdim * (jc - 1)] = t3[1];
+        A[(jc - 1) + (size_t)mixdim * (k - 1)] = t3[1];
+      }
+      // gamma = c^T beta^-1 with beta = a + w0^2 I (m x m), symmetric
+      std::vector<double> bm((size_t)m * m);
+      for (int j = 0; j < m; j++)
+        for (int i = 0; i < m; i++)
+          bm[i + (size_t)m * j] = A[i + (size_t)mixdim * j] + (i == j ? w0 * w0 : 0.0);
+      std::vector<double> gamma = cvec;
+      if (!solve_small(m, bm, gamma)) return fail(PSPW_ERR_LAPACK, "BroydenRhoMix: singular beta");
+      lin(d_rhoe, 1.0, col(H, kp), beta, col(F, kc), 0.0, nullptr);
+      for (int l = 1; l <= m; l++) lin(d_rhoe, 1.0, d_rhoe, -gamma[l - 1], col(U, l), 0.0, nullptr);
+      if ((rc = copy(col(H, kc), d_rhoe))) return rc;
+      break;
+    }
     default:
       return fail(PSPW_ERR_ARG, "mix: mixer not initialised (pspw_mix_init)");
   }
@@ -797,10 +839,14 @@ int pspw_mix_init(pspw_scf *s, int kind, int mixdim, double beta, double q0,
                   const double *rho_old) {
   int rc = scf_enter(s);
   if (rc) return rc;
-  if (kind < PSPW_MIX_SIMPLE || kind > PSPW_MIX_PULAY || (kind == PSPW_MIX_PULAY && mixdim < 2))
+  if (kind < PSPW_MIX_SIMPLE || kind > PSPW_MIX_BROYDEN ||
+      ((kind == PSPW_MIX_PULAY || kind == PSPW_MIX_BROYDEN) && mixdim < 2))
     return fail(PSPW_ERR_ARG, "mix_init: unknown mixer or MIXDIM < 2");
   const size_t n = s->cell->basis.nnr;
-  const int ncol = kind == PSPW_MIX_PULAY ? mixdim : (kind == PSPW_MIX_ANDERSON ? 3 : 1);
+  const int ncol = kind == PSPW_MIX_PULAY ? mixdim
+                   : kind == PSPW_MIX_ANDERSON ? 3
+                   : kind == PSPW_MIX_BROYDEN ? 2 : 1;
+  const int ngm = kind == PSPW_MIX_BROYDEN ? 2 * mixdim : 2;
   for (double **p : {&s->d_hist, &s->d_f, &s->d_gm})
     if (*p) {
       cudaFree(*p);
@@ -808,12 +854,13 @@ int pspw_mix_init(pspw_scf *s, int kind, int mixdim, double beta, double q0,
     }
   if (cudaMalloc(&s->d_hist, sizeof(double) * n * ncol) != cudaSuccess ||
       cudaMalloc(&s->d_f, sizeof(double) * n * ncol) != cudaSuccess ||
-      cudaMalloc(&s->d_gm, sizeof(double) * n * 2) != cudaSuccess)
+      cudaMalloc(&s->d_gm, sizeof(double) * n * ngm) != cudaSuccess)
     return fail(PSPW_ERR_OOM, "mix_init: device memory");
+  s->mix_a.assign((size_t)std::max(mixdim, 1) * std::max(mixdim, 1), 0.0);
   // the reference's history arrays start at zero (ChebySCFLoop.cpp:123-148)
   PSPW_CUDA(cudaMemsetAsync(s->d_hist, 0, sizeof(double) * n * ncol, s->cell->stream));
   PSPW_CUDA(cudaMemsetAsync(s->d_f, 0, sizeof(double) * n * ncol, s->cell->stream));
-  PSPW_CUDA(cudaMemsetAsync(s->d_gm, 0, sizeof(double) * n * 2, s->cell->stream));
+  PSPW_CUDA(cudaMemsetAsync(s->d_gm, 0, sizeof(double) * n * ngm, s->cell->stream));
   if (rho_old && (rc = up(s, s->d_hist, rho_old))) return rc;
   s->mix_kind = kind;
   s->mixdim = mixdim;

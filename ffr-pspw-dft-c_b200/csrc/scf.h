@@ -3,6 +3,8 @@
 // with the local-potential data and the mixing history kept on the device.
 #pragma once
 
+#include <vector>
+
 #include "engine.h"
 
 struct pspw_scf {
@@ -24,7 +26,8 @@ struct pspw_scf {
   double mix_beta = 0.0, mix_q0 = 0.0;
   double *d_hist = nullptr;   // rho_old history
   double *d_f = nullptr;      // residual history
-  double *d_gm = nullptr;     // Anderson differences (2 columns)
+  double *d_gm = nullptr;     // Anderson differences (2 columns); Broyden df then u
+  std::vector<double> mix_a;  // Broyden's a(MIXDIM, MIXDIM), kept between calls
 };
 
 namespace pspw {

@@ -91,14 +91,14 @@ extern "C" int pspw_cheby_scf(pspw_scf *s, const pspw_scf_params *p, const doubl
   const int k = std::max(2 * nx, 10);
   if (nx < 1 || p->degree < 1 || p->max_scf_iter < 1 || nx2 > ngw || k > ngw)
     return fail(PSPW_ERR_ARG, "cheby_scf: bad sizes");
-  if (p->imix == 4) return fail(PSPW_ERR_NOT_IMPL, "cheby_scf: Broyden mixing (IMIX = 4)");
   if (p->filter_prec != PSPW_PREC_F64 && p->filter_prec != PSPW_PREC_F32)
     return fail(PSPW_ERR_ARG, "cheby_scf: unknown filter precision");
   const int kind = (p->imix == PSPW_MIX_KERKER || p->imix == PSPW_MIX_ANDERSON ||
-                    p->imix == PSPW_MIX_PULAY)
+                    p->imix == PSPW_MIX_PULAY || p->imix == PSPW_MIX_BROYDEN)
                        ? p->imix
                        : PSPW_MIX_SIMPLE;
-  const double beta = kind == PSPW_MIX_PULAY ? p->pulay_beta : p->mix_beta;
+  const double beta =
+      (kind == PSPW_MIX_PULAY || kind == PSPW_MIX_BROYDEN) ? p->pulay_beta : p->mix_beta;
   int rc;
   // ---- device arrays
   DevBuf mem;
@@ -116,8 +116,9 @@ extern "C" int pspw_cheby_scf(pspw_scf *s, const pspw_scf_params *p, const doubl
   PSPW_CUDA(cudaMemcpyAsync(veff, rho_start, sizeof(double) * nnr, cudaMemcpyHostToDevice, st));
   PSPW_CUDA(cudaMemcpyAsync(dv0, v0, sizeof(double2) * ngw, cudaMemcpyHostToDevice, st));
   // simple and Kerker mixing start from rho_old = the start density; the
-  // Anderson and Pulay histories start at zero (ChebySCFLoop.cpp:123-148),
-  // so the first Pulay step mixes the new density with zero
+  // Anderson, Pulay and Broyden histories start at zero
+  // (ChebySCFLoop.cpp:123-148), so the first Pulay step mixes the new density
+  // with zero
   const bool mix_from_start = kind == PSPW_MIX_SIMPLE || kind == PSPW_MIX_KERKER;
   if ((rc = pspw_mix_init(s, kind, p->mixdim, beta, p->kerker_q0,
                           mix_from_start ? rho_start : nullptr)))

@@ -20,7 +20,7 @@ PREC_F32 = 1
 NL_AUTO = 0
 NL_SIMT = 1
 NL_TENSOR_CORE = 2
-MIX_SIMPLE, MIX_KERKER, MIX_ANDERSON, MIX_PULAY = 0, 1, 2, 3
+MIX_SIMPLE, MIX_KERKER, MIX_ANDERSON, MIX_PULAY, MIX_BROYDEN = 0, 1, 2, 3, 4
 
 OK = 0
 ERRORS = {1: "ARG", 2: "SHAPE", 3: "CUDA", 4: "OOM", 5: "NONFINITE", 6: "TIMEOUT", 7: "LAPACK",

@@ -228,8 +228,10 @@ int pspw_eval_enl(pspw_cell *cell, const double *c0, int ld, int ngw, int nx,
  *                   FFT x] on the wavefunction sphere of the cell (other
  *                   components unchanged, as in the reference).
  * mix_init / mix    SimpleRhoMix.cpp, KerkerRhoMix.cpp:5-50,
- *                   AndersonRhoMix.cpp:8-91, PulayRhoMix.cpp:5-91 (beta is a
- *                   parameter; the reference's Pulay uses 0.25).  The history
+ *                   AndersonRhoMix.cpp:8-91, PulayRhoMix.cpp:5-91,
+ *                   BroydenRhoMix.cpp:10-104 (beta is a parameter; the
+ *                   reference's Pulay uses 0.25 and its Broyden alpha = 0.25,
+ *                   w0 = 0.01, ChebySCFLoop.cpp:240,336).  The history
  *                   starts at zero as in ChebySCFLoop.cpp:123-148; rho_old
  *                   (may be null) fills its first column.  iter counts from
  *                   1; *d = the mixer's residual measure. */
@@ -238,6 +240,7 @@ typedef struct pspw_scf pspw_scf;
 #define PSPW_MIX_KERKER 1
 #define PSPW_MIX_ANDERSON 2
 #define PSPW_MIX_PULAY 3
+#define PSPW_MIX_BROYDEN 4
 int pspw_scf_create(pspw_cell *cell, int ng, const int *n1, const int *n2, const int *n3,
                     const double *g, int nsp, const double *sfac, const double *vps,
                     const double *rhops, double omega, double nel, double esr, double eself,
@@ -277,11 +280,12 @@ typedef struct {
   int degree;         /* CHEBYPOL_DEGREE */
   int max_scf_iter;   /* MAX_SCF_ITER */
   double conv;        /* SCF_CONV_CRIT on |ETOT - ETOT_old| (Ha) */
-  int imix;           /* IMIX: 1 Kerker, 2 Anderson, 3 Pulay, 4 Broyden (not
-                         built: PSPW_ERR_NOT_IMPL), other: simple */
+  int imix;           /* IMIX: 1 Kerker, 2 Anderson, 3 Pulay, 4 Broyden,
+                         other: simple */
   int mixdim;         /* MIXDIM (Pulay) */
   double mix_beta;    /* RHO_MIX_FAC (simple, Kerker, Anderson) */
-  double pulay_beta;  /* the Pulay warm-up beta (0.25 in the reference) */
+  double pulay_beta;  /* the Pulay warm-up beta and Broyden alpha (0.25 in the
+                         reference) */
   double kerker_q0;   /* KERKER_Q0 */
   int idiag;          /* IDIAG: >= 0 first iteration by Davidson, < 0 start from X */
   int max_diag_iter;  /* Davidson iteration cap; 0 = the reference's default */

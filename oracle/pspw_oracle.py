@@ -525,21 +525,47 @@ def eval_energy(rho, local, cell, ekin, enl):
 
 
 class Mixer:
-    """SimpleRhoMix.cpp, KerkerRhoMix.cpp:5-50, AndersonRhoMix.cpp:8-91 and
-    PulayRhoMix.cpp:5-91 with their history (zero at the start, as the
-    ChebySCF loop allocates it).  kind: 0 simple, 1 Kerker, 2 Anderson,
-    3 Pulay."""
+    """SimpleRhoMix.cpp, KerkerRhoMix.cpp:5-50, AndersonRhoMix.cpp:8-91,
+    PulayRhoMix.cpp:5-91 and BroydenRhoMix.cpp:10-104 with their history
+    (zero at the start, as the ChebySCF loop allocates it).  kind: 0 simple,
+    1 Kerker, 2 Anderson, 3 Pulay, 4 Broyden (alpha = beta, w0 = 0.01)."""
 
     def __init__(self, kind, nnr, cell, mixdim=0, beta=0.25, q0=0.0, omega=1.0, nel=0.0,
                  rho_old=None):
         self.kind, self.cell, self.mixdim, self.beta, self.q0 = kind, cell, mixdim, beta, q0
         self.omega, self.nel = omega, nel
-        ncol = mixdim if kind == 3 else (3 if kind == 2 else 1)
+        ncol = mixdim if kind == 3 else (3 if kind == 2 else (2 if kind == 4 else 1))
         self.h = np.zeros((nnr, ncol))
         self.f = np.zeros((nnr, ncol))
         self.g = np.zeros((nnr, 2))
+        if kind == 4:
+            self.df = np.zeros((nnr, mixdim))
+            self.u = np.zeros((nnr, mixdim))
+            self.a = np.zeros((mixdim, mixdim))
         if rho_old is not None:
             self.h[:, 0] = rho_old
+
+    def _broyden(self, it, rho):
+        alpha, w0, md, n = self.beta, 0.01, self.mixdim, len(rho)
+        h, f, df, u, a = self.h, self.f, self.df, self.u, self.a
+        m = min(it + 1, md)
+        jc, kp, kc = it % m, (it - 1) % 2, it % 2
+        f[:, kc] = rho - h[:, kp]
+        d = np.sqrt(float(f[:, kc] @ f[:, kc]) / n)
+        df[:, jc] = f[:, kc] - f[:, kp]
+        t1 = np.sqrt(float(df[:, jc] @ df[:, jc]))
+        if t1 > 1.e-8:
+            t1 = 1.0 / t1
+        df[:, jc] = t1 * df[:, jc]
+        u[:, jc] = alpha * df[:, jc] + t1 * (h[:, kp] - h[:, kc])
+        c = np.array([df[:, k] @ f[:, kc] for k in range(m)])
+        for k in range(m):
+            a[k, jc] = a[jc, k] = df[:, jc] @ df[:, k]
+        beta = a[:m, :m] + w0 * w0 * np.eye(m)
+        gamma = c @ np.linalg.inv(beta)
+        rho = h[:, kp] + alpha * f[:, kc] - u[:, :m] @ gamma
+        h[:, kc] = rho
+        return rho, d
 
     def mix(self, it, rhoe):
         rhoe = np.array(rhoe, dtype=float, copy=True)
@@ -587,6 +613,8 @@ class Mixer:
                         + b * (f[:, j0] + t1 * g[:, 0] + t2 * g[:, 0]))
             h[:, j0] = rhoe
             return rhoe, d
+        if self.kind == 4:
+            return self._broyden(it, rhoe)
         # Pulay
         md = self.mixdim
         if it < md:

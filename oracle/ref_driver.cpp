@@ -339,6 +339,13 @@ double ref_AndersonRhoMix(int iter, double beta, double *rhoe, double *rho_old, 
   return d;
 }
 
+double ref_BroydenRhoMix(int iter, double alpha, double w0, double *rho, double *rho_old,
+                         double *f, double *df, double *u, double *a, int mixdim, int nnr) {
+  double d = 0.0;
+  BroydenRhoMix(iter, alpha, w0, rho, rho_old, f, df, u, a, mixdim, nnr, d);
+  return d;
+}
+
 double ref_KerkerRhoMix(double beta, double q0, double *rhoe, double *rho_old, int nnr) {
   double d = 0.0;
   KerkerRhoMix(beta, q0, rhoe, rho_old, nnr, d);

@@ -60,6 +60,9 @@ class RefLib:
         L.ref_PulayRhoMix.restype = C.c_double
         L.ref_AndersonRhoMix.argtypes = [C.c_int, C.c_double, _dp, _dp, _dp, _dp, C.c_int]
         L.ref_AndersonRhoMix.restype = C.c_double
+        L.ref_BroydenRhoMix.argtypes = [C.c_int, C.c_double, C.c_double, _dp, _dp, _dp, _dp,
+                                        _dp, _dp, C.c_int, C.c_int]
+        L.ref_BroydenRhoMix.restype = C.c_double
         L.ref_KerkerRhoMix.argtypes = [C.c_double, C.c_double, _dp, _dp, C.c_int]
         L.ref_KerkerRhoMix.restype = C.c_double
         L.ref_SimpleRhoMix.argtypes = [C.c_double, _dp, _dp, C.c_int]

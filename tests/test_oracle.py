@@ -213,7 +213,7 @@ def _mix_sequence(c, n=6, seed=3):
 
 
 @need_ref
-@pytest.mark.parametrize("kind", [0, 1, 2, 3])
+@pytest.mark.parametrize("kind", [0, 1, 2, 3, 4])
 def test_live_mixers(scf_case, kind):
     import ctypes as C
     c = scf_case
@@ -221,12 +221,15 @@ def test_live_mixers(scf_case, kind):
     mixdim = 3
     R.lib.ref_set_mixing(0.6)
     seq = _mix_sequence(c)
-    om = O.Mixer(kind, nnr, c["ocell"], mixdim=mixdim, beta=0.3 if kind != 3 else 0.25, q0=0.6,
+    om = O.Mixer(kind, nnr, c["ocell"], mixdim=mixdim, beta=0.3 if kind < 3 else 0.25, q0=0.6,
                  omega=c["b"]["omega"], nel=c["nel"], rho_old=c["rho"] if kind < 2 else None)
-    cols = mixdim if kind == 3 else 3
+    cols = mixdim if kind == 3 else (2 if kind == 4 else 3)
     h = np.zeros((nnr, cols), order="F")
     f = np.zeros((nnr, cols), order="F")
     g = np.zeros((nnr, 2), order="F")
+    df = np.zeros((nnr, mixdim), order="F")
+    u = np.zeros((nnr, mixdim), order="F")
+    a = np.zeros((mixdim, mixdim), order="F")
     if kind < 2:
         h[:, 0] = c["rho"]
     for it, rin in enumerate(seq, start=1):
@@ -239,9 +242,14 @@ def test_live_mixers(scf_case, kind):
             d_r = R.lib.ref_AndersonRhoMix(it, 0.3, r_ref, h.reshape(-1, order="F"),
                                            f.reshape(-1, order="F"), g.reshape(-1, order="F"),
                                            nnr)
-        else:
+        elif kind == 3:
             d_r = R.lib.ref_PulayRhoMix(it, r_ref, h.reshape(-1, order="F"),
                                         f.reshape(-1, order="F"), mixdim, nnr)
+        else:
+            d_r = R.lib.ref_BroydenRhoMix(it, 0.25, 0.01, r_ref, h.reshape(-1, order="F"),
+                                          f.reshape(-1, order="F"), df.reshape(-1, order="F"),
+                                          u.reshape(-1, order="F"), a.reshape(-1, order="F"),
+                                          mixdim, nnr)
         r_o, d_o = om.mix(it, rin)
         assert np.abs(r_o - r_ref).max() < 1e-9 * np.abs(r_ref).max(), (kind, it)
         assert abs(d_o - d_r) < 1e-9 * max(1.0, abs(d_r)), (kind, it)

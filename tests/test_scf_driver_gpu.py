@@ -123,6 +123,13 @@ def test_cheby_scf_kerker(tmp_path):
     _check(lines, z, res)
 
 
+def test_cheby_scf_broyden(tmp_path):
+    """IMIX = 4: Broyden mixing with the loop's alpha = 0.25, w0 = 0.01."""
+    z, ctrl, lines = _reference_run(tmp_path, "broyden", imix=4, max_scf=60)
+    res = _run_engine(z, ctrl)
+    _check(lines, z, res)
+
+
 def test_cheby_scf_f32_filter(tmp_path):
     """The filter in FP32, everything else FP64: the same converged energy
     (to 1e-5 Ha/atom) and occupied eigenvalues."""

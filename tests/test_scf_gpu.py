@@ -18,7 +18,7 @@ if not ref_available("libref.so"):
     pytest.skip("oracle/_ref reference build not present", allow_module_level=True)
 
 import pspw_oracle as O  # noqa: E402
-from pspw import MIX_ANDERSON, MIX_KERKER, MIX_PULAY, MIX_SIMPLE, PspwError  # noqa: E402
+from pspw import MIX_ANDERSON, MIX_BROYDEN, MIX_KERKER, MIX_PULAY, MIX_SIMPLE, PspwError  # noqa: E402
 from scf_case import engine_scf, make_case  # noqa: E402
 
 
@@ -75,20 +75,23 @@ def test_kerker_prec(case):
     assert np.abs(k_e - k_r).max() < 1e-12 * np.abs(k_r).max()
 
 
-@pytest.mark.parametrize("kind", [MIX_SIMPLE, MIX_KERKER, MIX_ANDERSON, MIX_PULAY])
+@pytest.mark.parametrize("kind", [MIX_SIMPLE, MIX_KERKER, MIX_ANDERSON, MIX_PULAY, MIX_BROYDEN])
 def test_mixers_follow_the_reference(case, kind):
     c = case
     R, nnr, mixdim = c["ref"], c["nnr"], 3
     R.lib.ref_set_mixing(0.6)
     rng = np.random.default_rng(3)
     seq = [c["rho"] * (1.0 + 0.05 * rng.standard_normal(nnr)) for _ in range(7)]
-    beta = 0.3 if kind != MIX_PULAY else 0.25
+    beta = 0.3 if kind not in (MIX_PULAY, MIX_BROYDEN) else 0.25
     c["scf"].mix_init(kind, mixdim=mixdim, beta=beta, q0=0.6,
                       rho_old=c["rho"] if kind in (MIX_SIMPLE, MIX_KERKER) else None)
-    cols = mixdim if kind == MIX_PULAY else 3
+    cols = mixdim if kind == MIX_PULAY else (2 if kind == MIX_BROYDEN else 3)
     h = np.zeros((nnr, cols), order="F")
     f = np.zeros((nnr, cols), order="F")
     g = np.zeros((nnr, 2), order="F")
+    df = np.zeros((nnr, mixdim), order="F")
+    u = np.zeros((nnr, mixdim), order="F")
+    a = np.zeros((mixdim, mixdim), order="F")
     if kind in (MIX_SIMPLE, MIX_KERKER):
         h[:, 0] = c["rho"]
     for it, rin in enumerate(seq, start=1):
@@ -101,9 +104,14 @@ def test_mixers_follow_the_reference(case, kind):
             d_r = R.lib.ref_AndersonRhoMix(it, beta, r_ref, h.reshape(-1, order="F"),
                                            f.reshape(-1, order="F"), g.reshape(-1, order="F"),
                                            nnr)
-        else:
+        elif kind == MIX_PULAY:
             d_r = R.lib.ref_PulayRhoMix(it, r_ref, h.reshape(-1, order="F"),
                                         f.reshape(-1, order="F"), mixdim, nnr)
+        else:
+            d_r = R.lib.ref_BroydenRhoMix(it, beta, 0.01, r_ref, h.reshape(-1, order="F"),
+                                          f.reshape(-1, order="F"), df.reshape(-1, order="F"),
+                                          u.reshape(-1, order="F"), a.reshape(-1, order="F"),
+                                          mixdim, nnr)
         r_e, d_e = c["scf"].mix(it, rin)
         assert np.abs(r_e - r_ref).max() < 1e-9 * np.abs(r_ref).max(), (kind, it)
         assert abs(d_e - d_r) < 1e-9 * max(1.0, abs(d_r)), (kind, it)

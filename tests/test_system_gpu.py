@@ -71,6 +71,7 @@ def _read_dat(path):
 @pytest.mark.parametrize("name,nat,kw", [
     ("si8", 8, dict(max_scf=40)),
     ("molecule", 4, dict(imix=3, max_scf=60)),
+    ("molecule_broyden", 4, dict(imix=4, max_scf=60)),
 ])
 def test_system_cheby_scf_matches_reference_program(tmp_path, name, nat, kw):
     """Same INPUT, the reference main program against the engine's system
