@@ -335,4 +335,31 @@ int pspw_eval_enl(pspw_cell *c, const double *c0, int ld, int ngw, int nx, const
   return eval_enl_dev(c, dX, ngw, ngw, nx, focc, wkpt, enl, fnl);
 }
 
+int pspw_eval_rho_psi_dev(pspw_cell *c, double *d_rhoe, const double *d_eigvec, int ld, int ngw,
+                          int nx, const double *focc, double wkpt, double omega, double *ekin) {
+  int rc = enter(c);
+  if (rc) return rc;
+  if (!d_rhoe || !d_eigvec || !focc || nx < 0 || ld < ngw || ngw < 1)
+    return fail(PSPW_ERR_ARG, "EvalRhoPsi: bad argument");
+  if (ngw > c->basis.ngw) return fail(PSPW_ERR_SHAPE, "EvalRhoPsi: NGW exceeds the cell");
+  if (nx == 0) return PSPW_OK;
+  if ((rc = eval_rho_psi_dev(c, reinterpret_cast<const double2 *>(d_eigvec), ld, ngw, nx, focc,
+                             wkpt, omega, d_rhoe, ekin)))
+    return rc;
+  return sync(c);
+}
+
+int pspw_eval_enl_dev(pspw_cell *c, const double *d_c0, int ld, int ngw, int nx,
+                      const double *focc, double wkpt, double *enl, double *fnl) {
+  int rc = enter(c);
+  if (rc) return rc;
+  if (!d_c0 || !focc || !enl || nx < 0 || ld < ngw || ngw < 1)
+    return fail(PSPW_ERR_ARG, "EvalENL: bad argument");
+  if (ngw > c->basis.ngw) return fail(PSPW_ERR_SHAPE, "EvalENL: NGW exceeds the cell");
+  *enl = 0.0;
+  if (nx == 0 || c->proj.nproj == 0) return PSPW_OK;
+  return eval_enl_dev(c, reinterpret_cast<const double2 *>(d_c0), ld, ngw, nx, focc, wkpt, enl,
+                      fnl);
+}
+
 }  // extern "C"

@@ -824,6 +824,29 @@ int pspw_normalize_rho(pspw_scf *s, double *rho, int *warn) {
   return down(s, rho, d);
 }
 
+int pspw_xc_pz_dev(pspw_scf *s, const double *d_rho, double *d_vxc, double *exc) {
+  int rc = scf_enter(s);
+  if (rc) return rc;
+  if (!d_rho || !d_vxc || !exc) return fail(PSPW_ERR_ARG, "xc_pz: null argument");
+  return xc_pz_dev(s, d_rho, d_vxc, exc);
+}
+
+int pspw_normalize_rho_dev(pspw_scf *s, double *d_rho, int *warn) {
+  int rc = scf_enter(s);
+  if (rc) return rc;
+  if (!d_rho) return fail(PSPW_ERR_ARG, "normalize_rho: null argument");
+  return normalize_rho_dev(s, d_rho, s->omega, s->nel, warn);
+}
+
+int pspw_kerker_prec_dev(pspw_scf *s, double *d_x, double beta, double q0) {
+  int rc = scf_enter(s);
+  if (rc) return rc;
+  if (!d_x) return fail(PSPW_ERR_ARG, "kerker_prec: null argument");
+  if ((rc = kerker_prec_dev(s, d_x, beta, q0))) return rc;
+  PSPW_CUDA(cudaStreamSynchronize(s->cell->stream));
+  return device_status(s->cell);
+}
+
 int pspw_kerker_prec(pspw_scf *s, double *x, double beta, double q0) {
   int rc = scf_enter(s);
   if (rc) return rc;

@@ -82,6 +82,8 @@ SIGNATURES = {
     "pspw_lanczos": [_vp, _vp, _i, _i, _vp, _i, _vp],
     "pspw_eval_rho_psi": [_vp, _vp, _vp, _i, _i, _i, _vp, _d, _d, _vp],
     "pspw_eval_enl": [_vp, _vp, _i, _i, _i, _vp, _d, _vp, _vp],
+    "pspw_eval_rho_psi_dev": [_vp, _vp, _vp, _i, _i, _i, _vp, _d, _d, _vp],
+    "pspw_eval_enl_dev": [_vp, _vp, _i, _i, _i, _vp, _d, _vp, _vp],
     "pspw_scf_create": [_vp, _i, _vp, _vp, _vp, _vp, _i, _vp, _vp, _vp, _d, _d, _d, _d, _vp],
     "pspw_scf_destroy": [_vp],
     "pspw_eval_energy": [_vp, _vp, _d, _d, _vp],
@@ -89,6 +91,9 @@ SIGNATURES = {
     "pspw_xc_pz": [_vp, _vp, _vp, _vp],
     "pspw_normalize_rho": [_vp, _vp, _vp],
     "pspw_kerker_prec": [_vp, _vp, _d, _d],
+    "pspw_xc_pz_dev": [_vp, _vp, _vp, _vp],
+    "pspw_normalize_rho_dev": [_vp, _vp, _vp],
+    "pspw_kerker_prec_dev": [_vp, _vp, _d, _d],
     "pspw_mix_init": [_vp, _i, _i, _d, _d, _vp],
     "pspw_mix": [_vp, _i, _vp, _vp],
     "pspw_mix_dev": [_vp, _i, _vp, _vp],

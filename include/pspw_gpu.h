@@ -201,6 +201,13 @@ int pspw_eval_rho_psi(pspw_cell *cell, double *rhoe, const double *eigvec, int l
  * on the device. */
 int pspw_eval_enl(pspw_cell *cell, const double *c0, int ld, int ngw, int nx,
                   const double *focc, double wkpt, double *enl, double *fnl);
+/* the same two on device pointers (rhoe, eigvec, c0: device FP64; focc, enl,
+ * fnl, ekin: host) */
+int pspw_eval_rho_psi_dev(pspw_cell *cell, double *d_rhoe, const double *d_eigvec, int ld,
+                          int ngw, int nx, const double *focc, double wkpt, double omega,
+                          double *ekin);
+int pspw_eval_enl_dev(pspw_cell *cell, const double *d_c0, int ld, int ngw, int nx,
+                      const double *focc, double wkpt, double *enl, double *fnl);
 
 /* ------------------------------------------------------------------ SCF pieces
  * The steps of the SCF iteration around the eigensolver, on the device in
@@ -251,6 +258,10 @@ int pspw_eval_energy_dev(pspw_scf *scf, double *d_rhoe, double ekin, double enl,
 int pspw_xc_pz(pspw_scf *scf, const double *rho, double *vxc, double *exc);
 int pspw_normalize_rho(pspw_scf *scf, double *rho, int *warn);
 int pspw_kerker_prec(pspw_scf *scf, double *x, double beta, double q0);
+/* the same three on device vectors (NNR doubles on the cell's device) */
+int pspw_xc_pz_dev(pspw_scf *scf, const double *d_rho, double *d_vxc, double *exc);
+int pspw_normalize_rho_dev(pspw_scf *scf, double *d_rho, int *warn);
+int pspw_kerker_prec_dev(pspw_scf *scf, double *d_x, double beta, double q0);
 int pspw_mix_init(pspw_scf *scf, int kind, int mixdim, double beta, double q0,
                   const double *rho_old);
 int pspw_mix(pspw_scf *scf, int iter, double *rhoe, double *d);

@@ -115,3 +115,36 @@ def test_mixers_follow_the_reference(case, kind):
         r_e, d_e = c["scf"].mix(it, rin)
         assert np.abs(r_e - r_ref).max() < 1e-9 * np.abs(r_ref).max(), (kind, it)
         assert abs(d_e - d_r) < 1e-9 * max(1.0, abs(d_r)), (kind, it)
+
+
+def test_device_pointer_variants_match_host_variants(case):
+    """pspw_xc_pz_dev, pspw_normalize_rho_dev, pspw_kerker_prec_dev,
+    pspw_eval_energy_dev on torch device vectors give the host variants'
+    results bit for bit (same kernels)."""
+    import ctypes as C
+    from pspw._lib import check, lib
+    L, s, dev = lib(), case["scf"], torch.device("cuda", 0)
+    rho = case["rho"]
+    d = torch.from_numpy(rho.copy()).to(dev)
+    dv = torch.zeros_like(d)
+    e = C.c_double(0.0)
+    check(L.pspw_xc_pz_dev(s._h, d.data_ptr(), dv.data_ptr(), C.byref(e)))
+    v_h, e_h = s.xc_pz(rho)
+    assert np.array_equal(dv.cpu().numpy(), v_h) and e.value == e_h
+    x = torch.from_numpy(1.01 * rho).to(dev)
+    w = C.c_int(0)
+    check(L.pspw_normalize_rho_dev(s._h, x.data_ptr(), C.byref(w)))
+    n_h, w_h = s.normalize_rho(1.01 * rho)
+    assert np.array_equal(x.cpu().numpy(), n_h) and bool(w.value) == w_h
+    y0 = rho - rho.mean()
+    y = torch.from_numpy(y0.copy()).to(dev)
+    check(L.pspw_kerker_prec_dev(s._h, y.data_ptr(), 0.8, 0.6))
+    assert np.array_equal(y.cpu().numpy(), s.kerker_prec(y0, 0.8, 0.6))
+    r = torch.from_numpy(rho.copy()).to(dev)
+    e6 = np.zeros(6)
+    check(L.pspw_eval_energy_dev(s._h, r.data_ptr(), 12.5, 0.75, e6.ctypes.data))
+    torch.cuda.synchronize()
+    v_r, e_r = s.eval_energy(rho, 12.5, 0.75)
+    assert np.array_equal(r.cpu().numpy(), v_r)
+    assert np.array_equal(e6, np.array([e_r[k] for k in ("ETOT", "EKIN", "EHT", "EPSEU", "ENL",
+                                                         "EXC")]))

@@ -171,3 +171,33 @@ def test_lobpcg_long_run_and_mixed_precision(si8_12ry):
     ok = res64 < 1e-3
     assert ok.sum() >= 5
     assert np.abs(ev64[ok] - ev32[ok]).max() < 1e-5
+
+
+def test_eval_device_pointer_variants(gcell):
+    """pspw_eval_rho_psi_dev and pspw_eval_enl_dev on device blocks give the
+    host-buffer calls' results."""
+    import ctypes as C
+    from pspw._lib import check, lib
+    L, dev = lib(), torch.device("cuda", 0)
+    ngw = int(G["ngw"])
+    psi = np.asfortranarray(G["psi"])
+    nx = psi.shape[1]
+    X = torch.from_numpy(np.ascontiguousarray(psi.T)).to(dev)  # ngw x nx column-major
+    nnr = int(np.prod(G["nr"]))
+    rho = torch.full((nnr,), 0.125, dtype=torch.float64, device=dev)
+    ek = C.c_double(0.0)
+    fo = np.ascontiguousarray(G["focc"], dtype=float)
+    check(L.pspw_eval_rho_psi_dev(gcell.handle, rho.data_ptr(), X.data_ptr(), ngw, ngw, nx,
+                                  fo.ctypes.data, 1.0, float(G["omega"]), C.byref(ek)))
+    flat = np.concatenate([psi.reshape(-1, order="F"), np.zeros(int(G["ngwx"]), complex)])
+    rho_h, ek_h = gcell.eval_rho_psi(np.full(nnr, 0.125), flat, ngw, ngw, nx, G["focc"], 1.0,
+                                     float(G["omega"]))
+    assert np.array_equal(rho.cpu().numpy(), rho_h) and ek.value == ek_h
+    focc = np.array([2.0, 2.0, 1.0, 0.5])
+    e = C.c_double(0.0)
+    nproj = gcell.sizes()["nproj"]
+    fnl = np.zeros((nx, nproj), dtype=np.complex128, order="F")
+    check(L.pspw_eval_enl_dev(gcell.handle, X.data_ptr(), ngw, ngw, nx, focc.ctypes.data, 0.75,
+                              C.byref(e), fnl.ctypes.data))
+    e_h, fnl_h = gcell.eval_enl(psi, nx, focc, 0.75)
+    assert e.value == e_h and np.array_equal(fnl, fnl_h)
