@@ -2,7 +2,8 @@
 """Benchmark of the block H*psi path (Chebyshev-filter form) on B200.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl engine|reference]
-                    [--prec f32|f64] [--workload si64]
+                    [--prec f32|f64]
+                    [--workload si64|si216|scf-si8|scf-si64|setup-si64|setup-si216]
 
 One step = one call of the degree-10 Chebyshev filter (chebyfilt.cpp:6-74)
 on the Si64 cell (64 atoms, a = 20.52 bohr, ecutwfc 15 Ha, 64^3 grid,
@@ -168,6 +169,172 @@ def reference_sample(steps, warmup, bands_per_proc=4, procs=None):
                        f"oracle's FFTW-API shim (FFTW3 not installed), scipy OpenBLAS; {procs} "
                        f"processes x {bands_per_proc} bands of the Si64 cell = {nb_total} of 144 "
                        f"bands; {steps} timed calls")}, None
+
+
+# ------------------------------------------------------------------ SCF-loop and set-up rows
+# --workload scf-si8 | scf-si64: one step = one ChebySCF iteration
+# (ChebySCFLoop.cpp:275-366: filter, QR, Rayleigh-Ritz, EvalRhoPsi, EvalENL,
+# Pulay mixing, EvalEnergy, new bounds with a 10-step Lanczos) of the whole
+# program run from an INPUT in the reference's format (random start,
+# scf_conv_crit 0 so every iteration runs).  --workload setup-si64 |
+# setup-si216: one step = the whole set-up before the SCF loop (ReadInputFile,
+# ReadPseudopotentials, Setup, PrepareSCF, the starting density, EwaldEnergy).
+ROW_WORKLOADS = {
+    "scf-si8": dict(kind="scf", nrep=1, grid=(32, 32, 32), nempty=5,
+                    text="Si8, a=10.26 bohr, ECUT 30 Ry, grid 32^3, NGW 2945, NX 21 (23 bands)"),
+    "scf-si64": dict(kind="scf", nrep=2, grid=(64, 64, 64), nempty=14,
+                     text="Si64, a=20.52 bohr, ECUT 30 Ry, grid 64^3, NGW 23847, NX 142 "
+                          "(144 bands)"),
+    "setup-si64": dict(kind="setup", nrep=2, grid=(64, 64, 64), nempty=14,
+                       text="Si64, a=20.52 bohr, ECUT 30 Ry, grid 64^3, NGW 23847, NX 142"),
+    "setup-si216": dict(kind="setup", nrep=3, grid=(96, 96, 96), nempty=32,
+                        text="Si216, a=30.78 bohr, ECUT 30 Ry, grid 96^3, NGW 80725, NX 464"),
+}
+
+
+def _write_row_input(d, w, max_scf):
+    from pspw import synth
+    from pspw.inputs import write_input, write_synthetic_fhi
+    os.makedirs(d, exist_ok=True)
+    lat, pos = synth.si_diamond(w["nrep"])
+    write_synthetic_fhi(os.path.join(d, "X.fhi"))
+    write_input(os.path.join(d, "INPUT"), "X.fhi", pos, float(lat[0][0]), ecut_ry=30.0, iscf=1,
+                idiag=-1, imix=3, max_scf=max_scf, nempty=w["nempty"], fft_grid=w["grid"],
+                conv=0.0)
+    return d
+
+
+def _ref_program_seconds(d, timeout):
+    exe = os.path.join(ROOT, "oracle", "_ref", "ffr_pspw_dft.x")
+    t0 = time.perf_counter()
+    r = subprocess.run([exe], cwd=d, capture_output=True, text=True, timeout=timeout)
+    if r.returncode != 0:
+        raise RuntimeError(r.stdout[-500:])
+    return time.perf_counter() - t0
+
+
+def _ref_setup_seconds(d):
+    code = ("import sys, time, json; sys.path.insert(0, %r); from ref_lib import RefLib; "
+            "R = RefLib(); t = time.perf_counter(); R.program_setup(%r); "
+            "sys.stderr.write(json.dumps(time.perf_counter() - t))"
+            % (os.path.join(ROOT, "oracle"), d))
+    r = subprocess.run([sys.executable, "-c", code], capture_output=True, text=True,
+                       timeout=1800)
+    if r.returncode != 0:
+        raise RuntimeError(r.stderr[-500:])
+    return float(r.stderr.strip().splitlines()[-1])
+
+
+def row_reference(args, w, tmp):
+    """The reference on the row's workload, on the host cores (single
+    process: the reference's SCF loop and set-up are serial)."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    from ref_lib import ref_available
+    if not (ref_available() and os.path.exists(os.path.join(ROOT, "oracle", "_ref",
+                                                             "ffr_pspw_dft.x"))):
+        return None, "oracle/_ref not built (make -C oracle)"
+    if w["kind"] == "setup":
+        d = _write_row_input(os.path.join(tmp, "ref_setup"), w, 1)
+        ts = [_ref_setup_seconds(d) for _ in range(max(1, args.steps))]
+        t = sum(ts) / len(ts)
+        return {"value": 1.0 / t, "unit": "set-ups/s", "cores": len(os.sched_getaffinity(0)),
+                "kind": "reference",
+                "seconds_per_step": t,
+                "sample": f"reference ReadInputFile+Setup+PrepareSCF+starting density+"
+                          f"EwaldEnergy built from its sources (serial code), {len(ts)} "
+                          f"runs"}, None
+    if args.workload == "scf-si64":
+        # one reference iteration on Si64 takes minutes: its filter (more than
+        # 90 % of the iteration) timed on all host cores as a bounded sample
+        ref, why = reference_sample(steps=1, warmup=0)
+        if ref is None:
+            return None, why
+        bytes_filter = DEGREE * hpsi_bytes_model(23847, 64 ** 3, 144, 64)
+        t = bytes_filter / (ref["value"] * 1e9)
+        return {"value": 1.0 / t, "unit": "SCF iterations/s", "cores": ref["cores"],
+                "kind": "reference", "seconds_per_step": t,
+                "sample": "the reference's chebyfilt of the 144-band Si64 block only (the rest "
+                          "of the iteration not counted, so this is an upper bound of the "
+                          "reference's iteration rate); " + ref["sample"]}, None
+    k = max(1, args.steps)
+    t_short = _ref_program_seconds(_write_row_input(os.path.join(tmp, "ref_a"), w, 1), 3600)
+    t_long = _ref_program_seconds(_write_row_input(os.path.join(tmp, "ref_b"), w, 1 + k), 3600)
+    t = (t_long - t_short) / k
+    return {"value": 1.0 / t, "unit": "SCF iterations/s", "cores": len(os.sched_getaffinity(0)),
+            "kind": "reference", "seconds_per_step": t,
+            "sample": f"the reference program (main.cpp -> ChebySCFLoop) built from its "
+                      f"sources on the same INPUT, run with MAX_SCF_ITER 1 and {1 + k}: "
+                      f"(difference of wall times) / {k}; serial code, OpenBLAS with its "
+                      f"default threads for the dense steps"}, None
+
+
+def run_row(args, rank, world, local_rank):
+    import tempfile
+
+    import torch
+    from pspw import PREC_F32, PREC_F64, replica
+    from pspw.system import System
+    w = ROW_WORKLOADS[args.workload]
+    torch.cuda.set_device(local_rank)
+    prec = PREC_F64 if args.prec == "f64" else PREC_F32
+    tmp = tempfile.mkdtemp(prefix="pspw_row_")
+    config = {"workload": f"{args.workload}: {w['text']}", "input": "INPUT + synthetic FHI98 "
+              "pseudopotential in the reference's formats", "mixing": "Pulay (IMIX 3)",
+              "start": "random (IDIAG -1)", "filter_prec": args.prec,
+              "parallelism": f"replica x{world}",
+              "l2": "inputs (NNR grids, the NGW x (NX+2) block) larger than L2 at Si64; "
+                    "no flush"}
+    clocks = ClockSampler(local_rank)
+    if w["kind"] == "scf":
+        n_it = args.warmup + args.steps
+        S = System(_write_row_input(os.path.join(tmp, "engine"), w, n_it), device=local_rank)
+        S.cheby_scf(filter_prec=prec)  # warm-up run (allocations, first-touch)
+        replica.barrier()
+        clocks.start()
+        res = S.cheby_scf(filter_prec=prec)
+        clocks.stop()
+        h = res["hist"]
+        assert res["iterations"] == n_it and np.isfinite(h[:, 0]).all()
+        t = (h[n_it - 1, 3] - h[args.warmup - 1, 3]) * 1e-3 / args.steps
+        S.close()
+        unit, metric = "SCF iterations/s", "ChebySCF iterations/s (whole iteration on the device)"
+    else:
+        d = _write_row_input(os.path.join(tmp, "engine"), w, 1)
+        for _ in range(args.warmup):
+            System(d, device=local_rank).close()
+        replica.barrier()
+        clocks.start()
+        ts, parts = [], None
+        for _ in range(args.steps):
+            t0 = time.perf_counter()
+            S = System(d, device=local_rank)
+            ts.append(time.perf_counter() - t0)
+            parts = S.timing()
+            S.close()
+        clocks.stop()
+        t = sum(ts) / len(ts)
+        unit, metric = "set-ups/s", "system set-ups/s (INPUT to a ready cell, SCF handle and " \
+                                    "starting density)"
+    t_max = replica.max_over_ranks(t)
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        ref, why = row_reference(argparse.Namespace(steps=1, workload=args.workload), w, tmp)
+        cpu = ({k: (round(v, 6) if isinstance(v, float) else v) for k, v in ref.items()
+                if k in ("value", "unit", "cores", "kind", "sample")} if ref else
+               {"value": None, "unavailable": why})
+    if rank == 0:
+        out = {"metric": metric, "value": round(world / t_max, 4), "unit": unit, "n_gpus": world,
+               "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(t_max * 1e3, 3),
+               "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+               "dtype": "f64" if args.prec == "f64" else "c64 filter, f64 rest",
+               "data": "synthetic", "config": config, "cpu_baseline": cpu,
+               "clocks": clocks.summary(),
+               "timing": "host wall clock between iteration ends (the loop synchronises at "
+                         "each iteration end)" if w["kind"] == "scf" else
+                         "host wall clock around pspw_system_load"}
+        if w["kind"] == "setup":
+            out["phases_ms"] = {k: round(v, 3) for k, v in parts.items()}
+        print(json.dumps(out))
 
 
 # ------------------------------------------------------------------ engine arm
@@ -366,6 +533,39 @@ def main():
               "filter_window_ha": [LB, UB], "global_batch": 144 * world,
               "parallelism": f"replica x{world} (bands independent, no collective)",
               "l2": "flushed between steps (256 MB write, outside the timed interval)"}
+
+    if args.workload in ROW_WORKLOADS:
+        if args.impl == "reference":
+            if rank != 0:
+                return
+            import tempfile
+            w = ROW_WORKLOADS[args.workload]
+            ref, why = row_reference(args, w, tempfile.mkdtemp(prefix="pspw_row_ref_"))
+            if ref is None:
+                print(json.dumps({"impl": "reference", "unavailable": why}))
+                return
+            print(json.dumps({"impl": "reference", "metric": args.workload, "value":
+                              round(ref["value"], 6), "unit": ref["unit"], "n_gpus": args.gpus,
+                              "steps": args.steps, "warmup": args.warmup,
+                              "ms_per_step": round(ref["seconds_per_step"] * 1e3, 3),
+                              "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+                              "dtype": "c128", "data": "synthetic",
+                              "config": {"workload": f"{args.workload}: {w['text']}"},
+                              "cpu_baseline": {k: ref[k] for k in ("value", "unit", "cores",
+                                                                   "kind", "sample")},
+                              "e2e": {"value": round(ref["value"], 6), "unit": ref["unit"],
+                                      "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}))
+            return
+        import torch
+        if world > 1:
+            import datetime
+            torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                                 device_id=torch.device("cuda", local_rank))
+        run_row(args, rank, world, local_rank)
+        if world > 1:
+            torch.distributed.barrier()
+            torch.distributed.destroy_process_group()
+        return
 
     if args.impl == "reference":
         if rank != 0:

@@ -14,6 +14,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <chrono>
 #include <cmath>
 #include <cstring>
 #include <vector>
@@ -147,11 +148,17 @@ extern "C" int pspw_cheby_scf(pspw_scf *s, const pspw_scf_params *p, const doubl
   std::vector<double> evals(nx2), res(nx2);
   int iter_start = 1, done_iters = 0;
   *converged = 0;
+  const auto t_start = std::chrono::steady_clock::now();
   auto record = [&](int it, double etot, double detot, double drms) {
     if (hist && it >= 1 && it <= p->max_scf_iter) {
-      hist[3 * (it - 1)] = etot;
-      hist[3 * (it - 1) + 1] = detot;
-      hist[3 * (it - 1) + 2] = drms;
+      double *h = hist + 4 * (size_t)(it - 1);
+      h[0] = etot;
+      h[1] = detot;
+      h[2] = drms;
+      // the iteration's results are on the host here (its last step
+      // synchronised the stream), so the host clock marks its end
+      h[3] = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t_start)
+                 .count();
     }
   };
   // density, EKIN, ENL of the first nx columns of X (ld ngw), then mixing

@@ -116,8 +116,8 @@ class Scf:
         """The SCF loop of ChebySCFLoop.cpp on the device (pspw_cheby_scf).
         X: NGW x (NX+2) start block for idiag < 0 (ignored otherwise).
         Returns a dict with eig (NX), X (final block), rho (final mixed
-        density), hist (iterations x {ETOT, |dETOT|, d}), energies,
-        iterations and converged."""
+        density), hist (iterations x {ETOT, |dETOT|, d, ms since the call
+        began}), energies, iterations and converged."""
         ngw = self.cell.sizes()["ngw"]
         nx2 = nx + 2
         p = ScfParams(nx, nempty, degree, max_scf_iter, conv, imix, mixdim, mix_beta, pulay_beta,
@@ -130,7 +130,7 @@ class Scf:
         xf = np.asfortranarray(x)
         eig = np.zeros(nx)
         rho = np.zeros(self.nnr)
-        hist = np.zeros(3 * max_scf_iter)
+        hist = np.zeros(4 * max_scf_iter)
         its, cv = C.c_int(0), C.c_int(0)
         e6 = np.zeros(6)
         check(lib().pspw_cheby_scf(self._h, C.byref(p), fo.ctypes.data, rs.ctypes.data,
@@ -138,7 +138,7 @@ class Scf:
                                    rho.ctypes.data, hist.ctypes.data, C.byref(its), C.byref(cv),
                                    e6.ctypes.data))
         n = its.value
-        return dict(eig=eig, X=xf, rho=rho, hist=hist.reshape(-1, 3)[:n], iterations=n,
+        return dict(eig=eig, X=xf, rho=rho, hist=hist.reshape(-1, 4)[:n], iterations=n,
                     converged=bool(cv.value),
                     energies=dict(zip(("ETOT", "EKIN", "EHT", "EPSEU", "ENL", "EXC"),
                                       e6.tolist())))

@@ -91,19 +91,19 @@ class System:
     def cheby_scf(self, filter_prec=PREC_F64, outdir=None):
         """ChebySCFLoop() of the reference's main program on this system.
         Returns eig (NX), energies, iterations, converged and hist
-        (iterations x {ETOT, |dETOT|, d})."""
+        (iterations x {ETOT, |dETOT|, d, ms since the call began})."""
         nx = self.dims["nx"]
         eig, e6 = np.zeros(nx), np.zeros(6)
         its, cv = C.c_int(0), C.c_int(0)
         p = self.params()
-        hist = np.zeros(3 * max(1, p["max_scf_iter"]))
+        hist = np.zeros(4 * max(1, p["max_scf_iter"]))
         check(lib().pspw_system_cheby_scf(self._h, int(filter_prec),
                                           None if outdir is None else str(outdir).encode(),
                                           eig.ctypes.data, e6.ctypes.data, C.byref(its),
                                           C.byref(cv), hist.ctypes.data))
         n = its.value
         return dict(eig=eig, iterations=n, converged=bool(cv.value),
-                    hist=hist.reshape(-1, 3)[:n],
+                    hist=hist.reshape(-1, 4)[:n],
                     energies=dict(zip(("ETOT", "EKIN", "EHT", "EPSEU", "ENL", "EXC"),
                                       e6.tolist())))
 

@@ -280,8 +280,10 @@ int pspw_mix_dev(pspw_scf *scf, int iter, double *d_rhoe, double *d);
  *   X          NGW x (NX+2) complex: the start block when idiag < 0 (it is
  *              orthonormalised), the final block on return
  *   eig        NX eigenvalues (EIG); rho_out (may be null) the final mixed
- *              density; hist (may be null) 3 x max_scf_iter (ETOT, |dETOT|,
- *              the mixer's d) per iteration; e6 the final {ETOT, EKIN, EHT,
+ *              density; hist (may be null) 4 x max_scf_iter: per iteration
+ *              ETOT, |dETOT|, the mixer's d, and the milliseconds from the
+ *              start of the call to the end of the iteration (host clock,
+ *              taken after the iteration's results reached the host); e6 the final {ETOT, EKIN, EHT,
  *              EPSEU, ENL, EXC}; *iterations the last iteration done;
  *              *converged = 1 if |dETOT| <= conv was reached.
  * The pspw_scf handle supplies the local potential data, OMEGA and NEL. */
