@@ -296,6 +296,16 @@ def run_row(args, rank, world, local_rank):
         h = res["hist"]
         assert res["iterations"] == n_it and np.isfinite(h[:, 0]).all()
         t = (h[n_it - 1, 3] - h[args.warmup - 1, 3]) * 1e-3 / args.steps
+        # a third run with the phase timers on (CUDA events around each phase
+        # on the cell stream), reported as the mean per iteration
+        cell = S.cell()
+        cell.timing_reset()
+        cell.timing_enable(sum(1 << f for f in range(11, 19)))
+        S.cheby_scf(filter_prec=prec)
+        cell.timing_enable(0)
+        names = ("filter", "qr", "rayleigh_ritz_products", "eigendecomposition", "density",
+                 "enl", "mixing_energy", "lanczos_bounds")
+        parts = {nm: round(cell.timing_read(f)[0] / n_it, 3) for nm, f in zip(names, range(11, 19))}
         S.close()
         unit, metric = "SCF iterations/s", "ChebySCF iterations/s (whole iteration on the device)"
     else:
@@ -334,6 +344,8 @@ def run_row(args, rank, world, local_rank):
                          "host wall clock around pspw_system_load"}
         if w["kind"] == "setup":
             out["phases_ms"] = {k: round(v, 3) for k, v in parts.items()}
+        else:
+            out["phases_ms_per_iteration"] = parts
         print(json.dumps(out))
 
 

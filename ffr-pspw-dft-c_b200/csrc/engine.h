@@ -87,7 +87,16 @@ enum Family {
   kFamProj = 8,
   kFamBackproj = 9,
   kFamGemm = 10,     // subspace GEMMs of the solvers
-  kNumFamilies = 11
+  // phases of one ChebySCF iteration (pspw_cheby_scf)
+  kFamScfFilter = 11,
+  kFamScfQr = 12,
+  kFamScfRayleigh = 13,  // H X, X^H H X, rotation
+  kFamScfEig = 14,       // symmetrize + eigendecomposition of the NX+2 matrix
+  kFamScfDensity = 15,   // EvalRhoPsi
+  kFamScfEnl = 16,       // EvalENL
+  kFamScfMixEnergy = 17, // mixing + EvalEnergy + V_eff upload
+  kFamScfLanczos = 18,   // bounds for the next filter
+  kNumFamilies = 19
 };
 
 // Workspace slots of a cell (grown on demand, kept until the cell is freed).

@@ -100,6 +100,67 @@ __global__ void __launch_bounds__(256) k_zgemm(int m, int n, int k, cx<R> alpha,
   }
 }
 
+// The same for n <= 8 columns: 64 rows x 8 columns per block, thread
+// (r = t & 63, c = t >> 6) owns row r and columns c and c + 4; each output
+// accumulates the same products in the same order as k_zgemm.
+template <typename R, int BK, bool CONJ_A>
+__global__ void __launch_bounds__(256) k_zgemm_n8(int m, int n, int k, cx<R> alpha,
+                                                  const cx<R> *__restrict__ A, int lda,
+                                                  const cx<R> *__restrict__ B, int ldb,
+                                                  cx<R> beta, cx<R> *C, int ldc, int kchunk,
+                                                  cx<R> *__restrict__ part) {
+  using T = cx<R>;
+  __shared__ T As[BK][kGM + 1];
+  __shared__ T Bs[BK][8 + 1];
+  const int r = threadIdx.x & 63, cc = threadIdx.x >> 6;
+  const int m0 = blockIdx.x * kGM;
+  const int kb = blockIdx.z * kchunk;
+  const int ke = min(k, kb + kchunk);
+  T acc[2] = {czero<T>(), czero<T>()};
+  for (int k0 = kb; k0 < ke; k0 += BK) {
+    if (CONJ_A) {
+      for (int e = threadIdx.x; e < BK * kGM; e += 256) {
+        const int kk = e % BK, mm = e / BK;
+        const int gk = k0 + kk, gm = m0 + mm;
+        As[kk][mm] = (gk < ke && gm < m) ? cj(A[(size_t)gm * lda + gk]) : czero<T>();
+      }
+    } else {
+      for (int e = threadIdx.x; e < BK * kGM; e += 256) {
+        const int mm = e % kGM, kk = e / kGM;
+        const int gk = k0 + kk, gm = m0 + mm;
+        As[kk][mm] = (gk < ke && gm < m) ? A[(size_t)gk * lda + gm] : czero<T>();
+      }
+    }
+    for (int e = threadIdx.x; e < BK * 8; e += 256) {
+      const int kk = e % BK, nn = e / BK;
+      const int gk = k0 + kk;
+      Bs[kk][nn] = (gk < ke && nn < n) ? B[(size_t)nn * ldb + gk] : czero<T>();
+    }
+    __syncthreads();
+#pragma unroll 4
+    for (int kk = 0; kk < BK; kk++) {
+      const T av = As[kk][r];
+      cfma(acc[0], av, Bs[kk][cc]);
+      cfma(acc[1], av, Bs[kk][cc + 4]);
+    }
+    __syncthreads();
+  }
+  const int gm = m0 + r;
+  if (gm >= m) return;
+#pragma unroll
+  for (int j = 0; j < 2; j++) {
+    const int gn = cc + 4 * j;
+    if (gn >= n) continue;
+    if (part) {
+      part[((size_t)blockIdx.z * n + gn) * m + gm] = acc[j];
+    } else {
+      T r2 = cmul(alpha, acc[j]);
+      if (beta.x != (R)0 || beta.y != (R)0) r2 = r2 + cmul(beta, C[(size_t)gn * ldc + gm]);
+      C[(size_t)gn * ldc + gm] = r2;
+    }
+  }
+}
+
 template <typename R>
 __global__ void k_zgemm_reduce(int m, int n, int nsplit, const cx<R> *__restrict__ part,
                                cx<R> alpha, cx<R> beta, cx<R> *C, int ldc) {
@@ -144,12 +205,21 @@ int zgemm(pspw_cell *c, char opa, int m, int n, int k, cx<R> alpha, const cx<R> 
   dim3 grid(mt, nt, nsplit);
   cudaEvent_t ev;
   timing_begin(c, kFamGemm, &ev);
-  if (conj)
+  if (n <= 8) {
+    const dim3 g8(mt, 1, nsplit);
+    if (conj)
+      k_zgemm_n8<R, BK, true><<<g8, 256, 0, st>>>(m, n, k, alpha, A, lda, B, ldb, beta, C, ldc,
+                                                  kchunk, part);
+    else
+      k_zgemm_n8<R, BK, false><<<g8, 256, 0, st>>>(m, n, k, alpha, A, lda, B, ldb, beta, C, ldc,
+                                                   kchunk, part);
+  } else if (conj) {
     k_zgemm<R, BK, true><<<grid, 256, 0, st>>>(m, n, k, alpha, A, lda, B, ldb, beta, C, ldc,
                                                kchunk, part);
-  else
+  } else {
     k_zgemm<R, BK, false><<<grid, 256, 0, st>>>(m, n, k, alpha, A, lda, B, ldb, beta, C, ldc,
                                                 kchunk, part);
+  }
   c->kernel_launches++;
   if (nsplit > 1) {
     k_zgemm_reduce<R><<<std::min<size_t>(4 * 148, ((size_t)m * n + 255) / 256), 256, 0, st>>>(

@@ -435,6 +435,106 @@ __global__ void __launch_bounds__(256) k_backproj(ProjArg pa, const cx<R> *__res
   }
 }
 
+// Narrow tiles for blocks of at most 8 bands (the single vectors of Lanczos,
+// small batches): 64 rows x 8 bands per block, thread (r = t & 63,
+// c = t >> 6) owns row r and bands c and c + 4.  Every output accumulates the
+// same products in the same order as in the 64 x 64 kernels above, so the
+// results are identical; only the wasted columns are gone.
+constexpr int kNN = 8;
+
+template <typename R, int BK>
+__global__ void __launch_bounds__(256) k_proj_n8(ProjArg pa, const cx<R> *__restrict__ psi,
+                                                 int ld, int ngw, int nb, int kchunk,
+                                                 cx<R> *__restrict__ part) {
+  using T = cx<R>;
+  __shared__ T As[BK][kBM + 1];
+  __shared__ T Bs[BK][kNN + 1];
+  const int r = threadIdx.x & 63, cc = threadIdx.x >> 6;
+  const int p0 = blockIdx.x * kBM;
+  const int kb = blockIdx.z * kchunk;
+  const int ke = min(ngw, kb + kchunk);
+  T acc0 = czero<T>(), acc1 = czero<T>();
+  for (int k0 = kb; k0 < ke; k0 += BK) {
+    for (int e = threadIdx.x; e < BK * kBM; e += 256) {
+      const int kk = e % BK, m = e / BK;
+      const int ig = k0 + kk, p = p0 + m;
+      As[kk][m] = (ig < ke && p < pa.nproj) ? beta_at<R>(pa, ig, p) : czero<T>();
+    }
+    for (int e = threadIdx.x; e < BK * kNN; e += 256) {
+      const int kk = e % BK, n = e / BK;
+      const int ig = k0 + kk;
+      Bs[kk][n] = (ig < ke && n < nb) ? psi[(size_t)n * ld + ig] : czero<T>();
+    }
+    __syncthreads();
+#pragma unroll 4
+    for (int kk = 0; kk < BK; kk++) {
+      const T av = As[kk][r];
+      cfmac(acc0, av, Bs[kk][cc]);
+      cfmac(acc1, av, Bs[kk][cc + 4]);
+    }
+    __syncthreads();
+  }
+  const int p = p0 + r;
+  if (p < pa.nproj) {
+    if (cc < nb) part[((size_t)blockIdx.z * nb + cc) * pa.nproj + p] = acc0;
+    if (cc + 4 < nb) part[((size_t)blockIdx.z * nb + cc + 4) * pa.nproj + p] = acc1;
+  }
+}
+
+template <typename R, int BK>
+__global__ void __launch_bounds__(256) k_backproj_n8(ProjArg pa, const cx<R> *__restrict__ wp,
+                                                     int ngw, int nb, cx<R> *out, int ldo,
+                                                     const cx<R> *__restrict__ in, int ldi,
+                                                     const cx<R> *__restrict__ xm2, int ldx, R a,
+                                                     R bc, R gc) {
+  using T = cx<R>;
+  __shared__ T As[BK][kBM + 1];
+  __shared__ T Bs[BK][kNN + 1];
+  const int r = threadIdx.x & 63, cc = threadIdx.x >> 6;
+  const int g0 = blockIdx.x * kBM;
+  T acc[2] = {czero<T>(), czero<T>()};
+  for (int k0 = 0; k0 < pa.nproj; k0 += BK) {
+    for (int e = threadIdx.x; e < BK * kBM; e += 256) {
+      const int m = e % kBM, kk = e / kBM;
+      const int ig = g0 + m, p = k0 + kk;
+      As[kk][m] = (ig < ngw && p < pa.nproj) ? beta_at<R>(pa, ig, p) : czero<T>();
+    }
+    for (int e = threadIdx.x; e < BK * kNN; e += 256) {
+      const int kk = e % BK, n = e / BK;
+      const int p = k0 + kk;
+      Bs[kk][n] = (p < pa.nproj && n < nb) ? wp[(size_t)n * pa.nproj + p] : czero<T>();
+    }
+    __syncthreads();
+#pragma unroll 4
+    for (int kk = 0; kk < BK; kk++) {
+      const T av = As[kk][r];
+      cfma(acc[0], av, Bs[kk][cc]);
+      cfma(acc[1], av, Bs[kk][cc + 4]);
+    }
+    __syncthreads();
+  }
+  const int ig = g0 + r;
+  if (ig >= ngw) return;
+#pragma unroll
+  for (int j = 0; j < 2; j++) {
+    const int bb = cc + 4 * j;
+    if (bb >= nb) continue;
+    T h = out[(size_t)bb * ldo + ig] + acc[j];
+    T v = mk<T>(a * h.x, a * h.y);
+    if (bc != (R)0) {
+      const T u = in[(size_t)bb * ldi + ig];
+      v.x += bc * u.x;
+      v.y += bc * u.y;
+    }
+    if (gc != (R)0) {
+      const T u = xm2[(size_t)bb * ldx + ig];
+      v.x += gc * u.x;
+      v.y += gc * u.y;
+    }
+    out[(size_t)bb * ldo + ig] = v;
+  }
+}
+
 // out = a*out + bc*in + g*xm2 (no projectors)
 template <typename R>
 __global__ void k_axpby3(int ngw, int nb, cx<R> *out, int ldo, const cx<R> *__restrict__ in,
@@ -619,7 +719,12 @@ int hpsi_apply(pspw_cell *c, const void *in_v, int ld_in, void *out_v, int ld_ou
       if (rc) return rc;
     } else {
       run(kFamProj, [&] {
-        k_proj<R, BK><<<dim3(mt, nt, nsplit), 256, 0, st>>>(pa, in, ld_in, ngw, nb, kchunk, part);
+        if (nb <= kNN)
+          k_proj_n8<R, BK><<<dim3(mt, 1, nsplit), 256, 0, st>>>(pa, in, ld_in, ngw, nb, kchunk,
+                                                                part);
+        else
+          k_proj<R, BK><<<dim3(mt, nt, nsplit), 256, 0, st>>>(pa, in, ld_in, ngw, nb, kchunk,
+                                                              part);
       });
       run(kFamProj, [&] {
         k_proj_reduce<R><<<(nb * nproj + 255) / 256, 256, 0, st>>>(part, Prec<R>::pw(c), nsplit,
@@ -712,8 +817,12 @@ int hpsi_apply(pspw_cell *c, const void *in_v, int ld_in, void *out_v, int ld_ou
     } else {
       dim3 grid((ngw + kBM - 1) / kBM, (nb + kBN - 1) / kBN);
       run(kFamBackproj, [&] {
-        k_backproj<R, BK><<<grid, 256, 0, st>>>(pa, wp, ngw, nb, out, ld_out, in, ld_in, xm2,
-                                                ld_xm2, (R)a, (R)b, (R)g);
+        if (nb <= kNN)
+          k_backproj_n8<R, BK><<<grid.x, 256, 0, st>>>(pa, wp, ngw, nb, out, ld_out, in, ld_in,
+                                                       xm2, ld_xm2, (R)a, (R)b, (R)g);
+        else
+          k_backproj<R, BK><<<grid, 256, 0, st>>>(pa, wp, ngw, nb, out, ld_out, in, ld_in, xm2,
+                                                  ld_xm2, (R)a, (R)b, (R)g);
       });
     }
     timing_end(c, kFamNonlocal, ev);
@@ -751,7 +860,12 @@ int project_fp64(pspw_cell *c, const double2 *psi, int ld, int ngw, int nb, doub
   cx<R> *part = nullptr;
   int rc = ws_reserve(c, kWsProjPart, sizeof(cx<R>) * (size_t)nsplit * nb * nproj, (void **)&part);
   if (rc) return rc;
-  k_proj<R, BK><<<dim3(mt, nt, nsplit), 256, 0, c->stream>>>(pa, psi, ld, ngw, nb, kchunk, part);
+  if (nb <= kNN)
+    k_proj_n8<R, BK><<<dim3(mt, 1, nsplit), 256, 0, c->stream>>>(pa, psi, ld, ngw, nb, kchunk,
+                                                                 part);
+  else
+    k_proj<R, BK><<<dim3(mt, nt, nsplit), 256, 0, c->stream>>>(pa, psi, ld, ngw, nb, kchunk,
+                                                               part);
   k_proj_reduce<R><<<(nb * nproj + 255) / 256, 256, 0, c->stream>>>(part, nullptr, nsplit, nb,
                                                                     nproj, P);
   c->kernel_launches += 2;

@@ -59,6 +59,46 @@ double induced_norm_mat(const double *A, int lda, int N) {
   return res;
 }
 
+// An orthonormal basis of span(X) (X: ngw x n, ld ngw) in place, for the
+// Rayleigh-Ritz step that follows the filter (ChebySCFLoop.cpp:288-307):
+// the reference's Householder QR (ortho_qr.cpp) and any other orthonormal
+// basis of the same span give the same Ritz pairs, since Rayleigh-Ritz
+// depends on the span only (Q and Q D, D a diagonal of unit-modulus
+// phases, differ in the phases of the Ritz vectors alone).  CholeskyQR2:
+// twice G = X^H X = U^H U, X <- X U^-1 (two Gram GEMMs, two small Cholesky
+// factorisations, two triangular solves, instead of the geqrf + ungqr
+// panel sweeps).  Stable while cond(X) stays well below 1/sqrt(eps); the
+// ratio of the largest to the smallest diagonal of the first U bounds
+// cond(X) from below, and above 1e6 (or when the factorisation fails) the
+// block goes to the Householder QR instead.  G: n x n scratch (ld n).
+int span_orthonormalize(pspw_cell *c, double2 *X, int ngw, int n, double2 *G, int *info) {
+  const double2 one = make_double2(1.0, 0.0), zero = make_double2(0.0, 0.0);
+  int rc;
+  for (int pass = 0; pass < 2; pass++) {
+    if ((rc = zgemm<double>(c, 'C', n, n, ngw, one, X, ngw, X, ngw, zero, G, n))) return rc;
+    int pinfo = 0;
+    if ((rc = dev_potrf_upper(c, G, n, n, &pinfo))) return rc;
+    bool fallback = pinfo != 0;
+    if (!fallback && pass == 0) {
+      std::vector<double2> d(n);
+      PSPW_CUDA(cudaMemcpy2DAsync(d.data(), sizeof(double2), G, sizeof(double2) * (n + 1),
+                                  sizeof(double2), n, cudaMemcpyDeviceToHost, c->stream));
+      PSPW_CUDA(cudaStreamSynchronize(c->stream));
+      double lo = INFINITY, hi = 0.0;
+      for (const double2 &v : d) {
+        const double a = std::fabs(v.x);
+        lo = std::min(lo, a);
+        hi = std::max(hi, a);
+      }
+      fallback = !(lo > 0.0) || hi / lo > 1.0e6;
+    }
+    if (fallback) return dev_ortho_qr(c, X, ngw, ngw, n, info);
+    if ((rc = dev_trsm_right_upper(c, G, n, X, ngw, ngw, n))) return rc;
+  }
+  *info = 0;
+  return PSPW_OK;
+}
+
 struct DevBuf {
   std::vector<void *> p;
   ~DevBuf() {
@@ -167,13 +207,21 @@ extern "C" int pspw_cheby_scf(pspw_scf *s, const pspw_scf_params *p, const doubl
     int r;
     PSPW_CUDA(cudaMemsetAsync(rho, 0, sizeof(double) * nnr, st));
     double ekin = 0.0, enl = 0.0;
+    cudaEvent_t e;
+    timing_begin(c, kFamScfDensity, &e);
     if ((r = eval_rho_psi_dev(c, X, ngw, ngw, nx, focc, 1.0, s->omega, rho, &ekin))) return r;
+    timing_end(c, kFamScfDensity, e);
+    timing_begin(c, kFamScfEnl, &e);
     if ((r = eval_enl_dev(c, X, ngw, ngw, nx, focc, 1.0, &enl, nullptr))) return r;
+    timing_end(c, kFamScfEnl, e);
+    timing_begin(c, kFamScfMixEnergy, &e);
     if ((r = mix_dev(s, it, rho, drms))) return r;
     PSPW_CUDA(cudaMemcpyAsync(veff, rho, sizeof(double) * nnr, cudaMemcpyDeviceToDevice, st));
     if ((r = eval_energy_dev(s, veff, ekin, enl, en))) return r;
     *etot = en[0];
-    return pspw_cell_set_veff_device(c, veff, nnr);
+    r = pspw_cell_set_veff_device(c, veff, nnr);
+    timing_end(c, kFamScfMixEnergy, e);
+    return r;
   };
   if (p->idiag < 0) {
     // the caller's random block, orthonormalised (ChebySCFLoop.cpp:201-209)
@@ -200,7 +248,9 @@ extern "C" int pspw_cheby_scf(pspw_scf *s, const pspw_scf_params *p, const doubl
   double *dfn;
   if (!mem.get(&dfn, 1)) return fail(PSPW_ERR_OOM, "cheby_scf: device memory");
   for (int it = iter_start; it <= p->max_scf_iter; it++) {
+    cudaEvent_t ev;
     // filter the NX+2 block (ChebySCFLoop.cpp:285)
+    timing_begin(c, kFamScfFilter, &ev);
     if (p->filter_prec == PSPW_PREC_F32) {
       const size_t n = (size_t)ngw * nx2;
       k_z2c<<<4 * 148, 256, 0, st>>>(X, Xf, n);
@@ -211,16 +261,25 @@ extern "C" int pspw_cheby_scf(pspw_scf *s, const pspw_scf_params *p, const doubl
     } else if ((rc = pspw_chebyfilt_dev(c, PSPW_PREC_F64, X, ngw, ngw, nx2, p->degree, lb, ub))) {
       return rc;
     }
+    timing_end(c, kFamScfFilter, ev);
     int info = 0;
-    if ((rc = dev_ortho_qr(c, X, ngw, ngw, nx2, &info))) return rc;
+    timing_begin(c, kFamScfQr, &ev);
+    if ((rc = span_orthonormalize(c, X, ngw, nx2, T, &info))) return rc;
+    timing_end(c, kFamScfQr, ev);
     // Rayleigh-Ritz (ChebySCFLoop.cpp:293-307)
+    timing_begin(c, kFamScfRayleigh, &ev);
     if ((rc = hpsi_apply<double>(c, X, ngw, HX, ngw, ngw, nx2, 1.0, 0.0, 0.0, nullptr, ngw)))
       return rc;
     const double2 one = make_double2(1.0, 0.0), zero = make_double2(0.0, 0.0);
     if ((rc = zgemm<double>(c, 'C', nx2, nx2, ngw, one, X, ngw, HX, ngw, zero, T, nx2))) return rc;
+    timing_end(c, kFamScfRayleigh, ev);
+    timing_begin(c, kFamScfEig, &ev);
     if ((rc = dev_symmetrize(c, T, nx2, nx2))) return rc;
     if ((rc = dev_zheevd(c, T, nx2, wT, nx2, &info))) return rc;
+    timing_end(c, kFamScfEig, ev);
+    timing_begin(c, kFamScfRayleigh, &ev);
     if ((rc = zgemm<double>(c, 'N', ngw, nx2, nx2, one, X, ngw, T, nx2, zero, HX, ngw))) return rc;
+    timing_end(c, kFamScfRayleigh, ev);
     std::swap(X, HX);
     PSPW_CUDA(cudaMemcpyAsync(evals.data(), wT, sizeof(double) * nx2, cudaMemcpyDeviceToHost, st));
     PSPW_CUDA(cudaStreamSynchronize(st));
@@ -238,10 +297,12 @@ extern "C" int pspw_cheby_scf(pspw_scf *s, const pspw_scf_params *p, const doubl
     // new bounds (ChebySCFLoop.cpp:356-366)
     lb = evals[nx + 1];
     const int kl = k > 10 ? 10 : k;
+    timing_begin(c, kFamScfLanczos, &ev);
     if ((rc = lanczos_dev(c, dv0, ngw, kl, rT10.data(), k, df))) return rc;
     double fn = 0.0;
     if ((rc = dev_coldot(c, df, ngw, df, ngw, ngw, 1, dfn))) return rc;
     PSPW_CUDA(cudaMemcpyAsync(&fn, dfn, sizeof(double), cudaMemcpyDeviceToHost, st));
+    timing_end(c, kFamScfLanczos, ev);
     PSPW_CUDA(cudaStreamSynchronize(st));
     ub = induced_norm_mat(rT10.data(), k, kl) + std::sqrt(fn);
   }

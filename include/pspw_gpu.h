@@ -368,7 +368,11 @@ int pspw_print_3d_array(const double *a, int n1, int n2, int n3, const char *pat
  * of the enabled families, summed until reset.  Families (bit i of the mask):
  * 0 whole H*psi / filter call, 1 FFT pass chain, 2 projector GEMMs,
  * 3 sticks_inv, 4 planes_inv, 5 xlines, 6 planes_fwd, 7 sticks_fwd,
- * 8 projection GEMM (+ reduction), 9 back-projection GEMM. */
+ * 8 projection GEMM (+ reduction), 9 back-projection GEMM, 10 subspace GEMMs;
+ * phases of a pspw_cheby_scf iteration: 11 filter, 12 QR, 13 Rayleigh-Ritz
+ * products (H X, X^H H X, rotation), 14 symmetrize + eigendecomposition,
+ * 15 EvalRhoPsi, 16 EvalENL, 17 mixing + EvalEnergy + V_eff, 18 Lanczos
+ * bounds. */
 int pspw_timing_enable(pspw_cell *cell, int family_mask);
 int pspw_timing_read(pspw_cell *cell, int family, double *total_ms, long long *launches);
 int pspw_timing_reset(pspw_cell *cell);
