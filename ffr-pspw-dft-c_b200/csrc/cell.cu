@@ -207,6 +207,7 @@ int pspw_cell_destroy(pspw_cell *c) {
   if (!c) return PSPW_OK;
   cudaSetDevice(c->device);
   if (c->stream) cudaStreamSynchronize(c->stream);
+  if (c->stream2) cudaStreamSynchronize(c->stream2);
   Basis &B = c->basis;
   void *ptrs[] = {B.d_col_start, B.d_sg_ig, B.d_sg_z, B.d_sg_col, B.d_col_of_xy, B.d_xa_list,
                   B.d_xa_of_x, B.d_kin64, B.d_kin32, B.d_xkg64, c->proj.d_eigr64, c->proj.d_eigr32,
@@ -230,6 +231,9 @@ int pspw_cell_destroy(pspw_cell *c) {
   if (c->cusolver) cusolverDnDestroy(static_cast<cusolverDnHandle_t>(c->cusolver));
   if (c->cublas) cublasDestroy(static_cast<cublasHandle_t>(c->cublas));
   if (c->stream) cudaStreamDestroy(c->stream);
+  if (c->stream2) cudaStreamDestroy(c->stream2);
+  if (c->ev_fork) cudaEventDestroy(c->ev_fork);
+  if (c->ev_join) cudaEventDestroy(c->ev_join);
   delete c;
   return PSPW_OK;
 }
@@ -304,6 +308,10 @@ int cell_create(pspw_cell **out, int device, int nr1, int nr2, int nr3, int ngw,
     pspw_cell_destroy(c);
     return code;
   };
+  if (cudaStreamCreateWithFlags(&c->stream2, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaEventCreateWithFlags(&c->ev_fork, cudaEventDisableTiming) != cudaSuccess ||
+      cudaEventCreateWithFlags(&c->ev_join, cudaEventDisableTiming) != cudaSuccess)
+    return bail(fail(PSPW_ERR_CUDA, "cell_create: projection stream"));
   if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess)
     return bail(fail(PSPW_ERR_CUDA, "cell_create: stream"));
   Basis &B = c->basis;

@@ -143,6 +143,10 @@ struct Workspace {
 struct pspw_cell {
   int device = 0;
   cudaStream_t stream = nullptr;
+  // second stream for the projection, which runs concurrently with the local
+  // part of H*psi (fork and join events on the cell stream)
+  cudaStream_t stream2 = nullptr;
+  cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
   int ngwx = 0;
   double tpiba2 = 0.0;
   int band_batch = 0;

@@ -101,8 +101,9 @@ __global__ void __launch_bounds__(256) k_zgemm(int m, int n, int k, cx<R> alpha,
 }
 
 // The same for n <= 8 columns: 64 rows x 8 columns per block, thread
-// (r = t & 63, c = t >> 6) owns row r and columns c and c + 4; each output
-// accumulates the same products in the same order as k_zgemm.
+// (r = t & 63, c = t >> 6) owns row r and columns c and c + 4; within a K
+// slice each output accumulates the same products in the same order as
+// k_zgemm.
 template <typename R, int BK, bool CONJ_A>
 __global__ void __launch_bounds__(256) k_zgemm_n8(int m, int n, int k, cx<R> alpha,
                                                   const cx<R> *__restrict__ A, int lda,
@@ -177,6 +178,31 @@ __global__ void k_zgemm_reduce(int m, int n, int nsplit, const cx<R> *__restrict
   }
 }
 
+// split-K reduction for narrow products: one warp per output, lanes over
+// the slices in a fixed order, then a fixed shuffle tree
+template <typename R>
+__global__ void k_zgemm_reduce_warp(int m, int n, int nsplit, const cx<R> *__restrict__ part,
+                                    cx<R> alpha, cx<R> beta, cx<R> *C, int ldc) {
+  using T = cx<R>;
+  const size_t tot = (size_t)m * n;
+  const size_t o = (blockIdx.x * (size_t)blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  if (o >= tot) return;  // uniform per warp
+  T s = czero<T>();
+  for (int p = lane; p < nsplit; p += 32) s = s + part[(size_t)p * tot + o];
+#pragma unroll
+  for (int d = 16; d > 0; d >>= 1) {
+    s.x += __shfl_xor_sync(0xffffffffu, s.x, d);
+    s.y += __shfl_xor_sync(0xffffffffu, s.y, d);
+  }
+  if (lane == 0) {
+    const int gn = (int)(o / m), gm = (int)(o - (size_t)gn * m);
+    T r = cmul(alpha, s);
+    if (beta.x != (R)0 || beta.y != (R)0) r = r + cmul(beta, C[(size_t)gn * ldc + gm]);
+    C[(size_t)gn * ldc + gm] = r;
+  }
+}
+
 }  // namespace
 
 template <typename R>
@@ -189,7 +215,11 @@ int zgemm(pspw_cell *c, char opa, int m, int n, int k, cx<R> alpha, const cx<R> 
   const bool conj = (opa == 'C' || opa == 'c');
   const int mt = (m + kGM - 1) / kGM, nt = (n + kGN - 1) / kGN;
   int nsplit = 1;
-  if (k > 4 * BK && mt * nt < 2 * 148) {
+  const bool narrow = n <= 8;
+  if (narrow && k > 4 * BK && mt < 8 * 148) {
+    // narrow products (Lanczos, single columns): short slices, many blocks
+    nsplit = std::max(1, std::min((k + 63) / 64, (8 * 148 + mt - 1) / mt));
+  } else if (k > 4 * BK && mt * nt < 2 * 148) {
     nsplit = std::min((k + 255) / 256, (2 * 148 + mt * nt - 1) / (mt * nt));
     nsplit = std::max(1, nsplit);
   }
@@ -222,8 +252,12 @@ int zgemm(pspw_cell *c, char opa, int m, int n, int k, cx<R> alpha, const cx<R> 
   }
   c->kernel_launches++;
   if (nsplit > 1) {
-    k_zgemm_reduce<R><<<std::min<size_t>(4 * 148, ((size_t)m * n + 255) / 256), 256, 0, st>>>(
-        m, n, nsplit, part, alpha, beta, C, ldc);
+    if (narrow)
+      k_zgemm_reduce_warp<R><<<(unsigned)(((size_t)m * n * 32 + 255) / 256), 256, 0, st>>>(
+          m, n, nsplit, part, alpha, beta, C, ldc);
+    else
+      k_zgemm_reduce<R><<<std::min<size_t>(4 * 148, ((size_t)m * n + 255) / 256), 256, 0, st>>>(
+          m, n, nsplit, part, alpha, beta, C, ldc);
     c->kernel_launches++;
   }
   timing_end(c, kFamGemm, ev);

@@ -437,9 +437,9 @@ __global__ void __launch_bounds__(256) k_backproj(ProjArg pa, const cx<R> *__res
 
 // Narrow tiles for blocks of at most 8 bands (the single vectors of Lanczos,
 // small batches): 64 rows x 8 bands per block, thread (r = t & 63,
-// c = t >> 6) owns row r and bands c and c + 4.  Every output accumulates the
-// same products in the same order as in the 64 x 64 kernels above, so the
-// results are identical; only the wasted columns are gone.
+// c = t >> 6) owns row r and bands c and c + 4.  Within a K slice every
+// output accumulates the same products in the same order as in the 64 x 64
+// kernels above; only the wasted columns are gone.
 constexpr int kNN = 8;
 
 template <typename R, int BK>
@@ -533,6 +533,35 @@ __global__ void __launch_bounds__(256) k_backproj_n8(ProjArg pa, const cx<R> *__
     }
     out[(size_t)bb * ldo + ig] = v;
   }
+}
+
+// The split-K reduction of the narrow projection: one warp per output,
+// lanes over the slices in a fixed order, then a fixed shuffle tree.
+template <typename R>
+__global__ void k_proj_reduce_warp(const cx<R> *__restrict__ part, const R *__restrict__ w,
+                                   int nsplit, int nb, int nproj, cx<R> *__restrict__ wp) {
+  const int o = (int)((blockIdx.x * (size_t)blockDim.x + threadIdx.x) >> 5);
+  const int lane = threadIdx.x & 31;
+  if (o >= nb * nproj) return;  // uniform per warp
+  cx<R> s = czero<cx<R>>();
+  for (int k = lane; k < nsplit; k += 32) s = s + part[(size_t)k * nb * nproj + o];
+#pragma unroll
+  for (int d = 16; d > 0; d >>= 1) {
+    s.x += __shfl_xor_sync(0xffffffffu, s.x, d);
+    s.y += __shfl_xor_sync(0xffffffffu, s.y, d);
+  }
+  if (lane == 0) {
+    const R wl = w ? w[o % nproj] : R(1);
+    wp[o] = mk<cx<R>>(wl * s.x, wl * s.y);
+  }
+}
+
+// split-K slices for the projection of nb bands over ngw plane waves: about
+// two waves of the GPU for full tiles; for narrow blocks (nb <= 8) slices of
+// 64 G so enough blocks are in flight to hide the latency of building beta
+inline int proj_split(int ngw, int nb, int mt, int nt) {
+  if (nb <= kNN) return std::max(1, std::min((ngw + 63) / 64, (8 * 148 + mt - 1) / mt));
+  return std::max(1, std::min((ngw + 255) / 256, (2 * 148 + mt * nt - 1) / (mt * nt)));
 }
 
 // out = a*out + bc*in + g*xm2 (no projectors)
@@ -681,10 +710,28 @@ int hpsi_apply(pspw_cell *c, const void *in_v, int ld_in, void *out_v, int ld_ou
   if constexpr (sizeof(R) == 4) use_tc = nproj > 0 && nl_tc_usable(c);
   float *tc_part = nullptr, *tc_wt = nullptr;
   int tc_split = 0;
+  // The projection reads psi only: it runs on the cell's second stream,
+  // concurrently with the local part, and the back-projection waits for it.
+  // (Callers with a scratch plan, i.e. the allocation-free entry point, keep
+  // one stream.)  c->stream is switched for the projection's launches and
+  // switched back on every exit from this block.
+  const cudaStream_t main_st = c->stream;
+  const bool overlap = nproj > 0 && !plan && c->stream2 != nullptr;
+  struct StreamSwitch {
+    pspw_cell *c;
+    cudaStream_t main;
+    ~StreamSwitch() { c->stream = main; }
+  };
   if (nproj > 0) {
+    StreamSwitch restore{c, main_st};
+    if (overlap) {
+      PSPW_CUDA(cudaEventRecord(c->ev_fork, main_st));
+      PSPW_CUDA(cudaStreamWaitEvent(c->stream2, c->ev_fork, 0));
+      c->stream = c->stream2;
+      st = c->stream2;
+    }
     const int mt = (nproj + kBM - 1) / kBM, nt = (nb + kBN - 1) / kBN;
-    // split G so the grid covers the GPU about twice
-    int nsplit = std::max(1, std::min((ngw + 255) / 256, (2 * 148 + mt * nt - 1) / (mt * nt)));
+    int nsplit = proj_split(ngw, nb, mt, nt);
     if (plan) nsplit = std::max(1, std::min(nsplit, plan->max_split));
     int kchunk = (ngw + nsplit - 1) / nsplit;
     kchunk = (kchunk + BK - 1) / BK * BK;
@@ -727,12 +774,18 @@ int hpsi_apply(pspw_cell *c, const void *in_v, int ld_in, void *out_v, int ld_ou
                                                               part);
       });
       run(kFamProj, [&] {
-        k_proj_reduce<R><<<(nb * nproj + 255) / 256, 256, 0, st>>>(part, Prec<R>::pw(c), nsplit,
-                                                                  nb, nproj, wp);
+        if (nb <= kNN)
+          k_proj_reduce_warp<R><<<(nb * nproj * 32 + 255) / 256, 256, 0, st>>>(
+              part, Prec<R>::pw(c), nsplit, nb, nproj, wp);
+        else
+          k_proj_reduce<R><<<(nb * nproj + 255) / 256, 256, 0, st>>>(part, Prec<R>::pw(c), nsplit,
+                                                                    nb, nproj, wp);
       });
     }
     timing_end(c, kFamNonlocal, ev);
     PSPW_CUDA(cudaGetLastError());
+    if (overlap) PSPW_CUDA(cudaEventRecord(c->ev_join, c->stream2));
+    st = main_st;
   }
 
   // ---- local part, in batches of bands
@@ -804,6 +857,7 @@ int hpsi_apply(pspw_cell *c, const void *in_v, int ld_in, void *out_v, int ld_ou
 
   // ---- back-projection + recurrence epilogue
   if (nproj > 0) {
+    if (overlap) PSPW_CUDA(cudaStreamWaitEvent(st, c->ev_join, 0));
     timing_begin(c, kFamNonlocal, &ev);
     if (use_tc) {
       cudaEvent_t e;
@@ -853,7 +907,7 @@ int project_fp64(pspw_cell *c, const double2 *psi, int ld, int ngw, int nb, doub
   pa.nproj = nproj;
   constexpr int BK = 16;
   const int mt = (nproj + kBM - 1) / kBM, nt = (nb + kBN - 1) / kBN;
-  int nsplit = std::max(1, std::min((ngw + 255) / 256, (2 * 148 + mt * nt - 1) / (mt * nt)));
+  int nsplit = proj_split(ngw, nb, mt, nt);
   int kchunk = (ngw + nsplit - 1) / nsplit;
   kchunk = (kchunk + BK - 1) / BK * BK;
   nsplit = (ngw + kchunk - 1) / kchunk;
@@ -866,8 +920,12 @@ int project_fp64(pspw_cell *c, const double2 *psi, int ld, int ngw, int nb, doub
   else
     k_proj<R, BK><<<dim3(mt, nt, nsplit), 256, 0, c->stream>>>(pa, psi, ld, ngw, nb, kchunk,
                                                                part);
-  k_proj_reduce<R><<<(nb * nproj + 255) / 256, 256, 0, c->stream>>>(part, nullptr, nsplit, nb,
-                                                                    nproj, P);
+  if (nb <= kNN)
+    k_proj_reduce_warp<R><<<(nb * nproj * 32 + 255) / 256, 256, 0, c->stream>>>(
+        part, nullptr, nsplit, nb, nproj, P);
+  else
+    k_proj_reduce<R><<<(nb * nproj + 255) / 256, 256, 0, c->stream>>>(part, nullptr, nsplit, nb,
+                                                                      nproj, P);
   c->kernel_launches += 2;
   PSPW_CUDA(cudaGetLastError());
   return PSPW_OK;
