@@ -484,14 +484,16 @@ int cell_create(pspw_cell **out, int device, int nr1, int nr2, int nr3, int ngw,
 namespace pspw {
 namespace {
 
-// V_eff/NNR gathered into the digit-permuted (z, y, x) order of the
-// register-FFT path.
+// V_eff/NNR gathered into the digit-permuted order of the register-FFT path,
+// each z-plane stored x-major (z, x, y): the plane kernel's fused x step
+// reads, for one x position, the rows of 32 consecutive y in one coalesced
+// load.
 __global__ void k_veff_perm(const double *__restrict__ v, int n1, int n2, int n3, double s,
                             const int *__restrict__ px, const int *__restrict__ py,
                             const int *__restrict__ pz, double *o64, float *o32) {
   const int n = n1 * n2 * n3;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-    const int a = i % n1, b = (i / n1) % n2, cz = i / (n1 * n2);
+    const int b = i % n2, a = (i / n2) % n1, cz = i / (n1 * n2);
     const double x = v[((size_t)pz[cz] * n2 + py[b]) * n1 + px[a]] * s;
     o64[i] = x;
     o32[i] = (float)x;

@@ -141,26 +141,19 @@ __device__ __forceinline__ void fwd_stepS(T *base, Lines L, int es, const T *w) 
 }
 
 // The fused middle of an x-line sandwich: inverse block step, multiply by
-// the (permuted) potential row, forward block step with its twiddles.
+// the (permuted) potential, forward block step with its twiddles.  The
+// potential plane is stored x-major (vplane[x * ny + y]), so for each of the
+// N1 positions of a block the lines (rows y, fastest across threads) of a
+// warp read consecutive values: one coalesced load per position.
 template <int N1, int N2, typename T, typename R>
 __device__ __forceinline__ void inv_fwd_stepB_v(T *base, Lines L, const T *w,
-                                                const R *__restrict__ vrows, int vld) {
+                                                const R *__restrict__ vplane, int ny) {
   for (int it = threadIdx.x; it < L.nl * N2; it += blockDim.x) {
     const int l = it % L.nl, k = it / L.nl;
     T *line = base + L(l);
-    const R *vr = vrows + (size_t)l * vld + N1 * k;
-    // the N1 potential values of the block, in 16-byte loads where the row
-    // segment allows (one sector per thread instead of N1 lookups)
-    alignas(16) R s[N1];
-    if constexpr ((N1 * sizeof(R)) % 16 == 0) {
-      constexpr int NV = N1 * sizeof(R) / 16;
-      const uint4 *vv = reinterpret_cast<const uint4 *>(vr);
+    R s[N1];
 #pragma unroll
-      for (int q = 0; q < NV; q++) reinterpret_cast<uint4 *>(s)[q] = __ldg(vv + q);
-    } else {
-#pragma unroll
-      for (int i = 0; i < N1; i++) s[i] = vr[i];
-    }
+    for (int i = 0; i < N1; i++) s[i] = __ldg(vplane + (size_t)(N1 * k + i) * ny + l);
     T v[N1];
 #pragma unroll
     for (int i = 0; i < N1; i++) v[i] = line[i + N1 * k];
@@ -267,23 +260,6 @@ __device__ __forceinline__ void line_step(int kind, int n, T *base, Lines L, int
     else if (kind == kInvB) inv_stepB<A, B>(base, L, es, w);             \
     else if (kind == kFwdB) fwd_stepB<A, B>(base, L, es, w);             \
     else fwd_stepS<A, B>(base, L, es, w);                                \
-    break;                                                               \
-  }
-    PSPW_FOR_EACH_SPLIT(PSPW_CASE)
-#undef PSPW_CASE
-    default:
-      break;
-  }
-}
-
-template <typename T, typename R>
-__device__ __forceinline__ void line_vsandwich(int n, T *base, Lines L, const T *w, const R *vrows,
-                                               int vld) {
-  switch (n) {
-#define PSPW_CASE(NN)                                                    \
-  case NN: {                                                             \
-    constexpr int A = nsplit_for(NN).n1, B = nsplit_for(NN).n2;          \
-    inv_fwd_stepB_v<A, B>(base, L, w, vrows, vld);                       \
     break;                                                               \
   }
     PSPW_FOR_EACH_SPLIT(PSPW_CASE)

@@ -11,7 +11,7 @@
 // Lengths are template parameters so every kernel holds only its own
 // unrolled register DFTs (fft2.cuh).  Along each axis the inverse transform
 // leaves the digit-permuted order of fft2.cuh; S holds z in that order and
-// V_eff is stored permuted in (z, y, x), so no reordering pass exists.
+// V_eff is stored permuted in (z, x, y), so no reordering pass exists.
 #pragma once
 
 #include <algorithm>
@@ -150,7 +150,7 @@ __global__ void __launch_bounds__(PlaneCfg<NX, NY>::NT) k_plane(FastGeo g, int n
   __syncthreads();
   x_inv_expand<NY, AX, BX, NT>(plane, la, LS, xa, wx);
   __syncthreads();
-  inv_fwd_stepB_v<AX, BX>(plane, rows, wx, vperm + (size_t)zp * NY * NX, NX);
+  inv_fwd_stepB_v<AX, BX>(plane, rows, wx, vperm + (size_t)zp * NY * NX, NY);
   __syncthreads();
   x_fwd_compact<NY, AX, BX, NT>(plane, la, LS, xa);
   __syncthreads();
