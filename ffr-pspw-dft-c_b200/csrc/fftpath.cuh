@@ -44,9 +44,24 @@ __global__ void __launch_bounds__(256) k_sticks_inv(FastGeo g, const T *__restri
   __syncthreads();
   const T *pb = psi + (size_t)band * ld;
   const int k0 = g.col_start[c0], k1 = g.col_start[c0 + nc];
-  for (int k = k0 + threadIdx.x; k < k1; k += blockDim.x) {
-    const int ig = g.sg_ig[k];
-    if (ig < ngw_call) tile[(g.sg_col[k] - c0) * LS + g.sg_z[k]] = pb[ig];
+  // the gather in groups of four elements per thread: all index loads, then
+  // all psi loads, then the shared-memory stores, so each thread has four
+  // independent chains in flight instead of one
+  constexpr int U = 4;
+  for (int kb = k0 + threadIdx.x; kb < k1; kb += U * 256) {
+    int ig[U], off[U];
+#pragma unroll
+    for (int u = 0; u < U; u++) {
+      const int k = kb + u * 256;
+      ig[u] = k < k1 ? g.sg_ig[k] : ngw_call;
+      off[u] = k < k1 ? (g.sg_col[k] - c0) * LS + g.sg_z[k] : 0;
+    }
+    T v[U];
+#pragma unroll
+    for (int u = 0; u < U; u++) v[u] = ig[u] < ngw_call ? pb[ig[u]] : czero<T>();
+#pragma unroll
+    for (int u = 0; u < U; u++)
+      if (ig[u] < ngw_call) tile[off[u]] = v[u];
   }
   __syncthreads();
   const Lines L{nullptr, LS, nc};
@@ -89,13 +104,30 @@ __global__ void __launch_bounds__(256) k_sticks_fwd(FastGeo g, const T *__restri
   const T *pb = psi + (size_t)band * ld;
   T *ob = out + (size_t)band * ldo;
   const int k0 = g.col_start[c0], k1 = g.col_start[c0 + nc];
-  for (int k = k0 + threadIdx.x; k < k1; k += blockDim.x) {
-    const int ig = g.sg_ig[k];
-    if (ig < ngw_call) {
-      const R kk = kin[ig];
-      const T p = pb[ig];
-      const T f = tile[(g.sg_col[k] - c0) * LS + g.sg_z[k]];
-      ob[ig] = mk<T>(kk * p.x + f.x, kk * p.y + f.y);
+  // four elements per thread in flight, as in the inverse gather
+  constexpr int U = 4;
+  for (int kb = k0 + threadIdx.x; kb < k1; kb += U * 256) {
+    int ig[U], off[U];
+#pragma unroll
+    for (int u = 0; u < U; u++) {
+      const int k = kb + u * 256;
+      ig[u] = k < k1 ? g.sg_ig[k] : ngw_call;
+      off[u] = k < k1 ? (g.sg_col[k] - c0) * LS + g.sg_z[k] : 0;
+    }
+    R kk[U];
+    T p[U];
+#pragma unroll
+    for (int u = 0; u < U; u++) {
+      const bool on = ig[u] < ngw_call;
+      kk[u] = on ? kin[ig[u]] : (R)0;
+      p[u] = on ? pb[ig[u]] : czero<T>();
+    }
+#pragma unroll
+    for (int u = 0; u < U; u++) {
+      if (ig[u] < ngw_call) {
+        const T f = tile[off[u]];
+        ob[ig[u]] = mk<T>(kk[u] * p[u].x + f.x, kk[u] * p[u].y + f.y);
+      }
     }
   }
 }
