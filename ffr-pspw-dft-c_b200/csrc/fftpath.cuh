@@ -91,9 +91,21 @@ __global__ void __launch_bounds__(256) k_sticks_fwd(FastGeo g, const T *__restri
   const int nc = min(T1, g.ncol - c0);
   for (int t = threadIdx.x; t < NZ; t += blockDim.x) wz[t] = wz_g[t];
   const T *Sb = S + (size_t)band * NZ * g.ncol;
-  for (int e = threadIdx.x; e < T1 * NZ; e += blockDim.x) {
-    const int p = e / T1, t = e - p * T1;
-    tile[t * LS + p] = (t < nc) ? Sb[(size_t)p * g.ncol + c0 + t] : czero<T>();
+  // the transposing read of the stick buffer, four loads per thread in
+  // flight before their shared-memory stores
+  constexpr int U = 4;
+  for (int eb = threadIdx.x; eb < T1 * NZ; eb += U * 256) {
+    T v[U];
+#pragma unroll
+    for (int u = 0; u < U; u++) {
+      const int e = eb + u * 256, p = e / T1, t = e - p * T1;
+      v[u] = (e < T1 * NZ && t < nc) ? Sb[(size_t)p * g.ncol + c0 + t] : czero<T>();
+    }
+#pragma unroll
+    for (int u = 0; u < U; u++) {
+      const int e = eb + u * 256, p = e / T1, t = e - p * T1;
+      if (e < T1 * NZ) tile[t * LS + p] = v[u];
+    }
   }
   __syncthreads();
   const Lines L{nullptr, LS, nc};
@@ -105,7 +117,6 @@ __global__ void __launch_bounds__(256) k_sticks_fwd(FastGeo g, const T *__restri
   T *ob = out + (size_t)band * ldo;
   const int k0 = g.col_start[c0], k1 = g.col_start[c0 + nc];
   // four elements per thread in flight, as in the inverse gather
-  constexpr int U = 4;
   for (int kb = k0 + threadIdx.x; kb < k1; kb += U * 256) {
     int ig[U], off[U];
 #pragma unroll
