@@ -214,7 +214,7 @@ int pspw_cell_destroy(pspw_cell *c) {
                   c->proj.d_pkga64, c->proj.d_pkga32, c->proj.d_patom, c->proj.d_psp,
                   c->proj.d_plm, c->proj.d_pw64, c->proj.d_pw32, c->d_veff64, c->d_veff32,
                   B.d_col_x, B.d_col_y, B.d_pinv[0], B.d_pinv[1], B.d_pinv[2], c->d_vperm64,
-                  c->d_vperm32, c->proj.d_etp, c->proj.d_etb, B.d_wgrid};
+                  c->d_vperm32, c->proj.d_etp, c->proj.d_etb, B.d_wgrid, c->proj.d_beta64};
   for (void *p : ptrs)
     if (p) cudaFree(p);
   for (int i = 0; i < 3; i++) {

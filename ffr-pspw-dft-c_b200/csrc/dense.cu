@@ -287,4 +287,6 @@ int dev_zhegv(pspw_cell *c, double2 *A, int lda, double2 *B, int ldb, double *ev
   return zgemm<double>(c, 'N', n, n, n, one, B, ldb, A, lda, zero, evec, lde);
 }
 
+int cublas_handle(pspw_cell *c, cublasHandle_t *h) { return blas_handle(c, h); }
+
 }  // namespace pspw

@@ -4,11 +4,15 @@
 // All FP64 complex, column-major, on the cell stream.
 #pragma once
 
+#include <cublas_v2.h>
+
 #include "common.cuh"
 #include "engine.h"
 
 namespace pspw {
 
+// the cell's cuBLAS handle, bound to the cell's current stream
+int cublas_handle(pspw_cell *c, cublasHandle_t *h);
 // A (n x n, lda) <- eigenvectors, w[n] (device) <- ascending eigenvalues;
 // upper triangle of A is read (zheevd 'V','U').  *info_out = LAPACK info.
 int dev_zheevd(pspw_cell *c, double2 *A, int lda, double *w, int n, int *info_out);

@@ -21,17 +21,22 @@
 // Nonlocal part (ApplyHam_block.cpp:68-165): with beta_p(G) =
 // EIGR(G,a_p)*PKG_A(lm_p,G), the reference adds beta W beta^H psi (zdotu
 // against conj(EIGR)*PKG_A, back-projection with EIGR*PKG_A).  Here that is
-// two complex GEMMs whose A operand is generated from EIGR and PKG_A while it
-// is loaded, never stored: projection (split over G, partial sums reduced in
-// a fixed order, so results are deterministic) and back-projection, whose
-// epilogue also applies out = a*(H psi) + b*psi + g*x, the update of the
-// Chebyshev three-term recurrence (chebyfilt.cpp:36-59).
+// two complex GEMMs.  FP32: on the tensor cores (nl_tc.cu) for one species,
+// otherwise SIMT kernels whose beta operand is generated from EIGR and PKG_A
+// while it is loaded, never stored: projection (split over G, partial sums
+// reduced in a fixed order, so results are deterministic) and
+// back-projection, whose epilogue also applies out = a*(H psi) + b*psi + g*x,
+// the update of the Chebyshev three-term recurrence (chebyfilt.cpp:36-59).
+// FP64: beta stored once per cell (NGW x nproj) and both products as cuBLAS
+// ZGEMMs, the recurrence as a separate pass; the allocation-free entry point
+// keeps the SIMT kernels.
 #include <cuda_runtime.h>
 
 #include <algorithm>
 #include <cstdio>
 
 #include "common.cuh"
+#include "dense.h"
 #include "engine.h"
 #include "fft.cuh"
 #include "fftpath.h"
@@ -625,6 +630,68 @@ int set_smem(K kernel, size_t bytes) {
 
 }  // namespace
 
+// ---------------------------------------------------------------- FP64 projectors
+// beta(G, p) = EIGR(G, atom_p) PKG_A(lm_p, G), column-major NGW x nproj
+__global__ void k_build_beta64(ProjArg pa, int nproj, double2 *beta) {
+  const long long n = (long long)nproj * pa.ngw_cell;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x) {
+    const int p = (int)(i / pa.ngw_cell), ig = (int)(i % pa.ngw_cell);
+    beta[i] = beta_at<double>(pa, ig, p);
+  }
+}
+
+// wp(p, b) = W_p P(p, b) (nproj x nb column-major)
+__global__ void k_scale_proj(const double2 *__restrict__ P, const double *__restrict__ w,
+                             int nproj, int nb, double2 *wp) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= nproj * nb) return;
+  const double wl = w[i % nproj];
+  wp[i] = make_double2(wl * P[i].x, wl * P[i].y);
+}
+
+int ensure_beta64(pspw_cell *c, const ProjArg &pa) {
+  if (c->proj.d_beta64) return PSPW_OK;
+  const size_t n = (size_t)c->proj.nproj * c->basis.ngw;
+  if (cudaMalloc(&c->proj.d_beta64, n * sizeof(double2)) != cudaSuccess)
+    return fail(PSPW_ERR_OOM, "FP64 projector matrix");
+  k_build_beta64<<<(unsigned)std::min<size_t>((n + 255) / 256, 148 * 16), 256, 0, c->stream>>>(
+      pa, c->proj.nproj, c->proj.d_beta64);
+  c->kernel_launches++;
+  PSPW_CUDA(cudaGetLastError());
+  return PSPW_OK;
+}
+
+// P (nproj x nb) = beta^H psi over the first ngw plane waves (cuBLAS ZGEMM)
+int project_beta64(pspw_cell *c, const double2 *psi, int ld, int ngw, int nb, double2 *P) {
+  cublasHandle_t h;
+  int rc = cublas_handle(c, &h);
+  if (rc) return rc;
+  const cuDoubleComplex one = make_cuDoubleComplex(1.0, 0.0), zero = make_cuDoubleComplex(0.0, 0.0);
+  if (cublasZgemm(h, CUBLAS_OP_C, CUBLAS_OP_N, c->proj.nproj, nb, ngw, &one,
+                  reinterpret_cast<const cuDoubleComplex *>(c->proj.d_beta64), c->basis.ngw,
+                  reinterpret_cast<const cuDoubleComplex *>(psi), ld, &zero,
+                  reinterpret_cast<cuDoubleComplex *>(P), c->proj.nproj) != CUBLAS_STATUS_SUCCESS)
+    return fail(PSPW_ERR_CUDA, "cublasZgemm (projection)");
+  c->kernel_launches++;
+  return PSPW_OK;
+}
+
+// out(:, b) += beta wp(:, b) over the first ngw plane waves (cuBLAS ZGEMM)
+int backproject_beta64(pspw_cell *c, const double2 *wp, int ngw, int nb, double2 *out, int ldo) {
+  cublasHandle_t h;
+  int rc = cublas_handle(c, &h);
+  if (rc) return rc;
+  const cuDoubleComplex one = make_cuDoubleComplex(1.0, 0.0);
+  if (cublasZgemm(h, CUBLAS_OP_N, CUBLAS_OP_N, ngw, nb, c->proj.nproj, &one,
+                  reinterpret_cast<const cuDoubleComplex *>(c->proj.d_beta64), c->basis.ngw,
+                  reinterpret_cast<const cuDoubleComplex *>(wp), c->proj.nproj, &one,
+                  reinterpret_cast<cuDoubleComplex *>(out), ldo) != CUBLAS_STATUS_SUCCESS)
+    return fail(PSPW_ERR_CUDA, "cublasZgemm (back-projection)");
+  c->kernel_launches++;
+  return PSPW_OK;
+}
+
 // rho += sum_b wband[b] |psi_b(r)|^2 for any grid the generic FFT handles;
 // psi scattered for ig < ngw_scatter (EvalRhoPsi.cpp:117).
 int rho_generic(pspw_cell *c, const double2 *psi, int ld, int ngw_scatter, int nb,
@@ -749,7 +816,27 @@ int hpsi_apply(pspw_cell *c, const void *in_v, int ld_in, void *out_v, int ld_ou
       }
     }
     timing_begin(c, kFamNonlocal, &ev);
-    if (use_tc) {
+    bool done = false;
+    if constexpr (sizeof(R) == 8) {
+      // FP64 without a scratch plan: beta materialised once, cuBLAS ZGEMMs
+      if (!plan) {
+        int rc = ensure_beta64(c, pa);
+        if (rc) return rc;
+        cudaEvent_t e;
+        timing_begin(c, kFamProj, &e);
+        rc = project_beta64(c, reinterpret_cast<const double2 *>(in), ld_in, ngw, nb,
+                            reinterpret_cast<double2 *>(part));
+        if (rc) return rc;
+        k_scale_proj<<<(nb * nproj + 255) / 256, 256, 0, st>>>(
+            reinterpret_cast<const double2 *>(part), c->proj.d_pw64, nproj, nb,
+            reinterpret_cast<double2 *>(wp));
+        c->kernel_launches++;
+        timing_end(c, kFamProj, e);
+        done = true;
+      }
+    }
+    if (done) {
+    } else if (use_tc) {
       if (plan) {
         tc_part = static_cast<float *>(plan->part);
         tc_wt = static_cast<float *>(plan->wt);
@@ -870,7 +957,24 @@ int hpsi_apply(pspw_cell *c, const void *in_v, int ld_in, void *out_v, int ld_ou
       if (rc) return rc;
     } else {
       dim3 grid((ngw + kBM - 1) / kBM, (nb + kBN - 1) / kBN);
-      run(kFamBackproj, [&] {
+      bool done = false;
+      if constexpr (sizeof(R) == 8) {
+        if (!plan) {
+          cudaEvent_t e;
+          timing_begin(c, kFamBackproj, &e);
+          int rc = backproject_beta64(c, reinterpret_cast<const double2 *>(wp), ngw, nb,
+                                      reinterpret_cast<double2 *>(out), ld_out);
+          if (rc) return rc;
+          if (a != 1.0 || b != 0.0 || g != 0.0) {
+            k_axpby3<R><<<4 * 148, 256, 0, st>>>(ngw, nb, out, ld_out, in, ld_in, xm2, ld_xm2,
+                                                (R)a, (R)b, (R)g);
+            c->kernel_launches++;
+          }
+          timing_end(c, kFamBackproj, e);
+          done = true;
+        }
+      }
+      if (!done) run(kFamBackproj, [&] {
         if (nb <= kNN)
           k_backproj_n8<R, BK><<<grid.x, 256, 0, st>>>(pa, wp, ngw, nb, out, ld_out, in, ld_in,
                                                        xm2, ld_xm2, (R)a, (R)b, (R)g);
@@ -905,28 +1009,10 @@ int project_fp64(pspw_cell *c, const double2 *psi, int ld, int ngw, int nb, doub
   pa.pw = Prec<R>::pw(c);
   pa.ngw_cell = c->basis.ngw;
   pa.nproj = nproj;
-  constexpr int BK = 16;
-  const int mt = (nproj + kBM - 1) / kBM, nt = (nb + kBN - 1) / kBN;
-  int nsplit = proj_split(ngw, nb, mt, nt);
-  int kchunk = (ngw + nsplit - 1) / nsplit;
-  kchunk = (kchunk + BK - 1) / BK * BK;
-  nsplit = (ngw + kchunk - 1) / kchunk;
-  cx<R> *part = nullptr;
-  int rc = ws_reserve(c, kWsProjPart, sizeof(cx<R>) * (size_t)nsplit * nb * nproj, (void **)&part);
+  int rc = ensure_beta64(c, pa);
   if (rc) return rc;
-  if (nb <= kNN)
-    k_proj_n8<R, BK><<<dim3(mt, 1, nsplit), 256, 0, c->stream>>>(pa, psi, ld, ngw, nb, kchunk,
-                                                                 part);
-  else
-    k_proj<R, BK><<<dim3(mt, nt, nsplit), 256, 0, c->stream>>>(pa, psi, ld, ngw, nb, kchunk,
-                                                               part);
-  if (nb <= kNN)
-    k_proj_reduce_warp<R><<<(nb * nproj * 32 + 255) / 256, 256, 0, c->stream>>>(
-        part, nullptr, nsplit, nb, nproj, P);
-  else
-    k_proj_reduce<R><<<(nb * nproj + 255) / 256, 256, 0, c->stream>>>(part, nullptr, nsplit, nb,
-                                                                      nproj, P);
-  c->kernel_launches += 2;
+  // beta materialised: one cuBLAS ZGEMM (projections without the weights)
+  if ((rc = project_beta64(c, psi, ld, ngw, nb, P))) return rc;
   PSPW_CUDA(cudaGetLastError());
   return PSPW_OK;
 }
