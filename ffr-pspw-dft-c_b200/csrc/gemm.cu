@@ -1,7 +1,8 @@
 // Complex GEMM for the subspace steps of the eigensolvers (zgemm_ calls of
 // davidson_cpu.cpp, lobpcg_cpu.cpp, eig_zhegv.cpp, ChebySCFLoop.cpp):
 //   C = alpha * op(A) * B + beta * C,  op(A) = A or A^H,
-// column-major with leading dimensions, FP64 or FP32 complex.
+// column-major with leading dimensions, FP64 or FP32 complex.  FP64 goes to
+// cuBLAS ZGEMM (a plain library GEMM); FP32 uses the kernels below.
 //
 // Tiles of 64 x 64 outputs, 256 threads, 4 x 4 outputs per thread, the K loop
 // staged through shared memory.  When K is long and the output small (the
@@ -12,6 +13,7 @@
 #include <algorithm>
 
 #include "common.cuh"
+#include "dense.h"
 #include "engine.h"
 #include "gemm.h"
 
@@ -210,6 +212,27 @@ int zgemm(pspw_cell *c, char opa, int m, int n, int k, cx<R> alpha, const cx<R> 
           const cx<R> *B, int ldb, cx<R> beta, cx<R> *C, int ldc) {
   using T = cx<R>;
   if (m <= 0 || n <= 0) return PSPW_OK;
+  if constexpr (sizeof(R) == 8) {
+    // FP64: a plain library GEMM on the FP64 pipe (cuBLAS ZGEMM, deterministic)
+    if (k > 0) {
+      cublasHandle_t h;
+      int rc = cublas_handle(c, &h);
+      if (rc) return rc;
+      cudaEvent_t ev;
+      timing_begin(c, kFamGemm, &ev);
+      const cublasOperation_t ta = (opa == 'C' || opa == 'c') ? CUBLAS_OP_C : CUBLAS_OP_N;
+      if (cublasZgemm(h, ta, CUBLAS_OP_N, m, n, k,
+                      reinterpret_cast<const cuDoubleComplex *>(&alpha),
+                      reinterpret_cast<const cuDoubleComplex *>(A), lda,
+                      reinterpret_cast<const cuDoubleComplex *>(B), ldb,
+                      reinterpret_cast<const cuDoubleComplex *>(&beta),
+                      reinterpret_cast<cuDoubleComplex *>(C), ldc) != CUBLAS_STATUS_SUCCESS)
+        return fail(PSPW_ERR_CUDA, "cublasZgemm");
+      timing_end(c, kFamGemm, ev);
+      c->kernel_launches++;
+      return PSPW_OK;
+    }
+  }
   cudaStream_t st = c->stream;
   constexpr int BK = sizeof(R) == 8 ? 16 : 32;
   const bool conj = (opa == 'C' || opa == 'c');
