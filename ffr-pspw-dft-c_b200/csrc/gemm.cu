@@ -1,8 +1,9 @@
 // Complex GEMM for the subspace steps of the eigensolvers (zgemm_ calls of
 // davidson_cpu.cpp, lobpcg_cpu.cpp, eig_zhegv.cpp, ChebySCFLoop.cpp):
 //   C = alpha * op(A) * B + beta * C,  op(A) = A or A^H,
-// column-major with leading dimensions, FP64 or FP32 complex.  FP64 goes to
-// cuBLAS ZGEMM (a plain library GEMM); FP32 uses the kernels below.
+// column-major with leading dimensions, FP64 or FP32 complex.  FP64 products
+// with more than 8 columns go to cuBLAS ZGEMM (a plain library GEMM); the
+// rest use the kernels below.
 //
 // Tiles of 64 x 64 outputs, 256 threads, 4 x 4 outputs per thread, the K loop
 // staged through shared memory.  When K is long and the output small (the
@@ -213,8 +214,10 @@ int zgemm(pspw_cell *c, char opa, int m, int n, int k, cx<R> alpha, const cx<R> 
   using T = cx<R>;
   if (m <= 0 || n <= 0) return PSPW_OK;
   if constexpr (sizeof(R) == 8) {
-    // FP64: a plain library GEMM on the FP64 pipe (cuBLAS ZGEMM, deterministic)
-    if (k > 0) {
+    // FP64 with more than 8 columns: a plain library GEMM on the FP64 pipe
+    // (cuBLAS ZGEMM, deterministic); narrow products (the Lanczos vectors)
+    // stay on the split-K kernels below, which are faster at that shape
+    if (k > 0 && n > 8) {
       cublasHandle_t h;
       int rc = cublas_handle(c, &h);
       if (rc) return rc;

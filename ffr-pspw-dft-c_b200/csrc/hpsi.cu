@@ -668,6 +668,15 @@ int project_beta64(pspw_cell *c, const double2 *psi, int ld, int ngw, int nb, do
   int rc = cublas_handle(c, &h);
   if (rc) return rc;
   const cuDoubleComplex one = make_cuDoubleComplex(1.0, 0.0), zero = make_cuDoubleComplex(0.0, 0.0);
+  if (nb == 1) {  // a single vector (Lanczos): the matrix-vector form
+    if (cublasZgemv(h, CUBLAS_OP_C, ngw, c->proj.nproj, &one,
+                    reinterpret_cast<const cuDoubleComplex *>(c->proj.d_beta64), c->basis.ngw,
+                    reinterpret_cast<const cuDoubleComplex *>(psi), 1, &zero,
+                    reinterpret_cast<cuDoubleComplex *>(P), 1) != CUBLAS_STATUS_SUCCESS)
+      return fail(PSPW_ERR_CUDA, "cublasZgemv (projection)");
+    c->kernel_launches++;
+    return PSPW_OK;
+  }
   if (cublasZgemm(h, CUBLAS_OP_C, CUBLAS_OP_N, c->proj.nproj, nb, ngw, &one,
                   reinterpret_cast<const cuDoubleComplex *>(c->proj.d_beta64), c->basis.ngw,
                   reinterpret_cast<const cuDoubleComplex *>(psi), ld, &zero,
@@ -683,6 +692,15 @@ int backproject_beta64(pspw_cell *c, const double2 *wp, int ngw, int nb, double2
   int rc = cublas_handle(c, &h);
   if (rc) return rc;
   const cuDoubleComplex one = make_cuDoubleComplex(1.0, 0.0);
+  if (nb == 1) {
+    if (cublasZgemv(h, CUBLAS_OP_N, ngw, c->proj.nproj, &one,
+                    reinterpret_cast<const cuDoubleComplex *>(c->proj.d_beta64), c->basis.ngw,
+                    reinterpret_cast<const cuDoubleComplex *>(wp), 1, &one,
+                    reinterpret_cast<cuDoubleComplex *>(out), 1) != CUBLAS_STATUS_SUCCESS)
+      return fail(PSPW_ERR_CUDA, "cublasZgemv (back-projection)");
+    c->kernel_launches++;
+    return PSPW_OK;
+  }
   if (cublasZgemm(h, CUBLAS_OP_N, CUBLAS_OP_N, ngw, nb, c->proj.nproj, &one,
                   reinterpret_cast<const cuDoubleComplex *>(c->proj.d_beta64), c->basis.ngw,
                   reinterpret_cast<const cuDoubleComplex *>(wp), c->proj.nproj, &one,
