@@ -431,7 +431,13 @@ int local_fast(pspw_cell *c, const FastGeo &g, const cx<R> *in, int ld_in, cx<R>
   cudaStream_t st = c->stream;
   const size_t s_band = (size_t)B.n3 * B.ncol;
   int nbatch = c->band_batch;
-  if (nbatch <= 0) nbatch = (int)std::max<size_t>(1, (48u << 20) / (s_band * sizeof(T)));
+  if (nbatch <= 0) {
+    // at most ~48 MB of stick buffer per batch (it stays in L2), batches of
+    // equal size so no launch runs with a small tail batch
+    const int cap = (int)std::max<size_t>(1, (48u << 20) / (s_band * sizeof(T)));
+    const int nbatches = (nb + cap - 1) / cap;
+    nbatch = (nb + nbatches - 1) / nbatches;
+  }
   if (plan) nbatch = plan->nbatch;
   nbatch = std::min(nbatch, nb);
   T *S = nullptr;
