@@ -45,6 +45,28 @@ int check_cell(pspw_cell *c) {
   return PSPW_OK;
 }
 
+// X (ld) <-> Xs (ld ngw) between the caller's G order and the stick order
+template <typename T>
+__global__ void k_to_stick_order(const T *__restrict__ X, int ld, T *Xs, int ngw, int nb,
+                                 const int *__restrict__ sg_ig) {
+  const long long n = (long long)ngw * nb;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x) {
+    const int b = (int)(i / ngw), k = (int)(i % ngw);
+    Xs[i] = X[(size_t)b * ld + sg_ig[k]];
+  }
+}
+template <typename T>
+__global__ void k_from_stick_order(const T *__restrict__ Xs, int ldxs, T *X, int ld, int ngw,
+                                   int nb, const int *__restrict__ sg_ig) {
+  const long long n = (long long)ngw * nb;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x) {
+    const int b = (int)(i / ngw), k = (int)(i % ngw);
+    X[(size_t)b * ld + sg_ig[k]] = Xs[(size_t)b * ldxs + k];
+  }
+}
+
 // The Chebyshev filter of chebyfilt.cpp:6-74 on a device block X (in place).
 // Y_1 = (sigma1/e)(H X - c X); Y_d = (2 sigma_d/e)(H Y_{d-1} - c Y_{d-1})
 // - sigma sigma_d Y_{d-2}; the three blocks rotate instead of being copied.
@@ -64,6 +86,33 @@ int chebyfilt_dev(pspw_cell *c, void *Xv, int ld, int ngw, int nb, int degree, d
   if (rc) return rc;
   rc = ws_reserve(c, 7, blk, (void **)&w2);
   if (rc) return rc;
+  // On the register-FFT path with the whole sphere the filter runs in the
+  // stick order: the block is permuted once into it, every H*psi runs with
+  // the cell's stick-order arrays swapped in (contiguous stick gathers and
+  // scatters), and the result is permuted back.  The recurrence is the same
+  // arithmetic on the same numbers in another order of G.
+  const bool stick = c->basis.fast && ngw == c->basis.ngw;
+  T *X0 = X;
+  int ld0 = ld;
+  if (stick) {
+    T *xs = nullptr;
+    if ((rc = ws_reserve(c, kWsStickX, blk, (void **)&xs))) return rc;
+    const long long n = (long long)ngw * nb;
+    k_to_stick_order<T><<<(unsigned)std::min<long long>((n + 255) / 256, 148 * 16), 256, 0,
+                          c->stream>>>(X, ld, xs, ngw, nb, c->basis.d_sg_ig);
+    c->kernel_launches++;
+    PSPW_CUDA(cudaGetLastError());
+    if ((rc = swap_stick_order(c))) return rc;
+    X = xs;
+    ld = ngw;
+  }
+  struct SwapBack {
+    pspw_cell *c;
+    bool on;
+    ~SwapBack() {
+      if (on) swap_stick_order(c);
+    }
+  } back{c, stick};
   // buffers: X (ld), w1, w2 (ld = ngw)
   T *buf[3] = {X, w1, w2};
   int lds[3] = {ld, ngw, ngw};
@@ -81,6 +130,16 @@ int chebyfilt_dev(pspw_cell *c, void *Xv, int ld, int ngw, int nb, int degree, d
     im2 = im1;
     im1 = io;
     sigma = sigma2;
+  }
+  if (stick) {
+    back.on = false;
+    if ((rc = swap_stick_order(c))) return rc;  // the cell's own order again
+    const long long n = (long long)ngw * nb;
+    k_from_stick_order<T><<<(unsigned)std::min<long long>((n + 255) / 256, 148 * 16), 256, 0,
+                            c->stream>>>(buf[im1], lds[im1], X0, ld0, ngw, nb, c->basis.d_sg_ig);
+    c->kernel_launches++;
+    PSPW_CUDA(cudaGetLastError());
+    return PSPW_OK;
   }
   if (im1 != 0) return copy_block<T>(c, buf[im1], lds[im1], X, ld, ngw, nb);
   return PSPW_OK;

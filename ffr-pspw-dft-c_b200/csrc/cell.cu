@@ -11,6 +11,7 @@
 #include <cstring>
 #include <map>
 #include <string>
+#include <utility>
 #include <vector>
 
 #include "common.cuh"
@@ -214,7 +215,10 @@ int pspw_cell_destroy(pspw_cell *c) {
                   c->proj.d_pkga64, c->proj.d_pkga32, c->proj.d_patom, c->proj.d_psp,
                   c->proj.d_plm, c->proj.d_pw64, c->proj.d_pw32, c->d_veff64, c->d_veff32,
                   B.d_col_x, B.d_col_y, B.d_pinv[0], B.d_pinv[1], B.d_pinv[2], c->d_vperm64,
-                  c->d_vperm32, c->proj.d_etp, c->proj.d_etb, B.d_wgrid, c->proj.d_beta64};
+                  c->d_vperm32, c->proj.d_etp, c->proj.d_etb, B.d_wgrid, c->proj.d_beta64,
+                  c->stick.sg_ig, c->stick.kin64, c->stick.kin32, c->stick.eigr64,
+                  c->stick.eigr32, c->stick.pkga64, c->stick.pkga32, c->stick.etp,
+                  c->stick.etb, c->stick.beta64};
   for (void *p : ptrs)
     if (p) cudaFree(p);
   for (int i = 0; i < 3; i++) {
@@ -476,6 +480,72 @@ int cell_create(pspw_cell **out, int device, int nr1, int nr2, int nr3, int ngw,
   *c->h_err = 0;
   if ((rc = pspw::nl_tc_prepare(c))) return bail(rc);
   *out = c;
+  return PSPW_OK;
+}
+
+namespace {
+
+// out[(r * ngw + k) * inner + q] = in[(r * ngw + sg_ig[k]) * inner + q]
+template <typename T>
+__global__ void k_gather_stick_order(const T *__restrict__ in, int rows, int ngw, int inner,
+                                     const int *__restrict__ sg_ig, T *out) {
+  const long long n = (long long)rows * ngw * inner;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x) {
+    const int q = (int)(i % inner), k = (int)((i / inner) % ngw), r = (int)(i / ((long long)inner * ngw));
+    out[i] = in[((size_t)r * ngw + sg_ig[k]) * inner + q];
+  }
+}
+
+__global__ void k_iota(int *a, int n) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) a[i] = i;
+}
+
+template <typename T>
+int gather_copy(pspw_cell *c, const T *in, int rows, int inner, T **out) {
+  if (!in || rows <= 0) return PSPW_OK;
+  const int ngw = c->basis.ngw;
+  const size_t n = (size_t)rows * ngw * inner;
+  if (cudaMalloc(out, n * sizeof(T)) != cudaSuccess) return fail(PSPW_ERR_OOM, "stick-order copies");
+  k_gather_stick_order<T><<<(unsigned)std::min<size_t>((n + 255) / 256, 148 * 16), 256, 0,
+                            c->stream>>>(in, rows, ngw, inner, c->basis.d_sg_ig, *out);
+  c->kernel_launches++;
+  PSPW_CUDA(cudaGetLastError());
+  return PSPW_OK;
+}
+
+}  // namespace
+
+int swap_stick_order(pspw_cell *c) {
+  Basis &B = c->basis;
+  Projectors &P = c->proj;
+  auto &S = c->stick;
+  if (!S.built) {
+    int rc;
+    if (cudaMalloc(&S.sg_ig, sizeof(int) * (size_t)B.ngw) != cudaSuccess)
+      return fail(PSPW_ERR_OOM, "stick-order copies");
+    k_iota<<<(B.ngw + 255) / 256, 256, 0, c->stream>>>(S.sg_ig, B.ngw);
+    c->kernel_launches++;
+    if ((rc = gather_copy(c, B.d_kin64, 1, 1, &S.kin64)) ||
+        (rc = gather_copy(c, B.d_kin32, 1, 1, &S.kin32)) ||
+        (rc = gather_copy(c, P.d_eigr64, P.nproj > 0 ? P.nat : 0, 1, &S.eigr64)) ||
+        (rc = gather_copy(c, P.d_eigr32, P.nproj > 0 ? P.nat : 0, 1, &S.eigr32)) ||
+        (rc = gather_copy(c, P.d_pkga64, P.nproj > 0 ? P.nsp : 0, 4, &S.pkga64)) ||
+        (rc = gather_copy(c, P.d_pkga32, P.nproj > 0 ? P.nsp : 0, 4, &S.pkga32)))
+      return rc;
+    if (P.d_etp && S.eigr32 && (rc = nl_tc_build_tiles(c, S.eigr32, &S.etp, &S.etb))) return rc;
+    S.built = true;
+  }
+  std::swap(B.d_sg_ig, S.sg_ig);
+  std::swap(B.d_kin64, S.kin64);
+  std::swap(B.d_kin32, S.kin32);
+  std::swap(P.d_eigr64, S.eigr64);
+  std::swap(P.d_eigr32, S.eigr32);
+  std::swap(P.d_pkga64, S.pkga64);
+  std::swap(P.d_pkga32, S.pkga32);
+  std::swap(P.d_etp, S.etp);
+  std::swap(P.d_etb, S.etb);
+  std::swap(P.d_beta64, S.beta64);
   return PSPW_OK;
 }
 

@@ -126,7 +126,8 @@ enum WsSlot {
   kWsEnl = 33,         // EvalENL projections
   kWsScfA = 34,        // SCF-piece host entry points: vectors on the device
   kWsScfB = 35,
-  kWsCount = 36
+  kWsStickX = 36,      // the filter's block in stick order
+  kWsCount = 37
 };
 
 struct Timing {
@@ -169,6 +170,24 @@ struct pspw_cell {
   void *cublas = nullptr;    // cublasHandle_t, created on first use
   pspw::Timing timing;
   long long kernel_launches = 0;  // kernels this cell has enqueued
+  // Stick-order copies of the per-G arrays, for the Chebyshev filter: the
+  // filter permutes its block into the order of the stick lists once, runs
+  // all its H*psi with these arrays swapped in (the stick gathers and
+  // scatters then read and write contiguous runs), and permutes back.
+  // Built on the first filter call; swap_stick_order() exchanges them with
+  // the cell's own (a second call swaps back).
+  struct {
+    bool built = false;
+    int *sg_ig = nullptr;  // identity: G k of the stick list is G k
+    double *kin64 = nullptr;
+    float *kin32 = nullptr;
+    double2 *eigr64 = nullptr;
+    float2 *eigr32 = nullptr;
+    double *pkga64 = nullptr;
+    float *pkga32 = nullptr;
+    float *etp = nullptr, *etb = nullptr;
+    double2 *beta64 = nullptr;
+  } stick;
   // Error word the kernels raise when a bounded wait gives up (pinned,
   // mapped host memory: d_err is its device alias).  Read after every
   // stream synchronisation by device_status().
@@ -188,6 +207,9 @@ int cell_create(pspw_cell **out, int device, int nr1, int nr2, int nr3, int ngw,
                 int nax, const int *lm_end, int nlmax, const double *eigr, const double *pkg_a,
                 const double *wnl, const double2 *d_eigr, const double *d_pkg_a);
 int cuda_fail(cudaError_t e, const char *what);
+// build the stick-order copies (once) and exchange them with the cell's
+// per-G arrays; calling it again restores the cell
+int swap_stick_order(pspw_cell *c);
 #define PSPW_CUDA(call)                                   \
   do {                                                    \
     cudaError_t _e = (call);                              \

@@ -652,26 +652,32 @@ bool nl_tc_usable(const pspw_cell *c) {
   return fits(c->proj) && c->proj.d_etp && c->proj.d_etb && c->d_err;
 }
 
-int nl_tc_prepare(pspw_cell *c) {
+int nl_tc_build_tiles(pspw_cell *c, const float2 *eigr32, float **etp, float **etb) {
   Projectors &P = c->proj;
-  if (!fits(P) || P.d_etp) return PSPW_OK;
+  if (!fits(P)) return PSPW_OK;
   const int ngw = c->basis.ngw;
   const int npad = (P.nat + 15) / 16 * 16, nsa = (P.nat + 7) / 8;
   // projection tiles: every 8 G of the sphere, rounded up to whole steps of
   // kStepG G (the tail tiles hold zeros)
   const int nst = (ngw + kStepG - 1) / kStepG * (kStepG / 8), ngt = (ngw + 127) / 128;
   const size_t bp = (size_t)nst * npad * 128, bb = (size_t)ngt * nsa * 16384;
-  if (cudaMalloc(&P.d_etp, bp) != cudaSuccess || cudaMalloc(&P.d_etb, bb) != cudaSuccess)
-    return fail(PSPW_ERR_OOM, "cell_create: EIGR operand tiles");
+  if (cudaMalloc(etp, bp) != cudaSuccess || cudaMalloc(etb, bb) != cudaSuccess)
+    return fail(PSPW_ERR_OOM, "EIGR operand tiles");
   P.tc_npad = npad;
   const long long n1 = (long long)nst * npad * 4, n2 = (long long)ngt * nsa * 512;
-  k_build_etp<<<(unsigned)((n1 + 255) / 256), 256, 0, c->stream>>>(P.d_eigr32, ngw, P.nat, npad,
-                                                                   nst, P.d_etp);
-  k_build_etb<<<(unsigned)((n2 + 255) / 256), 256, 0, c->stream>>>(P.d_eigr32, ngw, P.nat, nsa,
-                                                                   ngt, P.d_etb);
+  k_build_etp<<<(unsigned)((n1 + 255) / 256), 256, 0, c->stream>>>(eigr32, ngw, P.nat, npad, nst,
+                                                                   *etp);
+  k_build_etb<<<(unsigned)((n2 + 255) / 256), 256, 0, c->stream>>>(eigr32, ngw, P.nat, nsa, ngt,
+                                                                   *etb);
   c->kernel_launches += 2;
   PSPW_CUDA(cudaGetLastError());
   return PSPW_OK;
+}
+
+int nl_tc_prepare(pspw_cell *c) {
+  Projectors &P = c->proj;
+  if (!fits(P) || P.d_etp) return PSPW_OK;
+  return nl_tc_build_tiles(c, P.d_eigr32, &P.d_etp, &P.d_etb);
 }
 
 size_t nl_tc_wtile_bytes(const pspw_cell *c, int nb) {

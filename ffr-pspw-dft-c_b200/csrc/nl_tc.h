@@ -12,6 +12,8 @@ bool nl_tc_usable(const pspw_cell *c);
 // Builds the EIGR operand tiles of a cell whose projectors fit the kernels
 // (no-op otherwise).  Called once at cell creation.
 int nl_tc_prepare(pspw_cell *c);
+// The same tiles from a given EIGR copy (FP32, [nat][ngw]) into new buffers.
+int nl_tc_build_tiles(pspw_cell *c, const float2 *eigr32, float **etp, float **etb);
 
 // Bytes of the projection operand tiles for nb bands.
 size_t nl_tc_wtile_bytes(const pspw_cell *c, int nb);
