@@ -76,12 +76,17 @@ __global__ void __launch_bounds__(256) k_sticks_inv(FastGeo g, const T *__restri
   }
 }
 
+// out = kin psi + FFT part; with rec, out = ca (kin psi + FFT part) + cb psi
+// + cg x (the Chebyshev recurrence, whose projector term ca W beta^H psi the
+// back-projection then adds)
 template <int NZ, typename T, typename R>
 __global__ void __launch_bounds__(256) k_sticks_fwd(FastGeo g, const T *__restrict__ wz_g,
                                                     const T *__restrict__ S,
                                                     const R *__restrict__ kin,
                                                     const T *__restrict__ psi, int ld,
-                                                    T *__restrict__ out, int ldo, int ngw_call) {
+                                                    T *__restrict__ out, int ldo, int ngw_call,
+                                                    bool rec, R ca, R cb, R cg,
+                                                    const T *__restrict__ xm2, int ldx) {
   constexpr int T1 = StickCfg<NZ>::T1, LS = StickCfg<NZ>::LS;
   constexpr int A = nsplit_for(NZ).n1, B = nsplit_for(NZ).n2;
   __shared__ T tile[T1 * LS];
@@ -115,6 +120,7 @@ __global__ void __launch_bounds__(256) k_sticks_fwd(FastGeo g, const T *__restri
   __syncthreads();
   const T *pb = psi + (size_t)band * ld;
   T *ob = out + (size_t)band * ldo;
+  const T *xb = (rec && cg != (R)0) ? xm2 + (size_t)band * ldx : nullptr;
   const int k0 = g.col_start[c0], k1 = g.col_start[c0 + nc];
   // four elements per thread in flight, as in the inverse gather
   for (int kb = k0 + threadIdx.x; kb < k1; kb += U * 256) {
@@ -137,7 +143,16 @@ __global__ void __launch_bounds__(256) k_sticks_fwd(FastGeo g, const T *__restri
     for (int u = 0; u < U; u++) {
       if (ig[u] < ngw_call) {
         const T f = tile[off[u]];
-        ob[ig[u]] = mk<T>(kk[u] * p[u].x + f.x, kk[u] * p[u].y + f.y);
+        T v = mk<T>(kk[u] * p[u].x + f.x, kk[u] * p[u].y + f.y);
+        if (rec) {
+          v = mk<T>(ca * v.x + cb * p[u].x, ca * v.y + cb * p[u].y);
+          if (xb) {
+            const T x = xb[ig[u]];
+            v.x += cg * x.x;
+            v.y += cg * x.y;
+          }
+        }
+        ob[ig[u]] = v;
       }
     }
   }
@@ -273,10 +288,11 @@ int launch_sticks_inv(const FastGeo &g, cudaStream_t st, int nbb, const T *wz, c
 
 template <int NZ, typename T, typename R>
 int launch_sticks_fwd(const FastGeo &g, cudaStream_t st, int nbb, const T *wz, const T *S,
-                      const R *kin, const T *in, int ld, T *out, int ldo, int ngw) {
+                      const R *kin, const T *in, int ld, T *out, int ldo, int ngw,
+                      const RecArg<T, R> &ra) {
   constexpr int T1 = StickCfg<NZ>::T1;
-  k_sticks_fwd<NZ, T, R><<<dim3((g.ncol + T1 - 1) / T1, nbb), 256, 0, st>>>(g, wz, S, kin, in, ld,
-                                                                           out, ldo, ngw);
+  k_sticks_fwd<NZ, T, R><<<dim3((g.ncol + T1 - 1) / T1, nbb), 256, 0, st>>>(
+      g, wz, S, kin, in, ld, out, ldo, ngw, ra.on, ra.ca, ra.cb, ra.cg, ra.xm2, ra.ldx);
   return PSPW_OK;
 }
 
@@ -306,10 +322,11 @@ int dispatch_sticks_inv(int n3, const FastGeo &g, cudaStream_t st, int nbb, cons
 
 template <typename T, typename R>
 int dispatch_sticks_fwd(int n3, const FastGeo &g, cudaStream_t st, int nbb, const T *wz,
-                        const T *S, const R *kin, const T *in, int ld, T *out, int ldo, int ngw) {
+                        const T *S, const R *kin, const T *in, int ld, T *out, int ldo, int ngw,
+                        const RecArg<T, R> &ra) {
   switch (n3) {
 #define PSPW_CASE(NN) \
-  case NN: return launch_sticks_fwd<NN, T, R>(g, st, nbb, wz, S, kin, in, ld, out, ldo, ngw);
+  case NN: return launch_sticks_fwd<NN, T, R>(g, st, nbb, wz, S, kin, in, ld, out, ldo, ngw, ra);
     PSPW_FOR_EACH_SPLIT(PSPW_CASE)
 #undef PSPW_CASE
     default: return -1;
@@ -424,7 +441,7 @@ int rho_fast(pspw_cell *c, const FastGeo &g, const cx<R> *psi, int ld, int ngw_s
 
 template <typename R>
 int local_fast(pspw_cell *c, const FastGeo &g, const cx<R> *in, int ld_in, cx<R> *out,
-               int ld_out, int ngw, int nb, const ScratchPlan *plan) {
+               int ld_out, int ngw, int nb, const ScratchPlan *plan, const RecArg<cx<R>, R> &ra) {
   using namespace fastpath;
   using T = cx<R>;
   const Basis &B = c->basis;
@@ -466,8 +483,10 @@ int local_fast(pspw_cell *c, const FastGeo &g, const cx<R> *in, int ld_in, cx<R>
     c->kernel_launches++;
     if (rc) return rc < 0 ? fail(PSPW_ERR_NOT_IMPL, "register-FFT path: plane not compiled") : rc;
     timing_begin(c, kFamSticksFwd, &e2);
+    RecArg<T, R> rab = ra;
+    if (rab.xm2) rab.xm2 += (size_t)b0 * rab.ldx;
     rc = dispatch_sticks_fwd<T, R>(B.n3, g, st, nbb, wz, S, PrecF<R>::kin(c), inb, ld_in, outb,
-                                   ld_out, ngw);
+                                   ld_out, ngw, rab);
     timing_end(c, kFamSticksFwd, e2);
     c->kernel_launches++;
     if (rc) return rc < 0 ? fail(PSPW_ERR_NOT_IMPL, "register-FFT path: length not compiled") : rc;

@@ -17,11 +17,22 @@ struct FastGeo {
 // True when (n1, n2, n3) has compiled stick and plane kernels.
 bool fast_supported(int n1, int n2, int n3);
 
+// The Chebyshev recurrence applied by the last local pass:
+// out = ca * (H_loc in) + cb * in + cg * xm2 when `on`.
+template <typename T, typename R>
+struct RecArg {
+  bool on = false;
+  R ca = 1, cb = 0, cg = 0;
+  const T *xm2 = nullptr;
+  int ldx = 0;
+};
+
 // Local part (kinetic + V_eff sandwich) of H*psi for nb bands:
-// out = kin*in + FFT^-1 sandwich, on the cell stream.
+// out = kin*in + FFT^-1 sandwich (or the recurrence of ra), on the cell
+// stream.
 template <typename R>
 int local_fast(pspw_cell *c, const FastGeo &g, const cx<R> *in, int ld_in, cx<R> *out,
-               int ld_out, int ngw, int nb, const ScratchPlan *plan);
+               int ld_out, int ngw, int nb, const ScratchPlan *plan, const RecArg<cx<R>, R> &ra);
 
 // rho (device, natural grid order) += sum_b wband[b] |psi_b(r)|^2, with the
 // scatter limited to G index < ngw_scatter.

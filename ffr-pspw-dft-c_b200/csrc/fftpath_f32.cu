@@ -10,7 +10,7 @@ bool fast_supported(int n1, int n2, int n3) {
 }
 
 template int local_fast<float>(pspw_cell *, const FastGeo &, const float2 *, int, float2 *, int,
-                               int, int, const ScratchPlan *);
+                               int, int, const ScratchPlan *, const RecArg<float2, float> &);
 
 template int rho_fast<float>(pspw_cell *, const FastGeo &, const float2 *, int, int, int,
                             const double *, double *);

@@ -4,7 +4,8 @@
 namespace pspw {
 
 template int local_fast<double>(pspw_cell *, const FastGeo &, const double2 *, int, double2 *,
-                                int, int, int, const ScratchPlan *);
+                                int, int, int, const ScratchPlan *,
+                                const RecArg<double2, double> &);
 
 template int rho_fast<double>(pspw_cell *, const FastGeo &, const double2 *, int, int, int,
                             const double *, double *);

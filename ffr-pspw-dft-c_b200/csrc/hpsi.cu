@@ -378,7 +378,7 @@ __global__ void __launch_bounds__(256) k_backproj(ProjArg pa, const cx<R> *__res
                                                   int nb, cx<R> *out, int ldo,
                                                   const cx<R> *__restrict__ in, int ldi,
                                                   const cx<R> *__restrict__ xm2, int ldx, R a,
-                                                  R bc, R gc) {
+                                                  R bc, R gc, bool pre) {
   using T = cx<R>;
   __shared__ T As[BK][kBM + 1];
   __shared__ T Bs[BK][kBN + 1];
@@ -423,6 +423,11 @@ __global__ void __launch_bounds__(256) k_backproj(ProjArg pa, const cx<R> *__res
     for (int i = 0; i < 4; i++) {
       const int ig = g0 + tx + 16 * i;
       if (ig >= ngw) continue;
+      if (pre) {  // out holds a*(H_loc psi) + bc*in + gc*xm2 already
+        const T o = out[(size_t)bb * ldo + ig];
+        out[(size_t)bb * ldo + ig] = mk<T>(o.x + a * acc[i][j].x, o.y + a * acc[i][j].y);
+        continue;
+      }
       T h = out[(size_t)bb * ldo + ig] + acc[i][j];
       T v = mk<T>(a * h.x, a * h.y);
       if (bc != (R)0) {
@@ -491,7 +496,7 @@ __global__ void __launch_bounds__(256) k_backproj_n8(ProjArg pa, const cx<R> *__
                                                      int ngw, int nb, cx<R> *out, int ldo,
                                                      const cx<R> *__restrict__ in, int ldi,
                                                      const cx<R> *__restrict__ xm2, int ldx, R a,
-                                                     R bc, R gc) {
+                                                     R bc, R gc, bool pre) {
   using T = cx<R>;
   __shared__ T As[BK][kBM + 1];
   __shared__ T Bs[BK][kNN + 1];
@@ -524,6 +529,11 @@ __global__ void __launch_bounds__(256) k_backproj_n8(ProjArg pa, const cx<R> *__
   for (int j = 0; j < 2; j++) {
     const int bb = cc + 4 * j;
     if (bb >= nb) continue;
+    if (pre) {
+      const T o = out[(size_t)bb * ldo + ig];
+      out[(size_t)bb * ldo + ig] = mk<T>(o.x + a * acc[j].x, o.y + a * acc[j].y);
+      continue;
+    }
     T h = out[(size_t)bb * ldo + ig] + acc[j];
     T v = mk<T>(a * h.x, a * h.y);
     if (bc != (R)0) {
@@ -686,14 +696,16 @@ int project_beta64(pspw_cell *c, const double2 *psi, int ld, int ngw, int nb, do
   return PSPW_OK;
 }
 
-// out(:, b) += beta wp(:, b) over the first ngw plane waves (cuBLAS ZGEMM)
-int backproject_beta64(pspw_cell *c, const double2 *wp, int ngw, int nb, double2 *out, int ldo) {
+// out(:, b) += alpha beta wp(:, b) over the first ngw plane waves (cuBLAS)
+int backproject_beta64(pspw_cell *c, const double2 *wp, int ngw, int nb, double2 *out, int ldo,
+                       double alpha) {
   cublasHandle_t h;
   int rc = cublas_handle(c, &h);
   if (rc) return rc;
-  const cuDoubleComplex one = make_cuDoubleComplex(1.0, 0.0);
+  const cuDoubleComplex one = make_cuDoubleComplex(1.0, 0.0),
+                        al = make_cuDoubleComplex(alpha, 0.0);
   if (nb == 1) {
-    if (cublasZgemv(h, CUBLAS_OP_N, ngw, c->proj.nproj, &one,
+    if (cublasZgemv(h, CUBLAS_OP_N, ngw, c->proj.nproj, &al,
                     reinterpret_cast<const cuDoubleComplex *>(c->proj.d_beta64), c->basis.ngw,
                     reinterpret_cast<const cuDoubleComplex *>(wp), 1, &one,
                     reinterpret_cast<cuDoubleComplex *>(out), 1) != CUBLAS_STATUS_SUCCESS)
@@ -701,7 +713,7 @@ int backproject_beta64(pspw_cell *c, const double2 *wp, int ngw, int nb, double2
     c->kernel_launches++;
     return PSPW_OK;
   }
-  if (cublasZgemm(h, CUBLAS_OP_N, CUBLAS_OP_N, ngw, nb, c->proj.nproj, &one,
+  if (cublasZgemm(h, CUBLAS_OP_N, CUBLAS_OP_N, ngw, nb, c->proj.nproj, &al,
                   reinterpret_cast<const cuDoubleComplex *>(c->proj.d_beta64), c->basis.ngw,
                   reinterpret_cast<const cuDoubleComplex *>(wp), c->proj.nproj, &one,
                   reinterpret_cast<cuDoubleComplex *>(out), ldo) != CUBLAS_STATUS_SUCCESS)
@@ -899,7 +911,14 @@ int hpsi_apply(pspw_cell *c, const void *in_v, int ld_in, void *out_v, int ld_ou
   if (B.fast) {
     const FastGeo fg{B.ncol, B.nxa, B.d_col_start, B.d_sg_ig, B.d_sg_z, B.d_sg_col, B.d_xa_list,
                      B.d_col_x, B.d_col_y, B.d_xa_of_x};
-    int rc = local_fast<R>(c, fg, in, ld_in, out, ld_out, ngw, nb, plan);
+    RecArg<T, R> ra;
+    ra.on = true;
+    ra.ca = (R)a;
+    ra.cb = (R)b;
+    ra.cg = (R)g;
+    ra.xm2 = xm2;
+    ra.ldx = ld_xm2;
+    int rc = local_fast<R>(c, fg, in, ld_in, out, ld_out, ngw, nb, plan, ra);
     if (rc) return rc;
   } else {
   const size_t s_band = (size_t)B.n3 * B.ncol, p_band = (size_t)B.n3 * B.n2 * B.nxa;
@@ -960,7 +979,11 @@ int hpsi_apply(pspw_cell *c, const void *in_v, int ld_in, void *out_v, int ld_ou
   }
   PSPW_CUDA(cudaGetLastError());
 
-  // ---- back-projection + recurrence epilogue
+  // ---- back-projection + recurrence epilogue.  On the register-FFT path the
+  // forward stick pass has applied the recurrence to the local part already
+  // (out = a H_loc in + b in + g xm2), so the back-projection only adds
+  // a * beta W beta^H in.
+  const bool pre = B.fast;
   if (nproj > 0) {
     if (overlap) PSPW_CUDA(cudaStreamWaitEvent(st, c->ev_join, 0));
     timing_begin(c, kFamNonlocal, &ev);
@@ -970,7 +993,7 @@ int hpsi_apply(pspw_cell *c, const void *in_v, int ld_in, void *out_v, int ld_ou
       const int rc = nl_tc_backproject(
           c, tc_wt, ngw, nb, reinterpret_cast<float2 *>(out), ld_out,
           reinterpret_cast<const float2 *>(in), ld_in, reinterpret_cast<const float2 *>(xm2),
-          ld_xm2, (float)a, (float)b, (float)g);
+          ld_xm2, (float)a, pre ? 0.f : (float)b, pre ? 0.f : (float)g, pre);
       timing_end(c, kFamBackproj, e);
       if (rc) return rc;
     } else {
@@ -981,9 +1004,9 @@ int hpsi_apply(pspw_cell *c, const void *in_v, int ld_in, void *out_v, int ld_ou
           cudaEvent_t e;
           timing_begin(c, kFamBackproj, &e);
           int rc = backproject_beta64(c, reinterpret_cast<const double2 *>(wp), ngw, nb,
-                                      reinterpret_cast<double2 *>(out), ld_out);
+                                      reinterpret_cast<double2 *>(out), ld_out, pre ? a : 1.0);
           if (rc) return rc;
-          if (a != 1.0 || b != 0.0 || g != 0.0) {
+          if (!pre && (a != 1.0 || b != 0.0 || g != 0.0)) {
             k_axpby3<R><<<4 * 148, 256, 0, st>>>(ngw, nb, out, ld_out, in, ld_in, xm2, ld_xm2,
                                                 (R)a, (R)b, (R)g);
             c->kernel_launches++;
@@ -995,14 +1018,14 @@ int hpsi_apply(pspw_cell *c, const void *in_v, int ld_in, void *out_v, int ld_ou
       if (!done) run(kFamBackproj, [&] {
         if (nb <= kNN)
           k_backproj_n8<R, BK><<<grid.x, 256, 0, st>>>(pa, wp, ngw, nb, out, ld_out, in, ld_in,
-                                                       xm2, ld_xm2, (R)a, (R)b, (R)g);
+                                                       xm2, ld_xm2, (R)a, (R)b, (R)g, pre);
         else
           k_backproj<R, BK><<<grid, 256, 0, st>>>(pa, wp, ngw, nb, out, ld_out, in, ld_in, xm2,
-                                                  ld_xm2, (R)a, (R)b, (R)g);
+                                                  ld_xm2, (R)a, (R)b, (R)g, pre);
       });
     }
     timing_end(c, kFamNonlocal, ev);
-  } else if (a != 1.0 || b != 0.0 || g != 0.0) {
+  } else if (!pre && (a != 1.0 || b != 0.0 || g != 0.0)) {
     run(kFamBackproj, [&] {
       k_axpby3<R><<<4 * 148, 256, 0, st>>>(ngw, nb, out, ld_out, in, ld_in, xm2, ld_xm2, (R)a,
                                           (R)b, (R)g);

@@ -389,7 +389,7 @@ template <int L>
 __global__ void __launch_bounds__(kThreads) k_backproj_tc(
     const float *__restrict__ etb, const float *__restrict__ wt, int nsa, int ngw, int nb, int nbt,
     const float *__restrict__ pkga, float2 *out, int ldo, const float2 *__restrict__ in, int ldi,
-    const float2 *__restrict__ xm2, int ldx, float ca, float cb, float cg, int *err) {
+    const float2 *__restrict__ xm2, int ldx, float ca, float cb, float cg, bool pre, int *err) {
   constexpr int per = 2 * L;
   extern __shared__ __align__(1024) unsigned char sm[];
   __shared__ Sync sy;
@@ -476,7 +476,10 @@ __global__ void __launch_bounds__(kThreads) k_backproj_tc(
           acci += pk[l] * __uint_as_float(v[2 * l + 1]);
         }
         const int bl = bstart + j;
-        if (gv && bl < nbb) {
+        if (gv && bl < nbb && pre) {
+          // the recurrence's other terms are in out already (stick pass)
+          out[(size_t)(b0 + bl) * ldo + g] = make_float2(hc.x + ca * accr, hc.y + ca * acci);
+        } else if (gv && bl < nbb) {
           float rr = ca * (hc.x + accr), ii = ca * (hc.y + acci);
           if (cb != 0.f) {
             rr += cb * uc.x;
@@ -631,14 +634,14 @@ int launch_project(pspw_cell *c, const Shape &s, const float2 *psi, int ld, int 
 template <int L>
 int launch_back(pspw_cell *c, const Shape &s, const float *wt, int ngw, int nb, float2 *out,
                 int ldo, const float2 *in, int ldi, const float2 *xm2, int ldx, float a, float b,
-                float g) {
+                float g, bool pre) {
   const int smem = back_smem(s);
   PSPW_CUDA(
       cudaFuncSetAttribute(k_backproj_tc<L>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
   dim3 grid((ngw + 127) / 128, s.nbtiles);
   k_backproj_tc<L><<<grid, kThreads, smem, c->stream>>>(c->proj.d_etb, wt, s.nsa, ngw, nb, s.nbt,
                                                         c->proj.d_pkga32, out, ldo, in, ldi, xm2,
-                                                        ldx, a, b, g, c->d_err);
+                                                        ldx, a, b, g, pre, c->d_err);
   c->kernel_launches++;
   PSPW_CUDA(cudaGetLastError());
   return PSPW_OK;
@@ -719,13 +722,13 @@ int nl_tc_project(pspw_cell *c, const float2 *psi, int ld, int ngw, int nb, floa
 
 int nl_tc_backproject(pspw_cell *c, const float *wt, int ngw, int nb, float2 *out, int ldo,
                       const float2 *in, int ldi, const float2 *xm2, int ldx, float a, float b,
-                      float g) {
+                      float g, bool pre) {
   const Shape s = shape_of(c, nb);
   switch (s.L) {
-    case 1: return launch_back<1>(c, s, wt, ngw, nb, out, ldo, in, ldi, xm2, ldx, a, b, g);
-    case 2: return launch_back<2>(c, s, wt, ngw, nb, out, ldo, in, ldi, xm2, ldx, a, b, g);
-    case 3: return launch_back<3>(c, s, wt, ngw, nb, out, ldo, in, ldi, xm2, ldx, a, b, g);
-    default: return launch_back<4>(c, s, wt, ngw, nb, out, ldo, in, ldi, xm2, ldx, a, b, g);
+    case 1: return launch_back<1>(c, s, wt, ngw, nb, out, ldo, in, ldi, xm2, ldx, a, b, g, pre);
+    case 2: return launch_back<2>(c, s, wt, ngw, nb, out, ldo, in, ldi, xm2, ldx, a, b, g, pre);
+    case 3: return launch_back<3>(c, s, wt, ngw, nb, out, ldo, in, ldi, xm2, ldx, a, b, g, pre);
+    default: return launch_back<4>(c, s, wt, ngw, nb, out, ldo, in, ldi, xm2, ldx, a, b, g, pre);
   }
 }
 

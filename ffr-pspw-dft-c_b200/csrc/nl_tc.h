@@ -27,9 +27,11 @@ int nl_tc_reserve(pspw_cell *c, int ngw, int nb, float **part, int *max_split, f
 int nl_tc_project(pspw_cell *c, const float2 *psi, int ld, int ngw, int nb, float *part,
                   int max_split, float *wt);
 
-// out = a*(out + sum_{a,lm} EIGR PKG_A W) + b*in + g*xm2 on the first ngw G.
+// out = a*(out + sum_{a,lm} EIGR PKG_A W) + b*in + g*xm2 on the first ngw G;
+// with pre, out already holds a*(H_loc psi) + b*in + g*xm2 and the kernel
+// adds a * sum EIGR PKG_A W.
 int nl_tc_backproject(pspw_cell *c, const float *wt, int ngw, int nb, float2 *out, int ldo,
                       const float2 *in, int ldi, const float2 *xm2, int ldx, float a, float b,
-                      float g);
+                      float g, bool pre = false);
 
 }  // namespace pspw
