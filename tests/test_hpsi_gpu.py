@@ -193,6 +193,36 @@ def test_chebyfilt_fp32(cfg0):
     assert relmax(out, ref) < 1e-4
 
 
+def test_chebyfilt_fewer_plane_waves_than_the_cell(cfg0):
+    # NGW_ik below the cell's sphere: the filter stays in the caller's G order
+    w, cell = cfg0
+    ngw = 2000
+    X = np.asfortranarray(w["psi"][:ngw, :5])
+    out = cell.chebyfilt(X, 4, 1.5, 5.0, PREC_F64)
+    oc = oracle_cell(w)
+    ref = O.chebyfilt(oc, X, 4, 1.5, 5.0, w["veff"])
+    assert relmax(out, ref) < TOL64
+
+
+def test_chebyfilt_device_leading_dimension_stick_order(cfg0):
+    # the whole sphere on the register-FFT path: the filter permutes the
+    # block into the stick order and back, here with ld > ngw
+    w, cell = cfg0
+    psi = w["psi"][:, :5]
+    ngw = psi.shape[0]
+    ld = ngw + 9
+    host = np.full((5, ld), 7.0 + 3.0j)
+    host[:, :ngw] = psi.T
+    d_x = torch.from_numpy(host).cuda()
+    torch.cuda.synchronize()
+    cell.chebyfilt_dev(d_x, ld, ngw, 5, 6, 1.5, 5.0, PREC_F64)
+    torch.cuda.synchronize()
+    got = d_x.cpu().numpy()
+    ref = O.chebyfilt(oracle_cell(w), psi, 6, 1.5, 5.0, w["veff"])
+    assert relmax(got[:, :ngw].T, ref) < TOL64
+    assert np.all(got[:, ngw:] == 7.0 + 3.0j)  # padding rows untouched
+
+
 def test_errors_are_reported(gcell):
     with pytest.raises(PspwError) as e:
         gcell.set_veff(np.zeros(17))
