@@ -467,7 +467,7 @@ def run_engine(args, rank, world, local_rank):
         if f in alg_flops:
             d["alg_tflops"] = round(alg_flops[f] * calls / (t * 1e-3) / 1e12, 2)
         fam_report[names.get(f, str(f))] = d
-    roof["traffic"] = _ncu_traffic(roof["kernel"], args.prec)
+    roof["traffic"] = _ncu_traffic(args.workload, roof["kernel"], args.prec)
     kernels_ms = fam_report
     hpsi_ms = ms_max / DEGREE
     hpsi_roof = {"bytes_per_hpsi": hpsi_bytes_model(ngw, nnr, nb, nat, fp64=fp64),
@@ -508,16 +508,18 @@ def run_engine(args, rank, world, local_rank):
                 ngw=ngw, nb=nb, sizes=sizes)
 
 
-def _ncu_traffic(kernel, prec):
-    """DRAM bytes per launch of `kernel` from the committed ncu summary, or None."""
+def _ncu_traffic(workload, kernel, prec):
+    """DRAM bytes per launch of `kernel` on `workload` from the committed ncu
+    summary (lines `workload kernel prec bytes`), or None if not captured."""
     path = os.path.join(ROOT, "profiles", "ncu_traffic.txt")
     if not os.path.exists(path):
         return None
     for line in open(path):
         parts = line.split()
-        if len(parts) >= 3 and parts[0] == kernel and parts[1] == prec:
+        if (len(parts) >= 4 and parts[0] == workload and parts[1] == kernel
+                and parts[2] == prec):
             try:
-                return int(float(parts[2]))
+                return int(float(parts[3]))
             except ValueError:
                 return None
     return None

@@ -127,6 +127,24 @@ int eval_rho_psi_dev(pspw_cell *c, const double2 *dX, int ld, int ngw, int nx, c
   return PSPW_OK;
 }
 
+// enl_p[p] = sum_ist focc[ist] |P(p, ist)|^2: one warp per projector, lanes
+// over the states in a fixed order, then a fixed shuffle tree
+__global__ void k_enl_per_projector(const double2 *__restrict__ P, const double *__restrict__ focc,
+                                    int nx, int nproj, double *enl_p) {
+  const int p = (int)((blockIdx.x * (size_t)blockDim.x + threadIdx.x) >> 5);
+  const int lane = threadIdx.x & 31;
+  if (p >= nproj) return;  // uniform per warp
+  double acc = 0.0;
+  for (int ist = lane; ist < nx; ist += 32) {
+    const double2 sf = P[(size_t)ist * nproj + p];
+    const double a = hypot(sf.x, sf.y);
+    acc += focc[ist] * (a * a);
+  }
+#pragma unroll
+  for (int d = 16; d > 0; d >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, d);
+  if (lane == 0) enl_p[p] = acc;
+}
+
 // EvalENL.cpp:5-49 for one k-point on a device block X (ngw x nx, ld).
 int eval_enl_dev(pspw_cell *c, const double2 *dX, int ld, int ngw, int nx, const double *focc,
                  double wkpt, double *enl, double *fnl) {
@@ -137,6 +155,28 @@ int eval_enl_dev(pspw_cell *c, const double2 *dX, int ld, int ngw, int nx, const
   int rc;
   if ((rc = ws_reserve(c, kSlotE, sizeof(double2) * (size_t)nx * nproj, (void **)&dP))) return rc;
   if ((rc = project_fp64(c, dX, ld, ngw, nx, dP))) return rc;
+  if (!fnl) {
+    // only the energy: the per-projector sums over states on the device (a
+    // fixed lane-strided order, not the reference's sequential one: equal to
+    // rounding), the sum over projectors in the reference's order on the host
+    double *dfo, *dep;
+    if ((rc = ws_reserve(c, kSlotD, sizeof(double) * ((size_t)nx + nproj), (void **)&dfo)))
+      return rc;
+    dep = dfo + nx;
+    PSPW_CUDA(cudaMemcpyAsync(dfo, focc, sizeof(double) * nx, cudaMemcpyHostToDevice, c->stream));
+    k_enl_per_projector<<<(nproj * 32 + 255) / 256, 256, 0, c->stream>>>(dP, dfo, nx, nproj, dep);
+    c->kernel_launches++;
+    std::vector<double> ep(nproj), w(nproj);
+    PSPW_CUDA(cudaMemcpyAsync(ep.data(), dep, sizeof(double) * nproj, cudaMemcpyDeviceToHost,
+                              c->stream));
+    PSPW_CUDA(cudaMemcpyAsync(w.data(), c->proj.d_pw64, sizeof(double) * nproj,
+                              cudaMemcpyDeviceToHost, c->stream));
+    if ((rc = sync(c))) return rc;
+    double e = 0.0;
+    for (int p = 0; p < nproj; p++) e = e + wkpt * ep[p] * w[p];
+    *enl = e;
+    return PSPW_OK;
+  }
   std::vector<double2> P((size_t)nx * nproj);
   std::vector<double> w(nproj);
   PSPW_CUDA(cudaMemcpyAsync(P.data(), dP, sizeof(double2) * P.size(), cudaMemcpyDeviceToHost,

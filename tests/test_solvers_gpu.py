@@ -201,3 +201,9 @@ def test_eval_device_pointer_variants(gcell):
                               C.byref(e), fnl.ctypes.data))
     e_h, fnl_h = gcell.eval_enl(psi, nx, focc, 0.75)
     assert e.value == e_h and np.array_equal(fnl, fnl_h)
+    # energy only (no FNL): the state sums run on the device in another
+    # order, so equal to rounding
+    e_only = C.c_double(0.0)
+    check(L.pspw_eval_enl_dev(gcell.handle, X.data_ptr(), ngw, ngw, nx, focc.ctypes.data, 0.75,
+                              C.byref(e_only), None))
+    assert abs(e_only.value - e_h) <= 1e-13 * max(1.0, abs(e_h))
