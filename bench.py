@@ -3,7 +3,7 @@
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl engine|reference]
                     [--prec f32|f64]
-                    [--workload si64|si216|scf-si8|scf-si64|setup-si64|setup-si216]
+                    [--workload si64|si216|scf-si8|scf-si64|converge-si64|eig-si216|setup-si64|setup-si216]
 
 One step = one call of the degree-10 Chebyshev filter (chebyfilt.cpp:6-74)
 on the Si64 cell (64 atoms, a = 20.52 bohr, ecutwfc 15 Ha, 64^3 grid,
@@ -185,6 +185,11 @@ ROW_WORKLOADS = {
     "scf-si64": dict(kind="scf", nrep=2, grid=(64, 64, 64), nempty=14,
                      text="Si64, a=20.52 bohr, ECUT 30 Ry, grid 64^3, NGW 23847, NX 142 "
                           "(144 bands)"),
+    "converge-si64": dict(kind="converge", nrep=2, grid=(64, 64, 64), nempty=14,
+                          text="Si64, a=20.52 bohr, ECUT 30 Ry, grid 64^3, NGW 23847, NX 142 "
+                               "(144 bands), to |dETOT| <= 1e-6 Ha"),
+    "eig-si216": dict(kind="eigsolve", nrep=3, grid=(96, 96, 96), nempty=32,
+                      text="Si216, a=30.78 bohr, ECUT 30 Ry, grid 96^3, NGW 80725, 512 states"),
     "setup-si64": dict(kind="setup", nrep=2, grid=(64, 64, 64), nempty=14,
                        text="Si64, a=20.52 bohr, ECUT 30 Ry, grid 64^3, NGW 23847, NX 142"),
     "setup-si216": dict(kind="setup", nrep=3, grid=(96, 96, 96), nempty=32,
@@ -192,7 +197,7 @@ ROW_WORKLOADS = {
 }
 
 
-def _write_row_input(d, w, max_scf):
+def _write_row_input(d, w, max_scf, conv=0.0):
     from pspw import synth
     from pspw.inputs import write_input, write_synthetic_fhi
     os.makedirs(d, exist_ok=True)
@@ -200,7 +205,7 @@ def _write_row_input(d, w, max_scf):
     write_synthetic_fhi(os.path.join(d, "X.fhi"))
     write_input(os.path.join(d, "INPUT"), "X.fhi", pos, float(lat[0][0]), ecut_ry=30.0, iscf=1,
                 idiag=-1, imix=3, max_scf=max_scf, nempty=w["nempty"], fft_grid=w["grid"],
-                conv=0.0)
+                conv=conv)
     return d
 
 
@@ -233,6 +238,12 @@ def row_reference(args, w, tmp):
     if not (ref_available() and os.path.exists(os.path.join(ROOT, "oracle", "_ref",
                                                              "ffr_pspw_dft.x"))):
         return None, "oracle/_ref not built (make -C oracle)"
+    if w["kind"] == "eigsolve":
+        return None, ("one reference LOBPCG iteration on Si216 (512 single-band ApplyHam "
+                      "calls, 1536^3 LAPACK) takes tens of minutes")
+    if w["kind"] == "converge":
+        return None, ("one reference ChebySCF iteration on Si64 takes minutes, a converged "
+                      "run hours; --workload scf-si64 --impl reference gives its rate")
     if w["kind"] == "setup":
         d = _write_row_input(os.path.join(tmp, "ref_setup"), w, 1)
         ts = [_ref_setup_seconds(d) for _ in range(max(1, args.steps))]
@@ -347,6 +358,151 @@ def run_row(args, rank, world, local_rank):
         else:
             out["phases_ms_per_iteration"] = parts
         print(json.dumps(out))
+
+
+MAX_SCF_CONVERGE = 200
+
+
+def run_converge(args, rank, world, local_rank):
+    """--workload converge-si64: one step = one whole ChebySCF run on Si64
+    from a random start to |dETOT| <= 1e-6 Ha (ChebySCFLoop.cpp:350), all
+    FP64 and in the mixed form (the filter and the H*v of the Lanczos filter
+    bounds in FP32; orthonormalisation, Rayleigh-Ritz, density, energies and
+    mixing in FP64).  The FP64 run is the accuracy reference of the mixed
+    run: its H*psi agrees with the reference's ApplyHam_block to 1e-12.
+    value = the mixed run's time to converged (host wall clock around
+    pspw_system_cheby_scf, which returns after its last synchronisation;
+    set-up not included)."""
+    import tempfile
+
+    import torch
+    from pspw import PREC_F32, PREC_F64, replica
+    from pspw.system import System
+    w = ROW_WORKLOADS[args.workload]
+    torch.cuda.set_device(local_rank)
+    tmp = tempfile.mkdtemp(prefix="pspw_conv_")
+    S = System(_write_row_input(os.path.join(tmp, "engine"), w, MAX_SCF_CONVERGE, conv=1e-6),
+               device=local_rank)
+    nat = 8 * w["nrep"] ** 3
+    modes = {"fp64": PREC_F64, "mixed": PREC_F32}
+    for prec in modes.values():  # warm-up runs (allocations, first touch)
+        S.cheby_scf(filter_prec=prec)
+    replica.barrier()
+    clocks = ClockSampler(local_rank)
+    clocks.start()
+    runs = {m: [] for m in modes}
+    last, conv_all = {}, {m: True for m in modes}
+    for _ in range(max(1, args.steps)):
+        for m, prec in modes.items():
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            res = S.cheby_scf(filter_prec=prec)
+            runs[m].append(time.perf_counter() - t0)
+            last[m] = res
+            conv_all[m] = conv_all[m] and res["converged"]
+    clocks.stop()
+    S.close()
+    t = {m: replica.max_over_ranks(sum(v) / len(v)) for m, v in runs.items()}
+    nocc = int(round(4 * nat / 2))
+    r64, r32 = last["fp64"], last["mixed"]
+    de = r32["eig"] - r64["eig"]
+    summary = {m: {"seconds": round(t[m], 4), "iterations": last[m]["iterations"],
+                   "converged_every_run": conv_all[m],
+                   "ms_per_iteration": round(t[m] * 1e3 / last[m]["iterations"], 3),
+                   "etot": last[m]["energies"]["ETOT"],
+                   "detot_last": [float(x) for x in last[m]["hist"][-6:, 1]]} for m in modes}
+    if rank == 0:
+        out = {"metric": "Si64 ChebySCF time to converged, FP32 filter / FP64 Rayleigh-Ritz",
+               "value": round(t["mixed"], 4), "unit": "s", "n_gpus": world,
+               "steps": args.steps, "warmup": 1, "ms_per_step": round(t["mixed"] * 1e3, 3),
+               "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
+               "dtype": "c64 filter, f64 rest", "data": "synthetic",
+               "config": {"workload": f"{args.workload}: {w['text']}",
+                          "input": "INPUT + synthetic FHI98 pseudopotential in the "
+                                   "reference's formats", "mixing": "Pulay (IMIX 3)",
+                          "start": "random (IDIAG -1)", "filter_degree": 10,
+                          "parallelism": f"replica x{world}",
+                          "l2": "inputs larger than L2; no flush"},
+               "modes": summary,
+               "speedup_mixed_vs_fp64": round(t["fp64"] / t["mixed"], 3),
+               "etot_error_ha_per_atom": abs(r32["energies"]["ETOT"] - r64["energies"]["ETOT"])
+               / nat,
+               "eig_max_error_ha_occupied": float(np.abs(de[:nocc]).max()),
+               "eig_max_error_ha_all": float(np.abs(de).max()),
+               "eig_mean_error_ha_occupied": float(np.abs(de[:nocc]).mean()),
+               "cpu_baseline": {"value": None,
+                                "unavailable": "one reference iteration on Si64 takes minutes "
+                                               "(see --workload scf-si64 for its rate)"},
+               "clocks": clocks.summary(),
+               "timing": "host wall clock around each whole SCF run"}
+        print(json.dumps(out))
+
+
+def run_eigsolve(args, rank, world, local_rank):
+    """--workload eig-si216: the block eigensolvers on the Si216 cell (96^3,
+    NGW 80725, 512 bands, fixed V_loc): davidson_cpu (2 x 512 subspace) and
+    lobpcg_cpu (Q of 3 x 512 columns, 1536 x 1536 Rayleigh-Ritz) on the
+    device, each run for `--steps` iterations from the reference's own
+    random start (random_col), with H*psi and the preconditioner in FP64 and
+    in FP32; orthonormalisation, Gram matrices and the subspace eigensolves
+    are FP64 in both.  Eigenvalues of the states the FP64 run resolves
+    (residual < 1e-3) are compared between the two.  value = LOBPCG
+    iterations per second with FP32 H*psi."""
+    import torch
+    from pspw import PREC_F32, PREC_F64, replica, workloads
+    torch.cuda.set_device(local_rank)
+    wl = workloads.si_cell(3, 96)
+    cell = workloads.make_cell(wl, device=local_rank)
+    ngw, nb, nempty = wl["ngw"], 512, 32
+    prec = cell.gen_prec(ngw, -10.0)
+    iters = max(1, args.steps)
+    out_modes = {}
+    clocks = ClockSampler(local_rank)
+    cell.lobpcg(ngw, nb, prec, nempty, max_iter=1, hprec=PREC_F32)  # warm-up (allocations)
+    cell.davidson(ngw, nb, prec, nempty, max_iter=1, hprec=PREC_F32)
+    replica.barrier()
+    clocks.start()
+    for solver in ("lobpcg", "davidson"):
+        run = getattr(cell, solver)
+        res = {}
+        for name, hp in (("fp64", PREC_F64), ("fp32", PREC_F32)):
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            ev, _, r, it = run(ngw, nb, prec, nempty, max_iter=iters, hprec=hp)
+            res[name] = (time.perf_counter() - t0, ev, r, it)
+        ok = res["fp64"][2] < 1e-3
+        d = np.abs(res["fp64"][1] - res["fp32"][1])
+        out_modes[solver] = {
+            m: {"seconds": round(v[0], 3), "iterations": v[3],
+                "ms_per_iteration": round(v[0] * 1e3 / max(1, v[3]), 2)}
+            for m, v in res.items()}
+        out_modes[solver]["resolved_states"] = int(ok.sum())
+        out_modes[solver]["eig_max_error_ha_resolved"] = float(d[ok].max()) if ok.any() else None
+        out_modes[solver]["speedup_fp32_vs_fp64"] = round(res["fp64"][0] / res["fp32"][0], 3)
+    clocks.stop()
+    cell.close()
+    lob = out_modes["lobpcg"]["fp32"]
+    t_it = replica.max_over_ranks(lob["seconds"] / max(1, lob["iterations"]))
+    if rank == 0:
+        print(json.dumps({
+            "metric": "Si216 LOBPCG iterations/s, FP32 H*psi, FP64 subspace steps",
+            "value": round(world / t_it, 4), "unit": "iterations/s", "n_gpus": world,
+            "steps": iters, "warmup": 1, "ms_per_step": round(t_it * 1e3, 2),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "c64 H*psi, f64 rest", "data": "synthetic",
+            "config": {"workload": "eig-si216: Si216, a=30.78 bohr, ECUT 30 Ry, grid 96^3, "
+                                   "NGW 80725, 512 states (32 empty), fixed V_loc",
+                       "start": "random_col (the reference's LCG start)",
+                       "preconditioner": "GenPrec tau=-10 (Teter)",
+                       "parallelism": f"replica x{world}",
+                       "l2": "inputs larger than L2; no flush"},
+            "solvers": out_modes,
+            "cpu_baseline": {"value": None,
+                             "unavailable": "one reference LOBPCG iteration on Si216 "
+                                            "(512 single-band ApplyHam calls, 1536^3 "
+                                            "LAPACK) takes tens of minutes"},
+            "clocks": clocks.summary(),
+            "timing": "host wall clock around each solver call"}))
 
 
 # ------------------------------------------------------------------ engine arm
@@ -575,7 +731,12 @@ def main():
             import datetime
             torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
                                                  device_id=torch.device("cuda", local_rank))
-        run_row(args, rank, world, local_rank)
+        if ROW_WORKLOADS[args.workload]["kind"] == "converge":
+            run_converge(args, rank, world, local_rank)
+        elif ROW_WORKLOADS[args.workload]["kind"] == "eigsolve":
+            run_eigsolve(args, rank, world, local_rank)
+        else:
+            run_row(args, rank, world, local_rank)
         if world > 1:
             torch.distributed.barrier()
             torch.distributed.destroy_process_group()

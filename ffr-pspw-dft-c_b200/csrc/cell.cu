@@ -546,6 +546,7 @@ int swap_stick_order(pspw_cell *c) {
   std::swap(P.d_etp, S.etp);
   std::swap(P.d_etb, S.etb);
   std::swap(P.d_beta64, S.beta64);
+  S.active = !S.active;
   return PSPW_OK;
 }
 

@@ -72,23 +72,38 @@ __global__ void k_symmetrize(double2 *v, int ldv, int n) {
 }
 
 // column dots: one block per column, fixed-order tree reduction
+// one block per column; four independent partial sums per thread keep four
+// loads in flight, then a fixed-order warp and block reduction
 __global__ void k_coldot(const double2 *__restrict__ x, int ldx, const double2 *__restrict__ y,
                          int ldy, int m, double *out) {
-  __shared__ double red[256];
-  const int j = blockIdx.x;
+  __shared__ double red[32];
+  const int j = blockIdx.x, nt = blockDim.x;
   const double2 *xc = x + (size_t)j * ldx, *yc = y + (size_t)j * ldy;
-  double s = 0.0;
-  for (int i = threadIdx.x; i < m; i += blockDim.x) {
+  double s0 = 0.0, s1 = 0.0, s2 = 0.0, s3 = 0.0;
+  int i = threadIdx.x;
+  for (; i + 3 * nt < m; i += 4 * nt) {
+    const double2 a0 = xc[i], b0 = yc[i], a1 = xc[i + nt], b1 = yc[i + nt];
+    const double2 a2 = xc[i + 2 * nt], b2 = yc[i + 2 * nt], a3 = xc[i + 3 * nt],
+                  b3 = yc[i + 3 * nt];
+    s0 += a0.x * b0.x + a0.y * b0.y;
+    s1 += a1.x * b1.x + a1.y * b1.y;
+    s2 += a2.x * b2.x + a2.y * b2.y;
+    s3 += a3.x * b3.x + a3.y * b3.y;
+  }
+  for (; i < m; i += nt) {
     const double2 a = xc[i], b = yc[i];
-    s += a.x * b.x + a.y * b.y;
+    s0 += a.x * b.x + a.y * b.y;
   }
-  red[threadIdx.x] = s;
+  double s = (s0 + s1) + (s2 + s3);
+  for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = nt >> 5;
+  if (lane == 0) red[warp] = s;
   __syncthreads();
-  for (int w = blockDim.x / 2; w > 0; w >>= 1) {
-    if (threadIdx.x < w) red[threadIdx.x] += red[threadIdx.x + w];
-    __syncthreads();
+  if (warp == 0) {
+    s = lane < nw ? red[lane] : 0.0;
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
+    if (lane == 0) out[j] = s;
   }
-  if (threadIdx.x == 0) out[j] = red[0];
 }
 
 __global__ void k_residual(const double *__restrict__ lam, const double2 *__restrict__ X, int ldx,
@@ -230,7 +245,9 @@ int dev_symmetrize(pspw_cell *c, double2 *v, int ldv, int n) {
 int dev_coldot(pspw_cell *c, const double2 *x, int ldx, const double2 *y, int ldy, int m, int n,
                double *out) {
   if (n <= 0) return PSPW_OK;
-  k_coldot<<<n, 256, 0, c->stream>>>(x, ldx, y, ldy, m, out);
+  // few columns (Lanczos, single vectors): wide blocks, so one column's
+  // loads spread over 32 warps
+  k_coldot<<<n, n < 148 ? 1024 : 256, 0, c->stream>>>(x, ldx, y, ldy, m, out);
   c->kernel_launches++;
   PSPW_CUDA(cudaGetLastError());
   return PSPW_OK;

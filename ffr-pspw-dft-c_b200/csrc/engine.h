@@ -178,6 +178,7 @@ struct pspw_cell {
   // the cell's own (a second call swaps back).
   struct {
     bool built = false;
+    bool active = false;   // the stick-order copies are the ones swapped in
     int *sg_ig = nullptr;  // identity: G k of the stick list is G k
     double *kin64 = nullptr;
     float *kin32 = nullptr;

@@ -53,7 +53,7 @@ __global__ void __launch_bounds__(256) k_sticks_inv(FastGeo g, const T *__restri
 #pragma unroll
     for (int u = 0; u < U; u++) {
       const int k = kb + u * 256;
-      ig[u] = k < k1 ? g.sg_ig[k] : ngw_call;
+      ig[u] = k < k1 ? (g.ig_iota ? k : g.sg_ig[k]) : ngw_call;
       off[u] = k < k1 ? (g.sg_col[k] - c0) * LS + g.sg_z[k] : 0;
     }
     T v[U];
@@ -128,7 +128,7 @@ __global__ void __launch_bounds__(256) k_sticks_fwd(FastGeo g, const T *__restri
 #pragma unroll
     for (int u = 0; u < U; u++) {
       const int k = kb + u * 256;
-      ig[u] = k < k1 ? g.sg_ig[k] : ngw_call;
+      ig[u] = k < k1 ? (g.ig_iota ? k : g.sg_ig[k]) : ngw_call;
       off[u] = k < k1 ? (g.sg_col[k] - c0) * LS + g.sg_z[k] : 0;
     }
     R kk[U];

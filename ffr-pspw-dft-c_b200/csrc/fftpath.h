@@ -12,6 +12,9 @@ struct FastGeo {
   int ncol, nxa;
   const int *col_start, *sg_ig, *sg_z, *sg_col, *xa_list, *col_x, *col_y;
   const int *xa_of_x;  // [n1] active index of x, or -1
+  // sg_ig is the identity (the block is in stick order): the kernels use k
+  // itself, so the psi loads do not wait for an index load
+  bool ig_iota = false;
 };
 
 // True when (n1, n2, n3) has compiled stick and plane kernels.

@@ -716,6 +716,7 @@ int pspw_scf_create(pspw_cell *c, int ng, const int *n1, const int *n2, const in
   if (gidx[0] != 0) return fail(PSPW_ERR_SHAPE, "scf_create: the first G must be G = 0");
   pspw_scf *s = new pspw_scf;
   s->cell = c;
+  s->device = c->device;
   s->ng = ng;
   s->nsp = nsp;
   s->omega = omega;
@@ -748,8 +749,11 @@ int pspw_scf_create(pspw_cell *c, int ng, const int *n1, const int *n2, const in
 
 int pspw_scf_destroy(pspw_scf *s) {
   if (!s) return PSPW_OK;
-  cudaSetDevice(s->cell->device);
-  cudaStreamSynchronize(s->cell->stream);
+  // the cell may already be gone (a garbage collector finalises handles in
+  // any order): only the device id is read, and the whole device is
+  // synchronised instead of the cell's stream
+  cudaSetDevice(s->device);
+  cudaDeviceSynchronize();
   void *p[] = {s->d_gidx, s->d_g, s->d_vp, s->d_rp, s->d_grid, s->d_vxc,
                s->d_tmp,  s->d_part, s->d_hist, s->d_f, s->d_gm};
   for (void *q : p)

@@ -9,13 +9,13 @@
 
 struct pspw_scf {
   pspw_cell *cell = nullptr;
+  int device = 0;  // the cell's device, so destroy needs no live cell
   int ng = 0, nsp = 0;
   double omega = 0.0, nel = 0.0, esr = 0.0, eself = 0.0;
   int *d_gidx = nullptr;    // [ng] 0-based grid index of density G ig
   double *d_g = nullptr;    // [ng] |G|^2 in (2 pi / alat)^2 units (G[0] = 0)
   double2 *d_vp = nullptr;  // [ng] sum_s SFAC(s,ig) VPS(s,ig)
   double2 *d_rp = nullptr;  // [ng] sum_s SFAC(s,ig) RHOPS(s,ig)
-  int *d_wgidx = nullptr;   // [ngw] grid index of wavefunction G (Kerker filter)
   double2 *d_grid = nullptr;  // NNR complex work grid
   double *d_vxc = nullptr;    // NNR
   double *d_tmp = nullptr;    // NNR real work vector

@@ -9,8 +9,9 @@
 //   (H X, X^H H X, symmetrize, eigendecomposition, rotation), EvalRhoPsi,
 //   EvalENL, mixing, EvalEnergy, |dETOT| test, new bounds from the Ritz
 //   values and a 10-step Lanczos (ChebySCFLoop.cpp:351-366).
-// The filter may run in FP32 (the mixed-precision mode); everything else is
-// FP64.
+// The filter may run in FP32 (the mixed-precision mode), and with it the
+// H*v products of the Lanczos bounds, which only set the filter's window;
+// everything else is FP64.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -134,6 +135,8 @@ extern "C" int pspw_cheby_scf(pspw_scf *s, const pspw_scf_params *p, const doubl
     return fail(PSPW_ERR_ARG, "cheby_scf: bad sizes");
   if (p->filter_prec != PSPW_PREC_F64 && p->filter_prec != PSPW_PREC_F32)
     return fail(PSPW_ERR_ARG, "cheby_scf: unknown filter precision");
+  // precision of the filter and of the Lanczos bounds' H*v
+  const int fprec = p->filter_prec;
   const int kind = (p->imix == PSPW_MIX_KERKER || p->imix == PSPW_MIX_ANDERSON ||
                     p->imix == PSPW_MIX_PULAY || p->imix == PSPW_MIX_BROYDEN)
                        ? p->imix
@@ -150,7 +153,7 @@ extern "C" int pspw_cheby_scf(pspw_scf *s, const pspw_scf_params *p, const doubl
       !mem.get(&T, (size_t)nx2 * nx2) || !mem.get(&dv0, ngw) || !mem.get(&df, ngw) ||
       !mem.get(&dRT, (size_t)k * k) || !mem.get(&veff, nnr) || !mem.get(&rho, nnr) ||
       !mem.get(&wT, std::max(k, nx2)) || !mem.get(&dprec, ngw) ||
-      (p->filter_prec == PSPW_PREC_F32 && !mem.get(&Xf, (size_t)ngw * nx2)))
+      (fprec == PSPW_PREC_F32 && !mem.get(&Xf, (size_t)ngw * nx2)))
     return fail(PSPW_ERR_OOM, "cheby_scf: device memory");
   cudaStream_t st = c->stream;
   // rhoe2 = rho_old = the starting density (ChebySCFLoop.cpp:164-175)
@@ -171,7 +174,9 @@ extern "C" int pspw_cheby_scf(pspw_scf *s, const pspw_scf_params *p, const doubl
   if ((rc = pspw_cell_set_veff_device(c, veff, nnr))) return rc;
   // ---- Lanczos bounds (ChebySCFLoop.cpp:180-198)
   std::vector<double> rT((size_t)k * k, 0.0), evT(std::max(k, nx2));
-  if ((rc = lanczos_dev(c, dv0, ngw, k, rT.data(), k, df))) return rc;
+  // the bounds only shape the filter, so in the mixed mode their H*v
+  // products run in the filter's precision
+  if ((rc = lanczos_dev(c, dv0, ngw, k, rT.data(), k, df, fprec))) return rc;
   {
     double *dr;
     if (!mem.get(&dr, (size_t)k * k)) return fail(PSPW_ERR_OOM, "cheby_scf: device memory");
@@ -251,7 +256,7 @@ extern "C" int pspw_cheby_scf(pspw_scf *s, const pspw_scf_params *p, const doubl
     cudaEvent_t ev;
     // filter the NX+2 block (ChebySCFLoop.cpp:285)
     timing_begin(c, kFamScfFilter, &ev);
-    if (p->filter_prec == PSPW_PREC_F32) {
+    if (fprec == PSPW_PREC_F32) {
       const size_t n = (size_t)ngw * nx2;
       k_z2c<<<4 * 148, 256, 0, st>>>(X, Xf, n);
       if ((rc = pspw_chebyfilt_dev(c, PSPW_PREC_F32, Xf, ngw, ngw, nx2, p->degree, lb, ub)))
@@ -268,6 +273,10 @@ extern "C" int pspw_cheby_scf(pspw_scf *s, const pspw_scf_params *p, const doubl
     timing_end(c, kFamScfQr, ev);
     // Rayleigh-Ritz (ChebySCFLoop.cpp:293-307)
     timing_begin(c, kFamScfRayleigh, &ev);
+    // H X in FP64: the Ritz pairs (and through them the density) carry no
+    // FP32 rounding; with an FP32 H X the subspace matrix's error (~1e-6 Ha)
+    // divided by the occupied-empty gap keeps |dETOT| of a 64-atom cell
+    // above 1e-6
     if ((rc = hpsi_apply<double>(c, X, ngw, HX, ngw, ngw, nx2, 1.0, 0.0, 0.0, nullptr, ngw)))
       return rc;
     const double2 one = make_double2(1.0, 0.0), zero = make_double2(0.0, 0.0);
@@ -298,7 +307,7 @@ extern "C" int pspw_cheby_scf(pspw_scf *s, const pspw_scf_params *p, const doubl
     lb = evals[nx + 1];
     const int kl = k > 10 ? 10 : k;
     timing_begin(c, kFamScfLanczos, &ev);
-    if ((rc = lanczos_dev(c, dv0, ngw, kl, rT10.data(), k, df))) return rc;
+    if ((rc = lanczos_dev(c, dv0, ngw, kl, rT10.data(), k, df, fprec))) return rc;
     double fn = 0.0;
     if ((rc = dev_coldot(c, df, ngw, df, ngw, ngw, 1, dfn))) return rc;
     PSPW_CUDA(cudaMemcpyAsync(&fn, dfn, sizeof(double), cudaMemcpyDeviceToHost, st));

@@ -356,7 +356,8 @@ int lobpcg_dev(pspw_cell *c, int hprec, double *lambda_host, double2 *X, int nba
 }
 
 // ------------------------------------------------------------ Lanczos
-int lanczos_dev(pspw_cell *c, double2 *v0, int ngw, int k, double *T_host, int ldT, double2 *f_out) {
+int lanczos_dev(pspw_cell *c, double2 *v0, int ngw, int k, double *T_host, int ldT, double2 *f_out,
+                int hprec) {
   double2 *V, *Hv, *f, *h, *s, *ns;
   double *T, *nf;
   int rc;
@@ -378,7 +379,7 @@ int lanczos_dev(pspw_cell *c, double2 *v0, int ngw, int k, double *T_host, int l
       k_lanczos_next<<<gridn(ngw), 256, 0, c->stream>>>(f, vj, ngw, nf, T, k, j);
       c->kernel_launches++;
     }
-    if ((rc = apply_h(c, PSPW_PREC_F64, vj, Hv, ngw, 1))) return rc;
+    if ((rc = apply_h(c, hprec, vj, Hv, ngw, 1))) return rc;
     // h = V^H Hv; f = Hv - V h; s = V^H f; h += s; f -= V s (:60-87)
     const int nj = j + 1;
     if ((rc = zgemm<double>(c, 'C', nj, 1, ngw, kOne, V, ngw, Hv, ngw, kZero, h, nj)) ||

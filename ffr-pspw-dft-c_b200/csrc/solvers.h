@@ -14,8 +14,12 @@ int davidson_dev(pspw_cell *c, int hprec, double *evals_host, double2 *X, int nb
                  const double *d_prec, int nempty, int max_iter, double *res_host, int *iters);
 int lobpcg_dev(pspw_cell *c, int hprec, double *lambda_host, double2 *X, int nbasis, int nstates,
                const double *d_prec, int nempty, int max_iter, double *res_host, int *iters);
-// v0: device, normalised in place; T_host k x k (ldT); f_out device or null
-int lanczos_dev(pspw_cell *c, double2 *v0, int ngw, int k, double *T_host, int ldT, double2 *f_out);
+// v0: device, normalised in place; T_host k x k (ldT); f_out device or null.
+// hprec: precision of the H*v products (PSPW_PREC_F64 reproduces lanczos.cpp;
+// PSPW_PREC_F32 for bounds that only shape a filter); the recurrence, the
+// reorthogonalisation and T stay FP64.
+int lanczos_dev(pspw_cell *c, double2 *v0, int ngw, int k, double *T_host, int ldT, double2 *f_out,
+                int hprec = PSPW_PREC_F64);
 
 // EvalRhoPsi / EvalENL on device blocks (capi_solvers.cu); see pspw_gpu.h.
 int eval_rho_psi_dev(pspw_cell *c, const double2 *dX, int ld, int ngw, int nx, const double *focc,

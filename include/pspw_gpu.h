@@ -302,7 +302,8 @@ typedef struct {
   double kerker_q0;   /* KERKER_Q0 */
   int idiag;          /* IDIAG: >= 0 first iteration by Davidson, < 0 start from X */
   int max_diag_iter;  /* Davidson iteration cap; 0 = the reference's default */
-  int filter_prec;    /* PSPW_PREC_F64, or PSPW_PREC_F32 for the filter only */
+  int filter_prec;    /* PSPW_PREC_F64, or PSPW_PREC_F32 for the filter and the H*v
+                         products of the Lanczos filter bounds (the rest FP64) */
 } pspw_scf_params;
 int pspw_cheby_scf(pspw_scf *scf, const pspw_scf_params *params, const double *focc,
                    const double *rho_start, const double *v0, double *X, double *eig,
