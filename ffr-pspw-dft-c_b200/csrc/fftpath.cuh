@@ -449,9 +449,11 @@ int local_fast(pspw_cell *c, const FastGeo &g, const cx<R> *in, int ld_in, cx<R>
   const size_t s_band = (size_t)B.n3 * B.ncol;
   int nbatch = c->band_batch;
   if (nbatch <= 0) {
-    // at most ~48 MB of stick buffer per batch (it stays in L2), batches of
-    // equal size so no launch runs with a small tail batch
-    const int cap = (int)std::max<size_t>(1, (48u << 20) / (s_band * sizeof(T)));
+    // at most ~96 MB of stick buffer per batch (it stays in the 126 MB L2
+    // between the three passes; on Si64 one batch of 144 bands, 73 MB, runs
+    // the filter 4 % faster than two of 72), batches of equal size so no
+    // launch runs with a small tail batch
+    const int cap = (int)std::max<size_t>(1, (96u << 20) / (s_band * sizeof(T)));
     const int nbatches = (nb + cap - 1) / cap;
     nbatch = (nb + nbatches - 1) / nbatches;
   }

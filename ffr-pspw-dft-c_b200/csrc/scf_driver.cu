@@ -48,6 +48,21 @@ __global__ void k_real_to_z(const double *__restrict__ a, double2 *b, int k, int
   b[i] = make_double2(r <= col ? a[r + (size_t)lda * col] : 0.0, 0.0);
 }
 
+// column j of X (m rows, ld) scaled by 1/sqrt(d[j]) where d[j] > 0
+__global__ void k_unit_cols(double2 *X, int ld, int m, int n, const double *__restrict__ d) {
+  const size_t tot = (size_t)m * n;
+  for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < tot;
+       e += (size_t)gridDim.x * blockDim.x) {
+    const int j = (int)(e / m), i = (int)(e - (size_t)j * m);
+    const double dj = d[j];
+    if (dj > 0.0) {
+      const double s = 1.0 / sqrt(dj);
+      double2 *p = X + (size_t)j * ld + i;
+      *p = make_double2(s * p->x, s * p->y);
+    }
+  }
+}
+
 // ChebySCFLoop.cpp:7-34: |A v1|^2 with v1 = 1/sqrt(N) (ones), A the leading
 // N x N block of the lda-strided matrix
 double induced_norm_mat(const double *A, int lda, int N) {
@@ -71,10 +86,20 @@ double induced_norm_mat(const double *A, int lda, int N) {
 // panel sweeps).  Stable while cond(X) stays well below 1/sqrt(eps); the
 // ratio of the largest to the smallest diagonal of the first U bounds
 // cond(X) from below, and above 1e6 (or when the factorisation fails) the
-// block goes to the Householder QR instead.  G: n x n scratch (ld n).
-int span_orthonormalize(pspw_cell *c, double2 *X, int ngw, int n, double2 *G, int *info) {
+// block goes to the Householder QR instead.  The columns are first scaled to
+// unit norm (the span is unchanged): the filter multiplies the eigen-
+// components of its block by factors that span orders of magnitude, so the
+// filtered columns are nearly orthogonal but of very different lengths, an
+// ill-conditioning that the scaling removes.  G: n x n scratch (ld n);
+// dn: n doubles of scratch.
+int span_orthonormalize(pspw_cell *c, double2 *X, int ngw, int n, double2 *G, double *dn,
+                        int *info) {
   const double2 one = make_double2(1.0, 0.0), zero = make_double2(0.0, 0.0);
   int rc;
+  if ((rc = dev_coldot(c, X, ngw, X, ngw, ngw, n, dn))) return rc;
+  k_unit_cols<<<4 * 148, 256, 0, c->stream>>>(X, ngw, ngw, n, dn);
+  c->kernel_launches++;
+  PSPW_CUDA(cudaGetLastError());
   for (int pass = 0; pass < 2; pass++) {
     if ((rc = zgemm<double>(c, 'C', n, n, ngw, one, X, ngw, X, ngw, zero, G, n))) return rc;
     int pinfo = 0;
@@ -148,8 +173,8 @@ extern "C" int pspw_cheby_scf(pspw_scf *s, const pspw_scf_params *p, const doubl
   DevBuf mem;
   double2 *X, *HX, *T, *dv0, *df, *dRT;
   float2 *Xf = nullptr;
-  double *veff, *rho, *wT, *dprec;
-  if (!mem.get(&X, (size_t)ngw * nx2) || !mem.get(&HX, (size_t)ngw * nx2) ||
+  double *veff, *rho, *wT, *dprec, *dcn;
+  if (!mem.get(&X, (size_t)ngw * nx2) || !mem.get(&dcn, nx2) || !mem.get(&HX, (size_t)ngw * nx2) ||
       !mem.get(&T, (size_t)nx2 * nx2) || !mem.get(&dv0, ngw) || !mem.get(&df, ngw) ||
       !mem.get(&dRT, (size_t)k * k) || !mem.get(&veff, nnr) || !mem.get(&rho, nnr) ||
       !mem.get(&wT, std::max(k, nx2)) || !mem.get(&dprec, ngw) ||
@@ -269,7 +294,7 @@ extern "C" int pspw_cheby_scf(pspw_scf *s, const pspw_scf_params *p, const doubl
     timing_end(c, kFamScfFilter, ev);
     int info = 0;
     timing_begin(c, kFamScfQr, &ev);
-    if ((rc = span_orthonormalize(c, X, ngw, nx2, T, &info))) return rc;
+    if ((rc = span_orthonormalize(c, X, ngw, nx2, T, dcn, &info))) return rc;
     timing_end(c, kFamScfQr, ev);
     // Rayleigh-Ritz (ChebySCFLoop.cpp:293-307)
     timing_begin(c, kFamScfRayleigh, &ev);
