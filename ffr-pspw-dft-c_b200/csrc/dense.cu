@@ -24,6 +24,13 @@ int solver_handle(pspw_cell *c, cusolverDnHandle_t *h) {
     cusolverDnHandle_t s;
     if (cusolverDnCreate(&s) != CUSOLVER_STATUS_SUCCESS)
       return fail(PSPW_ERR_CUDA, "cusolverDnCreate failed");
+    // the same bits on every run: the SCF loop's stopping iteration depends
+    // on differences far below the results' own accuracy
+    if (cusolverDnSetDeterministicMode(s, CUSOLVER_DETERMINISTIC_RESULTS) !=
+        CUSOLVER_STATUS_SUCCESS) {
+      cusolverDnDestroy(s);
+      return fail(PSPW_ERR_CUDA, "cusolverDnSetDeterministicMode failed");
+    }
     c->cusolver = s;
   }
   *h = static_cast<cusolverDnHandle_t>(c->cusolver);
@@ -36,6 +43,10 @@ int blas_handle(pspw_cell *c, cublasHandle_t *h) {
   if (!c->cublas) {
     cublasHandle_t s;
     if (cublasCreate(&s) != CUBLAS_STATUS_SUCCESS) return fail(PSPW_ERR_CUDA, "cublasCreate failed");
+    if (cublasSetAtomicsMode(s, CUBLAS_ATOMICS_NOT_ALLOWED) != CUBLAS_STATUS_SUCCESS) {
+      cublasDestroy(s);
+      return fail(PSPW_ERR_CUDA, "cublasSetAtomicsMode failed");
+    }
     c->cublas = s;
   }
   *h = static_cast<cublasHandle_t>(c->cublas);
