@@ -264,12 +264,16 @@ __global__ void k_species_sum(const double2 *__restrict__ sfac, const double *__
 }
 
 // qat(G) = sum_s q_s(|G|) SFAC(s, G) placed on the grid point of G
-// (FormFactorAtomic.cpp:139-160)
+// (FormFactorAtomic.cpp:139-160); where density G alias onto one grid point
+// (a grid smaller than the density sphere needs), the reference's loop in G
+// order leaves the last one's value, so only that one writes
 __global__ void k_atomic_grid(const double *__restrict__ qa, const double *__restrict__ qa0,
                               int nshell, const int *__restrict__ shell_of,
                               const double2 *__restrict__ sfac, const int *__restrict__ gidx,
-                              int ng, int nsp, double2 *grid) {
+                              const unsigned char *__restrict__ last, int ng, int nsp,
+                              double2 *grid) {
   for (int ig = blockIdx.x * blockDim.x + threadIdx.x; ig < ng; ig += gridDim.x * blockDim.x) {
+    if (!last[ig]) continue;
     double re = 0.0, im = 0.0;
     for (int s = 0; s < nsp; s++) {
       const double q = ig == 0 ? qa0[s] : qa[(size_t)s * nshell + shell_of[ig]];
@@ -700,7 +704,8 @@ int system_build(pspw_system *S, const std::string &dir) {
   }
   PSPW_CUDA(cudaMemcpyAsync(d_qa0, qa0.data(), sizeof(double) * nsp, cudaMemcpyHostToDevice, cst));
   PSPW_CUDA(cudaMemsetAsync(S->scf->d_grid, 0, sizeof(double2) * (size_t)S->nnr, cst));
-  k_atomic_grid<<<gb, 256, 0, cst>>>(d_qa, d_qa0, ngs, d_gof, S->d_sfac, S->scf->d_gidx, ng, nsp,
+  k_atomic_grid<<<gb, 256, 0, cst>>>(d_qa, d_qa0, ngs, d_gof, S->d_sfac, S->scf->d_gidx,
+                                     S->scf->d_glast, ng, nsp,
                                      S->scf->d_grid);
   PSPW_CUDA(cudaGetLastError());
   if ((rc = grid_fft(S->cell, S->scf->d_grid, +1))) return rc;

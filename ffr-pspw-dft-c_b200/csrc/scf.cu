@@ -168,8 +168,9 @@ __device__ __forceinline__ double2 cj(double2 a) { return make_double2(a.x, -a.y
 // transformed density, as in the reference (it scatters vtemp into c_fft
 // without clearing it, EvalEnergy.cpp:115-118).
 __global__ void __launch_bounds__(kRedThreads) k_energy_terms(
-    double2 *grid, const int *__restrict__ gidx, const double *__restrict__ g,
-    const double2 *__restrict__ vp, const double2 *__restrict__ rp, int ng, double tpiba2,
+    const double2 *__restrict__ grid, const int *__restrict__ gidx,
+    const double *__restrict__ g, const double2 *__restrict__ vp,
+    const double2 *__restrict__ rp, int ng, double tpiba2, double2 *__restrict__ vg,
     double *part) {
   double v[8] = {0, 0, 0, 0, 0, 0, 0, 0};  // eh, eh2, eg2, eps (re, im)
   const double fourpi = 4.0 * M_PI;
@@ -181,7 +182,7 @@ __global__ void __launch_bounds__(kRedThreads) k_energy_terms(
       const double2 e0 = cm(vpg, cj(rhet));  // eps = vp * conj(c_fft[0])
       v[6] += e0.x;
       v[7] += e0.y;
-      grid[idx] = vpg;  // vtemp[0] = vp + vh0, vh0 = 0
+      vg[ig] = vpg;  // vtemp[0] = vp + vh0, vh0 = 0
       continue;
     }
     const double2 rpg = rp[ig];
@@ -201,9 +202,18 @@ __global__ void __launch_bounds__(kRedThreads) k_energy_terms(
     v[5] += t3.y;
     v[6] += t4.x;
     v[7] += t4.y;
-    grid[idx] = make_double2(vcg.x + vpg.x, vcg.y + vpg.y);
+    vg[ig] = make_double2(vcg.x + vpg.x, vcg.y + vpg.y);
   }
   block_reduce_store<8>(v, part);
+}
+
+// c_fft(G) = vtemp(G) in G order (EvalEnergy.cpp:117-119): where density G
+// alias onto one grid point the last one's value stays, so only it writes.
+// A separate pass after k_energy_terms, which reads every rho(G) first.
+__global__ void k_scatter_last(const double2 *__restrict__ vg, const int *__restrict__ gidx,
+                               const unsigned char *__restrict__ last, int ng, double2 *grid) {
+  for (int ig = blockIdx.x * blockDim.x + threadIdx.x; ig < ng; ig += gridDim.x * blockDim.x)
+    if (last[ig]) grid[gidx[ig]] = vg[ig];
 }
 
 // ---------------------------------------------------------------- xc_PZ
@@ -429,8 +439,11 @@ int eval_energy_dev(pspw_scf *s, double *d_rho, double ekin, double enl, double 
   int rc = grid_fft(c, s->d_grid, -1);
   if (rc) return rc;
   k_energy_terms<<<kRedBlocks, kRedThreads, 0, c->stream>>>(s->d_grid, s->d_gidx, s->d_g, s->d_vp,
-                                                            s->d_rp, s->ng, c->tpiba2, s->d_part);
-  c->kernel_launches++;
+                                                            s->d_rp, s->ng, c->tpiba2, s->d_vg,
+                                                            s->d_part);
+  k_scatter_last<<<launch_blocks(s->ng), 256, 0, c->stream>>>(s->d_vg, s->d_gidx, s->d_glast,
+                                                              s->ng, s->d_grid);
+  c->kernel_launches += 2;
   PSPW_CUDA(cudaGetLastError());
   double t[8];
   if ((rc = finish_reduce<8>(s, t))) return rc;
@@ -714,6 +727,13 @@ int pspw_scf_create(pspw_cell *c, int ng, const int *n1, const int *n2, const in
     rp[ig] = make_double2(rr, ri);
   }
   if (gidx[0] != 0) return fail(PSPW_ERR_SHAPE, "scf_create: the first G must be G = 0");
+  // the last density G on each grid point (aliasing on small grids)
+  std::vector<unsigned char> glast(ng, 0);
+  {
+    std::vector<int> last_of(B.nnr, -1);
+    for (int ig = 0; ig < ng; ig++) last_of[gidx[ig]] = ig;
+    for (int ig = 0; ig < ng; ig++) glast[ig] = last_of[gidx[ig]] == ig;
+  }
   pspw_scf *s = new pspw_scf;
   s->cell = c;
   s->device = c->device;
@@ -728,6 +748,8 @@ int pspw_scf_create(pspw_cell *c, int ng, const int *n1, const int *n2, const in
             cudaMalloc(&s->d_g, sizeof(double) * ng) == cudaSuccess &&
             cudaMalloc(&s->d_vp, sizeof(double2) * ng) == cudaSuccess &&
             cudaMalloc(&s->d_rp, sizeof(double2) * ng) == cudaSuccess &&
+            cudaMalloc(&s->d_glast, ng) == cudaSuccess &&
+            cudaMalloc(&s->d_vg, sizeof(double2) * ng) == cudaSuccess &&
             cudaMalloc(&s->d_grid, sizeof(double2) * nnr) == cudaSuccess &&
             cudaMalloc(&s->d_vxc, sizeof(double) * nnr) == cudaSuccess &&
             cudaMalloc(&s->d_tmp, sizeof(double) * nnr) == cudaSuccess &&
@@ -736,6 +758,7 @@ int pspw_scf_create(pspw_cell *c, int ng, const int *n1, const int *n2, const in
             cudaMallocHost(&s->h_part, sizeof(double) * 16) == cudaSuccess;
   if (ok)
     ok = cudaMemcpy(s->d_gidx, gidx.data(), sizeof(int) * ng, cudaMemcpyHostToDevice) == cudaSuccess &&
+         cudaMemcpy(s->d_glast, glast.data(), ng, cudaMemcpyHostToDevice) == cudaSuccess &&
          cudaMemcpy(s->d_g, g, sizeof(double) * ng, cudaMemcpyHostToDevice) == cudaSuccess &&
          cudaMemcpy(s->d_vp, vp.data(), sizeof(double2) * ng, cudaMemcpyHostToDevice) == cudaSuccess &&
          cudaMemcpy(s->d_rp, rp.data(), sizeof(double2) * ng, cudaMemcpyHostToDevice) == cudaSuccess;
@@ -754,7 +777,7 @@ int pspw_scf_destroy(pspw_scf *s) {
   // synchronised instead of the cell's stream
   cudaSetDevice(s->device);
   cudaDeviceSynchronize();
-  void *p[] = {s->d_gidx, s->d_g, s->d_vp, s->d_rp, s->d_grid, s->d_vxc,
+  void *p[] = {s->d_gidx, s->d_glast, s->d_vg, s->d_g, s->d_vp, s->d_rp, s->d_grid, s->d_vxc,
                s->d_tmp,  s->d_part, s->d_hist, s->d_f, s->d_gm};
   for (void *q : p)
     if (q) cudaFree(q);

@@ -13,6 +13,11 @@ struct pspw_scf {
   int ng = 0, nsp = 0;
   double omega = 0.0, nel = 0.0, esr = 0.0, eself = 0.0;
   int *d_gidx = nullptr;    // [ng] 0-based grid index of density G ig
+  // [ng] 1 where ig is the last density G on its grid point: on a grid
+  // smaller than the density sphere needs, several G alias onto one point and
+  // the reference's sequential scatters leave the last one's value there
+  unsigned char *d_glast = nullptr;
+  double2 *d_vg = nullptr;  // [ng] V_H + V_loc per density G (EvalEnergy)
   double *d_g = nullptr;    // [ng] |G|^2 in (2 pi / alat)^2 units (G[0] = 0)
   double2 *d_vp = nullptr;  // [ng] sum_s SFAC(s,ig) VPS(s,ig)
   double2 *d_rp = nullptr;  // [ng] sum_s SFAC(s,ig) RHOPS(s,ig)

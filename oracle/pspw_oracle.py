@@ -512,7 +512,11 @@ def eval_energy(rho, local, cell, ekin, enl):
     eh = np.sum(0.5 * vcg * np.conj(rhog))
     eps = eps + np.sum(np.conj(rhet) * vp[1:])
     vtemp = np.concatenate([[vp[0]], vcg + vp[1:]])
+    # scatter in G order (EvalEnergy.cpp:117-119): on a grid smaller than the
+    # density sphere needs, G alias onto one point and the last one stays
     c[gidx] = vtemp
+    last = len(gidx) - 1 - np.unique(np.asarray(gidx)[::-1], return_index=True)[1]
+    c[np.asarray(gidx)[last]] = vtemp[last]
     v = fft_inverse(c, nr)
     vxc, exc = xc_pz(rho)
     veff = v.real + vxc

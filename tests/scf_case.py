@@ -6,11 +6,11 @@ import numpy as np
 from ref_lib import RefLib
 
 
-def make_case(ecut_ry=10.0, seed=7):
+def make_case(ecut_ry=10.0, seed=7, grid=None):
     from pspw import synth
     lat, pos = synth.si_diamond(1)
     R = RefLib("libref.so")
-    b = R.setup(lat, ecut_ry, None, [8], [pos], [4.0], [3], [3], 4)
+    b = R.setup(lat, ecut_ry, grid, [8], [pos], [4.0], [3], [3], 4)
     pkg_a, wnl = synth.kb_form_factors(b, lat)
     R.set_nl(pkg_a, wnl)
     b.update(pkg_a=pkg_a, wnl=wnl)
