@@ -210,23 +210,52 @@ int pspw_chebyfilt(pspw_cell *c, double *X, int ngw, int nstates, int degree, do
   if (rc) return rc;
   if (!X) return fail(PSPW_ERR_ARG, "chebyfilt: null block");
   if (nstates <= 0) return PSPW_OK;
+  if (prec != PSPW_PREC_F64 && prec != PSPW_PREC_F32)
+    return fail(PSPW_ERR_ARG, "unknown precision");
   const size_t n = (size_t)ngw * nstates;
   double2 *dx = nullptr;
+  float2 *fx = nullptr;
   if ((rc = ws_reserve(c, 4, n * sizeof(double2), (void **)&dx))) return rc;
-  PSPW_CUDA(cudaMemcpyAsync(dx, X, n * sizeof(double2), cudaMemcpyHostToDevice, c->stream));
-  if (prec == PSPW_PREC_F32) {
-    float2 *fx = nullptr;
-    if ((rc = ws_reserve(c, 8, n * sizeof(float2), (void **)&fx))) return rc;
-    k_z_to_c<<<4 * 148, 256, 0, c->stream>>>(dx, ngw, fx, ngw, ngw, nstates);
-    c->kernel_launches++;
-    if ((rc = pspw_chebyfilt_dev(c, PSPW_PREC_F32, fx, ngw, ngw, nstates, degree, lb, ub))) return rc;
-    k_c_to_z<<<4 * 148, 256, 0, c->stream>>>(fx, ngw, dx, ngw, ngw, nstates);
-    c->kernel_launches++;
-  } else {
-    if ((rc = pspw_chebyfilt_dev(c, PSPW_PREC_F64, dx, ngw, ngw, nstates, degree, lb, ub))) return rc;
+  if (prec == PSPW_PREC_F32 && (rc = ws_reserve(c, 8, n * sizeof(float2), (void **)&fx)))
+    return rc;
+  // Bands are independent under the filter, so the block goes in two band
+  // chunks: the copy stream brings chunk 1 in while the cell stream filters
+  // chunk 0, and takes chunk 0 out while it filters chunk 1 (a block of fewer
+  // than 32 bands goes whole).  Each chunk's copies and its filter are
+  // ordered by events; the call returns after the last copy out.
+  const int nchunk = nstates >= 32 ? 2 : 1;
+  const int b_split = (nstates + 1) / 2;
+  const int b0[2] = {0, nchunk == 2 ? b_split : nstates};
+  const int nbc[2] = {nchunk == 2 ? b_split : nstates, nstates - b_split};
+  cudaStream_t cs = c->stream_copy;
+  double2 *hX = reinterpret_cast<double2 *>(X);
+  for (int k = 0; k < nchunk; k++) {
+    const size_t off = (size_t)b0[k] * ngw, bytes = sizeof(double2) * (size_t)nbc[k] * ngw;
+    PSPW_CUDA(cudaMemcpyAsync(dx + off, hX + off, bytes, cudaMemcpyHostToDevice, cs));
+    PSPW_CUDA(cudaEventRecord(c->ev_in[k], cs));
   }
-  PSPW_CUDA(cudaMemcpyAsync(X, dx, n * sizeof(double2), cudaMemcpyDeviceToHost, c->stream));
+  for (int k = 0; k < nchunk && rc == PSPW_OK; k++) {
+    const size_t off = (size_t)b0[k] * ngw, bytes = sizeof(double2) * (size_t)nbc[k] * ngw;
+    PSPW_CUDA(cudaStreamWaitEvent(c->stream, c->ev_in[k], 0));
+    if (prec == PSPW_PREC_F32) {
+      k_z_to_c<<<4 * 148, 256, 0, c->stream>>>(dx + off, ngw, fx + off, ngw, ngw, nbc[k]);
+      c->kernel_launches++;
+      rc = pspw_chebyfilt_dev(c, PSPW_PREC_F32, fx + off, ngw, ngw, nbc[k], degree, lb, ub);
+      if (rc) break;
+      k_c_to_z<<<4 * 148, 256, 0, c->stream>>>(fx + off, ngw, dx + off, ngw, ngw, nbc[k]);
+      c->kernel_launches++;
+    } else {
+      rc = pspw_chebyfilt_dev(c, PSPW_PREC_F64, dx + off, ngw, ngw, nbc[k], degree, lb, ub);
+      if (rc) break;
+    }
+    PSPW_CUDA(cudaEventRecord(c->ev_out[k], c->stream));
+    PSPW_CUDA(cudaStreamWaitEvent(cs, c->ev_out[k], 0));
+    PSPW_CUDA(cudaMemcpyAsync(hX + off, dx + off, bytes, cudaMemcpyDeviceToHost, cs));
+  }
+  // no copy may still be writing the caller's block when this returns
+  PSPW_CUDA(cudaStreamSynchronize(cs));
   PSPW_CUDA(cudaStreamSynchronize(c->stream));
+  if (rc) return rc;
   return device_status(c);
 }
 

@@ -209,6 +209,7 @@ int pspw_cell_destroy(pspw_cell *c) {
   cudaSetDevice(c->device);
   if (c->stream) cudaStreamSynchronize(c->stream);
   if (c->stream2) cudaStreamSynchronize(c->stream2);
+  if (c->stream_copy) cudaStreamSynchronize(c->stream_copy);
   Basis &B = c->basis;
   void *ptrs[] = {B.d_col_start, B.d_sg_ig, B.d_sg_z, B.d_sg_col, B.d_col_of_xy, B.d_xa_list,
                   B.d_xa_of_x, B.d_kin64, B.d_kin32, B.d_xkg64, c->proj.d_eigr64, c->proj.d_eigr32,
@@ -238,6 +239,11 @@ int pspw_cell_destroy(pspw_cell *c) {
   if (c->stream2) cudaStreamDestroy(c->stream2);
   if (c->ev_fork) cudaEventDestroy(c->ev_fork);
   if (c->ev_join) cudaEventDestroy(c->ev_join);
+  if (c->stream_copy) cudaStreamDestroy(c->stream_copy);
+  for (int i = 0; i < 2; i++) {
+    if (c->ev_in[i]) cudaEventDestroy(c->ev_in[i]);
+    if (c->ev_out[i]) cudaEventDestroy(c->ev_out[i]);
+  }
   delete c;
   return PSPW_OK;
 }
@@ -316,6 +322,12 @@ int cell_create(pspw_cell **out, int device, int nr1, int nr2, int nr3, int ngw,
       cudaEventCreateWithFlags(&c->ev_fork, cudaEventDisableTiming) != cudaSuccess ||
       cudaEventCreateWithFlags(&c->ev_join, cudaEventDisableTiming) != cudaSuccess)
     return bail(fail(PSPW_ERR_CUDA, "cell_create: projection stream"));
+  if (cudaStreamCreateWithFlags(&c->stream_copy, cudaStreamNonBlocking) != cudaSuccess)
+    return bail(fail(PSPW_ERR_CUDA, "cell_create: copy stream"));
+  for (int i = 0; i < 2; i++)
+    if (cudaEventCreateWithFlags(&c->ev_in[i], cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&c->ev_out[i], cudaEventDisableTiming) != cudaSuccess)
+      return bail(fail(PSPW_ERR_CUDA, "cell_create: copy events"));
   if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess)
     return bail(fail(PSPW_ERR_CUDA, "cell_create: stream"));
   Basis &B = c->basis;

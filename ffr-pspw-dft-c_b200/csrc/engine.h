@@ -152,6 +152,10 @@ struct pspw_cell {
   // part of H*psi (fork and join events on the cell stream)
   cudaStream_t stream2 = nullptr;
   cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
+  // copy stream of the host-facing filter, which moves band chunks in and out
+  // while the cell stream filters the other chunk (events per chunk)
+  cudaStream_t stream_copy = nullptr;
+  cudaEvent_t ev_in[2] = {nullptr, nullptr}, ev_out[2] = {nullptr, nullptr};
   int ngwx = 0;
   double tpiba2 = 0.0;
   int band_batch = 0;

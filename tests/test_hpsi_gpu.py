@@ -193,6 +193,21 @@ def test_chebyfilt_fp32(cfg0):
     assert relmax(out, ref) < 1e-4
 
 
+@pytest.mark.parametrize("prec,tol", [(PREC_F64, TOL64), (PREC_F32, 1e-4)])
+def test_chebyfilt_host_block_in_two_chunks(cfg0, prec, tol):
+    # 37 bands (>= 32): the host-facing filter moves the block in two band
+    # chunks (19 + 18) on a copy stream while the cell stream filters the
+    # other chunk; every band still gets the whole filter
+    w, cell = cfg0
+    rng = np.random.default_rng(11)
+    psi = w["psi"]
+    X = np.asfortranarray(psi[:, rng.integers(0, psi.shape[1], 37)]
+                          * (1.0 + 0.1 * rng.standard_normal(37)))
+    out = cell.chebyfilt(X, 4, 1.5, 5.0, prec)
+    ref = O.chebyfilt(oracle_cell(w), X, 4, 1.5, 5.0, w["veff"])
+    assert relmax(out, ref) < tol
+
+
 def test_chebyfilt_fewer_plane_waves_than_the_cell(cfg0):
     # NGW_ik below the cell's sphere: the filter stays in the caller's G order
     w, cell = cfg0
