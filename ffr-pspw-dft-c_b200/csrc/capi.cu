@@ -234,8 +234,12 @@ int pspw_chebyfilt(pspw_cell *c, double *X, int ngw, int nstates, int degree, do
     PSPW_CUDA(cudaMemcpyAsync(dx + off, hX + off, bytes, cudaMemcpyHostToDevice, cs));
     PSPW_CUDA(cudaEventRecord(c->ev_in[k], cs));
   }
+  // every chunk's filter is enqueued before the copies out, so a copy into
+  // pageable host memory (which returns only when done) still overlaps the
+  // next chunk's filter
+  int nready = 0;
   for (int k = 0; k < nchunk && rc == PSPW_OK; k++) {
-    const size_t off = (size_t)b0[k] * ngw, bytes = sizeof(double2) * (size_t)nbc[k] * ngw;
+    const size_t off = (size_t)b0[k] * ngw;
     PSPW_CUDA(cudaStreamWaitEvent(c->stream, c->ev_in[k], 0));
     if (prec == PSPW_PREC_F32) {
       k_z_to_c<<<4 * 148, 256, 0, c->stream>>>(dx + off, ngw, fx + off, ngw, ngw, nbc[k]);
@@ -249,6 +253,10 @@ int pspw_chebyfilt(pspw_cell *c, double *X, int ngw, int nstates, int degree, do
       if (rc) break;
     }
     PSPW_CUDA(cudaEventRecord(c->ev_out[k], c->stream));
+    nready = k + 1;
+  }
+  for (int k = 0; k < nready && rc == PSPW_OK; k++) {
+    const size_t off = (size_t)b0[k] * ngw, bytes = sizeof(double2) * (size_t)nbc[k] * ngw;
     PSPW_CUDA(cudaStreamWaitEvent(cs, c->ev_out[k], 0));
     PSPW_CUDA(cudaMemcpyAsync(hX + off, dx + off, bytes, cudaMemcpyDeviceToHost, cs));
   }
