@@ -457,9 +457,10 @@ def run_eigsolve(args, rank, world, local_rank):
     device, each run for `--steps` iterations from the reference's own
     random start (random_col), with H*psi and the preconditioner in FP64 and
     in FP32; orthonormalisation, Gram matrices and the subspace eigensolves
-    are FP64 in both.  Eigenvalues of the states the FP64 run resolves
-    (residual < 1e-3) are compared between the two.  value = LOBPCG
-    iterations per second with FP32 H*psi."""
+    are FP64 in both.  Eigenvalues of the states both runs resolve
+    (residual below 1e-4, 1e-3, 1e-2) are compared between the two.
+    --solvers picks the solvers (default both).  value = iterations per
+    second of the first solver with FP32 H*psi."""
     import torch
     from pspw import PREC_F32, PREC_F64, replica, workloads
     torch.cuda.set_device(local_rank)
@@ -474,7 +475,7 @@ def run_eigsolve(args, rank, world, local_rank):
     cell.davidson(ngw, nb, prec, nempty, max_iter=1, hprec=PREC_F32)
     replica.barrier()
     clocks.start()
-    for solver in ("lobpcg", "davidson"):
+    for solver in args.solvers.split(","):
         run = getattr(cell, solver)
         res = {}
         for name, hp in (("fp64", PREC_F64), ("fp32", PREC_F32)):
@@ -482,16 +483,16 @@ def run_eigsolve(args, rank, world, local_rank):
             t0 = time.perf_counter()
             ev, _, r, it = run(ngw, nb, prec, nempty, max_iter=iters, hprec=hp)
             res[name] = (time.perf_counter() - t0, ev, r, it)
-        r64 = res["fp64"][2]
+        r64 = np.maximum(res["fp64"][2], res["fp32"][2])  # both runs resolve the state
         d = np.abs(res["fp64"][1] - res["fp32"][1])
         out_modes[solver] = {
             m: {"seconds": round(v[0], 3), "iterations": v[3],
                 "ms_per_iteration": round(v[0] * 1e3 / max(1, v[3]), 2)}
             for m, v in res.items()}
-        out_modes[solver]["residual_fp64_min_median_max"] = [float(np.min(r64)),
-                                                              float(np.median(r64)),
-                                                              float(np.max(r64))]
-        for tol in (1e-3, 1e-2):
+        out_modes[solver]["residual_min_median_max"] = [float(np.min(r64)),
+                                                         float(np.median(r64)),
+                                                         float(np.max(r64))]
+        for tol in (1e-4, 1e-3, 1e-2):
             ok = r64 < tol
             out_modes[solver][f"states_res_below_{tol:g}"] = int(ok.sum())
             out_modes[solver][f"eig_max_error_ha_res_below_{tol:g}"] = (
@@ -500,11 +501,12 @@ def run_eigsolve(args, rank, world, local_rank):
         out_modes[solver]["speedup_fp32_vs_fp64"] = round(res["fp64"][0] / res["fp32"][0], 3)
     clocks.stop()
     cell.close()
-    lob = out_modes["lobpcg"]["fp32"]
+    lob = out_modes[args.solvers.split(",")[0]]["fp32"]
     t_it = replica.max_over_ranks(lob["seconds"] / max(1, lob["iterations"]))
     if rank == 0:
         print(json.dumps({
-            "metric": "Si216 LOBPCG iterations/s, FP32 H*psi, FP64 subspace steps",
+            "metric": f"Si216 {args.solvers.split(',')[0]} iterations/s, FP32 H*psi, FP64 "
+                      "subspace steps",
             "value": round(world / t_it, 4), "unit": "iterations/s", "n_gpus": world,
             "steps": iters, "warmup": 1, "ms_per_step": round(t_it * 1e3, 2),
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
@@ -714,6 +716,8 @@ def main():
     ap.add_argument("--workload", default="si64")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--solvers", default="lobpcg,davidson",
+                    help="eig-si216: comma-separated solvers (lobpcg, davidson)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
 
