@@ -165,6 +165,64 @@ __global__ void __launch_bounds__(256) k_zgemm_n8(int m, int n, int k, cx<R> alp
   }
 }
 
+// Single-column products (the Lanczos recurrence: V^H v and v - V h with a
+// few columns V).  y = A^H x: one block per output, each thread sums a
+// strided slice of the k products with four partial sums, then a fixed-order
+// warp and block reduction.
+template <typename R>
+__global__ void __launch_bounds__(512) k_gemv_c(int k, cx<R> alpha, const cx<R> *__restrict__ A,
+                                                int lda, const cx<R> *__restrict__ x, cx<R> beta,
+                                                cx<R> *y) {
+  using T = cx<R>;
+  __shared__ T red[16];
+  const int j = blockIdx.x, nt = blockDim.x;
+  const T *a = A + (size_t)j * lda;
+  T s0 = czero<T>(), s1 = czero<T>(), s2 = czero<T>(), s3 = czero<T>();
+  int i = threadIdx.x;
+  for (; i + 3 * nt < k; i += 4 * nt) {
+    cfmac(s0, a[i], x[i]);
+    cfmac(s1, a[i + nt], x[i + nt]);
+    cfmac(s2, a[i + 2 * nt], x[i + 2 * nt]);
+    cfmac(s3, a[i + 3 * nt], x[i + 3 * nt]);
+  }
+  for (; i < k; i += nt) cfmac(s0, a[i], x[i]);
+  T t = (s0 + s1) + (s2 + s3);
+  for (int o = 16; o > 0; o >>= 1) {
+    t.x += __shfl_down_sync(0xffffffffu, t.x, o);
+    t.y += __shfl_down_sync(0xffffffffu, t.y, o);
+  }
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  if (lane == 0) red[warp] = t;
+  __syncthreads();
+  if (warp == 0) {
+    t = lane < (nt >> 5) ? red[lane] : czero<T>();
+    for (int o = 16; o > 0; o >>= 1) {
+      t.x += __shfl_down_sync(0xffffffffu, t.x, o);
+      t.y += __shfl_down_sync(0xffffffffu, t.y, o);
+    }
+    if (lane == 0) {
+      T r = cmul(alpha, t);
+      if (beta.x != (R)0 || beta.y != (R)0) r = r + cmul(beta, y[j]);
+      y[j] = r;
+    }
+  }
+}
+
+// y = alpha A x + beta y for A with few columns: one thread per row, the
+// columns summed in order
+template <typename R>
+__global__ void k_gemv_n(int m, int k, cx<R> alpha, const cx<R> *__restrict__ A, int lda,
+                         const cx<R> *__restrict__ x, cx<R> beta, cx<R> *y) {
+  using T = cx<R>;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < m; i += gridDim.x * blockDim.x) {
+    T s = czero<T>();
+    for (int j = 0; j < k; j++) cfma(s, A[(size_t)j * lda + i], x[j]);
+    T r = cmul(alpha, s);
+    if (beta.x != (R)0 || beta.y != (R)0) r = r + cmul(beta, y[i]);
+    y[i] = r;
+  }
+}
+
 template <typename R>
 __global__ void k_zgemm_reduce(int m, int n, int nsplit, const cx<R> *__restrict__ part,
                                cx<R> alpha, cx<R> beta, cx<R> *C, int ldc) {
@@ -237,6 +295,20 @@ int zgemm(pspw_cell *c, char opa, int m, int n, int k, cx<R> alpha, const cx<R> 
     }
   }
   cudaStream_t st = c->stream;
+  if (n == 1 && k > 0) {
+    // one column: matrix-vector kernels (the Lanczos recurrence)
+    cudaEvent_t ev;
+    timing_begin(c, kFamGemm, &ev);
+    if (opa == 'C' || opa == 'c')
+      k_gemv_c<R><<<m, 512, 0, st>>>(k, alpha, A, lda, B, beta, C);
+    else
+      k_gemv_n<R><<<(unsigned)std::min<long long>(((long long)m + 255) / 256, 4 * 148), 256, 0,
+                    st>>>(m, k, alpha, A, lda, B, beta, C);
+    c->kernel_launches++;
+    timing_end(c, kFamGemm, ev);
+    PSPW_CUDA(cudaGetLastError());
+    return PSPW_OK;
+  }
   constexpr int BK = sizeof(R) == 8 ? 16 : 32;
   const bool conj = (opa == 'C' || opa == 'c');
   const int mt = (m + kGM - 1) / kGM, nt = (n + kGN - 1) / kGN;
