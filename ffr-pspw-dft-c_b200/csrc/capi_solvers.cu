@@ -12,6 +12,7 @@
 #include "dense.h"
 #include "engine.h"
 #include "fftpath.h"
+#include "gemm.h"
 #include "solvers.h"
 
 namespace pspw {
@@ -403,3 +404,21 @@ int pspw_eval_enl_dev(pspw_cell *c, const double *d_c0, int ld, int ngw, int nx,
 }
 
 }  // extern "C"
+
+extern "C" int pspw_zgemm_dev(pspw_cell *c, char opa, int m, int n, int k, const double *alpha,
+                              const double *d_A, int lda, const double *d_B, int ldb,
+                              const double *beta, double *d_C, int ldc) {
+  int rc = enter(c);
+  if (rc) return rc;
+  if (!alpha || !beta || m < 0 || n < 0 || k < 0)
+    return fail(PSPW_ERR_ARG, "zgemm_dev: bad arguments");
+  if (m == 0 || n == 0) return PSPW_OK;
+  const bool conj = opa == 'C' || opa == 'c';
+  if (!d_A || !d_B || !d_C || lda < std::max(1, conj ? k : m) || ldb < std::max(1, k) ||
+      ldc < m)
+    return fail(PSPW_ERR_ARG, "zgemm_dev: null matrix or leading dimension too small");
+  return zgemm<double>(c, opa, m, n, k, make_double2(alpha[0], alpha[1]),
+                       reinterpret_cast<const double2 *>(d_A), lda,
+                       reinterpret_cast<const double2 *>(d_B), ldb,
+                       make_double2(beta[0], beta[1]), reinterpret_cast<double2 *>(d_C), ldc);
+}

@@ -677,6 +677,12 @@ int pspw_cell_set_nl_path(pspw_cell *c, int path) {
   return PSPW_OK;
 }
 
+int pspw_cell_check_device_wait(pspw_cell *c, int complete) {
+  if (!c) return fail(PSPW_ERR_ARG, "check_device_wait: null cell");
+  PSPW_CUDA(cudaSetDevice(c->device));
+  return pspw::nl_tc_wait_check(c, complete);
+}
+
 int pspw_timing_enable(pspw_cell *c, int mask) {
   if (!c) return fail(PSPW_ERR_ARG, "timing: null cell");
   c->timing.mask = mask;

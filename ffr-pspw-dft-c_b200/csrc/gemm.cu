@@ -1,14 +1,27 @@
 // Complex GEMM for the subspace steps of the eigensolvers (zgemm_ calls of
-// davidson_cpu.cpp, lobpcg_cpu.cpp, eig_zhegv.cpp, ChebySCFLoop.cpp):
+// davidson_cpu.cpp, lobpcg_cpu.cpp, eig_zhegv.cpp, ChebySCFLoop.cpp) and the
+// FP64 projector products of H*psi (ApplyHam_block.cpp:86-117):
 //   C = alpha * op(A) * B + beta * C,  op(A) = A or A^H,
-// column-major with leading dimensions, FP64 or FP32 complex.  FP64 products
-// with more than 8 columns go to cuBLAS ZGEMM (a plain library GEMM); the
-// rest use the kernels below.
+// column-major with leading dimensions, FP64 or FP32 complex.
 //
-// Tiles of 64 x 64 outputs, 256 threads, 4 x 4 outputs per thread, the K loop
-// staged through shared memory.  When K is long and the output small (the
-// Gram matrices X^H Y over NGW plane waves) K is split across blocks; the
-// slices are reduced in a fixed order, so results do not depend on timing.
+// FP64 products with more than 8 columns run on the FP64 tensor-core
+// instruction (DMMA: mma.sync m16n8k4 .f64, the only tensor-core form of
+// FP64 arithmetic on sm_100a; tcgen05 has no FP64 kind).  A complex product
+// is four real products on split real/imaginary fragments:
+//   Cr += Ar Br - Ai Bi,  Ci += Ar Bi + Ai Br   (A^H: Ai -> -Ai).
+// Blocks of 64 x 64 outputs, 8 warps of 32 x 16, K staged through a
+// four-deep cp.async ring of 8-wide complex tiles.  Operands whose K index
+// is contiguous in memory (A^H, B) are staged [row][k]; A in the 'N' form is
+// staged [k][m] (its M index is contiguous), both padded so that the 16-byte
+// fragment loads of a quarter warp hit distinct banks.
+//
+// FP32 products and FP64 products of at most 8 columns use the SIMT kernels
+// below: tiles of 64 x 64 outputs, 256 threads, 4 x 4 outputs per thread,
+// and a narrow 64 x 8 form.  Single columns use matrix-vector kernels.
+//
+// When K is long and the output small (the Gram matrices X^H Y over NGW
+// plane waves) K is split across blocks; the slices are reduced in a fixed
+// order, so results do not depend on timing.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -17,6 +30,7 @@
 #include "dense.h"
 #include "engine.h"
 #include "gemm.h"
+#include "tc.cuh"
 
 namespace pspw {
 namespace {
@@ -264,35 +278,206 @@ __global__ void k_zgemm_reduce_warp(int m, int n, int nsplit, const cx<R> *__res
   }
 }
 
+// ---------------------------------------------------------------- FP64 DMMA
+namespace dm {
+constexpr int BM = 64, BN = 64, BK = 8, STAGES = 4, THREADS = 256;
+// [row][k] tiles: BK + 4 = 12 complex per row (12 = 4 mod 8): the fragment
+// loads of a quarter warp (rows g, g+1; k = t..t+3) cover 8 distinct 16-byte
+// bank groups.  [k][m] tiles: BM + 2 = 66 per k (66 = 2 mod 8), likewise.
+constexpr int LDK = BK + 4, LDM = BM + 2;
+constexpr int A_ELEMS = BM * LDK > BK * LDM ? BM * LDK : BK * LDM;
+constexpr int B_ELEMS = BN * LDK;
+constexpr int STAGE = A_ELEMS + B_ELEMS;  // complex elements per ring slot
+constexpr size_t SMEM = sizeof(double2) * STAGE * STAGES;
+}  // namespace dm
+
+// d(16 x 8) += a(16 x 4) b(4 x 8), FP64: lane (g = lane / 4, t = lane % 4)
+// holds a = A[g][t], A[g+8][t]; b = B[t][g]; d = D[g][2t], D[g][2t+1],
+// D[g+8][2t], D[g+8][2t+1]
+__device__ __forceinline__ void dmma(double (&d)[4], double a0, double a1, double b) {
+  asm volatile(
+      "mma.sync.aligned.m16n8k4.row.col.f64.f64.f64.f64 {%0,%1,%2,%3}, {%4,%5}, {%6}, "
+      "{%0,%1,%2,%3};"
+      : "+d"(d[0]), "+d"(d[1]), "+d"(d[2]), "+d"(d[3])
+      : "d"(a0), "d"(a1), "d"(b));
+}
+
+// part or C over the block's K slice [blockIdx.z * kchunk, +kchunk)
+template <bool CONJ_A>
+__global__ void __launch_bounds__(dm::THREADS, 2)
+    k_zgemm_dmma(int m, int n, int k, double2 alpha, const double2 *__restrict__ A, int lda,
+                 const double2 *__restrict__ B, int ldb, double2 beta, double2 *C, int ldc,
+                 int kchunk, double2 *__restrict__ part) {
+  using namespace dm;
+  extern __shared__ __align__(16) double2 sm[];
+  const int m0 = blockIdx.x * BM, n0 = blockIdx.y * BN;
+  const int kb = blockIdx.z * kchunk, ke = min(k, kb + kchunk);
+  const int nkt = ke > kb ? (ke - kb + BK - 1) / BK : 0;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int wm = (warp & 1) * 32, wn = (warp >> 1) * 16;
+  const int g = lane >> 2, t = lane & 3;
+
+  // one ring slot: 2 x 512 16-byte copies, zero-filled outside the matrices
+  auto load = [&](int kt, int slot) {
+    double2 *As = sm + slot * STAGE, *Bs = As + A_ELEMS;
+    const int k0 = kb + kt * BK;
+#pragma unroll
+    for (int e = tid; e < BN * BK; e += THREADS) {
+      const int r = e / BK, kk = e % BK;
+      const int gn = n0 + r, gk = k0 + kk;
+      const bool ok = gn < n && gk < ke;
+      tc::cp_async16(Bs + r * LDK + kk, ok ? B + (size_t)gn * ldb + gk : B, ok);
+    }
+    if (CONJ_A) {  // A is k x m; A^H(mm, kk) = conj(A[mm * lda + kk]), K contiguous
+#pragma unroll
+      for (int e = tid; e < BM * BK; e += THREADS) {
+        const int r = e / BK, kk = e % BK;
+        const int gm = m0 + r, gk = k0 + kk;
+        const bool ok = gm < m && gk < ke;
+        tc::cp_async16(As + r * LDK + kk, ok ? A + (size_t)gm * lda + gk : A, ok);
+      }
+    } else {  // A is m x k; A(mm, kk) = A[kk * lda + mm], M contiguous
+#pragma unroll
+      for (int e = tid; e < BM * BK; e += THREADS) {
+        const int kk = e / BM, r = e % BM;
+        const int gm = m0 + r, gk = k0 + kk;
+        const bool ok = gm < m && gk < ke;
+        tc::cp_async16(As + kk * LDM + r, ok ? A + (size_t)gk * lda + gm : A, ok);
+      }
+    }
+  };
+
+  double cr[2][2][4], ci[2][2][4];  // [m16 sub-tile][n8 sub-tile][fragment]
+#pragma unroll
+  for (int i = 0; i < 2; i++)
+#pragma unroll
+    for (int j = 0; j < 2; j++)
+#pragma unroll
+      for (int q = 0; q < 4; q++) cr[i][j][q] = ci[i][j][q] = 0.0;
+
+#pragma unroll
+  for (int s = 0; s < STAGES - 1; s++) {
+    if (s < nkt) load(s, s);
+    tc::cp_async_commit();
+  }
+  for (int kt = 0; kt < nkt; kt++) {
+    tc::cp_async_wait<STAGES - 2>();
+    __syncthreads();  // slot kt % STAGES landed for all; slot (kt-1) % STAGES free
+    if (kt + STAGES - 1 < nkt) load(kt + STAGES - 1, (kt + STAGES - 1) % STAGES);
+    tc::cp_async_commit();
+    const double2 *As = sm + (kt % STAGES) * STAGE, *Bs = As + A_ELEMS;
+#pragma unroll
+    for (int ks = 0; ks < BK; ks += 4) {
+      double ar[2][2], ai[2][2], an[2][2], br[2], bi[2];
+#pragma unroll
+      for (int i = 0; i < 2; i++)
+#pragma unroll
+        for (int h = 0; h < 2; h++) {
+          const int row = wm + i * 16 + g + 8 * h;
+          const double2 v = CONJ_A ? As[row * LDK + ks + t] : As[(ks + t) * LDM + row];
+          ar[i][h] = v.x;
+          ai[i][h] = CONJ_A ? -v.y : v.y;  // imaginary part of op(A)
+          an[i][h] = -ai[i][h];
+        }
+#pragma unroll
+      for (int j = 0; j < 2; j++) {
+        const double2 v = Bs[(wn + j * 8 + g) * LDK + ks + t];
+        br[j] = v.x;
+        bi[j] = v.y;
+      }
+#pragma unroll
+      for (int i = 0; i < 2; i++)
+#pragma unroll
+        for (int j = 0; j < 2; j++) {
+          dmma(cr[i][j], ar[i][0], ar[i][1], br[j]);
+          dmma(cr[i][j], an[i][0], an[i][1], bi[j]);
+          dmma(ci[i][j], ar[i][0], ar[i][1], bi[j]);
+          dmma(ci[i][j], ai[i][0], ai[i][1], br[j]);
+        }
+    }
+  }
+  tc::cp_async_wait<0>();
+
+#pragma unroll
+  for (int i = 0; i < 2; i++)
+#pragma unroll
+    for (int j = 0; j < 2; j++)
+#pragma unroll
+      for (int q = 0; q < 4; q++) {
+        const int gm = m0 + wm + i * 16 + g + 8 * (q >> 1);
+        const int gn = n0 + wn + j * 8 + 2 * t + (q & 1);
+        if (gm >= m || gn >= n) continue;
+        const double2 acc = make_double2(cr[i][j][q], ci[i][j][q]);
+        if (part) {
+          part[((size_t)blockIdx.z * n + gn) * m + gm] = acc;
+        } else {
+          double2 r = cmul(alpha, acc);
+          if (beta.x != 0.0 || beta.y != 0.0) r = r + cmul(beta, C[(size_t)gn * ldc + gm]);
+          C[(size_t)gn * ldc + gm] = r;
+        }
+      }
+}
+
 }  // namespace
+
+// FP64, more than 8 columns: DMMA tiles, K split across blocks when the
+// output has fewer than two blocks per SM (the Gram matrices)
+static int zgemm_dmma(pspw_cell *c, bool conj, int m, int n, int k, double2 alpha, const double2 *A,
+               int lda, const double2 *B, int ldb, double2 beta, double2 *C, int ldc) {
+  using namespace dm;
+  cudaStream_t st = c->stream;
+  const int mt = (m + BM - 1) / BM, nt = (n + BN - 1) / BN;
+  static int sms = 0;
+  if (!sms) {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    if (sms <= 0) sms = 148;
+  }
+  int nsplit = 1;
+  if (k > 8 * BK && mt * nt < 2 * sms)
+    nsplit = std::max(1, std::min((k + 255) / 256, (2 * sms + mt * nt - 1) / (mt * nt)));
+  int kchunk = k > 0 ? (k + nsplit - 1) / nsplit : BK;
+  kchunk = (kchunk + BK - 1) / BK * BK;
+  nsplit = k > 0 ? (k + kchunk - 1) / kchunk : 1;
+  double2 *part = nullptr;
+  if (nsplit > 1) {
+    int rc = ws_reserve(c, 9, sizeof(double2) * (size_t)nsplit * m * n, (void **)&part);
+    if (rc) return rc;
+  }
+  PSPW_CUDA(cudaFuncSetAttribute(conj ? k_zgemm_dmma<true> : k_zgemm_dmma<false>,
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM));
+  cudaEvent_t ev;
+  timing_begin(c, kFamGemm, &ev);
+  const dim3 grid(mt, nt, nsplit);
+  if (conj)
+    k_zgemm_dmma<true><<<grid, THREADS, SMEM, st>>>(m, n, k, alpha, A, lda, B, ldb, beta, C, ldc,
+                                                    kchunk, part);
+  else
+    k_zgemm_dmma<false><<<grid, THREADS, SMEM, st>>>(m, n, k, alpha, A, lda, B, ldb, beta, C,
+                                                     ldc, kchunk, part);
+  c->kernel_launches++;
+  if (nsplit > 1) {
+    k_zgemm_reduce<double><<<std::min<size_t>(4 * 148, ((size_t)m * n + 255) / 256), 256, 0,
+                             st>>>(m, n, nsplit, part, alpha, beta, C, ldc);
+    c->kernel_launches++;
+  }
+  timing_end(c, kFamGemm, ev);
+  PSPW_CUDA(cudaGetLastError());
+  return PSPW_OK;
+}
 
 template <typename R>
 int zgemm(pspw_cell *c, char opa, int m, int n, int k, cx<R> alpha, const cx<R> *A, int lda,
           const cx<R> *B, int ldb, cx<R> beta, cx<R> *C, int ldc) {
   using T = cx<R>;
+  if (opa != 'N' && opa != 'n' && opa != 'C' && opa != 'c')
+    return fail(PSPW_ERR_ARG, "zgemm: op(A) must be 'N' or 'C'");
   if (m <= 0 || n <= 0) return PSPW_OK;
   if constexpr (sizeof(R) == 8) {
-    // FP64 with more than 8 columns: a plain library GEMM on the FP64 pipe
-    // (cuBLAS ZGEMM, deterministic); narrow products (the Lanczos vectors)
-    // stay on the split-K kernels below, which are faster at that shape
-    if (k > 0 && n > 8) {
-      cublasHandle_t h;
-      int rc = cublas_handle(c, &h);
-      if (rc) return rc;
-      cudaEvent_t ev;
-      timing_begin(c, kFamGemm, &ev);
-      const cublasOperation_t ta = (opa == 'C' || opa == 'c') ? CUBLAS_OP_C : CUBLAS_OP_N;
-      if (cublasZgemm(h, ta, CUBLAS_OP_N, m, n, k,
-                      reinterpret_cast<const cuDoubleComplex *>(&alpha),
-                      reinterpret_cast<const cuDoubleComplex *>(A), lda,
-                      reinterpret_cast<const cuDoubleComplex *>(B), ldb,
-                      reinterpret_cast<const cuDoubleComplex *>(&beta),
-                      reinterpret_cast<cuDoubleComplex *>(C), ldc) != CUBLAS_STATUS_SUCCESS)
-        return fail(PSPW_ERR_CUDA, "cublasZgemm");
-      timing_end(c, kFamGemm, ev);
-      c->kernel_launches++;
-      return PSPW_OK;
-    }
+    // FP64 with more than 8 columns: the DMMA kernel
+    if (n > 8) return zgemm_dmma(c, opa == 'C' || opa == 'c', m, n, k, alpha, A, lda, B, ldb,
+                                 beta, C, ldc);
   }
   cudaStream_t st = c->stream;
   if (n == 1 && k > 0) {

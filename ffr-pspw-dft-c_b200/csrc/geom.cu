@@ -965,13 +965,23 @@ int pspw_system_timing(pspw_system *S, double *ms8) {
 
 int pspw_system_cheby_scf(pspw_system *S, int filter_prec, const char *outdir, double *eig,
                           double *e6, int *iterations, int *converged, double *hist) {
-  if (!S || !eig || !e6 || !iterations || !converged)
-    return fail(PSPW_ERR_ARG, "system_cheby_scf: null argument");
-  if (!S->scf) return fail(PSPW_ERR_ARG, "system_cheby_scf: a host-only system");
+  if (!S) return fail(PSPW_ERR_ARG, "system_cheby_scf: null argument");
   pspw_scf_params p;
   int rc = pspw_system_params(S, &p);
   if (rc) return rc;
   p.filter_prec = filter_prec;
+  return pspw_system_cheby_scf_with(S, &p, outdir, eig, e6, iterations, converged, hist);
+}
+
+int pspw_system_cheby_scf_with(pspw_system *S, const pspw_scf_params *params, const char *outdir,
+                               double *eig, double *e6, int *iterations, int *converged,
+                               double *hist) {
+  if (!S || !params || !eig || !e6 || !iterations || !converged)
+    return fail(PSPW_ERR_ARG, "system_cheby_scf: null argument");
+  if (!S->scf) return fail(PSPW_ERR_ARG, "system_cheby_scf: a host-only system");
+  pspw_scf_params p = *params;
+  if (p.nx != S->nx) return fail(PSPW_ERR_ARG, "system_cheby_scf: params.nx is not the system's NX");
+  int rc = PSPW_OK;
   const int ngw = S->ngw, nx2 = S->nx + 2;
   // ChebySCFLoop.cpp:100-106 and 201-208: v0 (NGWX draws) then the random
   // start block, from rand() seeded 1 as in a fresh reference process

@@ -27,9 +27,9 @@
 // reduced in a fixed order, so results are deterministic) and
 // back-projection, whose epilogue also applies out = a*(H psi) + b*psi + g*x,
 // the update of the Chebyshev three-term recurrence (chebyfilt.cpp:36-59).
-// FP64: beta stored once per cell (NGW x nproj) and both products as cuBLAS
-// ZGEMMs, the recurrence as a separate pass; the allocation-free entry point
-// keeps the SIMT kernels.
+// FP64: beta stored once per cell (NGW x nproj) and both products on the
+// engine's FP64 tensor-core GEMM (gemm.cu, DMMA), the recurrence as a
+// separate pass; the allocation-free entry point keeps the SIMT kernels.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -40,6 +40,7 @@
 #include "engine.h"
 #include "fft.cuh"
 #include "fftpath.h"
+#include "gemm.h"
 #include "nl_tc.h"
 
 namespace pspw {
@@ -672,54 +673,20 @@ int ensure_beta64(pspw_cell *c, const ProjArg &pa) {
   return PSPW_OK;
 }
 
-// P (nproj x nb) = beta^H psi over the first ngw plane waves (cuBLAS ZGEMM)
+// P (nproj x nb) = beta^H psi over the first ngw plane waves (the engine's
+// complex GEMM: DMMA tiles for more than 8 bands, matrix-vector for one)
 int project_beta64(pspw_cell *c, const double2 *psi, int ld, int ngw, int nb, double2 *P) {
-  cublasHandle_t h;
-  int rc = cublas_handle(c, &h);
-  if (rc) return rc;
-  const cuDoubleComplex one = make_cuDoubleComplex(1.0, 0.0), zero = make_cuDoubleComplex(0.0, 0.0);
-  if (nb == 1) {  // a single vector (Lanczos): the matrix-vector form
-    if (cublasZgemv(h, CUBLAS_OP_C, ngw, c->proj.nproj, &one,
-                    reinterpret_cast<const cuDoubleComplex *>(c->proj.d_beta64), c->basis.ngw,
-                    reinterpret_cast<const cuDoubleComplex *>(psi), 1, &zero,
-                    reinterpret_cast<cuDoubleComplex *>(P), 1) != CUBLAS_STATUS_SUCCESS)
-      return fail(PSPW_ERR_CUDA, "cublasZgemv (projection)");
-    c->kernel_launches++;
-    return PSPW_OK;
-  }
-  if (cublasZgemm(h, CUBLAS_OP_C, CUBLAS_OP_N, c->proj.nproj, nb, ngw, &one,
-                  reinterpret_cast<const cuDoubleComplex *>(c->proj.d_beta64), c->basis.ngw,
-                  reinterpret_cast<const cuDoubleComplex *>(psi), ld, &zero,
-                  reinterpret_cast<cuDoubleComplex *>(P), c->proj.nproj) != CUBLAS_STATUS_SUCCESS)
-    return fail(PSPW_ERR_CUDA, "cublasZgemm (projection)");
-  c->kernel_launches++;
-  return PSPW_OK;
+  const double2 one = make_double2(1.0, 0.0), zero = make_double2(0.0, 0.0);
+  return zgemm<double>(c, 'C', c->proj.nproj, nb, ngw, one, c->proj.d_beta64, c->basis.ngw, psi,
+                       ld, zero, P, c->proj.nproj);
 }
 
-// out(:, b) += alpha beta wp(:, b) over the first ngw plane waves (cuBLAS)
+// out(:, b) += alpha beta wp(:, b) over the first ngw plane waves
 int backproject_beta64(pspw_cell *c, const double2 *wp, int ngw, int nb, double2 *out, int ldo,
                        double alpha) {
-  cublasHandle_t h;
-  int rc = cublas_handle(c, &h);
-  if (rc) return rc;
-  const cuDoubleComplex one = make_cuDoubleComplex(1.0, 0.0),
-                        al = make_cuDoubleComplex(alpha, 0.0);
-  if (nb == 1) {
-    if (cublasZgemv(h, CUBLAS_OP_N, ngw, c->proj.nproj, &al,
-                    reinterpret_cast<const cuDoubleComplex *>(c->proj.d_beta64), c->basis.ngw,
-                    reinterpret_cast<const cuDoubleComplex *>(wp), 1, &one,
-                    reinterpret_cast<cuDoubleComplex *>(out), 1) != CUBLAS_STATUS_SUCCESS)
-      return fail(PSPW_ERR_CUDA, "cublasZgemv (back-projection)");
-    c->kernel_launches++;
-    return PSPW_OK;
-  }
-  if (cublasZgemm(h, CUBLAS_OP_N, CUBLAS_OP_N, ngw, nb, c->proj.nproj, &al,
-                  reinterpret_cast<const cuDoubleComplex *>(c->proj.d_beta64), c->basis.ngw,
-                  reinterpret_cast<const cuDoubleComplex *>(wp), c->proj.nproj, &one,
-                  reinterpret_cast<cuDoubleComplex *>(out), ldo) != CUBLAS_STATUS_SUCCESS)
-    return fail(PSPW_ERR_CUDA, "cublasZgemm (back-projection)");
-  c->kernel_launches++;
-  return PSPW_OK;
+  const double2 one = make_double2(1.0, 0.0), al = make_double2(alpha, 0.0);
+  return zgemm<double>(c, 'N', ngw, nb, c->proj.nproj, al, c->proj.d_beta64, c->basis.ngw, wp,
+                       c->proj.nproj, one, out, ldo);
 }
 
 // rho += sum_b wband[b] |psi_b(r)|^2 for any grid the generic FFT handles;
@@ -848,7 +815,7 @@ int hpsi_apply(pspw_cell *c, const void *in_v, int ld_in, void *out_v, int ld_ou
     timing_begin(c, kFamNonlocal, &ev);
     bool done = false;
     if constexpr (sizeof(R) == 8) {
-      // FP64 without a scratch plan: beta materialised once, cuBLAS ZGEMMs
+      // FP64 without a scratch plan: beta materialised once, complex GEMMs
       if (!plan) {
         int rc = ensure_beta64(c, pa);
         if (rc) return rc;
@@ -1052,7 +1019,7 @@ int project_fp64(pspw_cell *c, const double2 *psi, int ld, int ngw, int nb, doub
   pa.nproj = nproj;
   int rc = ensure_beta64(c, pa);
   if (rc) return rc;
-  // beta materialised: one cuBLAS ZGEMM (projections without the weights)
+  // beta materialised: one complex GEMM (projections without the weights)
   if ((rc = project_beta64(c, psi, ld, ngw, nb, P))) return rc;
   PSPW_CUDA(cudaGetLastError());
   return PSPW_OK;

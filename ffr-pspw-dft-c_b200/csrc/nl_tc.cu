@@ -649,6 +649,29 @@ int launch_back(pspw_cell *c, const Shape &s, const float *wt, int ngw, int nb, 
 
 }  // namespace
 
+// One bounded barrier wait, the one every tensor-core kernel uses: with
+// complete == 0 nothing arrives on the barrier, so the wait gives up after
+// about a second and raises the cell's error word; otherwise the waiting
+// thread arrives first and the wait succeeds at once.
+__global__ void k_wait_check(int complete, int *err) {
+  __shared__ __align__(8) uint64_t bar;
+  if (threadIdx.x == 0) {
+    tc::mbar_init(&bar, 1);
+    tc::fence_mbar_init();
+    if (complete) tc::mbar_arrive(&bar);
+    if (!tc::mbar_wait(&bar, 0)) atomicOr(err, 1);
+  }
+}
+
+int nl_tc_wait_check(pspw_cell *c, int complete) {
+  if (!c->d_err) return fail(PSPW_ERR_NOT_IMPL, "the cell has no device error word");
+  k_wait_check<<<1, 32, 0, c->stream>>>(complete, c->d_err);
+  c->kernel_launches++;
+  PSPW_CUDA(cudaGetLastError());
+  PSPW_CUDA(cudaStreamSynchronize(c->stream));
+  return device_status(c);
+}
+
 bool nl_tc_usable(const pspw_cell *c) {
   static const bool off = std::getenv("PSPW_NL_SIMT") != nullptr;
   if (c->nl_path == PSPW_NL_SIMT || (off && c->nl_path != PSPW_NL_TENSOR_CORE)) return false;

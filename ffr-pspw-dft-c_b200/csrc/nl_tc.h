@@ -34,4 +34,9 @@ int nl_tc_backproject(pspw_cell *c, const float *wt, int ngw, int nb, float2 *ou
                       const float2 *in, int ldi, const float2 *xm2, int ldx, float a, float b,
                       float g, bool pre = false);
 
+// Runs one bounded device-side barrier wait on the cell stream and returns
+// the cell's status after it: PSPW_ERR_TIMEOUT when the barrier is never
+// completed (complete == 0), PSPW_OK otherwise.
+int nl_tc_wait_check(pspw_cell *c, int complete);
+
 }  // namespace pspw

@@ -16,7 +16,9 @@
 // names a stand-in object), so the address is looked up once per device with
 // cudaGetSymbolAddress, with that device current, and cached.  The first call
 // on each device performs that lookup, so it should be made before any
-// stream capture begins.
+// stream capture begins.  The cache lives as long as the process: a
+// cudaDeviceReset unloads the device image and leaves the cached address
+// stale, so the entry point is not to be called after a reset.
 //
 // All calls on a device share the one array and it keeps whatever the last
 // call left in it.  Nothing in it needs to start at zero: every element a

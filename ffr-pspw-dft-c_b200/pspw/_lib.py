@@ -62,6 +62,7 @@ SIGNATURES = {
     "pspw_cell_sizes": [_vp, _vp],
     "pspw_cell_set_band_batch": [_vp, _i],
     "pspw_cell_set_nl_path": [_vp, _i],
+    "pspw_cell_check_device_wait": [_vp, _i],
     "pspw_apply_ham_block": [_vp, _vp, _vp, _i, _i],
     "pspw_apply_ham_block_dev": [_vp, _i, _vp, _vp, _i, _i, _i],
     "pspw_apply_ham_block_dev_noalloc": [_vp, _i, _vp, _vp, _i, _i, _i],
@@ -107,7 +108,9 @@ SIGNATURES = {
     "pspw_system_scf": [_vp, _vp],
     "pspw_system_timing": [_vp, _vp],
     "pspw_system_cheby_scf": [_vp, _i, C.c_char_p, _vp, _vp, _vp, _vp, _vp],
+    "pspw_system_cheby_scf_with": [_vp, _vp, C.c_char_p, _vp, _vp, _vp, _vp, _vp],
     "pspw_print_3d_array": [_vp, _i, _i, _i, C.c_char_p],
+    "pspw_zgemm_dev": [_vp, C.c_char, _i, _i, _i, _vp, _vp, _i, _vp, _i, _vp, _vp, _i],
 }
 _RESTYPE = {"pspw_error_string": C.c_char_p, "pspw_last_error": C.c_char_p}
 

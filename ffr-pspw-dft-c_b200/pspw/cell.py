@@ -138,6 +138,11 @@ class Cell:
         """NL_AUTO / NL_SIMT / NL_TENSOR_CORE kernels for the FP32 projector GEMMs."""
         check(lib().pspw_cell_set_nl_path(self._h, int(path)))
 
+    def check_device_wait(self, complete):
+        """One bounded device-side barrier wait (the tensor-core kernels'
+        kind); raises PspwError(TIMEOUT) when nothing completes it."""
+        check(lib().pspw_cell_check_device_wait(self._h, int(complete)))
+
     # ---- host FP64 (the reference signatures' data)
     def apply_ham_block(self, vin):
         vin = _f(vin, np.complex128)
@@ -163,6 +168,15 @@ class Cell:
     def chebyfilt_dev(self, d_x, ld, ngw, nb, degree, lb, ub, prec):
         check(lib().pspw_chebyfilt_dev(self._h, int(prec), ptr(d_x), int(ld), int(ngw), int(nb),
                                        int(degree), float(lb), float(ub)))
+
+    def zgemm_dev(self, opa, m, n, k, alpha, d_a, lda, d_b, ldb, beta, d_c, ldc):
+        """C = alpha op(A) B + beta C on device FP64 complex matrices
+        (column-major; op 'N' or 'C'), enqueued on the cell stream."""
+        al = np.array([complex(alpha).real, complex(alpha).imag])
+        be = np.array([complex(beta).real, complex(beta).imag])
+        check(lib().pspw_zgemm_dev(self._h, opa.encode() if isinstance(opa, str) else opa,
+                                   int(m), int(n), int(k), al.ctypes.data, ptr(d_a), int(lda),
+                                   ptr(d_b), int(ldb), be.ctypes.data, ptr(d_c), int(ldc)))
 
     # ---- solvers and dense steps (host buffers; reference semantics)
     def gen_prec(self, nbasis, tau):

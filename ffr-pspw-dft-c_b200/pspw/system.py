@@ -88,19 +88,23 @@ class System:
         check(lib().pspw_system_timing(self._h, t.ctypes.data))
         return dict(zip(_TIMES, t.tolist()))
 
-    def cheby_scf(self, filter_prec=PREC_F64, outdir=None):
+    def cheby_scf(self, filter_prec=PREC_F64, outdir=None, **controls):
         """ChebySCFLoop() of the reference's main program on this system.
+        `controls` override the INPUT's SCF controls (pspw_scf_params
+        fields, e.g. pulay_beta=0.3, mixdim=6, conv=1e-8, max_scf_iter=200).
         Returns eig (NX), energies, iterations, converged and hist
         (iterations x {ETOT, |dETOT|, d, ms since the call began})."""
         nx = self.dims["nx"]
         eig, e6 = np.zeros(nx), np.zeros(6)
         its, cv = C.c_int(0), C.c_int(0)
         p = self.params()
+        p.update(controls, filter_prec=int(filter_prec))
         hist = np.zeros(4 * max(1, p["max_scf_iter"]))
-        check(lib().pspw_system_cheby_scf(self._h, int(filter_prec),
-                                          None if outdir is None else str(outdir).encode(),
-                                          eig.ctypes.data, e6.ctypes.data, C.byref(its),
-                                          C.byref(cv), hist.ctypes.data))
+        sp = ScfParams(**p)
+        check(lib().pspw_system_cheby_scf_with(self._h, C.byref(sp),
+                                               None if outdir is None else str(outdir).encode(),
+                                               eig.ctypes.data, e6.ctypes.data, C.byref(its),
+                                               C.byref(cv), hist.ctypes.data))
         n = its.value
         return dict(eig=eig, iterations=n, converged=bool(cv.value),
                     hist=hist.reshape(-1, 4)[:n],

@@ -112,11 +112,22 @@ int pspw_cell_set_band_batch(pspw_cell *cell, int nbatch);
  * reference has one CPU path).  AUTO takes the tensor-core (tcgen05, 3xTF32)
  * kernels when the cell has one species and at most 256 atoms, else the
  * SIMT kernels; TENSOR_CORE on a cell outside that range is
- * PSPW_ERR_NOT_IMPL.  The FP64 path always uses the SIMT kernels. */
+ * PSPW_ERR_NOT_IMPL.  The FP64 path does not depend on it: it stores the
+ * projectors once per cell and runs both products on the FP64 tensor-core
+ * GEMM (the allocation-free entry point keeps SIMT kernels). */
 #define PSPW_NL_AUTO 0
 #define PSPW_NL_SIMT 1
 #define PSPW_NL_TENSOR_CORE 2
 int pspw_cell_set_nl_path(pspw_cell *cell, int path);
+
+/* Check of the device timeout path (no reference counterpart).  Every
+ * barrier wait in the engine's tensor-core kernels gives up after about one
+ * second and raises the cell's error word, which the next call that
+ * synchronises reports as PSPW_ERR_TIMEOUT; the context and the cell stay
+ * usable.  This runs one such wait on the cell stream: with complete == 0
+ * nothing completes the barrier and the call returns PSPW_ERR_TIMEOUT after
+ * about a second; with complete != 0 it returns PSPW_OK. */
+int pspw_cell_check_device_wait(pspw_cell *cell, int complete);
 
 /* ------------------------------------------------------------------ H*psi
  * vout = H vin for nstates bands (ApplyHam_block.cpp:5-172): kinetic
@@ -138,7 +149,10 @@ int pspw_apply_ham_block_dev(pspw_cell *cell, int prec, const void *d_vin, void 
  * loads it until exit); cell/block sizes whose scratch does not fit are
  * rejected with PSPW_ERR_SHAPE.  The first call on a device looks up the
  * array's device address (cudaGetSymbolAddress) and should come before any
- * stream capture.  All calls share the array: calls that overlap on the GPU
+ * stream capture.  The address is kept per device index for the life of the
+ * process; cudaDeviceReset unloads the library's device image, so after a
+ * reset this entry point must not be called again in that process.  All
+ * calls share the array: calls that overlap on the GPU
  * race and must be serialised by the caller.  Set V_eff with
  * pspw_cell_set_veff_device, which does not allocate either. */
 int pspw_apply_ham_block_dev_noalloc(pspw_cell *cell, int prec, const void *d_vin, void *d_vout,
@@ -171,6 +185,13 @@ int pspw_chebyfilt_dev(pspw_cell *cell, int prec, void *d_X, int ld, int ngw, in
  * eigenvectors there; nempty = NEMPTY; max_iter <= 0 selects the reference
  * default max(30, nstates/2); hprec is the arithmetic of H*psi inside the
  * solver (the rest is FP64); resnrm[nstates] and iters may be NULL.
+ * Davidson with hprec = PSPW_PREC_F32 is supported for small blocks only:
+ * its 2 nstates subspace overlap becomes nearly singular on large blocks
+ * (measured on a 512-state, 216-atom cell), and the reference's eig_zhegv
+ * scales every overlap direction above 1.2e-15 by 1/sqrt(eigenvalue)
+ * (eig_zhegv.cpp:39-47), which turns the FP32 rounding of H R into
+ * spurious Ritz values.  Use FP64 H*psi with Davidson on large blocks, or
+ * LOBPCG, which stays bounded with FP32 H*psi.
  * eval_rho_psi: eigvec columns with leading dimension ld, the last plane
  * wave of each band is left out as in the reference, *ekin += EKIN part;
  * returns PSPW_ERR_CHARGE when a band's norm is off by more than 6e-3. */
@@ -208,6 +229,21 @@ int pspw_eval_rho_psi_dev(pspw_cell *cell, double *d_rhoe, const double *d_eigve
                           double *ekin);
 int pspw_eval_enl_dev(pspw_cell *cell, const double *d_c0, int ld, int ngw, int nx,
                       const double *focc, double wkpt, double *enl, double *fnl);
+
+/* ------------------------------------------------------------------ dense steps, device pointers
+ * The subspace products of the solvers and of the SCF loop (the zgemm_
+ * calls of davidson_cpu.cpp:120-178, lobpcg_cpu.cpp:103-309,
+ * eig_zhegv.cpp:50-60 and ChebySCFLoop.cpp:296-306) on device FP64 complex
+ * column-major matrices, enqueued on the cell stream.
+ *
+ * zgemm_dev   C = alpha op(A) B + beta C; op(A) = A ('N') or A^H ('C'),
+ *             any other opa is PSPW_ERR_ARG; alpha, beta: host {re, im}.
+ *             More than 8 columns run on the FP64 tensor-core instruction
+ *             (DMMA); long K with a small output is split over blocks and
+ *             reduced in a fixed order (bitwise repeatable). */
+int pspw_zgemm_dev(pspw_cell *cell, char opa, int m, int n, int k, const double *alpha,
+                   const double *d_A, int lda, const double *d_B, int ldb, const double *beta,
+                   double *d_C, int ldc);
 
 /* ------------------------------------------------------------------ SCF pieces
  * The steps of the SCF iteration around the eigensolver, on the device in
@@ -361,6 +397,13 @@ int pspw_system_scf(pspw_system *sys, pspw_scf **scf);
 int pspw_system_timing(pspw_system *sys, double *ms8);
 int pspw_system_cheby_scf(pspw_system *sys, int filter_prec, const char *outdir, double *eig,
                           double *e6, int *iterations, int *converged, double *hist);
+/* The same loop with explicit controls (no reference counterpart: the
+ * reference reads them from INPUT and hard-codes the Pulay warm-up beta
+ * 0.25, PulayRhoMix.cpp:10).  Start from pspw_system_params and change what
+ * differs, e.g. pulay_beta and mixdim; params->nx must be the system's NX. */
+int pspw_system_cheby_scf_with(pspw_system *system, const pspw_scf_params *params,
+                               const char *outdir, double *eig, double *e6, int *iterations,
+                               int *converged, double *hist);
 /* Print3DArray.cpp:5-22: n1*n2*n3 values, one `%18.10f` per line */
 int pspw_print_3d_array(const double *a, int n1, int n2, int n3, const char *path);
 

@@ -23,7 +23,7 @@ if not torch.cuda.is_available():  # pragma: no cover
     pytest.skip("needs a CUDA device", allow_module_level=True)
 
 from helpers import relmax  # noqa: E402
-from pspw import PREC_F32, PREC_F64, PspwError, workloads  # noqa: E402
+from pspw import PREC_F32, PREC_F64, Cell, PspwError, basis_gamma, synth, workloads  # noqa: E402
 from pspw._lib import check, lib, ptr  # noqa: E402
 
 
@@ -48,6 +48,36 @@ def _alloc(cell, d_in, d_out, ld, ngw, nb, prec):
 def test_noalloc_matches_allocating_entry_point_twice(si8, prec, dtype, tol):
     w, cell = si8
     psi = w["psi"]
+    ngw, nb = psi.shape
+    d_in = torch.from_numpy(np.ascontiguousarray(psi.T)).to(dtype).cuda()
+    ref = torch.zeros_like(d_in)
+    torch.cuda.synchronize()
+    _alloc(cell, d_in, ref, ngw, ngw, nb, prec)
+    check(lib().pspw_cell_synchronize(cell.handle))
+    expect = ref.cpu().numpy()
+    for call in range(2):
+        out = torch.full_like(d_in, float("nan"))
+        torch.cuda.synchronize()
+        _noalloc(cell, d_in, out, ngw, ngw, nb, prec)
+        check(lib().pspw_cell_synchronize(cell.handle))
+        got = out.cpu().numpy()
+        assert np.all(np.isfinite(got)), f"call {call}"
+        assert relmax(got, expect) < tol, f"call {call}"
+
+
+@pytest.mark.parametrize("prec,dtype,tol", [(PREC_F64, torch.complex128, 1e-12),
+                                            (PREC_F32, torch.complex64, 2e-5)])
+def test_noalloc_generic_fft_grid_twice(prec, dtype, tol):
+    # a 22 x 21 x 26 grid (radices 2, 3, 7, 11, 13) is outside the register
+    # FFT: the general passes run with their stick and plane buffers placed
+    # in the static array by the same plan
+    lat, pos = synth.si_diamond(1)
+    b = basis_gamma(lat, 8.0, (22, 21, 26), [8], [pos])
+    pkg_a, wnl = synth.kb_form_factors(b, lat)
+    b.update(pkg_a=pkg_a, wnl=wnl, lm_end=[4])
+    cell = Cell.from_arrays(b)
+    cell.set_veff(synth.local_potential(b["nr"], lat, pos))
+    psi = synth.wavefunctions(b, lat, 7, 3)
     ngw, nb = psi.shape
     d_in = torch.from_numpy(np.ascontiguousarray(psi.T)).to(dtype).cuda()
     ref = torch.zeros_like(d_in)
