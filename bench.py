@@ -3,7 +3,8 @@
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl engine|reference]
                     [--prec f32|f64]
-                    [--workload si64|si216|scf-si8|scf-si64|converge-si64|eig-si216|setup-si64|setup-si216]
+                    [--workload si64|si216|scf-si8|scf-si64|converge-si64|eig-si216|setup-si64|
+                                setup-si216|serve] [--rate R --jobs N --slots S]
 
 One step = one call of the degree-10 Chebyshev filter (chebyfilt.cpp:6-74)
 on the Si64 cell (64 atoms, a = 20.52 bohr, ecutwfc 15 Ha, 64^3 grid,
@@ -570,6 +571,97 @@ def run_eigsolve(args, rank, world, local_rank):
             "timing": "host wall clock around each solver call"}))
 
 
+# ------------------------------------------------------------------ SCF serving
+def run_serve(args, rank, world, local_rank):
+    """--workload serve: the SCF serving loop.  Jobs (isolated clusters of
+    2-64 atoms of four synthetic species with Gaussian wells of depth 1-4 Ha
+    and width 0.8-1.6 bohr, cubic boxes up to 24 bohr, ecutwfc 12-25 Ha,
+    ceil(0.6 * 4 * atoms) + 8 states, random start, Pulay mixing with beta 0.3
+    and a 6-step history, converged at |dETOT| <= 1e-6 Ha/atom) arrive by a
+    seeded Poisson process at --rate jobs/s and are submitted to the device
+    server (continuous batching over --slots concurrent jobs, admission by
+    HBM footprint).  Each precision form serves the same job sequence.
+    Latency = completion - arrival (queueing included); throughput = jobs /
+    (last completion - first arrival).  value = the mixed form's jobs/s."""
+    import tempfile
+
+    import torch
+    from pspw import PREC_F32, PREC_F64, replica, serve
+    torch.cuda.set_device(local_rank)
+    rng = np.random.default_rng(2028 + rank)
+    species = serve.species_set(rng)
+    tmp = tempfile.mkdtemp(prefix="pspw_serve_")
+    jobs = [serve.cluster_job(rng, os.path.join(tmp, f"job{k}"), species)
+            for k in range(args.jobs)]
+    arrivals = serve.poisson_arrivals(np.random.default_rng(77), args.rate, args.jobs)
+    warm = serve.cluster_job(np.random.default_rng(1), os.path.join(tmp, "warm"), species,
+                             natoms=4, ecut_ha=12.0, box=10.5)
+    clocks = ClockSampler(local_rank)
+    out_modes = {}
+    replica.barrier()
+    clocks.start()
+    for name, prec in (("fp64", PREC_F64), ("mixed", PREC_F32)):
+        srv = serve.Server(device=local_rank, slots=args.slots, filter_prec=prec,
+                           conv_per_atom=1e-6, max_scf_iter=100, pulay_beta=0.3, mixdim=6)
+        srv.wait(srv.submit(warm["dir"]))  # module loading, library handles
+        t0 = time.perf_counter()
+        ids, t_arr = [], []
+        for a, j in zip(arrivals, jobs):
+            delay = a - (time.perf_counter() - t0)
+            if delay > 0:
+                time.sleep(delay)
+            t_arr.append(srv.now())
+            ids.append(srv.submit(j["dir"]))
+        res = [srv.wait(i) for i in ids]
+        srv.close()
+        lat = [r["t_done"] - ta for r, ta in zip(res, t_arr)]
+        ok = [r["status"] == 0 for r in res]
+        conv = [bool(r["converged"]) for r in res]
+        span = max(r["t_done"] for r in res) - min(t_arr)
+        out_modes[name] = {
+            "jobs_per_s": round(len(res) / span, 4),
+            "latency_p50_s": round(serve.percentile(lat, 50), 4),
+            "latency_p99_s": round(serve.percentile(lat, 99), 4),
+            "latency_mean_s": round(float(np.mean(lat)), 4),
+            "queue_mean_s": round(float(np.mean([r["t_admit"] - ta
+                                                 for r, ta in zip(res, t_arr)])), 4),
+            "ok": int(sum(ok)), "converged": int(sum(conv)), "jobs": len(res),
+            "iterations_mean": round(float(np.mean([r["iterations"] for r in res])), 2),
+            "max_concurrent": int(max(sum(1 for q in res if q["t_admit"] <= r["t_admit"] < q["t_done"])
+                                      for r in res)),
+            "makespan_s": round(span, 3)}
+        out_modes[name]["_etot"] = [r["etot"] for r in res]
+    clocks.stop()
+    e64, e32 = out_modes["fp64"].pop("_etot"), out_modes["mixed"].pop("_etot")
+    nat = np.array([j["natoms"] for j in jobs])
+    de = np.abs(np.array(e32) - np.array(e64)) / nat
+    m = out_modes["mixed"]
+    if rank == 0:
+        print(json.dumps({
+            "metric": "SCF serving jobs/s (Poisson arrivals, continuous batching), mixed form; "
+                      "p50/p99 time-to-converged beside it",
+            "value": m["jobs_per_s"], "unit": "jobs/s", "n_gpus": world, "steps": args.jobs,
+            "warmup": 1, "ms_per_step": round(1e3 / m["jobs_per_s"], 3),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "c64 filter, f64 rest", "data": "synthetic",
+            "config": {"workload": f"serve: {args.jobs} cluster jobs (2-64 atoms, 4 species, "
+                                   f"box 10-24 bohr, ecutwfc 12-25 Ha), Poisson arrivals at "
+                                   f"{args.rate} jobs/s (seed 77), {args.slots} slots",
+                       "stop": "|dETOT| <= 1e-6 Ha/atom, at most 100 iterations",
+                       "mixing": "Pulay beta 0.3, history 6", "start": "random (IDIAG -1)",
+                       "parallelism": f"replica x{world}",
+                       "l2": "inputs larger than L2 for the large jobs; no flush"},
+            "modes": out_modes,
+            "etot_mixed_vs_fp64_ha_per_atom": {"max": float(de.max()),
+                                               "median": float(np.median(de))},
+            "cpu_baseline": {"value": None,
+                             "unavailable": "the reference runs one SCF job per process; one "
+                                            "such job of this mix takes minutes on the host"},
+            "clocks": clocks.summary(),
+            "timing": "server clock (host steady clock) from submission at the arrival time "
+                      "to the job's completion"}))
+
+
 # ------------------------------------------------------------------ engine arm
 def run_engine(args, rank, world, local_rank):
     import torch
@@ -826,6 +918,9 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-fp64-line", action="store_true",
                     help="si64/si216: skip the complex128 filter timed beside the FP32 one")
+    ap.add_argument("--rate", type=float, default=4.0, help="serve: arrivals per second")
+    ap.add_argument("--jobs", type=int, default=24, help="serve: jobs per precision form")
+    ap.add_argument("--slots", type=int, default=8, help="serve: concurrent jobs")
     ap.add_argument("--solvers", default="lobpcg,davidson",
                     help="eig-si216: comma-separated solvers (lobpcg, davidson)")
     args = ap.parse_args()
@@ -840,6 +935,16 @@ def main():
               "filter_window_ha": [LB, UB], "global_batch": 144 * world,
               "parallelism": f"replica x{world} (bands independent, no collective)",
               "l2": "flushed between steps (256 MB write, outside the timed interval)"}
+
+    if args.workload == "serve":
+        if args.impl == "reference":
+            if rank == 0:
+                print(json.dumps({"impl": "reference", "unavailable":
+                                  "the reference has no serving loop; it runs one SCF job per "
+                                  "process"}))
+            return
+        run_serve(args, rank, world, local_rank)
+        return
 
     if args.workload in ROW_WORKLOADS:
         if args.impl == "reference":

@@ -422,3 +422,15 @@ extern "C" int pspw_zgemm_dev(pspw_cell *c, char opa, int m, int n, int k, const
                        reinterpret_cast<const double2 *>(d_B), ldb,
                        make_double2(beta[0], beta[1]), reinterpret_cast<double2 *>(d_C), ldc);
 }
+
+extern "C" int pspw_eig_zheevd_dev(pspw_cell *c, double *d_A, int lda, double *d_w, int n) {
+  int rc = enter(c);
+  if (rc) return rc;
+  if (n < 0 || lda < std::max(1, n) || (n > 0 && (!d_A || !d_w)))
+    return fail(PSPW_ERR_ARG, "eig_zheevd_dev: bad arguments");
+  if (n == 0) return PSPW_OK;
+  int info = 0;
+  if ((rc = dev_zheevd(c, reinterpret_cast<double2 *>(d_A), lda, d_w, n, &info))) return rc;
+  if (info) return fail(PSPW_ERR_LAPACK, "zheevd: info = " + std::to_string(info));
+  return PSPW_OK;
+}

@@ -1,5 +1,7 @@
-// Device dense linear algebra for the eigensolvers.  The Hermitian
-// eigensolves, QR and Cholesky are cuSOLVER calls (the reference calls LAPACK
+// Device dense linear algebra for the eigensolvers.  Hermitian eigensolves
+// of order <= 160 (the Rayleigh-Ritz matrices of the SCF loop and of small
+// blocks) run on the engine's own kernels (heev.cu); larger ones, QR and
+// Cholesky are cuSOLVER calls (the reference calls LAPACK
 // zheevd/zgeqrf/zungqr/zpotrf at eig_zheevd.cpp:24, ortho_qr.cpp:19-26,
 // lobpcg_cpu.cpp:163); the triangular solve is cuBLAS ztrsm; the GEMMs and
 // the small column-wise kernels are this engine's own.
@@ -14,6 +16,7 @@
 #include "dense.h"
 #include "engine.h"
 #include "gemm.h"
+#include "heev.h"
 
 namespace pspw {
 
@@ -171,6 +174,14 @@ inline int grid_for(size_t n) { return (int)std::min<size_t>(4 * 148, (n + 255) 
 }  // namespace
 
 int dev_zheevd(pspw_cell *c, double2 *A, int lda, double *w, int n, int *info_out) {
+  if (n >= 1 && n <= kHeevMax) {
+    // the engine's own one-block reduction + bisection + inverse iteration
+    void *work = nullptr;
+    int rc = ws_reserve(c, kWsHeev, heev_small_workspace(n), &work);
+    if (rc) return rc;
+    if (info_out) *info_out = 0;
+    return dev_heev_small(c, A, lda, w, n, work);
+  }
   cusolverDnHandle_t h;
   int rc = solver_handle(c, &h);
   if (rc) return rc;

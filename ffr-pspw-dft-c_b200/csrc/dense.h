@@ -15,6 +15,7 @@ namespace pspw {
 int cublas_handle(pspw_cell *c, cublasHandle_t *h);
 // A (n x n, lda) <- eigenvectors, w[n] (device) <- ascending eigenvalues;
 // upper triangle of A is read (zheevd 'V','U').  *info_out = LAPACK info.
+// n <= 160: the engine's kernels (heev.cu, info always 0); else cuSOLVER.
 int dev_zheevd(pspw_cell *c, double2 *A, int lda, double *w, int n, int *info_out);
 // Householder QR of X (m x n, ld) replaced by its explicit Q (zgeqrf+zungqr).
 int dev_ortho_qr(pspw_cell *c, double2 *X, int ld, int m, int n, int *info_out);

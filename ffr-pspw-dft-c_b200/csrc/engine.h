@@ -127,7 +127,8 @@ enum WsSlot {
   kWsScfA = 34,        // SCF-piece host entry points: vectors on the device
   kWsScfB = 35,
   kWsStickX = 36,      // the filter's block in stick order
-  kWsCount = 37
+  kWsHeev = 37,        // the small Hermitian eigensolver's workspace
+  kWsCount = 38
 };
 
 struct Timing {

@@ -867,6 +867,18 @@ int pspw_system_info(pspw_system *S, int *dims16, double *scal16) {
   return PSPW_OK;
 }
 
+int pspw_system_species(pspw_system *S, int *natoms, int *nproj) {
+  if (!S || !natoms || !nproj) return fail(PSPW_ERR_ARG, "system_species: null argument");
+  int na = 0, np = 0;
+  for (int s = 0; s < S->nsp; s++) {
+    na += S->na[s];
+    np += S->na[s] * S->lm_end[s];
+  }
+  *natoms = na;
+  *nproj = np;
+  return PSPW_OK;
+}
+
 int pspw_system_params(pspw_system *S, pspw_scf_params *p) {
   if (!S || !p) return fail(PSPW_ERR_ARG, "system_params: null argument");
   const InputData &in = S->in;

@@ -1,0 +1,717 @@
+// Small dense Hermitian eigensolver on the device (n <= kHeevMax), for the
+// Rayleigh-Ritz step of the Chebyshev-filtered SCF loop (the eig_zheevd call
+// of ChebySCFLoop.cpp:299 on the (NX+2) x (NX+2) subspace matrix) and for
+// the eigenvalues of tridiagonal Lanczos matrices (ChebySCFLoop.cpp:186-190).
+//
+// The library eigensolver spends most of its time on launch and host
+// synchronisation overhead at this size; here the whole problem lives in one
+// block's shared memory for the O(n^3) part, and four launches do the rest:
+//
+//  1 k_hetrd      one block of 1024 threads.  Householder reduction to real
+//                 symmetric tridiagonal form T = Q^H A Q (Golub & Van Loan,
+//                 Matrix Computations, 4th ed., Alg. 8.3.1, with the complex
+//                 reflector choice that leaves the off-diagonal real).  The
+//                 lower triangle is held packed row by row in shared memory
+//                 (n (n+1)/2 complex, 206 KB at n = 160); per step the
+//                 Hermitian matrix-vector product (rows: contiguous, columns:
+//                 a gather) and the rank-2 update run warp per row.  All
+//                 reductions are fixed-order trees, so results are bitwise
+//                 repeatable.
+//  2 k_tri_bisect eigenvalues of T by bisection on Sturm counts, one warp per
+//                 eigenvalue: the 32 lanes evaluate the count at 32 interior
+//                 points of the current interval (5 bits per round).  The
+//                 count uses the characteristic-polynomial recurrence
+//                 p_i = (d_i - x) p_{i-1} - e_{i-1}^2 p_{i-2} with exact
+//                 power-of-two rescaling, which needs no division.
+//  3 k_tri_invit  eigenvectors of T by inverse iteration, one block per
+//                 cluster of eigenvalues closer than 1e-3 ||T|| (the
+//                 clustering threshold of LAPACK's dstein): every member's
+//                 (T - lambda I) is factored once (LU with partial pivoting,
+//                 small pivots raised to eps ||T||), three solves with block
+//                 Gram-Schmidt (twice) between them, then a Rayleigh-Ritz
+//                 step inside the cluster (parallel Jacobi in one warp)
+//                 unless its eigenvalues are equal to rounding.
+//  4 k_back_tr    eigenvectors of A = Q Z, one warp per vector, reflectors
+//                 applied from the last to the first.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdint>
+#include <string>
+
+#include "common.cuh"
+#include "engine.h"
+#include "heev.h"
+
+namespace pspw {
+namespace {
+
+constexpr int kT1 = 1024;      // threads of the reduction block
+constexpr int kMaxWarpsT1 = kT1 / 32;
+constexpr double kEps = 2.220446049250313e-16;
+constexpr int kInvitThreads = 128;
+constexpr int kInvitIters = 3;
+constexpr int kRRMax = 32;     // largest cluster with a Rayleigh-Ritz step
+
+__device__ __forceinline__ int lp(int i, int j) { return i * (i + 1) / 2 + j; }  // j <= i
+
+__device__ __forceinline__ double2 cconj(double2 a) { return make_double2(a.x, -a.y); }
+
+// sum over the block of one value per thread; every thread gets the same
+// bits (warp xor tree, then every thread adds the warp sums in order)
+__device__ double block_sum(double v, double *red) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  __syncthreads();
+  if (lane == 0) red[w] = v;
+  __syncthreads();
+  double s = 0.0;
+  for (int i = 0; i < nw; i++) s += red[i];
+  return s;
+}
+
+__device__ __forceinline__ double warp_sum(double v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+
+// ---------------------------------------------------------------- 1 reduction
+// A: n x n column-major (lda), only the upper triangle is read (as zheevd
+// 'U').  Out: d[n], e[n-1], reflectors V (column k holds v_k on rows
+// k+1..n-1, v_k(k+1) = 1), tau[n-1]; H_k = I - tau_k v_k v_k^H, Q = H_0 ...
+__global__ void __launch_bounds__(kT1, 1)
+    k_hetrd(const double2 *__restrict__ A, int lda, int n, double *__restrict__ d,
+            double *__restrict__ e, double2 *__restrict__ V, double2 *__restrict__ tau) {
+  extern __shared__ double2 L[];  // packed lower triangle, row-major
+  __shared__ double2 v[kHeevMax], y[kHeevMax];
+  __shared__ double red[kMaxWarpsT1];
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nw = blockDim.x >> 5;
+  const int nt = blockDim.x;
+  // L(i, j) = conj(A(j, i)) for j <= i
+  for (int i = warp; i < n; i += nw)
+    for (int j = lane; j <= i; j += 32) L[lp(i, j)] = cconj(A[j + (size_t)i * lda]);
+  __syncthreads();
+  for (int k = 0; k < n - 1; k++) {
+    const int k1 = k + 1;
+    const double2 alpha = L[lp(k1, k)];
+    double part = 0.0;
+    for (int i = k1 + 1 + tid; i < n; i += nt) {
+      const double2 x = L[lp(i, k)];
+      part += x.x * x.x + x.y * x.y;
+    }
+    const double xn2 = block_sum(part, red);
+    // the reflector: H^H (alpha, x) = (beta, 0), beta real; every thread
+    // computes the same values from the same inputs
+    double beta;
+    double2 t, sc = make_double2(0.0, 0.0);
+    if (xn2 == 0.0 && alpha.y == 0.0) {
+      beta = alpha.x;
+      t = make_double2(0.0, 0.0);
+    } else {
+      beta = -copysign(sqrt(alpha.x * alpha.x + alpha.y * alpha.y + xn2), alpha.x);
+      t = make_double2((beta - alpha.x) / beta, -alpha.y / beta);
+      const double2 den = make_double2(alpha.x - beta, alpha.y);  // 1 / (alpha - beta)
+      const double dd = den.x * den.x + den.y * den.y;
+      sc = make_double2(den.x / dd, -den.y / dd);
+    }
+    const bool reflect = t.x != 0.0 || t.y != 0.0;
+    for (int i = k1 + tid; i < n; i += nt) {
+      const double2 vi = i == k1 ? make_double2(1.0, 0.0)
+                                 : (reflect ? cmul(L[lp(i, k)], sc) : make_double2(0.0, 0.0));
+      v[i] = vi;
+      V[(size_t)k * n + i] = vi;
+    }
+    if (tid == 0) {
+      d[k] = L[lp(k, k)].x;
+      e[k] = beta;
+      tau[k] = t;
+    }
+    __syncthreads();
+    if (!reflect) continue;  // uniform
+    // y = t * A22 v, A22 the trailing Hermitian block (rows and columns >= k1)
+    for (int i = k1 + warp; i < n; i += nw) {
+      double sr = 0.0, si = 0.0;
+      for (int j = k1 + lane; j <= i; j += 32) {  // row i of the lower part
+        const double2 a = L[lp(i, j)], b = v[j];
+        sr = fma(a.x, b.x, sr);
+        sr = fma(-a.y, b.y, sr);
+        si = fma(a.x, b.y, si);
+        si = fma(a.y, b.x, si);
+      }
+      for (int j = i + 1 + lane; j < n; j += 32) {  // column i below the diagonal, conjugated
+        const double2 a = L[lp(j, i)], b = v[j];
+        sr = fma(a.x, b.x, sr);
+        sr = fma(a.y, b.y, sr);
+        si = fma(a.x, b.y, si);
+        si = fma(-a.y, b.x, si);
+      }
+      sr = warp_sum(sr);
+      si = warp_sum(si);
+      if (lane == 0) y[i] = cmul(t, make_double2(sr, si));
+    }
+    __syncthreads();
+    // w = y - (1/2) t (y^H v) v
+    double pr = 0.0, pi = 0.0;
+    for (int i = k1 + tid; i < n; i += nt) {
+      const double2 a = y[i], b = v[i];
+      pr += a.x * b.x + a.y * b.y;
+      pi += a.x * b.y - a.y * b.x;
+    }
+    const double yr = block_sum(pr, red);
+    const double yi = block_sum(pi, red);
+    const double2 al = cmul(make_double2(-0.5 * t.x, -0.5 * t.y), make_double2(yr, yi));
+    for (int i = k1 + tid; i < n; i += nt) y[i] = y[i] + cmul(al, v[i]);
+    __syncthreads();
+    // A22 -= v w^H + w v^H (lower part; the diagonal stays real)
+    for (int i = k1 + warp; i < n; i += nw) {
+      const double2 vi = v[i], wi = y[i];
+      for (int j = k1 + lane; j <= i; j += 32) {
+        const double2 vj = v[j], wj = y[j];
+        double2 a = L[lp(i, j)];
+        a.x -= vi.x * wj.x + vi.y * wj.y + wi.x * vj.x + wi.y * vj.y;
+        a.y -= vi.y * wj.x - vi.x * wj.y + wi.y * vj.x - wi.x * vj.y;
+        if (j == i) a.y = 0.0;
+        L[lp(i, j)] = a;
+      }
+    }
+    __syncthreads();
+  }
+  if (tid == 0) d[n - 1] = L[lp(n - 1, n - 1)].x;
+}
+
+// ---------------------------------------------------------------- 2 bisection
+// number of eigenvalues of T below x (e2 = squared off-diagonal)
+__device__ int sturm_below(const double *d, const double *e2, int n, double x) {
+  double pm = 1.0, p = d[0] - x;
+  int s = p == 0.0 ? -1 : (p < 0.0 ? -1 : 1);
+  int cnt = s < 0;
+  for (int i = 1; i < n; i++) {
+    const double pn = fma(d[i] - x, p, -e2[i - 1] * pm);
+    pm = p;
+    p = pn;
+    const double ap = fabs(p);
+    if (ap > 0x1p+200) {
+      p *= 0x1p-200;
+      pm *= 0x1p-200;
+    } else if (ap < 0x1p-200 && ap != 0.0) {
+      p *= 0x1p+200;
+      pm *= 0x1p+200;
+    }
+    const int sn = p == 0.0 ? -s : (p < 0.0 ? -1 : 1);
+    cnt += sn != s;
+    s = sn;
+  }
+  return cnt;
+}
+
+// Gershgorin interval and ||T||_inf of the tridiagonal (every thread of the
+// calling warp gets the same values)
+__device__ void tri_bounds(const double *d, const double *e, int n, double *lo, double *hi,
+                           double *tn) {
+  double a = INFINITY, b = -INFINITY, c = 0.0;
+  for (int i = threadIdx.x & 31; i < n; i += 32) {
+    const double r = (i > 0 ? fabs(e[i - 1]) : 0.0) + (i + 1 < n ? fabs(e[i]) : 0.0);
+    a = fmin(a, d[i] - r);
+    b = fmax(b, d[i] + r);
+    c = fmax(c, fabs(d[i]) + r);
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    a = fmin(a, __shfl_xor_sync(0xffffffffu, a, o));
+    b = fmax(b, __shfl_xor_sync(0xffffffffu, b, o));
+    c = fmax(c, __shfl_xor_sync(0xffffffffu, c, o));
+  }
+  *lo = a;
+  *hi = b;
+  *tn = c;
+}
+
+// one warp per eigenvalue index (ascending); d, e: device, n <= max shared
+__global__ void __launch_bounds__(128) k_tri_bisect(const double *__restrict__ dg,
+                                                    const double *__restrict__ eg, int n,
+                                                    double *__restrict__ lam) {
+  extern __shared__ double sh[];
+  double *d = sh, *e = sh + n, *e2 = sh + 2 * n;
+  for (int i = threadIdx.x; i < n; i += blockDim.x) {
+    d[i] = dg[i];
+    if (i + 1 < n) {
+      e[i] = eg[i];
+      e2[i] = eg[i] * eg[i];
+    }
+  }
+  __syncthreads();
+  const int j = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+  const int lane = threadIdx.x & 31;
+  if (j >= n) return;  // whole warp
+  double lo, hi, tn;
+  tri_bounds(d, e, n, &lo, &hi, &tn);
+  const double pad = 2.0 * kEps * tn + 1e-300;
+  lo -= pad;
+  hi += pad;
+  for (int it = 0; it < 20; it++) {
+    if (hi - lo <= fmax(2.0 * kEps * fmax(fabs(lo), fabs(hi)), kEps * tn)) break;
+    const double x = lo + (hi - lo) * (double)(lane + 1) / 33.0;
+    const unsigned above = __ballot_sync(0xffffffffu, sturm_below(d, e2, n, x) > j);
+    const double xs = __shfl_sync(0xffffffffu, x, above ? __ffs(above) - 1 : 31);
+    if (above) {
+      const int f = __ffs(above) - 1;
+      const double xl = __shfl_sync(0xffffffffu, x, f > 0 ? f - 1 : 0);
+      if (f > 0) lo = xl;
+      hi = xs;
+    } else {
+      lo = xs;
+    }
+  }
+  if (lane == 0) lam[j] = 0.5 * (lo + hi);
+}
+
+// ---------------------------------------------------------------- 3 vectors of T
+// LU of (T - s I) with row interchanges: u0 (pivots, stored inverted), u1,
+// u2 (the two super-diagonals), ml (multipliers), pv (interchange flags)
+struct TriLU {
+  double u0[kHeevMax], u1[kHeevMax], u2[kHeevMax], ml[kHeevMax];
+  unsigned char pv[kHeevMax];
+};
+
+__device__ void tri_factor(const double *d, const double *e, int n, double s, double floor_,
+                           TriLU &f) {
+  double c0 = d[0] - s, c1 = n > 1 ? e[0] : 0.0, c2 = 0.0;
+  for (int i = 0; i < n - 1; i++) {
+    const double s0 = e[i], s1 = d[i + 1] - s, s2 = i + 2 < n ? e[i + 1] : 0.0;
+    if (fabs(c0) >= fabs(s0)) {
+      if (fabs(c0) < floor_) c0 = c0 >= 0.0 ? floor_ : -floor_;
+      const double m = s0 / c0;
+      f.u0[i] = 1.0 / c0;
+      f.u1[i] = c1;
+      f.u2[i] = c2;
+      f.ml[i] = m;
+      f.pv[i] = 0;
+      c0 = s1 - m * c1;
+      c1 = s2 - m * c2;
+      c2 = 0.0;
+    } else {
+      const double m = c0 / s0;
+      f.u0[i] = 1.0 / s0;
+      f.u1[i] = s1;
+      f.u2[i] = s2;
+      f.ml[i] = m;
+      f.pv[i] = 1;
+      c0 = c1 - m * s1;
+      c1 = c2 - m * s2;
+      c2 = 0.0;
+    }
+  }
+  if (fabs(c0) < floor_) c0 = c0 >= 0.0 ? floor_ : -floor_;
+  f.u0[n - 1] = 1.0 / c0;
+}
+
+// z <- (T - s I)^-1 z (strided column of Z), scaled to avoid overflow
+__device__ void tri_solve(const TriLU &f, int n, double *z) {
+  for (int i = 0; i < n - 1; i++) {
+    if (f.pv[i]) {
+      const double t = z[i];
+      z[i] = z[i + 1];
+      z[i + 1] = t;
+    }
+    z[i + 1] = fma(-f.ml[i], z[i], z[i + 1]);
+  }
+  double scale = 1.0;
+  for (int i = n - 1; i >= 0; i--) {
+    double s = z[i] * scale;
+    if (i + 1 < n) s = fma(-f.u1[i], z[i + 1], s);
+    if (i + 2 < n) s = fma(-f.u2[i], z[i + 2], s);
+    s *= f.u0[i];
+    z[i] = s;
+    if (fabs(s) > 0x1p+600) {  // rescale what is done; the rest of the
+      for (int r = i; r < n; r++) z[r] *= 0x1p-600;  // right-hand side follows
+      scale *= 0x1p-600;
+    }
+  }
+}
+
+__device__ __forceinline__ double start_value(int i, int col) {
+  uint32_t h = (uint32_t)i * 2654435761u ^ ((uint32_t)col * 2246822519u + 0x9e3779b9u);
+  h ^= h >> 15;
+  h *= 2246822519u;
+  h ^= h >> 13;
+  return (double)(h & 0xffffu) * (1.0 / 65536.0) - 0.5 + 1e-3;
+}
+
+// One block per eigenvalue index j; the block of a cluster's first index
+// computes the cluster's vectors into columns of Z (n x n, column-major).
+__global__ void __launch_bounds__(kInvitThreads)
+    k_tri_invit(const double *__restrict__ d, const double *__restrict__ e,
+                const double *__restrict__ lam, int n, double *__restrict__ Z,
+                TriLU *__restrict__ lu) {
+  __shared__ double red[kInvitThreads / 32];
+  __shared__ double S[kRRMax * kRRMax], U[kRRMax * kRRMax];
+  __shared__ double coef[kHeevMax];
+  const int j = blockIdx.x, tid = threadIdx.x;
+  double glo, ghi, tn;
+  tri_bounds(d, e, n, &glo, &ghi, &tn);  // every warp computes the same
+  const double gaptol = 1e-3 * tn;
+  if (j > 0 && !(lam[j] - lam[j - 1] > gaptol)) return;  // not a cluster's first index
+  int c = 1;
+  while (j + c < n && lam[j + c] - lam[j + c - 1] <= gaptol) c++;
+  double *zc = Z + (size_t)j * n;  // the cluster's c columns
+  if (tn == 0.0) {  // T = 0: the unit vectors
+    for (int r = tid; r < c * n; r += blockDim.x) zc[r] = (r % n) == j + r / n ? 1.0 : 0.0;
+    return;
+  }
+  const double floor_ = kEps * fmax(tn, 1e-200);
+  for (int m = tid; m < c; m += blockDim.x) {
+    tri_factor(d, e, n, lam[j + m], floor_, lu[j + m]);
+    for (int i = 0; i < n; i++) zc[(size_t)m * n + i] = start_value(i, j + m);
+  }
+  __syncthreads();
+  for (int it = 0; it < kInvitIters; it++) {
+    for (int m = tid; m < c; m += blockDim.x) tri_solve(lu[j + m], n, zc + (size_t)m * n);
+    __syncthreads();
+    // block Gram-Schmidt, twice per column, in column order
+    for (int m = 0; m < c; m++) {
+      double *zm = zc + (size_t)m * n;
+      for (int pass = 0; pass < 2; pass++) {
+        for (int q = 0; q < m; q++) {
+          double p = 0.0;
+          for (int i = tid; i < n; i += blockDim.x) p += zc[(size_t)q * n + i] * zm[i];
+          const double s = block_sum(p, red);
+          if (tid == 0) coef[q] = s;
+        }
+        __syncthreads();
+        for (int i = tid; i < n; i += blockDim.x) {
+          double v = zm[i];
+          for (int q = 0; q < m; q++) v = fma(-coef[q], zc[(size_t)q * n + i], v);
+          zm[i] = v;
+        }
+        __syncthreads();
+      }
+      double p = 0.0;
+      for (int i = tid; i < n; i += blockDim.x) p += zm[i] * zm[i];
+      const double nrm = sqrt(block_sum(p, red));
+      const double inv = nrm > 0.0 ? 1.0 / nrm : 0.0;
+      for (int i = tid; i < n; i += blockDim.x) zm[i] *= inv;
+      __syncthreads();
+    }
+  }
+  // Rayleigh-Ritz inside a cluster whose eigenvalues differ beyond rounding
+  if (c > 1 && c <= kRRMax && lam[j + c - 1] - lam[j] > 4.0 * c * floor_) {
+    const int warp = tid >> 5, lane = tid & 31, nw = blockDim.x >> 5;
+    for (int ab = warp; ab < c * c; ab += nw) {  // S(a, b) = z_a . T z_b
+      const int a = ab % c, b = ab / c;
+      const double *za = zc + (size_t)a * n, *zb = zc + (size_t)b * n;
+      double p = 0.0;
+      for (int i = lane; i < n; i += 32) {
+        double tz = d[i] * zb[i];
+        if (i > 0) tz = fma(e[i - 1], zb[i - 1], tz);
+        if (i + 1 < n) tz = fma(e[i], zb[i + 1], tz);
+        p = fma(za[i], tz, p);
+      }
+      p = warp_sum(p);
+      if (lane == 0) S[a + b * kRRMax] = p;
+    }
+    __syncthreads();
+    if (warp == 0) {
+      // symmetrise, U = I, then cyclic parallel Jacobi (round-robin pairs,
+      // one lane per pair; c odd gets a dummy index)
+      for (int r = lane; r < c * c; r += 32) {
+        const int a = r % c, b = r / c;
+        U[a + b * kRRMax] = a == b ? 1.0 : 0.0;
+      }
+      __syncwarp();
+      for (int r = lane; r < c * c; r += 32) {
+        const int a = r % c, b = r / c;
+        if (a < b) {
+          const double s = 0.5 * (S[a + b * kRRMax] + S[b + a * kRRMax]);
+          S[a + b * kRRMax] = s;
+          S[b + a * kRRMax] = s;
+        }
+      }
+      __syncwarp();
+      const int cp = c + (c & 1);
+      for (int sweep = 0; sweep < 30; sweep++) {
+        double off = 0.0, dia = 0.0;
+        for (int r = lane; r < c * c; r += 32) {
+          const int a = r % c, b = r / c;
+          const double v = S[a + b * kRRMax];
+          if (a != b) off += v * v; else dia += v * v;
+        }
+        off = warp_sum(off);
+        dia = warp_sum(dia);
+        if (off <= 1e-30 * dia || off == 0.0) break;
+        for (int round = 0; round < cp - 1; round++) {
+          // pair `lane` of this round (circle method, index cp-1 fixed)
+          int p = -1, q = -1;
+          if (lane < cp / 2) {
+            const int a = lane == 0 ? cp - 1 : (round + lane) % (cp - 1);
+            const int b = (round + cp - 1 - lane) % (cp - 1);
+            p = min(a, b);
+            q = max(a, b);
+            if (q >= c) p = q = -1;  // dummy index
+          }
+          double cs = 1.0, sn = 0.0;
+          if (p >= 0) {
+            const double app = S[p + p * kRRMax], aqq = S[q + q * kRRMax],
+                         apq = S[p + q * kRRMax];
+            if (apq != 0.0) {
+              const double th = 0.5 * (aqq - app) / apq;
+              const double tt = copysign(1.0, th) / (fabs(th) + sqrt(th * th + 1.0));
+              cs = 1.0 / sqrt(tt * tt + 1.0);
+              sn = tt * cs;
+            }
+          }
+          __syncwarp();
+          // columns p, q of S and U
+          if (p >= 0 && sn != 0.0)
+            for (int r = 0; r < c; r++) {
+              const double sp = S[r + p * kRRMax], sq = S[r + q * kRRMax];
+              S[r + p * kRRMax] = cs * sp - sn * sq;
+              S[r + q * kRRMax] = sn * sp + cs * sq;
+              const double up = U[r + p * kRRMax], uq = U[r + q * kRRMax];
+              U[r + p * kRRMax] = cs * up - sn * uq;
+              U[r + q * kRRMax] = sn * up + cs * uq;
+            }
+          __syncwarp();
+          // rows p, q of S
+          if (p >= 0 && sn != 0.0)
+            for (int r = 0; r < c; r++) {
+              const double sp = S[p + r * kRRMax], sq = S[q + r * kRRMax];
+              S[p + r * kRRMax] = cs * sp - sn * sq;
+              S[q + r * kRRMax] = sn * sp + cs * sq;
+            }
+          __syncwarp();
+        }
+      }
+      // order the Ritz pairs ascending (selection sort of the permutation)
+      if (lane == 0) {
+        int perm[kRRMax];
+        for (int a = 0; a < c; a++) perm[a] = a;
+        for (int a = 0; a < c; a++) {
+          int best = a;
+          for (int b = a + 1; b < c; b++)
+            if (S[perm[b] * (kRRMax + 1)] < S[perm[best] * (kRRMax + 1)]) best = b;
+          const int t2 = perm[a];
+          perm[a] = perm[best];
+          perm[best] = t2;
+        }
+        for (int a = 0; a < c; a++) coef[a] = (double)perm[a];
+      }
+    }
+    __syncthreads();
+    // z' = Z U(:, perm), one row per thread
+    for (int i = tid; i < n; i += blockDim.x) {
+      double row[kRRMax];
+      for (int a = 0; a < c; a++) row[a] = zc[(size_t)a * n + i];
+      for (int a = 0; a < c; a++) {
+        const int pa = (int)coef[a];
+        double s = 0.0;
+        for (int b = 0; b < c; b++) s = fma(row[b], U[b + pa * kRRMax], s);
+        zc[(size_t)a * n + i] = s;
+      }
+    }
+  }
+}
+
+// ---------------------------------------------------------------- 4 back-transform
+// column j of A <- Q z_j, one warp per column; lane l holds rows l, l+32, ..
+__global__ void __launch_bounds__(128) k_back_tr(const double2 *__restrict__ V,
+                                                 const double2 *__restrict__ tau,
+                                                 const double *__restrict__ Z, int n,
+                                                 double2 *__restrict__ A, int lda) {
+  constexpr int R = (kHeevMax + 31) / 32;
+  const int j = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+  const int lane = threadIdx.x & 31;
+  if (j >= n) return;
+  double2 y[R];
+#pragma unroll
+  for (int r = 0; r < R; r++) {
+    const int i = lane + 32 * r;
+    y[r] = make_double2(i < n ? Z[(size_t)j * n + i] : 0.0, 0.0);
+  }
+  for (int k = n - 2; k >= 0; k--) {
+    const double2 t = tau[k];
+    if (t.x == 0.0 && t.y == 0.0) continue;
+    const double2 *vk = V + (size_t)k * n;
+    double sr = 0.0, si = 0.0;  // s = v^H y over rows > k
+#pragma unroll
+    for (int r = 0; r < R; r++) {
+      const int i = lane + 32 * r;
+      if (i > k && i < n) {
+        const double2 a = vk[i];
+        sr += a.x * y[r].x + a.y * y[r].y;
+        si += a.x * y[r].y - a.y * y[r].x;
+      }
+    }
+    sr = warp_sum(sr);
+    si = warp_sum(si);
+    const double2 ts = cmul(t, make_double2(sr, si));
+#pragma unroll
+    for (int r = 0; r < R; r++) {
+      const int i = lane + 32 * r;
+      if (i > k && i < n) y[r] = y[r] - cmul(vk[i], ts);
+    }
+  }
+#pragma unroll
+  for (int r = 0; r < R; r++) {
+    const int i = lane + 32 * r;
+    if (i < n) A[(size_t)j * lda + i] = y[r];
+  }
+}
+
+// ---------------------------------------------------------------- Cholesky
+// G = U^H U (upper U) and U^-1, one block, for the CholeskyQR passes of the
+// span orthonormalisation: G (n x n, ldg, upper triangle read) -> Uinv
+// (n x n, ldu, upper, zeros below), stat[0] = 0 or k + 1 when the k-th pivot
+// is not positive, stat[1] = max |U_kk| / min |U_kk|.  Works on the lower
+// factor L = U^H, packed row-major in shared memory.
+__global__ void __launch_bounds__(kT1, 1)
+    k_chol_inv(const double2 *__restrict__ G, int ldg, int n, double2 *__restrict__ Uinv, int ldu,
+               double *__restrict__ stat) {
+  extern __shared__ double2 L[];
+  __shared__ double2 stage[kHeevMax];
+  __shared__ int s_fail;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nw = blockDim.x >> 5;
+  for (int i = warp; i < n; i += nw)
+    for (int j = lane; j <= i; j += 32) L[lp(i, j)] = cconj(G[j + (size_t)i * ldg]);
+  if (tid == 0) s_fail = 0;
+  __syncthreads();
+  double dmax = 0.0, dmin = INFINITY;
+  for (int k = 0; k < n; k++) {
+    const double akk = L[lp(k, k)].x;  // every thread reads the same value
+    if (!(akk > 0.0)) {
+      if (tid == 0) s_fail = k + 1;
+      break;  // uniform
+    }
+    const double dk = sqrt(akk), inv = 1.0 / dk;
+    dmax = fmax(dmax, dk);
+    dmin = fmin(dmin, dk);
+    __syncthreads();  // all reads of L(k, k) done
+    if (tid == 0) L[lp(k, k)] = make_double2(dk, 0.0);
+    for (int i = k + 1 + tid; i < n; i += blockDim.x) {
+      const double2 a = L[lp(i, k)];
+      L[lp(i, k)] = make_double2(a.x * inv, a.y * inv);
+    }
+    __syncthreads();
+    // trailing update L(i, j) -= L(i, k) conj(L(j, k)), k < j <= i
+    for (int i = k + 1 + warp; i < n; i += nw) {
+      const double2 lik = L[lp(i, k)];
+      for (int j = k + 1 + lane; j <= i; j += 32) {
+        const double2 ljk = L[lp(j, k)];
+        double2 a = L[lp(i, j)];
+        a.x -= lik.x * ljk.x + lik.y * ljk.y;
+        a.y -= lik.y * ljk.x - lik.x * ljk.y;
+        L[lp(i, j)] = a;
+      }
+    }
+    __syncthreads();
+  }
+  __syncthreads();
+  if (s_fail) {
+    if (tid == 0) {
+      stat[0] = (double)s_fail;
+      stat[1] = INFINITY;
+    }
+    return;
+  }
+  // M = L^-1 in place, row by row: M(i, i) = 1 / L(i, i),
+  // M(i, j) = -M(i, i) sum_{k=j}^{i-1} L(i, k) M(k, j)  (j < i); rows < i of
+  // the packed array already hold M, row i still holds L until the row is
+  // complete (its new values wait in `stage`)
+  for (int i = 0; i < n; i++) {
+    const double mii = 1.0 / L[lp(i, i)].x;
+    for (int j = warp; j < i; j += nw) {
+      double sr = 0.0, si = 0.0;
+      for (int k = j + lane; k < i; k += 32) {
+        const double2 a = L[lp(i, k)], b = L[lp(k, j)];
+        sr = fma(a.x, b.x, sr);
+        sr = fma(-a.y, b.y, sr);
+        si = fma(a.x, b.y, si);
+        si = fma(a.y, b.x, si);
+      }
+      sr = warp_sum(sr);
+      si = warp_sum(si);
+      if (lane == 0) stage[j] = make_double2(-mii * sr, -mii * si);
+    }
+    __syncthreads();
+    for (int j = tid; j < i; j += blockDim.x) L[lp(i, j)] = stage[j];
+    if (tid == 0) L[lp(i, i)] = make_double2(mii, 0.0);
+    __syncthreads();
+  }
+  // Uinv = M^H: Uinv(r, c) = conj(M(c, r)) for r <= c, 0 below
+  for (int cidx = warp; cidx < n; cidx += nw)
+    for (int r = lane; r < n; r += 32)
+      Uinv[(size_t)cidx * ldu + r] = r <= cidx ? cconj(L[lp(cidx, r)]) : make_double2(0.0, 0.0);
+  if (tid == 0) {
+    stat[0] = 0.0;
+    stat[1] = dmax / dmin;
+  }
+}
+
+}  // namespace
+
+size_t heev_small_workspace(int n) {
+  const size_t nn = (size_t)n * n;
+  return sizeof(double2) * (nn + n) + sizeof(double) * (nn + 2 * (size_t)n) +
+         sizeof(TriLU) * (size_t)n + 6 * 256;
+}
+
+int dev_heev_small(pspw_cell *c, double2 *A, int lda, double *w, int n, void *work) {
+  if (n < 1 || n > kHeevMax || lda < n)
+    return fail(PSPW_ERR_ARG, "heev_small: n must be in 1.." + std::to_string(kHeevMax));
+  cudaStream_t st = c->stream;
+  const size_t nn = (size_t)n * n;
+  char *p = static_cast<char *>(work);
+  auto take = [&](size_t bytes) {
+    void *q = p;
+    p += (bytes + 255) / 256 * 256;
+    return q;
+  };
+  double2 *V = static_cast<double2 *>(take(sizeof(double2) * nn));
+  double2 *tau = static_cast<double2 *>(take(sizeof(double2) * n));
+  double *d = static_cast<double *>(take(sizeof(double) * n));
+  double *e = static_cast<double *>(take(sizeof(double) * n));
+  double *Z = static_cast<double *>(take(sizeof(double) * nn));
+  TriLU *lu = static_cast<TriLU *>(take(sizeof(TriLU) * n));
+  const int smem1 = (int)(sizeof(double2) * (size_t)n * (n + 1) / 2);
+  if (smem1 > 48 * 1024)
+    PSPW_CUDA(cudaFuncSetAttribute(k_hetrd, cudaFuncAttributeMaxDynamicSharedMemorySize, smem1));
+  k_hetrd<<<1, kT1, smem1, st>>>(A, lda, n, d, e, V, tau);
+  const int wpb = 4;
+  k_tri_bisect<<<(n + wpb - 1) / wpb, 32 * wpb, sizeof(double) * 3 * n, st>>>(d, e, n, w);
+  k_tri_invit<<<n, kInvitThreads, 0, st>>>(d, e, w, n, Z, lu);
+  k_back_tr<<<(n + 3) / 4, 128, 0, st>>>(V, tau, Z, n, A, lda);
+  c->kernel_launches += 4;
+  PSPW_CUDA(cudaGetLastError());
+  return PSPW_OK;
+}
+
+int dev_chol_inv_upper(pspw_cell *c, const double2 *G, int ldg, int n, double2 *Uinv, int ldu,
+                       double *stat) {
+  if (n < 1 || n > kHeevMax || ldg < n || ldu < n)
+    return fail(PSPW_ERR_ARG, "chol_inv_upper: n must be in 1.." + std::to_string(kHeevMax));
+  const int smem = (int)(sizeof(double2) * (size_t)n * (n + 1) / 2);
+  if (smem > 48 * 1024)
+    PSPW_CUDA(
+        cudaFuncSetAttribute(k_chol_inv, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+  k_chol_inv<<<1, kT1, smem, c->stream>>>(G, ldg, n, Uinv, ldu, stat);
+  c->kernel_launches++;
+  PSPW_CUDA(cudaGetLastError());
+  return PSPW_OK;
+}
+
+int dev_tri_eigvals(pspw_cell *c, const double *d, const double *e, int n, double *w) {
+  if (n < 1 || n > kTriEigMax) return fail(PSPW_ERR_ARG, "tri_eigvals: bad size");
+  const int wpb = 4;
+  const size_t smem = sizeof(double) * 3 * (size_t)n;
+  if (smem > 48 * 1024)
+    PSPW_CUDA(
+        cudaFuncSetAttribute(k_tri_bisect, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  k_tri_bisect<<<(n + wpb - 1) / wpb, 32 * wpb, smem, c->stream>>>(d, e, n, w);
+  c->kernel_launches++;
+  PSPW_CUDA(cudaGetLastError());
+  return PSPW_OK;
+}
+
+}  // namespace pspw

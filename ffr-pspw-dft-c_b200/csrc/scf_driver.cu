@@ -24,6 +24,7 @@
 #include "dense.h"
 #include "engine.h"
 #include "gemm.h"
+#include "heev.h"
 #include "scf.h"
 #include "solvers.h"
 
@@ -81,45 +82,38 @@ double induced_norm_mat(const double *A, int lda, int N) {
 // basis of the same span give the same Ritz pairs, since Rayleigh-Ritz
 // depends on the span only (Q and Q D, D a diagonal of unit-modulus
 // phases, differ in the phases of the Ritz vectors alone).  CholeskyQR2:
-// twice G = X^H X = U^H U, X <- X U^-1 (two Gram GEMMs, two small Cholesky
-// factorisations, two triangular solves, instead of the geqrf + ungqr
-// panel sweeps).  Stable while cond(X) stays well below 1/sqrt(eps); the
-// ratio of the largest to the smallest diagonal of the first U bounds
-// cond(X) from below, and above 1e6 (or when the factorisation fails) the
-// block goes to the Householder QR instead.  The columns are first scaled to
-// unit norm (the span is unchanged): the filter multiplies the eigen-
-// components of its block by factors that span orders of magnitude, so the
-// filtered columns are nearly orthogonal but of very different lengths, an
-// ill-conditioning that the scaling removes.  G: n x n scratch (ld n);
-// dn: n doubles of scratch.
-int span_orthonormalize(pspw_cell *c, double2 *X, int ngw, int n, double2 *G, double *dn,
-                        int *info) {
+// twice G = X^H X = U^H U, X <- X U^-1, with the Gram matrices and the
+// products by U^-1 on the FP64 tensor-core GEMM and the factorisation and
+// inversion of U in one block (heev.cu).  Stable while cond(X) stays well
+// below 1/sqrt(eps); the ratio of the largest to the smallest diagonal of
+// the first U bounds cond(X) from below, and above 1e6 (or when the
+// factorisation fails) the block goes to the Householder QR instead.  The
+// columns are first scaled to unit norm (the span is unchanged): the filter
+// multiplies the eigen-components of its block by factors that span orders
+// of magnitude, so the filtered columns are nearly orthogonal but of very
+// different lengths, an ill-conditioning that the scaling removes.
+// G, U: n x n scratch (ld n); dn: n doubles; stat: 2 doubles; W: ngw x n.
+int span_orthonormalize(pspw_cell *c, double2 *X, int ngw, int n, double2 *G, double2 *U,
+                        double *dn, double *stat, double2 *W, int *info) {
   const double2 one = make_double2(1.0, 0.0), zero = make_double2(0.0, 0.0);
   int rc;
   if ((rc = dev_coldot(c, X, ngw, X, ngw, ngw, n, dn))) return rc;
   k_unit_cols<<<4 * 148, 256, 0, c->stream>>>(X, ngw, ngw, n, dn);
   c->kernel_launches++;
   PSPW_CUDA(cudaGetLastError());
+  if (n > kHeevMax) {  // beyond the one-block factorisation: Householder
+    return dev_ortho_qr(c, X, ngw, ngw, n, info);
+  }
   for (int pass = 0; pass < 2; pass++) {
-    if ((rc = zgemm<double>(c, 'C', n, n, ngw, one, X, ngw, X, ngw, zero, G, n))) return rc;
-    int pinfo = 0;
-    if ((rc = dev_potrf_upper(c, G, n, n, &pinfo))) return rc;
-    bool fallback = pinfo != 0;
-    if (!fallback && pass == 0) {
-      std::vector<double2> d(n);
-      PSPW_CUDA(cudaMemcpy2DAsync(d.data(), sizeof(double2), G, sizeof(double2) * (n + 1),
-                                  sizeof(double2), n, cudaMemcpyDeviceToHost, c->stream));
-      PSPW_CUDA(cudaStreamSynchronize(c->stream));
-      double lo = INFINITY, hi = 0.0;
-      for (const double2 &v : d) {
-        const double a = std::fabs(v.x);
-        lo = std::min(lo, a);
-        hi = std::max(hi, a);
-      }
-      fallback = !(lo > 0.0) || hi / lo > 1.0e6;
-    }
+    double2 *src = pass == 0 ? X : W, *dst = pass == 0 ? W : X;
+    if ((rc = zgemm<double>(c, 'C', n, n, ngw, one, src, ngw, src, ngw, zero, G, n))) return rc;
+    if ((rc = dev_chol_inv_upper(c, G, n, n, U, n, stat))) return rc;
+    double h[2];
+    PSPW_CUDA(cudaMemcpyAsync(h, stat, sizeof h, cudaMemcpyDeviceToHost, c->stream));
+    PSPW_CUDA(cudaStreamSynchronize(c->stream));
+    const bool fallback = h[0] != 0.0 || (pass == 0 && !(h[1] <= 1.0e6));
     if (fallback) return dev_ortho_qr(c, X, ngw, ngw, n, info);
-    if ((rc = dev_trsm_right_upper(c, G, n, X, ngw, ngw, n))) return rc;
+    if ((rc = zgemm<double>(c, 'N', ngw, n, n, one, src, ngw, U, n, zero, dst, ngw))) return rc;
   }
   *info = 0;
   return PSPW_OK;
@@ -171,11 +165,12 @@ extern "C" int pspw_cheby_scf(pspw_scf *s, const pspw_scf_params *p, const doubl
   int rc;
   // ---- device arrays
   DevBuf mem;
-  double2 *X, *HX, *T, *dv0, *df, *dRT;
+  double2 *X, *HX, *T, *dU, *dv0, *df, *dRT;
   float2 *Xf = nullptr;
-  double *veff, *rho, *wT, *dprec, *dcn;
+  double *veff, *rho, *wT, *dprec, *dcn, *dstat;
   if (!mem.get(&X, (size_t)ngw * nx2) || !mem.get(&dcn, nx2) || !mem.get(&HX, (size_t)ngw * nx2) ||
-      !mem.get(&T, (size_t)nx2 * nx2) || !mem.get(&dv0, ngw) || !mem.get(&df, ngw) ||
+      !mem.get(&T, (size_t)nx2 * nx2) || !mem.get(&dU, (size_t)nx2 * nx2) ||
+      !mem.get(&dstat, 2) || !mem.get(&dv0, ngw) || !mem.get(&df, ngw) ||
       !mem.get(&dRT, (size_t)k * k) || !mem.get(&veff, nnr) || !mem.get(&rho, nnr) ||
       !mem.get(&wT, std::max(k, nx2)) || !mem.get(&dprec, ngw) ||
       (fprec == PSPW_PREC_F32 && !mem.get(&Xf, (size_t)ngw * nx2)))
@@ -294,7 +289,7 @@ extern "C" int pspw_cheby_scf(pspw_scf *s, const pspw_scf_params *p, const doubl
     timing_end(c, kFamScfFilter, ev);
     int info = 0;
     timing_begin(c, kFamScfQr, &ev);
-    if ((rc = span_orthonormalize(c, X, ngw, nx2, T, dcn, &info))) return rc;
+    if ((rc = span_orthonormalize(c, X, ngw, nx2, T, dU, dcn, dstat, HX, &info))) return rc;
     timing_end(c, kFamScfQr, ev);
     // Rayleigh-Ritz (ChebySCFLoop.cpp:293-307)
     timing_begin(c, kFamScfRayleigh, &ev);

@@ -110,7 +110,14 @@ SIGNATURES = {
     "pspw_system_cheby_scf": [_vp, _i, C.c_char_p, _vp, _vp, _vp, _vp, _vp],
     "pspw_system_cheby_scf_with": [_vp, _vp, C.c_char_p, _vp, _vp, _vp, _vp, _vp],
     "pspw_print_3d_array": [_vp, _i, _i, _i, C.c_char_p],
+    "pspw_system_species": [_vp, _vp, _vp],
+    "pspw_server_create": [_i, _vp, _vp],
+    "pspw_server_submit": [_vp, C.c_char_p, _vp],
+    "pspw_server_wait": [_vp, _i, _vp, _vp, _i],
+    "pspw_server_now": [_vp, _vp],
+    "pspw_server_destroy": [_vp],
     "pspw_zgemm_dev": [_vp, C.c_char, _i, _i, _i, _vp, _vp, _i, _vp, _i, _vp, _vp, _i],
+    "pspw_eig_zheevd_dev": [_vp, _vp, _i, _vp, _i],
 }
 _RESTYPE = {"pspw_error_string": C.c_char_p, "pspw_last_error": C.c_char_p}
 

@@ -178,6 +178,11 @@ class Cell:
                                    int(m), int(n), int(k), al.ctypes.data, ptr(d_a), int(lda),
                                    ptr(d_b), int(ldb), be.ctypes.data, ptr(d_c), int(ldc)))
 
+    def eig_zheevd_dev(self, d_a, lda, d_w, n):
+        """eig_zheevd on device pointers (upper triangle read; eigenvectors
+        into A, ascending eigenvalues into w), enqueued on the cell stream."""
+        check(lib().pspw_eig_zheevd_dev(self._h, ptr(d_a), int(lda), ptr(d_w), int(n)))
+
     # ---- solvers and dense steps (host buffers; reference semantics)
     def gen_prec(self, nbasis, tau):
         p = np.zeros(nbasis)

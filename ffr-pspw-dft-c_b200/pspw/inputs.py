@@ -6,12 +6,13 @@ inputs."""
 from __future__ import annotations
 
 
-def write_synthetic_fhi(path, zv=4.0, well=1.0):
+def write_synthetic_fhi(path, zv=4.0, well=1.0, width=1.2):
     """A synthetic norm-conserving pseudopotential in the FHI98 text layout
     the reference reads (ReadPseudopotentials.cpp:27-62): `ZV nang`, ten
     skipped lines, then per angular momentum `mmax clog` and mmax rows
     `i r u(r) V(r)` on a logarithmic mesh.  The model: V_loc = -ZV erf(r)/r
-    + well exp(-(r/1.2)^2), V_s = V_loc + 1.5 exp(-(r/0.9)^2),
+    + well exp(-(r/width)^2) (a negative `well` is an attractive Gaussian
+    of depth -well), V_s = V_loc + 1.5 exp(-(r/0.9)^2),
     V_p = V_loc - 0.7 exp(-(r/1.1)^2), V_d = V_loc; u_l(r) = r^(l+1)
     exp(-r^2/4) normalised."""
     from math import erf, exp, sqrt
@@ -19,7 +20,7 @@ def write_synthetic_fhi(path, zv=4.0, well=1.0):
     rs = [r1 * fac ** i for i in range(mmax)]
 
     def vloc(r):
-        return -zv * erf(r) / r + well * exp(-(r / 1.2) ** 2)
+        return -zv * erf(r) / r + well * exp(-(r / width) ** 2)
 
     def vl(l, r):
         if l == 0:
@@ -48,6 +49,32 @@ def write_input(path, fhi_name, positions, a, ecut_ry=8.0, iscf=1, idiag=0, imix
     txt = (f"iscf\n {iscf}\n\nidiag\n {idiag}\n\nimix\n {imix}\n\nrho_mix_fac\n 0.3\n\n"
            f"max_scf_iter\n {max_scf}\n\nnempty\n {nempty}\n\necut\n {ecut_ry}\n\n"
            f"atoms\n 1\n {len(positions)}\n {fhi_name}\n 3 3\n bohr\n{pos}\n\n"
+           f"latvec\n {a} 0.0 0.0\n 0.0 {a} 0.0\n 0.0 0.0 {a}\n\n"
+           f"k_points\n 1\n 0.0 0.0 0.0 1.0\n")
+    if fft_grid is not None:
+        txt += f"\nfft_grid\n {fft_grid[0]} {fft_grid[1]} {fft_grid[2]}\n"
+    if conv is not None:
+        txt += f"\nscf_conv_crit\n {conv:.6e}\n"
+    if degree is not None:
+        txt += f"\nchebypol_degree\n {degree}\n"
+    with open(path, "w") as f:
+        f.write(txt)
+
+
+def write_input_species(path, species, a, ecut_ry, nempty, fft_grid=None, imix=3, idiag=-1,
+                        max_scf=100, conv=None, degree=None):
+    """An INPUT file with several species in a cubic cell of side a (bohr):
+    species = [(fhi_name, positions (n, 3) in bohr), ...], in the atoms
+    block layout ReadInputFile.cpp:53-92 reads (NSP; NA per species; per
+    species the file, `LMAX LLOC`, the coordinate type and NA lines)."""
+    nas = " ".join(str(len(p)) for _, p in species)
+    blocks = []
+    for name, pos in species:
+        lines = "\n".join(f"  {p[0]:.9f} {p[1]:.9f} {p[2]:.9f}" for p in pos)
+        blocks.append(f" {name}\n 3 3\n bohr\n{lines}")
+    txt = (f"iscf\n 1\n\nidiag\n {idiag}\n\nimix\n {imix}\n\nrho_mix_fac\n 0.3\n\n"
+           f"max_scf_iter\n {max_scf}\n\nnempty\n {nempty}\n\necut\n {ecut_ry}\n\n"
+           f"atoms\n {len(species)}\n {nas}\n" + "\n".join(blocks) + "\n\n"
            f"latvec\n {a} 0.0 0.0\n 0.0 {a} 0.0\n 0.0 0.0 {a}\n\n"
            f"k_points\n 1\n 0.0 0.0 0.0 1.0\n")
     if fft_grid is not None:

@@ -244,6 +244,14 @@ int pspw_eval_enl_dev(pspw_cell *cell, const double *d_c0, int ld, int ngw, int 
 int pspw_zgemm_dev(pspw_cell *cell, char opa, int m, int n, int k, const double *alpha,
                    const double *d_A, int lda, const double *d_B, int ldb, const double *beta,
                    double *d_C, int ldc);
+/* eig_zheevd_dev  eig_zheevd.cpp:5-34 on device pointers: A (n x n, lda,
+ *             upper triangle read) <- orthonormal eigenvectors, w[n] (device)
+ *             <- eigenvalues ascending.  n <= 160 (the Rayleigh-Ritz matrix
+ *             of the Chebyshev SCF loop is (NX+2) x (NX+2)) runs on the
+ *             engine's own kernels: Householder tridiagonalisation in one
+ *             block's shared memory, bisection, inverse iteration; larger n
+ *             on cuSOLVER zheevd.  Bitwise repeatable. */
+int pspw_eig_zheevd_dev(pspw_cell *cell, double *d_A, int lda, double *d_w, int n);
 
 /* ------------------------------------------------------------------ SCF pieces
  * The steps of the SCF iteration around the eigensolver, on the device in
@@ -405,6 +413,53 @@ int pspw_system_cheby_scf_with(pspw_system *system, const pspw_scf_params *param
                                const char *outdir, double *eig, double *e6, int *iterations,
                                int *converged, double *hist);
 /* Print3DArray.cpp:5-22: n1*n2*n3 values, one `%18.10f` per line */
+/* Atoms and KB projectors of a system (no reference counterpart; the
+ * reference keeps them in the globals NA, L_MAX, L_LOC): natoms = sum NA,
+ * nproj = sum over species of NA * lm_end.  Valid for host-only systems. */
+int pspw_system_species(pspw_system *system, int *natoms, int *nproj);
+
+/* ------------------------------------------------------------------ serving
+ * Independent SCF jobs on one GPU with continuous batching (no reference
+ * counterpart: the reference runs one job per process, main.cpp:20-50).  A
+ * job is a directory holding an INPUT and the pseudopotential files it
+ * names.  The server runs `slots` jobs at a time on `device`; a job is
+ * admitted when a slot is free and the estimated device footprints of the
+ * running jobs plus its own stay within hbm_budget_bytes (<= 0: 80 % of the
+ * free memory at creation; a job larger than the budget runs alone); jobs
+ * that arrive while others run are admitted as slots and memory free up.
+ * Each job runs pspw_system_load + pspw_system_cheby_scf_with on its own
+ * streams, with its blocks, densities and mixing history on the device from
+ * admission to completion, so the kernels of concurrent jobs overlap.  SCF
+ * controls: the job's INPUT, with filter_prec, and, where positive,
+ * conv_per_atom (|dETOT| <= conv_per_atom * natoms), max_scf_iter,
+ * pulay_beta and mixdim overriding it.  Times are seconds since the
+ * server's creation.  submit returns at once; wait blocks until the job has
+ * finished and copies its result (and up to neig eigenvalues; eig may be
+ * NULL).  destroy waits for the submitted jobs to finish. */
+typedef struct pspw_server pspw_server;
+typedef struct {
+  int slots;               /* jobs running at the same time */
+  double hbm_budget_bytes; /* admission limit on the summed footprints */
+  int filter_prec;         /* PSPW_PREC_F64 or PSPW_PREC_F32 (the mixed form) */
+  double conv_per_atom;    /* Ha per atom; <= 0: the INPUT's SCF_CONV_CRIT */
+  int max_scf_iter;        /* <= 0: the INPUT's */
+  double pulay_beta;       /* <= 0: 0.25, the reference's */
+  int mixdim;              /* <= 0: the INPUT's */
+} pspw_server_config;
+typedef struct {
+  int id, status;          /* status: PSPW_OK or the job's error code */
+  int natoms, nbands, ngw, nnr, iterations, converged;
+  double etot;             /* final total energy (Ha) */
+  double footprint_bytes;  /* the estimate the admission used */
+  double t_submit, t_admit, t_scf, t_done;  /* submitted, admitted, SCF start, done */
+} pspw_job_result;
+int pspw_server_create(int device, const pspw_server_config *cfg, pspw_server **out);
+int pspw_server_submit(pspw_server *server, const char *dir, int *job_id);
+int pspw_server_wait(pspw_server *server, int job_id, pspw_job_result *result, double *eig,
+                     int neig);
+int pspw_server_now(pspw_server *server, double *seconds);
+int pspw_server_destroy(pspw_server *server);
+
 int pspw_print_3d_array(const double *a, int n1, int n2, int n3, const char *path);
 
 /* ------------------------------------------------------------------ timing

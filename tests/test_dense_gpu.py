@@ -104,3 +104,75 @@ def test_device_wait_times_out_and_cell_stays_usable(cell):
     cell.apply_ham_block_dev(d_in, d_out, ngw, ngw, d_in.shape[0], PREC_F64)
     torch.cuda.synchronize()
     assert relmax(d_out.cpu().numpy().T, G["hpsi"]) < TOL
+
+
+# ---------------------------------------------------------------- Hermitian eigensolver
+def _eig_dev(cell, a, pad=0):
+    n = a.shape[0]
+    lda = n + pad
+    h = np.full((n, lda), np.nan + 0j)
+    h[:, :n] = a.T  # column j of A = row j of the torch tensor
+    d_a = torch.from_numpy(h).cuda()
+    d_w = torch.zeros(n, dtype=torch.float64, device="cuda")
+    torch.cuda.synchronize()
+    cell.eig_zheevd_dev(d_a, lda, d_w, n)
+    torch.cuda.synchronize()
+    return d_w.cpu().numpy(), d_a.cpu().numpy()[:, :n].T.copy()
+
+
+def _check_eig(cell, a, pad=0, tol=1e-12):
+    w, v = _eig_dev(cell, a, pad)
+    full = np.triu(a) + np.triu(a, 1).conj().T  # the upper triangle defines A
+    ref = np.linalg.eigvalsh(full)
+    nrm = max(np.abs(ref).max(), 1e-300)
+    n = len(w)
+    assert np.all(np.diff(w) >= 0)
+    assert np.abs(w - ref).max() <= tol * nrm
+    assert np.abs(full @ v - v * w).max() <= tol * nrm
+    assert np.abs(v.conj().T @ v - np.eye(n)).max() <= tol * max(1, n / 16)
+    return w, v
+
+
+@pytest.mark.parametrize("n", [1, 2, 3, 17, 64, 146, 160, 161, 200])
+def test_eig_zheevd_dev_random(cell, n):
+    # n <= 160: the engine's kernels; above: cuSOLVER
+    rng = np.random.default_rng(n)
+    m = rng.standard_normal((n, n)) + 1j * rng.standard_normal((n, n))
+    a = m + m.conj().T
+    a[np.tril_indices(n, -1)] = np.nan  # only the upper triangle may be read
+    _check_eig(cell, a, pad=n % 3)
+
+
+def _with_spectrum(lam, seed):
+    n = len(lam)
+    rng = np.random.default_rng(seed)
+    q, _ = np.linalg.qr(rng.standard_normal((n, n)) + 1j * rng.standard_normal((n, n)))
+    a = (q * lam) @ q.conj().T
+    return 0.5 * (a + a.conj().T)
+
+
+def test_eig_zheevd_dev_degenerate_and_clustered(cell):
+    n = 146
+    lam = np.repeat(np.linspace(-0.3, 0.6, 49), 3)[:n]  # triplets, as in a cubic crystal
+    _check_eig(cell, _with_spectrum(lam, 1))
+    rng = np.random.default_rng(2)
+    lam = np.sort(rng.uniform(-0.3, 0.6, n))
+    lam[10:15] = lam[10] + np.array([0.0, 1e-12, 1e-9, 2e-6, 3e-4])  # a chain inside 1e-3
+    lam[80:84] = lam[80]
+    _check_eig(cell, _with_spectrum(np.sort(lam), 3))
+
+
+def test_eig_zheevd_dev_special_matrices(cell):
+    _check_eig(cell, np.diag(np.arange(40, dtype=float) - 7.5).astype(complex))
+    w, v = _eig_dev(cell, np.zeros((9, 9), dtype=complex))
+    assert np.all(w == 0) and np.abs(v.conj().T @ v - np.eye(9)).max() < 1e-14
+    t = np.diag(np.full(50, 2.0)) - np.diag(np.ones(49), 1) - np.diag(np.ones(49), -1)
+    _check_eig(cell, t.astype(complex))  # already tridiagonal (reflectors with tau = 0)
+    _check_eig(cell, 1e-150 * _with_spectrum(np.linspace(1, 2, 30), 4))  # tiny scale
+
+
+def test_eig_zheevd_dev_is_bitwise_repeatable(cell):
+    a = _with_spectrum(np.linspace(-1, 1, 146), 5)
+    w1, v1 = _eig_dev(cell, a)
+    w2, v2 = _eig_dev(cell, a)
+    assert np.array_equal(w1, w2) and np.array_equal(v1, v2)
