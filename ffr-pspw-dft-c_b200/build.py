@@ -35,7 +35,7 @@ CXXFLAGS = ["-O2", "-std=c++17", "-fPIC", "-ffp-contract=off", "-fvisibility=hid
 # libpspw_gpu.so
 GPU_SOURCES = ["basis.cpp", "cell.cu", "hpsi.cu", "fftpath_f32.cu", "fftpath_f64.cu", "capi.cu",
                "noalloc.cu", "gemm.cu", "heev.cu", "dense.cu", "solvers.cu", "capi_solvers.cu", "nl_tc.cu",
-               "scf.cu", "scf_driver.cu", "input.cpp", "geom.cu", "serve.cpp"]
+               "scf.cu", "scf_driver.cu", "input.cpp", "geom.cu", "serve.cpp", "batch.cu"]
 GPU_LIBS = ["-lcusolver", "-lcublas", "-lcudart"]
 # libpspw_dropin.so (links libpspw_gpu.so)
 DROPIN_SOURCES = ["dropin.cpp"]

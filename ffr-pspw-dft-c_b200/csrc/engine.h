@@ -63,8 +63,8 @@ struct Projectors {
   double *d_pkga64 = nullptr;  // [nsp][ngw][4]
   float *d_pkga32 = nullptr;
   // FP64 path: beta_p(G) = EIGR(G, atom_p) PKG_A(lm_p, G) as an NGW x nproj
-  // column-major matrix, built on the first FP64 projector call (cuBLAS
-  // ZGEMMs use it as an operand)
+  // column-major matrix, built on the first FP64 projector call (the DMMA
+  // GEMMs of gemm.cu use it as an operand)
   double2 *d_beta64 = nullptr;
   int *d_patom = nullptr;    // [nproj] atom (species-major global index)
   int *d_psp = nullptr;      // [nproj] species

@@ -111,6 +111,16 @@ SIGNATURES = {
     "pspw_system_cheby_scf_with": [_vp, _vp, C.c_char_p, _vp, _vp, _vp, _vp, _vp],
     "pspw_print_3d_array": [_vp, _i, _i, _i, C.c_char_p],
     "pspw_system_species": [_vp, _vp, _vp],
+    "pspw_batch_create": [_i, _vp, _vp, _i, _vp],
+    "pspw_batch_blocks": [_vp, _i, _vp, _vp],
+    "pspw_batch_upload": [_vp, _i, _vp],
+    "pspw_batch_download": [_vp, _i, _vp],
+    "pspw_batch_tune": [_vp, _i],
+    "pspw_batch_schedule": [_vp, _i, _vp, _vp, _vp],
+    "pspw_batch_apply": [_vp],
+    "pspw_batch_stream": [_vp, _vp],
+    "pspw_batch_synchronize": [_vp],
+    "pspw_batch_destroy": [_vp],
     "pspw_server_create": [_i, _vp, _vp],
     "pspw_server_submit": [_vp, C.c_char_p, _vp],
     "pspw_server_wait": [_vp, _i, _vp, _vp, _i],

@@ -418,6 +418,37 @@ int pspw_system_cheby_scf_with(pspw_system *system, const pspw_scf_params *param
  * nproj = sum over species of NA * lm_end.  Valid for host-only systems. */
 int pspw_system_species(pspw_system *system, int *natoms, int *nproj);
 
+/* ------------------------------------------------------------------ batches
+ * Block H*psi on many independent cells in one launch (no reference
+ * counterpart; the reference applies ApplyHam_block to one cell per
+ * process).  create: ncells cells on one device, each with V_eff set, and
+ * nbands[i] bands per cell, in precision prec; the batch allocates each
+ * cell's input and output block (NGW x nbands, ld = the cell's NGW), which
+ * blocks returns.  tune: for every cell, times the schedules that give the
+ * same result (band batches of the FFT passes; tensor-core or SIMT
+ * projector kernels for FP32 cells of one species), `reps` timed calls
+ * each, keeps the fastest (cached per cell shape for the process) and
+ * drops the captured graph.  apply: one CUDA graph launch on the batch
+ * stream doing H*psi for every cell (captured on the first apply after
+ * create or tune; the cells' kernels run on concurrent branches), returns
+ * without synchronising.  A cell's result is the same alone and in the
+ * batch.  The cells must stay alive and unchanged (V_eff, schedules) while
+ * the batch exists. */
+typedef struct pspw_batch pspw_batch;
+int pspw_batch_create(int ncells, pspw_cell *const *cells, const int *nbands, int prec,
+                      pspw_batch **out);
+int pspw_batch_blocks(pspw_batch *batch, int i, void **d_in, void **d_out);
+/* host copies of cell i's input (before apply) and output (after; waits for
+ * the batch stream); complex values of the batch's precision, NGW x nbands */
+int pspw_batch_upload(pspw_batch *batch, int i, const void *host_in);
+int pspw_batch_download(pspw_batch *batch, int i, void *host_out);
+int pspw_batch_tune(pspw_batch *batch, int reps);
+int pspw_batch_schedule(pspw_batch *batch, int i, int *band_batch, int *nl_path, double *ms);
+int pspw_batch_apply(pspw_batch *batch);
+int pspw_batch_stream(pspw_batch *batch, void **stream);
+int pspw_batch_synchronize(pspw_batch *batch);
+int pspw_batch_destroy(pspw_batch *batch);
+
 /* ------------------------------------------------------------------ serving
  * Independent SCF jobs on one GPU with continuous batching (no reference
  * counterpart: the reference runs one job per process, main.cpp:20-50).  A
