@@ -422,6 +422,8 @@ int cell_create(pspw_cell **out, int device, int nr1, int nr2, int nr3, int ngw,
   P.nat = nat;
   P.nsp = nsp;
   P.nproj = nproj;
+  P.sp_na.assign(na, na + nsp);
+  P.sp_lm.assign(lm_end, lm_end + nsp);
   if (nproj > 0) {
     std::vector<double2> e64(dev_src ? 0 : (size_t)nat * ngw);
     std::vector<float2> e32(dev_src ? 0 : (size_t)nat * ngw);
@@ -670,8 +672,8 @@ int pspw_cell_set_nl_path(pspw_cell *c, int path) {
   c->nl_path = PSPW_NL_AUTO;
   if (path == PSPW_NL_TENSOR_CORE && !pspw::nl_tc_usable(c)) {
     c->nl_path = keep;
-    return fail(PSPW_ERR_NOT_IMPL, "set_nl_path: tensor-core projector kernels need one species "
-                                   "and 1..256 atoms");
+    return fail(PSPW_ERR_NOT_IMPL, "set_nl_path: tensor-core projector kernels need at most "
+                                   "256 atoms and 4 projectors per atom in every species");
   }
   c->nl_path = path;
   return PSPW_OK;

@@ -75,7 +75,9 @@ struct Projectors {
   // GEMMs (one species only; built at cell creation, nl_tc.cu)
   float *d_etp = nullptr;  // projection: per 8 G, [npad atoms x 16] hi then lo
   float *d_etb = nullptr;  // back-projection: per (128 G, 8 atoms), [128 x 16] hi then lo
-  int tc_npad = 0;         // atoms padded to a multiple of 16
+  // (both hold one block of tiles per species with projectors, species in order)
+  int tc_npad = 0;         // atoms padded to a multiple of 16 (largest species)
+  std::vector<int> sp_na, sp_lm;  // per species: atoms, projectors per atom (host)
 };
 
 // Timing families (bit i of the mask enables family i).

@@ -48,6 +48,7 @@
 
 #include <algorithm>
 #include <cstdlib>
+#include <vector>
 
 #include "common.cuh"
 #include "engine.h"
@@ -548,19 +549,52 @@ struct Shape {
   int L, per, nat, npad, nsa, nbt, ncolN, nbtiles;
 };
 
-bool fits(const Projectors &P) {
-  return P.nsp == 1 && P.nat >= 1 && P.nat <= 256 && P.nproj > 0 && P.nproj % P.nat == 0 &&
-         P.nproj / P.nat <= 4;
+// A species with projectors: its atoms (a range of the species-major atom
+// order), its projectors per atom, its first projector, and the offsets
+// (floats) of its blocks in the EIGR tile buffers, which hold one block per
+// such species in species order.
+struct Group {
+  int sp, atom0, nat, L, p0;
+  size_t etp_off, etb_off;
+};
+
+std::vector<Group> groups_of(const Projectors &P, int ngw_cell) {
+  std::vector<Group> g;
+  const size_t nst = (size_t)(ngw_cell + kStepG - 1) / kStepG * (kStepG / 8);
+  const size_t ngt = (size_t)(ngw_cell + 127) / 128;
+  int atom0 = 0, p0 = 0;
+  size_t eo = 0, bo = 0;
+  for (int s = 0; s < (int)P.sp_na.size(); s++) {
+    const int na = P.sp_na[s], L = P.sp_lm[s];
+    if (na > 0 && L > 0) {
+      g.push_back({s, atom0, na, L, p0, eo, bo});
+      eo += nst * (size_t)((na + 15) / 16 * 16) * 32;  // npad x 128 bytes per 8 G
+      bo += ngt * (size_t)((na + 7) / 8) * 4096;       // 16 KB per (128 G, 8 atoms)
+    }
+    atom0 += na;
+    p0 += na * std::max(0, L);
+  }
+  return g;
 }
 
-Shape shape_of(const pspw_cell *c, int nb) {
-  const Projectors &P = c->proj;
+bool fits(const Projectors &P) {
+  if (P.nproj <= 0 || (int)P.sp_na.size() != P.nsp || (int)P.sp_lm.size() != P.nsp) return false;
+  bool any = false;
+  for (int s = 0; s < P.nsp; s++) {
+    if (P.sp_na[s] <= 0 || P.sp_lm[s] <= 0) continue;
+    if (P.sp_na[s] > 256 || P.sp_lm[s] > 4) return false;
+    any = true;
+  }
+  return any;
+}
+
+Shape shape_of(const Group &gp, int nb) {
   Shape s;
-  s.nat = P.nat;
-  s.L = P.nproj / P.nat;
+  s.nat = gp.nat;
+  s.L = gp.L;
   s.per = 2 * s.L;
-  s.npad = (P.nat + 15) / 16 * 16;
-  s.nsa = (P.nat + 7) / 8;
+  s.npad = (gp.nat + 15) / 16 * 16;
+  s.nsa = (gp.nat + 7) / 8;
   // bands per back-projection N tile: nbt*2L a multiple of 16, at most 128
   int nmax = kMaxBackN / s.per;
   while ((nmax * s.per) % 16) nmax--;
@@ -571,6 +605,10 @@ Shape shape_of(const pspw_cell *c, int nb) {
   s.nbtiles = (nb + nbt - 1) / nbt;
   return s;
 }
+
+size_t up256(size_t n) { return (n + 255) / 256 * 256; }
+
+size_t group_wtile_bytes(const Shape &s) { return up256((size_t)s.nbtiles * s.nsa * s.ncolN * 128); }
 
 // Dynamic shared memory, raised where needed so that no more blocks fit on
 // an SM than its 512 TMEM columns can serve at once (an allocation would
@@ -595,19 +633,22 @@ int back_smem(const Shape &s) {
   return block_smem(kNTB * (2 * kTileBytes128 + s.ncolN * 128), tmem_cols(s.ncolN));
 }
 
-// splits of the projection's K range: enough blocks to fill the GPU once
-int proj_splits(pspw_cell *c, const Shape &s, int ngw, int nb, int *kg_out) {
-  const int mt = (nb * s.per + 127) / 128;
-  static int sms = 0;
-  if (!sms) {
-    int dev = 0;
+int sm_count() {
+  static const int n = [] {
+    int dev = 0, v = 0;
     cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    if (sms <= 0) sms = 148;
-  }
+    cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, dev);
+    return v > 0 ? v : 148;
+  }();
+  return n;
+}
+
+// splits of the projection's K range: enough blocks to fill the GPU once
+int proj_splits(const Shape &s, int ngw, int nb, int *kg_out) {
+  const int mt = (nb * s.per + 127) / 128;
   const int smem = proj_smem(s);
   const int per_sm = std::max(1, std::min(233472 / (smem + 1024), 512 / proj_tmem_cols(s)));
-  int nsplit = std::max(1, std::min((ngw + 63) / 64, per_sm * sms / mt));
+  int nsplit = std::max(1, std::min((ngw + 63) / 64, per_sm * sm_count() / mt));
   int kg = (ngw + nsplit - 1) / nsplit;
   kg = (kg + kStepG - 1) / kStepG * kStepG;
   *kg_out = kg;
@@ -616,15 +657,15 @@ int proj_splits(pspw_cell *c, const Shape &s, int ngw, int nb, int *kg_out) {
 
 template <int L>
 int launch_project(pspw_cell *c, const Shape &s, const float2 *psi, int ld, int ngw, int nb,
-                   float *part, int nsplit, int kg, float *wt) {
-  const Projectors &P = c->proj;
+                   float *part, int nsplit, int kg, float *wt, const float *etp,
+                   const float *pkga, const float *pw) {
   const int mt = (nb * s.per + 127) / 128;
   const int smem = proj_smem(s);
   PSPW_CUDA(cudaFuncSetAttribute(k_proj_tc<L>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
   k_proj_tc<L><<<dim3(mt, nsplit), kThreadsP, smem, c->stream>>>(
-      psi, ld, ngw, nb, P.d_etp, P.d_pkga32, s.nat, s.npad, kg, part, c->d_err);
+      psi, ld, ngw, nb, etp, pkga, s.nat, s.npad, kg, part, c->d_err);
   const int total = s.nbtiles * s.nsa * s.nbt * L * 4;  // one warp each
-  k_proj_tc_wtiles<L><<<(total + 7) / 8, 256, 0, c->stream>>>(part, nsplit, nb, s.nat, P.d_pw32,
+  k_proj_tc_wtiles<L><<<(total + 7) / 8, 256, 0, c->stream>>>(part, nsplit, nb, s.nat, pw,
                                                               s.nbt, s.nsa, total, wt);
   c->kernel_launches += 2;
   PSPW_CUDA(cudaGetLastError());
@@ -632,16 +673,16 @@ int launch_project(pspw_cell *c, const Shape &s, const float2 *psi, int ld, int 
 }
 
 template <int L>
-int launch_back(pspw_cell *c, const Shape &s, const float *wt, int ngw, int nb, float2 *out,
-                int ldo, const float2 *in, int ldi, const float2 *xm2, int ldx, float a, float b,
-                float g, bool pre) {
+int launch_back(pspw_cell *c, const Shape &s, const float *wt, const float *etb,
+                const float *pkga, int ngw, int nb, float2 *out, int ldo, const float2 *in,
+                int ldi, const float2 *xm2, int ldx, float a, float b, float g, bool pre) {
   const int smem = back_smem(s);
   PSPW_CUDA(
       cudaFuncSetAttribute(k_backproj_tc<L>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
   dim3 grid((ngw + 127) / 128, s.nbtiles);
-  k_backproj_tc<L><<<grid, kThreads, smem, c->stream>>>(c->proj.d_etb, wt, s.nsa, ngw, nb, s.nbt,
-                                                        c->proj.d_pkga32, out, ldo, in, ldi, xm2,
-                                                        ldx, a, b, g, pre, c->d_err);
+  k_backproj_tc<L><<<grid, kThreads, smem, c->stream>>>(etb, wt, s.nsa, ngw, nb, s.nbt, pkga,
+                                                        out, ldo, in, ldi, xm2, ldx, a, b, g, pre,
+                                                        c->d_err);
   c->kernel_launches++;
   PSPW_CUDA(cudaGetLastError());
   return PSPW_OK;
@@ -682,20 +723,32 @@ int nl_tc_build_tiles(pspw_cell *c, const float2 *eigr32, float **etp, float **e
   Projectors &P = c->proj;
   if (!fits(P)) return PSPW_OK;
   const int ngw = c->basis.ngw;
-  const int npad = (P.nat + 15) / 16 * 16, nsa = (P.nat + 7) / 8;
+  const std::vector<Group> gs = groups_of(P, ngw);
   // projection tiles: every 8 G of the sphere, rounded up to whole steps of
-  // kStepG G (the tail tiles hold zeros)
+  // kStepG G (the tail tiles hold zeros); one block per species
   const int nst = (ngw + kStepG - 1) / kStepG * (kStepG / 8), ngt = (ngw + 127) / 128;
-  const size_t bp = (size_t)nst * npad * 128, bb = (size_t)ngt * nsa * 16384;
-  if (cudaMalloc(etp, bp) != cudaSuccess || cudaMalloc(etb, bb) != cudaSuccess)
+  size_t fe = 0, fb = 0;
+  int npad_max = 0;
+  for (const Group &g : gs) {
+    const int npad = (g.nat + 15) / 16 * 16, nsa = (g.nat + 7) / 8;
+    fe = g.etp_off + (size_t)nst * npad * 32;
+    fb = g.etb_off + (size_t)ngt * nsa * 4096;
+    npad_max = std::max(npad_max, npad);
+  }
+  if (cudaMalloc(etp, fe * sizeof(float)) != cudaSuccess ||
+      cudaMalloc(etb, fb * sizeof(float)) != cudaSuccess)
     return fail(PSPW_ERR_OOM, "EIGR operand tiles");
-  P.tc_npad = npad;
-  const long long n1 = (long long)nst * npad * 4, n2 = (long long)ngt * nsa * 512;
-  k_build_etp<<<(unsigned)((n1 + 255) / 256), 256, 0, c->stream>>>(eigr32, ngw, P.nat, npad, nst,
-                                                                   *etp);
-  k_build_etb<<<(unsigned)((n2 + 255) / 256), 256, 0, c->stream>>>(eigr32, ngw, P.nat, nsa, ngt,
-                                                                   *etb);
-  c->kernel_launches += 2;
+  P.tc_npad = npad_max;
+  for (const Group &g : gs) {
+    const int npad = (g.nat + 15) / 16 * 16, nsa = (g.nat + 7) / 8;
+    const float2 *e = eigr32 + (size_t)g.atom0 * ngw;
+    const long long n1 = (long long)nst * npad * 4, n2 = (long long)ngt * nsa * 512;
+    k_build_etp<<<(unsigned)((n1 + 255) / 256), 256, 0, c->stream>>>(e, ngw, g.nat, npad, nst,
+                                                                     *etp + g.etp_off);
+    k_build_etb<<<(unsigned)((n2 + 255) / 256), 256, 0, c->stream>>>(e, ngw, g.nat, nsa, ngt,
+                                                                     *etb + g.etb_off);
+    c->kernel_launches += 2;
+  }
   PSPW_CUDA(cudaGetLastError());
   return PSPW_OK;
 }
@@ -708,51 +761,83 @@ int nl_tc_prepare(pspw_cell *c) {
 
 size_t nl_tc_wtile_bytes(const pspw_cell *c, int nb) {
   if (!fits(c->proj)) return 0;
-  const Shape s = shape_of(c, nb);
-  return (size_t)s.nbtiles * s.nsa * s.ncolN * 128;
+  size_t n = 0;
+  for (const Group &g : groups_of(c->proj, c->basis.ngw)) n += group_wtile_bytes(shape_of(g, nb));
+  return n;
 }
 
 int nl_tc_reserve(pspw_cell *c, int ngw, int nb, float **part, int *max_split, float **wt) {
-  const Shape s = shape_of(c, nb);
-  int kg = 0;
-  const int nsplit = proj_splits(c, s, ngw, nb, &kg);
-  int rc = ws_reserve(c, kWsProjPart, sizeof(float) * (size_t)nsplit * nb * s.per * s.nat,
+  int ms = 1;
+  for (const Group &g : groups_of(c->proj, c->basis.ngw)) {
+    int kg = 0;
+    ms = std::max(ms, proj_splits(shape_of(g, nb), ngw, nb, &kg));
+  }
+  // the partial sums of any one species fit max_split x 2 nb nproj floats
+  int rc = ws_reserve(c, kWsProjPart, sizeof(float) * (size_t)ms * 2 * nb * c->proj.nproj,
                       (void **)part);
   if (rc) return rc;
   rc = ws_reserve(c, kWsWTile, nl_tc_wtile_bytes(c, nb), (void **)wt);
   if (rc) return rc;
-  *max_split = nsplit;
+  *max_split = ms;
   return PSPW_OK;
 }
 
 int nl_tc_project(pspw_cell *c, const float2 *psi, int ld, int ngw, int nb, float *part,
                   int max_split, float *wt) {
-  const Shape s = shape_of(c, nb);
-  int kg = 0;
-  int nsplit = proj_splits(c, s, ngw, nb, &kg);
-  if (nsplit > max_split) {
-    nsplit = std::max(1, max_split);
-    kg = ((ngw + nsplit - 1) / nsplit + kStepG - 1) / kStepG * kStepG;
-    nsplit = (ngw + kg - 1) / kg;
+  const Projectors &P = c->proj;
+  const size_t cap = (size_t)std::max(1, max_split) * 2 * nb * P.nproj;  // floats of part
+  size_t woff = 0;
+  for (const Group &g : groups_of(P, c->basis.ngw)) {
+    const Shape s = shape_of(g, nb);
+    int kg = 0;
+    int nsplit = proj_splits(s, ngw, nb, &kg);
+    const int lim = (int)std::max<size_t>(1, cap / ((size_t)nb * s.per * s.nat));
+    if (nsplit > lim) {
+      nsplit = lim;
+      kg = ((ngw + nsplit - 1) / nsplit + kStepG - 1) / kStepG * kStepG;
+      nsplit = (ngw + kg - 1) / kg;
+    }
+    float *w = wt + woff / sizeof(float);
+    const float *etp = P.d_etp + g.etp_off, *pk = P.d_pkga32 + (size_t)g.sp * c->basis.ngw * 4,
+                *pw = P.d_pw32 + g.p0;
+    int rc;
+    switch (s.L) {
+      case 1: rc = launch_project<1>(c, s, psi, ld, ngw, nb, part, nsplit, kg, w, etp, pk, pw); break;
+      case 2: rc = launch_project<2>(c, s, psi, ld, ngw, nb, part, nsplit, kg, w, etp, pk, pw); break;
+      case 3: rc = launch_project<3>(c, s, psi, ld, ngw, nb, part, nsplit, kg, w, etp, pk, pw); break;
+      default: rc = launch_project<4>(c, s, psi, ld, ngw, nb, part, nsplit, kg, w, etp, pk, pw);
+    }
+    if (rc) return rc;
+    woff += group_wtile_bytes(s);
   }
-  switch (s.L) {
-    case 1: return launch_project<1>(c, s, psi, ld, ngw, nb, part, nsplit, kg, wt);
-    case 2: return launch_project<2>(c, s, psi, ld, ngw, nb, part, nsplit, kg, wt);
-    case 3: return launch_project<3>(c, s, psi, ld, ngw, nb, part, nsplit, kg, wt);
-    default: return launch_project<4>(c, s, psi, ld, ngw, nb, part, nsplit, kg, wt);
-  }
+  return PSPW_OK;
 }
 
 int nl_tc_backproject(pspw_cell *c, const float *wt, int ngw, int nb, float2 *out, int ldo,
                       const float2 *in, int ldi, const float2 *xm2, int ldx, float a, float b,
                       float g, bool pre) {
-  const Shape s = shape_of(c, nb);
-  switch (s.L) {
-    case 1: return launch_back<1>(c, s, wt, ngw, nb, out, ldo, in, ldi, xm2, ldx, a, b, g, pre);
-    case 2: return launch_back<2>(c, s, wt, ngw, nb, out, ldo, in, ldi, xm2, ldx, a, b, g, pre);
-    case 3: return launch_back<3>(c, s, wt, ngw, nb, out, ldo, in, ldi, xm2, ldx, a, b, g, pre);
-    default: return launch_back<4>(c, s, wt, ngw, nb, out, ldo, in, ldi, xm2, ldx, a, b, g, pre);
+  const Projectors &P = c->proj;
+  size_t woff = 0;
+  bool first = true;
+  for (const Group &gp : groups_of(P, c->basis.ngw)) {
+    const Shape s = shape_of(gp, nb);
+    const float *w = wt + woff / sizeof(float);
+    const float *etb = P.d_etb + gp.etb_off, *pk = P.d_pkga32 + (size_t)gp.sp * c->basis.ngw * 4;
+    // the first species applies the recurrence's update; the others add
+    // their a * sum to it (the `pre` form)
+    const bool pr = first ? pre : true;
+    int rc;
+    switch (s.L) {
+      case 1: rc = launch_back<1>(c, s, w, etb, pk, ngw, nb, out, ldo, in, ldi, xm2, ldx, a, b, g, pr); break;
+      case 2: rc = launch_back<2>(c, s, w, etb, pk, ngw, nb, out, ldo, in, ldi, xm2, ldx, a, b, g, pr); break;
+      case 3: rc = launch_back<3>(c, s, w, etb, pk, ngw, nb, out, ldo, in, ldi, xm2, ldx, a, b, g, pr); break;
+      default: rc = launch_back<4>(c, s, w, etb, pk, ngw, nb, out, ldo, in, ldi, xm2, ldx, a, b, g, pr);
+    }
+    if (rc) return rc;
+    woff += group_wtile_bytes(s);
+    first = false;
   }
+  return PSPW_OK;
 }
 
 }  // namespace pspw

@@ -5,8 +5,9 @@
 
 namespace pspw {
 
-// True when the cell's projectors fit the tensor-core kernels (one species,
-// 1..256 atoms, at most 4 projectors per atom) and the kernels are selected.
+// True when the cell's projectors fit the tensor-core kernels (every species
+// with projectors: 1..256 atoms, at most 4 projectors per atom) and the
+// kernels are selected.  The kernels run once per such species.
 bool nl_tc_usable(const pspw_cell *c);
 
 // Builds the EIGR operand tiles of a cell whose projectors fit the kernels

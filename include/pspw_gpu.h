@@ -110,9 +110,10 @@ int pspw_cell_set_band_batch(pspw_cell *cell, int nbatch);
 
 /* Kernels of the FP32 projector GEMMs (no reference counterpart: the
  * reference has one CPU path).  AUTO takes the tensor-core (tcgen05, 3xTF32)
- * kernels when the cell has one species and at most 256 atoms, else the
- * SIMT kernels; TENSOR_CORE on a cell outside that range is
- * PSPW_ERR_NOT_IMPL.  The FP64 path does not depend on it: it stores the
+ * kernels when every species with projectors has at most 256 atoms and at
+ * most 4 projectors per atom (one projection and one back-projection per
+ * such species), else the SIMT kernels; TENSOR_CORE on a cell outside that
+ * range is PSPW_ERR_NOT_IMPL.  The FP64 path does not depend on it: it stores the
  * projectors once per cell and runs both products on the FP64 tensor-core
  * GEMM (the allocation-free entry point keeps SIMT kernels). */
 #define PSPW_NL_AUTO 0

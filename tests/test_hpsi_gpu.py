@@ -346,11 +346,71 @@ def test_fp32_tensor_core_fewer_plane_waves_than_the_cell(cfg0):
     assert relmax(out, ref) < TOL32
 
 
-def test_tensor_core_path_refused_for_two_species():
+def _multi_species_cell(na, lm_end, rc, seed):
     lat, pos = synth.si_diamond(1)
-    b = basis_gamma(lat, 8.0, None, [5, 3], [pos[:5], pos[5:]])
-    pkg_a, wnl = synth.kb_form_factors(b, lat, nsp=2, rc=[1.0, 0.8])
-    b.update(pkg_a=pkg_a, wnl=wnl, lm_end=[4, 1])
+    rng = np.random.default_rng(seed)
+    pos = pos + rng.uniform(-0.3, 0.3, pos.shape)  # no two species share a site pattern
+    tau, k = [], 0
+    for n in na:
+        tau.append(pos[k:k + n])
+        k += n
+    b = basis_gamma(lat, 8.0, None, na, tau)
+    pkg_a, wnl = synth.kb_form_factors(b, lat, nsp=len(na), rc=rc)
+    for s, lm in enumerate(lm_end):
+        wnl[s, :4] = [1.5 - 0.3 * s, -0.8 + 0.2 * s, -0.8 + 0.2 * s, -0.8 + 0.2 * s]
+        pkg_a[lm:, :, s] = 0.0
+    b.update(pkg_a=pkg_a, wnl=wnl, lm_end=lm_end)
+    veff = synth.local_potential(b["nr"], lat, pos)
+    return b, veff, lat
+
+
+@pytest.mark.parametrize("na,lm_end,rc", [
+    ([5, 3], [4, 1], [1.0, 0.8]),                          # two species, s+p and s
+    ([2, 2, 3, 1], [4, 1, 4, 3], [1.0, 0.8, 1.2, 0.9]),    # four species (the serving jobs')
+    ([3, 4, 1], [4, 0, 2], [1.0, 0.8, 1.1]),               # a species without projectors
+])
+def test_fp32_tensor_core_several_species(na, lm_end, rc):
+    """tcgen05 projector GEMMs per species (each species' atoms, PKG_A and
+    weights; the back-projections add into one output) against the oracle
+    and the SIMT kernels."""
+    b, veff, lat = _multi_species_cell(na, lm_end, rc, len(na))
+    cell = Cell.from_arrays(b)
+    cell.set_veff(veff)
+    psi = synth.wavefunctions(b, lat, 11, 5).astype(np.complex64).astype(complex)
+    oc = oracle_cell(b)
+    oc.update(na=na, lm_end=lm_end)
+    ref = O.apply_ham_block(oc, psi, veff)
+    cell.set_nl_path(NL_TENSOR_CORE)
+    out_tc = _hpsi32(cell, psi, ld=psi.shape[0] + 1)
+    cell.set_nl_path(NL_SIMT)
+    out_simt = _hpsi32(cell, psi)
+    assert relmax(out_tc, ref) < TOL32
+    assert relmax(out_simt, ref) < TOL32
+    assert relmax(out_tc, out_simt) < TOL32
+
+
+def test_fp32_tensor_core_several_species_filter():
+    # the filter's recurrence epilogue is applied once, by the first species
+    na, lm_end = [4, 4], [4, 2]
+    b, veff, lat = _multi_species_cell(na, lm_end, [1.0, 0.9], 7)
+    cell = Cell.from_arrays(b)
+    cell.set_veff(veff)
+    cell.set_nl_path(NL_TENSOR_CORE)
+    X = synth.wavefunctions(b, lat, 9, 2)
+    out = cell.chebyfilt(X, 6, 1.5, 5.0, PREC_F32)
+    oc = oracle_cell(b)
+    oc.update(na=na, lm_end=lm_end)
+    ref = O.chebyfilt(oc, X, 6, 1.5, 5.0, veff)
+    assert relmax(out, ref) < 1e-4
+
+
+def test_tensor_core_path_refused_beyond_256_atoms_per_species():
+    # 264 atoms of one species: the tensor-core kernels take at most 256
+    lat, pos = synth.si_diamond(1)
+    big = np.concatenate([pos + 0.01 * k for k in range(33)])[:264]
+    b = basis_gamma(lat, 4.0, None, [264], [big])
+    pkg_a, wnl = synth.kb_form_factors(b, lat)
+    b.update(pkg_a=pkg_a, wnl=wnl, lm_end=[1])
     cell = Cell.from_arrays(b)
     with pytest.raises(PspwError) as e:
         cell.set_nl_path(NL_TENSOR_CORE)
