@@ -4,7 +4,7 @@
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl engine|reference]
                     [--prec f32|f64]
                     [--workload si64|si216|scf-si8|scf-si64|converge-si64|eig-si216|setup-si64|
-                                setup-si216|serve|batch] [--rate R --jobs N --slots S]
+                                setup-si216|serve|batch|dense] [--rate R --jobs N --slots S]
 
 One step = one call of the degree-10 Chebyshev filter (chebyfilt.cpp:6-74)
 on the Si64 cell (64 atoms, a = 20.52 bohr, ecutwfc 15 Ha, 64^3 grid,
@@ -571,6 +571,99 @@ def run_eigsolve(args, rank, world, local_rank):
             "timing": "host wall clock around each solver call"}))
 
 
+# ------------------------------------------------------------------ dense FP64 steps
+DENSE_SHAPES = [  # (name, op, m, n, k)
+    ("Gram X^H Y, Si64 SCF (146 x 146 over NGW 23847)", "C", 146, 146, 23847),
+    ("rotation X Q, Si64 SCF (23847 x 146, k 146)", "N", 23847, 146, 146),
+    ("FP64 projection beta^H psi, Si64 (256 x 144 over NGW 23847)", "C", 256, 144, 23847),
+    ("FP64 back-projection beta W, Si64 (23847 x 144, k 256)", "N", 23847, 144, 256),
+    ("Gram Q^H HQ, Si216 LOBPCG (1536 x 1536 over NGW 80725)", "C", 1536, 1536, 80725),
+]
+
+
+def run_dense(args, rank, world, local_rank):
+    """--workload dense: the FP64 dense steps of the SCF loop and the
+    solvers, timed with CUDA events on the cell stream: the engine's DMMA
+    complex GEMM at the shapes the Si64 SCF and the Si216 LOBPCG use, beside
+    cuBLAS ZGEMM on the same operands (torch.matmul of complex128 tensors,
+    the library baseline), and the 146 x 146 Hermitian eigensolve against
+    cuSOLVER zheevd (torch.linalg.eigh).  Complex MAC = 8 flops."""
+    import torch
+    from pspw import workloads
+    torch.cuda.set_device(local_rank)
+    dev = torch.device("cuda", local_rank)
+    w = workloads.workload("si8")
+    cell = workloads.make_cell(w, device=local_rank)
+    stream = torch.cuda.ExternalStream(cell.stream(), device=dev)
+    g = torch.Generator(device=dev).manual_seed(5)
+    reps = max(3, args.steps)
+
+    def crand(rows, cols):
+        return torch.complex(torch.randn(rows, cols, device=dev, dtype=torch.float64,
+                                         generator=g),
+                             torch.randn(rows, cols, device=dev, dtype=torch.float64,
+                                         generator=g))
+
+    def timed(fn):
+        with torch.cuda.stream(stream):
+            for _ in range(2):
+                fn()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            for _ in range(reps):
+                fn()
+            e1.record(stream)
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / reps
+
+    rows = []
+    for name, op, m, n, k in DENSE_SHAPES:
+        # column-major operands as torch row-major transposes
+        At = crand(m, k) if op == "C" else crand(k, m)   # A^H: A is k x m -> tensor (m, k)
+        Bt = crand(n, k)
+        Ct = torch.zeros(n, m, dtype=torch.complex128, device=dev)
+        lda = k if op == "C" else m
+        ms_own = timed(lambda: cell.zgemm_dev(op, m, n, k, 1.0, At, lda, Bt, k, 0.0, Ct, m))
+        A_lib = At.conj() if op == "C" else At.T  # (m, k)
+        B_lib = Bt.T
+        ms_lib = timed(lambda: torch.matmul(A_lib, B_lib))
+        ref = torch.matmul(A_lib, B_lib)
+        err = float((Ct.T - ref).abs().max() / ref.abs().max())
+        fl = 8.0 * m * n * k
+        rows.append({"gemm": name, "m": m, "n": n, "k": k, "op": op,
+                     "engine_ms": round(ms_own, 4), "engine_tflops": round(fl / ms_own / 1e9, 2),
+                     "cublas_ms": round(ms_lib, 4), "cublas_tflops": round(fl / ms_lib / 1e9, 2),
+                     "rel_diff": err})
+        del At, Bt, Ct, A_lib, B_lib, ref
+    # Hermitian eigensolve of order 146 (the Si64 Rayleigh-Ritz matrix)
+    n = 146
+    M = crand(n, n)
+    H = (M + M.conj().T) * 0.5
+    Hc = H.clone()
+    wv = torch.zeros(n, dtype=torch.float64, device=dev)
+
+    def own_eig():
+        Hc.copy_(H)
+        cell.eig_zheevd_dev(Hc, n, wv, n)
+
+    ms_eig = timed(own_eig)
+    ms_eig_lib = timed(lambda: torch.linalg.eigh(H))
+    wl = torch.linalg.eigvalsh(H)
+    eig_err = float((wv - wl).abs().max() / wl.abs().max())
+    if rank == 0:
+        out = {"metric": "FP64 dense steps: DMMA complex GEMM TFLOP/s at the Si64 SCF shapes",
+               "value": rows[0]["engine_tflops"], "unit": "TFLOP/s", "n_gpus": world,
+               "steps": reps, "warmup": 2, "ms_per_step": rows[0]["engine_ms"],
+               "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+               "dtype": "c128", "data": "synthetic (normal random matrices)",
+               "config": {"workload": "dense: the SCF loop's and LOBPCG's FP64 GEMM shapes, "
+                                      "the 146 x 146 Hermitian eigensolve"},
+               "gemm": rows,
+               "eig146": {"engine_ms": round(ms_eig, 4), "cusolver_ms": round(ms_eig_lib, 4),
+                          "eigenvalue_rel_diff": eig_err}}
+        print(json.dumps(out))
+
+
 # ------------------------------------------------------------------ batched cells
 def run_batch(args, rank, world, local_rank):
     """--workload batch: block H*psi over 32 independent orthorhombic cells
@@ -878,6 +971,9 @@ def run_engine(args, rank, world, local_rank):
             d["alg_tflops"] = round(alg_flops[f] * calls / (t * 1e-3) / 1e12, 2)
         fam_report[names.get(f, str(f))] = d
     roof["traffic"] = _ncu_traffic(args.workload, roof["kernel"], args.prec)
+    roof["traffic_source"] = ("profiles/ncu_traffic.txt: dram__bytes_read.sum + "
+                              "dram__bytes_write.sum per launch from an ncu capture of this "
+                              "command (not measured in this run)")
     kernels_ms = fam_report
     hpsi_ms = ms_max / DEGREE
     hpsi_roof = {"bytes_per_hpsi": hpsi_bytes_model(ngw, nnr, nb, nat, fp64=fp64),
@@ -1029,6 +1125,16 @@ def main():
               "filter_window_ha": [LB, UB], "global_batch": 144 * world,
               "parallelism": f"replica x{world} (bands independent, no collective)",
               "l2": "flushed between steps (256 MB write, outside the timed interval)"}
+
+    if args.workload == "dense":
+        if args.impl == "reference":
+            if rank == 0:
+                print(json.dumps({"impl": "reference", "unavailable":
+                                  "a microbenchmark of the engine's dense kernels against "
+                                  "cuBLAS/cuSOLVER; no CPU counterpart is timed"}))
+            return
+        run_dense(args, rank, world, local_rank)
+        return
 
     if args.workload == "batch":
         if args.impl == "reference":

@@ -124,9 +124,7 @@ void run_job(pspw_server *s, Job *job) {
     if (!rc) {
       // admit when it fits, or when nothing else runs (a job larger than the
       // whole budget runs alone)
-      s->cv_budget.wait(lk, [&] {
-        return s->stop || s->running == 0 || s->used + foot <= s->budget;
-      });
+      s->cv_budget.wait(lk, [&] { return s->running == 0 || s->used + foot <= s->budget; });
       s->used += foot;
       s->running++;
       admitted = true;
