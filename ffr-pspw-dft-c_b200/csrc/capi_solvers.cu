@@ -287,7 +287,7 @@ int pspw_eig_zhegv(pspw_cell *c, double *A, int lda, double *B, int ldb, double 
   return pspw_eig_zhegv_eval(c, A, lda, B, ldb, nullptr, evec, lde, n);
 }
 
-static int solver_entry(bool lobpcg, pspw_cell *c, double *evals, double *X, int nbasis,
+static int solver_entry(int kind, pspw_cell *c, double *evals, double *X, int nbasis,
                         int nstates, const double *prec, int nempty, int max_iter, int hprec,
                         double *resnrm, int *iters) {
   int rc = enter(c);
@@ -302,9 +302,13 @@ static int solver_entry(bool lobpcg, pspw_cell *c, double *evals, double *X, int
       (rc = ws_reserve(c, kSlotB, sizeof(double) * (size_t)nbasis, (void **)&dp)))
     return rc;
   PSPW_CUDA(cudaMemcpyAsync(dp, prec, sizeof(double) * nbasis, cudaMemcpyHostToDevice, c->stream));
-  rc = lobpcg ? lobpcg_dev(c, hprec, evals, dX, nbasis, nstates, dp, nempty, max_iter, resnrm, iters)
-              : davidson_dev(c, hprec, evals, dX, nbasis, nstates, dp, nempty, max_iter, resnrm,
-                             iters);
+  if (kind == 1)
+    rc = lobpcg_dev(c, hprec, evals, dX, nbasis, nstates, dp, nempty, max_iter, resnrm, iters);
+  else if (kind == 2)
+    rc = lobpcg_ortho_dev(c, hprec, evals, dX, nbasis, nstates, dp, nempty, max_iter, resnrm,
+                          iters);
+  else
+    rc = davidson_dev(c, hprec, evals, dX, nbasis, nstates, dp, nempty, max_iter, resnrm, iters);
   if (rc) return rc;
   PSPW_CUDA(cudaMemcpyAsync(X, dX, sizeof(double2) * (size_t)nbasis * nstates,
                             cudaMemcpyDeviceToHost, c->stream));
@@ -314,14 +318,21 @@ static int solver_entry(bool lobpcg, pspw_cell *c, double *evals, double *X, int
 int pspw_davidson(pspw_cell *c, double *evals, double *X, int nbasis, int nstates,
                   const double *prec, int nempty, int max_iter, int hprec, double *resnrm,
                   int *iters) {
-  return solver_entry(false, c, evals, X, nbasis, nstates, prec, nempty, max_iter, hprec, resnrm,
+  return solver_entry(0, c, evals, X, nbasis, nstates, prec, nempty, max_iter, hprec, resnrm,
                       iters);
 }
 
 int pspw_lobpcg(pspw_cell *c, double *lambda, double *X, int nbasis, int nstates,
                 const double *prec, int nempty, int max_iter, int hprec, double *resnrm,
                 int *iters) {
-  return solver_entry(true, c, lambda, X, nbasis, nstates, prec, nempty, max_iter, hprec, resnrm,
+  return solver_entry(1, c, lambda, X, nbasis, nstates, prec, nempty, max_iter, hprec, resnrm,
+                      iters);
+}
+
+int pspw_lobpcg_ortho(pspw_cell *c, double *lambda, double *X, int nbasis, int nstates,
+                      const double *prec, int nempty, int max_iter, int hprec, double *resnrm,
+                      int *iters) {
+  return solver_entry(2, c, lambda, X, nbasis, nstates, prec, nempty, max_iter, hprec, resnrm,
                       iters);
 }
 

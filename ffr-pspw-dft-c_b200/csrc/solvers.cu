@@ -356,6 +356,150 @@ int lobpcg_dev(pspw_cell *c, int hprec, double *lambda_host, double2 *X, int nba
 }
 
 // ------------------------------------------------------------ Lanczos
+// LOBPCG with an orthonormal search basis (an opt-in alternative to the
+// reference's lobpcg_cpu; no counterpart in the reference).  The reference
+// orthonormalises W and P each on its own, so near convergence the overlap
+// of [X W P] becomes nearly singular and eig_zhegv (which scales overlap
+// directions by 1/sqrt(eigenvalue) down to 1.2e-15) amplifies rounding.
+// Here W and P are made orthogonal to X (and W to P) by two block
+// projections and then orthonormalised (Cholesky QR, Householder QR when
+// the Cholesky factorisation fails), so [X W P] is orthonormal and the
+// Rayleigh-Ritz step is a standard Hermitian eigenproblem; P is the
+// component of the new Ritz vectors along [W P] (Hetmaniuk and Lehoucq,
+// "Basis selection in LOBPCG", J. Comput. Phys. 218 (2006) 324-332;
+// Knyazev, SIAM J. Sci. Comput. 23 (2001) 517-541).  Same random start,
+// preconditioner and convergence test as the reference (lobpcg_cpu.cpp:82-86,
+// 142-146, 239-262).
+int lobpcg_ortho_dev(pspw_cell *c, int hprec, double *lambda_host, double2 *X, int nbasis,
+                     int nstates, const double *d_prec, int nempty, int max_iter, double *res_host,
+                     int *iters) {
+  const int nb = nstates, n3 = 3 * nb;
+  const size_t blk = (size_t)nbasis * nb;
+  double2 *Q, *HQ, *t1, *T, *tX, *tH, *tY;
+  double *lam, *lam3, *dots;
+  int rc;
+  if ((rc = block(c, 0, (size_t)nbasis * n3, &Q)) || (rc = block(c, 1, (size_t)nbasis * n3, &HQ)) ||
+      (rc = block(c, 2, (size_t)nb * nb, &t1)) || (rc = block(c, 3, (size_t)n3 * n3, &T)) ||
+      (rc = block(c, 6, blk, &tX)) || (rc = block(c, 9, blk, &tH)) || (rc = block(c, 11, blk, &tY)) ||
+      (rc = dblock(c, 7, nb, &lam)) || (rc = dblock(c, 8, nb, &dots)) ||
+      (rc = dblock(c, 10, n3, &lam3)))
+    return rc;
+  double2 *Xq = Q, *W = Q + blk, *P = Q + 2 * blk;
+  double2 *HXq = HQ, *HW = HQ + blk, *HP = HQ + 2 * blk;
+  std::vector<double2> X0;
+  random_start(X0, nbasis, nb);
+  if ((rc = h2d(c, Xq, X0.data(), sizeof(double2) * blk))) return rc;
+  int info = 0;
+  if ((rc = dev_ortho_qr(c, Xq, nbasis, nbasis, nb, &info))) return rc;
+  if (info) return fail(PSPW_ERR_LAPACK, "zgeqrf/zungqr: info = " + std::to_string(info));
+  if ((rc = apply_h(c, hprec, Xq, HXq, nbasis, nb))) return rc;
+  // Y -= B (B^H Y) and HY -= HB (B^H Y)
+  auto project_out = [&](double2 *Y, double2 *HY, const double2 *Bm, const double2 *HB) -> int {
+    int r;
+    if ((r = zgemm<double>(c, 'C', nb, nb, nbasis, kOne, Bm, nbasis, Y, nbasis, kZero, t1, nb)) ||
+        (r = zgemm<double>(c, 'N', nbasis, nb, nb, kMOne, Bm, nbasis, t1, nb, kOne, Y, nbasis)))
+      return r;
+    if (HY && (r = zgemm<double>(c, 'N', nbasis, nb, nb, kMOne, HB, nbasis, t1, nb, kOne, HY,
+                                 nbasis)))
+      return r;
+    return PSPW_OK;
+  };
+  // orthonormalise Y (and its H image HY, when given) by Cholesky QR;
+  // *ok = false when the Gram matrix is not positive definite
+  auto cholqr = [&](double2 *Y, double2 *HY, bool *ok) -> int {
+    int r;
+    if ((r = zgemm<double>(c, 'C', nb, nb, nbasis, kOne, Y, nbasis, Y, nbasis, kZero, t1, nb)) ||
+        (r = dev_symmetrize(c, t1, nb, nb)))
+      return r;
+    int inf = 0;
+    if ((r = dev_potrf_upper(c, t1, nb, nb, &inf))) return r;
+    *ok = inf == 0;
+    if (!*ok) return PSPW_OK;
+    if ((r = dev_trsm_right_upper(c, t1, nb, Y, nbasis, nbasis, nb))) return r;
+    if (HY && (r = dev_trsm_right_upper(c, t1, nb, HY, nbasis, nbasis, nb))) return r;
+    return PSPW_OK;
+  };
+  std::vector<double> res(nb);
+  const int maxiter = default_maxiter(nb, max_iter);
+  const double TOL = 1.0e-6;
+  bool have_p = false;
+  int iter = 1;
+  for (;;) {
+    // Rayleigh-Ritz on the current basis: X orthonormal, T = X^H HX
+    // (first pass), then residuals W = HX - X diag(lambda)
+    if (iter == 1) {
+      if ((rc = zgemm<double>(c, 'C', nb, nb, nbasis, kOne, Xq, nbasis, HXq, nbasis, kZero, t1,
+                              nb)) ||
+          (rc = dev_symmetrize(c, t1, nb, nb)) || (rc = dev_zheevd(c, t1, nb, lam, nb, &info)))
+        return rc;
+      if (info) return fail(PSPW_ERR_LAPACK, "zheevd: info = " + std::to_string(info));
+      if ((rc = zgemm<double>(c, 'N', nbasis, nb, nb, kOne, Xq, nbasis, t1, nb, kZero, tX,
+                              nbasis)) ||
+          (rc = d2d(c, Xq, tX, sizeof(double2) * blk)) ||
+          (rc = zgemm<double>(c, 'N', nbasis, nb, nb, kOne, HXq, nbasis, t1, nb, kZero, tX,
+                              nbasis)) ||
+          (rc = d2d(c, HXq, tX, sizeof(double2) * blk)))
+        return rc;
+    }
+    if ((rc = dev_residual(c, lam, Xq, nbasis, HXq, nbasis, W, nbasis, nbasis, nb)) ||
+        (rc = dev_coldot(c, W, nbasis, W, nbasis, nbasis, nb, dots)) ||
+        (rc = d2h(c, res.data(), dots, sizeof(double) * nb)))
+      return rc;
+    int nconv = 0;
+    double rn = 0.0;
+    for (auto &v : res) {
+      v = std::sqrt(v);
+      nconv += v < TOL;
+      rn += v;
+    }
+    if ((nconv >= nb - nempty) || (rn / nb < TOL)) break;
+    if (iter > maxiter) break;
+    // W = prec (X lambda - HX), orthogonal to X and P, orthonormal
+    if ((rc = dev_scale_prec(c, nullptr, d_prec, W, nbasis, nbasis, nb))) return rc;
+    for (int pass = 0; pass < 2; pass++) {
+      if ((rc = project_out(W, nullptr, Xq, nullptr))) return rc;
+      if (have_p && (rc = project_out(W, nullptr, P, nullptr))) return rc;
+    }
+    bool ok = false;
+    if ((rc = cholqr(W, nullptr, &ok))) return rc;
+    if (!ok) {
+      if ((rc = dev_ortho_qr(c, W, nbasis, nbasis, nb, &info))) return rc;
+      if (info) return fail(PSPW_ERR_LAPACK, "zgeqrf/zungqr: info = " + std::to_string(info));
+    }
+    if ((rc = apply_h(c, hprec, W, HW, nbasis, nb))) return rc;
+    // standard Rayleigh-Ritz on the orthonormal [X W P]
+    const int nq = have_p ? n3 : 2 * nb;
+    if ((rc = zgemm<double>(c, 'C', nq, nq, nbasis, kOne, Q, nbasis, HQ, nbasis, kZero, T, n3)) ||
+        (rc = dev_symmetrize(c, T, n3, nq)) || (rc = dev_zheevd(c, T, n3, lam3, nq, &info)))
+      return rc;
+    if (info) return fail(PSPW_ERR_LAPACK, "zheevd: info = " + std::to_string(info));
+    if ((rc = d2d(c, lam, lam3, sizeof(double) * nb))) return rc;
+    // P = [W P] U(nb:, 0:nb), HP likewise (before X is overwritten)
+    if ((rc = zgemm<double>(c, 'N', nbasis, nb, nq - nb, kOne, W, nbasis, T + nb, n3, kZero, tX,
+                            nbasis)) ||
+        (rc = zgemm<double>(c, 'N', nbasis, nb, nq - nb, kOne, HW, nbasis, T + nb, n3, kZero, tH,
+                            nbasis)))
+      return rc;
+    // X = Q U(:, 0:nb), HX = HQ U(:, 0:nb)
+    if ((rc = zgemm<double>(c, 'N', nbasis, nb, nq, kOne, Q, nbasis, T, n3, kZero, tY, nbasis)) ||
+        (rc = d2d(c, Xq, tY, sizeof(double2) * blk)) ||
+        (rc = zgemm<double>(c, 'N', nbasis, nb, nq, kOne, HQ, nbasis, T, n3, kZero, tY, nbasis)) ||
+        (rc = d2d(c, HXq, tY, sizeof(double2) * blk)) ||
+        (rc = d2d(c, P, tX, sizeof(double2) * blk)) || (rc = d2d(c, HP, tH, sizeof(double2) * blk)))
+      return rc;
+    // P orthogonal to the new X, orthonormal; dropped when that fails
+    for (int pass = 0; pass < 2; pass++)
+      if ((rc = project_out(P, HP, Xq, HXq))) return rc;
+    if ((rc = cholqr(P, HP, &ok))) return rc;
+    have_p = ok;
+    iter++;
+  }
+  if (iters) *iters = iter;
+  if (res_host) std::copy(res.begin(), res.end(), res_host);
+  if ((rc = d2d(c, X, Xq, sizeof(double2) * blk))) return rc;
+  return d2h(c, lambda_host, lam, sizeof(double) * nb);
+}
+
 int lanczos_dev(pspw_cell *c, double2 *v0, int ngw, int k, double *T_host, int ldT, double2 *f_out,
                 int hprec) {
   double2 *V, *Hv, *f, *h, *s, *ns;

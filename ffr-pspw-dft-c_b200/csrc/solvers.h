@@ -14,6 +14,11 @@ int davidson_dev(pspw_cell *c, int hprec, double *evals_host, double2 *X, int nb
                  const double *d_prec, int nempty, int max_iter, double *res_host, int *iters);
 int lobpcg_dev(pspw_cell *c, int hprec, double *lambda_host, double2 *X, int nbasis, int nstates,
                const double *d_prec, int nempty, int max_iter, double *res_host, int *iters);
+// LOBPCG with an orthonormal [X W P] basis and a standard Rayleigh-Ritz
+// eigenproblem (an opt-in alternative to lobpcg_dev; same start, same test).
+int lobpcg_ortho_dev(pspw_cell *c, int hprec, double *lambda_host, double2 *X, int nbasis,
+                     int nstates, const double *d_prec, int nempty, int max_iter, double *res_host,
+                     int *iters);
 // v0: device, normalised in place; T_host k x k (ldT); f_out device or null.
 // hprec: precision of the H*v products (PSPW_PREC_F64 reproduces lanczos.cpp;
 // PSPW_PREC_F32 for bounds that only shape a filter); the recurrence, the

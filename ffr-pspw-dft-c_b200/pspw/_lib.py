@@ -80,6 +80,7 @@ SIGNATURES = {
     "pspw_eig_zhegv_eval": [_vp, _vp, _i, _vp, _i, _vp, _vp, _i, _i],
     "pspw_davidson": [_vp, _vp, _vp, _i, _i, _vp, _i, _i, _i, _vp, _vp],
     "pspw_lobpcg": [_vp, _vp, _vp, _i, _i, _vp, _i, _i, _i, _vp, _vp],
+    "pspw_lobpcg_ortho": [_vp, _vp, _vp, _i, _i, _vp, _i, _i, _i, _vp, _vp],
     "pspw_lanczos": [_vp, _vp, _i, _i, _vp, _i, _vp],
     "pspw_eval_rho_psi": [_vp, _vp, _vp, _i, _i, _i, _vp, _d, _d, _vp],
     "pspw_eval_enl": [_vp, _vp, _i, _i, _i, _vp, _d, _vp, _vp],

@@ -228,6 +228,10 @@ class Cell:
     def lobpcg(self, nbasis, nstates, prec, nempty, max_iter=None, hprec=PREC_F64):
         return self._solver("pspw_lobpcg", nbasis, nstates, prec, nempty, max_iter, hprec)
 
+    def lobpcg_ortho(self, nbasis, nstates, prec, nempty, max_iter=None, hprec=PREC_F64):
+        """LOBPCG with an orthonormal [X W P] basis (opt-in, see pspw_gpu.h)."""
+        return self._solver("pspw_lobpcg_ortho", nbasis, nstates, prec, nempty, max_iter, hprec)
+
     def lanczos(self, v0, k):
         v = np.array(np.asarray(v0, dtype=np.complex128), copy=True)
         T = np.zeros((k, k), order="F")

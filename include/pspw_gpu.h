@@ -210,6 +210,18 @@ int pspw_davidson(pspw_cell *cell, double *evals, double *X, int nbasis, int nst
 int pspw_lobpcg(pspw_cell *cell, double *lambda, double *X, int nbasis, int nstates,
                 const double *prec, int nempty, int max_iter, int hprec, double *resnrm,
                 int *iters);
+/* LOBPCG with an orthonormal search basis (no reference counterpart; an
+ * opt-in alternative to pspw_lobpcg with the same arguments, start and
+ * convergence test).  The reference's lobpcg_cpu orthonormalises W and P
+ * each on its own and solves a generalised Rayleigh-Ritz problem whose
+ * overlap becomes nearly singular near convergence; here W and P are made
+ * orthogonal to X (W also to P) before their Cholesky QR, so [X W P] is
+ * orthonormal and the Rayleigh-Ritz step is a standard Hermitian
+ * eigenproblem; P is dropped for one iteration when it cannot be
+ * orthonormalised. */
+int pspw_lobpcg_ortho(pspw_cell *cell, double *lambda, double *X, int nbasis, int nstates,
+                      const double *prec, int nempty, int max_iter, int hprec, double *resnrm,
+                      int *iters);
 int pspw_lanczos(pspw_cell *cell, double *v0, int ngw, int k, double *T, int ldT, double *f);
 int pspw_eval_rho_psi(pspw_cell *cell, double *rhoe, const double *eigvec, int ld, int ngw,
                       int nx, const double *focc, double wkpt, double omega, double *ekin);
