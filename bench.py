@@ -648,6 +648,16 @@ def run_dense(args, rank, world, local_rank):
 
     ms_eig = timed(own_eig)
     ms_eig_lib = timed(lambda: torch.linalg.eigh(H))
+    # the SCF's orthonormalisation of the filtered block (23847 x 146)
+    X0 = crand(146, 23847)
+    Xs = X0.clone()
+
+    def own_span():
+        Xs.copy_(X0)
+        cell.ortho_span_dev(Xs, 23847, 146)
+
+    ms_span = timed(own_span)
+    ms_qr_lib = timed(lambda: torch.linalg.qr(X0.T))
     wl = torch.linalg.eigvalsh(H)
     eig_err = float((wv - wl).abs().max() / wl.abs().max())
     if rank == 0:
@@ -660,7 +670,9 @@ def run_dense(args, rank, world, local_rank):
                                       "the 146 x 146 Hermitian eigensolve"},
                "gemm": rows,
                "eig146": {"engine_ms": round(ms_eig, 4), "cusolver_ms": round(ms_eig_lib, 4),
-                          "eigenvalue_rel_diff": eig_err}}
+                          "eigenvalue_rel_diff": eig_err},
+               "ortho_span_23847x146": {"engine_ms": round(ms_span, 4),
+                                        "cusolver_householder_qr_ms": round(ms_qr_lib, 4)}}
         print(json.dumps(out))
 
 

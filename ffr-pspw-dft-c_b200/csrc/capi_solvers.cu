@@ -425,8 +425,8 @@ extern "C" int pspw_zgemm_dev(pspw_cell *c, char opa, int m, int n, int k, const
     return fail(PSPW_ERR_ARG, "zgemm_dev: bad arguments");
   if (m == 0 || n == 0) return PSPW_OK;
   const bool conj = opa == 'C' || opa == 'c';
-  if (!d_A || !d_B || !d_C || lda < std::max(1, conj ? k : m) || ldb < std::max(1, k) ||
-      ldc < m)
+  if ((k > 0 && (!d_A || !d_B)) || !d_C || lda < std::max(1, conj ? k : m) ||
+      ldb < std::max(1, k) || ldc < m)
     return fail(PSPW_ERR_ARG, "zgemm_dev: null matrix or leading dimension too small");
   return zgemm<double>(c, opa, m, n, k, make_double2(alpha[0], alpha[1]),
                        reinterpret_cast<const double2 *>(d_A), lda,

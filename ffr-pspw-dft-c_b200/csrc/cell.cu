@@ -10,6 +10,7 @@
 #include <cstdio>
 #include <cstring>
 #include <map>
+#include <mutex>
 #include <string>
 #include <utility>
 #include <vector>
@@ -48,6 +49,23 @@ int ws_reserve(pspw_cell *c, int slot, size_t bytes, void **out) {
     w.bytes = want;
   }
   *out = w.ptr;
+  return PSPW_OK;
+}
+
+int smem_allow_max(const void *kernel) {
+  static std::mutex mu;
+  static std::map<std::pair<int, const void *>, bool> done;
+  int dev = 0;
+  PSPW_CUDA(cudaGetDevice(&dev));
+  std::lock_guard<std::mutex> lk(mu);
+  if (done.count({dev, kernel})) return PSPW_OK;
+  cudaFuncAttributes a;
+  PSPW_CUDA(cudaFuncGetAttributes(&a, kernel));
+  int optin = 0;
+  PSPW_CUDA(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
+  PSPW_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 optin - (int)a.sharedSizeBytes));
+  done[{dev, kernel}] = true;
   return PSPW_OK;
 }
 

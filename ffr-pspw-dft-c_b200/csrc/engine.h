@@ -130,7 +130,8 @@ enum WsSlot {
   kWsScfB = 35,
   kWsStickX = 36,      // the filter's block in stick order
   kWsHeev = 37,        // the small Hermitian eigensolver's workspace
-  kWsCount = 38
+  kWsSpan = 38,        // pspw_ortho_span_dev: G, U, W, norms (38..41)
+  kWsCount = 42
 };
 
 struct Timing {
@@ -229,6 +230,19 @@ int ws_reserve(pspw_cell *c, int slot, size_t bytes, void **out);
 // After a stream synchronisation: PSPW_ERR_TIMEOUT (and the flag cleared)
 // when a kernel gave up on a bounded wait since the last check.
 int device_status(pspw_cell *c);
+
+// Raises a kernel's dynamic shared-memory limit on the current device to the
+// most the device allows beside the kernel's static shared memory, once per
+// (device, kernel).  Kernels whose dynamic size depends on the problem use
+// this instead of setting the limit to each launch's size: the limit is a
+// per-kernel setting shared by every host thread, so per-size values set by
+// concurrent callers (several cells or jobs at once) could leave it below
+// what another thread's launch requests.
+int smem_allow_max(const void *kernel);
+template <typename K>
+int smem_allow_max(K *kernel) {
+  return smem_allow_max(reinterpret_cast<const void *>(kernel));
+}
 
 // timing hooks (no-ops unless the family is enabled)
 void timing_begin(pspw_cell *c, int family, cudaEvent_t *ev);

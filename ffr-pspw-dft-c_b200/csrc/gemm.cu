@@ -9,8 +9,9 @@
 // FP64 arithmetic on sm_100a; tcgen05 has no FP64 kind).  A complex product
 // is four real products on split real/imaginary fragments:
 //   Cr += Ar Br - Ai Bi,  Ci += Ar Bi + Ai Br   (A^H: Ai -> -Ai).
-// Blocks of 64 x 64 outputs, 8 warps of 32 x 16, K staged through a
-// four-deep cp.async ring of 8-wide complex tiles.  Operands whose K index
+// Warps of 32 x 16 outputs in blocks of 64 x 64, 64 x 32 or 32 x 32 (the
+// shape that pads the output least), K staged through a four-deep cp.async
+// ring of 8-wide complex tiles.  Operands whose K index
 // is contiguous in memory (A^H, B) are staged [row][k]; A in the 'N' form is
 // staged [k][m] (its M index is contiguous), both padded so that the 16-byte
 // fragment loads of a quarter warp hit distinct banks.
@@ -279,17 +280,24 @@ __global__ void k_zgemm_reduce_warp(int m, int n, int nsplit, const cx<R> *__res
 }
 
 // ---------------------------------------------------------------- FP64 DMMA
-namespace dm {
-constexpr int BM = 64, BN = 64, BK = 8, STAGES = 4, THREADS = 256;
-// [row][k] tiles: BK + 4 = 12 complex per row (12 = 4 mod 8): the fragment
-// loads of a quarter warp (rows g, g+1; k = t..t+3) cover 8 distinct 16-byte
-// bank groups.  [k][m] tiles: BM + 2 = 66 per k (66 = 2 mod 8), likewise.
-constexpr int LDK = BK + 4, LDM = BM + 2;
-constexpr int A_ELEMS = BM * LDK > BK * LDM ? BM * LDK : BK * LDM;
-constexpr int B_ELEMS = BN * LDK;
-constexpr int STAGE = A_ELEMS + B_ELEMS;  // complex elements per ring slot
-constexpr size_t SMEM = sizeof(double2) * STAGE * STAGES;
-}  // namespace dm
+// Block tiles of (32 WM) x (16 WN) outputs, WM x WN warps of 32 x 16 each:
+// 64 x 64 (8 warps), 64 x 32 (4 warps) or 32 x 32 (2 warps); the host picks
+// the tile that pads the output least (e.g. 146 columns: 160 with 32-wide
+// tiles against 192 with 64-wide ones).
+template <int WM, int WN>
+struct Dm {
+  static constexpr int BM = 32 * WM, BN = 16 * WN, BK = 8, STAGES = 4;
+  static constexpr int THREADS = 32 * WM * WN;
+  // [row][k] tiles: BK + 4 = 12 complex per row (12 = 4 mod 8): the fragment
+  // loads of a quarter warp (rows g, g+1; k = t..t+3) cover 8 distinct
+  // 16-byte bank groups.  [k][m] tiles: BM + 2 per k (= 2 mod 8), likewise.
+  static constexpr int LDK = BK + 4, LDM = BM + 2;
+  static constexpr int A_ELEMS = BM * LDK > BK * LDM ? BM * LDK : BK * LDM;
+  static constexpr int B_ELEMS = BN * LDK;
+  static constexpr int STAGE = A_ELEMS + B_ELEMS;  // complex elements per ring slot
+  static constexpr size_t SMEM = sizeof(double2) * STAGE * STAGES;
+  static constexpr int MIN_BLOCKS = 16 / (WM * WN);  // 2, 4 or 8 blocks of registers per SM
+};
 
 // d(16 x 8) += a(16 x 4) b(4 x 8), FP64: lane (g = lane / 4, t = lane % 4)
 // holds a = A[g][t], A[g+8][t]; b = B[t][g]; d = D[g][2t], D[g][2t+1],
@@ -303,21 +311,23 @@ __device__ __forceinline__ void dmma(double (&d)[4], double a0, double a1, doubl
 }
 
 // part or C over the block's K slice [blockIdx.z * kchunk, +kchunk)
-template <bool CONJ_A>
-__global__ void __launch_bounds__(dm::THREADS, 2)
+template <bool CONJ_A, int WM, int WN>
+__global__ void __launch_bounds__(Dm<WM, WN>::THREADS, Dm<WM, WN>::MIN_BLOCKS)
     k_zgemm_dmma(int m, int n, int k, double2 alpha, const double2 *__restrict__ A, int lda,
                  const double2 *__restrict__ B, int ldb, double2 beta, double2 *C, int ldc,
                  int kchunk, double2 *__restrict__ part) {
-  using namespace dm;
+  using D = Dm<WM, WN>;
+  constexpr int BM = D::BM, BN = D::BN, BK = D::BK, STAGES = D::STAGES, THREADS = D::THREADS;
+  constexpr int LDK = D::LDK, LDM = D::LDM, A_ELEMS = D::A_ELEMS, STAGE = D::STAGE;
   extern __shared__ __align__(16) double2 sm[];
   const int m0 = blockIdx.x * BM, n0 = blockIdx.y * BN;
   const int kb = blockIdx.z * kchunk, ke = min(k, kb + kchunk);
   const int nkt = ke > kb ? (ke - kb + BK - 1) / BK : 0;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  const int wm = (warp & 1) * 32, wn = (warp >> 1) * 16;
+  const int wm = (warp % WM) * 32, wn = (warp / WM) * 16;
   const int g = lane >> 2, t = lane & 3;
 
-  // one ring slot: 2 x 512 16-byte copies, zero-filled outside the matrices
+  // one ring slot of 16-byte copies, zero-filled outside the matrices
   auto load = [&](int kt, int slot) {
     double2 *As = sm + slot * STAGE, *Bs = As + A_ELEMS;
     const int k0 = kb + kt * BK;
@@ -420,42 +430,45 @@ __global__ void __launch_bounds__(dm::THREADS, 2)
 
 }  // namespace
 
-// FP64, more than 8 columns: DMMA tiles, K split across blocks when the
-// output has fewer than two blocks per SM (the Gram matrices)
-static int zgemm_dmma(pspw_cell *c, bool conj, int m, int n, int k, double2 alpha, const double2 *A,
-               int lda, const double2 *B, int ldb, double2 beta, double2 *C, int ldc) {
-  using namespace dm;
-  cudaStream_t st = c->stream;
-  const int mt = (m + BM - 1) / BM, nt = (n + BN - 1) / BN;
-  static int sms = 0;
-  if (!sms) {
-    int dev = 0;
+static int sm_count_now() {
+  static const int n = [] {
+    int dev = 0, v = 0;
     cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    if (sms <= 0) sms = 148;
-  }
+    cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, dev);
+    return v > 0 ? v : 148;
+  }();
+  return n;
+}
+
+template <int WM, int WN>
+static int launch_dmma(pspw_cell *c, bool conj, int m, int n, int k, double2 alpha,
+                       const double2 *A, int lda, const double2 *B, int ldb, double2 beta,
+                       double2 *C, int ldc) {
+  using D = Dm<WM, WN>;
+  cudaStream_t st = c->stream;
+  const int mt = (m + D::BM - 1) / D::BM, nt = (n + D::BN - 1) / D::BN;
+  // K split over blocks when the output has fewer blocks than the SMs hold
+  const int target = D::MIN_BLOCKS * sm_count_now();
   int nsplit = 1;
-  if (k > 8 * BK && mt * nt < 2 * sms)
-    nsplit = std::max(1, std::min((k + 255) / 256, (2 * sms + mt * nt - 1) / (mt * nt)));
-  int kchunk = k > 0 ? (k + nsplit - 1) / nsplit : BK;
-  kchunk = (kchunk + BK - 1) / BK * BK;
+  if (k > 8 * D::BK && mt * nt < target)
+    nsplit = std::max(1, std::min((k + 255) / 256, (target + mt * nt - 1) / (mt * nt)));
+  int kchunk = k > 0 ? (k + nsplit - 1) / nsplit : D::BK;
+  kchunk = (kchunk + D::BK - 1) / D::BK * D::BK;
   nsplit = k > 0 ? (k + kchunk - 1) / kchunk : 1;
   double2 *part = nullptr;
   if (nsplit > 1) {
-    int rc = ws_reserve(c, 9, sizeof(double2) * (size_t)nsplit * m * n, (void **)&part);
+    int rc = ws_reserve(c, kWsGemmPart, sizeof(double2) * (size_t)nsplit * m * n, (void **)&part);
     if (rc) return rc;
   }
-  PSPW_CUDA(cudaFuncSetAttribute(conj ? k_zgemm_dmma<true> : k_zgemm_dmma<false>,
-                                 cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM));
+  auto kern = conj ? k_zgemm_dmma<true, WM, WN> : k_zgemm_dmma<false, WM, WN>;
+  if (D::SMEM > 48 * 1024) {
+    const int rc = smem_allow_max(kern);
+    if (rc) return rc;
+  }
   cudaEvent_t ev;
   timing_begin(c, kFamGemm, &ev);
-  const dim3 grid(mt, nt, nsplit);
-  if (conj)
-    k_zgemm_dmma<true><<<grid, THREADS, SMEM, st>>>(m, n, k, alpha, A, lda, B, ldb, beta, C, ldc,
-                                                    kchunk, part);
-  else
-    k_zgemm_dmma<false><<<grid, THREADS, SMEM, st>>>(m, n, k, alpha, A, lda, B, ldb, beta, C,
-                                                     ldc, kchunk, part);
+  kern<<<dim3(mt, nt, nsplit), D::THREADS, D::SMEM, st>>>(m, n, k, alpha, A, lda, B, ldb, beta,
+                                                          C, ldc, kchunk, part);
   c->kernel_launches++;
   if (nsplit > 1) {
     k_zgemm_reduce<double><<<std::min<size_t>(4 * 148, ((size_t)m * n + 255) / 256), 256, 0,
@@ -465,6 +478,22 @@ static int zgemm_dmma(pspw_cell *c, bool conj, int m, int n, int k, double2 alph
   timing_end(c, kFamGemm, ev);
   PSPW_CUDA(cudaGetLastError());
   return PSPW_OK;
+}
+
+// FP64, more than 8 columns: DMMA tiles of the shape that pads the output
+// least (ties go to the larger tile, which re-reads its operands less)
+static int zgemm_dmma(pspw_cell *c, bool conj, int m, int n, int k, double2 alpha,
+                      const double2 *A, int lda, const double2 *B, int ldb, double2 beta,
+                      double2 *C, int ldc) {
+  auto padded = [&](int bm, int bn) {
+    return (double)((m + bm - 1) / bm * bm) * (double)((n + bn - 1) / bn * bn);
+  };
+  const double a64 = padded(64, 64), a6432 = padded(64, 32), a32 = padded(32, 32);
+  if (a64 <= a6432 && a64 <= a32)
+    return launch_dmma<2, 4>(c, conj, m, n, k, alpha, A, lda, B, ldb, beta, C, ldc);
+  if (a6432 <= a32)
+    return launch_dmma<2, 2>(c, conj, m, n, k, alpha, A, lda, B, ldb, beta, C, ldc);
+  return launch_dmma<1, 2>(c, conj, m, n, k, alpha, A, lda, B, ldb, beta, C, ldc);
 }
 
 template <typename R>

@@ -82,12 +82,36 @@ __device__ __forceinline__ double warp_sum(double v) {
 // A: n x n column-major (lda), only the upper triangle is read (as zheevd
 // 'U').  Out: d[n], e[n-1], reflectors V (column k holds v_k on rows
 // k+1..n-1, v_k(k+1) = 1), tau[n-1]; H_k = I - tau_k v_k v_k^H, Q = H_0 ...
+// sums of two values over the block (as block_sum, one barrier pair)
+__device__ void block_sum2(double &a, double &b, double *red) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    a += __shfl_xor_sync(0xffffffffu, a, o);
+    b += __shfl_xor_sync(0xffffffffu, b, o);
+  }
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  __syncthreads();
+  if (lane == 0) {
+    red[2 * w] = a;
+    red[2 * w + 1] = b;
+  }
+  __syncthreads();
+  a = 0.0;
+  b = 0.0;
+  for (int i = 0; i < nw; i++) {
+    a += red[2 * i];
+    b += red[2 * i + 1];
+  }
+}
+
+constexpr int kRowsPerWarp = (kHeevMax + kMaxWarpsT1 - 1) / kMaxWarpsT1;  // 5
+
 __global__ void __launch_bounds__(kT1, 1)
     k_hetrd(const double2 *__restrict__ A, int lda, int n, double *__restrict__ d,
             double *__restrict__ e, double2 *__restrict__ V, double2 *__restrict__ tau) {
   extern __shared__ double2 L[];  // packed lower triangle, row-major
   __shared__ double2 v[kHeevMax], y[kHeevMax];
-  __shared__ double red[kMaxWarpsT1];
+  __shared__ double red[2 * kMaxWarpsT1];
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nw = blockDim.x >> 5;
   const int nt = blockDim.x;
   // L(i, j) = conj(A(j, i)) for j <= i
@@ -97,12 +121,13 @@ __global__ void __launch_bounds__(kT1, 1)
   for (int k = 0; k < n - 1; k++) {
     const int k1 = k + 1;
     const double2 alpha = L[lp(k1, k)];
-    double part = 0.0;
+    double part = 0.0, unused = 0.0;
     for (int i = k1 + 1 + tid; i < n; i += nt) {
       const double2 x = L[lp(i, k)];
       part += x.x * x.x + x.y * x.y;
     }
-    const double xn2 = block_sum(part, red);
+    block_sum2(part, unused, red);
+    const double xn2 = part;
     // the reflector: H^H (alpha, x) = (beta, 0), beta real; every thread
     // computes the same values from the same inputs
     double beta;
@@ -131,45 +156,59 @@ __global__ void __launch_bounds__(kT1, 1)
     }
     __syncthreads();
     if (!reflect) continue;  // uniform
-    // y = t * A22 v, A22 the trailing Hermitian block (rows and columns >= k1)
-    for (int i = k1 + warp; i < n; i += nw) {
-      double sr = 0.0, si = 0.0;
+    // y = t * A22 v, A22 the trailing Hermitian block (rows and columns >=
+    // k1); each warp accumulates all its rows first, then reduces them
+    // together, so the shuffle trees of its rows overlap
+    double sr[kRowsPerWarp], si[kRowsPerWarp];
+#pragma unroll
+    for (int r = 0; r < kRowsPerWarp; r++) {
+      sr[r] = 0.0;
+      si[r] = 0.0;
+      const int i = k1 + warp + nw * r;
+      if (i >= n) continue;
       for (int j = k1 + lane; j <= i; j += 32) {  // row i of the lower part
         const double2 a = L[lp(i, j)], b = v[j];
-        sr = fma(a.x, b.x, sr);
-        sr = fma(-a.y, b.y, sr);
-        si = fma(a.x, b.y, si);
-        si = fma(a.y, b.x, si);
+        sr[r] = fma(a.x, b.x, sr[r]);
+        sr[r] = fma(-a.y, b.y, sr[r]);
+        si[r] = fma(a.x, b.y, si[r]);
+        si[r] = fma(a.y, b.x, si[r]);
       }
       for (int j = i + 1 + lane; j < n; j += 32) {  // column i below the diagonal, conjugated
         const double2 a = L[lp(j, i)], b = v[j];
-        sr = fma(a.x, b.x, sr);
-        sr = fma(a.y, b.y, sr);
-        si = fma(a.x, b.y, si);
-        si = fma(-a.y, b.x, si);
+        sr[r] = fma(a.x, b.x, sr[r]);
+        sr[r] = fma(a.y, b.y, sr[r]);
+        si[r] = fma(a.x, b.y, si[r]);
+        si[r] = fma(-a.y, b.x, si[r]);
       }
-      sr = warp_sum(sr);
-      si = warp_sum(si);
-      if (lane == 0) y[i] = cmul(t, make_double2(sr, si));
     }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1)
+#pragma unroll
+      for (int r = 0; r < kRowsPerWarp; r++) {
+        sr[r] += __shfl_xor_sync(0xffffffffu, sr[r], o);
+        si[r] += __shfl_xor_sync(0xffffffffu, si[r], o);
+      }
+    if (lane == 0)
+#pragma unroll
+      for (int r = 0; r < kRowsPerWarp; r++) {
+        const int i = k1 + warp + nw * r;
+        if (i < n) y[i] = cmul(t, make_double2(sr[r], si[r]));
+      }
     __syncthreads();
-    // w = y - (1/2) t (y^H v) v
+    // w = y - (1/2) t (y^H v) v, formed where it is used
     double pr = 0.0, pi = 0.0;
     for (int i = k1 + tid; i < n; i += nt) {
       const double2 a = y[i], b = v[i];
       pr += a.x * b.x + a.y * b.y;
       pi += a.x * b.y - a.y * b.x;
     }
-    const double yr = block_sum(pr, red);
-    const double yi = block_sum(pi, red);
-    const double2 al = cmul(make_double2(-0.5 * t.x, -0.5 * t.y), make_double2(yr, yi));
-    for (int i = k1 + tid; i < n; i += nt) y[i] = y[i] + cmul(al, v[i]);
-    __syncthreads();
+    block_sum2(pr, pi, red);
+    const double2 al = cmul(make_double2(-0.5 * t.x, -0.5 * t.y), make_double2(pr, pi));
     // A22 -= v w^H + w v^H (lower part; the diagonal stays real)
     for (int i = k1 + warp; i < n; i += nw) {
-      const double2 vi = v[i], wi = y[i];
+      const double2 vi = v[i], wi = y[i] + cmul(al, vi);
       for (int j = k1 + lane; j <= i; j += 32) {
-        const double2 vj = v[j], wj = y[j];
+        const double2 vj = v[j], wj = y[j] + cmul(al, vj);
         double2 a = L[lp(i, j)];
         a.x -= vi.x * wj.x + vi.y * wj.y + wi.x * vj.x + wi.y * vj.y;
         a.y -= vi.y * wj.x - vi.x * wj.y + wi.y * vj.x - wi.x * vj.y;
@@ -248,7 +287,11 @@ __global__ void __launch_bounds__(128) k_tri_bisect(const double *__restrict__ d
   if (j >= n) return;  // whole warp
   double lo, hi, tn;
   tri_bounds(d, e, n, &lo, &hi, &tn);
-  const double pad = 2.0 * kEps * tn + 1e-300;
+  if (tn == 0.0) {  // T = 0
+    if (lane == 0) lam[j] = 0.0;
+    return;
+  }
+  const double pad = 2.0 * kEps * tn;
   lo -= pad;
   hi += pad;
   for (int it = 0; it < 20; it++) {
@@ -308,7 +351,7 @@ __device__ void tri_factor(const double *d, const double *e, int n, double s, do
   f.u0[n - 1] = 1.0 / c0;
 }
 
-// z <- (T - s I)^-1 z (strided column of Z), scaled to avoid overflow
+// z <- (T - s I)^-1 z, scaled to avoid overflow (z: a thread-local copy)
 __device__ void tri_solve(const TriLU &f, int n, double *z) {
   for (int i = 0; i < n - 1; i++) {
     if (f.pv[i]) {
@@ -343,15 +386,15 @@ __device__ __forceinline__ double start_value(int i, int col) {
 // One block per eigenvalue index j; the block of a cluster's first index
 // computes the cluster's vectors into columns of Z (n x n, column-major).
 __global__ void __launch_bounds__(kInvitThreads)
-    k_tri_invit(const double *__restrict__ d, const double *__restrict__ e,
-                const double *__restrict__ lam, int n, double *__restrict__ Z,
-                TriLU *__restrict__ lu) {
+    k_tri_invit(const double *__restrict__ dg, const double *__restrict__ eg,
+                const double *__restrict__ lam, int n, double *__restrict__ Z) {
   __shared__ double red[kInvitThreads / 32];
   __shared__ double S[kRRMax * kRRMax], U[kRRMax * kRRMax];
   __shared__ double coef[kHeevMax];
+  __shared__ double d[kHeevMax], e[kHeevMax];
   const int j = blockIdx.x, tid = threadIdx.x;
   double glo, ghi, tn;
-  tri_bounds(d, e, n, &glo, &ghi, &tn);  // every warp computes the same
+  tri_bounds(dg, eg, n, &glo, &ghi, &tn);  // every warp computes the same
   const double gaptol = 1e-3 * tn;
   if (j > 0 && !(lam[j] - lam[j - 1] > gaptol)) return;  // not a cluster's first index
   int c = 1;
@@ -361,14 +404,29 @@ __global__ void __launch_bounds__(kInvitThreads)
     for (int r = tid; r < c * n; r += blockDim.x) zc[r] = (r % n) == j + r / n ? 1.0 : 0.0;
     return;
   }
-  const double floor_ = kEps * fmax(tn, 1e-200);
-  for (int m = tid; m < c; m += blockDim.x) {
-    tri_factor(d, e, n, lam[j + m], floor_, lu[j + m]);
-    for (int i = 0; i < n; i++) zc[(size_t)m * n + i] = start_value(i, j + m);
+  for (int i = tid; i < n; i += blockDim.x) {
+    d[i] = dg[i];
+    e[i] = i + 1 < n ? eg[i] : 0.0;
   }
+  const double floor_ = kEps * fmax(tn, 1e-200);
+  for (int m = tid; m < c; m += blockDim.x)
+    for (int i = 0; i < n; i++) zc[(size_t)m * n + i] = start_value(i, j + m);
   __syncthreads();
+  // each member's factorisation and its vector during a solve live in the
+  // thread's own (local, L1-cached) memory; members beyond the block size
+  // (clusters larger than the block) are factored again for every solve
+  TriLU f;
+  double zl[kHeevMax];
+  if (tid < c) tri_factor(d, e, n, lam[j + tid], floor_, f);
   for (int it = 0; it < kInvitIters; it++) {
-    for (int m = tid; m < c; m += blockDim.x) tri_solve(lu[j + m], n, zc + (size_t)m * n);
+    for (int m = tid; m < c; m += blockDim.x) {
+      if (m != tid) tri_factor(d, e, n, lam[j + m], floor_, f);
+      double *zm = zc + (size_t)m * n;
+      for (int i = 0; i < n; i++) zl[i] = zm[i];
+      tri_solve(f, n, zl);
+      for (int i = 0; i < n; i++) zm[i] = zl[i];
+      if (m != tid && tid < c) tri_factor(d, e, n, lam[j + tid], floor_, f);
+    }
     __syncthreads();
     // block Gram-Schmidt, twice per column, in column order
     for (int m = 0; m < c; m++) {
@@ -570,79 +628,88 @@ __global__ void __launch_bounds__(kT1, 1)
     k_chol_inv(const double2 *__restrict__ G, int ldg, int n, double2 *__restrict__ Uinv, int ldu,
                double *__restrict__ stat) {
   extern __shared__ double2 L[];
-  __shared__ double2 stage[kHeevMax];
-  __shared__ int s_fail;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nw = blockDim.x >> 5;
   for (int i = warp; i < n; i += nw)
     for (int j = lane; j <= i; j += 32) L[lp(i, j)] = cconj(G[j + (size_t)i * ldg]);
-  if (tid == 0) s_fail = 0;
   __syncthreads();
+  // right-looking Cholesky, one barrier per step: step k updates the
+  // trailing triangle with the unscaled column k (L(i,k) conj(L(j,k)) /
+  // L(k,k)) and then scales column k, which no later step reads
   double dmax = 0.0, dmin = INFINITY;
+  int failed = 0;
   for (int k = 0; k < n; k++) {
     const double akk = L[lp(k, k)].x;  // every thread reads the same value
     if (!(akk > 0.0)) {
-      if (tid == 0) s_fail = k + 1;
+      failed = k + 1;
       break;  // uniform
     }
-    const double dk = sqrt(akk), inv = 1.0 / dk;
+    const double ia = 1.0 / akk, dk = sqrt(akk);
     dmax = fmax(dmax, dk);
     dmin = fmin(dmin, dk);
-    __syncthreads();  // all reads of L(k, k) done
-    if (tid == 0) L[lp(k, k)] = make_double2(dk, 0.0);
-    for (int i = k + 1 + tid; i < n; i += blockDim.x) {
-      const double2 a = L[lp(i, k)];
-      L[lp(i, k)] = make_double2(a.x * inv, a.y * inv);
-    }
-    __syncthreads();
-    // trailing update L(i, j) -= L(i, k) conj(L(j, k)), k < j <= i
     for (int i = k + 1 + warp; i < n; i += nw) {
       const double2 lik = L[lp(i, k)];
       for (int j = k + 1 + lane; j <= i; j += 32) {
         const double2 ljk = L[lp(j, k)];
         double2 a = L[lp(i, j)];
-        a.x -= lik.x * ljk.x + lik.y * ljk.y;
-        a.y -= lik.y * ljk.x - lik.x * ljk.y;
+        a.x -= (lik.x * ljk.x + lik.y * ljk.y) * ia;
+        a.y -= (lik.y * ljk.x - lik.x * ljk.y) * ia;
         L[lp(i, j)] = a;
       }
     }
     __syncthreads();
+    const double idk = 1.0 / dk;
+    for (int i = k + 1 + tid; i < n; i += blockDim.x) {
+      const double2 a = L[lp(i, k)];
+      L[lp(i, k)] = make_double2(a.x * idk, a.y * idk);
+    }
+    if (tid == 0) L[lp(k, k)] = make_double2(dk, 0.0);
   }
   __syncthreads();
-  if (s_fail) {
+  if (failed) {
     if (tid == 0) {
-      stat[0] = (double)s_fail;
+      stat[0] = (double)failed;
       stat[1] = INFINITY;
     }
     return;
   }
-  // M = L^-1 in place, row by row: M(i, i) = 1 / L(i, i),
-  // M(i, j) = -M(i, i) sum_{k=j}^{i-1} L(i, k) M(k, j)  (j < i); rows < i of
-  // the packed array already hold M, row i still holds L until the row is
-  // complete (its new values wait in `stage`)
-  for (int i = 0; i < n; i++) {
-    const double mii = 1.0 / L[lp(i, i)].x;
-    for (int j = warp; j < i; j += nw) {
+  // M = L^-1 column by column, no barriers: warp w owns columns w, w + nw,
+  // ...; lane l keeps M(i, j) for i = l (mod 32) in registers, and
+  // M(i, j) = -(1 / L(i, i)) sum_{k=j}^{i-1} L(i, k) M(k, j).
+  // Uinv = M^H: Uinv(r, c) = conj(M(c, r)) for r <= c, 0 below.
+  for (int j = warp; j < n; j += nw) {
+    double2 mk[kRowsPerWarp];
+#pragma unroll
+    for (int q = 0; q < kRowsPerWarp; q++) mk[q] = make_double2(0.0, 0.0);
+    const double mjj = 1.0 / L[lp(j, j)].x;
+#pragma unroll
+    for (int q = 0; q < kRowsPerWarp; q++)
+      if (lane + 32 * q == j) mk[q] = make_double2(mjj, 0.0);
+    if (lane == 0) Uinv[(size_t)j * ldu + j] = make_double2(mjj, 0.0);
+    for (int r = lane; r < n; r += 32)
+      if (r > j) Uinv[(size_t)j * ldu + r] = make_double2(0.0, 0.0);
+    for (int i = j + 1; i < n; i++) {
       double sr = 0.0, si = 0.0;
-      for (int k = j + lane; k < i; k += 32) {
-        const double2 a = L[lp(i, k)], b = L[lp(k, j)];
-        sr = fma(a.x, b.x, sr);
-        sr = fma(-a.y, b.y, sr);
-        si = fma(a.x, b.y, si);
-        si = fma(a.y, b.x, si);
+#pragma unroll
+      for (int q = 0; q < kRowsPerWarp; q++) {
+        const int kk = lane + 32 * q;
+        if (kk >= j && kk < i) {
+          const double2 a = L[lp(i, kk)], b = mk[q];
+          sr = fma(a.x, b.x, sr);
+          sr = fma(-a.y, b.y, sr);
+          si = fma(a.x, b.y, si);
+          si = fma(a.y, b.x, si);
+        }
       }
       sr = warp_sum(sr);
       si = warp_sum(si);
-      if (lane == 0) stage[j] = make_double2(-mii * sr, -mii * si);
+      const double mii = -1.0 / L[lp(i, i)].x;
+      const double2 mij = make_double2(mii * sr, mii * si);
+#pragma unroll
+      for (int q = 0; q < kRowsPerWarp; q++)
+        if (lane + 32 * q == i) mk[q] = mij;
+      if (lane == 0) Uinv[(size_t)i * ldu + j] = cconj(mij);
     }
-    __syncthreads();
-    for (int j = tid; j < i; j += blockDim.x) L[lp(i, j)] = stage[j];
-    if (tid == 0) L[lp(i, i)] = make_double2(mii, 0.0);
-    __syncthreads();
   }
-  // Uinv = M^H: Uinv(r, c) = conj(M(c, r)) for r <= c, 0 below
-  for (int cidx = warp; cidx < n; cidx += nw)
-    for (int r = lane; r < n; r += 32)
-      Uinv[(size_t)cidx * ldu + r] = r <= cidx ? cconj(L[lp(cidx, r)]) : make_double2(0.0, 0.0);
   if (tid == 0) {
     stat[0] = 0.0;
     stat[1] = dmax / dmin;
@@ -653,8 +720,7 @@ __global__ void __launch_bounds__(kT1, 1)
 
 size_t heev_small_workspace(int n) {
   const size_t nn = (size_t)n * n;
-  return sizeof(double2) * (nn + n) + sizeof(double) * (nn + 2 * (size_t)n) +
-         sizeof(TriLU) * (size_t)n + 6 * 256;
+  return sizeof(double2) * (nn + n) + sizeof(double) * (nn + 2 * (size_t)n) + 6 * 256;
 }
 
 int dev_heev_small(pspw_cell *c, double2 *A, int lda, double *w, int n, void *work) {
@@ -673,14 +739,15 @@ int dev_heev_small(pspw_cell *c, double2 *A, int lda, double *w, int n, void *wo
   double *d = static_cast<double *>(take(sizeof(double) * n));
   double *e = static_cast<double *>(take(sizeof(double) * n));
   double *Z = static_cast<double *>(take(sizeof(double) * nn));
-  TriLU *lu = static_cast<TriLU *>(take(sizeof(TriLU) * n));
   const int smem1 = (int)(sizeof(double2) * (size_t)n * (n + 1) / 2);
-  if (smem1 > 48 * 1024)
-    PSPW_CUDA(cudaFuncSetAttribute(k_hetrd, cudaFuncAttributeMaxDynamicSharedMemorySize, smem1));
+  if (smem1 > 48 * 1024) {
+    const int rc = smem_allow_max(k_hetrd);
+    if (rc) return rc;
+  }
   k_hetrd<<<1, kT1, smem1, st>>>(A, lda, n, d, e, V, tau);
   const int wpb = 4;
   k_tri_bisect<<<(n + wpb - 1) / wpb, 32 * wpb, sizeof(double) * 3 * n, st>>>(d, e, n, w);
-  k_tri_invit<<<n, kInvitThreads, 0, st>>>(d, e, w, n, Z, lu);
+  k_tri_invit<<<n, kInvitThreads, 0, st>>>(d, e, w, n, Z);
   k_back_tr<<<(n + 3) / 4, 128, 0, st>>>(V, tau, Z, n, A, lda);
   c->kernel_launches += 4;
   PSPW_CUDA(cudaGetLastError());
@@ -692,9 +759,10 @@ int dev_chol_inv_upper(pspw_cell *c, const double2 *G, int ldg, int n, double2 *
   if (n < 1 || n > kHeevMax || ldg < n || ldu < n)
     return fail(PSPW_ERR_ARG, "chol_inv_upper: n must be in 1.." + std::to_string(kHeevMax));
   const int smem = (int)(sizeof(double2) * (size_t)n * (n + 1) / 2);
-  if (smem > 48 * 1024)
-    PSPW_CUDA(
-        cudaFuncSetAttribute(k_chol_inv, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+  if (smem > 48 * 1024) {
+    const int rc = smem_allow_max(k_chol_inv);
+    if (rc) return rc;
+  }
   k_chol_inv<<<1, kT1, smem, c->stream>>>(G, ldg, n, Uinv, ldu, stat);
   c->kernel_launches++;
   PSPW_CUDA(cudaGetLastError());
@@ -705,9 +773,10 @@ int dev_tri_eigvals(pspw_cell *c, const double *d, const double *e, int n, doubl
   if (n < 1 || n > kTriEigMax) return fail(PSPW_ERR_ARG, "tri_eigvals: bad size");
   const int wpb = 4;
   const size_t smem = sizeof(double) * 3 * (size_t)n;
-  if (smem > 48 * 1024)
-    PSPW_CUDA(
-        cudaFuncSetAttribute(k_tri_bisect, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  if (smem > 48 * 1024) {
+    const int rc = smem_allow_max(k_tri_bisect);
+    if (rc) return rc;
+  }
   k_tri_bisect<<<(n + wpb - 1) / wpb, 32 * wpb, smem, c->stream>>>(d, e, n, w);
   c->kernel_launches++;
   PSPW_CUDA(cudaGetLastError());

@@ -634,9 +634,7 @@ size_t pass_smem(int lines, int n) {
 
 template <typename T, typename K>
 int set_smem(K kernel, size_t bytes) {
-  if (bytes > 48 * 1024)
-    PSPW_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
-  return PSPW_OK;
+  return bytes > 48 * 1024 ? smem_allow_max(kernel) : PSPW_OK;
 }
 
 }  // namespace

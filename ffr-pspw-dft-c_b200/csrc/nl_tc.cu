@@ -661,7 +661,8 @@ int launch_project(pspw_cell *c, const Shape &s, const float2 *psi, int ld, int 
                    const float *pkga, const float *pw) {
   const int mt = (nb * s.per + 127) / 128;
   const int smem = proj_smem(s);
-  PSPW_CUDA(cudaFuncSetAttribute(k_proj_tc<L>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+  int rc = smem_allow_max(k_proj_tc<L>);
+  if (rc) return rc;
   k_proj_tc<L><<<dim3(mt, nsplit), kThreadsP, smem, c->stream>>>(
       psi, ld, ngw, nb, etp, pkga, s.nat, s.npad, kg, part, c->d_err);
   const int total = s.nbtiles * s.nsa * s.nbt * L * 4;  // one warp each
@@ -677,8 +678,8 @@ int launch_back(pspw_cell *c, const Shape &s, const float *wt, const float *etb,
                 const float *pkga, int ngw, int nb, float2 *out, int ldo, const float2 *in,
                 int ldi, const float2 *xm2, int ldx, float a, float b, float g, bool pre) {
   const int smem = back_smem(s);
-  PSPW_CUDA(
-      cudaFuncSetAttribute(k_backproj_tc<L>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+  int rc = smem_allow_max(k_backproj_tc<L>);
+  if (rc) return rc;
   dim3 grid((ngw + 127) / 128, s.nbtiles);
   k_backproj_tc<L><<<grid, kThreads, smem, c->stream>>>(etb, wt, s.nsa, ngw, nb, s.nbt, pkga,
                                                         out, ldo, in, ldi, xm2, ldx, a, b, g, pre,

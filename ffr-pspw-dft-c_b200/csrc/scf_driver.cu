@@ -18,6 +18,7 @@
 #include <chrono>
 #include <cmath>
 #include <cstring>
+#include <string>
 #include <vector>
 
 #include "common.cuh"
@@ -118,6 +119,24 @@ int span_orthonormalize(pspw_cell *c, double2 *X, int ngw, int n, double2 *G, do
   *info = 0;
   return PSPW_OK;
 }
+
+}  // namespace
+
+// C entry of the span orthonormalisation (scratch from the cell's workspaces)
+int ortho_span_dev(pspw_cell *c, double2 *X, int ngw, int n, int *info) {
+  double2 *G, *U, *W;
+  double *dn, *stat;
+  int rc;
+  if ((rc = ws_reserve(c, kWsSpan, sizeof(double2) * (size_t)n * n, (void **)&G)) ||
+      (rc = ws_reserve(c, kWsSpan + 1, sizeof(double2) * (size_t)n * n, (void **)&U)) ||
+      (rc = ws_reserve(c, kWsSpan + 2, sizeof(double2) * (size_t)ngw * n, (void **)&W)) ||
+      (rc = ws_reserve(c, kWsSpan + 3, sizeof(double) * ((size_t)n + 2), (void **)&dn)))
+    return rc;
+  stat = dn + n;
+  return span_orthonormalize(c, X, ngw, n, G, U, dn, stat, W, info);
+}
+
+namespace {
 
 struct DevBuf {
   std::vector<void *> p;
@@ -345,4 +364,14 @@ extern "C" int pspw_cheby_scf(pspw_scf *s, const pspw_scf_params *p, const doubl
   for (int i = 0; i < 6; i++) e6[i] = en[i];
   *iterations = done_iters;
   return device_status(c);
+}
+
+extern "C" int pspw_ortho_span_dev(pspw_cell *c, double *d_X, int ngw, int n) {
+  if (!c || !d_X || n < 1 || ngw < n) return fail(PSPW_ERR_ARG, "ortho_span_dev: bad arguments");
+  PSPW_CUDA(cudaSetDevice(c->device));
+  int info = 0;
+  const int rc = ortho_span_dev(c, reinterpret_cast<double2 *>(d_X), ngw, n, &info);
+  if (rc) return rc;
+  if (info) return fail(PSPW_ERR_LAPACK, "ortho_span_dev: info = " + std::to_string(info));
+  return PSPW_OK;
 }

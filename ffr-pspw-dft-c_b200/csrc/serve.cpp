@@ -158,6 +158,11 @@ void run_job(pspw_server *s, Job *job) {
       pspw_system_destroy(S);
     }
   }
+  if (rc) {
+    const char *m = pspw_last_error();  // this worker thread's last message
+    std::strncpy(r.error, m ? m : "", sizeof r.error - 1);
+    r.error[sizeof r.error - 1] = '\0';
+  }
   std::lock_guard<std::mutex> lk(s->mu);
   r.status = rc;
   r.t_done = s->now();

@@ -129,6 +129,7 @@ SIGNATURES = {
     "pspw_server_destroy": [_vp],
     "pspw_zgemm_dev": [_vp, C.c_char, _i, _i, _i, _vp, _vp, _i, _vp, _i, _vp, _vp, _i],
     "pspw_eig_zheevd_dev": [_vp, _vp, _i, _vp, _i],
+    "pspw_ortho_span_dev": [_vp, _vp, _i, _i],
 }
 _RESTYPE = {"pspw_error_string": C.c_char_p, "pspw_last_error": C.c_char_p}
 

@@ -183,6 +183,11 @@ class Cell:
         into A, ascending eigenvalues into w), enqueued on the cell stream."""
         check(lib().pspw_eig_zheevd_dev(self._h, ptr(d_a), int(lda), ptr(d_w), int(n)))
 
+    def ortho_span_dev(self, d_x, ngw, n):
+        """Orthonormal basis of span(X) in place (device, ld ngw): the SCF
+        loop's CholeskyQR2 step."""
+        check(lib().pspw_ortho_span_dev(self._h, ptr(d_x), int(ngw), int(n)))
+
     # ---- solvers and dense steps (host buffers; reference semantics)
     def gen_prec(self, nbasis, tau):
         p = np.zeros(nbasis)

@@ -31,7 +31,7 @@ class JobResult(C.Structure):
                 ("ngw", C.c_int), ("nnr", C.c_int), ("iterations", C.c_int),
                 ("converged", C.c_int), ("etot", C.c_double), ("footprint_bytes", C.c_double),
                 ("t_submit", C.c_double), ("t_admit", C.c_double), ("t_scf", C.c_double),
-                ("t_done", C.c_double)]
+                ("t_done", C.c_double), ("error", C.c_char * 160)]
 
 
 class Server:
@@ -56,6 +56,7 @@ class Server:
         check(lib().pspw_server_wait(self._h, int(job_id), C.byref(r), eig.ctypes.data,
                                      int(neig)))
         out = {name: getattr(r, name) for name, _ in JobResult._fields_}
+        out["error"] = r.error.decode(errors="replace")
         if neig:
             out["eig"] = eig[:neig]
         return out

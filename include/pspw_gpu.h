@@ -265,6 +265,16 @@ int pspw_zgemm_dev(pspw_cell *cell, char opa, int m, int n, int k, const double 
  *             block's shared memory, bisection, inverse iteration; larger n
  *             on cuSOLVER zheevd.  Bitwise repeatable. */
 int pspw_eig_zheevd_dev(pspw_cell *cell, double *d_A, int lda, double *d_w, int n);
+/* ortho_span_dev  an orthonormal basis of span(X) in place, the step that
+ *             ortho_qr performs in the Chebyshev SCF loop
+ *             (ChebySCFLoop.cpp:288-291): columns scaled to unit norm, then
+ *             CholeskyQR2 (Gram matrices and products by U^-1 on the DMMA
+ *             GEMM, Cholesky factor and inverse in one block) for n <= 160,
+ *             the Householder QR when the first Cholesky factor shows
+ *             cond(X) above 1e6 or n > 160.  X: device, ngw x n, ld ngw.
+ *             The basis spans the same space as ortho_qr's and Rayleigh-Ritz
+ *             gives the same Ritz pairs; the columns themselves differ. */
+int pspw_ortho_span_dev(pspw_cell *cell, double *d_X, int ngw, int n);
 
 /* ------------------------------------------------------------------ SCF pieces
  * The steps of the SCF iteration around the eigensolver, on the device in
@@ -496,6 +506,7 @@ typedef struct {
   double etot;             /* final total energy (Ha) */
   double footprint_bytes;  /* the estimate the admission used */
   double t_submit, t_admit, t_scf, t_done;  /* submitted, admitted, SCF start, done */
+  char error[160];         /* the job's error message when status != PSPW_OK */
 } pspw_job_result;
 int pspw_server_create(int device, const pspw_server_config *cfg, pspw_server **out);
 int pspw_server_submit(pspw_server *server, const char *dir, int *job_id);

@@ -176,3 +176,23 @@ def test_eig_zheevd_dev_is_bitwise_repeatable(cell):
     w1, v1 = _eig_dev(cell, a)
     w2, v2 = _eig_dev(cell, a)
     assert np.array_equal(w1, w2) and np.array_equal(v1, v2)
+
+
+# ---------------------------------------------------------------- span orthonormalisation
+@pytest.mark.parametrize("ngw,n,cond", [(3000, 146, 1e2), (2945, 23, 1e4), (5000, 60, 1e8)])
+def test_ortho_span_dev(cell, ngw, n, cond):
+    """CholeskyQR2 on unit-norm columns (and the Householder QR past the
+    conditioning limit): orthonormal columns spanning the input's space."""
+    rng = np.random.default_rng(n)
+    q, _ = np.linalg.qr(rng.standard_normal((ngw, n)) + 1j * rng.standard_normal((ngw, n)))
+    v, _ = np.linalg.qr(rng.standard_normal((n, n)) + 1j * rng.standard_normal((n, n)))
+    x = (q * np.logspace(0, -np.log10(cond), n)) @ v  # condition number `cond`
+    x *= np.logspace(0, 3, n)  # and columns of very different lengths
+    d = torch.from_numpy(np.ascontiguousarray(x.T)).cuda()
+    torch.cuda.synchronize()
+    cell.ortho_span_dev(d, ngw, n)
+    torch.cuda.synchronize()
+    y = d.cpu().numpy().T
+    assert np.abs(y.conj().T @ y - np.eye(n)).max() < 1e-12
+    # span(Y) = span(X): X is reproduced by its projection on Y
+    assert np.abs(x - y @ (y.conj().T @ x)).max() < 1e-9 * np.abs(x).max() * cond

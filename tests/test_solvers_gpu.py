@@ -180,15 +180,18 @@ def test_lobpcg_ortho_converges_to_the_same_eigenvalues(si8_12ry):
     b, cell, veff = si8_12ry
     ngw = b["ngw"]
     prec = O.gen_prec(b["xkg"][:ngw], b["alat"], b["tpiba2"], -10.0)
-    ev, X, res, it = cell.lobpcg_ortho(ngw, 12, prec, 4, max_iter=200)
-    assert it < 200 and np.sort(res)[: 12 - 4].max() < 1e-6
+    # this cell converges slowly with the reference's preconditioner (about
+    # 230 iterations for 8 states below 1e-6 in a numpy run of the same
+    # algorithm on its dense H), so the cap is well above that
+    ev, X, res, it = cell.lobpcg_ortho(ngw, 12, prec, 4, max_iter=500)
+    assert it < 500 and np.sort(res)[: 12 - 4].max() < 1e-6
     # exact lowest eigenvalues: H on the identity block, Hermitian eigensolve
     H = cell.apply_ham_block(np.eye(ngw, dtype=complex))
     exact = np.linalg.eigvalsh(0.5 * (H + H.conj().T))[:12]
     ok = res < 1e-6
     assert np.abs(ev[ok] - exact[ok]).max() < 1e-9
     assert np.abs(X.conj().T @ X - np.eye(12)).max() < 1e-12
-    ev32, _, res32, it32 = cell.lobpcg_ortho(ngw, 12, prec, 4, max_iter=200, hprec=PREC_F32)
+    ev32, _, res32, it32 = cell.lobpcg_ortho(ngw, 12, prec, 4, max_iter=300, hprec=PREC_F32)
     ok = (res < 1e-5) & (res32 < 1e-4)
     assert ok.sum() >= 8
     assert np.abs(ev32[ok] - exact[ok]).max() < 1e-5
