@@ -82,52 +82,55 @@ __device__ __forceinline__ double warp_sum(double v) {
 // A: n x n column-major (lda), only the upper triangle is read (as zheevd
 // 'U').  Out: d[n], e[n-1], reflectors V (column k holds v_k on rows
 // k+1..n-1, v_k(k+1) = 1), tau[n-1]; H_k = I - tau_k v_k v_k^H, Q = H_0 ...
-// sums of two values over the block (as block_sum, one barrier pair)
-__device__ void block_sum2(double &a, double &b, double *red) {
+// Sum of one value per thread over the block, the same bits in every
+// thread: warp xor trees, then every warp reduces the warp sums with the
+// same tree.  `red` holds one value per warp; the leading barrier protects
+// it from the previous call's readers.
+__device__ double block_sum_fast(double v, double *red) {
 #pragma unroll
-  for (int o = 16; o > 0; o >>= 1) {
-    a += __shfl_xor_sync(0xffffffffu, a, o);
-    b += __shfl_xor_sync(0xffffffffu, b, o);
-  }
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
   __syncthreads();
-  if (lane == 0) {
-    red[2 * w] = a;
-    red[2 * w + 1] = b;
-  }
+  if (lane == 0) red[w] = v;
   __syncthreads();
-  a = 0.0;
-  b = 0.0;
-  for (int i = 0; i < nw; i++) {
-    a += red[2 * i];
-    b += red[2 * i + 1];
-  }
+  double s = lane < nw ? red[lane] : 0.0;
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+  return s;
 }
 
-constexpr int kRowsPerWarp = (kHeevMax + kMaxWarpsT1 - 1) / kMaxWarpsT1;  // 5
+constexpr int kTR = 256;                      // threads of the reduction block
+constexpr int kTRW = kTR / 32;                // its warps
+constexpr int kRowsW = (kHeevMax + kTRW - 1) / kTRW;  // trailing rows per warp
+constexpr int kColsL = (kHeevMax + 31) / 32;          // trailing columns per lane
 
-__global__ void __launch_bounds__(kT1, 1)
+// Householder reduction, one block of kTR threads.  Per step the trailing
+// Hermitian matrix-vector product reads each stored row once: warp w takes
+// rows k1 + w + 8 t; lane l the columns k1 + l + 32 q of those rows.  The
+// row's own sum (lower part) is reduced over the lanes, all rows of a warp
+// in one batched shuffle tree; the transposed contributions conj(L(i,j)) v_i
+// to y_j collect in the lane's registers and then in one partial vector per
+// warp, summed in warp order.
+__global__ void __launch_bounds__(kTR, 1)
     k_hetrd(const double2 *__restrict__ A, int lda, int n, double *__restrict__ d,
             double *__restrict__ e, double2 *__restrict__ V, double2 *__restrict__ tau) {
-  extern __shared__ double2 L[];  // packed lower triangle, row-major
+  extern __shared__ double2 L[];  // packed lower triangle, row-major; then partials
+  double2 *P = L + (size_t)n * (n + 1) / 2;  // [kTRW][n] column partials
   __shared__ double2 v[kHeevMax], y[kHeevMax];
-  __shared__ double red[2 * kMaxWarpsT1];
-  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nw = blockDim.x >> 5;
-  const int nt = blockDim.x;
-  // L(i, j) = conj(A(j, i)) for j <= i
-  for (int i = warp; i < n; i += nw)
+  __shared__ double red[kTRW];
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  for (int i = warp; i < n; i += kTRW)
     for (int j = lane; j <= i; j += 32) L[lp(i, j)] = cconj(A[j + (size_t)i * lda]);
   __syncthreads();
   for (int k = 0; k < n - 1; k++) {
     const int k1 = k + 1;
     const double2 alpha = L[lp(k1, k)];
-    double part = 0.0, unused = 0.0;
-    for (int i = k1 + 1 + tid; i < n; i += nt) {
+    double part = 0.0;
+    for (int i = k1 + 1 + tid; i < n; i += kTR) {
       const double2 x = L[lp(i, k)];
       part += x.x * x.x + x.y * x.y;
     }
-    block_sum2(part, unused, red);
-    const double xn2 = part;
+    const double xn2 = block_sum_fast(part, red);
     // the reflector: H^H (alpha, x) = (beta, 0), beta real; every thread
     // computes the same values from the same inputs
     double beta;
@@ -143,7 +146,7 @@ __global__ void __launch_bounds__(kT1, 1)
       sc = make_double2(den.x / dd, -den.y / dd);
     }
     const bool reflect = t.x != 0.0 || t.y != 0.0;
-    for (int i = k1 + tid; i < n; i += nt) {
+    for (int i = k1 + tid; i < n; i += kTR) {
       const double2 vi = i == k1 ? make_double2(1.0, 0.0)
                                  : (reflect ? cmul(L[lp(i, k)], sc) : make_double2(0.0, 0.0));
       v[i] = vi;
@@ -156,64 +159,81 @@ __global__ void __launch_bounds__(kT1, 1)
     }
     __syncthreads();
     if (!reflect) continue;  // uniform
-    // y = t * A22 v, A22 the trailing Hermitian block (rows and columns >=
-    // k1); each warp accumulates all its rows first, then reduces them
-    // together, so the shuffle trees of its rows overlap
-    double sr[kRowsPerWarp], si[kRowsPerWarp];
+    // y = t * A22 v
+    double rs[kRowsW][2];
+    double2 ca[kColsL];
 #pragma unroll
-    for (int r = 0; r < kRowsPerWarp; r++) {
-      sr[r] = 0.0;
-      si[r] = 0.0;
-      const int i = k1 + warp + nw * r;
+    for (int q = 0; q < kColsL; q++) ca[q] = make_double2(0.0, 0.0);
+#pragma unroll
+    for (int r = 0; r < kRowsW; r++) {
+      rs[r][0] = 0.0;
+      rs[r][1] = 0.0;
+      const int i = k1 + warp + kTRW * r;
       if (i >= n) continue;
-      for (int j = k1 + lane; j <= i; j += 32) {  // row i of the lower part
-        const double2 a = L[lp(i, j)], b = v[j];
-        sr[r] = fma(a.x, b.x, sr[r]);
-        sr[r] = fma(-a.y, b.y, sr[r]);
-        si[r] = fma(a.x, b.y, si[r]);
-        si[r] = fma(a.y, b.x, si[r]);
-      }
-      for (int j = i + 1 + lane; j < n; j += 32) {  // column i below the diagonal, conjugated
-        const double2 a = L[lp(j, i)], b = v[j];
-        sr[r] = fma(a.x, b.x, sr[r]);
-        sr[r] = fma(a.y, b.y, sr[r]);
-        si[r] = fma(a.x, b.y, si[r]);
-        si[r] = fma(-a.y, b.x, si[r]);
+      const double2 vi = v[i];
+      const double2 *row = L + lp(i, 0);
+#pragma unroll
+      for (int q = 0; q < kColsL; q++) {
+        const int j = k1 + lane + 32 * q;
+        if (j > i) break;
+        const double2 a = row[j], b = v[j];
+        rs[r][0] = fma(a.x, b.x, rs[r][0]);
+        rs[r][0] = fma(-a.y, b.y, rs[r][0]);
+        rs[r][1] = fma(a.x, b.y, rs[r][1]);
+        rs[r][1] = fma(a.y, b.x, rs[r][1]);
+        if (j < i) {  // conj(L(i,j)) v_i belongs to y_j
+          ca[q].x = fma(a.x, vi.x, ca[q].x);
+          ca[q].x = fma(a.y, vi.y, ca[q].x);
+          ca[q].y = fma(a.x, vi.y, ca[q].y);
+          ca[q].y = fma(-a.y, vi.x, ca[q].y);
+        }
       }
     }
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1)
 #pragma unroll
-      for (int r = 0; r < kRowsPerWarp; r++) {
-        sr[r] += __shfl_xor_sync(0xffffffffu, sr[r], o);
-        si[r] += __shfl_xor_sync(0xffffffffu, si[r], o);
+      for (int r = 0; r < kRowsW; r++) {
+        rs[r][0] += __shfl_xor_sync(0xffffffffu, rs[r][0], o);
+        rs[r][1] += __shfl_xor_sync(0xffffffffu, rs[r][1], o);
       }
+#pragma unroll
+    for (int q = 0; q < kColsL; q++) {
+      const int j = k1 + lane + 32 * q;
+      if (j < n) P[(size_t)warp * n + j] = ca[q];
+    }
     if (lane == 0)
 #pragma unroll
-      for (int r = 0; r < kRowsPerWarp; r++) {
-        const int i = k1 + warp + nw * r;
-        if (i < n) y[i] = cmul(t, make_double2(sr[r], si[r]));
+      for (int r = 0; r < kRowsW; r++) {
+        const int i = k1 + warp + kTRW * r;
+        if (i < n) y[i] = make_double2(rs[r][0], rs[r][1]);
       }
     __syncthreads();
-    // w = y - (1/2) t (y^H v) v, formed where it is used
-    double pr = 0.0, pi = 0.0;
-    for (int i = k1 + tid; i < n; i += nt) {
-      const double2 a = y[i], b = v[i];
-      pr += a.x * b.x + a.y * b.y;
-      pi += a.x * b.y - a.y * b.x;
+    double pr = 0.0, pim = 0.0;
+    for (int i = k1 + tid; i < n; i += kTR) {
+      double2 s2 = y[i];
+#pragma unroll
+      for (int w = 0; w < kTRW; w++) s2 = s2 + P[(size_t)w * n + i];
+      s2 = cmul(t, s2);
+      y[i] = s2;
+      const double2 b = v[i];
+      pr += s2.x * b.x + s2.y * b.y;
+      pim += s2.x * b.y - s2.y * b.x;
     }
-    block_sum2(pr, pi, red);
-    const double2 al = cmul(make_double2(-0.5 * t.x, -0.5 * t.y), make_double2(pr, pi));
+    // al = -(1/2) t (y^H v); w = y + al v is formed where it is used
+    const double yr = block_sum_fast(pr, red);
+    const double yi = block_sum_fast(pim, red);
+    const double2 al = cmul(make_double2(-0.5 * t.x, -0.5 * t.y), make_double2(yr, yi));
     // A22 -= v w^H + w v^H (lower part; the diagonal stays real)
-    for (int i = k1 + warp; i < n; i += nw) {
+    for (int i = k1 + warp; i < n; i += kTRW) {
       const double2 vi = v[i], wi = y[i] + cmul(al, vi);
+      double2 *row = L + lp(i, 0);
       for (int j = k1 + lane; j <= i; j += 32) {
         const double2 vj = v[j], wj = y[j] + cmul(al, vj);
-        double2 a = L[lp(i, j)];
+        double2 a = row[j];
         a.x -= vi.x * wj.x + vi.y * wj.y + wi.x * vj.x + wi.y * vj.y;
         a.y -= vi.y * wj.x - vi.x * wj.y + wi.y * vj.x - wi.x * vj.y;
         if (j == i) a.y = 0.0;
-        L[lp(i, j)] = a;
+        row[j] = a;
       }
     }
     __syncthreads();
@@ -225,13 +245,21 @@ __global__ void __launch_bounds__(kT1, 1)
 // number of eigenvalues of T below x (e2 = squared off-diagonal)
 __device__ int sturm_below(const double *d, const double *e2, int n, double x) {
   double pm = 1.0, p = d[0] - x;
-  int s = p == 0.0 ? -1 : (p < 0.0 ? -1 : 1);
+  int s = p < 0.0 || p == 0.0 ? -1 : 1;
   int cnt = s < 0;
-  for (int i = 1; i < n; i++) {
-    const double pn = fma(d[i] - x, p, -e2[i - 1] * pm);
-    pm = p;
-    p = pn;
-    const double ap = fabs(p);
+  int i = 1;
+  // two steps per rescale check: with ||T|| in [1, 2) a step changes |p| by
+  // at most a factor of 16, far inside the 2^200 margins
+  for (; i + 1 < n; i += 2) {
+    const double p1 = fma(d[i] - x, p, -e2[i - 1] * pm);
+    const int s1 = p1 == 0.0 ? -s : (p1 < 0.0 ? -1 : 1);
+    const double p2 = fma(d[i + 1] - x, p1, -e2[i] * p);
+    const int s2 = p2 == 0.0 ? -s1 : (p2 < 0.0 ? -1 : 1);
+    cnt += (s1 != s) + (s2 != s1);
+    s = s2;
+    pm = p1;
+    p = p2;
+    const double ap = fabs(p) + fabs(pm);
     if (ap > 0x1p+200) {
       p *= 0x1p-200;
       pm *= 0x1p-200;
@@ -239,9 +267,14 @@ __device__ int sturm_below(const double *d, const double *e2, int n, double x) {
       p *= 0x1p+200;
       pm *= 0x1p+200;
     }
-    const int sn = p == 0.0 ? -s : (p < 0.0 ? -1 : 1);
+  }
+  for (; i < n; i++) {
+    const double pn = fma(d[i] - x, p, -e2[i - 1] * pm);
+    const int sn = pn == 0.0 ? -s : (pn < 0.0 ? -1 : 1);
     cnt += sn != s;
     s = sn;
+    pm = p;
+    p = pn;
   }
   return cnt;
 }
@@ -276,27 +309,39 @@ __global__ void __launch_bounds__(128) k_tri_bisect(const double *__restrict__ d
   double *d = sh, *e = sh + n, *e2 = sh + 2 * n;
   for (int i = threadIdx.x; i < n; i += blockDim.x) {
     d[i] = dg[i];
-    if (i + 1 < n) {
-      e[i] = eg[i];
-      e2[i] = eg[i] * eg[i];
-    }
+    e[i] = i + 1 < n ? eg[i] : 0.0;
   }
   __syncthreads();
   const int j = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
   const int lane = threadIdx.x & 31;
-  if (j >= n) return;  // whole warp
   double lo, hi, tn;
-  tri_bounds(d, e, n, &lo, &hi, &tn);
+  if (threadIdx.x < 32) tri_bounds(d, e, n, &lo, &hi, &tn);
+  __shared__ double s_tn;
+  if (threadIdx.x == 0) s_tn = tn;
+  __syncthreads();
+  tn = s_tn;
   if (tn == 0.0) {  // T = 0
-    if (lane == 0) lam[j] = 0.0;
+    if (j < n && lane == 0) lam[j] = 0.0;
     return;
   }
+  // T scaled by a power of two to ||T|| in [1, 2) (exact), so the Sturm
+  // recurrence neither overflows nor underflows for matrices of any scale
+  const double sc = ldexp(1.0, -ilogb(tn));
+  __syncthreads();
+  for (int i = threadIdx.x; i < n; i += blockDim.x) {
+    d[i] *= sc;
+    e[i] *= sc;
+    e2[i] = e[i] * e[i];
+  }
+  __syncthreads();
+  if (j >= n) return;  // whole warp
+  tri_bounds(d, e, n, &lo, &hi, &tn);
   const double pad = 2.0 * kEps * tn;
   lo -= pad;
   hi += pad;
   for (int it = 0; it < 20; it++) {
     if (hi - lo <= fmax(2.0 * kEps * fmax(fabs(lo), fabs(hi)), kEps * tn)) break;
-    const double x = lo + (hi - lo) * (double)(lane + 1) / 33.0;
+    const double x = lo + (hi - lo) * ((double)(lane + 1) * (1.0 / 33.0));
     const unsigned above = __ballot_sync(0xffffffffu, sturm_below(d, e2, n, x) > j);
     const double xs = __shfl_sync(0xffffffffu, x, above ? __ffs(above) - 1 : 31);
     if (above) {
@@ -308,7 +353,7 @@ __global__ void __launch_bounds__(128) k_tri_bisect(const double *__restrict__ d
       lo = xs;
     }
   }
-  if (lane == 0) lam[j] = 0.5 * (lo + hi);
+  if (lane == 0) lam[j] = 0.5 * (lo + hi) / sc;
 }
 
 // ---------------------------------------------------------------- 3 vectors of T
@@ -573,44 +618,61 @@ __global__ void __launch_bounds__(kInvitThreads)
 }
 
 // ---------------------------------------------------------------- 4 back-transform
-// column j of A <- Q z_j, one warp per column; lane l holds rows l, l+32, ..
-__global__ void __launch_bounds__(128) k_back_tr(const double2 *__restrict__ V,
-                                                 const double2 *__restrict__ tau,
-                                                 const double *__restrict__ Z, int n,
-                                                 double2 *__restrict__ A, int lda) {
+// column j of A <- Q z_j, one warp per column, 16 columns per block; lane l
+// holds rows l, l+32, ...  The reflectors pass through shared memory in
+// chunks of kBTChunk (one barrier per chunk), shared by the block's warps.
+constexpr int kBTWarps = 16, kBTChunk = 8;
+__global__ void __launch_bounds__(32 * kBTWarps) k_back_tr(const double2 *__restrict__ V,
+                                                            const double2 *__restrict__ tau,
+                                                            const double *__restrict__ Z, int n,
+                                                            double2 *__restrict__ A, int lda) {
   constexpr int R = (kHeevMax + 31) / 32;
-  const int j = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
-  const int lane = threadIdx.x & 31;
-  if (j >= n) return;
+  __shared__ double2 vs[kBTChunk][kHeevMax];
+  __shared__ double2 ts[kBTChunk];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int j = blockIdx.x * kBTWarps + warp;
+  const bool col = j < n;
   double2 y[R];
 #pragma unroll
   for (int r = 0; r < R; r++) {
     const int i = lane + 32 * r;
-    y[r] = make_double2(i < n ? Z[(size_t)j * n + i] : 0.0, 0.0);
+    y[r] = make_double2(col && i < n ? Z[(size_t)j * n + i] : 0.0, 0.0);
   }
-  for (int k = n - 2; k >= 0; k--) {
-    const double2 t = tau[k];
-    if (t.x == 0.0 && t.y == 0.0) continue;
-    const double2 *vk = V + (size_t)k * n;
-    double sr = 0.0, si = 0.0;  // s = v^H y over rows > k
+  for (int kc = n - 2; kc >= 0; kc -= kBTChunk) {
+    const int k0 = max(0, kc - kBTChunk + 1);  // reflectors k0..kc, applied kc first
+    __syncthreads();
+    for (int e = threadIdx.x; e < (kc - k0 + 1) * n; e += blockDim.x) {
+      const int kk = e / n, i = e % n;
+      vs[kk][i] = i > k0 + kk ? V[(size_t)(k0 + kk) * n + i] : make_double2(0.0, 0.0);
+    }
+    if (threadIdx.x <= kc - k0) ts[threadIdx.x] = tau[k0 + threadIdx.x];
+    __syncthreads();
+    if (!col) continue;
+    for (int k = kc; k >= k0; k--) {
+      const double2 t = ts[k - k0];
+      if (t.x == 0.0 && t.y == 0.0) continue;
+      const double2 *vk = vs[k - k0];
+      double sr = 0.0, si = 0.0;  // s = v^H y over rows > k (zeros elsewhere)
 #pragma unroll
-    for (int r = 0; r < R; r++) {
-      const int i = lane + 32 * r;
-      if (i > k && i < n) {
-        const double2 a = vk[i];
-        sr += a.x * y[r].x + a.y * y[r].y;
-        si += a.x * y[r].y - a.y * y[r].x;
+      for (int r = 0; r < R; r++) {
+        const int i = lane + 32 * r;
+        if (i < n) {
+          const double2 a = vk[i];
+          sr += a.x * y[r].x + a.y * y[r].y;
+          si += a.x * y[r].y - a.y * y[r].x;
+        }
+      }
+      sr = warp_sum(sr);
+      si = warp_sum(si);
+      const double2 tsum = cmul(t, make_double2(sr, si));
+#pragma unroll
+      for (int r = 0; r < R; r++) {
+        const int i = lane + 32 * r;
+        if (i < n) y[r] = y[r] - cmul(vk[i], tsum);
       }
     }
-    sr = warp_sum(sr);
-    si = warp_sum(si);
-    const double2 ts = cmul(t, make_double2(sr, si));
-#pragma unroll
-    for (int r = 0; r < R; r++) {
-      const int i = lane + 32 * r;
-      if (i > k && i < n) y[r] = y[r] - cmul(vk[i], ts);
-    }
   }
+  if (!col) return;
 #pragma unroll
   for (int r = 0; r < R; r++) {
     const int i = lane + 32 * r;
@@ -677,12 +739,12 @@ __global__ void __launch_bounds__(kT1, 1)
   // M(i, j) = -(1 / L(i, i)) sum_{k=j}^{i-1} L(i, k) M(k, j).
   // Uinv = M^H: Uinv(r, c) = conj(M(c, r)) for r <= c, 0 below.
   for (int j = warp; j < n; j += nw) {
-    double2 mk[kRowsPerWarp];
+    double2 mk[kColsL];
 #pragma unroll
-    for (int q = 0; q < kRowsPerWarp; q++) mk[q] = make_double2(0.0, 0.0);
+    for (int q = 0; q < kColsL; q++) mk[q] = make_double2(0.0, 0.0);
     const double mjj = 1.0 / L[lp(j, j)].x;
 #pragma unroll
-    for (int q = 0; q < kRowsPerWarp; q++)
+    for (int q = 0; q < kColsL; q++)
       if (lane + 32 * q == j) mk[q] = make_double2(mjj, 0.0);
     if (lane == 0) Uinv[(size_t)j * ldu + j] = make_double2(mjj, 0.0);
     for (int r = lane; r < n; r += 32)
@@ -690,7 +752,7 @@ __global__ void __launch_bounds__(kT1, 1)
     for (int i = j + 1; i < n; i++) {
       double sr = 0.0, si = 0.0;
 #pragma unroll
-      for (int q = 0; q < kRowsPerWarp; q++) {
+      for (int q = 0; q < kColsL; q++) {
         const int kk = lane + 32 * q;
         if (kk >= j && kk < i) {
           const double2 a = L[lp(i, kk)], b = mk[q];
@@ -705,7 +767,7 @@ __global__ void __launch_bounds__(kT1, 1)
       const double mii = -1.0 / L[lp(i, i)].x;
       const double2 mij = make_double2(mii * sr, mii * si);
 #pragma unroll
-      for (int q = 0; q < kRowsPerWarp; q++)
+      for (int q = 0; q < kColsL; q++)
         if (lane + 32 * q == i) mk[q] = mij;
       if (lane == 0) Uinv[(size_t)i * ldu + j] = cconj(mij);
     }
@@ -739,16 +801,16 @@ int dev_heev_small(pspw_cell *c, double2 *A, int lda, double *w, int n, void *wo
   double *d = static_cast<double *>(take(sizeof(double) * n));
   double *e = static_cast<double *>(take(sizeof(double) * n));
   double *Z = static_cast<double *>(take(sizeof(double) * nn));
-  const int smem1 = (int)(sizeof(double2) * (size_t)n * (n + 1) / 2);
+  const int smem1 = (int)(sizeof(double2) * ((size_t)n * (n + 1) / 2 + (size_t)kTRW * n));
   if (smem1 > 48 * 1024) {
     const int rc = smem_allow_max(k_hetrd);
     if (rc) return rc;
   }
-  k_hetrd<<<1, kT1, smem1, st>>>(A, lda, n, d, e, V, tau);
+  k_hetrd<<<1, kTR, smem1, st>>>(A, lda, n, d, e, V, tau);
   const int wpb = 4;
   k_tri_bisect<<<(n + wpb - 1) / wpb, 32 * wpb, sizeof(double) * 3 * n, st>>>(d, e, n, w);
   k_tri_invit<<<n, kInvitThreads, 0, st>>>(d, e, w, n, Z);
-  k_back_tr<<<(n + 3) / 4, 128, 0, st>>>(V, tau, Z, n, A, lda);
+  k_back_tr<<<(n + kBTWarps - 1) / kBTWarps, 32 * kBTWarps, 0, st>>>(V, tau, Z, n, A, lda);
   c->kernel_launches += 4;
   PSPW_CUDA(cudaGetLastError());
   return PSPW_OK;

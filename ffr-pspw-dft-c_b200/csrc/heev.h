@@ -10,8 +10,9 @@
 namespace pspw {
 
 // largest order of dev_heev_small (its reduction keeps the packed lower
-// triangle, n (n+1)/2 complex values, in one block's shared memory)
-constexpr int kHeevMax = 160;
+// triangle, n (n+1)/2 complex values, and 8 partial vectors in one block's
+// shared memory)
+constexpr int kHeevMax = 150;
 // largest order of dev_tri_eigvals
 constexpr int kTriEigMax = 4096;
 
