@@ -774,8 +774,9 @@ def run_serve(args, rank, world, local_rank):
     """--workload serve: the SCF serving loop.  Jobs (isolated clusters of
     2-64 atoms of four synthetic species with Gaussian wells of depth 1-4 Ha
     and width 0.8-1.6 bohr, cubic boxes up to 24 bohr, ecutwfc 12-25 Ha,
-    ceil(0.6 * 4 * atoms) + 8 states, random start, Pulay mixing with beta 0.3
-    and a 6-step history, converged at |dETOT| <= 1e-6 Ha/atom) arrive by a
+    ceil(0.6 * 4 * atoms) + 8 states, random start, the reference's Pulay
+    mixing (warm-up beta 0.25, INPUT history), converged at |dETOT| <= 1e-6
+    Ha/atom within 200 iterations) arrive by a
     seeded Poisson process at --rate jobs/s and are submitted to the device
     server (continuous batching over --slots concurrent jobs, admission by
     HBM footprint).  Each precision form serves the same job sequence.
@@ -800,7 +801,7 @@ def run_serve(args, rank, world, local_rank):
     clocks.start()
     for name, prec in (("fp64", PREC_F64), ("mixed", PREC_F32)):
         srv = serve.Server(device=local_rank, slots=args.slots, filter_prec=prec,
-                           conv_per_atom=1e-6, max_scf_iter=100, pulay_beta=0.3, mixdim=6)
+                           conv_per_atom=1e-6, max_scf_iter=200, pulay_beta=0.0, mixdim=0)
         srv.wait(srv.submit(warm["dir"]))  # module loading, library handles
         t0 = time.perf_counter()
         ids, t_arr = [], []
@@ -845,8 +846,9 @@ def run_serve(args, rank, world, local_rank):
             "config": {"workload": f"serve: {args.jobs} cluster jobs (2-64 atoms, 4 species, "
                                    f"box 10-24 bohr, ecutwfc 12-25 Ha), Poisson arrivals at "
                                    f"{args.rate} jobs/s (seed 77), {args.slots} slots",
-                       "stop": "|dETOT| <= 1e-6 Ha/atom, at most 100 iterations",
-                       "mixing": "Pulay beta 0.3, history 6", "start": "random (IDIAG -1)",
+                       "stop": "|dETOT| <= 1e-6 Ha/atom, at most 200 iterations",
+                       "mixing": "the reference's Pulay (beta 0.25, INPUT history)",
+                       "start": "random (IDIAG -1)",
                        "parallelism": f"replica x{world}",
                        "l2": "inputs larger than L2 for the large jobs; no flush"},
             "modes": out_modes,
