@@ -39,6 +39,7 @@ struct pspw_batch {
   std::vector<cudaEvent_t> join;
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t exec = nullptr;
+  long long kernels = 0;  // kernel launches in one apply (counted at capture)
 };
 
 namespace pspw {
@@ -105,6 +106,8 @@ int capture(pspw_batch *b) {
     if (rc) return rc;
   }
   for (pspw_cell *c : b->cells) PSPW_CUDA(cudaStreamSynchronize(c->stream));
+  long long before = 0;
+  for (pspw_cell *c : b->cells) before += c->kernel_launches;
   PSPW_CUDA(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeRelaxed));
   int rc = PSPW_OK;
   cudaEventRecord(b->fork, b->stream);
@@ -123,6 +126,9 @@ int capture(pspw_batch *b) {
   }
   if (e != cudaSuccess) return cuda_fail(e, "batch: stream capture");
   b->graph = g;
+  long long after = 0;
+  for (pspw_cell *c : b->cells) after += c->kernel_launches;
+  b->kernels = after - before;
   PSPW_CUDA(cudaGraphInstantiate(&b->exec, g, 0));
   return PSPW_OK;
 }
@@ -279,6 +285,12 @@ int pspw_batch_apply(pspw_batch *b) {
     if (rc) return rc;
   }
   PSPW_CUDA(cudaGraphLaunch(b->exec, b->stream));
+  return PSPW_OK;
+}
+
+int pspw_batch_kernels(pspw_batch *b, long long *kernels) {
+  if (!b || !kernels) return fail(PSPW_ERR_ARG, "batch_kernels: bad arguments");
+  *kernels = b->kernels;
   return PSPW_OK;
 }
 

@@ -119,6 +119,7 @@ SIGNATURES = {
     "pspw_batch_tune": [_vp, _i],
     "pspw_batch_schedule": [_vp, _i, _vp, _vp, _vp],
     "pspw_batch_apply": [_vp],
+    "pspw_batch_kernels": [_vp, _vp],
     "pspw_batch_stream": [_vp, _vp],
     "pspw_batch_synchronize": [_vp],
     "pspw_batch_destroy": [_vp],

@@ -88,6 +88,12 @@ class Batch:
     def apply(self):
         check(lib().pspw_batch_apply(self._h))
 
+    def kernels(self):
+        """Kernel launches one apply replays."""
+        n = C.c_longlong()
+        check(lib().pspw_batch_kernels(self._h, C.byref(n)))
+        return n.value
+
     def stream(self):
         s = C.c_void_p()
         check(lib().pspw_batch_stream(self._h, C.byref(s)))

@@ -468,6 +468,8 @@ int pspw_batch_download(pspw_batch *batch, int i, void *host_out);
 int pspw_batch_tune(pspw_batch *batch, int reps);
 int pspw_batch_schedule(pspw_batch *batch, int i, int *band_batch, int *nl_path, double *ms);
 int pspw_batch_apply(pspw_batch *batch);
+/* kernel launches one apply replays (0 before the first apply) */
+int pspw_batch_kernels(pspw_batch *batch, long long *kernels);
 int pspw_batch_stream(pspw_batch *batch, void **stream);
 int pspw_batch_synchronize(pspw_batch *batch);
 int pspw_batch_destroy(pspw_batch *batch);

@@ -48,6 +48,7 @@ def test_batch_equals_cells_alone(cells, prec):
         b.upload(i, d["psi"])
     b.tune(reps=2)
     b.apply()
+    assert b.kernels() >= 4 * len(cells)  # every cell's passes are in the graph
     first = [b.download(i) for i in range(len(cells))]
     b.apply()
     second = [b.download(i) for i in range(len(cells))]
