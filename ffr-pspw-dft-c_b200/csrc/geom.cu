@@ -895,6 +895,8 @@ int pspw_system_params(pspw_system *S, pspw_scf_params *p) {
   p->idiag = in.idiag;
   p->max_diag_iter = in.user_max_diag_iter ? in.max_diag_iter : 0;
   p->filter_prec = PSPW_PREC_F64;
+  p->tmetal = in.tmetal ? 1 : 0;
+  p->ekt = in.ekt;
   return PSPW_OK;
 }
 

@@ -48,11 +48,11 @@ namespace pspw {
 namespace {
 
 constexpr int kT1 = 1024;      // threads of the reduction block
-constexpr int kMaxWarpsT1 = kT1 / 32;
 constexpr double kEps = 2.220446049250313e-16;
 constexpr int kInvitThreads = 128;
 constexpr int kInvitIters = 3;
 constexpr int kRRMax = 32;     // largest cluster with a Rayleigh-Ritz step
+constexpr int kZs = 16;        // largest cluster whose vectors stay in shared memory
 
 __device__ __forceinline__ int lp(int i, int j) { return i * (i + 1) / 2 + j; }  // j <= i
 
@@ -82,163 +82,215 @@ __device__ __forceinline__ double warp_sum(double v) {
 // A: n x n column-major (lda), only the upper triangle is read (as zheevd
 // 'U').  Out: d[n], e[n-1], reflectors V (column k holds v_k on rows
 // k+1..n-1, v_k(k+1) = 1), tau[n-1]; H_k = I - tau_k v_k v_k^H, Q = H_0 ...
-// Sum of one value per thread over the block, the same bits in every
-// thread: warp xor trees, then every warp reduces the warp sums with the
-// same tree.  `red` holds one value per warp; the leading barrier protects
-// it from the previous call's readers.
-__device__ double block_sum_fast(double v, double *red) {
-#pragma unroll
-  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
-  __syncthreads();
-  if (lane == 0) red[w] = v;
-  __syncthreads();
-  double s = lane < nw ? red[lane] : 0.0;
-#pragma unroll
-  for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
-  return s;
+constexpr int kTR = 640;                      // threads of the reduction block
+constexpr int kTRW = kTR / 32;                // its warps; the last one steers
+constexpr int kSteer = kTRW - 1;
+constexpr int kGrp = 4;                       // threads per trailing row
+constexpr int kColsL = (kHeevMax + 31) / 32;  // column entries per lane
+static_assert(kSteer * 32 / kGrp >= kHeevMax, "one row group per trailing row");
+
+__device__ __forceinline__ double2 cfma_(double2 a, double2 b, double2 c) {  // c + a b
+  c.x = fma(a.x, b.x, c.x);
+  c.x = fma(-a.y, b.y, c.x);
+  c.y = fma(a.x, b.y, c.y);
+  c.y = fma(a.y, b.x, c.y);
+  return c;
 }
 
-constexpr int kTR = 256;                      // threads of the reduction block
-constexpr int kTRW = kTR / 32;                // its warps
-constexpr int kRowsW = (kHeevMax + kTRW - 1) / kTRW;  // trailing rows per warp
-constexpr int kColsL = (kHeevMax + 31) / 32;          // trailing columns per lane
+__device__ __forceinline__ double2 cfmac_(double2 a, double2 b, double2 c) {  // c + conj(a) b
+  c.x = fma(a.x, b.x, c.x);
+  c.x = fma(a.y, b.y, c.x);
+  c.y = fma(a.x, b.y, c.y);
+  c.y = fma(-a.y, b.x, c.y);
+  return c;
+}
 
-// Householder reduction, one block of kTR threads.  Per step the trailing
-// Hermitian matrix-vector product reads each stored row once: warp w takes
-// rows k1 + w + 8 t; lane l the columns k1 + l + 32 q of those rows.  The
-// row's own sum (lower part) is reduced over the lanes, all rows of a warp
-// in one batched shuffle tree; the transposed contributions conj(L(i,j)) v_i
-// to y_j collect in the lane's registers and then in one partial vector per
-// warp, summed in warp order.
+// a - (v_i conj(w_j) + w_i conj(v_j)): one element of the rank-2 update
+__device__ __forceinline__ double2 her2_(double2 a, double2 vi, double2 wi, double2 vj,
+                                         double2 wj) {
+  a.x -= vi.x * wj.x + vi.y * wj.y + wi.x * vj.x + wi.y * vj.y;
+  a.y -= vi.y * wj.x - vi.x * wj.y + wi.y * vj.x - wi.x * vj.y;
+  return a;
+}
+
+// The steering warp's part of a step: column c of the trailing matrix,
+// updated with the reflector of step c - 1 when `upd` (v, w of that step),
+// gives d[c] and, for c < n - 1, the reflector of step c: e[c], tau[c],
+// column c of V and its copy vn in shared memory, t and the reflect flag.
+__device__ void hetrd_steer(const double2 *L, int n, int c, bool upd, const double2 *v,
+                            const double2 *w, double2 *vn, double *d, double *e, double2 *V,
+                            double2 *tau, double isa, double2 *s_t, int *s_refl) {
+  const int lane = threadIdx.x & 31;
+  double2 a[kColsL];
+  const double2 vc = upd ? v[c] : make_double2(0.0, 0.0), wc = upd ? w[c] : vc;
+  double part = 0.0;
+#pragma unroll
+  for (int q = 0; q < kColsL; q++) {
+    const int i = c + lane + 32 * q;
+    a[q] = make_double2(0.0, 0.0);
+    if (i < n) {
+      double2 x = L[lp(i, c)];
+      if (upd) x = her2_(x, v[i], w[i], vc, wc);
+      if (i == c) x.y = 0.0;
+      a[q] = x;
+      if (i >= c + 2) part += x.x * x.x + x.y * x.y;
+    }
+  }
+  if (lane == 0) d[c] = a[0].x * isa;
+  if (c >= n - 1) return;  // the last diagonal entry
+  const double xn2 = warp_sum(part);
+  double2 alpha;
+  alpha.x = __shfl_sync(0xffffffffu, a[0].x, 1);  // row c + 1
+  alpha.y = __shfl_sync(0xffffffffu, a[0].y, 1);
+  // H^H (alpha, x) = (beta, 0), beta real (every lane the same values)
+  double beta;
+  double2 t, sc = make_double2(0.0, 0.0);
+  if (xn2 == 0.0 && alpha.y == 0.0) {
+    beta = alpha.x;
+    t = make_double2(0.0, 0.0);
+  } else {
+    beta = -copysign(sqrt(alpha.x * alpha.x + alpha.y * alpha.y + xn2), alpha.x);
+    t = make_double2((beta - alpha.x) / beta, -alpha.y / beta);
+    const double2 den = make_double2(alpha.x - beta, alpha.y);  // 1 / (alpha - beta)
+    const double dd = den.x * den.x + den.y * den.y;
+    sc = make_double2(den.x / dd, -den.y / dd);
+  }
+  const bool reflect = t.x != 0.0 || t.y != 0.0;
+#pragma unroll
+  for (int q = 0; q < kColsL; q++) {
+    const int i = c + lane + 32 * q;
+    if (i > c && i < n) {
+      const double2 vi = i == c + 1 ? make_double2(1.0, 0.0)
+                                    : (reflect ? cmul(a[q], sc) : make_double2(0.0, 0.0));
+      vn[i] = vi;
+      V[(size_t)c * n + i] = vi;
+    }
+  }
+  if (lane == 0) {
+    e[c] = beta * isa;
+    tau[c] = t;
+    *s_t = t;
+    *s_refl = reflect;
+  }
+}
+
+// Householder reduction, one block of kTR threads.  Step k applies
+// H_k = I - t v v^H to the trailing matrix A22 (rows and columns k+1..n-1):
+// y = t A22 v, w = y - (1/2) t (y^H v) v, A22 -= v w^H + w v^H.
+//  - row groups: warps 0..kSteer-1 hold one trailing row i per group of
+//    kGrp threads (sub s takes the columns = s mod kGrp); the row's
+//    Hermitian product reads its stored part L(i, k+1..i) along the row and
+//    the part above the diagonal as conj(L(j, i)) down column i, so every
+//    sum is private to the group (two shuffles combine the subs);
+//  - the steering warp updates column k+1 alone, while the groups update
+//    the rest, and forms the next step's reflector from it (look-ahead):
+//    three barriers per step, and one warp evaluates the reflector.
+// All sums run in a fixed order, so results are bitwise repeatable.
 __global__ void __launch_bounds__(kTR, 1)
     k_hetrd(const double2 *__restrict__ A, int lda, int n, double *__restrict__ d,
             double *__restrict__ e, double2 *__restrict__ V, double2 *__restrict__ tau) {
-  extern __shared__ double2 L[];  // packed lower triangle, row-major; then partials
-  double2 *P = L + (size_t)n * (n + 1) / 2;  // [kTRW][n] column partials
-  __shared__ double2 v[kHeevMax], y[kHeevMax];
-  __shared__ double red[kTRW];
+  extern __shared__ double2 L[];  // packed lower triangle, row-major
+  __shared__ double2 vbuf[2][kHeevMax], w[kHeevMax], s_t[2];
+  __shared__ double red[kTRW][2];
+  __shared__ int s_refl[2];
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int g = tid / kGrp, sub = tid % kGrp;
+  // the largest |A(i,j)| sets a power-of-two scale (exact), so the sums of
+  // squares of the reflectors neither overflow nor underflow
+  double amax = 0.0;
   for (int i = warp; i < n; i += kTRW)
-    for (int j = lane; j <= i; j += 32) L[lp(i, j)] = cconj(A[j + (size_t)i * lda]);
+    for (int j = lane; j <= i; j += 32) {
+      const double2 a = A[j + (size_t)i * lda];
+      amax = fmax(amax, fmax(fabs(a.x), fabs(a.y)));
+    }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) amax = fmax(amax, __shfl_xor_sync(0xffffffffu, amax, o));
+  if (lane == 0) red[warp][0] = amax;
+  __syncthreads();
+  amax = 0.0;
+  for (int q = 0; q < kTRW; q++) amax = fmax(amax, red[q][0]);
+  const double sa = amax > 0.0 ? ldexp(1.0, -ilogb(amax)) : 1.0, isa = 1.0 / sa;
+  for (int i = warp; i < n; i += kTRW)
+    for (int j = lane; j <= i; j += 32) {
+      const double2 a = A[j + (size_t)i * lda];
+      L[lp(i, j)] = make_double2(a.x * sa, -a.y * sa);
+    }
+  __syncthreads();
+  if (warp == kSteer)
+    hetrd_steer(L, n, 0, false, nullptr, nullptr, vbuf[0], d, e, V, tau, isa, &s_t[0],
+                &s_refl[0]);
   __syncthreads();
   for (int k = 0; k < n - 1; k++) {
-    const int k1 = k + 1;
-    const double2 alpha = L[lp(k1, k)];
-    double part = 0.0;
-    for (int i = k1 + 1 + tid; i < n; i += kTR) {
-      const double2 x = L[lp(i, k)];
-      part += x.x * x.x + x.y * x.y;
-    }
-    const double xn2 = block_sum_fast(part, red);
-    // the reflector: H^H (alpha, x) = (beta, 0), beta real; every thread
-    // computes the same values from the same inputs
-    double beta;
-    double2 t, sc = make_double2(0.0, 0.0);
-    if (xn2 == 0.0 && alpha.y == 0.0) {
-      beta = alpha.x;
-      t = make_double2(0.0, 0.0);
-    } else {
-      beta = -copysign(sqrt(alpha.x * alpha.x + alpha.y * alpha.y + xn2), alpha.x);
-      t = make_double2((beta - alpha.x) / beta, -alpha.y / beta);
-      const double2 den = make_double2(alpha.x - beta, alpha.y);  // 1 / (alpha - beta)
-      const double dd = den.x * den.x + den.y * den.y;
-      sc = make_double2(den.x / dd, -den.y / dd);
-    }
-    const bool reflect = t.x != 0.0 || t.y != 0.0;
-    for (int i = k1 + tid; i < n; i += kTR) {
-      const double2 vi = i == k1 ? make_double2(1.0, 0.0)
-                                 : (reflect ? cmul(L[lp(i, k)], sc) : make_double2(0.0, 0.0));
-      v[i] = vi;
-      V[(size_t)k * n + i] = vi;
-    }
-    if (tid == 0) {
-      d[k] = L[lp(k, k)].x;
-      e[k] = beta;
-      tau[k] = t;
-    }
-    __syncthreads();
-    if (!reflect) continue;  // uniform
-    // y = t * A22 v
-    double rs[kRowsW][2];
-    double2 ca[kColsL];
+    const int k1 = k + 1, m = n - k1, par = k & 1;
+    const double2 *v = vbuf[par];
+    if (s_refl[par]) {  // uniform
+      const double2 t = s_t[par];
+      const int i = k1 + g;
+      const bool row = warp != kSteer && g < m;
+      // y_i = t (A22 v)_i
+      double2 acc0 = make_double2(0.0, 0.0), acc1 = acc0, vi = acc0;
+      if (row) {
+        vi = v[i];
+        const double2 *Li = L + lp(i, 0);
+        int j = k1 + sub;
+        for (; j + kGrp <= i; j += 2 * kGrp) {
+          acc0 = cfma_(Li[j], v[j], acc0);
+          acc1 = cfma_(Li[j + kGrp], v[j + kGrp], acc1);
+        }
+        if (j <= i) acc0 = cfma_(Li[j], v[j], acc0);
+        j = i + 1 + sub;
+        int pj = lp(j, i);
+        for (; j + kGrp < n; j += 2 * kGrp) {
+          acc0 = cfmac_(L[pj], v[j], acc0);
+          const int pj1 = pj + kGrp * j + kGrp * (kGrp + 1) / 2;  // lp(j + kGrp, i)
+          acc1 = cfmac_(L[pj1], v[j + kGrp], acc1);
+          pj = pj1 + kGrp * (j + kGrp) + kGrp * (kGrp + 1) / 2;
+        }
+        if (j < n) acc0 = cfmac_(L[pj], v[j], acc0);
+      }
+      double2 acc = make_double2(acc0.x + acc1.x, acc0.y + acc1.y);
 #pragma unroll
-    for (int q = 0; q < kColsL; q++) ca[q] = make_double2(0.0, 0.0);
-#pragma unroll
-    for (int r = 0; r < kRowsW; r++) {
-      rs[r][0] = 0.0;
-      rs[r][1] = 0.0;
-      const int i = k1 + warp + kTRW * r;
-      if (i >= n) continue;
-      const double2 vi = v[i];
-      const double2 *row = L + lp(i, 0);
-#pragma unroll
-      for (int q = 0; q < kColsL; q++) {
-        const int j = k1 + lane + 32 * q;
-        if (j > i) break;
-        const double2 a = row[j], b = v[j];
-        rs[r][0] = fma(a.x, b.x, rs[r][0]);
-        rs[r][0] = fma(-a.y, b.y, rs[r][0]);
-        rs[r][1] = fma(a.x, b.y, rs[r][1]);
-        rs[r][1] = fma(a.y, b.x, rs[r][1]);
-        if (j < i) {  // conj(L(i,j)) v_i belongs to y_j
-          ca[q].x = fma(a.x, vi.x, ca[q].x);
-          ca[q].x = fma(a.y, vi.y, ca[q].x);
-          ca[q].y = fma(a.x, vi.y, ca[q].y);
-          ca[q].y = fma(-a.y, vi.x, ca[q].y);
+      for (int o = 1; o < kGrp; o <<= 1) {
+        acc.x += __shfl_xor_sync(0xffffffffu, acc.x, o);
+        acc.y += __shfl_xor_sync(0xffffffffu, acc.y, o);
+      }
+      const double2 y = cmul(t, acc);
+      double pr = 0.0, pim = 0.0;
+      if (row && sub == 0) {
+        pr = y.x * vi.x + y.y * vi.y;
+        pim = y.x * vi.y - y.y * vi.x;
+      }
+      pr = warp_sum(pr);
+      pim = warp_sum(pim);
+      if (lane == 0) {
+        red[warp][0] = pr;
+        red[warp][1] = pim;
+      }
+      __syncthreads();
+      // al = -(1/2) t (y^H v): the same tree over the warp sums in every warp
+      double yr = lane < kTRW ? red[lane][0] : 0.0, yi = lane < kTRW ? red[lane][1] : 0.0;
+      yr = warp_sum(yr);
+      yi = warp_sum(yi);
+      const double2 al = cmul(make_double2(-0.5 * t.x, -0.5 * t.y), make_double2(yr, yi));
+      const double2 wi = y + cmul(al, vi);
+      if (row && sub == 0) w[i] = wi;
+      __syncthreads();
+      // A22 -= v w^H + w v^H on rows k+2.., columns k+2..i (column k+1 is
+      // the steering warp's)
+      if (row && g > 0) {
+        double2 *Li = L + lp(i, 0);
+        for (int j = k1 + 1 + sub; j <= i; j += kGrp) {
+          double2 a = her2_(Li[j], vi, wi, v[j], w[j]);
+          if (j == i) a.y = 0.0;
+          Li[j] = a;
         }
       }
     }
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1)
-#pragma unroll
-      for (int r = 0; r < kRowsW; r++) {
-        rs[r][0] += __shfl_xor_sync(0xffffffffu, rs[r][0], o);
-        rs[r][1] += __shfl_xor_sync(0xffffffffu, rs[r][1], o);
-      }
-#pragma unroll
-    for (int q = 0; q < kColsL; q++) {
-      const int j = k1 + lane + 32 * q;
-      if (j < n) P[(size_t)warp * n + j] = ca[q];
-    }
-    if (lane == 0)
-#pragma unroll
-      for (int r = 0; r < kRowsW; r++) {
-        const int i = k1 + warp + kTRW * r;
-        if (i < n) y[i] = make_double2(rs[r][0], rs[r][1]);
-      }
-    __syncthreads();
-    double pr = 0.0, pim = 0.0;
-    for (int i = k1 + tid; i < n; i += kTR) {
-      double2 s2 = y[i];
-#pragma unroll
-      for (int w = 0; w < kTRW; w++) s2 = s2 + P[(size_t)w * n + i];
-      s2 = cmul(t, s2);
-      y[i] = s2;
-      const double2 b = v[i];
-      pr += s2.x * b.x + s2.y * b.y;
-      pim += s2.x * b.y - s2.y * b.x;
-    }
-    // al = -(1/2) t (y^H v); w = y + al v is formed where it is used
-    const double yr = block_sum_fast(pr, red);
-    const double yi = block_sum_fast(pim, red);
-    const double2 al = cmul(make_double2(-0.5 * t.x, -0.5 * t.y), make_double2(yr, yi));
-    // A22 -= v w^H + w v^H (lower part; the diagonal stays real)
-    for (int i = k1 + warp; i < n; i += kTRW) {
-      const double2 vi = v[i], wi = y[i] + cmul(al, vi);
-      double2 *row = L + lp(i, 0);
-      for (int j = k1 + lane; j <= i; j += 32) {
-        const double2 vj = v[j], wj = y[j] + cmul(al, vj);
-        double2 a = row[j];
-        a.x -= vi.x * wj.x + vi.y * wj.y + wi.x * vj.x + wi.y * vj.y;
-        a.y -= vi.y * wj.x - vi.x * wj.y + wi.y * vj.x - wi.x * vj.y;
-        if (j == i) a.y = 0.0;
-        row[j] = a;
-      }
-    }
+    if (warp == kSteer)
+      hetrd_steer(L, n, k1, s_refl[par] != 0, v, w, vbuf[par ^ 1], d, e, V, tau, isa,
+                  &s_t[par ^ 1], &s_refl[par ^ 1]);
     __syncthreads();
   }
-  if (tid == 0) d[n - 1] = L[lp(n - 1, n - 1)].x;
 }
 
 // ---------------------------------------------------------------- 2 bisection
@@ -371,51 +423,60 @@ __device__ void tri_factor(const double *d, const double *e, int n, double s, do
     const double s0 = e[i], s1 = d[i + 1] - s, s2 = i + 2 < n ? e[i + 1] : 0.0;
     if (fabs(c0) >= fabs(s0)) {
       if (fabs(c0) < floor_) c0 = c0 >= 0.0 ? floor_ : -floor_;
-      const double m = s0 / c0;
-      f.u0[i] = 1.0 / c0;
+      const double r = 1.0 / c0, m = s0 * r;
+      f.u0[i] = r;
       f.u1[i] = c1;
       f.u2[i] = c2;
       f.ml[i] = m;
       f.pv[i] = 0;
       c0 = s1 - m * c1;
       c1 = s2 - m * c2;
-      c2 = 0.0;
     } else {
-      const double m = c0 / s0;
-      f.u0[i] = 1.0 / s0;
+      const double r = 1.0 / s0, m = c0 * r;
+      f.u0[i] = r;
       f.u1[i] = s1;
       f.u2[i] = s2;
       f.ml[i] = m;
       f.pv[i] = 1;
       c0 = c1 - m * s1;
       c1 = c2 - m * s2;
-      c2 = 0.0;
     }
+    c2 = 0.0;
   }
   if (fabs(c0) < floor_) c0 = c0 >= 0.0 ? floor_ : -floor_;
   f.u0[n - 1] = 1.0 / c0;
 }
 
-// z <- (T - s I)^-1 z, scaled to avoid overflow (z: a thread-local copy)
+// z <- (T - s I)^-1 z, scaled to avoid overflow.  The recurrences carry
+// their last values in registers; loads of z and of the factors do not
+// depend on them.
 __device__ void tri_solve(const TriLU &f, int n, double *z) {
+  double zi = z[0];
   for (int i = 0; i < n - 1; i++) {
+    double zn = z[i + 1];
     if (f.pv[i]) {
-      const double t = z[i];
-      z[i] = z[i + 1];
-      z[i + 1] = t;
+      const double t = zi;
+      zi = zn;
+      zn = t;
     }
-    z[i + 1] = fma(-f.ml[i], z[i], z[i + 1]);
+    z[i] = zi;
+    zi = fma(-f.ml[i], zi, zn);
   }
-  double scale = 1.0;
+  z[n - 1] = zi;
+  double scale = 1.0, z1 = 0.0, z2 = 0.0;  // z[i + 1], z[i + 2]
   for (int i = n - 1; i >= 0; i--) {
     double s = z[i] * scale;
-    if (i + 1 < n) s = fma(-f.u1[i], z[i + 1], s);
-    if (i + 2 < n) s = fma(-f.u2[i], z[i + 2], s);
+    s = fma(-f.u1[i], z1, s);
+    s = fma(-f.u2[i], z2, s);
     s *= f.u0[i];
     z[i] = s;
+    z2 = z1;
+    z1 = s;
     if (fabs(s) > 0x1p+600) {  // rescale what is done; the rest of the
       for (int r = i; r < n; r++) z[r] *= 0x1p-600;  // right-hand side follows
       scale *= 0x1p-600;
+      z1 *= 0x1p-600;
+      z2 *= 0x1p-600;
     }
   }
 }
@@ -428,49 +489,35 @@ __device__ __forceinline__ double start_value(int i, int col) {
   return (double)(h & 0xffffu) * (1.0 / 65536.0) - 0.5 + 1e-3;
 }
 
-// One block per eigenvalue index j; the block of a cluster's first index
-// computes the cluster's vectors into columns of Z (n x n, column-major).
-__global__ void __launch_bounds__(kInvitThreads)
-    k_tri_invit(const double *__restrict__ dg, const double *__restrict__ eg,
-                const double *__restrict__ lam, int n, double *__restrict__ Z) {
-  __shared__ double red[kInvitThreads / 32];
-  __shared__ double S[kRRMax * kRRMax], U[kRRMax * kRRMax];
-  __shared__ double coef[kHeevMax];
-  __shared__ double d[kHeevMax], e[kHeevMax];
-  const int j = blockIdx.x, tid = threadIdx.x;
-  double glo, ghi, tn;
-  tri_bounds(dg, eg, n, &glo, &ghi, &tn);  // every warp computes the same
-  const double gaptol = 1e-3 * tn;
-  if (j > 0 && !(lam[j] - lam[j - 1] > gaptol)) return;  // not a cluster's first index
-  int c = 1;
-  while (j + c < n && lam[j + c] - lam[j + c - 1] <= gaptol) c++;
-  double *zc = Z + (size_t)j * n;  // the cluster's c columns
-  if (tn == 0.0) {  // T = 0: the unit vectors
-    for (int r = tid; r < c * n; r += blockDim.x) zc[r] = (r % n) == j + r / n ? 1.0 : 0.0;
-    return;
-  }
+// inverse iteration, Gram-Schmidt and Rayleigh-Ritz for the cluster of
+// c eigenvalues lam[j..j+c-1]; zc: the cluster's columns (ld n)
+__device__ void invit_cluster(const double *__restrict__ dg, const double *__restrict__ eg,
+                              const double *__restrict__ lam, int n, int j, int c, double tn,
+                              double *zc, double *d, double *e, double *red, double *S, double *U,
+                              double *coef) {
+  const int tid = threadIdx.x;
+  // T and the shifts scaled by a power of two to ||T|| in [1, 2) (exact),
+  // so the solves' growth (up to 1/eps) cannot overflow for any scale of T
+  const double sc = ldexp(1.0, -ilogb(tn));
   for (int i = tid; i < n; i += blockDim.x) {
-    d[i] = dg[i];
-    e[i] = i + 1 < n ? eg[i] : 0.0;
+    d[i] = dg[i] * sc;
+    e[i] = i + 1 < n ? eg[i] * sc : 0.0;
   }
-  const double floor_ = kEps * fmax(tn, 1e-200);
+  tn *= sc;
+  const double floor_ = kEps * tn;
   for (int m = tid; m < c; m += blockDim.x)
     for (int i = 0; i < n; i++) zc[(size_t)m * n + i] = start_value(i, j + m);
   __syncthreads();
-  // each member's factorisation and its vector during a solve live in the
-  // thread's own (local, L1-cached) memory; members beyond the block size
+  // each member's factorisation lives in the thread's own (local,
+  // L1-cached) memory; members beyond the block size
   // (clusters larger than the block) are factored again for every solve
   TriLU f;
-  double zl[kHeevMax];
-  if (tid < c) tri_factor(d, e, n, lam[j + tid], floor_, f);
+  if (tid < c) tri_factor(d, e, n, lam[j + tid] * sc, floor_, f);
   for (int it = 0; it < kInvitIters; it++) {
     for (int m = tid; m < c; m += blockDim.x) {
-      if (m != tid) tri_factor(d, e, n, lam[j + m], floor_, f);
-      double *zm = zc + (size_t)m * n;
-      for (int i = 0; i < n; i++) zl[i] = zm[i];
-      tri_solve(f, n, zl);
-      for (int i = 0; i < n; i++) zm[i] = zl[i];
-      if (m != tid && tid < c) tri_factor(d, e, n, lam[j + tid], floor_, f);
+      if (m != tid) tri_factor(d, e, n, lam[j + m] * sc, floor_, f);
+      tri_solve(f, n, zc + (size_t)m * n);
+      if (m != tid && tid < c) tri_factor(d, e, n, lam[j + tid] * sc, floor_, f);
     }
     __syncthreads();
     // block Gram-Schmidt, twice per column, in column order
@@ -500,7 +547,7 @@ __global__ void __launch_bounds__(kInvitThreads)
     }
   }
   // Rayleigh-Ritz inside a cluster whose eigenvalues differ beyond rounding
-  if (c > 1 && c <= kRRMax && lam[j + c - 1] - lam[j] > 4.0 * c * floor_) {
+  if (c > 1 && c <= kRRMax && (lam[j + c - 1] - lam[j]) * sc > 4.0 * c * floor_) {
     const int warp = tid >> 5, lane = tid & 31, nw = blockDim.x >> 5;
     for (int ab = warp; ab < c * c; ab += nw) {  // S(a, b) = z_a . T z_b
       const int a = ab % c, b = ab / c;
@@ -617,6 +664,37 @@ __global__ void __launch_bounds__(kInvitThreads)
   }
 }
 
+// One block per eigenvalue index j; the block of a cluster's first index
+// computes the cluster's vectors into columns of Z (n x n, column-major),
+// in shared memory for clusters of up to kZs members (the common case),
+// else in place in Z.
+__global__ void __launch_bounds__(kInvitThreads)
+    k_tri_invit(const double *__restrict__ dg, const double *__restrict__ eg,
+                const double *__restrict__ lam, int n, double *__restrict__ Z) {
+  __shared__ double red[kInvitThreads / 32];
+  __shared__ double S[kRRMax * kRRMax], U[kRRMax * kRRMax];
+  __shared__ double coef[kHeevMax];
+  __shared__ double d[kHeevMax], e[kHeevMax];
+  const int j = blockIdx.x, tid = threadIdx.x;
+  double glo, ghi, tn;
+  tri_bounds(dg, eg, n, &glo, &ghi, &tn);  // every warp computes the same
+  const double gaptol = 1e-3 * tn;
+  if (j > 0 && !(lam[j] - lam[j - 1] > gaptol)) return;  // not a cluster's first index
+  int c = 1;
+  while (j + c < n && lam[j + c] - lam[j + c - 1] <= gaptol) c++;
+  __shared__ double zs[kZs * kHeevMax];
+  double *zc = c <= kZs ? zs : Z + (size_t)j * n;  // the cluster's c columns
+  if (tn == 0.0) {  // T = 0: the unit vectors
+    for (int r = tid; r < c * n; r += blockDim.x) zc[r] = (r % n) == j + r / n ? 1.0 : 0.0;
+  } else {
+    invit_cluster(dg, eg, lam, n, j, c, tn, zc, d, e, red, S, U, coef);
+  }
+  if (c <= kZs) {
+    __syncthreads();
+    for (int r = tid; r < c * n; r += blockDim.x) Z[(size_t)j * n + r] = zs[r];
+  }
+}
+
 // ---------------------------------------------------------------- 4 back-transform
 // column j of A <- Q z_j, one warp per column, 16 columns per block; lane l
 // holds rows l, l+32, ...  The reflectors pass through shared memory in
@@ -690,22 +768,34 @@ __global__ void __launch_bounds__(kT1, 1)
     k_chol_inv(const double2 *__restrict__ G, int ldg, int n, double2 *__restrict__ Uinv, int ldu,
                double *__restrict__ stat) {
   extern __shared__ double2 L[];
+  __shared__ double piv[2][4];  // akk, 1 / akk, sqrt(akk), 1 / sqrt(akk) by step parity
+  __shared__ double dinv[kHeevMax];
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nw = blockDim.x >> 5;
   for (int i = warp; i < n; i += nw)
     for (int j = lane; j <= i; j += 32) L[lp(i, j)] = cconj(G[j + (size_t)i * ldg]);
+  if (tid == 0) {
+    const double a = G[0].x, r = sqrt(a);
+    piv[0][0] = a;
+    piv[0][1] = 1.0 / a;
+    piv[0][2] = r;
+    piv[0][3] = 1.0 / r;
+  }
   __syncthreads();
   // right-looking Cholesky, one barrier per step: step k updates the
   // trailing triangle with the unscaled column k (L(i,k) conj(L(j,k)) /
-  // L(k,k)) and then scales column k, which no later step reads
+  // L(k,k)) and then scales column k, which no later step reads.  The
+  // thread that updates the next diagonal entry evaluates its pivot
+  // quantities once for the block.
   double dmax = 0.0, dmin = INFINITY;
   int failed = 0;
   for (int k = 0; k < n; k++) {
-    const double akk = L[lp(k, k)].x;  // every thread reads the same value
+    const int par = k & 1;
+    const double akk = piv[par][0];
     if (!(akk > 0.0)) {
       failed = k + 1;
       break;  // uniform
     }
-    const double ia = 1.0 / akk, dk = sqrt(akk);
+    const double ia = piv[par][1], dk = piv[par][2], idk = piv[par][3];
     dmax = fmax(dmax, dk);
     dmin = fmin(dmin, dk);
     for (int i = k + 1 + warp; i < n; i += nw) {
@@ -716,10 +806,16 @@ __global__ void __launch_bounds__(kT1, 1)
         a.x -= (lik.x * ljk.x + lik.y * ljk.y) * ia;
         a.y -= (lik.y * ljk.x - lik.x * ljk.y) * ia;
         L[lp(i, j)] = a;
+        if (j == k + 1 && i == j) {  // the next pivot
+          const double r = sqrt(a.x);
+          piv[par ^ 1][0] = a.x;
+          piv[par ^ 1][1] = 1.0 / a.x;
+          piv[par ^ 1][2] = r;
+          piv[par ^ 1][3] = 1.0 / r;
+        }
       }
     }
     __syncthreads();
-    const double idk = 1.0 / dk;
     for (int i = k + 1 + tid; i < n; i += blockDim.x) {
       const double2 a = L[lp(i, k)];
       L[lp(i, k)] = make_double2(a.x * idk, a.y * idk);
@@ -734,42 +830,35 @@ __global__ void __launch_bounds__(kT1, 1)
     }
     return;
   }
-  // M = L^-1 column by column, no barriers: warp w owns columns w, w + nw,
-  // ...; lane l keeps M(i, j) for i = l (mod 32) in registers, and
-  // M(i, j) = -(1 / L(i, i)) sum_{k=j}^{i-1} L(i, k) M(k, j).
+  for (int i = tid; i < n; i += blockDim.x) dinv[i] = 1.0 / L[lp(i, i)].x;
+  __syncthreads();
+  // M = L^-1 column by column, no barriers and no reductions: warp w owns
+  // columns w, w + nw, ...; lane l keeps the running sums
+  // s_i = sum_{k=j}^{i-1} L(i, k) M(k, j) of rows i = l (mod 32) in
+  // registers, M(k, j) = -(1 / L(k, k)) s_k is broadcast from its owner and
+  // added into the rows below (forward substitution by columns).
   // Uinv = M^H: Uinv(r, c) = conj(M(c, r)) for r <= c, 0 below.
   for (int j = warp; j < n; j += nw) {
-    double2 mk[kColsL];
+    double2 sacc[kColsL];
 #pragma unroll
-    for (int q = 0; q < kColsL; q++) mk[q] = make_double2(0.0, 0.0);
-    const double mjj = 1.0 / L[lp(j, j)].x;
-#pragma unroll
-    for (int q = 0; q < kColsL; q++)
-      if (lane + 32 * q == j) mk[q] = make_double2(mjj, 0.0);
-    if (lane == 0) Uinv[(size_t)j * ldu + j] = make_double2(mjj, 0.0);
+    for (int q = 0; q < kColsL; q++) sacc[q] = make_double2(0.0, 0.0);
     for (int r = lane; r < n; r += 32)
       if (r > j) Uinv[(size_t)j * ldu + r] = make_double2(0.0, 0.0);
-    for (int i = j + 1; i < n; i++) {
-      double sr = 0.0, si = 0.0;
+    for (int k = j; k < n; k++) {
+      const int qk = k >> 5;
+      double2 sk = sacc[0];
+#pragma unroll
+      for (int q = 1; q < kColsL; q++) sk = q == qk ? sacc[q] : sk;
+      sk.x = __shfl_sync(0xffffffffu, sk.x, k & 31);
+      sk.y = __shfl_sync(0xffffffffu, sk.y, k & 31);
+      const double di = dinv[k];
+      const double2 mk = k == j ? make_double2(di, 0.0) : make_double2(-di * sk.x, -di * sk.y);
+      if (lane == 0) Uinv[(size_t)k * ldu + j] = cconj(mk);
 #pragma unroll
       for (int q = 0; q < kColsL; q++) {
-        const int kk = lane + 32 * q;
-        if (kk >= j && kk < i) {
-          const double2 a = L[lp(i, kk)], b = mk[q];
-          sr = fma(a.x, b.x, sr);
-          sr = fma(-a.y, b.y, sr);
-          si = fma(a.x, b.y, si);
-          si = fma(a.y, b.x, si);
-        }
+        const int i = lane + 32 * q;
+        if (32 * q + 31 > k && i > k && i < n) sacc[q] = cfma_(L[lp(i, k)], mk, sacc[q]);
       }
-      sr = warp_sum(sr);
-      si = warp_sum(si);
-      const double mii = -1.0 / L[lp(i, i)].x;
-      const double2 mij = make_double2(mii * sr, mii * si);
-#pragma unroll
-      for (int q = 0; q < kColsL; q++)
-        if (lane + 32 * q == i) mk[q] = mij;
-      if (lane == 0) Uinv[(size_t)i * ldu + j] = cconj(mij);
     }
   }
   if (tid == 0) {
@@ -801,7 +890,7 @@ int dev_heev_small(pspw_cell *c, double2 *A, int lda, double *w, int n, void *wo
   double *d = static_cast<double *>(take(sizeof(double) * n));
   double *e = static_cast<double *>(take(sizeof(double) * n));
   double *Z = static_cast<double *>(take(sizeof(double) * nn));
-  const int smem1 = (int)(sizeof(double2) * ((size_t)n * (n + 1) / 2 + (size_t)kTRW * n));
+  const int smem1 = (int)(sizeof(double2) * ((size_t)n * (n + 1) / 2));
   if (smem1 > 48 * 1024) {
     const int rc = smem_allow_max(k_hetrd);
     if (rc) return rc;

@@ -153,6 +153,33 @@ struct DevBuf {
   }
 };
 
+// Fermi-Dirac occupations of the nx states (ascending Ritz values, Ha) at
+// the electronic temperature ekt (eV): f_i = 2 / (1 + exp((e_i - ef) / ekt))
+// with the eigenvalues in eV (AU = 2 x 13.6058), cut to 2 and 0 beyond
+// |x| = 30, and the Fermi level ef found by bisection until sum_i f_i w
+// equals nel within 1e-7 (FermiEnergy.cpp:69-107).  The reference starts
+// its bisection from the interval [-40000, 40000] eV; any bracket of the
+// spectrum gives the same level.
+void fermi_occupations(const double *eig, int nx, double nel, double w, double ekt, double *f) {
+  const double au = 2.0 * 13.6058;
+  auto fill = [&](double ef) {
+    double sum = 0.0;
+    for (int i = 0; i < nx; i++) {
+      const double x = (eig[i] * au - ef) / ekt;
+      f[i] = x <= -30.0 ? 2.0 : (x < 30.0 ? 2.0 / (1.0 + std::exp(x)) : 0.0);
+      sum += f[i] * w;
+    }
+    return sum;
+  };
+  double lo = eig[0] * au - 40.0 * ekt, hi = eig[nx - 1] * au + 40.0 * ekt;
+  for (int it = 0; it < 200; it++) {
+    const double ef = 0.5 * (lo + hi), sum = fill(ef);
+    if (std::fabs(sum - nel) < 1e-7) return;
+    if (sum > nel) hi = ef; else lo = ef;
+  }
+  fill(0.5 * (lo + hi));
+}
+
 }  // namespace
 }  // namespace pspw
 
@@ -173,6 +200,10 @@ extern "C" int pspw_cheby_scf(pspw_scf *s, const pspw_scf_params *p, const doubl
     return fail(PSPW_ERR_ARG, "cheby_scf: bad sizes");
   if (p->filter_prec != PSPW_PREC_F64 && p->filter_prec != PSPW_PREC_F32)
     return fail(PSPW_ERR_ARG, "cheby_scf: unknown filter precision");
+  if (p->tmetal && !(p->ekt > 0.0)) return fail(PSPW_ERR_ARG, "cheby_scf: TMETAL needs EKT > 0");
+  if (p->tmetal && 2.0 * nx < s->nel) return fail(PSPW_ERR_ARG, "cheby_scf: too few states");
+  // occupations: the caller's, or Fermi-Dirac ones after every Rayleigh-Ritz step
+  std::vector<double> occ(focc, focc + nx);
   // precision of the filter and of the Lanczos bounds' H*v
   const int fprec = p->filter_prec;
   const int kind = (p->imix == PSPW_MIX_KERKER || p->imix == PSPW_MIX_ANDERSON ||
@@ -253,10 +284,11 @@ extern "C" int pspw_cheby_scf(pspw_scf *s, const pspw_scf_params *p, const doubl
     double ekin = 0.0, enl = 0.0;
     cudaEvent_t e;
     timing_begin(c, kFamScfDensity, &e);
-    if ((r = eval_rho_psi_dev(c, X, ngw, ngw, nx, focc, 1.0, s->omega, rho, &ekin))) return r;
+    if (p->tmetal) fermi_occupations(evals.data(), nx, s->nel, 1.0, p->ekt, occ.data());
+    if ((r = eval_rho_psi_dev(c, X, ngw, ngw, nx, occ.data(), 1.0, s->omega, rho, &ekin))) return r;
     timing_end(c, kFamScfDensity, e);
     timing_begin(c, kFamScfEnl, &e);
-    if ((r = eval_enl_dev(c, X, ngw, ngw, nx, focc, 1.0, &enl, nullptr))) return r;
+    if ((r = eval_enl_dev(c, X, ngw, ngw, nx, occ.data(), 1.0, &enl, nullptr))) return r;
     timing_end(c, kFamScfEnl, e);
     timing_begin(c, kFamScfMixEnergy, &e);
     if ((r = mix_dev(s, it, rho, drms))) return r;

@@ -62,11 +62,12 @@ def write_input(path, fhi_name, positions, a, ecut_ry=8.0, iscf=1, idiag=0, imix
 
 
 def write_input_species(path, species, a, ecut_ry, nempty, fft_grid=None, imix=3, idiag=-1,
-                        max_scf=100, conv=None, degree=None):
+                        max_scf=100, conv=None, degree=None, ekt=None):
     """An INPUT file with several species in a cubic cell of side a (bohr):
     species = [(fhi_name, positions (n, 3) in bohr), ...], in the atoms
     block layout ReadInputFile.cpp:53-92 reads (NSP; NA per species; per
-    species the file, `LMAX LLOC`, the coordinate type and NA lines)."""
+    species the file, `LMAX LLOC`, the coordinate type and NA lines).
+    ekt (eV) adds `tmetal .true.` and `ekt` (ReadInputFile.cpp:116-125)."""
     nas = " ".join(str(len(p)) for _, p in species)
     blocks = []
     for name, pos in species:
@@ -83,5 +84,7 @@ def write_input_species(path, species, a, ecut_ry, nempty, fft_grid=None, imix=3
         txt += f"\nscf_conv_crit\n {conv:.6e}\n"
     if degree is not None:
         txt += f"\nchebypol_degree\n {degree}\n"
+    if ekt is not None:
+        txt += f"\ntmetal\n .true.\n\nekt\n {ekt}\n"
     with open(path, "w") as f:
         f.write(txt)

@@ -16,7 +16,7 @@ class ScfParams(C.Structure):
                 ("max_scf_iter", C.c_int), ("conv", C.c_double), ("imix", C.c_int),
                 ("mixdim", C.c_int), ("mix_beta", C.c_double), ("pulay_beta", C.c_double),
                 ("kerker_q0", C.c_double), ("idiag", C.c_int), ("max_diag_iter", C.c_int),
-                ("filter_prec", C.c_int)]
+                ("filter_prec", C.c_int), ("tmetal", C.c_int), ("ekt", C.c_double)]
 
 
 def _c(a, dtype):

@@ -371,6 +371,11 @@ typedef struct {
   int max_diag_iter;  /* Davidson iteration cap; 0 = the reference's default */
   int filter_prec;    /* PSPW_PREC_F64, or PSPW_PREC_F32 for the filter and the H*v
                          products of the Lanczos filter bounds (the rest FP64) */
+  int tmetal;         /* TMETAL: 0 fixed occupations (the reference's loop);
+                         1 Fermi-Dirac occupations of the Ritz values after
+                         every Rayleigh-Ritz step (FermiEnergy.cpp, which the
+                         reference reads but never calls) */
+  double ekt;         /* EKT: the electronic temperature of TMETAL, in eV */
 } pspw_scf_params;
 int pspw_cheby_scf(pspw_scf *scf, const pspw_scf_params *params, const double *focc,
                    const double *rho_start, const double *v0, double *X, double *eig,

@@ -133,9 +133,9 @@ def _check_eig(cell, a, pad=0, tol=1e-12):
     return w, v
 
 
-@pytest.mark.parametrize("n", [1, 2, 3, 17, 64, 146, 160, 161, 200])
+@pytest.mark.parametrize("n", [1, 2, 3, 17, 64, 146, 150, 151, 200])
 def test_eig_zheevd_dev_random(cell, n):
-    # n <= 160: the engine's kernels; above: cuSOLVER
+    # n <= 150: the engine's kernels; above: cuSOLVER
     rng = np.random.default_rng(n)
     m = rng.standard_normal((n, n)) + 1j * rng.standard_normal((n, n))
     a = m + m.conj().T
@@ -169,6 +169,7 @@ def test_eig_zheevd_dev_special_matrices(cell):
     t = np.diag(np.full(50, 2.0)) - np.diag(np.ones(49), 1) - np.diag(np.ones(49), -1)
     _check_eig(cell, t.astype(complex))  # already tridiagonal (reflectors with tau = 0)
     _check_eig(cell, 1e-150 * _with_spectrum(np.linspace(1, 2, 30), 4))  # tiny scale
+    _check_eig(cell, 1e150 * _with_spectrum(np.linspace(-1, 2, 30), 6))  # huge scale
 
 
 def test_eig_zheevd_dev_is_bitwise_repeatable(cell):

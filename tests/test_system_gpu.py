@@ -99,3 +99,22 @@ def test_system_cheby_scf_matches_reference_program(tmp_path, name, nat, kw):
     r1, e1 = _read_dat(os.path.join(d, "FINAL_RHO.dat")), _read_dat(os.path.join(out, "FINAL_RHO.dat"))
     assert _rel(e1, r1) < 1e-3
     S.close()
+
+
+def test_tmetal_on_a_gapped_cell_is_the_fixed_occupation_loop(tmp_path):
+    """TMETAL (Fermi-Dirac occupations of the Ritz values, the reference's
+    FermiEnergy.cpp formula) at its default EKT of 0.004 eV on the gapped Si8
+    cell: every state lies more than 30 EKT from the Fermi level, so every
+    occupation is exactly 2 or 0 and the loop is the fixed-occupation loop,
+    bit for bit.  EKT <= 0 is refused."""
+    from pspw import PspwError
+    from pspw.system import System
+    d = _case(tmp_path, "si8", max_scf=12)
+    S = System(d, device=0)
+    a = S.cheby_scf(max_scf_iter=12)
+    b = S.cheby_scf(max_scf_iter=12, tmetal=1, ekt=0.004)
+    assert a["iterations"] == b["iterations"] == len(a["hist"])
+    assert np.array_equal(a["hist"][:, :3], b["hist"][:, :3])
+    with pytest.raises(PspwError):
+        S.cheby_scf(max_scf_iter=2, tmetal=1, ekt=0.0)
+    S.close()
