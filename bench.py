@@ -497,9 +497,10 @@ def run_converge(args, rank, world, local_rank):
 
 def run_eigsolve(args, rank, world, local_rank):
     """--workload eig-si216: the block eigensolvers on the Si216 cell (96^3,
-    NGW 80725, 512 bands, fixed V_loc): davidson_cpu (2 x 512 subspace) and
-    lobpcg_cpu (Q of 3 x 512 columns, 1536 x 1536 Rayleigh-Ritz) on the
-    device, each run for `--steps` iterations from the reference's own
+    NGW 80725, 512 bands, fixed V_loc): davidson_cpu (2 x 512 subspace),
+    lobpcg_cpu (Q of 3 x 512 columns, 1536 x 1536 Rayleigh-Ritz) and the
+    opt-in lobpcg_ortho (orthonormal [X W P] basis) on the device, each run
+    for at most `--steps` iterations from the reference's own
     random start (random_col), with H*psi and the preconditioner in FP64 and
     in FP32; orthonormalisation, Gram matrices and the subspace eigensolves
     are FP64 in both.  Eigenvalues of the states both runs resolve
@@ -773,8 +774,9 @@ def run_serve(args, rank, world, local_rank):
     """--workload serve: the SCF serving loop.  Jobs (isolated clusters of
     2-64 atoms of four synthetic species with Gaussian wells of depth 1-4 Ha
     and width 0.8-1.6 bohr, cubic boxes up to 24 bohr, ecutwfc 12-25 Ha,
-    ceil(0.6 * 4 * atoms) + 8 states, random start, the reference's Pulay
-    mixing (warm-up beta 0.25, INPUT history), converged at |dETOT| <= 1e-6
+    ceil(0.6 * 4 * atoms) + 8 states, random start, the reference's Broyden
+    mixing (IMIX 4, alpha 0.25; its Pulay mixing converges few of these
+    random clusters within 200 iterations), converged at |dETOT| <= 1e-6
     Ha/atom within 200 iterations) arrive by a
     seeded Poisson process at --rate jobs/s and are submitted to the device
     server (continuous batching over --slots concurrent jobs, admission by
@@ -789,7 +791,7 @@ def run_serve(args, rank, world, local_rank):
     rng = np.random.default_rng(2028 + rank)
     species = serve.species_set(rng)
     tmp = tempfile.mkdtemp(prefix="pspw_serve_")
-    jobs = [serve.cluster_job(rng, os.path.join(tmp, f"job{k}"), species)
+    jobs = [serve.cluster_job(rng, os.path.join(tmp, f"job{k}"), species, imix=4)
             for k in range(args.jobs)]
     arrivals = serve.poisson_arrivals(np.random.default_rng(77), args.rate, args.jobs)
     warm = serve.cluster_job(np.random.default_rng(1), os.path.join(tmp, "warm"), species,
@@ -823,6 +825,10 @@ def run_serve(args, rank, world, local_rank):
             "latency_mean_s": round(float(np.mean(lat)), 4),
             "queue_mean_s": round(float(np.mean([r["t_admit"] - ta
                                                  for r, ta in zip(res, t_arr)])), 4),
+            "latency_converged_p50_s": (round(serve.percentile(
+                [x for x, cv in zip(lat, conv) if cv], 50), 4) if any(conv) else None),
+            "latency_converged_p99_s": (round(serve.percentile(
+                [x for x, cv in zip(lat, conv) if cv], 99), 4) if any(conv) else None),
             "ok": int(sum(ok)), "converged": int(sum(conv)), "jobs": len(res),
             "iterations_mean": round(float(np.mean([r["iterations"] for r in res])), 2),
             "max_concurrent": int(max(sum(1 for q in res if q["t_admit"] <= r["t_admit"] < q["t_done"])
@@ -846,7 +852,7 @@ def run_serve(args, rank, world, local_rank):
                                    f"box 10-24 bohr, ecutwfc 12-25 Ha), Poisson arrivals at "
                                    f"{args.rate} jobs/s (seed 77), {args.slots} slots",
                        "stop": "|dETOT| <= 1e-6 Ha/atom, at most 200 iterations",
-                       "mixing": "the reference's Pulay (beta 0.25, INPUT history)",
+                       "mixing": "the reference's Broyden (IMIX 4, alpha 0.25)",
                        "start": "random (IDIAG -1)",
                        "parallelism": f"replica x{world}",
                        "l2": "inputs larger than L2 for the large jobs; no flush"},
@@ -1125,7 +1131,8 @@ def main():
     ap.add_argument("--slots", type=int, default=8, help="serve: concurrent jobs")
     ap.add_argument("--cells", type=int, default=32, help="batch: cells per batch")
     ap.add_argument("--solvers", default="lobpcg,davidson",
-                    help="eig-si216: comma-separated solvers (lobpcg, davidson)")
+                    help="eig-si216: comma-separated solvers (lobpcg, davidson, "
+                         "lobpcg_ortho)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
 

@@ -78,6 +78,16 @@ __device__ __forceinline__ double warp_sum(double v) {
   return v;
 }
 
+// two warp sums with their shuffles interleaved (one tree's latency)
+__device__ __forceinline__ void warp_sum2(double &a, double &b) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    const double x = __shfl_xor_sync(0xffffffffu, a, o), y = __shfl_xor_sync(0xffffffffu, b, o);
+    a += x;
+    b += y;
+  }
+}
+
 // ---------------------------------------------------------------- 1 reduction
 // A: n x n column-major (lda), only the upper triangle is read (as zheevd
 // 'U').  Out: d[n], e[n-1], reflectors V (column k holds v_k on rows
@@ -150,10 +160,11 @@ __device__ void hetrd_steer(const double2 *L, int n, int c, bool upd, const doub
     t = make_double2(0.0, 0.0);
   } else {
     beta = -copysign(sqrt(alpha.x * alpha.x + alpha.y * alpha.y + xn2), alpha.x);
-    t = make_double2((beta - alpha.x) / beta, -alpha.y / beta);
     const double2 den = make_double2(alpha.x - beta, alpha.y);  // 1 / (alpha - beta)
     const double dd = den.x * den.x + den.y * den.y;
-    sc = make_double2(den.x / dd, -den.y / dd);
+    const double ib = 1.0 / beta, idd = 1.0 / dd;
+    t = make_double2((beta - alpha.x) * ib, -alpha.y * ib);
+    sc = make_double2(den.x * idd, -den.y * idd);
   }
   const bool reflect = t.x != 0.0 || t.y != 0.0;
 #pragma unroll
@@ -227,6 +238,8 @@ __global__ void __launch_bounds__(kTR, 1)
       const double2 t = s_t[par];
       const int i = k1 + g;
       const bool row = warp != kSteer && g < m;
+      // warps with trailing rows (uniform per warp)
+      const bool wrows = warp != kSteer && warp * (32 / kGrp) < m;
       // y_i = t (A22 v)_i
       double2 acc0 = make_double2(0.0, 0.0), acc1 = acc0, vi = acc0;
       if (row) {
@@ -248,32 +261,40 @@ __global__ void __launch_bounds__(kTR, 1)
         }
         if (j < n) acc0 = cfmac_(L[pj], v[j], acc0);
       }
-      double2 acc = make_double2(acc0.x + acc1.x, acc0.y + acc1.y);
+      double2 y = make_double2(0.0, 0.0);
+      if (wrows) {
+        double2 acc = make_double2(acc0.x + acc1.x, acc0.y + acc1.y);
 #pragma unroll
-      for (int o = 1; o < kGrp; o <<= 1) {
-        acc.x += __shfl_xor_sync(0xffffffffu, acc.x, o);
-        acc.y += __shfl_xor_sync(0xffffffffu, acc.y, o);
-      }
-      const double2 y = cmul(t, acc);
-      double pr = 0.0, pim = 0.0;
-      if (row && sub == 0) {
-        pr = y.x * vi.x + y.y * vi.y;
-        pim = y.x * vi.y - y.y * vi.x;
-      }
-      pr = warp_sum(pr);
-      pim = warp_sum(pim);
-      if (lane == 0) {
-        red[warp][0] = pr;
-        red[warp][1] = pim;
+        for (int o = 1; o < kGrp; o <<= 1) {
+          const double x = __shfl_xor_sync(0xffffffffu, acc.x, o),
+                       z = __shfl_xor_sync(0xffffffffu, acc.y, o);
+          acc.x += x;
+          acc.y += z;
+        }
+        y = cmul(t, acc);
+        double pr = 0.0, pim = 0.0;
+        if (row && sub == 0) {
+          pr = y.x * vi.x + y.y * vi.y;
+          pim = y.x * vi.y - y.y * vi.x;
+        }
+        warp_sum2(pr, pim);
+        if (lane == 0) {
+          red[warp][0] = pr;
+          red[warp][1] = pim;
+        }
       }
       __syncthreads();
-      // al = -(1/2) t (y^H v): the same tree over the warp sums in every warp
-      double yr = lane < kTRW ? red[lane][0] : 0.0, yi = lane < kTRW ? red[lane][1] : 0.0;
-      yr = warp_sum(yr);
-      yi = warp_sum(yi);
-      const double2 al = cmul(make_double2(-0.5 * t.x, -0.5 * t.y), make_double2(yr, yi));
-      const double2 wi = y + cmul(al, vi);
-      if (row && sub == 0) w[i] = wi;
+      double2 wi = make_double2(0.0, 0.0);
+      if (wrows) {
+        // al = -(1/2) t (y^H v): the same tree over the warp sums in every
+        // warp (warps without rows count zero)
+        const int nwr = min(kSteer, (m + 32 / kGrp - 1) / (32 / kGrp));
+        double yr = lane < nwr ? red[lane][0] : 0.0, yi = lane < nwr ? red[lane][1] : 0.0;
+        warp_sum2(yr, yi);
+        const double2 al = cmul(make_double2(-0.5 * t.x, -0.5 * t.y), make_double2(yr, yi));
+        wi = y + cmul(al, vi);
+        if (row && sub == 0) w[i] = wi;
+      }
       __syncthreads();
       // A22 -= v w^H + w v^H on rows k+2.., columns k+2..i (column k+1 is
       // the steering warp's)
@@ -489,12 +510,105 @@ __device__ __forceinline__ double start_value(int i, int col) {
   return (double)(h & 0xffffu) * (1.0 / 65536.0) - 0.5 + 1e-3;
 }
 
+// Eigenvector of an isolated eigenvalue s of T (d, e: scaled to ||T|| in
+// [1, 2), shared memory) from its twisted factorisation (Parlett & Dhillon,
+// "Fernando's solution to Wilkinson's problem", Linear Algebra Appl. 267,
+// 1997; Dhillon & Parlett, LAPACK's dlar1v): T - s I = L D L^T from the top
+// and U R U^T from the bottom, run at the same time by two warps,
+//   D_0 = d_0 - s,      l_i = e_i / D_i,      D_{i+1} = d_{i+1} - s - l_i e_i
+//   R_{n-1} = d_{n-1} - s, u_i = e_i / R_{i+1}, R_i = d_i - s - u_i e_i,
+// pivots below `floor_` raised to it; the twist r minimises
+// |gamma_r| = |D_r + R_r - (d_r - s)|, and z solves N_r^T z = e_r:
+// z_r = 1, z_i = -l_i z_{i+1} above r, z_{i+1} = -u_i z_i below, then z is
+// normalised.  One pass replaces inverse iteration for eigenvalues further
+// than the clustering gap from their neighbours.  wk: 4 n doubles.
+__device__ void tri_vec_twisted(const double *d, const double *e, int n, double s, double floor_,
+                                double *z, double *wk, double *red) {
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  double *D = wk, *l = wk + n, *R = wk + 2 * n, *u = wk + 3 * n;
+  if (lane == 0 && warp == 0) {
+    double p = d[0] - s;
+    for (int i = 0; i + 1 < n; i++) {
+      if (fabs(p) < floor_) p = p >= 0.0 ? floor_ : -floor_;
+      D[i] = p;
+      const double li = e[i] / p;
+      l[i] = li;
+      p = (d[i + 1] - s) - li * e[i];
+    }
+    if (fabs(p) < floor_) p = p >= 0.0 ? floor_ : -floor_;
+    D[n - 1] = p;
+  } else if (lane == 0 && warp == 1) {
+    double p = d[n - 1] - s;
+    for (int i = n - 2; i >= 0; i--) {
+      if (fabs(p) < floor_) p = p >= 0.0 ? floor_ : -floor_;
+      R[i + 1] = p;
+      const double ui = e[i] / p;
+      u[i] = ui;
+      p = (d[i] - s) - ui * e[i];
+    }
+    if (fabs(p) < floor_) p = p >= 0.0 ? floor_ : -floor_;
+    R[0] = p;
+  }
+  __syncthreads();
+  // twist index: the smallest |gamma_r|, ties to the smaller r
+  double best = INFINITY;
+  int br = 0;
+  for (int r = tid; r < n; r += blockDim.x) {
+    const double g = fabs(D[r] + R[r] - (d[r] - s));
+    if (g < best) {
+      best = g;
+      br = r;
+    }
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    const double ob = __shfl_xor_sync(0xffffffffu, best, o);
+    const int orr = __shfl_xor_sync(0xffffffffu, br, o);
+    if (ob < best || (ob == best && orr < br)) {
+      best = ob;
+      br = orr;
+    }
+  }
+  __shared__ int s_r[kInvitThreads / 32];
+  if (lane == 0) {
+    red[warp] = best;
+    s_r[warp] = br;
+  }
+  __syncthreads();
+  int r = s_r[0];
+  best = red[0];
+  for (int w = 1; w < (int)(blockDim.x >> 5); w++)
+    if (red[w] < best || (red[w] == best && s_r[w] < r)) {
+      best = red[w];
+      r = s_r[w];
+    }
+  if (lane == 0 && warp == 0) {
+    double zi = 1.0;
+    z[r] = 1.0;
+    for (int i = r - 1; i >= 0; i--) {
+      zi = -l[i] * zi;
+      z[i] = zi;
+    }
+  } else if (lane == 0 && warp == 1) {
+    double zi = 1.0;
+    for (int i = r; i + 1 < n; i++) {
+      zi = -u[i] * zi;
+      z[i + 1] = zi;
+    }
+  }
+  __syncthreads();
+  double p = 0.0;
+  for (int i = tid; i < n; i += blockDim.x) p += z[i] * z[i];
+  const double inv = 1.0 / sqrt(block_sum(p, red));
+  for (int i = tid; i < n; i += blockDim.x) z[i] *= inv;
+}
+
 // inverse iteration, Gram-Schmidt and Rayleigh-Ritz for the cluster of
 // c eigenvalues lam[j..j+c-1]; zc: the cluster's columns (ld n)
 __device__ void invit_cluster(const double *__restrict__ dg, const double *__restrict__ eg,
                               const double *__restrict__ lam, int n, int j, int c, double tn,
                               double *zc, double *d, double *e, double *red, double *S, double *U,
-                              double *coef) {
+                              double *coef, double *wk) {
   const int tid = threadIdx.x;
   // T and the shifts scaled by a power of two to ||T|| in [1, 2) (exact),
   // so the solves' growth (up to 1/eps) cannot overflow for any scale of T
@@ -505,6 +619,11 @@ __device__ void invit_cluster(const double *__restrict__ dg, const double *__res
   }
   tn *= sc;
   const double floor_ = kEps * tn;
+  if (c == 1) {  // an isolated eigenvalue: one twisted factorisation
+    __syncthreads();
+    tri_vec_twisted(d, e, n, lam[j] * sc, floor_, zc, wk, red);
+    return;
+  }
   for (int m = tid; m < c; m += blockDim.x)
     for (int i = 0; i < n; i++) zc[(size_t)m * n + i] = start_value(i, j + m);
   __syncthreads();
@@ -687,7 +806,8 @@ __global__ void __launch_bounds__(kInvitThreads)
   if (tn == 0.0) {  // T = 0: the unit vectors
     for (int r = tid; r < c * n; r += blockDim.x) zc[r] = (r % n) == j + r / n ? 1.0 : 0.0;
   } else {
-    invit_cluster(dg, eg, lam, n, j, c, tn, zc, d, e, red, S, U, coef);
+    // an isolated eigenvalue's work space: the rows of zs after its vector
+    invit_cluster(dg, eg, lam, n, j, c, tn, zc, d, e, red, S, U, coef, zs + kHeevMax);
   }
   if (c <= kZs) {
     __syncthreads();
@@ -699,7 +819,7 @@ __global__ void __launch_bounds__(kInvitThreads)
 // column j of A <- Q z_j, one warp per column, 16 columns per block; lane l
 // holds rows l, l+32, ...  The reflectors pass through shared memory in
 // chunks of kBTChunk (one barrier per chunk), shared by the block's warps.
-constexpr int kBTWarps = 16, kBTChunk = 8;
+constexpr int kBTWarps = 8, kBTChunk = 8;
 __global__ void __launch_bounds__(32 * kBTWarps) k_back_tr(const double2 *__restrict__ V,
                                                             const double2 *__restrict__ tau,
                                                             const double *__restrict__ Z, int n,
@@ -740,8 +860,7 @@ __global__ void __launch_bounds__(32 * kBTWarps) k_back_tr(const double2 *__rest
           si += a.x * y[r].y - a.y * y[r].x;
         }
       }
-      sr = warp_sum(sr);
-      si = warp_sum(si);
+      warp_sum2(sr, si);
       const double2 tsum = cmul(t, make_double2(sr, si));
 #pragma unroll
       for (int r = 0; r < R; r++) {
@@ -840,24 +959,30 @@ __global__ void __launch_bounds__(kT1, 1)
   // Uinv = M^H: Uinv(r, c) = conj(M(c, r)) for r <= c, 0 below.
   for (int j = warp; j < n; j += nw) {
     double2 sacc[kColsL];
+    int ro[kColsL];  // lp(i, 0) of the lane's rows
 #pragma unroll
-    for (int q = 0; q < kColsL; q++) sacc[q] = make_double2(0.0, 0.0);
+    for (int q = 0; q < kColsL; q++) {
+      const int i = lane + 32 * q;
+      sacc[q] = make_double2(0.0, 0.0);
+      ro[q] = i * (i + 1) / 2;
+    }
     for (int r = lane; r < n; r += 32)
       if (r > j) Uinv[(size_t)j * ldu + r] = make_double2(0.0, 0.0);
-    for (int k = j; k < n; k++) {
-      const int qk = k >> 5;
-      double2 sk = sacc[0];
+    // k in blocks of 32: the owner of row k is lane k % 32, slot kb
 #pragma unroll
-      for (int q = 1; q < kColsL; q++) sk = q == qk ? sacc[q] : sk;
-      sk.x = __shfl_sync(0xffffffffu, sk.x, k & 31);
-      sk.y = __shfl_sync(0xffffffffu, sk.y, k & 31);
-      const double di = dinv[k];
-      const double2 mk = k == j ? make_double2(di, 0.0) : make_double2(-di * sk.x, -di * sk.y);
-      if (lane == 0) Uinv[(size_t)k * ldu + j] = cconj(mk);
+    for (int kb = 0; kb < kColsL; kb++) {
+      const int ka = max(j, 32 * kb), kz = min(n, 32 * kb + 32);
+      for (int k = ka; k < kz; k++) {
+        const int kl = k & 31;
+        const double sx = __shfl_sync(0xffffffffu, sacc[kb].x, kl),
+                     sy = __shfl_sync(0xffffffffu, sacc[kb].y, kl);
+        const double di = dinv[k];
+        const double2 mk = k == j ? make_double2(di, 0.0) : make_double2(-di * sx, -di * sy);
+        if (lane == 0) Uinv[(size_t)k * ldu + j] = cconj(mk);
+        if (lane > kl && lane + 32 * kb < n) sacc[kb] = cfma_(L[ro[kb] + k], mk, sacc[kb]);
 #pragma unroll
-      for (int q = 0; q < kColsL; q++) {
-        const int i = lane + 32 * q;
-        if (32 * q + 31 > k && i > k && i < n) sacc[q] = cfma_(L[lp(i, k)], mk, sacc[q]);
+        for (int q = kb + 1; q < kColsL; q++)
+          if (lane + 32 * q < n) sacc[q] = cfma_(L[ro[q] + k], mk, sacc[q]);
       }
     }
   }

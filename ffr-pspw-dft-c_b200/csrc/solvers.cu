@@ -500,8 +500,8 @@ int lobpcg_ortho_dev(pspw_cell *c, int hprec, double *lambda_host, double2 *X, i
   return d2h(c, lambda_host, lam, sizeof(double) * nb);
 }
 
-int lanczos_dev(pspw_cell *c, double2 *v0, int ngw, int k, double *T_host, int ldT, double2 *f_out,
-                int hprec) {
+int lanczos_enqueue(pspw_cell *c, double2 *v0, int ngw, int k, int hprec, double **T_dev,
+                    double2 **f_dev) {
   double2 *V, *Hv, *f, *h, *s, *ns;
   double *T, *nf;
   int rc;
@@ -540,6 +540,17 @@ int lanczos_dev(pspw_cell *c, double2 *v0, int ngw, int k, double *T_host, int l
     c->kernel_launches += 2;
   }
   PSPW_CUDA(cudaGetLastError());
+  *T_dev = T;
+  *f_dev = f;
+  return PSPW_OK;
+}
+
+int lanczos_dev(pspw_cell *c, double2 *v0, int ngw, int k, double *T_host, int ldT, double2 *f_out,
+                int hprec) {
+  double *T;
+  double2 *f;
+  int rc;
+  if ((rc = lanczos_enqueue(c, v0, ngw, k, hprec, &T, &f))) return rc;
   if (f_out && (rc = d2d(c, f_out, f, sizeof(double2) * ngw))) return rc;
   std::vector<double> Th((size_t)k * k);
   if ((rc = d2h(c, Th.data(), T, sizeof(double) * Th.size()))) return rc;

@@ -78,7 +78,7 @@ class Server:
             pass
 
 
-def smooth_grid(n, lo=24, hi=72):
+def smooth_grid(n, lo=24, hi=128):
     """Smallest 2,3,5-smooth length >= n, clipped to [lo, hi]."""
     m = max(int(math.ceil(n)), lo)
     while True:
@@ -98,14 +98,17 @@ def species_set(rng, nsp=4):
 
 def cluster_job(rng, directory, species, natoms=None, ecut_ha=None, box=None, min_sep=2.2,
                 vacuum=6.0, natoms_range=(2, 64), ecut_range=(12.0, 25.0), box_max=24.0,
-                ekt=None):
+                ekt=None, imix=3):
     """Write one cluster job into `directory`; returns its description.
     Atoms are placed uniformly (rejection sampling, pairwise distance >=
     min_sep) in the central cube of the box, leaving `vacuum` bohr between
     periodic images; the FFT grid is the smallest 5-smooth length above
-    2 G_max L / 2 pi + 1 for ecutrho = 4 ecutwfc, clipped to 24..72.
+    2 G_max L / 2 pi + 1 for ecutrho = 4 ecutwfc, kept within 24..128 (the
+    ranges above need at most 120, so the density sphere always fits the
+    grid: a smaller grid would alias it).
     ekt (eV): Fermi-Dirac occupations at that temperature (INPUT `tmetal`,
-    `ekt`); None keeps the reference's fixed occupations."""
+    `ekt`); None keeps the reference's fixed occupations.  imix: the INPUT's
+    mixer (3 Pulay, 4 Broyden, ...)."""
     os.makedirs(directory, exist_ok=True)
     nat = int(natoms if natoms is not None else rng.integers(natoms_range[0], natoms_range[1] + 1))
     lo = max(10.0, vacuum + (nat * 12.0) ** (1.0 / 3.0))
@@ -135,7 +138,7 @@ def cluster_job(rng, directory, species, natoms=None, ecut_ha=None, box=None, mi
     nx = int(math.ceil(0.6 * nval)) + 8
     nempty = nx - (nval + 1) // 2
     write_input_species(os.path.join(directory, "INPUT"), groups, L, 2.0 * ec, nempty,
-                        fft_grid=(n, n, n), imix=3, idiag=-1, max_scf=100, conv=1e-6 * nat,
+                        fft_grid=(n, n, n), imix=imix, idiag=-1, max_scf=100, conv=1e-6 * nat,
                         ekt=ekt)
     return {"dir": directory, "natoms": nat, "box": L, "ecut_ha": ec, "grid": n, "nx": nx,
             "species": [int(k) for k in kinds]}

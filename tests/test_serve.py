@@ -12,8 +12,9 @@ def test_smooth_grid():
     assert serve.smooth_grid(49) == 50
     assert serve.smooth_grid(61) == 64
     assert serve.smooth_grid(70) == 72
-    assert serve.smooth_grid(300) == 72  # clipped
-    for n in range(24, 73):
+    assert serve.smooth_grid(109.03) == 120  # 24 bohr at 25 Ha
+    assert serve.smooth_grid(300) == 128  # clipped
+    for n in range(24, 129):
         m = serve.smooth_grid(n)
         k = m
         for p in (2, 3, 5):
