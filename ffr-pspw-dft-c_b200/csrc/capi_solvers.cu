@@ -302,11 +302,14 @@ static int solver_entry(int kind, pspw_cell *c, double *evals, double *X, int nb
       (rc = ws_reserve(c, kSlotB, sizeof(double) * (size_t)nbasis, (void **)&dp)))
     return rc;
   PSPW_CUDA(cudaMemcpyAsync(dp, prec, sizeof(double) * nbasis, cudaMemcpyHostToDevice, c->stream));
+  if (kind == 3)
+    PSPW_CUDA(cudaMemcpyAsync(dX, X, sizeof(double2) * (size_t)nbasis * nstates,
+                              cudaMemcpyHostToDevice, c->stream));
   if (kind == 1)
     rc = lobpcg_dev(c, hprec, evals, dX, nbasis, nstates, dp, nempty, max_iter, resnrm, iters);
-  else if (kind == 2)
+  else if (kind == 2 || kind == 3)
     rc = lobpcg_ortho_dev(c, hprec, evals, dX, nbasis, nstates, dp, nempty, max_iter, resnrm,
-                          iters);
+                          iters, kind == 3);
   else
     rc = davidson_dev(c, hprec, evals, dX, nbasis, nstates, dp, nempty, max_iter, resnrm, iters);
   if (rc) return rc;
@@ -333,6 +336,13 @@ int pspw_lobpcg_ortho(pspw_cell *c, double *lambda, double *X, int nbasis, int n
                       const double *prec, int nempty, int max_iter, int hprec, double *resnrm,
                       int *iters) {
   return solver_entry(2, c, lambda, X, nbasis, nstates, prec, nempty, max_iter, hprec, resnrm,
+                      iters);
+}
+
+int pspw_lobpcg_ortho_from(pspw_cell *c, double *lambda, double *X, int nbasis, int nstates,
+                           const double *prec, int nempty, int max_iter, int hprec,
+                           double *resnrm, int *iters) {
+  return solver_entry(3, c, lambda, X, nbasis, nstates, prec, nempty, max_iter, hprec, resnrm,
                       iters);
 }
 

@@ -7,30 +7,32 @@
 // synchronisation overhead at this size; here the whole problem lives in one
 // block's shared memory for the O(n^3) part, and four launches do the rest:
 //
-//  1 k_hetrd      one block of 1024 threads.  Householder reduction to real
+//  1 k_hetrd      one block of 640 threads.  Householder reduction to real
 //                 symmetric tridiagonal form T = Q^H A Q (Golub & Van Loan,
 //                 Matrix Computations, 4th ed., Alg. 8.3.1, with the complex
 //                 reflector choice that leaves the off-diagonal real).  The
 //                 lower triangle is held packed row by row in shared memory
-//                 (n (n+1)/2 complex, 206 KB at n = 160); per step the
-//                 Hermitian matrix-vector product (rows: contiguous, columns:
-//                 a gather) and the rank-2 update run warp per row.  All
-//                 reductions are fixed-order trees, so results are bitwise
-//                 repeatable.
+//                 (n (n+1)/2 complex, 181 KB at n = 150); trailing rows
+//                 belong to groups of four threads, and a steering warp
+//                 forms the next step's reflector one column ahead (see the
+//                 kernel).  All reductions are fixed-order trees, so results
+//                 are bitwise repeatable.
 //  2 k_tri_bisect eigenvalues of T by bisection on Sturm counts, one warp per
 //                 eigenvalue: the 32 lanes evaluate the count at 32 interior
 //                 points of the current interval (5 bits per round).  The
 //                 count uses the characteristic-polynomial recurrence
 //                 p_i = (d_i - x) p_{i-1} - e_{i-1}^2 p_{i-2} with exact
 //                 power-of-two rescaling, which needs no division.
-//  3 k_tri_invit  eigenvectors of T by inverse iteration, one block per
-//                 cluster of eigenvalues closer than 1e-3 ||T|| (the
-//                 clustering threshold of LAPACK's dstein): every member's
-//                 (T - lambda I) is factored once (LU with partial pivoting,
-//                 small pivots raised to eps ||T||), three solves with block
-//                 Gram-Schmidt (twice) between them, then a Rayleigh-Ritz
-//                 step inside the cluster (parallel Jacobi in one warp)
-//                 unless its eigenvalues are equal to rounding.
+//  3 k_tri_invit  eigenvectors of T, one block per cluster of eigenvalues
+//                 closer than 1e-3 ||T|| (the clustering threshold of
+//                 LAPACK's dstein).  An isolated eigenvalue takes one twisted
+//                 factorisation (tri_vec_twisted).  A cluster takes inverse
+//                 iteration: every member's (T - lambda I) is factored once
+//                 (LU with partial pivoting, small pivots raised to
+//                 eps ||T||), three solves with block Gram-Schmidt (twice)
+//                 between them, then a Rayleigh-Ritz step inside the cluster
+//                 (parallel Jacobi in one warp) unless its eigenvalues are
+//                 equal to rounding.
 //  4 k_back_tr    eigenvectors of A = Q Z, one warp per vector, reflectors
 //                 applied from the last to the first.
 #include <cuda_runtime.h>
@@ -53,6 +55,7 @@ constexpr int kInvitThreads = 128;
 constexpr int kInvitIters = 3;
 constexpr int kRRMax = 32;     // largest cluster with a Rayleigh-Ritz step
 constexpr int kZs = 16;        // largest cluster whose vectors stay in shared memory
+constexpr int kCB = 8;         // panel width of the blocked Cholesky
 
 __device__ __forceinline__ int lp(int i, int j) { return i * (i + 1) / 2 + j; }  // j <= i
 
@@ -887,64 +890,80 @@ __global__ void __launch_bounds__(kT1, 1)
     k_chol_inv(const double2 *__restrict__ G, int ldg, int n, double2 *__restrict__ Uinv, int ldu,
                double *__restrict__ stat) {
   extern __shared__ double2 L[];
-  __shared__ double piv[2][4];  // akk, 1 / akk, sqrt(akk), 1 / sqrt(akk) by step parity
   __shared__ double dinv[kHeevMax];
+  __shared__ int s_failed;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nw = blockDim.x >> 5;
   for (int i = warp; i < n; i += nw)
     for (int j = lane; j <= i; j += 32) L[lp(i, j)] = cconj(G[j + (size_t)i * ldg]);
-  if (tid == 0) {
-    const double a = G[0].x, r = sqrt(a);
-    piv[0][0] = a;
-    piv[0][1] = 1.0 / a;
-    piv[0][2] = r;
-    piv[0][3] = 1.0 / r;
-  }
+  if (tid == 0) s_failed = 0;
   __syncthreads();
-  // right-looking Cholesky, one barrier per step: step k updates the
-  // trailing triangle with the unscaled column k (L(i,k) conj(L(j,k)) /
-  // L(k,k)) and then scales column k, which no later step reads.  The
-  // thread that updates the next diagonal entry evaluates its pivot
-  // quantities once for the block.
-  double dmax = 0.0, dmin = INFINITY;
-  int failed = 0;
-  for (int k = 0; k < n; k++) {
-    const int par = k & 1;
-    const double akk = piv[par][0];
-    if (!(akk > 0.0)) {
-      failed = k + 1;
-      break;  // uniform
-    }
-    const double ia = piv[par][1], dk = piv[par][2], idk = piv[par][3];
-    dmax = fmax(dmax, dk);
-    dmin = fmin(dmin, dk);
-    for (int i = k + 1 + warp; i < n; i += nw) {
-      const double2 lik = L[lp(i, k)];
-      for (int j = k + 1 + lane; j <= i; j += 32) {
-        const double2 ljk = L[lp(j, k)];
-        double2 a = L[lp(i, j)];
-        a.x -= (lik.x * ljk.x + lik.y * ljk.y) * ia;
-        a.y -= (lik.y * ljk.x - lik.x * ljk.y) * ia;
-        L[lp(i, j)] = a;
-        if (j == k + 1 && i == j) {  // the next pivot
-          const double r = sqrt(a.x);
-          piv[par ^ 1][0] = a.x;
-          piv[par ^ 1][1] = 1.0 / a.x;
-          piv[par ^ 1][2] = r;
-          piv[par ^ 1][3] = 1.0 / r;
+  // blocked right-looking Cholesky: warp 0 factors a panel of kCB columns
+  // (warp-synchronous steps), then every warp applies the panel's rank-kCB
+  // update to the trailing triangle: two barriers per panel
+  double dmax = 0.0, dmin = INFINITY;  // kept by thread 0
+  for (int k0 = 0; k0 < n; k0 += kCB) {
+    const int k1 = min(n, k0 + kCB);
+    if (warp == 0) {
+      for (int k = k0; k < k1; k++) {
+        const double akk = L[lp(k, k)].x;
+        if (!(akk > 0.0)) {
+          if (lane == 0) s_failed = k + 1;
+          break;  // warp-uniform
         }
+        const double dk = sqrt(akk), idk = 1.0 / dk;
+        dmax = fmax(dmax, dk);
+        dmin = fmin(dmin, dk);
+        __syncwarp();
+        if (lane == 0) L[lp(k, k)] = make_double2(dk, 0.0);
+        for (int i = k + 1 + lane; i < n; i += 32) {
+          const double2 a = L[lp(i, k)];
+          L[lp(i, k)] = make_double2(a.x * idk, a.y * idk);
+        }
+        __syncwarp();
+        // the panel's later columns: L(i, j) -= L(i, k) conj(L(j, k))
+        for (int j = k + 1; j < k1; j++) {
+          const double2 ljk = L[lp(j, k)];
+          for (int i = j + lane; i < n; i += 32) {
+            const double2 lik = L[lp(i, k)];
+            double2 a = L[lp(i, j)];
+            a.x -= lik.x * ljk.x + lik.y * ljk.y;
+            a.y -= lik.y * ljk.x - lik.x * ljk.y;
+            if (i == j) a.y = 0.0;
+            L[lp(i, j)] = a;
+          }
+        }
+        __syncwarp();
       }
     }
     __syncthreads();
-    for (int i = k + 1 + tid; i < n; i += blockDim.x) {
-      const double2 a = L[lp(i, k)];
-      L[lp(i, k)] = make_double2(a.x * idk, a.y * idk);
+    if (s_failed) break;  // uniform
+    // trailing triangle: rows i >= k1 (warp per row), columns k1..i (lanes)
+    const int kb = k1 - k0;
+    for (int i = k1 + warp; i < n; i += nw) {
+      double2 li[kCB];
+      const int ri = lp(i, 0);
+#pragma unroll
+      for (int q = 0; q < kCB; q++) li[q] = q < kb ? L[ri + k0 + q] : make_double2(0.0, 0.0);
+      for (int j = k1 + lane; j <= i; j += 32) {
+        const int rj = lp(j, 0) + k0;
+        double2 a = L[ri + j];
+#pragma unroll
+        for (int q = 0; q < kCB; q++) {
+          if (q < kb) {
+            const double2 lj = L[rj + q];
+            a.x -= li[q].x * lj.x + li[q].y * lj.y;
+            a.y -= li[q].y * lj.x - li[q].x * lj.y;
+          }
+        }
+        if (j == i) a.y = 0.0;
+        L[ri + j] = a;
+      }
     }
-    if (tid == 0) L[lp(k, k)] = make_double2(dk, 0.0);
+    __syncthreads();
   }
-  __syncthreads();
-  if (failed) {
+  if (s_failed) {
     if (tid == 0) {
-      stat[0] = (double)failed;
+      stat[0] = (double)s_failed;
       stat[1] = INFINITY;
     }
     return;

@@ -320,55 +320,9 @@ extern "C" int pspw_cheby_scf(pspw_scf *s, const pspw_scf_params *p, const doubl
     iter_start = 2;
     done_iters = 1;
   }
-  std::vector<double> rT10((size_t)k * k, 0.0), tl(100);
+  std::vector<double> rT10((size_t)k * k, 0.0);
   double *dfn;
   if (!mem.get(&dfn, 1)) return fail(PSPW_ERR_OOM, "cheby_scf: device memory");
-  // The in-loop Lanczos bounds (10 steps, about 150 small launches) run the
-  // same launches on the same buffers every iteration: the first call runs
-  // eagerly (it allocates the blocks), the second is captured into a CUDA
-  // graph that later iterations replay.
-  struct GraphExec {
-    cudaGraphExec_t e = nullptr;
-    long long launches = 0;
-    ~GraphExec() {
-      if (e) cudaGraphExecDestroy(e);
-    }
-  } lz;
-  int lz_calls = 0;
-  double *lzT = nullptr;
-  auto lanczos_bounds = [&](int kl, double *fn) -> int {
-    int r;
-    if (lz.e) {
-      PSPW_CUDA(cudaGraphLaunch(lz.e, st));
-      c->kernel_launches += lz.launches;
-    } else {
-      const bool cap = lz_calls >= 1;
-      const long long before = c->kernel_launches;
-      if (cap) PSPW_CUDA(cudaStreamBeginCapture(st, cudaStreamCaptureModeRelaxed));
-      double2 *fd = nullptr;
-      r = lanczos_enqueue(c, dv0, ngw, kl, fprec, &lzT, &fd);
-      if (!r && cudaMemcpyAsync(df, fd, sizeof(double2) * ngw, cudaMemcpyDeviceToDevice, st))
-        r = fail(PSPW_ERR_CUDA, "cheby_scf: Lanczos residual copy");
-      if (!r) r = dev_coldot(c, df, ngw, df, ngw, ngw, 1, dfn);
-      if (cap) {
-        cudaGraph_t g = nullptr;
-        const cudaError_t e = cudaStreamEndCapture(st, &g);
-        if (!r && e != cudaSuccess) r = cuda_fail(e, "cheby_scf: Lanczos capture");
-        if (!r && cudaGraphInstantiate(&lz.e, g, 0) != cudaSuccess)
-          r = fail(PSPW_ERR_CUDA, "cheby_scf: Lanczos graph");
-        if (g) cudaGraphDestroy(g);
-        if (r) return r;
-        lz.launches = c->kernel_launches - before;
-        PSPW_CUDA(cudaGraphLaunch(lz.e, st));
-      } else if (r) {
-        return r;
-      }
-    }
-    lz_calls++;
-    PSPW_CUDA(cudaMemcpyAsync(tl.data(), lzT, sizeof(double) * kl * kl, cudaMemcpyDeviceToHost, st));
-    PSPW_CUDA(cudaMemcpyAsync(fn, dfn, sizeof(double), cudaMemcpyDeviceToHost, st));
-    return PSPW_OK;
-  };
   for (int it = iter_start; it <= p->max_scf_iter; it++) {
     cudaEvent_t ev;
     // filter the NX+2 block (ChebySCFLoop.cpp:285)
@@ -424,12 +378,12 @@ extern "C" int pspw_cheby_scf(pspw_scf *s, const pspw_scf_params *p, const doubl
     lb = evals[nx + 1];
     const int kl = k > 10 ? 10 : k;
     timing_begin(c, kFamScfLanczos, &ev);
+    if ((rc = lanczos_dev(c, dv0, ngw, kl, rT10.data(), k, df, fprec))) return rc;
     double fn = 0.0;
-    if ((rc = lanczos_bounds(kl, &fn))) return rc;
+    if ((rc = dev_coldot(c, df, ngw, df, ngw, ngw, 1, dfn))) return rc;
+    PSPW_CUDA(cudaMemcpyAsync(&fn, dfn, sizeof(double), cudaMemcpyDeviceToHost, st));
     timing_end(c, kFamScfLanczos, ev);
     PSPW_CUDA(cudaStreamSynchronize(st));
-    for (int jj = 0; jj < kl; jj++)
-      for (int ii = 0; ii < kl; ii++) rT10[(size_t)jj * k + ii] = tl[(size_t)jj * kl + ii];
     ub = induced_norm_mat(rT10.data(), k, kl) + std::sqrt(fn);
   }
   // results

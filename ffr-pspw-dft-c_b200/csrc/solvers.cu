@@ -372,7 +372,7 @@ int lobpcg_dev(pspw_cell *c, int hprec, double *lambda_host, double2 *X, int nba
 // 142-146, 239-262).
 int lobpcg_ortho_dev(pspw_cell *c, int hprec, double *lambda_host, double2 *X, int nbasis,
                      int nstates, const double *d_prec, int nempty, int max_iter, double *res_host,
-                     int *iters) {
+                     int *iters, bool from_x) {
   const int nb = nstates, n3 = 3 * nb;
   const size_t blk = (size_t)nbasis * nb;
   double2 *Q, *HQ, *t1, *T, *tX, *tH, *tY;
@@ -386,9 +386,13 @@ int lobpcg_ortho_dev(pspw_cell *c, int hprec, double *lambda_host, double2 *X, i
     return rc;
   double2 *Xq = Q, *W = Q + blk, *P = Q + 2 * blk;
   double2 *HXq = HQ, *HW = HQ + blk, *HP = HQ + 2 * blk;
-  std::vector<double2> X0;
-  random_start(X0, nbasis, nb);
-  if ((rc = h2d(c, Xq, X0.data(), sizeof(double2) * blk))) return rc;
+  if (from_x) {  // the caller's start block
+    if ((rc = d2d(c, Xq, X, sizeof(double2) * blk))) return rc;
+  } else {
+    std::vector<double2> X0;
+    random_start(X0, nbasis, nb);
+    if ((rc = h2d(c, Xq, X0.data(), sizeof(double2) * blk))) return rc;
+  }
   int info = 0;
   if ((rc = dev_ortho_qr(c, Xq, nbasis, nbasis, nb, &info))) return rc;
   if (info) return fail(PSPW_ERR_LAPACK, "zgeqrf/zungqr: info = " + std::to_string(info));
@@ -500,8 +504,8 @@ int lobpcg_ortho_dev(pspw_cell *c, int hprec, double *lambda_host, double2 *X, i
   return d2h(c, lambda_host, lam, sizeof(double) * nb);
 }
 
-int lanczos_enqueue(pspw_cell *c, double2 *v0, int ngw, int k, int hprec, double **T_dev,
-                    double2 **f_dev) {
+int lanczos_dev(pspw_cell *c, double2 *v0, int ngw, int k, double *T_host, int ldT, double2 *f_out,
+                int hprec) {
   double2 *V, *Hv, *f, *h, *s, *ns;
   double *T, *nf;
   int rc;
@@ -540,17 +544,6 @@ int lanczos_enqueue(pspw_cell *c, double2 *v0, int ngw, int k, int hprec, double
     c->kernel_launches += 2;
   }
   PSPW_CUDA(cudaGetLastError());
-  *T_dev = T;
-  *f_dev = f;
-  return PSPW_OK;
-}
-
-int lanczos_dev(pspw_cell *c, double2 *v0, int ngw, int k, double *T_host, int ldT, double2 *f_out,
-                int hprec) {
-  double *T;
-  double2 *f;
-  int rc;
-  if ((rc = lanczos_enqueue(c, v0, ngw, k, hprec, &T, &f))) return rc;
   if (f_out && (rc = d2d(c, f_out, f, sizeof(double2) * ngw))) return rc;
   std::vector<double> Th((size_t)k * k);
   if ((rc = d2h(c, Th.data(), T, sizeof(double) * Th.size()))) return rc;

@@ -18,18 +18,13 @@ int lobpcg_dev(pspw_cell *c, int hprec, double *lambda_host, double2 *X, int nba
 // eigenproblem (an opt-in alternative to lobpcg_dev; same start, same test).
 int lobpcg_ortho_dev(pspw_cell *c, int hprec, double *lambda_host, double2 *X, int nbasis,
                      int nstates, const double *d_prec, int nempty, int max_iter, double *res_host,
-                     int *iters);
+                     int *iters, bool from_x = false);
 // v0: device, normalised in place; T_host k x k (ldT); f_out device or null.
 // hprec: precision of the H*v products (PSPW_PREC_F64 reproduces lanczos.cpp;
 // PSPW_PREC_F32 for bounds that only shape a filter); the recurrence, the
 // reorthogonalisation and T stay FP64.
 int lanczos_dev(pspw_cell *c, double2 *v0, int ngw, int k, double *T_host, int ldT, double2 *f_out,
                 int hprec = PSPW_PREC_F64);
-// The same recurrence enqueued on the cell stream without any host
-// synchronisation or allocation once its blocks exist (capturable in a CUDA
-// graph): T (k x k, ld k) and f stay on the device, in the cell's blocks.
-int lanczos_enqueue(pspw_cell *c, double2 *v0, int ngw, int k, int hprec, double **T_dev,
-                    double2 **f_dev);
 
 // EvalRhoPsi / EvalENL on device blocks (capi_solvers.cu); see pspw_gpu.h.
 int eval_rho_psi_dev(pspw_cell *c, const double2 *dX, int ld, int ngw, int nx, const double *focc,

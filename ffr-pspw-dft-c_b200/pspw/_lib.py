@@ -81,6 +81,7 @@ SIGNATURES = {
     "pspw_davidson": [_vp, _vp, _vp, _i, _i, _vp, _i, _i, _i, _vp, _vp],
     "pspw_lobpcg": [_vp, _vp, _vp, _i, _i, _vp, _i, _i, _i, _vp, _vp],
     "pspw_lobpcg_ortho": [_vp, _vp, _vp, _i, _i, _vp, _i, _i, _i, _vp, _vp],
+    "pspw_lobpcg_ortho_from": [_vp, _vp, _vp, _i, _i, _vp, _i, _i, _i, _vp, _vp],
     "pspw_lanczos": [_vp, _vp, _i, _i, _vp, _i, _vp],
     "pspw_eval_rho_psi": [_vp, _vp, _vp, _i, _i, _i, _vp, _d, _d, _vp],
     "pspw_eval_enl": [_vp, _vp, _i, _i, _i, _vp, _d, _vp, _vp],

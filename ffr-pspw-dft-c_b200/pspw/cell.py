@@ -216,8 +216,11 @@ class Cell:
                                         E.ctypes.data, n, n))
         return w, E
 
-    def _solver(self, name, nbasis, nstates, prec, nempty, max_iter, hprec):
-        X = np.zeros((nbasis, nstates), dtype=np.complex128, order="F")
+    def _solver(self, name, nbasis, nstates, prec, nempty, max_iter, hprec, X0=None):
+        if X0 is None:
+            X = np.zeros((nbasis, nstates), dtype=np.complex128, order="F")
+        else:
+            X = np.array(np.asarray(X0, dtype=np.complex128)[:nbasis, :nstates], order="F")
         ev = np.zeros(nstates)
         res = np.zeros(nstates)
         it = C.c_int()
@@ -233,9 +236,16 @@ class Cell:
     def lobpcg(self, nbasis, nstates, prec, nempty, max_iter=None, hprec=PREC_F64):
         return self._solver("pspw_lobpcg", nbasis, nstates, prec, nempty, max_iter, hprec)
 
-    def lobpcg_ortho(self, nbasis, nstates, prec, nempty, max_iter=None, hprec=PREC_F64):
-        """LOBPCG with an orthonormal [X W P] basis (opt-in, see pspw_gpu.h)."""
-        return self._solver("pspw_lobpcg_ortho", nbasis, nstates, prec, nempty, max_iter, hprec)
+    def lobpcg_ortho(self, nbasis, nstates, prec, nempty, max_iter=None, hprec=PREC_F64,
+                     X0=None):
+        """LOBPCG with an orthonormal [X W P] basis (opt-in, see pspw_gpu.h),
+        from the reference's random start, or from the block X0
+        (nbasis x nstates) when given."""
+        if X0 is None:
+            return self._solver("pspw_lobpcg_ortho", nbasis, nstates, prec, nempty, max_iter,
+                                hprec)
+        return self._solver("pspw_lobpcg_ortho_from", nbasis, nstates, prec, nempty, max_iter,
+                            hprec, X0)
 
     def lanczos(self, v0, k):
         v = np.array(np.asarray(v0, dtype=np.complex128), copy=True)

@@ -222,6 +222,12 @@ int pspw_lobpcg(pspw_cell *cell, double *lambda, double *X, int nbasis, int nsta
 int pspw_lobpcg_ortho(pspw_cell *cell, double *lambda, double *X, int nbasis, int nstates,
                       const double *prec, int nempty, int max_iter, int hprec, double *resnrm,
                       int *iters);
+/* The same solver started from the caller's block: X (host, nbasis x
+ * nstates) is read as the start (orthonormalised first) and overwritten
+ * with the result. */
+int pspw_lobpcg_ortho_from(pspw_cell *cell, double *lambda, double *X, int nbasis, int nstates,
+                           const double *prec, int nempty, int max_iter, int hprec,
+                           double *resnrm, int *iters);
 int pspw_lanczos(pspw_cell *cell, double *v0, int ngw, int k, double *T, int ldT, double *f);
 int pspw_eval_rho_psi(pspw_cell *cell, double *rhoe, const double *eigvec, int ld, int ngw,
                       int nx, const double *focc, double wkpt, double omega, double *ekin);
@@ -259,19 +265,20 @@ int pspw_zgemm_dev(pspw_cell *cell, char opa, int m, int n, int k, const double 
                    double *d_C, int ldc);
 /* eig_zheevd_dev  eig_zheevd.cpp:5-34 on device pointers: A (n x n, lda,
  *             upper triangle read) <- orthonormal eigenvectors, w[n] (device)
- *             <- eigenvalues ascending.  n <= 160 (the Rayleigh-Ritz matrix
+ *             <- eigenvalues ascending.  n <= 150 (the Rayleigh-Ritz matrix
  *             of the Chebyshev SCF loop is (NX+2) x (NX+2)) runs on the
  *             engine's own kernels: Householder tridiagonalisation in one
- *             block's shared memory, bisection, inverse iteration; larger n
- *             on cuSOLVER zheevd.  Bitwise repeatable. */
+ *             block's shared memory, bisection, twisted factorisations
+ *             (inverse iteration for clusters); larger n on cuSOLVER
+ *             zheevd.  Bitwise repeatable. */
 int pspw_eig_zheevd_dev(pspw_cell *cell, double *d_A, int lda, double *d_w, int n);
 /* ortho_span_dev  an orthonormal basis of span(X) in place, the step that
  *             ortho_qr performs in the Chebyshev SCF loop
  *             (ChebySCFLoop.cpp:288-291): columns scaled to unit norm, then
  *             CholeskyQR2 (Gram matrices and products by U^-1 on the DMMA
- *             GEMM, Cholesky factor and inverse in one block) for n <= 160,
+ *             GEMM, Cholesky factor and inverse in one block) for n <= 150,
  *             the Householder QR when the first Cholesky factor shows
- *             cond(X) above 1e6 or n > 160.  X: device, ngw x n, ld ngw.
+ *             cond(X) above 1e6 or n > 150.  X: device, ngw x n, ld ngw.
  *             The basis spans the same space as ortho_qr's and Rayleigh-Ritz
  *             gives the same Ritz pairs; the columns themselves differ. */
 int pspw_ortho_span_dev(pspw_cell *cell, double *d_X, int ngw, int n);

@@ -191,6 +191,11 @@ def test_lobpcg_ortho_converges_to_the_same_eigenvalues(si8_12ry):
     ok = res < 1e-6
     assert np.abs(ev[ok] - exact[ok]).max() < 1e-9
     assert np.abs(X.conj().T @ X - np.eye(12)).max() < 1e-12
+    # started from its own result (pspw_lobpcg_ortho_from) the solver
+    # passes the convergence test at once, on the same eigenvalues
+    evw, _, resw, itw = cell.lobpcg_ortho(ngw, 12, prec, 4, max_iter=50, X0=X)
+    assert itw <= 3 and np.sort(resw)[: 12 - 4].max() < 1e-6
+    assert np.abs(evw[ok] - ev[ok]).max() < 1e-9
     ev32, _, res32, it32 = cell.lobpcg_ortho(ngw, 12, prec, 4, max_iter=300, hprec=PREC_F32)
     ok = (res < 1e-5) & (res32 < 1e-4)
     assert ok.sum() >= 8
