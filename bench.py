@@ -511,9 +511,10 @@ def cheby_start(cell, ngw, nb, torch, dev, iters=30, extra=32, degree=10, seed=1
     S = torch.zeros(m, m, dtype=torch.complex128, device=dev)
     w = torch.zeros(m, dtype=torch.float64, device=dev)
     rng = np.random.default_rng(seed)
+    # upper bound of the spectrum: largest Ritz value of a 10-step Lanczos
+    # plus the residual norm (Zhou and Saad, J. Comput. Phys. 219 (2006))
     T, f, _ = cell.lanczos(rng.standard_normal(ngw) + 1j * rng.standard_normal(ngw), 10)
-    t1 = T @ np.full(10, 1.0 / np.sqrt(10.0))
-    ub = float(t1 @ t1) + float(np.linalg.norm(f))
+    ub = float(np.linalg.eigvalsh(0.5 * (T + T.T)).max()) + float(np.linalg.norm(f))
 
     def rayleigh_ritz():
         nonlocal X

@@ -222,9 +222,16 @@ __global__ void __launch_bounds__(PlaneCfg<NX, NY>::NT) k_plane(FastGeo g, int n
 // Density accumulation (EvalRhoPsi.cpp:139-150): inverse y and x FFTs of one
 // z-plane for each band of a group, acc += w_b |psi_b(r)|^2 in FP64; the
 // group's plane goes to part[group][zpos][ypos][xpos] (permuted order).
+// the FP64 accumulator plane starts on a 16-byte boundary after the plane
+// kernel's layout (whose int table leaves it 4 bytes off for odd NX)
+template <int NX, int NY, typename T>
+constexpr size_t plane_rho_acc_off() {
+  return (plane_smem<NX, NY, T>() + 15) / 16 * 16;
+}
+
 template <int NX, int NY, typename T>
 constexpr size_t plane_rho_smem() {
-  return plane_smem<NX, NY, T>() + sizeof(double) * (size_t)NX * NY;
+  return plane_rho_acc_off<NX, NY, T>() + sizeof(double) * (size_t)NX * NY;
 }
 
 template <int NX, int NY, typename T>
@@ -240,7 +247,7 @@ __global__ void __launch_bounds__(PlaneCfg<NX, NY>::NT) k_plane_rho(
   T *wx = plane + NY * LS;
   T *wy = wx + NX;
   int *xoff = reinterpret_cast<int *>(wy + NY);
-  double *acc = reinterpret_cast<double *>(smem_raw + plane_smem<NX, NY, T>());
+  double *acc = reinterpret_cast<double *>(smem_raw + plane_rho_acc_off<NX, NY, T>());
   const int zp = blockIdx.x, grp = blockIdx.y;
   for (int t = threadIdx.x; t < NX; t += blockDim.x) wx[t] = wx_g[t];
   for (int t = threadIdx.x; t < NY; t += blockDim.x) wy[t] = wy_g[t];

@@ -136,6 +136,28 @@ def test_non_power_of_two_grids(nr):
     assert relmax(out, ref) < TOL64
 
 
+@pytest.mark.parametrize("n", [25, 27, 45])
+def test_density_on_odd_square_grids(n):
+    """EvalRhoPsi (EvalRhoPsi.cpp:83-157) on square grids of odd length,
+    where the density kernel's FP64 accumulator plane follows a table of n
+    ints in shared memory and must start on a 16-byte boundary; against the
+    oracle (1e-12 relative max-norm)."""
+    lat, pos = synth.si_diamond(1)
+    b = basis_gamma(lat, 8.0, (n, n, n), [8], [pos])
+    pkg_a, wnl = synth.kb_form_factors(b, lat)
+    b.update(pkg_a=pkg_a, wnl=wnl, lm_end=[4])
+    ngw, ngwx = b["ngw"], b["ngwx"]
+    psi = synth.wavefunctions(b, lat, 4, 9)
+    flat = np.concatenate([psi.reshape(-1, order="F"), np.zeros(ngwx, complex)])
+    focc = np.full(4, 2.0)
+    omega = float(b["omega"])
+    cell = Cell.from_arrays(b)
+    rho, ekin = cell.eval_rho_psi(np.zeros(n ** 3), flat, ngw, ngw, 4, focc, 1.0, omega)
+    ref, ek_ref, _ = O.eval_rho_psi(oracle_cell(b), flat, ngw, ngw, 4, focc, 1.0, omega, ngwx)
+    assert relmax(rho, ref) < TOL64
+    assert abs(ekin - ek_ref) < TOL64 * abs(ek_ref)
+
+
 @pytest.mark.parametrize("lm_end", [[1], [0], [3]])
 def test_projector_counts(lm_end):
     d = dict(G)
