@@ -897,9 +897,12 @@ __global__ void __launch_bounds__(kT1, 1)
     for (int j = lane; j <= i; j += 32) L[lp(i, j)] = cconj(G[j + (size_t)i * ldg]);
   if (tid == 0) s_failed = 0;
   __syncthreads();
-  // blocked right-looking Cholesky: warp 0 factors a panel of kCB columns
-  // (warp-synchronous steps), then every warp applies the panel's rank-kCB
-  // update to the trailing triangle: two barriers per panel
+  // blocked right-looking Cholesky with panels of kCB columns: warp 0
+  // factors the panel's kCB x kCB diagonal block (warp-synchronous steps),
+  // one thread per row solves the rows below it against that block, and
+  // every warp applies the panel's rank-kCB update to the trailing triangle:
+  // three barriers per panel
+  __shared__ double s_idk[kCB];
   double dmax = 0.0, dmin = INFINITY;  // kept by thread 0
   for (int k0 = 0; k0 < n; k0 += kCB) {
     const int k1 = min(n, k0 + kCB);
@@ -914,17 +917,21 @@ __global__ void __launch_bounds__(kT1, 1)
         dmax = fmax(dmax, dk);
         dmin = fmin(dmin, dk);
         __syncwarp();
-        if (lane == 0) L[lp(k, k)] = make_double2(dk, 0.0);
-        for (int i = k + 1 + lane; i < n; i += 32) {
+        if (lane == 0) {
+          L[lp(k, k)] = make_double2(dk, 0.0);
+          s_idk[k - k0] = idk;
+        }
+        if (lane < k1 - k - 1) {
+          const int i = k + 1 + lane;
           const double2 a = L[lp(i, k)];
           L[lp(i, k)] = make_double2(a.x * idk, a.y * idk);
         }
         __syncwarp();
-        // the panel's later columns: L(i, j) -= L(i, k) conj(L(j, k))
+        // the block's later columns: L(i, j) -= L(i, k) conj(L(j, k))
         for (int j = k + 1; j < k1; j++) {
-          const double2 ljk = L[lp(j, k)];
-          for (int i = j + lane; i < n; i += 32) {
-            const double2 lik = L[lp(i, k)];
+          if (lane < k1 - j) {
+            const int i = j + lane;
+            const double2 lik = L[lp(i, k)], ljk = L[lp(j, k)];
             double2 a = L[lp(i, j)];
             a.x -= lik.x * ljk.x + lik.y * ljk.y;
             a.y -= lik.y * ljk.x - lik.x * ljk.y;
@@ -937,8 +944,34 @@ __global__ void __launch_bounds__(kT1, 1)
     }
     __syncthreads();
     if (s_failed) break;  // uniform
-    // trailing triangle: rows i >= k1 (warp per row), columns k1..i (lanes)
     const int kb = k1 - k0;
+    // rows below the block: L(i, k) = (A(i, k) - sum_{p<k} L(i, p) conj(L(k, p))) / L(k, k)
+    for (int i = k1 + tid; i < n; i += blockDim.x) {
+      double2 r[kCB];
+      const int ri = lp(i, 0) + k0;
+#pragma unroll
+      for (int q = 0; q < kCB; q++) r[q] = q < kb ? L[ri + q] : make_double2(0.0, 0.0);
+#pragma unroll
+      for (int q = 0; q < kCB; q++) {
+        if (q < kb) {
+          double2 a = r[q];
+          const int rq = lp(k0 + q, 0) + k0;
+#pragma unroll
+          for (int p2 = 0; p2 < q; p2++) {
+            const double2 lq = L[rq + p2];
+            a.x -= r[p2].x * lq.x + r[p2].y * lq.y;
+            a.y -= r[p2].y * lq.x - r[p2].x * lq.y;
+          }
+          const double id = s_idk[q];
+          r[q] = make_double2(a.x * id, a.y * id);
+        }
+      }
+#pragma unroll
+      for (int q = 0; q < kCB; q++)
+        if (q < kb) L[ri + q] = r[q];
+    }
+    __syncthreads();
+    // trailing triangle: rows i >= k1 (warp per row), columns k1..i (lanes)
     for (int i = k1 + warp; i < n; i += nw) {
       double2 li[kCB];
       const int ri = lp(i, 0);
