@@ -131,7 +131,8 @@ enum WsSlot {
   kWsStickX = 36,      // the filter's block in stick order
   kWsHeev = 37,        // the small Hermitian eigensolver's workspace
   kWsSpan = 38,        // pspw_ortho_span_dev: G, U, W, norms (38..41)
-  kWsCount = 42
+  kWsChol = 42,        // the Cholesky factor handed to the triangular inverse
+  kWsCount = 43
 };
 
 struct Timing {

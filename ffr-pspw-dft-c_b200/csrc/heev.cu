@@ -819,60 +819,54 @@ __global__ void __launch_bounds__(kInvitThreads)
 }
 
 // ---------------------------------------------------------------- 4 back-transform
-// column j of A <- Q z_j, one warp per column, 16 columns per block; lane l
-// holds rows l, l+32, ...  The reflectors pass through shared memory in
-// chunks of kBTChunk (one barrier per chunk), shared by the block's warps.
-constexpr int kBTWarps = 8, kBTChunk = 8;
+// column j of A <- Q z_j, one warp per column, kBTWarps columns per block;
+// lane l holds rows l, l+32, ...  Each warp reads the reflectors straight
+// from global memory (coalesced, L2-resident), the next one loaded into
+// registers while the current one is applied.
+constexpr int kBTWarps = 2;
 __global__ void __launch_bounds__(32 * kBTWarps) k_back_tr(const double2 *__restrict__ V,
                                                             const double2 *__restrict__ tau,
                                                             const double *__restrict__ Z, int n,
                                                             double2 *__restrict__ A, int lda) {
   constexpr int R = (kHeevMax + 31) / 32;
-  __shared__ double2 vs[kBTChunk][kHeevMax];
-  __shared__ double2 ts[kBTChunk];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int j = blockIdx.x * kBTWarps + warp;
-  const bool col = j < n;
-  double2 y[R];
+  if (j >= n) return;  // whole warp
+  double2 y[R], vn[R];
 #pragma unroll
   for (int r = 0; r < R; r++) {
     const int i = lane + 32 * r;
-    y[r] = make_double2(col && i < n ? Z[(size_t)j * n + i] : 0.0, 0.0);
+    y[r] = make_double2(i < n ? Z[(size_t)j * n + i] : 0.0, 0.0);
   }
-  for (int kc = n - 2; kc >= 0; kc -= kBTChunk) {
-    const int k0 = max(0, kc - kBTChunk + 1);  // reflectors k0..kc, applied kc first
-    __syncthreads();
-    for (int e = threadIdx.x; e < (kc - k0 + 1) * n; e += blockDim.x) {
-      const int kk = e / n, i = e % n;
-      vs[kk][i] = i > k0 + kk ? V[(size_t)(k0 + kk) * n + i] : make_double2(0.0, 0.0);
-    }
-    if (threadIdx.x <= kc - k0) ts[threadIdx.x] = tau[k0 + threadIdx.x];
-    __syncthreads();
-    if (!col) continue;
-    for (int k = kc; k >= k0; k--) {
-      const double2 t = ts[k - k0];
-      if (t.x == 0.0 && t.y == 0.0) continue;
-      const double2 *vk = vs[k - k0];
-      double sr = 0.0, si = 0.0;  // s = v^H y over rows > k (zeros elsewhere)
+  // v_k holds rows > k (rows <= k read as zero); applied from k = n-2 down
+  auto load = [&](int k, double2 *v) {
 #pragma unroll
-      for (int r = 0; r < R; r++) {
-        const int i = lane + 32 * r;
-        if (i < n) {
-          const double2 a = vk[i];
-          sr += a.x * y[r].x + a.y * y[r].y;
-          si += a.x * y[r].y - a.y * y[r].x;
-        }
-      }
-      warp_sum2(sr, si);
-      const double2 tsum = cmul(t, make_double2(sr, si));
-#pragma unroll
-      for (int r = 0; r < R; r++) {
-        const int i = lane + 32 * r;
-        if (i < n) y[r] = y[r] - cmul(vk[i], tsum);
-      }
+    for (int r = 0; r < R; r++) {
+      const int i = lane + 32 * r;
+      v[r] = (k >= 0 && i > k && i < n) ? V[(size_t)k * n + i] : make_double2(0.0, 0.0);
     }
+  };
+  load(n - 2, vn);
+  double2 tn = n >= 2 ? tau[n - 2] : make_double2(0.0, 0.0);
+  for (int k = n - 2; k >= 0; k--) {
+    double2 v[R];
+#pragma unroll
+    for (int r = 0; r < R; r++) v[r] = vn[r];
+    const double2 t = tn;
+    load(k - 1, vn);
+    tn = k >= 1 ? tau[k - 1] : make_double2(0.0, 0.0);
+    if (t.x == 0.0 && t.y == 0.0) continue;  // uniform
+    double sr = 0.0, si = 0.0;  // s = v^H y
+#pragma unroll
+    for (int r = 0; r < R; r++) {
+      sr += v[r].x * y[r].x + v[r].y * y[r].y;
+      si += v[r].x * y[r].y - v[r].y * y[r].x;
+    }
+    warp_sum2(sr, si);
+    const double2 tsum = cmul(t, make_double2(sr, si));
+#pragma unroll
+    for (int r = 0; r < R; r++) y[r] = y[r] - cmul(v[r], tsum);
   }
-  if (!col) return;
 #pragma unroll
   for (int r = 0; r < R; r++) {
     const int i = lane + 32 * r;
@@ -881,16 +875,15 @@ __global__ void __launch_bounds__(32 * kBTWarps) k_back_tr(const double2 *__rest
 }
 
 // ---------------------------------------------------------------- Cholesky
-// G = U^H U (upper U) and U^-1, one block, for the CholeskyQR passes of the
-// span orthonormalisation: G (n x n, ldg, upper triangle read) -> Uinv
-// (n x n, ldu, upper, zeros below), stat[0] = 0 or k + 1 when the k-th pivot
-// is not positive, stat[1] = max |U_kk| / min |U_kk|.  Works on the lower
-// factor L = U^H, packed row-major in shared memory.
+// G = U^H U (upper U), one block, for the CholeskyQR passes of the span
+// orthonormalisation: G (n x n, ldg, upper triangle read) -> the lower factor
+// L = U^H packed row-major into Lg, stat[0] = 0 or k + 1 when the k-th pivot
+// is not positive, stat[1] = max |U_kk| / min |U_kk|.  Works on L packed in
+// shared memory; k_tri_inv then forms U^-1 on many blocks.
 __global__ void __launch_bounds__(kT1, 1)
-    k_chol_inv(const double2 *__restrict__ G, int ldg, int n, double2 *__restrict__ Uinv, int ldu,
+    k_chol_inv(const double2 *__restrict__ G, int ldg, int n, double2 *__restrict__ Lg,
                double *__restrict__ stat) {
   extern __shared__ double2 L[];
-  __shared__ double dinv[kHeevMax];
   __shared__ int s_failed;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nw = blockDim.x >> 5;
   for (int i = warp; i < n; i += nw)
@@ -927,17 +920,22 @@ __global__ void __launch_bounds__(kT1, 1)
           L[lp(i, k)] = make_double2(a.x * idk, a.y * idk);
         }
         __syncwarp();
-        // the block's later columns: L(i, j) -= L(i, k) conj(L(j, k))
-        for (int j = k + 1; j < k1; j++) {
-          if (lane < k1 - j) {
-            const int i = j + lane;
-            const double2 lik = L[lp(i, k)], ljk = L[lp(j, k)];
-            double2 a = L[lp(i, j)];
-            a.x -= lik.x * ljk.x + lik.y * ljk.y;
-            a.y -= lik.y * ljk.x - lik.x * ljk.y;
-            if (i == j) a.y = 0.0;
-            L[lp(i, j)] = a;
+        // the block's later columns, one element per lane (at most 28):
+        // L(i, j) -= L(i, k) conj(L(j, k)), k < j <= i < k1
+        const int d = k1 - k - 1;
+        if (lane < d * (d + 1) / 2) {
+          int jj = 0, rem = lane;
+          while (rem >= d - jj) {
+            rem -= d - jj;
+            jj++;
           }
+          const int j = k + 1 + jj, i = j + rem;
+          const double2 lik = L[lp(i, k)], ljk = L[lp(j, k)];
+          double2 a = L[lp(i, j)];
+          a.x -= lik.x * ljk.x + lik.y * ljk.y;
+          a.y -= lik.y * ljk.x - lik.x * ljk.y;
+          if (i == j) a.y = 0.0;
+          L[lp(i, j)] = a;
         }
         __syncwarp();
       }
@@ -1001,46 +999,65 @@ __global__ void __launch_bounds__(kT1, 1)
     }
     return;
   }
-  for (int i = tid; i < n; i += blockDim.x) dinv[i] = 1.0 / L[lp(i, i)].x;
-  __syncthreads();
-  // M = L^-1 column by column, no barriers and no reductions: warp w owns
-  // columns w, w + nw, ...; lane l keeps the running sums
-  // s_i = sum_{k=j}^{i-1} L(i, k) M(k, j) of rows i = l (mod 32) in
-  // registers, M(k, j) = -(1 / L(k, k)) s_k is broadcast from its owner and
-  // added into the rows below (forward substitution by columns).
-  // Uinv = M^H: Uinv(r, c) = conj(M(c, r)) for r <= c, 0 below.
-  for (int j = warp; j < n; j += nw) {
-    double2 sacc[kColsL];
-    int ro[kColsL];  // lp(i, 0) of the lane's rows
-#pragma unroll
-    for (int q = 0; q < kColsL; q++) {
-      const int i = lane + 32 * q;
-      sacc[q] = make_double2(0.0, 0.0);
-      ro[q] = i * (i + 1) / 2;
-    }
-    for (int r = lane; r < n; r += 32)
-      if (r > j) Uinv[(size_t)j * ldu + r] = make_double2(0.0, 0.0);
-    // k in blocks of 32: the owner of row k is lane k % 32, slot kb
-#pragma unroll
-    for (int kb = 0; kb < kColsL; kb++) {
-      const int ka = max(j, 32 * kb), kz = min(n, 32 * kb + 32);
-      for (int k = ka; k < kz; k++) {
-        const int kl = k & 31;
-        const double sx = __shfl_sync(0xffffffffu, sacc[kb].x, kl),
-                     sy = __shfl_sync(0xffffffffu, sacc[kb].y, kl);
-        const double di = dinv[k];
-        const double2 mk = k == j ? make_double2(di, 0.0) : make_double2(-di * sx, -di * sy);
-        if (lane == 0) Uinv[(size_t)k * ldu + j] = cconj(mk);
-        if (lane > kl && lane + 32 * kb < n) sacc[kb] = cfma_(L[ro[kb] + k], mk, sacc[kb]);
-#pragma unroll
-        for (int q = kb + 1; q < kColsL; q++)
-          if (lane + 32 * q < n) sacc[q] = cfma_(L[ro[q] + k], mk, sacc[q]);
-      }
-    }
-  }
+  // the factor goes to global memory for the triangular inverse
+  const int np = n * (n + 1) / 2;
+  for (int e = tid; e < np; e += blockDim.x) Lg[e] = L[e];
   if (tid == 0) {
     stat[0] = 0.0;
     stat[1] = dmax / dmin;
+  }
+}
+
+// Uinv = (L^-1)^H from the packed factor Lg, kInvWarps columns per block,
+// one warp per column: block b stages the packed rows j0..n-1 of L (j0 its
+// first column) in shared memory, then warp w forms column j = j0 + w of
+// M = L^-1 by forward substitution: lane l keeps the running sums
+// s_i = sum_{k=j}^{i-1} L(i, k) M(k, j) of rows i = l (mod 32) in registers,
+// M(k, j) = -(1 / L(k, k)) s_k is broadcast from its owner and added into
+// the rows below.  Uinv(r, c) = conj(M(c, r)) for r <= c, 0 below.  Nothing
+// is written when the factorisation failed (stat[0] != 0).
+constexpr int kInvWarps = 4;
+__global__ void __launch_bounds__(32 * kInvWarps) k_tri_inv(const double2 *__restrict__ Lg, int n,
+                                                           double2 *__restrict__ Uinv, int ldu,
+                                                           const double *__restrict__ stat) {
+  extern __shared__ double2 Ls[];  // packed rows j0..n-1
+  __shared__ double dinv[kHeevMax];
+  if (stat[0] != 0.0) return;  // uniform
+  const int j0 = blockIdx.x * kInvWarps, tid = threadIdx.x;
+  const int warp = tid >> 5, lane = tid & 31;
+  const int base = lp(j0, 0), np = n * (n + 1) / 2;
+  for (int e = tid; e < np - base; e += blockDim.x) Ls[e] = Lg[base + e];
+  __syncthreads();
+  for (int i = j0 + tid; i < n; i += blockDim.x) dinv[i] = 1.0 / Ls[lp(i, i) - base].x;
+  __syncthreads();
+  const int j = j0 + warp;
+  if (j >= n) return;  // whole warp
+  double2 sacc[kColsL];
+  int ro[kColsL];  // lp(i, 0) - base of the lane's rows
+#pragma unroll
+  for (int q = 0; q < kColsL; q++) {
+    const int i = lane + 32 * q;
+    sacc[q] = make_double2(0.0, 0.0);
+    ro[q] = i * (i + 1) / 2 - base;
+  }
+  for (int r = lane; r < n; r += 32)
+    if (r > j) Uinv[(size_t)j * ldu + r] = make_double2(0.0, 0.0);
+  // k in blocks of 32: the owner of row k is lane k % 32, slot kb
+#pragma unroll
+  for (int kb = 0; kb < kColsL; kb++) {
+    const int ka = max(j, 32 * kb), kz = min(n, 32 * kb + 32);
+    for (int k = ka; k < kz; k++) {
+      const int kl = k & 31;
+      const double sx = __shfl_sync(0xffffffffu, sacc[kb].x, kl),
+                   sy = __shfl_sync(0xffffffffu, sacc[kb].y, kl);
+      const double di = dinv[k];
+      const double2 mk = k == j ? make_double2(di, 0.0) : make_double2(-di * sx, -di * sy);
+      if (lane == 0) Uinv[(size_t)k * ldu + j] = cconj(mk);
+      if (lane > kl && lane + 32 * kb < n) sacc[kb] = cfma_(Ls[ro[kb] + k], mk, sacc[kb]);
+#pragma unroll
+      for (int q = kb + 1; q < kColsL; q++)
+        if (lane + 32 * q < n) sacc[q] = cfma_(Ls[ro[q] + k], mk, sacc[q]);
+    }
   }
 }
 
@@ -1068,7 +1085,7 @@ int dev_heev_small(pspw_cell *c, double2 *A, int lda, double *w, int n, void *wo
   double *e = static_cast<double *>(take(sizeof(double) * n));
   double *Z = static_cast<double *>(take(sizeof(double) * nn));
   const int smem1 = (int)(sizeof(double2) * ((size_t)n * (n + 1) / 2));
-  if (smem1 > 48 * 1024) {
+  {
     const int rc = smem_allow_max(k_hetrd);
     if (rc) return rc;
   }
@@ -1086,13 +1103,16 @@ int dev_chol_inv_upper(pspw_cell *c, const double2 *G, int ldg, int n, double2 *
                        double *stat) {
   if (n < 1 || n > kHeevMax || ldg < n || ldu < n)
     return fail(PSPW_ERR_ARG, "chol_inv_upper: n must be in 1.." + std::to_string(kHeevMax));
-  const int smem = (int)(sizeof(double2) * (size_t)n * (n + 1) / 2);
-  if (smem > 48 * 1024) {
-    const int rc = smem_allow_max(k_chol_inv);
-    if (rc) return rc;
-  }
-  k_chol_inv<<<1, kT1, smem, c->stream>>>(G, ldg, n, Uinv, ldu, stat);
-  c->kernel_launches++;
+  const int np = n * (n + 1) / 2;
+  const int smem = (int)(sizeof(double2) * (size_t)np);
+  double2 *Lg = nullptr;
+  int rc;
+  if ((rc = ws_reserve(c, kWsChol, sizeof(double2) * (size_t)np, (void **)&Lg))) return rc;
+  if ((rc = smem_allow_max(k_chol_inv)) || (rc = smem_allow_max(k_tri_inv))) return rc;
+  k_chol_inv<<<1, kT1, smem, c->stream>>>(G, ldg, n, Lg, stat);
+  k_tri_inv<<<(n + kInvWarps - 1) / kInvWarps, 32 * kInvWarps, smem, c->stream>>>(Lg, n, Uinv,
+                                                                               ldu, stat);
+  c->kernel_launches += 2;
   PSPW_CUDA(cudaGetLastError());
   return PSPW_OK;
 }
