@@ -95,6 +95,47 @@ def test_noalloc_generic_fft_grid_twice(prec, dtype, tol):
         assert relmax(got, expect) < tol, f"call {call}"
 
 
+@pytest.mark.parametrize("prec,dtype,tol", [(PREC_F64, torch.complex128, 1e-12),
+                                            (PREC_F32, torch.complex64, 2e-5)])
+def test_noalloc_call_captured_in_a_cuda_graph(si8, prec, dtype, tol):
+    """The entry point recorded into a CUDA graph on the cell stream (relaxed
+    capture mode) after one eager warm-up call; the graph replayed twice
+    gives the eager result both times."""
+    rt = C.CDLL("libcudart.so.12")  # the runtime the library is linked with
+    w, cell = si8
+    psi = w["psi"]
+    ngw, nb = psi.shape
+    d_in = torch.from_numpy(np.ascontiguousarray(psi.T)).to(dtype).cuda()
+    ref = torch.zeros_like(d_in)
+    out = torch.zeros_like(d_in)
+    torch.cuda.synchronize()
+    _alloc(cell, d_in, ref, ngw, ngw, nb, prec)
+    _noalloc(cell, d_in, out, ngw, ngw, nb, prec)  # warm-up
+    check(lib().pspw_cell_synchronize(cell.handle))
+    expect = ref.cpu().numpy()
+    st = C.c_void_p(cell.stream())
+    graph, gexec = C.c_void_p(), C.c_void_p()
+    assert rt.cudaStreamBeginCapture(st, 2) == 0  # cudaStreamCaptureModeRelaxed
+    try:
+        _noalloc(cell, d_in, out, ngw, ngw, nb, prec)
+    finally:
+        end = rt.cudaStreamEndCapture(st, C.byref(graph))
+    assert end == 0
+    assert rt.cudaGraphInstantiate(C.byref(gexec), graph, C.c_ulonglong(0)) == 0
+    try:
+        for rep in range(2):
+            out.fill_(float("nan"))
+            torch.cuda.synchronize()
+            assert rt.cudaGraphLaunch(gexec, st) == 0
+            assert rt.cudaStreamSynchronize(st) == 0
+            got = out.cpu().numpy()
+            assert np.all(np.isfinite(got)), f"replay {rep}"
+            assert relmax(got, expect) < tol, f"replay {rep}"
+    finally:
+        rt.cudaGraphExecDestroy(gexec)
+        rt.cudaGraphDestroy(graph)
+
+
 def test_noalloc_second_call_leaves_free_memory_unchanged(si8):
     w, cell = si8
     psi = w["psi"][:, :5]
