@@ -49,7 +49,7 @@
 namespace pspw {
 namespace {
 
-constexpr int kT1 = 1024;      // threads of the reduction block
+constexpr int kT1 = 1024;      // threads of the Cholesky block
 constexpr double kEps = 2.220446049250313e-16;
 constexpr int kInvitThreads = 128;
 constexpr int kInvitIters = 3;
