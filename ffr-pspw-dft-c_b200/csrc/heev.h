@@ -9,8 +9,8 @@
 
 namespace pspw {
 
-// largest order of dev_heev_small (its reduction keeps the packed lower
-// triangle, n (n+1)/2 complex values, and 8 partial vectors in one block's
+// largest order of dev_heev_small and dev_chol_inv_upper (their one-block
+// kernels keep the packed lower triangle, n (n+1)/2 complex values, in
 // shared memory)
 constexpr int kHeevMax = 150;
 // largest order of dev_tri_eigvals
@@ -27,7 +27,9 @@ int dev_heev_small(pspw_cell *c, double2 *A, int lda, double *w, int n, void *wo
 // Cholesky factor and its inverse for CholeskyQR: G (n x n, ldg, upper
 // triangle read) = U^H U; Uinv (n x n, ldu) <- U^-1 (upper, zeros below);
 // stat[0] (device) <- 0, or k + 1 if the k-th pivot is not positive;
-// stat[1] <- max |U_kk| / min |U_kk|.  n <= kHeevMax, one block.
+// stat[1] <- max |U_kk| / min |U_kk|.  n <= kHeevMax: the factor in one
+// block, the inverse on ceil(n / 4) blocks (one warp per column); Uinv is
+// left untouched when the factorisation fails.
 int dev_chol_inv_upper(pspw_cell *c, const double2 *G, int ldg, int n, double2 *Uinv, int ldu,
                        double *stat);
 
