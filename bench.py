@@ -885,6 +885,7 @@ def run_serve(args, rank, world, local_rank):
             "latency_converged_p99_s": (round(serve.percentile(
                 [x for x, cv in zip(lat, conv) if cv], 99), 4) if any(conv) else None),
             "ok": int(sum(ok)), "converged": int(sum(conv)), "jobs": len(res),
+            "errors": sorted({r["error"] for r in res if r["status"] != 0}),
             "iterations_mean": round(float(np.mean([r["iterations"] for r in res])), 2),
             "max_concurrent": int(max(sum(1 for q in res if q["t_admit"] <= r["t_admit"] < q["t_done"])
                                       for r in res)),

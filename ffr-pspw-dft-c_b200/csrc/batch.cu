@@ -208,6 +208,9 @@ int pspw_batch_upload(pspw_batch *b, int i, const void *host_in) {
   const size_t sc = b->prec == PSPW_PREC_F64 ? sizeof(double2) : sizeof(float2);
   PSPW_CUDA(cudaMemcpy(b->in[i], host_in, sc * (size_t)b->cells[i]->basis.ngw * b->nb[i],
                        cudaMemcpyHostToDevice));
+  // the copy from pageable memory may return before its DMA lands; the
+  // batch stream is non-blocking, so the legacy stream is synchronised here
+  PSPW_CUDA(cudaStreamSynchronize(cudaStreamLegacy));
   return PSPW_OK;
 }
 

@@ -138,10 +138,17 @@ int factor_radices(int n, int *rad, int *nf) {
   return PSPW_OK;
 }
 
+// A synchronous copy from pageable host memory returns once the data is
+// staged, before its DMA has landed, and the engine's streams are
+// non-blocking (not ordered after the legacy stream that copy runs on): the
+// legacy stream is synchronised before any kernel may read the table.
 template <typename T>
 int upload(T **d, const std::vector<T> &h) {
   PSPW_CUDA(cudaMalloc((void **)d, std::max<size_t>(1, h.size()) * sizeof(T)));
-  if (!h.empty()) PSPW_CUDA(cudaMemcpy(*d, h.data(), h.size() * sizeof(T), cudaMemcpyHostToDevice));
+  if (!h.empty()) {
+    PSPW_CUDA(cudaMemcpy(*d, h.data(), h.size() * sizeof(T), cudaMemcpyHostToDevice));
+    PSPW_CUDA(cudaStreamSynchronize(cudaStreamLegacy));
+  }
   return PSPW_OK;
 }
 

@@ -66,10 +66,15 @@ int read_info(pspw_cell *c, const int *d_info, int *info_out) {
   return PSPW_OK;
 }
 
-#define SOLVER_CHECK(call, what)                                              \
-  do {                                                                        \
-    cusolverStatus_t _s = (call);                                             \
-    if (_s != CUSOLVER_STATUS_SUCCESS) return fail(PSPW_ERR_CUDA, what);      \
+// a failed cuSOLVER call reports its status and the thread's pending CUDA
+// error (a library call fails with EXECUTION_FAILED when one is pending)
+#define SOLVER_CHECK(call, what)                                                        \
+  do {                                                                                  \
+    cusolverStatus_t _s = (call);                                                       \
+    if (_s != CUSOLVER_STATUS_SUCCESS)                                                  \
+      return fail(PSPW_ERR_CUDA, std::string(what) + ": cusolver status " +             \
+                                     std::to_string((int)_s) + ", pending CUDA error: " + \
+                                     cudaGetErrorString(cudaPeekAtLastError()));        \
   } while (0)
 
 __global__ void k_symmetrize(double2 *v, int ldv, int n) {

@@ -761,7 +761,10 @@ int pspw_scf_create(pspw_cell *c, int ng, const int *n1, const int *n2, const in
          cudaMemcpy(s->d_glast, glast.data(), ng, cudaMemcpyHostToDevice) == cudaSuccess &&
          cudaMemcpy(s->d_g, g, sizeof(double) * ng, cudaMemcpyHostToDevice) == cudaSuccess &&
          cudaMemcpy(s->d_vp, vp.data(), sizeof(double2) * ng, cudaMemcpyHostToDevice) == cudaSuccess &&
-         cudaMemcpy(s->d_rp, rp.data(), sizeof(double2) * ng, cudaMemcpyHostToDevice) == cudaSuccess;
+         cudaMemcpy(s->d_rp, rp.data(), sizeof(double2) * ng, cudaMemcpyHostToDevice) == cudaSuccess &&
+         // the copies' DMA lands before any kernel on the (non-blocking)
+         // cell streams reads the tables
+         cudaStreamSynchronize(cudaStreamLegacy) == cudaSuccess;
   if (!ok) {
     pspw_scf_destroy(s);
     return fail(PSPW_ERR_OOM, "scf_create: device memory");
