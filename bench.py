@@ -46,6 +46,8 @@ sys.path.insert(0, os.path.join(ROOT, "ffr-pspw-dft-c_b200"))
 import numpy as np  # noqa: E402
 
 DEGREE = 10
+# --nl-overlap values: the cell's PSPW_OVERLAP_* modes
+OVERLAP_MODES = {"auto": 0, "on": 1, "off": 2}
 LB, UB = 0.5, 16.0  # filter window (Ha) for the Si64 cell's spectrum
 METRIC = "Hpsi GB/s (algorithmic, FP32 byte model; Chebyshev filter degree 10)"
 WORKLOAD = ("Chebyshev filter (degree 10, chebyfilt.cpp) on Si64: 64 atoms, a=20.52 bohr, "
@@ -300,6 +302,7 @@ def run_row(args, rank, world, local_rank):
     if w["kind"] == "scf":
         n_it = args.warmup + args.steps
         S = System(_write_row_input(os.path.join(tmp, "engine"), w, n_it), device=local_rank)
+        S.cell().set_nl_overlap(OVERLAP_MODES[args.nl_overlap])
         S.cheby_scf(filter_prec=prec)  # warm-up run (allocations, first-touch)
         replica.barrier()
         clocks.start()
@@ -931,6 +934,7 @@ def run_engine(args, rank, world, local_rank):
     dev = torch.device("cuda", local_rank)
     w = workloads.workload(args.workload)
     cell = workloads.make_cell(w, device=local_rank)
+    cell.set_nl_overlap(OVERLAP_MODES[args.nl_overlap])
     sizes = cell.sizes()
     psi = w["psi"]
     ngw, nb = psi.shape
@@ -1179,6 +1183,9 @@ def main():
     ap.add_argument("--prec", default="f32", choices=["f32", "f64"])
     ap.add_argument("--workload", default="si64")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--nl-overlap", default="auto", choices=sorted(OVERLAP_MODES),
+                    help="projection concurrent with the FFT passes (on), after them (off), "
+                         "or the engine's per-precision default (auto)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-fp64-line", action="store_true",
                     help="si64/si216: skip the complex128 filter timed beside the FP32 one")

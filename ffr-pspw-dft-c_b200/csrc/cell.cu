@@ -704,6 +704,13 @@ int pspw_cell_set_nl_path(pspw_cell *c, int path) {
   return PSPW_OK;
 }
 
+int pspw_cell_set_nl_overlap(pspw_cell *c, int mode) {
+  if (!c || mode < PSPW_OVERLAP_AUTO || mode > PSPW_OVERLAP_OFF)
+    return fail(PSPW_ERR_ARG, "set_nl_overlap: bad argument");
+  c->nl_overlap = mode;
+  return PSPW_OK;
+}
+
 int pspw_cell_check_device_wait(pspw_cell *c, int complete) {
   if (!c) return fail(PSPW_ERR_ARG, "check_device_wait: null cell");
   PSPW_CUDA(cudaSetDevice(c->device));

@@ -164,7 +164,8 @@ struct pspw_cell {
   int ngwx = 0;
   double tpiba2 = 0.0;
   int band_batch = 0;
-  int nl_path = 0;  // PSPW_NL_AUTO / _SIMT / _TENSOR_CORE
+  int nl_path = 0;     // PSPW_NL_AUTO / _SIMT / _TENSOR_CORE
+  int nl_overlap = 0;  // PSPW_OVERLAP_AUTO / _ON / _OFF
   pspw::Basis basis;
   pspw::Projectors proj;
   double *d_veff64 = nullptr;  // V_eff / NNR on the grid (forward-FFT scale folded in)

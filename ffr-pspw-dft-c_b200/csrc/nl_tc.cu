@@ -308,54 +308,57 @@ __global__ void __launch_bounds__(kThreadsP) k_proj_tc(const float2 *__restrict_
 // Reduction of the projection slices, written as the B' operand tiles of the
 // back-projection: tile (band tile bt, atom step s) holds ncolN = nbt*2L rows
 // x 16 fp32 (8 atoms x re/im), hi then lo.  Every element of every tile is
-// written (zeros outside nb x nat).  One warp per (bt, s, band, lm, pair of
-// atoms): lane l sums slices l, l+32, ... and a fixed shuffle tree adds the
-// lanes, so the result does not depend on scheduling.
+// written (zeros outside nb x nat).
+// grid (ceil(4 nsa / 32), nbtiles * nbt * L); 128 threads.  Block y is one
+// (band, lm); lane l of warp q serves atom pair 32 blockIdx.x + l (atoms
+// 2 pair, 2 pair + 1) over slices q, q + 4, ..., so a warp reads whole rows
+// of part; the four partial sums are added in the order q = 0..3, so the
+// result does not depend on scheduling.
+constexpr int kWtWarps = 4;
 template <int L>
-__global__ void k_proj_tc_wtiles(const float *__restrict__ part, int nsplit, int nb, int nat,
-                                 const float *__restrict__ w, int nbt, int nsa, int total,
-                                 float *__restrict__ wt) {
+__global__ void __launch_bounds__(32 * kWtWarps) k_proj_tc_wtiles(
+    const float *__restrict__ part, int nsplit, int nb, int nat, const float *__restrict__ w,
+    int nbt, int nsa, float *__restrict__ wt) {
   constexpr int per = 2 * L;
-  const int item = (int)((blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5);
-  const int lane = threadIdx.x & 31;
-  if (item >= total) return;
-  int t = item;
-  const int c = t & 3;
-  t >>= 2;
-  const int lm = t % L;
-  t /= L;
-  const int bl = t % nbt;
-  t /= nbt;
-  const int s = t % nsa;
-  const int bt = t / nsa;
-  const int b = bt * nbt + bl;
+  __shared__ float4 ps[kWtWarps][32];
+  const int q = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int pair = blockIdx.x * 32 + lane;
+  const int lm = blockIdx.y % L, b = blockIdx.y / L;
+  const int a0 = 2 * pair;
   const int Mtot = nb * per;
-  const int a0 = 8 * s + 2 * c;
   // x = (Re, Im) of atom a0, (Re, Im) of atom a0 + 1
-  float x[4] = {0.f, 0.f, 0.f, 0.f};
-  if (b < nb) {
-    const int mre = b * per + 2 * lm;
-    for (int sl = lane; sl < nsplit; sl += 32) {
-      const float *p0 = part + ((size_t)sl * Mtot + mre) * nat;
-      const float *p1 = p0 + nat;
-      if (a0 < nat) {
-        x[0] += p0[a0];
-        x[1] += p1[a0];
-      }
-      if (a0 + 1 < nat) {
-        x[2] += p0[a0 + 1];
-        x[3] += p1[a0 + 1];
+  float4 x = make_float4(0.f, 0.f, 0.f, 0.f);
+  if (b < nb && a0 < nat) {
+    const bool two = a0 + 1 < nat;
+    const size_t rs = (size_t)Mtot * nat;  // slice stride
+    const float *p0 = part + (size_t)(b * per + 2 * lm) * nat + a0;
+#pragma unroll 4
+    for (int sl = q; sl < nsplit; sl += kWtWarps) {
+      const float *r0 = p0 + sl * rs, *r1 = r0 + nat;
+      x.x += r0[0];
+      x.y += r1[0];
+      if (two) {
+        x.z += r0[1];
+        x.w += r1[1];
       }
     }
   }
+  ps[q][lane] = x;
+  __syncthreads();
+  if (q != 0 || pair >= 4 * nsa) return;
 #pragma unroll
-  for (int o = 16; o > 0; o >>= 1)
-#pragma unroll
-    for (int q = 0; q < 4; q++) x[q] += __shfl_xor_sync(0xffffffffu, x[q], o);
-  if (lane != 0) return;
+  for (int i = 1; i < kWtWarps; i++) {
+    const float4 y = ps[i][lane];
+    x.x += y.x;
+    x.y += y.y;
+    x.z += y.z;
+    x.w += y.w;
+  }
   const float w0 = a0 < nat ? w[a0 * L + lm] : 0.f;
   const float w1 = a0 + 1 < nat ? w[(a0 + 1) * L + lm] : 0.f;
-  const float2 W0 = make_float2(w0 * x[0], w0 * x[1]), W1 = make_float2(w1 * x[2], w1 * x[3]);
+  const float2 W0 = make_float2(w0 * x.x, w0 * x.y), W1 = make_float2(w1 * x.z, w1 * x.w);
+  const int s = pair >> 2, c = pair & 3;
+  const int bt = b / nbt, bl = b % nbt;
   const int ncolN = nbt * per;
   unsigned char *hi = reinterpret_cast<unsigned char *>(wt + ((size_t)bt * nsa + s) * ncolN * 32);
   unsigned char *lo = hi + ncolN * 64;
@@ -386,11 +389,13 @@ __device__ __forceinline__ void ld_band(uint32_t taddr, uint32_t *v) {
 // etb: per (G tile, 8 atoms), [128 x 16] hi then lo.  wt: see k_proj_tc_wtiles.
 // Epilogue thread (warp w, lane l): G row 32 (w % 4) + l, bands of half w / 4
 // of the band tile.
-template <int L>
+// PRE: the recurrence's other terms are in out already (stick pass), so the
+// epilogue only adds ca times the projector term.
+template <int L, bool PRE>
 __global__ void __launch_bounds__(kThreads) k_backproj_tc(
     const float *__restrict__ etb, const float *__restrict__ wt, int nsa, int ngw, int nb, int nbt,
     const float *__restrict__ pkga, float2 *out, int ldo, const float2 *__restrict__ in, int ldi,
-    const float2 *__restrict__ xm2, int ldx, float ca, float cb, float cg, bool pre, int *err) {
+    const float2 *__restrict__ xm2, int ldx, float ca, float cb, float cg, int *err) {
   constexpr int per = 2 * L;
   extern __shared__ __align__(1024) unsigned char sm[];
   __shared__ Sync sy;
@@ -450,47 +455,58 @@ __global__ void __launch_bounds__(kThreads) k_backproj_tc(
       pk[2] = p4.z;
       pk[3] = p4.w;
     }
-    // the first band's operands are fetched while the MMAs run
-    auto fetch = [&](int j, float2 &h, float2 &u, float2 &x) {
-      const int bl = bstart + j;
-      if (gv && bl < nbb) {
-        const size_t bb = (size_t)(b0 + bl);
-        h = out[bb * ldo + g];
-        if (cb != 0.f) u = in[bb * ldi + g];
-        if (cg != 0.f) x = xm2[bb * ldx + g];
+    // the operands of CH bands are loaded at once (the first CH while the
+    // MMAs run), so one memory latency covers CH bands
+    constexpr int CH = PRE ? 8 : 4;
+    float2 hv[CH], uv[CH], xv[CH];
+    auto fetch = [&](int j0) {
+#pragma unroll
+      for (int i = 0; i < CH; i++) {
+        const int bl = bstart + j0 + i;
+        hv[i] = uv[i] = xv[i] = make_float2(0.f, 0.f);
+        if (gv && j0 + i < nbh && bl < nbb) {
+          const size_t bb = (size_t)(b0 + bl);
+          hv[i] = out[bb * ldo + g];
+          if (!PRE && cb != 0.f) uv[i] = in[bb * ldi + g];
+          if (!PRE && cg != 0.f) xv[i] = xm2[bb * ldx + g];
+        }
       }
     };
-    float2 h = make_float2(0.f, 0.f), u = h, x = h;
-    fetch(0, h, u, x);
+    fetch(0);
     const bool ok = __all_sync(0xffffffffu, tc::mbar_wait_abort(&sy.done, 0, &sy.abort));
     tc::fence_after_sync();
     if (ok) {
-      for (int j = 0; j < nbh; j++) {
-        const float2 hc = h, uc = u, xc = x;
-        if (j + 1 < nbh) fetch(j + 1, h, u, x);
-        uint32_t v[per];
-        ld_band<per>(lane_base + (uint32_t)((bstart + j) * per), v);
-        float accr = 0.f, acci = 0.f;
+      for (int j0 = 0; j0 < nbh; j0 += CH) {
+        if (j0 > 0) fetch(j0);
 #pragma unroll
-        for (int l = 0; l < L; l++) {
-          accr += pk[l] * __uint_as_float(v[2 * l]);
-          acci += pk[l] * __uint_as_float(v[2 * l + 1]);
-        }
-        const int bl = bstart + j;
-        if (gv && bl < nbb && pre) {
-          // the recurrence's other terms are in out already (stick pass)
-          out[(size_t)(b0 + bl) * ldo + g] = make_float2(hc.x + ca * accr, hc.y + ca * acci);
-        } else if (gv && bl < nbb) {
-          float rr = ca * (hc.x + accr), ii = ca * (hc.y + acci);
-          if (cb != 0.f) {
-            rr += cb * uc.x;
-            ii += cb * uc.y;
+        for (int i = 0; i < CH; i++) {
+          const int j = j0 + i;
+          if (j >= nbh) break;  // block-uniform: the TMEM load below is warp-collective
+          uint32_t v[per];
+          ld_band<per>(lane_base + (uint32_t)((bstart + j) * per), v);
+          float accr = 0.f, acci = 0.f;
+#pragma unroll
+          for (int l = 0; l < L; l++) {
+            accr += pk[l] * __uint_as_float(v[2 * l]);
+            acci += pk[l] * __uint_as_float(v[2 * l + 1]);
           }
-          if (cg != 0.f) {
-            rr += cg * xc.x;
-            ii += cg * xc.y;
+          const int bl = bstart + j;
+          if (!gv || bl >= nbb) continue;
+          const float2 hc = hv[i];
+          if (PRE) {
+            out[(size_t)(b0 + bl) * ldo + g] = make_float2(hc.x + ca * accr, hc.y + ca * acci);
+          } else {
+            float rr = ca * (hc.x + accr), ii = ca * (hc.y + acci);
+            if (cb != 0.f) {
+              rr += cb * uv[i].x;
+              ii += cb * uv[i].y;
+            }
+            if (cg != 0.f) {
+              rr += cg * xv[i].x;
+              ii += cg * xv[i].y;
+            }
+            out[(size_t)(b0 + bl) * ldo + g] = make_float2(rr, ii);
           }
-          out[(size_t)(b0 + bl) * ldo + g] = make_float2(rr, ii);
         }
       }
     }
@@ -665,9 +681,9 @@ int launch_project(pspw_cell *c, const Shape &s, const float2 *psi, int ld, int 
   if (rc) return rc;
   k_proj_tc<L><<<dim3(mt, nsplit), kThreadsP, smem, c->stream>>>(
       psi, ld, ngw, nb, etp, pkga, s.nat, s.npad, kg, part, c->d_err);
-  const int total = s.nbtiles * s.nsa * s.nbt * L * 4;  // one warp each
-  k_proj_tc_wtiles<L><<<(total + 7) / 8, 256, 0, c->stream>>>(part, nsplit, nb, s.nat, pw,
-                                                              s.nbt, s.nsa, total, wt);
+  const dim3 wgrid((4 * s.nsa + 31) / 32, s.nbtiles * s.nbt * L);
+  k_proj_tc_wtiles<L><<<wgrid, 32 * kWtWarps, 0, c->stream>>>(part, nsplit, nb, s.nat, pw, s.nbt,
+                                                               s.nsa, wt);
   c->kernel_launches += 2;
   PSPW_CUDA(cudaGetLastError());
   return PSPW_OK;
@@ -678,12 +694,12 @@ int launch_back(pspw_cell *c, const Shape &s, const float *wt, const float *etb,
                 const float *pkga, int ngw, int nb, float2 *out, int ldo, const float2 *in,
                 int ldi, const float2 *xm2, int ldx, float a, float b, float g, bool pre) {
   const int smem = back_smem(s);
-  int rc = smem_allow_max(k_backproj_tc<L>);
+  auto kern = pre ? k_backproj_tc<L, true> : k_backproj_tc<L, false>;
+  int rc = smem_allow_max(kern);
   if (rc) return rc;
   dim3 grid((ngw + 127) / 128, s.nbtiles);
-  k_backproj_tc<L><<<grid, kThreads, smem, c->stream>>>(etb, wt, s.nsa, ngw, nb, s.nbt, pkga,
-                                                        out, ldo, in, ldi, xm2, ldx, a, b, g, pre,
-                                                        c->d_err);
+  kern<<<grid, kThreads, smem, c->stream>>>(etb, wt, s.nsa, ngw, nb, s.nbt, pkga, out, ldo, in,
+                                            ldi, xm2, ldx, a, b, g, c->d_err);
   c->kernel_launches++;
   PSPW_CUDA(cudaGetLastError());
   return PSPW_OK;

@@ -20,6 +20,9 @@ PREC_F32 = 1
 NL_AUTO = 0
 NL_SIMT = 1
 NL_TENSOR_CORE = 2
+OVERLAP_AUTO = 0
+OVERLAP_ON = 1
+OVERLAP_OFF = 2
 MIX_SIMPLE, MIX_KERKER, MIX_ANDERSON, MIX_PULAY, MIX_BROYDEN = 0, 1, 2, 3, 4
 
 OK = 0
@@ -62,6 +65,7 @@ SIGNATURES = {
     "pspw_cell_sizes": [_vp, _vp],
     "pspw_cell_set_band_batch": [_vp, _i],
     "pspw_cell_set_nl_path": [_vp, _i],
+    "pspw_cell_set_nl_overlap": [_vp, _i],
     "pspw_cell_check_device_wait": [_vp, _i],
     "pspw_apply_ham_block": [_vp, _vp, _vp, _i, _i],
     "pspw_apply_ham_block_dev": [_vp, _i, _vp, _vp, _i, _i, _i],

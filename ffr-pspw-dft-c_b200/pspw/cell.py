@@ -138,6 +138,11 @@ class Cell:
         """NL_AUTO / NL_SIMT / NL_TENSOR_CORE kernels for the FP32 projector GEMMs."""
         check(lib().pspw_cell_set_nl_path(self._h, int(path)))
 
+    def set_nl_overlap(self, mode):
+        """OVERLAP_AUTO / OVERLAP_ON / OVERLAP_OFF: the projection of H*psi
+        concurrent with the FFT passes or after them (same results)."""
+        check(lib().pspw_cell_set_nl_overlap(self._h, int(mode)))
+
     def check_device_wait(self, complete):
         """One bounded device-side barrier wait (the tensor-core kernels'
         kind); raises PspwError(TIMEOUT) when nothing completes it."""

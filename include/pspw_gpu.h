@@ -121,6 +121,16 @@ int pspw_cell_set_band_batch(pspw_cell *cell, int nbatch);
 #define PSPW_NL_TENSOR_CORE 2
 int pspw_cell_set_nl_path(pspw_cell *cell, int path);
 
+/* Whether the projection of H*psi runs on the cell's second stream,
+ * concurrently with the FFT passes (AUTO, ON), or after them on the cell
+ * stream (OFF); no reference counterpart.  Results do not depend on it (the
+ * same kernels run in the same order of arithmetic).  The allocation-free
+ * entry point always keeps one stream. */
+#define PSPW_OVERLAP_AUTO 0
+#define PSPW_OVERLAP_ON 1
+#define PSPW_OVERLAP_OFF 2
+int pspw_cell_set_nl_overlap(pspw_cell *cell, int mode);
+
 /* Check of the device timeout path (no reference counterpart).  Every
  * barrier wait in the engine's tensor-core kernels gives up after about one
  * second and raises the cell's error word, which the next call that

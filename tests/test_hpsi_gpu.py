@@ -15,8 +15,8 @@ if not torch.cuda.is_available():  # pragma: no cover
 
 import pspw_oracle as O  # noqa: E402
 from helpers import engine_cell_args, golden, oracle_cell, relmax  # noqa: E402
-from pspw import (NL_SIMT, NL_TENSOR_CORE, PREC_F32, PREC_F64, Cell, PspwError,  # noqa: E402
-                  basis_gamma, synth)
+from pspw import (NL_SIMT, NL_TENSOR_CORE, OVERLAP_AUTO, OVERLAP_OFF, OVERLAP_ON,  # noqa: E402
+                  PREC_F32, PREC_F64, Cell, PspwError, basis_gamma, synth)
 from pspw import workloads  # noqa: E402
 
 TOL64 = 1e-12
@@ -286,6 +286,38 @@ def test_si64_subset_parity_and_hermiticity():
     assert relmax(out, ref) < TOL64
     m = psi.conj().T @ out
     assert np.abs(m - m.conj().T).max() < 1e-12 * np.abs(m).max()
+
+
+@pytest.mark.parametrize("prec", [PREC_F32, PREC_F64])
+def test_projection_overlap_gives_identical_bits(prec):
+    """The projection concurrent with the FFT passes (second stream) or after
+    them: the same kernels in the same order of arithmetic, so the same bits;
+    the Si64 cell (64 atoms, 64^3 grid) with 24 bands, and the Chebyshev
+    filter, whose back-projection epilogue applies the recurrence."""
+    w = workloads.workload("si64")
+    cell = workloads.make_cell(w)
+    psi = w["psi"][:, :24]
+    ngw, nb = psi.shape
+    cdt = torch.complex64 if prec == PREC_F32 else torch.complex128
+    d_in = torch.from_numpy(np.ascontiguousarray(psi.T)).to(cdt).cuda()
+    outs, filt = [], []
+    for mode in (OVERLAP_ON, OVERLAP_OFF, OVERLAP_AUTO):
+        cell.set_nl_overlap(mode)
+        d_out = torch.zeros_like(d_in)
+        torch.cuda.synchronize()
+        cell.apply_ham_block_dev(d_in, d_out, ngw, ngw, nb, prec)
+        x = d_in.clone()
+        torch.cuda.synchronize()
+        cell.chebyfilt_dev(x, ngw, ngw, nb, 4, 0.5, 16.0, prec)
+        torch.cuda.synchronize()
+        outs.append(d_out.cpu())
+        filt.append(x.cpu())
+    for o in outs[1:]:
+        assert torch.equal(o, outs[0])
+    for f in filt[1:]:
+        assert torch.equal(f, filt[0])
+    with pytest.raises(PspwError):
+        cell.set_nl_overlap(3)
 
 
 def _hpsi32(cell, psi, ld=None):
