@@ -117,8 +117,9 @@ int eval_rho_psi_dev(pspw_cell *c, const double2 *dX, int ld, int ngw, int nx, c
   }
   PSPW_CUDA(cudaMemcpyAsync(dw, wband.data(), sizeof(double) * nx, cudaMemcpyHostToDevice, c->stream));
   if (B.fast) {
-    const FastGeo g{B.ncol, B.nxa, B.d_col_start, B.d_sg_ig, B.d_sg_z, B.d_sg_col, B.d_xa_list,
-                    B.d_col_x, B.d_col_y, B.d_xa_of_x};
+    const FastGeo g{B.ncol,    B.nxa,       B.d_col_start, B.d_sg_ig,
+                    B.d_sg_z,  B.d_sg_col,  B.d_xa_list,   B.d_col_x,
+                    B.d_col_y, B.d_xa_of_x, false,         B.d_sg_off};
     if ((rc = rho_fast<double>(c, g, dX, ld, m, nx, dw, d_rho))) return rc;
   } else if ((rc = rho_generic(c, dX, ld, m, nx, dw, d_rho))) {
     return rc;

@@ -236,7 +236,8 @@ int pspw_cell_destroy(pspw_cell *c) {
   if (c->stream2) cudaStreamSynchronize(c->stream2);
   if (c->stream_copy) cudaStreamSynchronize(c->stream_copy);
   Basis &B = c->basis;
-  void *ptrs[] = {B.d_col_start, B.d_sg_ig, B.d_sg_z, B.d_sg_col, B.d_col_of_xy, B.d_xa_list,
+  void *ptrs[] = {B.d_col_start, B.d_sg_ig, B.d_sg_z, B.d_sg_col, B.d_sg_off, B.d_col_of_xy,
+                  B.d_xa_list,
                   B.d_xa_of_x, B.d_kin64, B.d_kin32, B.d_xkg64, c->proj.d_eigr64, c->proj.d_eigr32,
                   c->proj.d_pkga64, c->proj.d_pkga32, c->proj.d_patom, c->proj.d_psp,
                   c->proj.d_plm, c->proj.d_pw64, c->proj.d_pw32, c->d_veff64, c->d_veff32,
@@ -394,11 +395,16 @@ int cell_create(pspw_cell **out, int device, int nr1, int nr2, int nr3, int ngw,
     return ca != cb ? ca < cb : gi3[a] < gi3[b];
   });
   std::vector<int> sg_ig(ngw), sg_z(ngw), sg_col(ngw);
+  std::vector<unsigned short> sg_off(ngw);
+  const int tile = stick_tile(nr3);
   for (int k = 0; k < ngw; k++) {
     const int ig = order[k];
     sg_ig[k] = ig;
     sg_z[k] = gi3[ig];
     sg_col[k] = col_of_xy[(size_t)gi1[ig] + (size_t)nr1 * gi2[ig]];
+    // below 2^16 on every compiled length (at most 16 x 129); the generic
+    // path does not read it
+    sg_off[k] = (unsigned short)std::min(65535, (sg_col[k] % tile) * (nr3 + 1) + sg_z[k]);
   }
   std::vector<int> xa_of_x(nr1, -1), xa_list;
   for (int k = 0; k < ncol; k++) xa_of_x[col_x[k]] = 0;
@@ -420,6 +426,7 @@ int cell_create(pspw_cell **out, int device, int nr1, int nr2, int nr3, int ngw,
   }
   if ((rc = upload(&B.d_col_start, col_start)) || (rc = upload(&B.d_sg_ig, sg_ig)) ||
       (rc = upload(&B.d_sg_z, sg_z)) || (rc = upload(&B.d_sg_col, sg_col)) ||
+      (rc = upload(&B.d_sg_off, sg_off)) ||
       (rc = upload(&B.d_col_of_xy, col_of_xy)) || (rc = upload(&B.d_xa_list, xa_list)) ||
       (rc = upload(&B.d_xa_of_x, xa_of_x)) || (rc = upload(&B.d_kin64, kin64)) ||
       (rc = upload(&B.d_xkg64, xkg64)) || (rc = upload(&B.d_wgrid, wgrid)) ||

@@ -38,6 +38,9 @@ struct Basis {
   int *d_sg_ig = nullptr;      // [ngw] G index (0-based, caller order)
   int *d_sg_z = nullptr;       // [ngw] i3 of that G
   int *d_sg_col = nullptr;     // [ngw] stick of that G
+  // [ngw] (stick mod stick_tile(n3)) * (n3 + 1) + i3: the G's offset in the
+  // register-FFT stick kernels' tile
+  unsigned short *d_sg_off = nullptr;
   int *d_col_of_xy = nullptr;  // [n1*n2] stick at (i1,i2) or -1
   int *d_xa_list = nullptr;    // [nxa] i1 of active x
   int *d_xa_of_x = nullptr;    // [n1] active index or -1

@@ -24,7 +24,7 @@ namespace fastpath {
 
 template <int NZ>
 struct StickCfg {
-  static constexpr int T1 = (2048 / NZ) < 1 ? 1 : ((2048 / NZ) > 32 ? 32 : (2048 / NZ));
+  static constexpr int T1 = stick_tile(NZ);
   static constexpr int LS = NZ + 1;
 };
 
@@ -54,7 +54,7 @@ __global__ void __launch_bounds__(256) k_sticks_inv(FastGeo g, const T *__restri
     for (int u = 0; u < U; u++) {
       const int k = kb + u * 256;
       ig[u] = k < k1 ? (g.ig_iota ? k : g.sg_ig[k]) : ngw_call;
-      off[u] = k < k1 ? (g.sg_col[k] - c0) * LS + g.sg_z[k] : 0;
+      off[u] = k < k1 ? g.sg_off[k] : 0;  // (sg_col[k] - c0) * LS + sg_z[k]
     }
     T v[U];
 #pragma unroll

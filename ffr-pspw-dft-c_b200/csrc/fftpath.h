@@ -7,6 +7,12 @@
 
 namespace pspw {
 
+// Sticks per block of the stick kernels for a z length nz (their tile of
+// sticks x (nz + 1) elements); the host's tile offsets use the same value.
+__host__ __device__ constexpr int stick_tile(int nz) {
+  return (2048 / nz) < 1 ? 1 : ((2048 / nz) > 32 ? 32 : (2048 / nz));
+}
+
 // What the stick/plane kernels read about the basis (device pointers).
 struct FastGeo {
   int ncol, nxa;
@@ -15,6 +21,12 @@ struct FastGeo {
   // sg_ig is the identity (the block is in stick order): the kernels use k
   // itself, so the psi loads do not wait for an index load
   bool ig_iota = false;
+  // [ngw] offset of G entry k in its block's tile of the stick kernels,
+  // (stick mod stick_tile(n3)) * (n3 + 1) + i3: k_sticks_inv's one 2-byte
+  // load instead of the stick and z loads (39 -> 34 registers).
+  // k_sticks_fwd keeps the two loads: with this one it took 40 registers
+  // instead of 32 and held 6 blocks per SM instead of 8.
+  const unsigned short *sg_off = nullptr;
 };
 
 // True when (n1, n2, n3) has compiled stick and plane kernels.

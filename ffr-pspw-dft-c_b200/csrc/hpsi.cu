@@ -877,8 +877,9 @@ int hpsi_apply(pspw_cell *c, const void *in_v, int ld_in, void *out_v, int ld_ou
   Geo geo{B.n1, B.n2, B.n3, B.ncol, B.nxa, B.ngw, B.d_col_start, B.d_sg_ig, B.d_sg_z,
           B.d_sg_col, B.d_col_of_xy, B.d_xa_list, B.d_xa_of_x};
   if (B.fast) {
-    const FastGeo fg{B.ncol, B.nxa, B.d_col_start, B.d_sg_ig, B.d_sg_z, B.d_sg_col, B.d_xa_list,
-                     B.d_col_x, B.d_col_y, B.d_xa_of_x, c->stick.active};
+    const FastGeo fg{B.ncol,    B.nxa,       B.d_col_start, B.d_sg_ig,
+                     B.d_sg_z,  B.d_sg_col,  B.d_xa_list,   B.d_col_x,
+                     B.d_col_y, B.d_xa_of_x, c->stick.active, B.d_sg_off};
     RecArg<T, R> ra;
     ra.on = true;
     ra.ca = (R)a;

@@ -65,23 +65,42 @@ __global__ void k_lanczos_next(const double2 *__restrict__ f, double2 *__restric
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
     vj[i] = make_double2(beta * f[i].x, beta * f[i].y);
 }
-__global__ void k_add_inplace(double2 *h, const double2 *__restrict__ s, int n) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i < n) h[i] = make_double2(h[i].x + s[i].x, h[i].y + s[i].y);
-}
 // y += x
 __global__ void k_axpy1(const double2 *__restrict__ x, double2 *y, size_t n) {
   for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
        i += (size_t)gridDim.x * blockDim.x)
     y[i] = make_double2(y[i].x + x[i].x, y[i].y + x[i].y);
 }
-__global__ void k_neg(const double2 *__restrict__ a, double2 *b, int n) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i < n) b[i] = make_double2(-a[i].x, -a[i].y);
+// f = x - V h over the nj columns of V (lanczos.cpp:60-70): one thread per
+// row, the columns summed in order
+__global__ void k_lz_sub(int n, int nj, const double2 *__restrict__ V, int ldv,
+                         const double2 *__restrict__ h, const double2 *__restrict__ x,
+                         double2 *__restrict__ f) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    double2 t = make_double2(0.0, 0.0);
+    for (int q = 0; q < nj; q++) cfma(t, V[(size_t)q * ldv + i], h[q]);
+    f[i] = make_double2(x[i].x - t.x, x[i].y - t.y);
+  }
 }
-__global__ void k_T_col(const double2 *__restrict__ h, double *T, int ldT, int j) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i <= j) T[(size_t)j * ldT + i] = h[i].x;
+// The end of Lanczos step j (lanczos.cpp:72-91): f -= V s, and (block 0)
+// h += s with column j of T = Re h, taken before the correction for the
+// first column (:36-38) and after it for the others (:89-91)
+__global__ void k_lz_update(int n, int nj, const double2 *__restrict__ V, int ldv, double2 *h,
+                            const double2 *__restrict__ s, double2 *f, double *T, int ldT,
+                            int j) {
+  if (blockIdx.x == 0)
+    for (int i = threadIdx.x; i < nj; i += blockDim.x) {
+      double2 hv = h[i];
+      if (j == 0) T[(size_t)j * ldT + i] = hv.x;
+      hv = make_double2(hv.x + s[i].x, hv.y + s[i].y);
+      h[i] = hv;
+      if (j > 0) T[(size_t)j * ldT + i] = hv.x;
+    }
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    double2 t = make_double2(0.0, 0.0);
+    for (int q = 0; q < nj; q++) cfma(t, V[(size_t)q * ldv + i], s[q]);
+    f[i] = make_double2(f[i].x - t.x, f[i].y - t.y);
+  }
 }
 
 inline int gridn(size_t n) { return (int)std::min<size_t>(4 * 148, (n + 255) / 256 + 1); }
@@ -528,19 +547,13 @@ int lanczos_dev(pspw_cell *c, double2 *v0, int ngw, int k, double *T_host, int l
       c->kernel_launches++;
     }
     if ((rc = apply_h(c, hprec, vj, Hv, ngw, 1))) return rc;
-    // h = V^H Hv; f = Hv - V h; s = V^H f; h += s; f -= V s (:60-87)
+    // h = V^H Hv; f = Hv - V h; s = V^H f; h += s; f -= V s (:60-87), four
+    // launches
     const int nj = j + 1;
-    if ((rc = zgemm<double>(c, 'C', nj, 1, ngw, kOne, V, ngw, Hv, ngw, kZero, h, nj)) ||
-        (rc = d2d(c, f, Hv, sizeof(double2) * ngw)) ||
-        (rc = zgemm<double>(c, 'N', ngw, 1, nj, kMOne, V, ngw, h, nj, kOne, f, ngw)) ||
-        (rc = zgemm<double>(c, 'C', nj, 1, ngw, kOne, V, ngw, f, ngw, kZero, s, nj)))
-      return rc;
-    // the first column of T takes h before its correction (:36-38), the
-    // others after it (:89-91)
-    if (j == 0) k_T_col<<<1, 256, 0, c->stream>>>(h, T, k, j);
-    k_add_inplace<<<(nj + 255) / 256, 256, 0, c->stream>>>(h, s, nj);
-    if ((rc = zgemm<double>(c, 'N', ngw, 1, nj, kMOne, V, ngw, s, nj, kOne, f, ngw))) return rc;
-    if (j > 0) k_T_col<<<(nj + 255) / 256, 256, 0, c->stream>>>(h, T, k, j);
+    if ((rc = zgemm<double>(c, 'C', nj, 1, ngw, kOne, V, ngw, Hv, ngw, kZero, h, nj))) return rc;
+    k_lz_sub<<<gridn(ngw), 256, 0, c->stream>>>(ngw, nj, V, ngw, h, Hv, f);
+    if ((rc = zgemm<double>(c, 'C', nj, 1, ngw, kOne, V, ngw, f, ngw, kZero, s, nj))) return rc;
+    k_lz_update<<<gridn(ngw), 256, 0, c->stream>>>(ngw, nj, V, ngw, h, s, f, T, k, j);
     c->kernel_launches += 2;
   }
   PSPW_CUDA(cudaGetLastError());
