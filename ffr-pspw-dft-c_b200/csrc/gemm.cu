@@ -315,14 +315,18 @@ template <bool CONJ_A, int WM, int WN>
 __global__ void __launch_bounds__(Dm<WM, WN>::THREADS, Dm<WM, WN>::MIN_BLOCKS)
     k_zgemm_dmma(int m, int n, int k, double2 alpha, const double2 *__restrict__ A, int lda,
                  const double2 *__restrict__ B, int ldb, double2 beta, double2 *C, int ldc,
-                 int kchunk, double2 *__restrict__ part) {
+                 int kchunk, double2 *__restrict__ part, int tri) {
   using D = Dm<WM, WN>;
   constexpr int BM = D::BM, BN = D::BN, BK = D::BK, STAGES = D::STAGES, THREADS = D::THREADS;
   constexpr int LDK = D::LDK, LDM = D::LDM, A_ELEMS = D::A_ELEMS, STAGE = D::STAGE;
   extern __shared__ __align__(16) double2 sm[];
   const int m0 = blockIdx.x * BM, n0 = blockIdx.y * BN;
-  const int kb = blockIdx.z * kchunk, ke = min(k, kb + kchunk);
-  const int nkt = ke > kb ? (ke - kb + BK - 1) / BK : 0;
+  const int kb = blockIdx.z * kchunk;
+  // kZgemmUpperB: rows of B past n0 + BN - 1 are zero in this column tile
+  const int ke = min(min(k, kb + kchunk), tri == kZgemmUpperB ? n0 + BN : k);
+  // kZgemmUpperC: a tile wholly below the diagonal keeps a zero product
+  const bool skip = tri == kZgemmUpperC && m0 >= n0 + BN;
+  const int nkt = ke > kb && !skip ? (ke - kb + BK - 1) / BK : 0;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int wm = (warp % WM) * 32, wn = (warp / WM) * 16;
   const int g = lane >> 2, t = lane & 3;
@@ -443,7 +447,7 @@ static int sm_count_now() {
 template <int WM, int WN>
 static int launch_dmma(pspw_cell *c, bool conj, int m, int n, int k, double2 alpha,
                        const double2 *A, int lda, const double2 *B, int ldb, double2 beta,
-                       double2 *C, int ldc) {
+                       double2 *C, int ldc, int tri) {
   using D = Dm<WM, WN>;
   cudaStream_t st = c->stream;
   const int mt = (m + D::BM - 1) / D::BM, nt = (n + D::BN - 1) / D::BN;
@@ -468,7 +472,7 @@ static int launch_dmma(pspw_cell *c, bool conj, int m, int n, int k, double2 alp
   cudaEvent_t ev;
   timing_begin(c, kFamGemm, &ev);
   kern<<<dim3(mt, nt, nsplit), D::THREADS, D::SMEM, st>>>(m, n, k, alpha, A, lda, B, ldb, beta,
-                                                          C, ldc, kchunk, part);
+                                                          C, ldc, kchunk, part, tri);
   c->kernel_launches++;
   if (nsplit > 1) {
     k_zgemm_reduce<double><<<std::min<size_t>(4 * 148, ((size_t)m * n + 255) / 256), 256, 0,
@@ -484,16 +488,28 @@ static int launch_dmma(pspw_cell *c, bool conj, int m, int n, int k, double2 alp
 // least (ties go to the larger tile, which re-reads its operands less)
 static int zgemm_dmma(pspw_cell *c, bool conj, int m, int n, int k, double2 alpha,
                       const double2 *A, int lda, const double2 *B, int ldb, double2 beta,
-                      double2 *C, int ldc) {
+                      double2 *C, int ldc, int tri = 0) {
   auto padded = [&](int bm, int bn) {
     return (double)((m + bm - 1) / bm * bm) * (double)((n + bn - 1) / bn * bn);
   };
   const double a64 = padded(64, 64), a6432 = padded(64, 32), a32 = padded(32, 32);
   if (a64 <= a6432 && a64 <= a32)
-    return launch_dmma<2, 4>(c, conj, m, n, k, alpha, A, lda, B, ldb, beta, C, ldc);
+    return launch_dmma<2, 4>(c, conj, m, n, k, alpha, A, lda, B, ldb, beta, C, ldc, tri);
   if (a6432 <= a32)
-    return launch_dmma<2, 2>(c, conj, m, n, k, alpha, A, lda, B, ldb, beta, C, ldc);
-  return launch_dmma<1, 2>(c, conj, m, n, k, alpha, A, lda, B, ldb, beta, C, ldc);
+    return launch_dmma<2, 2>(c, conj, m, n, k, alpha, A, lda, B, ldb, beta, C, ldc, tri);
+  return launch_dmma<1, 2>(c, conj, m, n, k, alpha, A, lda, B, ldb, beta, C, ldc, tri);
+}
+
+int zgemm_tri(pspw_cell *c, char opa, int tri, int m, int n, int k, double2 alpha,
+              const double2 *A, int lda, const double2 *B, int ldb, double2 beta, double2 *C,
+              int ldc) {
+  if (opa != 'N' && opa != 'n' && opa != 'C' && opa != 'c')
+    return fail(PSPW_ERR_ARG, "zgemm_tri: op(A) must be 'N' or 'C'");
+  if (tri == kZgemmUpperC && m != n) return fail(PSPW_ERR_ARG, "zgemm_tri: C must be square");
+  if (n <= 8 || m <= 0 || k <= 0)  // the narrow kernels: the full product
+    return zgemm<double>(c, opa, m, n, k, alpha, A, lda, B, ldb, beta, C, ldc);
+  return zgemm_dmma(c, opa == 'C' || opa == 'c', m, n, k, alpha, A, lda, B, ldb, beta, C, ldc,
+                    tri);
 }
 
 template <typename R>

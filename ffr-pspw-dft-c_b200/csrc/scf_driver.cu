@@ -93,7 +93,11 @@ double induced_norm_mat(const double *A, int lda, int N) {
 // multiplies the eigen-components of its block by factors that span orders
 // of magnitude, so the filtered columns are nearly orthogonal but of very
 // different lengths, an ill-conditioning that the scaling removes.
-// G, U: n x n scratch (ld n); dn: n doubles; stat: 2 doubles; W: ngw x n.
+// Both passes are enqueued before the host reads the two pivot statuses
+// (one synchronisation): the first pass writes W only, so X is intact for
+// the Householder fallback, and a failed first factorisation leaves U as it
+// was, which only makes the second pass's numbers meaningless.
+// G, U: n x n scratch (ld n); dn: n doubles; stat: 4 doubles; W: ngw x n.
 int span_orthonormalize(pspw_cell *c, double2 *X, int ngw, int n, double2 *G, double2 *U,
                         double *dn, double *stat, double2 *W, int *info) {
   const double2 one = make_double2(1.0, 0.0), zero = make_double2(0.0, 0.0);
@@ -106,16 +110,23 @@ int span_orthonormalize(pspw_cell *c, double2 *X, int ngw, int n, double2 *G, do
     return dev_ortho_qr(c, X, ngw, ngw, n, info);
   }
   for (int pass = 0; pass < 2; pass++) {
-    double2 *src = pass == 0 ? X : W, *dst = pass == 0 ? W : X;
-    if ((rc = zgemm<double>(c, 'C', n, n, ngw, one, src, ngw, src, ngw, zero, G, n))) return rc;
-    if ((rc = dev_chol_inv_upper(c, G, n, n, U, n, stat))) return rc;
-    double h[2];
-    PSPW_CUDA(cudaMemcpyAsync(h, stat, sizeof h, cudaMemcpyDeviceToHost, c->stream));
-    PSPW_CUDA(cudaStreamSynchronize(c->stream));
-    const bool fallback = h[0] != 0.0 || (pass == 0 && !(h[1] <= 1.0e6));
-    if (fallback) return dev_ortho_qr(c, X, ngw, ngw, n, info);
-    if ((rc = zgemm<double>(c, 'N', ngw, n, n, one, src, ngw, U, n, zero, dst, ngw))) return rc;
+    double2 *src = pass == 0 ? X : W;
+    // the factorisation reads the upper triangle of G only
+    if ((rc = zgemm_tri(c, 'C', kZgemmUpperC, n, n, ngw, one, src, ngw, src, ngw, zero, G, n)))
+      return rc;
+    if ((rc = dev_chol_inv_upper(c, G, n, n, U, n, stat + 2 * pass))) return rc;
+    // U^-1 is upper triangular (zeros stored below the diagonal)
+    if (pass == 0 &&
+        (rc = zgemm_tri(c, 'N', kZgemmUpperB, ngw, n, n, one, X, ngw, U, n, zero, W, ngw)))
+      return rc;
   }
+  double h[4];
+  PSPW_CUDA(cudaMemcpyAsync(h, stat, sizeof h, cudaMemcpyDeviceToHost, c->stream));
+  PSPW_CUDA(cudaStreamSynchronize(c->stream));
+  const bool fallback = h[0] != 0.0 || !(h[1] <= 1.0e6) || h[2] != 0.0;
+  if (fallback) return dev_ortho_qr(c, X, ngw, ngw, n, info);
+  if ((rc = zgemm_tri(c, 'N', kZgemmUpperB, ngw, n, n, one, W, ngw, U, n, zero, X, ngw)))
+    return rc;
   *info = 0;
   return PSPW_OK;
 }
@@ -130,7 +141,7 @@ int ortho_span_dev(pspw_cell *c, double2 *X, int ngw, int n, int *info) {
   if ((rc = ws_reserve(c, kWsSpan, sizeof(double2) * (size_t)n * n, (void **)&G)) ||
       (rc = ws_reserve(c, kWsSpan + 1, sizeof(double2) * (size_t)n * n, (void **)&U)) ||
       (rc = ws_reserve(c, kWsSpan + 2, sizeof(double2) * (size_t)ngw * n, (void **)&W)) ||
-      (rc = ws_reserve(c, kWsSpan + 3, sizeof(double) * ((size_t)n + 2), (void **)&dn)))
+      (rc = ws_reserve(c, kWsSpan + 3, sizeof(double) * ((size_t)n + 4), (void **)&dn)))
     return rc;
   stat = dn + n;
   return span_orthonormalize(c, X, ngw, n, G, U, dn, stat, W, info);
@@ -220,7 +231,7 @@ extern "C" int pspw_cheby_scf(pspw_scf *s, const pspw_scf_params *p, const doubl
   double *veff, *rho, *wT, *dprec, *dcn, *dstat;
   if (!mem.get(&X, (size_t)ngw * nx2) || !mem.get(&dcn, nx2) || !mem.get(&HX, (size_t)ngw * nx2) ||
       !mem.get(&T, (size_t)nx2 * nx2) || !mem.get(&dU, (size_t)nx2 * nx2) ||
-      !mem.get(&dstat, 2) || !mem.get(&dv0, ngw) || !mem.get(&df, ngw) ||
+      !mem.get(&dstat, 4) || !mem.get(&dv0, ngw) || !mem.get(&df, ngw) ||
       !mem.get(&dRT, (size_t)k * k) || !mem.get(&veff, nnr) || !mem.get(&rho, nnr) ||
       !mem.get(&wT, std::max(k, nx2)) || !mem.get(&dprec, ngw) ||
       (fprec == PSPW_PREC_F32 && !mem.get(&Xf, (size_t)ngw * nx2)))
