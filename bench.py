@@ -1303,6 +1303,16 @@ def main():
         torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
                                              device_id=torch.device("cuda", local_rank))
     r = run_engine(args, rank, world, local_rank)
+    if args.workload != "si64":  # the line names the cell it ran on
+        s = r["sizes"]
+        grid = [s["n1"], s["n2"], s["n3"]]
+        config = dict(config, grid=grid, ngw=r["ngw"], bands=r["nb"],
+                      global_batch=r["nb"] * world,
+                      cell=f"{args.workload} diamond-cubic, synthetic pseudopotential",
+                      workload=(f"Chebyshev filter (degree {DEGREE}, chebyfilt.cpp) on "
+                                f"{args.workload}: {s['nat']} atoms, grid "
+                                f"{grid[0]}x{grid[1]}x{grid[2]}, NGW {r['ngw']}, {r['nb']} "
+                                f"bands, s+p KB projectors"))
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         ref, why = reference_sample(steps=1, warmup=0)
