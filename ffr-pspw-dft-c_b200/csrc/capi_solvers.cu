@@ -82,9 +82,12 @@ constexpr int kSlotE = kWsEnl;
 }  // namespace
 
 // EvalRhoPsi.cpp:83-157 on a device block (ld >= ngw): the charge check and
-// EKIN from column sums, then d_rho += sum_i wkpt focc_i |psi_i(r)|^2 / omega
+// EKIN from column sums, and d_rho += sum_i wkpt focc_i |psi_i(r)|^2 / omega
 // with the scatter stopping at ig < ngw - 1 (EvalRhoPsi.cpp:117).
-// *ekin += the kinetic energy (x TPIBA2).
+// *ekin += the kinetic energy (x TPIBA2).  The band weights do not depend on
+// the sums, so the sums and the density pass are enqueued together and the
+// host reads the sums once, after both (on a wrong charge d_rho has been
+// accumulated when the error returns).
 int eval_rho_psi_dev(pspw_cell *c, const double2 *dX, int ld, int ngw, int nx, const double *focc,
                      double wkpt, double omega, double *d_rho, double *ekin) {
   const Basis &B = c->basis;
@@ -94,14 +97,25 @@ int eval_rho_psi_dev(pspw_cell *c, const double2 *dX, int ld, int ngw, int nx, c
   if ((rc = ws_reserve(c, kSlotB, sizeof(double) * 2 * (size_t)nx, (void **)&dsum)) ||
       (rc = ws_reserve(c, kSlotD, sizeof(double) * (size_t)nx, (void **)&dw)))
     return rc;
+  std::vector<double> wband(nx);
+  for (int i = 0; i < nx; i++) wband[i] = (wkpt * focc[i]) / omega;
+  PSPW_CUDA(cudaMemcpyAsync(dw, wband.data(), sizeof(double) * nx, cudaMemcpyHostToDevice, c->stream));
   k_charge_sums<<<nx, 256, 0, c->stream>>>(dX, ld, m, B.d_xkg64, dsum, dsum + nx);
   c->kernel_launches++;
+  if (B.fast) {
+    const FastGeo g{B.ncol,    B.nxa,       B.d_col_start, B.d_sg_ig,
+                    B.d_sg_z,  B.d_sg_col,  B.d_xa_list,   B.d_col_x,
+                    B.d_col_y, B.d_xa_of_x, false,         B.d_sg_off};
+    if ((rc = rho_fast<double>(c, g, dX, ld, m, nx, dw, d_rho))) return rc;
+  } else if ((rc = rho_generic(c, dX, ld, m, nx, dw, d_rho))) {
+    return rc;
+  }
+  // (a copy into pageable memory returns when it is done: the one wait)
   std::vector<double> sums(2 * (size_t)nx);
   PSPW_CUDA(cudaMemcpyAsync(sums.data(), dsum, sizeof(double) * 2 * nx, cudaMemcpyDeviceToHost,
                             c->stream));
   if ((rc = sync(c))) return rc;
   double xkin = 0.0;
-  std::vector<double> wband(nx);
   for (int i = 0; i < nx; i++) {
     const double ss = sums[i];
     if (std::fabs(ss - 1.0) > 6.e-3) {  // EvalRhoPsi.cpp:129-133
@@ -113,18 +127,7 @@ int eval_rho_psi_dev(pspw_cell *c, const double2 *dX, int ld, int ngw, int nx, c
     }
     const double wdotf = wkpt * focc[i];
     xkin = xkin + sums[nx + i] * (wdotf * 0.5);
-    wband[i] = wdotf / omega;
   }
-  PSPW_CUDA(cudaMemcpyAsync(dw, wband.data(), sizeof(double) * nx, cudaMemcpyHostToDevice, c->stream));
-  if (B.fast) {
-    const FastGeo g{B.ncol,    B.nxa,       B.d_col_start, B.d_sg_ig,
-                    B.d_sg_z,  B.d_sg_col,  B.d_xa_list,   B.d_col_x,
-                    B.d_col_y, B.d_xa_of_x, false,         B.d_sg_off};
-    if ((rc = rho_fast<double>(c, g, dX, ld, m, nx, dw, d_rho))) return rc;
-  } else if ((rc = rho_generic(c, dX, ld, m, nx, dw, d_rho))) {
-    return rc;
-  }
-  if ((rc = sync(c))) return rc;  // wband lives on the host stack
   if (ekin) *ekin = *ekin + xkin * c->tpiba2;  // EvalRhoPsi.cpp:154
   return PSPW_OK;
 }
