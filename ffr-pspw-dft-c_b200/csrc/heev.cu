@@ -98,9 +98,11 @@ __device__ __forceinline__ void warp_sum2(double &a, double &b) {
 constexpr int kTR = 640;                      // threads of the reduction block
 constexpr int kTRW = kTR / 32;                // its warps; the last one steers
 constexpr int kSteer = kTRW - 1;
-constexpr int kGrp = 4;                       // threads per trailing row
+constexpr int kGrp = 4;                       // threads per trailing row (product)
+constexpr int kUpd = 8;                       // threads per pair of rows (update)
 constexpr int kColsL = (kHeevMax + 31) / 32;  // column entries per lane
 static_assert(kSteer * 32 / kGrp >= kHeevMax, "one row group per trailing row");
+static_assert(kSteer * 32 / kUpd >= (kHeevMax - 1) / 2 + 1, "one update group per pair of rows");
 
 __device__ __forceinline__ double2 cfma_(double2 a, double2 b, double2 c) {  // c + a b
   c.x = fma(a.x, b.x, c.x);
@@ -300,13 +302,25 @@ __global__ void __launch_bounds__(kTR, 1)
       }
       __syncthreads();
       // A22 -= v w^H + w v^H on rows k+2.., columns k+2..i (column k+1 is
-      // the steering warp's)
-      if (row && g > 0) {
-        double2 *Li = L + lp(i, 0);
-        for (int j = k1 + 1 + sub; j <= i; j += kGrp) {
-          double2 a = her2_(Li[j], vi, wi, v[j], w[j]);
-          if (j == i) a.y = 0.0;
-          Li[j] = a;
+      // the steering warp's).  The rows go in pairs (k+2+p, n-1-p), whose
+      // lengths add up to m, to groups of kUpd threads, so every group has
+      // the same work; one row per group would leave the longest row's
+      // group alone on the critical path while the others wait at the
+      // barrier.  Each element gets the same update as in any order.
+      if (warp != kSteer) {
+        const int p = tid / kUpd, su = tid % kUpd;
+        const int r1 = k1 + 1 + p, r2 = n - 1 - p;
+        if (r1 <= r2) {
+          const int len1 = r1 - k1, len = r1 == r2 ? len1 : m;  // elements of the pair
+          const double2 v1 = v[r1], w1 = w[r1], v2 = v[r2], w2 = w[r2];
+          for (int e = su; e < len; e += kUpd) {
+            const bool first = e < len1;
+            const int r = first ? r1 : r2, j = k1 + 1 + (first ? e : e - len1);
+            double2 *a = L + lp(r, j);
+            double2 x = her2_(*a, first ? v1 : v2, first ? w1 : w2, v[j], w[j]);
+            if (j == r) x.y = 0.0;
+            *a = x;
+          }
         }
       }
     }
